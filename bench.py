@@ -1,0 +1,319 @@
+#!/usr/bin/env python
+"""Throughput of the DepoTransform signal-simulation path on B200.
+
+Workload (default): the full-APA plain forward -- three planes (U/V 800 wires
+at 4.67 mm, W 960 wires at 4.79 mm, +-35.7 deg), 6000 ticks, 20 seeded
+straight muon tracks with one depo per 0.1 mm (~520k depos), drift + diffusion
++ erf patches + FFT convolution + frame.  One step = one event through
+DepoTransform::operator() with its depos already resident in HBM.
+
+Output: one JSON line (rank 0).  Multi-GPU: one process per GPU (torchrun),
+every rank simulates its own event (events are independent: weak scaling, no
+data-path collective).
+
+``--impl reference`` times the CPU restatement of the reference (oracle/,
+FP32, one event per step) on the host cores instead.
+"""
+
+import argparse
+import csv
+import importlib
+import io
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "depos/s fwd & fwd+adjoint on 1 B200 vs plain GPU fwd, rel-L2≤1e-5 vs FP64"
+UNIT = "depos/s"
+
+
+def load_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return d.get("hbm_gbs", 6650.0), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.p = None
+
+    def start(self):
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.Q,
+                                       "--format=csv,noheader,nounits", "-lms", "200"],
+                                      stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return None
+        self.p.terminate()
+        try:
+            out, _ = self.p.communicate(timeout=5)
+        except Exception:
+            self.p.kill()
+            out, _ = self.p.communicate()
+        rows = [r for r in csv.reader(io.StringIO(out)) if len(r) >= 9]
+        if not rows:
+            return None
+        sm = [float(r[1]) for r in rows if r[1].strip().replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].strip().replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = set()
+        for r in rows:
+            for k, nm in enumerate(names):
+                if r[5 + k].strip().lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(rows)}
+
+
+def dist_setup(args):
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+def stage_bytes(wins, cfg, n_depos, G=11):
+    """Per-stage algorithmic bytes of one event (sum over planes):
+    raster    32 B patch record per depo-plane + the group grids written once
+    time_fft  group grids read + packed spectra written
+    wire_conv group spectra read + one plane spectrum written
+    inverse   plane spectrum read + frame window written."""
+    nticks = int(round(cfg["readout_time"] / cfg["tick"]))
+    out = {"raster": 0, "time_fft": 0, "wire_conv": 0, "inverse_fft+frame": 0}
+    for w, pl in zip(wins, cfg["planes"]):
+        if w["ndepos_added"] == 0:
+            continue
+        N = w["nt_gpu"]
+        M = N // 2
+        nin = w["charge_rows"]
+        nout = nin + 2 * w["npad"]
+        grid = G * nin * N * 4
+        out["raster"] += 32 * n_depos + grid
+        out["time_fft"] += 2 * grid
+        out["wire_conv"] += G * nin * M * 8 + nout * M * 8
+        rows = max(0, min(pl["nwires"], w["end_ch"]) - max(0, w["start_ch"]))
+        cols = max(0, min(nticks, w["end_tick"]) - max(0, w["start_tick"]))
+        out["inverse_fft+frame"] += nout * M * 8 + rows * cols * 4
+    return out
+
+
+def run_b200(args):
+    import torch
+    rank, world, local = dist_setup(args)
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    wct = importlib.import_module("wire-cell-toolkit_b200")
+    synth = importlib.import_module("wire-cell-toolkit_b200.synth")
+    cfg = synth.apa_config()
+    depos = synth.apa_depos(seed=2 + rank)
+    n = len(depos)
+    dt = wct.from_config(cfg, device=local)
+    stream = torch.cuda.current_stream()
+    d_depos = torch.from_numpy(depos).to("cuda")
+    nrows, nticks = dt.frame_shape()
+    d_frame = torch.empty((nrows, nticks), dtype=torch.float32, device="cuda")
+    flush = torch.empty(320 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")  # > L2 (126 MB)
+
+    def step():
+        return dt.forward_device(d_depos.data_ptr(), n, d_frame.data_ptr(), stream.cuda_stream)
+
+    for _ in range(args.warmup):
+        flush.fill_(1.0)
+        wins, _ = step()
+    torch.cuda.synchronize()
+    dt.stage_times(reset=True)
+    dt.set_profiling(True)
+    clocks = ClockSampler(local)
+    if world > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    evs = []
+    for k in range(args.steps):
+        flush.fill_(float(k))  # L2 flush between timed steps, outside the timed events
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        wins, _ = step()
+        b.record(stream)
+        evs.append((a, b))
+    torch.cuda.synchronize()
+    if world > 1:
+        torch.distributed.barrier()
+    clk = clocks.stop()
+    dt.set_profiling(False)
+    total_ms = sum(a.elapsed_time(b) for a, b in evs)
+    stages, launches = dt.stage_times(reset=True)
+    t = torch.tensor([total_ms], dtype=torch.float64, device="cuda")
+    if world > 1:
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    max_ms = float(t.item())
+    total_depos = n * world
+    value = total_depos * args.steps / (max_ms / 1e3)
+
+    # --- end to end through the public host API: pinned host depos in, frame out
+    h_depos = torch.from_numpy(depos).pin_memory()
+    h_frame = torch.empty((nrows, nticks), dtype=torch.float32).pin_memory()
+    hd = h_depos.numpy()
+    hf = h_frame.numpy()
+    for _ in range(max(1, args.warmup)):
+        dt(hd, out=hf)
+    if world > 1:
+        torch.distributed.barrier()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        dt(hd, out=hf)
+    e2e_s = time.perf_counter() - t0
+    te = torch.tensor([e2e_s], dtype=torch.float64, device="cuda")
+    if world > 1:
+        torch.distributed.all_reduce(te, op=torch.distributed.ReduceOp.MAX)
+    e2e_value = total_depos * args.steps / float(te.item())
+
+    # --- roofline of the dominant stage (live CUDA events on the launch stream)
+    peak, peak_kind = load_peaks()
+    sb = stage_bytes(wins, cfg, n)
+    dom = max((k for k in sb), key=lambda k: stages[k][0])
+    dom_ms = stages[dom][0]
+    dom_launches = max(1, stages[dom][1])
+    bytes_per_launch = sb[dom] * args.steps / dom_launches
+    ms_per_launch = dom_ms / dom_launches
+    achieved = bytes_per_launch / (ms_per_launch / 1e3) / 1e9 if ms_per_launch > 0 else 0.0
+    traffic = None
+    tp = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(tp):
+        try:
+            traffic = json.load(open(tp)).get(dom)
+        except Exception:
+            traffic = None
+
+    result = {
+        "metric": METRIC,
+        "value": value,
+        "unit": UNIT,
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": max_ms / args.steps,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32",
+        "data": "synthetic",
+        "config": {
+            "workload": "full-APA plain forward: U/V 800 + W 960 wires, 6000 ticks, 20 muon tracks, "
+                        "%d depos per event per GPU, drift+diffusion+FFT convolution" % n,
+            "depos_per_event": n,
+            "planes": [dict(w) for w in wins],
+            "l2": "flushed between timed steps (320 MB write, untimed)",
+            "parallelism": "events sharded over %d GPU(s), no collective" % world,
+        },
+        "roofline": {
+            "bound": "hbm",
+            "kernel": dom,
+            "achieved": achieved,
+            "peak": peak,
+            "unit": "GB/s",
+            "frac": achieved / peak,
+            "peak_kind": peak_kind,
+            "traffic": traffic,
+            "algorithmic_bytes_per_launch": bytes_per_launch,
+            "ms_per_launch": ms_per_launch,
+        },
+        "stages_ms_per_step": {k: v[0] / args.steps for k, v in stages.items()},
+        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(depos.nbytes),
+                "d2h_bytes_per_step": int(nrows * nticks * 4)},
+        "gpu_launches": launches,
+        "clocks": clk,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        result["cpu_baseline"] = cpu_baseline(cfg, depos, nthreads=1)
+    if rank == 0:
+        print(json.dumps(result), flush=True)
+    if world > 1:
+        torch.distributed.destroy_process_group()
+
+
+def cpu_baseline(cfg, depos, nthreads=1):
+    """The oracle (FP32 restatement of the reference) on one full event."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    O.lib()
+    t0 = time.perf_counter()
+    O.run(cfg, depos, nthreads=nthreads)
+    dt = time.perf_counter() - t0
+    return {"value": len(depos) / dt, "unit": UNIT, "cores": nthreads, "kind": "port",
+            "sample": "one full-APA event (%d depos), FP32 restatement, %d thread(s), %.1f s" %
+                      (len(depos), nthreads, dt)}
+
+
+def run_reference(args):
+    rank, world, local = dist_setup(args)
+    if rank != 0:
+        return
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    O.lib()
+    synth = importlib.import_module("wire-cell-toolkit_b200.synth")
+    cfg = synth.apa_config()
+    depos = synth.apa_depos(seed=2)
+    nth = max(1, min(len(cfg["planes"]), os.cpu_count() or 1))
+    for _ in range(args.warmup):
+        O.run(cfg, depos, nthreads=nth)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        O.run(cfg, depos, nthreads=nth)
+    dt = time.perf_counter() - t0
+    value = len(depos) * args.steps / dt
+    sample = "one full-APA event (%d depos) per step, FP32 restatement, planes on %d threads" % (len(depos), nth)
+    print(json.dumps({
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt / args.steps * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": "full-APA plain forward, %d depos per event" % len(depos)},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": nth, "kind": "port", "sample": sample},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser(description=__doc__)
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_b200(args)
+
+
+if __name__ == "__main__":
+    main()

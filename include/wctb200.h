@@ -1,0 +1,172 @@
+/*
+ * wctb200 -- B200-native Wire-Cell DepoTransform (signal simulation hot path)
+ *
+ * C ABI of libwctb200.so.  Plain pointers and sizes only; every entry point
+ * returns an int status (WCT_OK on success) and never throws.  The message of
+ * the last failure on the calling thread is available from wct_last_error().
+ *
+ * Each entry point cites the reference interface it stands in for (paths in
+ * the wire-cell-toolkit source tree).  Units are the Wire-Cell system of
+ * units (util/inc/WireCellUtil/Units.h): mm = 1, ns = 1, positron charge = 1.
+ *
+ * Depo layout (IDepo, iface/inc/WireCellIface/IDepo.h:14-51): 7 doubles per
+ * depo: time, charge, x, y, z, extent_long, extent_tran.
+ *
+ * Frame layout: dense float32 rows, one row per wire of every plane (faces in
+ * the order added, planes in the order added within a face), nticks columns
+ * (readout_time / tick).  Row r of plane p holds ImpactTransform::waveform(r)
+ * (gen/src/ImpactTransform.cxx:312-347); traces with the reference's exact-zero
+ * trimming are produced by wct_dt_traces().
+ */
+#ifndef WCTB200_H
+#define WCTB200_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+    WCT_OK = 0,
+    WCT_ERR_ARG = 1,      /* bad argument (null pointer, index out of range) */
+    WCT_ERR_CONFIG = 2,   /* invalid configuration (DepoTransform::configure would throw) */
+    WCT_ERR_CUDA = 3,     /* CUDA runtime failure */
+    WCT_ERR_STATE = 4,    /* call out of order (e.g. forward before responses are set) */
+    WCT_ERR_RESPONSE = 5, /* response lookup outside the PIR extent (PlaneImpactResponse::closest throws) */
+    WCT_ERR_SIZE = 6,     /* a patch or window exceeds a compiled limit */
+    WCT_EOS = 7           /* end of stream acknowledged */
+};
+
+typedef struct wct_depotransform wct_depotransform; /* one DepoTransform component */
+typedef struct wct_pir wct_pir;                     /* one PlaneImpactResponse */
+
+/* Pimpos constructor arguments of one wire plane (util/inc/WireCellUtil/Pimpos.h:35-68)
+ * plus the channel ident of each wire (IWire::channel). */
+typedef struct {
+    int nwires;
+    int nimpacts;          /* impact bins per wire region (Pimpos nbins, default 10) */
+    double pitchmin;       /* pitch location of wire 0 */
+    double pitchmax;       /* pitch location of wire nwires-1 */
+    double wire[3];        /* wire direction */
+    double pitch[3];       /* pitch direction */
+    double origin[3];      /* Pimpos origin */
+    const int* channels;   /* nwires channel idents (copied) */
+} wct_plane_desc;
+
+/* One plane's field response (Response::Schema::PlaneResponse,
+ * util/inc/WireCellUtil/Response.h:28-110). */
+typedef struct {
+    int npaths;            /* PathResponse count, ordered by increasing pitchpos */
+    int nsamples;          /* samples per path current */
+    const double* pitchpos;/* [npaths] */
+    const double* current; /* [npaths][nsamples] induced current */
+    double pitch;          /* PlaneResponse::pitch */
+    double tstart;         /* FieldResponse::tstart */
+    double period;         /* FieldResponse::period */
+} wct_fr_plane;
+
+/* Per-plane window of one forward call: ImpactTransform's m_start_ch,
+ * m_end_ch, m_start_tick, m_end_tick (gen/src/ImpactTransform.cxx:90-115)
+ * and BinnedDiffusion_transform's counters. */
+typedef struct {
+    int face, plane;
+    int start_ch, end_ch;       /* wire window (may extend past [0, nwires)) */
+    int start_tick, end_tick;   /* tick window (may extend past [0, nticks)) */
+    int nw_fft, nt_fft;         /* the reference's FFT sizes for this window */
+    int nt_gpu;                 /* time FFT length used on the device */
+    int charge_rows;            /* wires of the charge grid (window before padding) */
+    int npad;                   /* response half width in wires */
+    int ndepos_added;           /* depos accepted by BinnedDiffusion_transform::add */
+    int outside_time, outside_pitch;
+} wct_plane_window;
+
+const char* wct_version(void);
+/* Message of the last failing call on this thread (empty if none). */
+const char* wct_last_error(void);
+
+/* ---- PlaneImpactResponse (gen/src/PlaneImpactResponse.cxx:56-320) ---- */
+
+/* Build a plane impact response: PlaneImpactResponse::configure + build_responses
+ * (gen/src/PlaneImpactResponse.cxx:56-269).  short_wave holds nshort short
+ * responses (ColdElecResponse/RCResponse samples, IWaveform::waveform_samples)
+ * concatenated, short_len their lengths; nticks is the PIR "nticks". */
+int wct_pir_create(const wct_fr_plane* fr, int nshort, const int* short_len, const double* short_wave,
+                   double overall_short_padding, double tick, int nticks, wct_pir** out);
+/* PlaneImpactResponse::closest (gen/src/PlaneImpactResponse.cxx:294-320): path index
+ * of the response closest to relpitch, or WCT_ERR_RESPONSE where the reference throws. */
+int wct_pir_closest(const wct_pir* pir, double relpitch, int* path);
+/* pitch(), impact(), half extent, nwires(), nimp_per_wire(), path count, nticks, waveform_pad. */
+int wct_pir_info(const wct_pir* pir, double* pitch, double* impact, double* half_extent, int* nwires,
+                 int* nimp_per_wire, int* npaths, int* nticks, int* waveform_pad);
+/* IImpactResponse::waveform() of one path: nticks floats. */
+int wct_pir_waveform(const wct_pir* pir, int path, float* out);
+int wct_pir_destroy(wct_pir* pir);
+
+/* ---- DepoTransform (gen/src/DepoTransform.cxx, IDepoFramer) ---- */
+
+/* DepoTransform::configure (gen/src/DepoTransform.cxx:76-113) from JSON with
+ * the reference keys: anode, pirs, dft, rng, fluctuate, nsigma, start_time,
+ * readout_time, tick, drift_speed, first_frame_number.  Optional extra keys:
+ * "drifter" {DL, DT, lifetime, drift_speed, time_offset, xregions:[{anode,
+ * response, cathode}]} to drift depos on the device before the transform
+ * (Drifter, gen/src/Drifter.cxx:94-123), and "device" (CUDA ordinal). */
+int wct_dt_create(const char* json_config, wct_depotransform** out);
+/* DepoTransform::default_configuration (gen/src/DepoTransform.cxx:114-153) as JSON. */
+int wct_dt_default_configuration(char* buf, size_t len);
+/* Add an anode face with its sensitive volume (IAnodeFace::sensitive,
+ * gen/src/AnodePlane.cxx:259-290); bb_lo == NULL means no volume cut. */
+int wct_dt_add_face(wct_depotransform* dt, const double* bb_lo, const double* bb_hi, int* face);
+/* Add a wire plane to a face (IAnodeFace::planes order). */
+int wct_dt_add_plane(wct_depotransform* dt, int face, const wct_plane_desc* desc, int* plane);
+/* Use a PIR for a plane: ImpactTransform's response selection
+ * (gen/src/ImpactTransform.cxx:26-74) over pirs[plane]. */
+int wct_dt_set_response_pir(wct_depotransform* dt, int face, int plane, const wct_pir* pir);
+/* Same from a ready table: table[g][j][k] for impact group g < ngroups, wire
+ * offset j - npad in [-npad, npad], tick k < nsamples (the closest() waveform
+ * for that group and offset). */
+int wct_dt_set_response_table(wct_depotransform* dt, int face, int plane, int ngroups, int npad, int nsamples,
+                              double pitch, double impact, int waveform_pad, const float* table);
+/* Frame geometry: total wire rows and nticks. */
+int wct_dt_frame_shape(const wct_depotransform* dt, int* nrows, int* nticks);
+
+/* DepoTransform::operator() (gen/src/DepoTransform.cxx:155-224) on host
+ * buffers: depos [ndepos][7] in, dense frame [nrows][nticks] out, one window
+ * per plane (may be NULL), frame ident out (may be NULL). */
+int wct_dt_forward(wct_depotransform* dt, const double* depos, size_t ndepos, float* frame,
+                   wct_plane_window* windows, int* frame_ident);
+/* The same on device buffers, enqueued on stream (cudaStream_t, NULL = the
+ * component's own stream).  Returns after the work is enqueued; one small
+ * device-to-host read of the window sizes synchronises the stream mid-way. */
+int wct_dt_forward_device(wct_depotransform* dt, const double* d_depos, size_t ndepos, float* d_frame,
+                          wct_plane_window* windows, int* frame_ident, void* stream);
+/* End of stream (DepoTransform.cxx:157-162): acknowledges with WCT_EOS. */
+int wct_dt_eos(wct_depotransform* dt);
+/* Trace assembly (DepoTransform.cxx:193-208 with Waveform::edge,
+ * util/src/Waveform.cxx:136-153) from a host frame: for every wire with a
+ * non-zero sample, channel, first tick and length of [first nonzero, last
+ * nonzero].  Arrays have room for nrows entries; *ntraces receives the count. */
+int wct_dt_traces(const wct_depotransform* dt, const float* frame, int* channel, int* tbin, int* length,
+                  long* offset, int* ntraces);
+/* Patch placement of every input depo on one plane from the last forward
+ * call: out[i] = {toffset, poffset, nt, np} of GaussianDiffusion::set_sampling
+ * (gen/src/GaussianDiffusion.cxx:116-149); nt = np = 0 where the depo adds no
+ * patch (dropped by the drift, the sensitive volume, BinnedDiffusion_transform::add
+ * or an empty sample range).  n must equal the last call's depo count. */
+int wct_dt_patch_records(const wct_depotransform* dt, int face, int plane, int* out, size_t n);
+/* Stage profiling (the engine-level timers of pgraph/src/Graph.cxx:118-122,
+ * here per device stage): when enabled, every forward call records CUDA
+ * events around its stages on the launch stream.  wct_dt_stage_times
+ * returns, per stage, the accumulated milliseconds and launch count since the
+ * last reset (stages: 0 drift+prep, 1 raster, 2 time FFT, 3 wire convolution,
+ * 4 inverse FFT + frame, 5 other), and the total number of kernel launches. */
+int wct_dt_set_profiling(wct_depotransform* dt, int on);
+int wct_dt_stage_times(wct_depotransform* dt, double* ms, long* launches, int nstages, long* total_launches,
+                       int reset);
+int wct_dt_destroy(wct_depotransform* dt);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* WCTB200_H */

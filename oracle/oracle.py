@@ -1,0 +1,352 @@
+"""TEST INFRASTRUCTURE ONLY -- the parity oracle, never the product.
+
+ctypes front end of ``liboracle.so`` (oracle/wct_oracle.cpp, the CPU
+restatement of the reference DepoTransform chain, FP32 and FP64
+instantiations) plus an independent FP64 formulation of the same frame in
+NumPy (direct linear convolution of the impact-group charge grids), used to
+cross-check the restatement's FFT pair-packing.
+
+Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg import
+this module.
+"""
+
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "liboracle.so")
+REF_PATH = os.path.join(HERE, "_ref", "libref_binning.so")
+
+_lib = None
+_ref = None
+
+
+def build():
+    """Compile liboracle.so (and _ref when the reference tree is present)."""
+    import subprocess
+    subprocess.run(["make", "-s", "-C", HERE], check=True)
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            build()
+        _lib = C.CDLL(LIB_PATH)
+        _lib.orc_fft_best_length.restype = C.c_int
+        _lib.orc_fft_best_length.argtypes = [C.c_long, C.c_int]
+        _lib.orc_binning_bin.restype = C.c_int
+        _lib.orc_binning_bin.argtypes = [C.c_int, C.c_double, C.c_double, C.c_double]
+        _lib.orc_sample_bin_range.argtypes = [C.c_int, C.c_double, C.c_double, C.c_double, C.c_double,
+                                              C.POINTER(C.c_int)]
+        _lib.orc_fft_f32.argtypes = [C.c_void_p, C.c_int, C.c_int]
+        _lib.orc_fft_f64.argtypes = [C.c_void_p, C.c_int, C.c_int]
+        _lib.orc_set_sampling.restype = C.c_int
+        _lib.orc_set_sampling.argtypes = [C.c_double] * 5 + [C.c_int, C.c_double, C.c_double, C.c_int, C.c_double,
+                                                             C.c_double, C.c_double, C.c_int, C.c_int, C.c_void_p,
+                                                             C.c_void_p, C.c_void_p]
+        _lib.orc_drift.restype = C.c_int
+        _lib.orc_drift.argtypes = [C.c_void_p, C.c_void_p]
+        _lib.orc_pir_build.restype = C.c_int
+        _lib.orc_pir_build.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p]
+        _lib.orc_run.restype = C.c_int
+        _lib.orc_run.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
+        _lib.orc_edge.argtypes = [C.c_void_p, C.c_int, C.c_void_p]
+    return _lib
+
+
+def ref():
+    """The reference-compiled Binning harness, or None when it was not built."""
+    global _ref
+    if _ref is None and os.path.exists(REF_PATH):
+        _ref = C.CDLL(REF_PATH)
+        for n, rt, at in [
+            ("ref_bin", C.c_int, [C.c_int, C.c_double, C.c_double, C.c_double]),
+            ("ref_edge", C.c_double, [C.c_int, C.c_double, C.c_double, C.c_int]),
+            ("ref_center", C.c_double, [C.c_int, C.c_double, C.c_double, C.c_int]),
+            ("ref_binsize", C.c_double, [C.c_int, C.c_double, C.c_double]),
+            ("ref_gcumulative", C.c_double, [C.c_double, C.c_double, C.c_double]),
+            ("ref_gbounds", C.c_double, [C.c_double, C.c_double, C.c_double, C.c_double]),
+            ("ref_gaussian_sum", C.c_double, [C.c_int, C.c_double, C.c_double, C.c_double, C.c_double,
+                                              C.c_void_p]),
+        ]:
+            f = getattr(_ref, n)
+            f.restype = rt
+            f.argtypes = at
+        _ref.ref_sample_bin_range.argtypes = [C.c_int, C.c_double, C.c_double, C.c_double, C.c_double,
+                                              C.POINTER(C.c_int)]
+    return _ref
+
+
+class OrcPlane(C.Structure):
+    _fields_ = [
+        ("nwires", C.c_int), ("nimp", C.c_int),
+        ("pitchmin", C.c_double), ("pitchmax", C.c_double),
+        ("wire", C.c_double * 3), ("pitch", C.c_double * 3), ("origin", C.c_double * 3),
+        ("npaths", C.c_int), ("nfr", C.c_int),
+        ("pitchpos", C.c_void_p), ("current", C.c_void_p), ("fr_pitch", C.c_double),
+    ]
+
+
+class OrcJob(C.Structure):
+    _fields_ = [
+        ("start_time", C.c_double), ("readout_time", C.c_double), ("tick", C.c_double),
+        ("drift_speed", C.c_double), ("nsigma", C.c_double),
+        ("drift", C.c_int),
+        ("DL", C.c_double), ("DT", C.c_double), ("lifetime", C.c_double), ("drifter_speed", C.c_double),
+        ("toffset", C.c_double),
+        ("nxregions", C.c_int), ("xregions", C.c_void_p),
+        ("have_bb", C.c_int), ("bb_lo", C.c_double * 3), ("bb_hi", C.c_double * 3),
+        ("fr_tstart", C.c_double), ("fr_period", C.c_double),
+        ("nshort", C.c_int), ("short_len", C.c_void_p), ("short_wave", C.c_void_p),
+        ("overall_short_padding", C.c_double), ("pir_nticks", C.c_int),
+        ("nplanes", C.c_int), ("planes", C.c_void_p),
+        ("ndepos", C.c_int), ("depos", C.c_void_p),
+        ("fp64", C.c_int), ("nthreads", C.c_int),
+    ]
+
+
+class OrcPlaneOut(C.Structure):
+    _fields_ = [(n, C.c_int) for n in ("start_ch", "end_ch", "start_tick", "end_tick", "nw", "nt",
+                                        "ndepos_added", "outside_time", "outside_pitch")]
+
+
+class Job:
+    """Owns the numpy buffers an OrcJob points into."""
+
+    def __init__(self, cfg, depos, drift=True, fp64=False, nthreads=1):
+        self.keep = []
+        j = OrcJob()
+        j.start_time = cfg["start_time"]
+        j.readout_time = cfg["readout_time"]
+        j.tick = cfg["tick"]
+        j.drift_speed = cfg["drift_speed"]
+        j.nsigma = cfg["nsigma"]
+        dr = cfg.get("drifter")
+        j.drift = 1 if (drift and dr) else 0
+        if dr:
+            j.DL, j.DT, j.lifetime = dr["DL"], dr["DT"], dr["lifetime"]
+            j.drifter_speed, j.toffset = dr["drift_speed"], dr.get("time_offset", 0.0)
+            xr = self._arr(np.array(dr["xregions"], dtype=np.float64).reshape(-1, 3))
+            j.nxregions = xr.shape[0]
+            j.xregions = xr.ctypes.data
+        bb = cfg.get("face_bb")
+        if bb is not None:
+            j.have_bb = 1
+            for i in range(3):
+                j.bb_lo[i] = bb[0][i]
+                j.bb_hi[i] = bb[1][i]
+        j.fr_tstart = cfg["fr"][0]["tstart"]
+        j.fr_period = cfg["fr"][0]["period"]
+        shorts = [np.asarray(s, dtype=np.float64) for s in cfg.get("short_responses", [])]
+        j.nshort = len(shorts)
+        if shorts:
+            sl = self._arr(np.array([len(s) for s in shorts], dtype=np.int32))
+            sw = self._arr(np.concatenate(shorts))
+            j.short_len = sl.ctypes.data
+            j.short_wave = sw.ctypes.data
+        j.overall_short_padding = cfg["overall_short_padding"]
+        j.pir_nticks = cfg["pir_nticks"]
+        planes = (OrcPlane * len(cfg["planes"]))()
+        for i, (pl, fr) in enumerate(zip(cfg["planes"], cfg["fr"])):
+            p = planes[i]
+            p.nwires = pl["nwires"]
+            p.nimp = pl["nimp"]
+            p.pitchmin = pl["pitchmin"]
+            p.pitchmax = pl["pitchmax"]
+            for k in range(3):
+                p.wire[k] = pl["wire"][k]
+                p.pitch[k] = pl["pitch"][k]
+                p.origin[k] = pl["origin"][k]
+            pp = self._arr(np.ascontiguousarray(fr["pitchpos"], dtype=np.float64))
+            cu = self._arr(np.ascontiguousarray(fr["current"], dtype=np.float64))
+            p.npaths = pp.shape[0]
+            p.nfr = cu.shape[1]
+            p.pitchpos = pp.ctypes.data
+            p.current = cu.ctypes.data
+            p.fr_pitch = fr["pitch"]
+        self.keep.append(planes)
+        j.nplanes = len(cfg["planes"])
+        j.planes = C.cast(planes, C.c_void_p)
+        d = self._arr(np.ascontiguousarray(depos, dtype=np.float64).reshape(-1, 7))
+        j.ndepos = d.shape[0]
+        j.depos = d.ctypes.data
+        j.fp64 = 1 if fp64 else 0
+        j.nthreads = nthreads
+        self.job = j
+        self.cfg = cfg
+
+    def _arr(self, a):
+        self.keep.append(a)
+        return a
+
+
+def fft_best_length(n, keep=False):
+    return lib().orc_fft_best_length(int(n), 1 if keep else 0)
+
+
+def run(cfg, depos, drift=True, fp64=False, nthreads=1, records=False):
+    """Run the restated DepoTransform. Returns dict(frames=[per-plane
+    [nwires][nticks]], windows=[OrcPlaneOut as dict], records=optional)."""
+    job = Job(cfg, depos, drift=drift, fp64=fp64, nthreads=nthreads)
+    nticks = int(cfg["readout_time"] / cfg["tick"])
+    nw = [pl["nwires"] for pl in cfg["planes"]]
+    dt = np.float64 if fp64 else np.float32
+    frame = np.zeros((sum(nw), nticks), dtype=dt)
+    pouts = (OrcPlaneOut * len(nw))()
+    rec = None
+    if records:
+        rec = np.zeros((len(nw), job.job.ndepos, 5), dtype=np.int32)
+    rc = lib().orc_run(C.byref(job.job), frame.ctypes.data, C.cast(pouts, C.c_void_p),
+                       rec.ctypes.data if rec is not None else None)
+    if rc != 0:
+        raise RuntimeError("oracle run failed: %d" % rc)
+    frames = []
+    r0 = 0
+    for n in nw:
+        frames.append(frame[r0:r0 + n])
+        r0 += n
+    wins = [{f: getattr(p, f) for f, _ in OrcPlaneOut._fields_} for p in pouts]
+    return dict(frames=frames, windows=wins, records=rec)
+
+
+def drift(cfg, depos):
+    job = Job(cfg, depos, drift=True)
+    out = np.zeros((job.job.ndepos, 8))
+    n = lib().orc_drift(C.byref(job.job), out.ctypes.data)
+    return out[:n]
+
+
+def pir_build(cfg, iplane, fp64=False):
+    job = Job(cfg, np.zeros((0, 7)), fp64=fp64)
+    fr = cfg["fr"][iplane]
+    npaths = len(fr["pitchpos"])
+    wf = np.zeros((npaths, cfg["pir_nticks"]))
+    bywire = np.full((npaths, 16), -1, dtype=np.int32)
+    pie = np.zeros(3)
+    code = lib().orc_pir_build(C.byref(job.job), iplane, wf.ctypes.data, bywire.ctypes.data, pie.ctypes.data)
+    if code < 0:
+        raise RuntimeError("pir build failed")
+    nwires, nimp = divmod(code, 1000)
+    bw = bywire.reshape(-1)[: nwires * nimp].reshape(nwires, nimp)
+    return dict(waveforms=wf, bywire=bw, pitch=pie[0], impact=pie[1], half_extent=pie[2])
+
+
+def set_sampling(t, q, pc, st, sp, tbins, ibins, nsigma=3.0, fp64=False, cap=1 << 16):
+    patch = np.zeros(cap)
+    w = np.zeros(4096)
+    oi = np.zeros(4, dtype=np.int32)
+    rc = lib().orc_set_sampling(t, q, pc, st, sp, tbins[0], tbins[1], tbins[2], ibins[0], ibins[1], ibins[2],
+                                nsigma, 1 if fp64 else 0, cap, patch.ctypes.data, w.ctypes.data, oi.ctypes.data)
+    if rc != 0:
+        raise RuntimeError("patch too large")
+    to, po, nt, npp = [int(x) for x in oi]
+    return dict(toffset=to, poffset=po, nt=nt, np=npp, patch=patch[: nt * npp].reshape(npp, nt), weights=w[:npp])
+
+
+def edge(wave):
+    w = np.ascontiguousarray(wave, dtype=np.float32)
+    out = np.zeros(2, dtype=np.int32)
+    lib().orc_edge(w.ctypes.data, w.size, out.ctypes.data)
+    return int(out[0]), int(out[1])
+
+
+def traces(frame_rows, channels):
+    """DepoTransform trace assembly (gen/src/DepoTransform.cxx:193-208):
+    list of (channel, tbin, charges) with exact-zero trimming."""
+    out = []
+    for iw in range(frame_rows.shape[0]):
+        a, b = edge(frame_rows[iw])
+        if a == frame_rows.shape[1]:
+            continue
+        out.append((int(channels[iw]), a, frame_rows[iw, a:b].astype(np.float32)))
+    return out
+
+
+# ---------------------------------------------------------------------------
+# Independent FP64 formulation (direct linear convolution), for small cases.
+# ---------------------------------------------------------------------------
+def direct_fp64(cfg, depos, iplane, pir=None, drift=True):
+    """Frame of one plane as V[w,t] = sum_g sum_j sum_tau R_g[j][tau] Q_g[w-j][t-tau],
+    with Q_g accumulated in FP64 from FP64 patches and R_g[j] the FP64 PIR
+    waveforms selected by the reference's closest() rule.  Independent of the
+    restatement's FFT convolution; used to pin it on small inputs."""
+    import math
+    if pir is None:
+        pir = pir_build(cfg, iplane, fp64=True)
+    d = drift_fn(cfg, depos) if drift else np.asarray(depos, dtype=np.float64)
+    pl = cfg["planes"][iplane]
+    nticks = int(cfg["readout_time"] / cfg["tick"])
+    nwires = pl["nwires"]
+    nimp = pl["nimp"]
+    regionsize = (pl["pitchmax"] - pl["pitchmin"]) / (nwires - 1)
+    pmin = pl["pitchmin"] - 0.5 * regionsize
+    pmax = pl["pitchmax"] + 0.5 * regionsize
+    ib = (nwires * nimp, pmin, pmax)
+    tb = (int(cfg["readout_time"] / cfg["tick"]), cfg["start_time"], cfg["start_time"] + cfg["readout_time"])
+    pdir = np.array(pl["pitch"], dtype=np.float64)
+    pdir = pdir / math.sqrt(float(np.dot(pdir, pdir)))
+    org = np.array(pl["origin"], dtype=np.float64)
+    bb = cfg.get("face_bb")
+    G = int(round(pir["pitch"] / pir["impact"])) + 1
+    npad = int(round((pir["bywire"].shape[0] - 1) / 2.0))
+    Q = np.zeros((G, nwires, nticks))
+    for row in d:
+        t, q, x, y, z, el, et = row[:7]
+        if bb is not None:
+            p3 = (x, y, z)
+            if any(not (min(bb[0][k], bb[1][k]) <= p3[k] <= max(bb[0][k], bb[1][k])) for k in range(3)
+                   if bb[0][k] != bb[1][k]):
+                continue
+        pc = float(np.dot(pdir, np.array([x, y, z]) - org))
+        st = el / cfg["drift_speed"]
+        # rejection (gen/src/BinnedDiffusion_transform.cxx:37-76)
+        def rej(c, s, lo, hi):
+            eff = cfg["nsigma"] if s > 0 else 0.0
+            dmin = (lo - c) / s if s else lo - c
+            dmax = (hi - c) / s if s else hi - c
+            return dmin > eff or dmax < -eff
+        if rej(t, st, tb[1], tb[2]) or rej(pc, et, ib[1], ib[2]):
+            continue
+        P = set_sampling(t, q, pc, st, et, tb, ib, cfg["nsigma"], fp64=True)
+        for ip in range(P["np"]):
+            k = P["poffset"] + ip
+            w = k // nimp
+            red = k - (w * nimp + nimp // 2)
+            g0 = red + G // 2
+            Q[g0, w, P["toffset"]:P["toffset"] + P["nt"]] += P["patch"][ip] * P["weights"][ip]
+            Q[g0 + 1, w, P["toffset"]:P["toffset"] + P["nt"]] += P["patch"][ip] * (1.0 - P["weights"][ip])
+    # responses R_g[j] by the closest() rule (gen/src/ImpactTransform.cxx:34-74)
+    out = np.zeros((nwires, nticks))
+    from numpy.fft import rfft, irfft
+    nfft = 1
+    while nfft < nticks + pir["waveforms"].shape[1]:
+        nfft *= 2
+    for g in range(G):
+        rel = -pir["pitch"] / 2.0 + pir["impact"] * g + (1e-9 if g != G - 1 else -1e-9)
+        Qf = rfft(Q[g], nfft, axis=1)
+        for j in range(-npad, npad + 1):
+            rp = rel - j * pir["pitch"]
+            relwire = cround(rp / pir["pitch"])
+            wi = pir["bywire"].shape[0] // 2 + relwire
+            rem = rp - relwire * pir["pitch"]
+            ii = cround(rem / pir["impact"]) + pir["bywire"].shape[1] // 2
+            path = pir["bywire"][wi][ii]
+            Rf = rfft(pir["waveforms"][path], nfft)
+            conv = irfft(Qf * Rf[None, :], nfft, axis=1)[:, :nticks]
+            lo, hi = max(0, j), min(nwires, nwires + j)
+            out[lo:hi] += conv[lo - j:hi - j]
+    return out
+
+
+def cround(x):
+    """C round(): halves away from zero."""
+    import math
+    return int(math.copysign(math.floor(abs(x) + 0.5), x))
+
+
+def drift_fn(cfg, depos):
+    o = drift(cfg, depos)
+    return o[:, :7]

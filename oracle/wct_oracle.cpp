@@ -1,0 +1,1209 @@
+// ============================================================================
+// TEST INFRASTRUCTURE ONLY -- NOT PART OF THE PRODUCT.
+//
+// CPU restatement of the Wire-Cell Toolkit signal-simulation hot path
+// (Gen::DepoTransform chain), used as
+//   * the parity oracle of the GPU path (tests/ and __graft_entry__.smoke()),
+//   * the timed CPU baseline of bench.py (cpu_baseline, --impl reference).
+// The product library never links, loads or calls this file.
+//
+// It is instantiated twice:
+//   * real_t = float  : step-for-step FP32 restatement of the reference
+//                       (FP32 patches, FP32 FFTs, FP64 drift/erf/weights),
+//   * real_t = double : the same algorithm with every FP32 step in FP64
+//                       (the "FP64 oracle").
+// Every function cites the reference file:line it restates (paths relative to
+// the wire-cell-toolkit source tree).
+//
+// Deliberate differences from the reference, all without numerical effect
+// beyond double round-off:
+//   * the reference iterates its GaussianDiffusion std::set in heap-pointer
+//     order (BinnedDiffusion_transform.cxx:279); this restatement iterates in
+//     input order, which only changes the order of double additions;
+//   * FFTs are this file's own mixed-radix Stockham transforms instead of
+//     FFTW (aux/src/FftwDFT.cxx); they follow the same IDFT conventions
+//     (forward unnormalised, inverse 1/n, iface/inc/WireCellIface/IDFT.h:10-80).
+// ============================================================================
+
+#include <algorithm>
+#include <atomic>
+#include <cmath>
+#include <complex>
+#include <cstdint>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <stdexcept>
+#include <thread>
+#include <unordered_map>
+#include <vector>
+
+namespace orc {
+
+// ---------------------------------------------------------------------------
+// fft_best_length -- util/src/FFTBestLength.cxx:12-59 (same size tables).
+// ---------------------------------------------------------------------------
+static const size_t kSizesAny[] = {
+    33,   35,   40,   42,   44,   56,   64,   66,   70,   77,   80,   96,   98,   100,  112,  121,  128,
+    140,  143,  160,  168,  169,  200,  224,  256,  280,  320,  400,  448,  512,  560,  640,  686,  768,
+    800,  847,  896,  1024, 1120, 1280, 1331, 1372, 1400, 1536, 1600, 1792, 2048, 2560, 2662, 2744, 3200,
+    3584, 4096, 4116, 4480, 4802, 5120, 5324, 5376, 5544, 5600, 5632, 5929, 6174, 6272, 6292, 6655, 7168,
+    7840, 8192, 8232, 8960, 9317, 10240, 10648, 11979, 14336, 15972, 16384};
+static const size_t kSizesEven[] = {
+    40,   42,   44,   56,   64,   66,   70,   72,   80,   96,   98,   100,  112,  120,  128,  140,  160,
+    168,  200,  224,  256,  280,  320,  400,  448,  512,  560,  640,  686,  768,  800,  896,  1024, 1120,
+    1280, 1372, 1400, 1536, 1600, 1792, 2048, 2560, 2662, 2744, 3200, 3584, 4096, 4116, 4480, 4802, 5120,
+    5324, 5376, 5544, 5600, 5632, 6174, 6272, 6292, 6468, 7168, 7840, 8192, 8232, 8960, 10240, 10648, 11200,
+    11858, 11880, 14336, 15972, 16384};
+static const size_t kSizesOdd[] = {
+    33,   35,   39,   49,   55,   63,   65,   77,   81,   91,   99,   121,  143,  169,  175,  187,  225,
+    231,  245,  275,  297,  343,  363,  375,  385,  405,  441,  455,  495,  539,  605,  637,  693,  735,
+    847,  875,  891,  945,  1001, 1089, 1331, 1573, 1859, 1875, 2197, 2299, 2431, 2541, 2625, 2695, 3025,
+    3267, 3993, 4095, 4125, 4719, 4725, 5005, 5145, 5445, 5929, 6655, 7007, 7623, 7865, 9317, 9801, 11979,
+    14157, 14175, 15379, 16335};
+
+template <size_t N>
+static size_t first_at_least(const size_t (&tab)[N], size_t n)
+{
+    if (n <= tab[N - 1]) {
+        for (size_t i = 0; i < N; ++i)
+            if (tab[i] >= n) return tab[i];
+    }
+    return n;
+}
+
+size_t fft_best_length(size_t n, bool keep_odd_even)
+{
+    if (!keep_odd_even) return first_at_least(kSizesAny, n);
+    if (n % 2 == 0) return first_at_least(kSizesEven, n);
+    return first_at_least(kSizesOdd, n);
+}
+
+// ---------------------------------------------------------------------------
+// Binning -- util/inc/WireCellUtil/Binning.h:25-103.
+// ---------------------------------------------------------------------------
+struct Binning {
+    int nbins{0};
+    double minv{0}, maxv{0}, binsize{0};
+    Binning() = default;
+    Binning(int n, double lo, double hi) : nbins(n), minv(lo), maxv(hi), binsize((hi - lo) / n) {}
+    int bin(double v) const { return int((v - minv) / binsize); }           // Binning.h:75
+    double center(int i) const { return minv + (i + 0.5) * binsize; }        // Binning.h:79
+    double edge(int i) const { return minv + i * binsize; }                  // Binning.h:88
+    std::pair<int, int> sample_bin_range(double lo, double hi) const         // Binning.h:99-102
+    {
+        return {std::max(bin(lo), 0), std::min(bin(hi) + 1, nbins)};
+    }
+};
+
+// ---------------------------------------------------------------------------
+// Minimal 3-vector with the operation order of util/inc/WireCellUtil/D3Vector.h.
+// ---------------------------------------------------------------------------
+struct V3 {
+    double x{0}, y{0}, z{0};
+    double dot(const V3& o) const { return x * o.x + y * o.y + z * o.z; }   // D3Vector.h:125-129
+    double mag() const { return std::sqrt(x * x + y * y + z * z); }         // D3Vector.h:144
+    V3 norm() const                                                         // D3Vector.h:147-154
+    {
+        double m = mag();
+        if (m <= 0) return V3{};
+        return V3{x / m, y / m, z / m};
+    }
+    V3 cross(const V3& r) const                                             // D3Vector.h:157-164
+    {
+        return V3{y * r.z - z * r.y, z * r.x - x * r.z, x * r.y - y * r.x};
+    }
+    V3 operator-(const V3& o) const { return V3{x - o.x, y - o.y, z - o.z}; }
+};
+
+// ---------------------------------------------------------------------------
+// Pimpos -- util/src/Pimpos.cxx:5-68.
+// ---------------------------------------------------------------------------
+struct Pimpos {
+    int nimp{10};
+    V3 origin;
+    V3 axis[3];
+    Binning region, impact;
+    Pimpos(int nwires, double minp, double maxp, V3 wire, V3 pitch, V3 org, int nbins)
+        : nimp(nbins), origin(org)
+    {
+        axis[1] = wire.norm();
+        axis[2] = pitch.norm();
+        axis[0] = axis[1].cross(axis[2]);
+        const int nimpstot = nwires * nbins;
+        const double regionsize = (maxp - minp) / (nwires - 1);
+        const double pmin = minp - 0.5 * regionsize;
+        const double pmax = maxp + 0.5 * regionsize;
+        region = Binning(nwires, pmin, pmax);
+        impact = Binning(nimpstot, pmin, pmax);
+    }
+    double distance(const V3& pt) const { return axis[2].dot(pt - origin); }  // Pimpos.cxx:58
+    int wire_impact(int w) const { return (0.5 + w) * nimp; }                 // Pimpos.cxx:41
+    std::pair<int, int> wire_impacts(int w) const                             // Pimpos.cxx:43-47
+    {
+        const int wi = wire_impact(w);
+        return {wi - nimp / 2, wi + nimp / 2};
+    }
+};
+
+// ---------------------------------------------------------------------------
+// FFT: mixed-radix Stockham autosort, IDFT conventions
+// (iface/inc/WireCellIface/IDFT.h:10-80: forward unnormalised, inverse 1/n).
+// ---------------------------------------------------------------------------
+template <typename T>
+struct FFTPlan {
+    int n{0};
+    std::vector<int> radix;
+    std::vector<std::complex<T>> tw;  // exp(-2 pi i m / n), m in [0, n)
+};
+
+template <typename T>
+static const FFTPlan<T>& fft_plan(int n)
+{
+    static std::mutex mtx;
+    static std::map<int, std::unique_ptr<FFTPlan<T>>> cache;
+    std::lock_guard<std::mutex> lk(mtx);
+    auto it = cache.find(n);
+    if (it != cache.end()) return *it->second;
+    auto p = std::make_unique<FFTPlan<T>>();
+    p->n = n;
+    int m = n;
+    while (m % 4 == 0) { p->radix.push_back(4); m /= 4; }
+    while (m % 2 == 0) { p->radix.push_back(2); m /= 2; }
+    for (int f = 3; m > 1; f += 2) {
+        while (m % f == 0) { p->radix.push_back(f); m /= f; }
+    }
+    p->tw.resize(n);
+    for (int k = 0; k < n; ++k) {
+        long double a = -2.0L * 3.14159265358979323846264338327950288L * (long double)k / (long double)n;
+        p->tw[k] = std::complex<T>((T)std::cos(a), (T)std::sin(a));
+    }
+    auto& ref = *p;
+    cache[n] = std::move(p);
+    return ref;
+}
+
+// In-place 1-D DFT of length n (sign -1 forward, +1 backward, unnormalised).
+template <typename T>
+static void fft_1d(std::complex<T>* data, int n, int sign, std::complex<T>* work)
+{
+    if (n <= 1) return;
+    const FFTPlan<T>& P = fft_plan<T>(n);
+    using C = std::complex<T>;
+    C* src = data;
+    C* dst = work;
+    int Ns = 1;
+    C v[64];
+    C y[64];
+    for (int R : P.radix) {
+        const int nR = n / R;
+        const int twstep = n / (Ns * R);
+        for (int j = 0; j < nR; ++j) {
+            const int k = j % Ns;
+            for (int r = 0; r < R; ++r) {
+                C a = src[j + r * nR];
+                if (r && k) {
+                    C w = P.tw[(size_t)((long long)k * r * twstep % n)];
+                    if (sign > 0) w = std::conj(w);
+                    a *= w;
+                }
+                v[r] = a;
+            }
+            if (R == 2) {
+                y[0] = v[0] + v[1];
+                y[1] = v[0] - v[1];
+            }
+            else if (R == 4) {
+                C a0 = v[0] + v[2], a1 = v[0] - v[2];
+                C b0 = v[1] + v[3], b1 = v[1] - v[3];
+                C jb1 = (sign < 0) ? C(b1.imag(), -b1.real()) : C(-b1.imag(), b1.real());
+                y[0] = a0 + b0;
+                y[2] = a0 - b0;
+                y[1] = a1 + jb1;
+                y[3] = a1 - jb1;
+            }
+            else {
+                const int rstep = n / R;
+                for (int a = 0; a < R; ++a) {
+                    C s = 0;
+                    for (int b = 0; b < R; ++b) {
+                        C w = P.tw[(size_t)(((a * b) % R) * rstep)];
+                        if (sign > 0) w = std::conj(w);
+                        s += v[b] * w;
+                    }
+                    y[a] = s;
+                }
+            }
+            const int idxD = (j / Ns) * Ns * R + k;
+            for (int r = 0; r < R; ++r) dst[idxD + r * Ns] = y[r];
+        }
+        std::swap(src, dst);
+        Ns *= R;
+    }
+    if (src != data) std::copy(src, src + n, data);
+}
+
+template <typename T>
+struct Dft {
+    using C = std::complex<T>;
+    // aux/src/FftwDFT.cxx:88-115 (1d)
+    static void fwd1d(C* x, int n)
+    {
+        std::vector<C> w(n);
+        fft_1d<T>(x, n, -1, w.data());
+    }
+    static void inv1d(C* x, int n)
+    {
+        std::vector<C> w(n);
+        fft_1d<T>(x, n, +1, w.data());
+        for (int i = 0; i < n; ++i) x[i] /= (T)n;
+    }
+    // Row-major [nrows][ncols]; axis=1 transforms each row, axis=0 each column
+    // (aux/src/FftwDFT.cxx:119-176, 1b methods).
+    static void do1b(C* a, int nrows, int ncols, int axis, int sign, bool norm)
+    {
+        if (axis == 1) {
+            std::vector<C> w(ncols);
+            for (int r = 0; r < nrows; ++r) {
+                fft_1d<T>(a + (size_t)r * ncols, ncols, sign, w.data());
+                if (norm)
+                    for (int c = 0; c < ncols; ++c) a[(size_t)r * ncols + c] /= (T)ncols;
+            }
+        }
+        else {
+            std::vector<C> col(nrows), w(nrows);
+            for (int c = 0; c < ncols; ++c) {
+                for (int r = 0; r < nrows; ++r) col[r] = a[(size_t)r * ncols + c];
+                fft_1d<T>(col.data(), nrows, sign, w.data());
+                for (int r = 0; r < nrows; ++r) a[(size_t)r * ncols + c] = norm ? col[r] / (T)nrows : col[r];
+            }
+        }
+    }
+    static void fwd1b(C* a, int nr, int nc, int axis) { do1b(a, nr, nc, axis, -1, false); }
+    static void inv1b(C* a, int nr, int nc, int axis) { do1b(a, nr, nc, axis, +1, true); }
+    // aux/src/FftwDFT.cxx:179-217 (2d)
+    static void fwd2d(C* a, int nr, int nc)
+    {
+        do1b(a, nr, nc, 1, -1, false);
+        do1b(a, nr, nc, 0, -1, false);
+    }
+};
+
+// util/inc/WireCellUtil/Spectrum.h:56-89 (hermitian_mirror) +
+// aux/src/DftTools.cxx:39-50 (inv_c2r).
+template <typename T>
+static std::vector<T> inv_c2r(const std::vector<std::complex<T>>& spec)
+{
+    using C = std::complex<T>;
+    const size_t len = spec.size();
+    std::vector<C> sym(len);
+    const size_t half = len / 2 + 1;
+    std::copy(spec.begin(), spec.begin() + std::min(half, len), sym.begin());
+    sym[0] = C(std::real(sym[0]), 0);
+    const size_t mid = len / 2;
+    if (len % 2) {
+        for (size_t i = 1; i <= mid; ++i) sym[len - i] = sym[i];
+    }
+    else {
+        sym[mid] = C(std::real(sym[mid]), 0);
+        for (size_t i = 1; i < mid; ++i) sym[len - i] = sym[i];
+    }
+    for (size_t i = mid + 1; i < len; ++i) sym[i] = std::conj(sym[i]);
+    Dft<T>::inv1d(sym.data(), (int)len);
+    std::vector<T> out(len);
+    for (size_t i = 0; i < len; ++i) out[i] = std::real(sym[i]);
+    return out;
+}
+
+// aux/src/DftTools.cxx:24-30 (fwd_r2c, full complex length)
+template <typename T>
+static std::vector<std::complex<T>> fwd_r2c(const std::vector<T>& v)
+{
+    std::vector<std::complex<T>> c(v.size());
+    for (size_t i = 0; i < v.size(); ++i) c[i] = std::complex<T>(v[i], 0);
+    Dft<T>::fwd1d(c.data(), (int)c.size());
+    return c;
+}
+
+// ---------------------------------------------------------------------------
+// Depos. Layout of one depo: t, q, x, y, z, extent_long, extent_tran.
+// ---------------------------------------------------------------------------
+struct Depo {
+    double t, q, x, y, z, el, et;
+    int index;  // position in the caller's input array
+};
+
+// ---------------------------------------------------------------------------
+// Drifter::insert (no fluctuation) -- gen/src/Drifter.cxx:127-196,
+// Xregion tests gen/src/Drifter.cxx:53-60.
+// ---------------------------------------------------------------------------
+struct XRegion {
+    double anode, response, cathode;
+    bool inside_response(double x) const { return (anode < x and x < response) or (response < x and x < anode); }
+    bool inside_bulk(double x) const { return (response < x and x < cathode) or (cathode < x and x < response); }
+};
+
+struct DriftParams {
+    double DL, DT, lifetime, speed, toffset;
+    std::vector<XRegion> xregions;
+};
+
+static bool drift_one(const DriftParams& dp, const Depo& in, Depo& out)
+{
+    const double Qi = in.q;
+    if (Qi == 0.0) return false;
+    double respx = 0, direction = 0.0;
+    const XRegion* xr = nullptr;
+    for (auto& r : dp.xregions)
+        if (r.inside_response(in.x)) { xr = &r; break; }
+    if (xr) { respx = xr->response; direction = -1.0; }
+    else {
+        for (auto& r : dp.xregions)
+            if (r.inside_bulk(in.x)) { xr = &r; break; }
+        if (xr) { respx = xr->response; direction = 1.0; }
+    }
+    if (!xr) return false;
+    const double dt = std::abs((respx - in.x) / dp.speed);
+    double dL = in.el, dT = in.et;
+    double Qf = Qi;
+    if (direction > 0) {
+        const double absorbprob = 1 - exp(-dt / dp.lifetime);
+        double dQ = Qi * absorbprob;
+        Qf = Qi - dQ;
+        dL = sqrt(2.0 * dp.DL * dt + dL * dL);
+        dT = sqrt(2.0 * dp.DT * dt + dT * dT);
+    }
+    out = in;
+    out.t = in.t + direction * dt + dp.toffset;
+    out.x = respx;
+    out.q = Qf;
+    out.el = dL;
+    out.et = dT;
+    return true;
+}
+
+// Drifter::flush -- time-ordered output (gen/src/Drifter.cxx:198-209).
+static std::vector<Depo> drift_all(const DriftParams& dp, const std::vector<Depo>& in)
+{
+    std::vector<Depo> out;
+    out.reserve(in.size());
+    for (auto& d : in) {
+        Depo o;
+        if (drift_one(dp, d, o)) out.push_back(o);
+    }
+    std::stable_sort(out.begin(), out.end(), [](const Depo& a, const Depo& b) { return a.t < b.t; });
+    return out;
+}
+
+// BoundingBox::inside -- util/src/BoundingBox.cxx:37-56.
+static bool bb_inside(const double* lo, const double* hi, const Depo& d)
+{
+    const double p[3] = {d.x, d.y, d.z};
+    for (int i = 0; i < 3; ++i) {
+        const double b1 = lo[i], b2 = hi[i];
+        if (b1 < b2) {
+            if (p[i] < b1 or p[i] > b2) return false;
+            continue;
+        }
+        if (b2 < b1) {
+            if (p[i] < b2 or p[i] > b1) return false;
+            continue;
+        }
+    }
+    return true;
+}
+
+// ---------------------------------------------------------------------------
+// GausDesc -- gen/inc/WireCellGen/GaussianDiffusion.h:20-63 and
+// gen/src/GaussianDiffusion.cxx:30-92.
+// ---------------------------------------------------------------------------
+struct GausDesc {
+    double center, sigma;
+    double distance(double x) const
+    {
+        double ret = 0.0;
+        if (!sigma) ret = x - center;
+        else ret = (x - center) / sigma;
+        return ret;
+    }
+    std::pair<double, double> sigma_range(double nsigma) const
+    {
+        return {center - sigma * nsigma, center + sigma * nsigma};
+    }
+    std::vector<double> binint(double start, double step, int nbins) const
+    {
+        std::vector<double> bins;
+        if (!sigma) {
+            bins.assign(1, 1.0);
+        }
+        else {
+            bins.assign(nbins, 0.0);
+            std::vector<double> erfs(nbins + 1, 0.0);
+            const double sqrt2 = sqrt(2.0);
+            for (int ind = 0; ind <= nbins; ++ind) {
+                double x = (start + step * ind - center) / (sqrt2 * sigma);
+                erfs[ind] = 0.5 * std::erf(x);
+            }
+            for (int ib = 0; ib < nbins; ++ib) bins[ib] = erfs[ib + 1] - erfs[ib];
+        }
+        return bins;
+    }
+    std::vector<double> weight(double start, double step, int nbins, const std::vector<double>& pvec) const
+    {
+        std::vector<double> wt;
+        if (!sigma) {
+            wt.assign(1, (start + step - center) / step);
+        }
+        else {
+            wt.assign(nbins, 0.0);
+            const double pi = 4.0 * atan(1);
+            double x2 = start;
+            double x1 = 0;
+            double gaus2 = exp(-0.5 * (start - center) / sigma * (start - center) / sigma);
+            double gaus1 = 0;
+            for (int ind = 0; ind < nbins; ind++) {
+                x1 = x2;
+                x2 = x1 + step;
+                double rel = (x2 - center) / sigma;
+                gaus1 = gaus2;
+                gaus2 = exp(-0.5 * rel * rel);
+                wt[ind] = -1.0 * sigma / (x1 - x2) * (gaus2 - gaus1) / sqrt(2.0 * pi) / pvec[ind] +
+                          (center - x2) / (x1 - x2);
+            }
+        }
+        return wt;
+    }
+};
+
+// One sampled diffusion patch (GaussianDiffusion, gen/src/GaussianDiffusion.cxx:116-229).
+template <typename T>
+struct Patch {
+    int toffset{-1}, poffset{-1};
+    int nt{0}, np{0};
+    std::vector<T> val;        // [np][nt]
+    std::vector<double> qw;    // np linear weights
+};
+
+template <typename T>
+static void set_sampling(const Depo& depo, const GausDesc& td, const GausDesc& pd, const Binning& tb,
+                         const Binning& pb, double nsigma, Patch<T>& out)
+{
+    out.toffset = out.poffset = -1;
+    out.nt = out.np = 0;
+    out.val.clear();
+    out.qw.clear();
+    auto tr = td.sigma_range(nsigma);
+    auto tbr = tb.sample_bin_range(tr.first, tr.second);
+    const int ntss = std::max(tbr.second - tbr.first, 0);
+    out.toffset = tbr.first;
+    auto tvec = td.binint(tb.edge(out.toffset), tb.binsize, ntss);
+    if (!ntss || tbr.second <= tbr.first) { out.nt = out.np = 0; return; }
+
+    auto pr = pd.sigma_range(nsigma);
+    auto pbr = pb.sample_bin_range(pr.first, pr.second);
+    const int npss = std::max(pbr.second - pbr.first, 0);
+    out.poffset = pbr.first;
+    auto pvec = pd.binint(pb.edge(out.poffset), pb.binsize, npss);
+    if (!npss || pbr.second <= pbr.first) { out.nt = out.np = 0; return; }
+
+    out.qw = pd.weight(pb.edge(out.poffset), pb.binsize, npss, pvec);  // weightstrat 2 (linear)
+    out.nt = ntss;
+    out.np = npss;
+    out.val.assign((size_t)npss * ntss, (T)0);
+    double raw_sum = 0.0;
+    for (int ip = 0; ip < npss; ++ip) {
+        for (int it = 0; it < ntss; ++it) {
+            const double v = pvec[ip] * tvec[it];
+            raw_sum += v;
+            out.val[(size_t)ip * ntss + it] = (T)v;
+        }
+    }
+    const double depo_charge = depo.q;
+    const T scale = (T)(depo_charge / raw_sum);  // Eigen float array *= double scalar
+    for (auto& v : out.val) v *= scale;
+}
+
+// ---------------------------------------------------------------------------
+// PlaneImpactResponse -- gen/src/PlaneImpactResponse.cxx:89-320.
+// ---------------------------------------------------------------------------
+template <typename T>
+struct ImpactResp {
+    std::vector<std::complex<T>> spectrum;
+    std::vector<T> waveform;
+    int waveform_pad{0};
+};
+
+template <typename T>
+struct PIR {
+    std::vector<ImpactResp<T>> ir;
+    std::vector<std::vector<int>> bywire;
+    double half_extent{0}, pitch{0}, impact{0};
+    int nwires() const { return (int)bywire.size(); }
+    int nimp_per_wire() const { return (int)bywire[0].size(); }
+
+    // PlaneImpactResponse.cxx:278-292
+    std::pair<int, int> closest_wire_impact(double relpitch) const
+    {
+        const int center_wire = nwires() / 2;
+        const int relwire = int(round(relpitch / pitch));
+        const int wire_index = center_wire + relwire;
+        const double remainder_pitch = relpitch - relwire * pitch;
+        const int impact_index = int(round(remainder_pitch / impact)) + nimp_per_wire() / 2;
+        return {wire_index, impact_index};
+    }
+    // PlaneImpactResponse.cxx:294-320; returns -1 where the reference throws.
+    int closest(double relpitch) const
+    {
+        if (relpitch < -half_extent || relpitch > half_extent) return -1;
+        auto wi = closest_wire_impact(relpitch);
+        if (wi.first < 0 || wi.first >= (int)bywire.size()) return -1;
+        const auto& region = bywire[wi.first];
+        if (wi.second < 0 || wi.second >= (int)region.size()) return -1;
+        int irind = region[wi.second];
+        if (irind < 0 || irind > (int)ir.size()) return -1;
+        return irind;
+    }
+};
+
+struct FRPlane {
+    int npaths, nsamp;
+    const double* pitchpos;  // [npaths]
+    const double* current;   // [npaths][nsamp]
+    double pitch;            // PlaneResponse::pitch
+};
+
+// PlaneImpactResponse::build_responses, gen/src/PlaneImpactResponse.cxx:89-269
+// (no long responses: they are empty in every configuration handled here).
+template <typename T>
+static void build_pir(const FRPlane& fr, double tstart, double period, const std::vector<std::vector<double>>& shorts,
+                      double overall_short_padding, double tick, int nbins, PIR<T>& pir)
+{
+    using C = std::complex<T>;
+    const size_t n_short = fft_best_length((size_t)(overall_short_padding / tick), false);
+    std::vector<C> short_spec(n_short, C(1.0, 0.0));
+    for (auto& sw : shorts) {
+        std::vector<T> wave(sw.begin(), sw.end());
+        wave.resize(n_short, 0);
+        auto spec = fwd_r2c<T>(wave);
+        for (size_t i = 0; i < n_short; ++i) short_spec[i] *= spec[i];
+    }
+    const int npaths = fr.npaths;
+    const int n_per = 6;
+    const int n_wires = npaths / n_per;
+    const int n_wires_half = n_wires / 2;
+    pir.impact = std::abs(fr.pitchpos[1] - fr.pitchpos[0]);
+    pir.half_extent = std::max(std::abs(fr.pitchpos[0]), std::abs(fr.pitchpos[npaths - 1]));
+    pir.pitch = 2.0 * std::abs(fr.pitchpos[n_per - 1] - fr.pitchpos[0]);
+
+    const int rawresp_size = fr.nsamp;
+    Binning rawbins(rawresp_size, tstart, tstart + rawresp_size * period);
+    const double oopsilon = 1e-15 * fr.pitch;
+    std::map<int, std::vector<int>> wire_to_ind;
+    const int waveform_pad = (int)(overall_short_padding / tick);
+    pir.ir.clear();
+    for (int ipath = 0; ipath < npaths; ++ipath) {
+        const int wirenum = int(ceil((fr.pitchpos[ipath] - oopsilon) / fr.pitch));
+        wire_to_ind[wirenum].push_back(ipath);
+        std::vector<T> wave(n_short, 0.0);
+        for (int rind = 0; rind < rawresp_size; ++rind) {
+            const double time = rawbins.center(rind);
+            const size_t bin = time / tick;
+            if (bin >= n_short) throw std::runtime_error("out of bounds field response");
+            const double induced_charge = fr.current[(size_t)ipath * fr.nsamp + rind] * period;
+            wave[bin] += induced_charge;
+        }
+        auto spec = fwd_r2c<T>(wave);
+        if (!shorts.empty())
+            for (size_t f = 0; f < n_short; ++f) spec[f] *= short_spec[f];
+        std::vector<T> wf = inv_c2r<T>(spec);
+        wf.resize(nbins, 0);
+        ImpactResp<T> r;
+        r.spectrum = fwd_r2c<T>(wf);
+        r.waveform = wf;
+        r.waveform_pad = waveform_pad;
+        pir.ir.push_back(std::move(r));
+    }
+    pir.bywire.clear();
+    for (int irel = -n_wires_half; irel <= n_wires_half; ++irel) {
+        auto direct = wire_to_ind[irel];
+        auto other = wire_to_ind[-irel];
+        std::vector<int> idx(direct.begin(), direct.end());
+        if (!other.empty())
+            for (auto it = other.rbegin() + 1; it != other.rend(); ++it) idx.push_back(*it);
+        pir.bywire.push_back(idx);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// BinnedDiffusion_transform -- gen/src/BinnedDiffusion_transform.cxx.
+// ---------------------------------------------------------------------------
+struct Diff {
+    Depo depo;
+    GausDesc td, pd;
+};
+
+struct PlaneRecord {  // per (plane, input depo) bookkeeping for bit-exact checks
+    int added{0}, toffset{-1}, poffset{-1}, nt{0}, np{0};
+};
+
+template <typename T>
+struct BinnedDiffusion {
+    const Pimpos& pimpos;
+    Binning tbins;
+    double nsigma;
+    std::vector<Diff> diffs;
+    int outside_time{0}, outside_pitch{0};
+    BinnedDiffusion(const Pimpos& p, const Binning& tb, double ns) : pimpos(p), tbins(tb), nsigma(ns) {}
+
+    // BinnedDiffusion_transform.cxx:37-92
+    bool add(const Depo& depo, double sigma_time, double sigma_pitch)
+    {
+        const double center_time = depo.t;
+        const double center_pitch = pimpos.distance(V3{depo.x, depo.y, depo.z});
+        GausDesc td{center_time, sigma_time};
+        {
+            double nmin = td.distance(tbins.minv);
+            double nmax = td.distance(tbins.maxv);
+            double eff = sigma_time > 0 ? nsigma : 0;
+            if (nmin > eff || nmax < -eff) { ++outside_time; return false; }
+        }
+        const Binning& ib = pimpos.impact;
+        GausDesc pd{center_pitch, sigma_pitch};
+        {
+            double nmin = pd.distance(ib.minv);
+            double nmax = pd.distance(ib.maxv);
+            double eff = sigma_pitch > 0 ? nsigma : 0;
+            if (nmin > eff || nmax < -eff) { ++outside_pitch; return false; }
+        }
+        diffs.push_back(Diff{depo, td, pd});
+        return true;
+    }
+
+    // BinnedDiffusion_transform.cxx:227-391
+    void get_charge_vec(std::vector<std::vector<std::tuple<int, int, double>>>& vvc, const std::vector<int>& vec_impact,
+                        std::vector<PlaneRecord>* rec)
+    {
+        const Binning& ib = pimpos.impact;
+        std::map<int, int> map_redimp_vec;
+        std::vector<std::unordered_map<long int, int>> vmpp(vec_impact.size());
+        for (size_t i = 0; i != vec_impact.size(); i++) map_redimp_vec[vec_impact[i]] = int(i);
+        const Binning& rb = pimpos.region;
+        std::map<int, int> map_imp_ch, map_imp_redimp;
+        for (int w = 0; w != rb.nbins; w++) {
+            int wimp = pimpos.wire_impact(w);
+            auto rr = pimpos.wire_impacts(w);
+            for (int imp = rr.first; imp != rr.second; imp++) {
+                map_imp_ch[imp] = w;
+                map_imp_redimp[imp] = imp - wimp;
+            }
+        }
+        const int min_imp = 0, max_imp = ib.nbins;
+        int counter = 0;
+        Patch<T> patch;
+        for (auto& d : diffs) {
+            set_sampling<T>(d.depo, d.td, d.pd, tbins, ib, nsigma, patch);
+            counter++;
+            if (rec) {
+                auto& r = (*rec)[d.depo.index];
+                r.toffset = patch.toffset;
+                r.poffset = patch.poffset;
+                r.nt = patch.nt;
+                r.np = patch.np;
+            }
+            const int np = patch.np, nt = patch.nt;
+            for (int pbin = 0; pbin != np; pbin++) {
+                int abs_pbin = pbin + patch.poffset;
+                if (abs_pbin < min_imp || abs_pbin >= max_imp) continue;
+                double weight = patch.qw[pbin];
+                const int channel = map_imp_ch[abs_pbin];
+                const int redimp = map_imp_redimp[abs_pbin];
+                const int a0 = map_redimp_vec[redimp];
+                const int a1 = map_redimp_vec[redimp + 1];
+                auto& m0 = vmpp.at(a0);
+                auto& m1 = vmpp.at(a1);
+                auto& v0 = vvc.at(a0);
+                auto& v1 = vvc.at(a1);
+                for (int tbin = 0; tbin != nt; tbin++) {
+                    int abs_tbin = tbin + patch.toffset;
+                    double charge = patch.val[(size_t)pbin * nt + tbin];
+                    long int key = channel * 100000 + abs_tbin;
+                    auto it = m0.find(key);
+                    if (it == m0.end()) {
+                        m0[key] = v0.size();
+                        v0.emplace_back(channel, abs_tbin, charge * weight);
+                    }
+                    else {
+                        std::get<2>(v0.at(it->second)) += charge * weight;
+                    }
+                    auto it1 = m1.find(key);
+                    if (it1 == m1.end()) {
+                        m1[key] = v1.size();
+                        v1.emplace_back(channel, abs_tbin, charge * (1 - weight));
+                    }
+                    else {
+                        std::get<2>(v1.at(it1->second)) += charge * (1 - weight);
+                    }
+                }
+            }
+            if (counter % 5000 == 0)
+                for (auto& m : vmpp) m.clear();
+        }
+    }
+
+    // BinnedDiffusion_transform.cxx:416-464
+    std::pair<double, double> range(bool pitch) const
+    {
+        int ncount = -1;
+        double vmin = 0, vmax = 0;
+        for (auto& d : diffs) {
+            ++ncount;
+            const GausDesc& g = pitch ? d.pd : d.td;
+            const double lo = g.center - g.sigma * nsigma;
+            const double hi = g.center + g.sigma * nsigma;
+            if (!ncount) { vmin = lo; vmax = hi; continue; }
+            vmin = std::min(vmin, lo);
+            vmax = std::max(vmax, hi);
+        }
+        return {vmin, vmax};
+    }
+    std::pair<int, int> impact_bin_range() const
+    {
+        auto mm = range(true);
+        const Binning& ib = pimpos.impact;
+        return {std::max(ib.bin(mm.first), 0), std::min(ib.bin(mm.second) + 1, ib.nbins)};
+    }
+    std::pair<int, int> time_bin_range() const
+    {
+        auto mm = range(false);
+        return {std::max(tbins.bin(mm.first), 0), std::min(tbins.bin(mm.second) + 1, tbins.nbins)};
+    }
+};
+
+// ---------------------------------------------------------------------------
+// ImpactTransform -- gen/src/ImpactTransform.cxx:19-347.
+// ---------------------------------------------------------------------------
+struct Window {
+    int start_ch, end_ch, start_tick, end_tick, nw, nt;
+};
+
+template <typename T>
+struct ImpactTransform {
+    using C = std::complex<T>;
+    Window win{};
+    std::vector<T> decon;  // [nw][nt]
+
+    // Time-domain response reduced to nt samples, then r2c (ImpactTransform.cxx:158-168).
+    static std::vector<C> reduced_spectrum(const ImpactResp<T>& r, int nt)
+    {
+        std::vector<T> t = inv_c2r<T>(r.spectrum);
+        std::vector<T> red(nt, 0);
+        for (int i = 0; i < nt; ++i) {
+            if (i >= (int)t.size()) break;
+            red[i] = t[i];
+        }
+        return fwd_r2c<T>(red);
+    }
+
+    ImpactTransform(const PIR<T>& pir, BinnedDiffusion<T>& bd, std::vector<PlaneRecord>* rec)
+    {
+        const int G = std::round(pir.pitch / pir.impact) + 1;
+        const int npad = std::round((pir.nwires() - 1) / 2.);
+        std::vector<int> vec_impact;
+        std::vector<std::map<int, int>> vmr;  // group -> {wire offset -> ir index}
+        for (int i = 0; i != G; i++) {
+            double rel;
+            if (i != G - 1) rel = -pir.pitch / 2. + pir.impact * i + 1e-9;
+            else rel = -pir.pitch / 2. + pir.impact * i - 1e-9;
+            vec_impact.push_back(std::round(rel / pir.impact));
+            std::map<int, int> mr;
+            for (int j = 0; j != pir.nwires(); j++) {
+                int k = pir.closest(rel - (j - npad) * pir.pitch);
+                if (k < 0) continue;
+                mr[j - npad] = k;
+            }
+            vmr.push_back(mr);
+        }
+        std::vector<std::vector<std::tuple<int, int, double>>> vvc(G);
+        bd.get_charge_vec(vvc, vec_impact, rec);
+
+        auto ir = bd.impact_bin_range();
+        auto tr = bd.time_bin_range();
+        int start_ch = std::floor(ir.first * 1.0 / (G - 1)) - 1;
+        int end_ch = std::ceil(ir.second * 1.0 / (G - 1)) + 2;
+        if ((end_ch - start_ch) % 2 == 1) end_ch += 1;
+        int start_tick = tr.first - 1;
+        int end_tick = tr.second + 2;
+        if ((end_tick - start_tick) % 2 == 1) end_tick += 1;
+        const size_t ntotal_wires = fft_best_length(end_ch - start_ch + 2 * npad, true);
+        int npad_wire = (ntotal_wires - end_ch + start_ch) / 2;
+        win.start_ch = start_ch - npad_wire;
+        win.end_ch = end_ch + npad_wire;
+        int npad_time = pir.ir[pir.closest(0)].waveform_pad;
+        const size_t ntotal_ticks = fft_best_length(end_tick - start_tick + npad_time, false);
+        npad_time = ntotal_ticks - end_tick + start_tick;
+        win.start_tick = start_tick;
+        win.end_tick = end_tick + npad_time;
+        const int NW = end_ch - start_ch + 2 * npad_wire;
+        const int NT = win.end_tick - win.start_tick;
+        win.nw = NW;
+        win.nt = NT;
+        std::vector<C> acc((size_t)NW * NT, C(0, 0));
+        auto at = [&](std::vector<C>& a, int r, int c) -> C& { return a[(size_t)r * NT + c]; };
+
+        auto build_resp = [&](int i) {
+            std::vector<C> resp((size_t)NW * NT, C(0, 0));
+            auto& mr = vmr.at(i);
+            auto row = [&](int rr, int woff) {
+                auto rs = reduced_spectrum(pir.ir.at(mr.at(woff)), NT);
+                for (int c = 0; c < NT; ++c) resp[(size_t)rr * NT + c] = rs[c];
+            };
+            row(0, 0);
+            for (int irow = 0; irow != npad; irow++) {
+                row(irow + 1, irow + 1);
+                row(end_ch - start_ch - 1 - irow + 2 * npad_wire, -irow - 1);
+            }
+            Dft<T>::fwd1b(resp.data(), NW, NT, 0);
+            return resp;
+        };
+
+        const int num_double = (G - 1) / 2;
+        for (int i = 0; i != num_double; i++) {
+            std::vector<C> c((size_t)NW * NT, C(0, 0));
+            for (auto& e : vvc.at(i))
+                at(c, std::get<0>(e) + npad_wire - start_ch, std::get<1>(e) - win.start_tick) += (T)std::get<2>(e);
+            vvc.at(i).clear();
+            int ii = num_double * 2 - i;
+            for (auto& e : vvc.at(ii))
+                at(c, end_ch + npad_wire - 1 - std::get<0>(e), std::get<1>(e) - win.start_tick) +=
+                    C(0, (T)std::get<2>(e));
+            vvc.at(ii).clear();
+            Dft<T>::fwd2d(c.data(), NW, NT);
+            auto resp = build_resp(i);
+            for (size_t k = 0; k < c.size(); ++k) c[k] *= resp[k];
+            Dft<T>::inv1b(c.data(), NW, NT, 0);
+            for (size_t k = 0; k < c.size(); ++k) acc[k] += c[k];
+        }
+        {
+            int i = num_double;
+            std::vector<T> dtw((size_t)NW * NT, 0);
+            for (auto& e : vvc.at(i)) {
+                T& v = dtw[(size_t)(std::get<0>(e) + npad_wire - start_ch) * NT + (std::get<1>(e) - win.start_tick)];
+                v = (T)(v + std::get<2>(e));
+            }
+            vvc.at(i).clear();
+            std::vector<C> d((size_t)NW * NT);
+            for (size_t k = 0; k < d.size(); ++k) d[k] = C(dtw[k], 0);
+            Dft<T>::fwd1b(d.data(), NW, NT, 1);
+            Dft<T>::fwd1b(d.data(), NW, NT, 0);
+            auto resp = build_resp(i);
+            for (size_t k = 0; k < d.size(); ++k) d[k] *= resp[k];
+            Dft<T>::inv1b(d.data(), NW, NT, 0);
+            for (size_t k = 0; k < d.size(); ++k) acc[k] += d[k];
+        }
+        Dft<T>::inv1b(acc.data(), NW, NT, 1);
+        decon.assign((size_t)NW * NT, 0);
+        for (int r = 0; r < NW; ++r)
+            for (int c2 = 0; c2 < NT; ++c2)
+                decon[(size_t)r * NT + c2] = std::real(acc[(size_t)r * NT + c2]) +
+                                             std::imag(acc[(size_t)(NW - 1 - r) * NT + c2]);
+    }
+
+    // ImpactTransform::waveform, ImpactTransform.cxx:312-347 (no long response).
+    void waveform(int iwire, int nsamples, T* out) const
+    {
+        std::fill(out, out + nsamples, (T)0);
+        if (iwire < win.start_ch || iwire >= win.end_ch) return;
+        for (int i = 0; i != nsamples; i++)
+            if (i >= win.start_tick && i < win.end_tick)
+                out[i] = decon[(size_t)(iwire - win.start_ch) * win.nt + (i - win.start_tick)];
+    }
+};
+
+}  // namespace orc
+
+// ============================================================================
+// C interface for the Python test harness (ctypes).
+// ============================================================================
+extern "C" {
+
+struct OrcPlane {
+    int nwires;
+    int nimp;
+    double pitchmin, pitchmax;
+    double wire[3], pitch[3], origin[3];
+    // field response of this plane (Response::Schema::PlaneResponse)
+    int npaths, nfr;
+    const double* pitchpos;  // [npaths]
+    const double* current;   // [npaths][nfr]
+    double fr_pitch;
+};
+
+struct OrcJob {
+    // DepoTransform configuration (gen/src/DepoTransform.cxx:76-153)
+    double start_time, readout_time, tick, drift_speed, nsigma;
+    // Drifter configuration (gen/src/Drifter.cxx:94-123); drift=0 means the depos are already drifted.
+    int drift;
+    double DL, DT, lifetime, drifter_speed, toffset;
+    int nxregions;
+    const double* xregions;  // [n][3] anode, response, cathode
+    // face sensitive volume (two corners); have_bb=0 means no cut
+    int have_bb;
+    double bb_lo[3], bb_hi[3];
+    // PlaneImpactResponse configuration (gen/src/PlaneImpactResponse.cxx:35-87)
+    double fr_tstart, fr_period;
+    int nshort;
+    const int* short_len;
+    const double* short_wave;  // concatenated
+    double overall_short_padding;
+    int pir_nticks;
+    int nplanes;
+    const OrcPlane* planes;
+    int ndepos;
+    const double* depos;  // [n][7] t, q, x, y, z, extent_long, extent_tran
+    int fp64;
+    int nthreads;
+};
+
+struct OrcPlaneOut {
+    int start_ch, end_ch, start_tick, end_tick, nw, nt;
+    int ndepos_added, outside_time, outside_pitch;
+};
+
+int orc_fft_best_length(long n, int keep) { return (int)orc::fft_best_length((size_t)n, keep != 0); }
+
+int orc_binning_bin(int nbins, double lo, double hi, double v) { return orc::Binning(nbins, lo, hi).bin(v); }
+
+void orc_sample_bin_range(int nbins, double lo, double hi, double a, double b, int* out)
+{
+    auto r = orc::Binning(nbins, lo, hi).sample_bin_range(a, b);
+    out[0] = r.first;
+    out[1] = r.second;
+}
+
+// 1-D complex transforms for tests: data is interleaved re,im.
+void orc_fft_f32(float* data, int n, int inverse)
+{
+    auto* c = reinterpret_cast<std::complex<float>*>(data);
+    if (inverse) orc::Dft<float>::inv1d(c, n);
+    else orc::Dft<float>::fwd1d(c, n);
+}
+void orc_fft_f64(double* data, int n, int inverse)
+{
+    auto* c = reinterpret_cast<std::complex<double>*>(data);
+    if (inverse) orc::Dft<double>::inv1d(c, n);
+    else orc::Dft<double>::fwd1d(c, n);
+}
+
+// One GaussianDiffusion::set_sampling for tests. out_i: toffset, poffset, nt, np.
+// patch receives np*nt values (caller provides capacity cap), weights np values.
+int orc_set_sampling(double t, double q, double pitch_center, double sigma_t, double sigma_p, int ntbins, double tmin,
+                     double tmax, int nibins, double imin, double imax, double nsigma, int fp64, int cap,
+                     double* patch, double* weights, int* out_i)
+{
+    orc::Depo d{t, q, 0, 0, 0, 0, 0, 0};
+    orc::GausDesc td{t, sigma_t}, pd{pitch_center, sigma_p};
+    orc::Binning tb(ntbins, tmin, tmax), pb(nibins, imin, imax);
+    auto emit = [&](auto& P) {
+        out_i[0] = P.toffset;
+        out_i[1] = P.poffset;
+        out_i[2] = P.nt;
+        out_i[3] = P.np;
+        if ((long)P.nt * P.np > cap) return -1;
+        for (size_t i = 0; i < P.val.size(); ++i) patch[i] = P.val[i];
+        for (int i = 0; i < P.np; ++i) weights[i] = P.qw[i];
+        return 0;
+    };
+    if (fp64) {
+        orc::Patch<double> P;
+        orc::set_sampling<double>(d, td, pd, tb, pb, nsigma, P);
+        return emit(P);
+    }
+    orc::Patch<float> P;
+    orc::set_sampling<float>(d, td, pd, tb, pb, nsigma, P);
+    return emit(P);
+}
+
+// Drifter::insert + flush for tests: returns the number of output depos
+// (time ordered); out has room for n*8 doubles (7 fields + input index).
+int orc_drift(const OrcJob* job, double* out)
+{
+    orc::DriftParams dp{job->DL, job->DT, job->lifetime, job->drifter_speed, job->toffset, {}};
+    for (int i = 0; i < job->nxregions; ++i)
+        dp.xregions.push_back({job->xregions[3 * i], job->xregions[3 * i + 1], job->xregions[3 * i + 2]});
+    std::vector<orc::Depo> in;
+    for (int i = 0; i < job->ndepos; ++i) {
+        const double* p = job->depos + 7 * (size_t)i;
+        in.push_back({p[0], p[1], p[2], p[3], p[4], p[5], p[6], i});
+    }
+    auto o = orc::drift_all(dp, in);
+    for (size_t i = 0; i < o.size(); ++i) {
+        double* q = out + 8 * i;
+        q[0] = o[i].t; q[1] = o[i].q; q[2] = o[i].x; q[3] = o[i].y; q[4] = o[i].z;
+        q[5] = o[i].el; q[6] = o[i].et; q[7] = o[i].index;
+    }
+    return (int)o.size();
+}
+
+// PIR build for tests: fills waveforms [npaths][pir_nticks] (as double),
+// bywire [nwires][nimp] indices; returns nwires*1000+nimp, or -1 on error.
+int orc_pir_build(const OrcJob* job, int iplane, double* waveforms, int* bywire, double* pitch_impact_extent)
+{
+    auto run = [&](auto tag) -> int {
+        using T = decltype(tag);
+        const OrcPlane& pl = job->planes[iplane];
+        std::vector<std::vector<double>> shorts;
+        size_t off = 0;
+        for (int s = 0; s < job->nshort; ++s) {
+            shorts.emplace_back(job->short_wave + off, job->short_wave + off + job->short_len[s]);
+            off += job->short_len[s];
+        }
+        orc::FRPlane fr{pl.npaths, pl.nfr, pl.pitchpos, pl.current, pl.fr_pitch};
+        orc::PIR<T> pir;
+        orc::build_pir<T>(fr, job->fr_tstart, job->fr_period, shorts, job->overall_short_padding, job->tick,
+                          job->pir_nticks, pir);
+        for (size_t p = 0; p < pir.ir.size(); ++p)
+            for (int k = 0; k < job->pir_nticks; ++k)
+                waveforms[p * job->pir_nticks + k] = pir.ir[p].waveform[k];
+        const int nw = pir.nwires(), ni = pir.nimp_per_wire();
+        for (int w = 0; w < nw; ++w)
+            for (int k = 0; k < ni; ++k)
+                bywire[w * ni + k] = k < (int)pir.bywire[w].size() ? pir.bywire[w][k] : -1;
+        pitch_impact_extent[0] = pir.pitch;
+        pitch_impact_extent[1] = pir.impact;
+        pitch_impact_extent[2] = pir.half_extent;
+        return nw * 1000 + ni;
+    };
+    try {
+        return job->fp64 ? run(double{}) : run(float{});
+    }
+    catch (...) {
+        return -1;
+    }
+}
+
+// The whole DepoTransform::operator() (gen/src/DepoTransform.cxx:155-224) for
+// one face: optional drift, sensitive cut, then per plane BinnedDiffusion +
+// ImpactTransform + waveform extraction.
+//   frame : [sum_p nwires_p][nticks] dense waveforms (float or double per fp64)
+//   pout  : per-plane window and counters
+//   rec   : optional [nplanes][ndepos][5] ints (added, toffset, poffset, nt, np)
+//           indexed by the depo's position in the input array
+// Returns 0 on success.
+int orc_run(const OrcJob* job, void* frame, OrcPlaneOut* pout, int* rec)
+{
+    try {
+        std::vector<orc::Depo> depos;
+        for (int i = 0; i < job->ndepos; ++i) {
+            const double* p = job->depos + 7 * (size_t)i;
+            depos.push_back({p[0], p[1], p[2], p[3], p[4], p[5], p[6], i});
+        }
+        if (job->drift) {
+            orc::DriftParams dp{job->DL, job->DT, job->lifetime, job->drifter_speed, job->toffset, {}};
+            for (int i = 0; i < job->nxregions; ++i)
+                dp.xregions.push_back({job->xregions[3 * i], job->xregions[3 * i + 1], job->xregions[3 * i + 2]});
+            depos = orc::drift_all(dp, depos);  // keeps each depo's input index
+        }
+        // face sensitive volume: DepoTools.cxx:110-123
+        std::vector<orc::Depo> face;
+        for (auto& d : depos)
+            if (!job->have_bb || orc::bb_inside(job->bb_lo, job->bb_hi, d)) face.push_back(d);
+
+        const int nticks = (int)(job->readout_time / job->tick);
+        std::vector<std::vector<double>> shorts;
+        size_t off = 0;
+        for (int s = 0; s < job->nshort; ++s) {
+            shorts.emplace_back(job->short_wave + off, job->short_wave + off + job->short_len[s]);
+            off += job->short_len[s];
+        }
+        std::vector<size_t> row0(job->nplanes + 1, 0);
+        for (int p = 0; p < job->nplanes; ++p) row0[p + 1] = row0[p] + job->planes[p].nwires;
+        const size_t ndep_rec = (size_t)job->ndepos;
+
+        auto do_plane = [&](int ip, auto tag) {
+            using T = decltype(tag);
+            const OrcPlane& pl = job->planes[ip];
+            orc::Pimpos pim(pl.nwires, pl.pitchmin, pl.pitchmax, orc::V3{pl.wire[0], pl.wire[1], pl.wire[2]},
+                            orc::V3{pl.pitch[0], pl.pitch[1], pl.pitch[2]},
+                            orc::V3{pl.origin[0], pl.origin[1], pl.origin[2]}, pl.nimp);
+            orc::FRPlane fr{pl.npaths, pl.nfr, pl.pitchpos, pl.current, pl.fr_pitch};
+            orc::PIR<T> pir;
+            orc::build_pir<T>(fr, job->fr_tstart, job->fr_period, shorts, job->overall_short_padding, job->tick,
+                              job->pir_nticks, pir);
+            orc::Binning tbins(job->readout_time / job->tick, job->start_time, job->start_time + job->readout_time);
+            orc::BinnedDiffusion<T> bd(pim, tbins, job->nsigma);
+            std::vector<orc::PlaneRecord> precs(ndep_rec);
+            for (auto& d : face) {
+                bool ok = bd.add(d, d.el / job->drift_speed, d.et);
+                precs[d.index].added = ok ? 1 : 0;
+            }
+            orc::ImpactTransform<T> it(pir, bd, &precs);
+            OrcPlaneOut& po = pout[ip];
+            po.start_ch = it.win.start_ch;
+            po.end_ch = it.win.end_ch;
+            po.start_tick = it.win.start_tick;
+            po.end_tick = it.win.end_tick;
+            po.nw = it.win.nw;
+            po.nt = it.win.nt;
+            po.ndepos_added = (int)bd.diffs.size();
+            po.outside_time = bd.outside_time;
+            po.outside_pitch = bd.outside_pitch;
+            T* fr_out = reinterpret_cast<T*>(frame) + row0[ip] * (size_t)nticks;
+            for (int w = 0; w < pl.nwires; ++w) it.waveform(w, nticks, fr_out + (size_t)w * nticks);
+            if (rec) {
+                for (size_t k = 0; k < ndep_rec; ++k) {
+                    int* r = rec + ((size_t)ip * ndep_rec + k) * 5;
+                    r[0] = precs[k].added;
+                    r[1] = precs[k].toffset;
+                    r[2] = precs[k].poffset;
+                    r[3] = precs[k].nt;
+                    r[4] = precs[k].np;
+                }
+            }
+        };
+        std::atomic<int> err{0};
+        auto worker = [&](int ip) {
+            try {
+                if (job->fp64) do_plane(ip, double{});
+                else do_plane(ip, float{});
+            }
+            catch (...) {
+                err = 1;
+            }
+        };
+        const int nth = std::max(1, std::min(job->nthreads, job->nplanes));
+        if (nth == 1) {
+            for (int ip = 0; ip < job->nplanes; ++ip) worker(ip);
+        }
+        else {
+            std::vector<std::thread> th;
+            std::atomic<int> next{0};
+            for (int t = 0; t < nth; ++t)
+                th.emplace_back([&]() {
+                    for (int ip = next++; ip < job->nplanes; ip = next++) worker(ip);
+                });
+            for (auto& t : th) t.join();
+        }
+        return err ? -2 : 0;
+    }
+    catch (...) {
+        return -1;
+    }
+}
+
+// Waveform::edge (util/src/Waveform.cxx:136-153) over a float row.
+void orc_edge(const float* wave, int size, int* out)
+{
+    int imin = size, imax = size;
+    for (int ind = 0; ind < size; ++ind) {
+        if (wave[ind] != 0.0f) {
+            if (imin == size) imin = ind;
+            if (imin < size) imax = ind + 1;
+        }
+    }
+    out[0] = imin;
+    out[1] = imax;
+}
+
+}  // extern "C"

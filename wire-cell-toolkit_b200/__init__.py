@@ -1,0 +1,318 @@
+"""wctb200: B200-native Wire-Cell DepoTransform.
+
+Python front end of ``libwctb200.so`` (C ABI in include/wctb200.h).  The
+classes mirror the reference components used on the signal-simulation path:
+
+* :class:`PlaneImpactResponse`  Gen::PlaneImpactResponse (gen/src/PlaneImpactResponse.cxx)
+* :class:`DepoTransform`        Gen::DepoTransform, an IDepoFramer (gen/src/DepoTransform.cxx)
+
+The compute path is the CUDA library; there is no CPU fallback.  Importing
+works without a GPU (the library loads), but every compute call needs one.
+"""
+
+import ctypes as C
+import json
+import os
+
+import numpy as np
+
+from . import _build
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = _build.LIB
+
+WCT_OK, WCT_ERR_ARG, WCT_ERR_CONFIG, WCT_ERR_CUDA, WCT_ERR_STATE, WCT_ERR_RESPONSE, WCT_ERR_SIZE, WCT_EOS = range(8)
+
+_lib = None
+
+
+class WctError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__("wctb200 error %d: %s" % (code, msg))
+        self.code = code
+
+
+class PlaneDesc(C.Structure):
+    _fields_ = [
+        ("nwires", C.c_int), ("nimpacts", C.c_int),
+        ("pitchmin", C.c_double), ("pitchmax", C.c_double),
+        ("wire", C.c_double * 3), ("pitch", C.c_double * 3), ("origin", C.c_double * 3),
+        ("channels", C.c_void_p),
+    ]
+
+
+class FrPlane(C.Structure):
+    _fields_ = [
+        ("npaths", C.c_int), ("nsamples", C.c_int),
+        ("pitchpos", C.c_void_p), ("current", C.c_void_p),
+        ("pitch", C.c_double), ("tstart", C.c_double), ("period", C.c_double),
+    ]
+
+
+class PlaneWindow(C.Structure):
+    _fields_ = [(n, C.c_int) for n in (
+        "face", "plane", "start_ch", "end_ch", "start_tick", "end_tick", "nw_fft", "nt_fft", "nt_gpu",
+        "charge_rows", "npad", "ndepos_added", "outside_time", "outside_pitch")]
+
+    def as_dict(self):
+        return {f: getattr(self, f) for f, _ in self._fields_}
+
+
+# name -> (restype, argtypes); every function listed here is declared in include/wctb200.h
+SIGNATURES = {
+    "wct_version": (C.c_char_p, []),
+    "wct_last_error": (C.c_char_p, []),
+    "wct_pir_create": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_double, C.c_double, C.c_int,
+                                 C.POINTER(C.c_void_p)]),
+    "wct_pir_closest": (C.c_int, [C.c_void_p, C.c_double, C.POINTER(C.c_int)]),
+    "wct_pir_info": (C.c_int, [C.c_void_p] + [C.c_void_p] * 8),
+    "wct_pir_waveform": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p]),
+    "wct_pir_destroy": (C.c_int, [C.c_void_p]),
+    "wct_dt_create": (C.c_int, [C.c_char_p, C.POINTER(C.c_void_p)]),
+    "wct_dt_default_configuration": (C.c_int, [C.c_char_p, C.c_size_t]),
+    "wct_dt_add_face": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(C.c_int)]),
+    "wct_dt_add_plane": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.POINTER(C.c_int)]),
+    "wct_dt_set_response_pir": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_void_p]),
+    "wct_dt_set_response_table": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_double,
+                                            C.c_double, C.c_int, C.c_void_p]),
+    "wct_dt_frame_shape": (C.c_int, [C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
+    "wct_dt_forward": (C.c_int, [C.c_void_p, C.c_void_p, C.c_size_t, C.c_void_p, C.c_void_p, C.POINTER(C.c_int)]),
+    "wct_dt_forward_device": (C.c_int, [C.c_void_p, C.c_void_p, C.c_size_t, C.c_void_p, C.c_void_p,
+                                        C.POINTER(C.c_int), C.c_void_p]),
+    "wct_dt_eos": (C.c_int, [C.c_void_p]),
+    "wct_dt_traces": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                C.POINTER(C.c_int)]),
+    "wct_dt_patch_records": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_size_t]),
+    "wct_dt_set_profiling": (C.c_int, [C.c_void_p, C.c_int]),
+    "wct_dt_stage_times": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.POINTER(C.c_long), C.c_int]),
+    "wct_dt_destroy": (C.c_int, [C.c_void_p]),
+}
+
+STAGES = ("drift+prep", "raster", "time_fft", "wire_conv", "inverse_fft+frame", "other")
+
+
+def build(force=False):
+    return _build.build(force=force)
+
+
+def lib():
+    """Load libwctb200.so (building it first if it is missing or stale)."""
+    global _lib
+    if _lib is None:
+        if _build.stale():
+            _build.build()
+        _lib = C.CDLL(LIB_PATH)
+        for name, (rt, at) in SIGNATURES.items():
+            f = getattr(_lib, name)
+            f.restype = rt
+            f.argtypes = at
+    return _lib
+
+
+def _check(rc):
+    if rc != WCT_OK:
+        raise WctError(rc, lib().wct_last_error().decode())
+    return rc
+
+
+class PlaneImpactResponse:
+    """Gen::PlaneImpactResponse built from a Response::Schema plane and short
+    responses (gen/src/PlaneImpactResponse.cxx:56-269)."""
+
+    def __init__(self, fr, short_responses, overall_short_padding, tick, nticks):
+        L = lib()
+        pp = np.ascontiguousarray(fr["pitchpos"], dtype=np.float64)
+        cur = np.ascontiguousarray(fr["current"], dtype=np.float64)
+        d = FrPlane(pp.shape[0], cur.shape[1], pp.ctypes.data, cur.ctypes.data, fr["pitch"], fr["tstart"],
+                    fr["period"])
+        shorts = [np.asarray(s, dtype=np.float64) for s in short_responses]
+        sl = np.array([len(s) for s in shorts] or [0], dtype=np.int32)
+        sw = np.concatenate(shorts) if shorts else np.zeros(1)
+        h = C.c_void_p()
+        _check(L.wct_pir_create(C.byref(d), len(shorts), sl.ctypes.data, sw.ctypes.data, overall_short_padding,
+                                tick, nticks, C.byref(h)))
+        self.h = h
+
+    def info(self):
+        pitch, impact, he = C.c_double(), C.c_double(), C.c_double()
+        nw, ni, npth, nt, wp = C.c_int(), C.c_int(), C.c_int(), C.c_int(), C.c_int()
+        _check(lib().wct_pir_info(self.h, C.byref(pitch), C.byref(impact), C.byref(he), C.byref(nw), C.byref(ni),
+                                  C.byref(npth), C.byref(nt), C.byref(wp)))
+        return dict(pitch=pitch.value, impact=impact.value, half_extent=he.value, nwires=nw.value,
+                    nimp_per_wire=ni.value, npaths=npth.value, nticks=nt.value, waveform_pad=wp.value)
+
+    def closest(self, relpitch):
+        k = C.c_int()
+        _check(lib().wct_pir_closest(self.h, relpitch, C.byref(k)))
+        return k.value
+
+    def waveform(self, path):
+        out = np.zeros(self.info()["nticks"], dtype=np.float32)
+        _check(lib().wct_pir_waveform(self.h, path, out.ctypes.data))
+        return out
+
+    def __del__(self):
+        if getattr(self, "h", None) and _lib is not None:
+            _lib.wct_pir_destroy(self.h)
+            self.h = None
+
+
+class DepoTransform:
+    """Gen::DepoTransform (IDepoFramer) on the B200.
+
+    ``cfg`` is the reference configuration (gen/src/DepoTransform.cxx:76-153)
+    as a dict, optionally with a "drifter" sub-configuration to drift the
+    depos on the device first."""
+
+    CONFIG_KEYS = ("anode", "pirs", "dft", "rng", "fluctuate", "nsigma", "start_time", "readout_time", "tick",
+                   "drift_speed", "first_frame_number", "drifter", "device")
+
+    def __init__(self, cfg=None):
+        L = lib()
+        js = json.dumps(_jsonable({k: v for k, v in (cfg or {}).items() if k in self.CONFIG_KEYS}))
+        h = C.c_void_p()
+        _check(L.wct_dt_create(js.encode(), C.byref(h)))
+        self.h = h
+        self._pirs = []
+        self.planes = []
+
+    @staticmethod
+    def default_configuration():
+        buf = C.create_string_buffer(4096)
+        _check(lib().wct_dt_default_configuration(buf, 4096))
+        return json.loads(buf.value.decode())
+
+    def add_face(self, bb=None):
+        f = C.c_int()
+        if bb is None:
+            _check(lib().wct_dt_add_face(self.h, None, None, C.byref(f)))
+        else:
+            lo = np.ascontiguousarray(bb[0], dtype=np.float64)
+            hi = np.ascontiguousarray(bb[1], dtype=np.float64)
+            _check(lib().wct_dt_add_face(self.h, lo.ctypes.data, hi.ctypes.data, C.byref(f)))
+        return f.value
+
+    def add_plane(self, face, pl):
+        ch = np.ascontiguousarray(pl.get("channels", np.arange(pl["nwires"])), dtype=np.int32)
+        d = PlaneDesc(pl["nwires"], pl.get("nimp", 10), pl["pitchmin"], pl["pitchmax"], (C.c_double * 3)(*pl["wire"]),
+                      (C.c_double * 3)(*pl["pitch"]), (C.c_double * 3)(*pl["origin"]), ch.ctypes.data)
+        p = C.c_int()
+        _check(lib().wct_dt_add_plane(self.h, face, C.byref(d), C.byref(p)))
+        self.planes.append((face, p.value, pl["nwires"]))
+        return p.value
+
+    def set_response_pir(self, face, plane, pir):
+        _check(lib().wct_dt_set_response_pir(self.h, face, plane, pir.h))
+        self._pirs.append(pir)
+
+    def set_response_table(self, face, plane, table, pitch, impact, waveform_pad):
+        t = np.ascontiguousarray(table, dtype=np.float32)
+        G, J, K = t.shape
+        _check(lib().wct_dt_set_response_table(self.h, face, plane, G, (J - 1) // 2, K, pitch, impact, waveform_pad,
+                                               t.ctypes.data))
+
+    def frame_shape(self):
+        r, t = C.c_int(), C.c_int()
+        _check(lib().wct_dt_frame_shape(self.h, C.byref(r), C.byref(t)))
+        return r.value, t.value
+
+    def __call__(self, depos, out=None):
+        """Host-buffer forward: returns (frame [nrows][nticks] float32, windows, ident).
+        ``out`` may supply the frame buffer (e.g. pinned host memory)."""
+        d = np.ascontiguousarray(depos, dtype=np.float64).reshape(-1, 7)
+        nrows, nticks = self.frame_shape()
+        if out is not None:
+            assert out.shape == (nrows, nticks) and out.dtype == np.float32 and out.flags.c_contiguous
+            frame = out
+        else:
+            frame = np.empty((nrows, nticks), dtype=np.float32)
+        wins = (PlaneWindow * len(self.planes))()
+        ident = C.c_int()
+        _check(lib().wct_dt_forward(self.h, d.ctypes.data if len(d) else None, len(d), frame.ctypes.data,
+                                    C.cast(wins, C.c_void_p), C.byref(ident)))
+        return frame, [w.as_dict() for w in wins], ident.value
+
+    def forward_device(self, d_depos_ptr, ndepos, d_frame_ptr, stream=None):
+        """Device-buffer forward (pointers as ints, e.g. torch.Tensor.data_ptr())."""
+        wins = (PlaneWindow * len(self.planes))()
+        ident = C.c_int()
+        _check(lib().wct_dt_forward_device(self.h, C.c_void_p(d_depos_ptr), ndepos, C.c_void_p(d_frame_ptr),
+                                           C.cast(wins, C.c_void_p), C.byref(ident),
+                                           C.c_void_p(stream) if stream else None))
+        return [w.as_dict() for w in wins], ident.value
+
+    def patch_records(self, face, plane, n):
+        """[n][4] (toffset, poffset, nt, np) per input depo from the last forward call."""
+        out = np.zeros((n, 4), dtype=np.int32)
+        _check(lib().wct_dt_patch_records(self.h, face, plane, out.ctypes.data, n))
+        return out
+
+    def set_profiling(self, on=True):
+        _check(lib().wct_dt_set_profiling(self.h, 1 if on else 0))
+
+    def stage_times(self, reset=True):
+        """{stage: (ms, launches)} accumulated since the last reset, and the total launch count."""
+        ms = np.zeros(6)
+        nl = np.zeros(6, dtype=np.int64)
+        tot = C.c_long()
+        _check(lib().wct_dt_stage_times(self.h, ms.ctypes.data, nl.ctypes.data, 6, C.byref(tot), 1 if reset else 0))
+        return {STAGES[i]: (float(ms[i]), int(nl[i])) for i in range(6)}, tot.value
+
+    def eos(self):
+        return lib().wct_dt_eos(self.h)
+
+    def traces(self, frame):
+        """IFrame traces: list of (channel, tbin, charges) with Waveform::edge trimming."""
+        f = np.ascontiguousarray(frame, dtype=np.float32)
+        n = f.shape[0]
+        ch = np.zeros(n, np.int32)
+        tb = np.zeros(n, np.int32)
+        ln = np.zeros(n, np.int32)
+        off = np.zeros(n, np.int64)
+        k = C.c_int()
+        _check(lib().wct_dt_traces(self.h, f.ctypes.data, ch.ctypes.data, tb.ctypes.data, ln.ctypes.data,
+                                   off.ctypes.data, C.byref(k)))
+        flat = f.reshape(-1)
+        return [(int(ch[i]), int(tb[i]), flat[off[i]:off[i] + ln[i]]) for i in range(k.value)]
+
+    def __del__(self):
+        if getattr(self, "h", None) and _lib is not None:
+            _lib.wct_dt_destroy(self.h)
+            self.h = None
+
+
+def _jsonable(o):
+    if isinstance(o, dict):
+        return {k: _jsonable(v) for k, v in o.items()}
+    if isinstance(o, (list, tuple)):
+        return [_jsonable(v) for v in o]
+    if isinstance(o, np.ndarray):
+        return o.tolist()
+    if isinstance(o, (np.floating, np.integer)):
+        return o.item()
+    return o
+
+
+def drifter_json(dr):
+    """Drifter configuration with xregions as objects (gen/src/Drifter.cxx:36-52)."""
+    d = dict(dr)
+    d["xregions"] = [dict(anode=a, response=r, cathode=c) for (a, r, c) in dr["xregions"]]
+    return d
+
+
+def from_config(cfg, device=0):
+    """Build a DepoTransform for a synthetic workload description (see synth.py):
+    one face with cfg["planes"], PIRs from cfg["fr"] and the short responses."""
+    dcfg = {k: cfg[k] for k in ("tick", "start_time", "readout_time", "drift_speed", "nsigma", "fluctuate",
+                                 "first_frame_number") if k in cfg}
+    if cfg.get("drifter"):
+        dcfg["drifter"] = drifter_json(cfg["drifter"])
+    dcfg["device"] = device
+    dt = DepoTransform(dcfg)
+    face = dt.add_face(cfg.get("face_bb"))
+    for pl, fr in zip(cfg["planes"], cfg["fr"]):
+        p = dt.add_plane(face, pl)
+        pir = PlaneImpactResponse(fr, cfg.get("short_responses", []), cfg["overall_short_padding"], cfg["tick"],
+                                  cfg["pir_nticks"])
+        dt.set_response_pir(face, p, pir)
+    return dt

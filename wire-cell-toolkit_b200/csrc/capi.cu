@@ -1,0 +1,867 @@
+// Host side of the DepoTransform component and the C ABI (include/wctb200.h).
+//
+// DepoTransformCore mirrors Gen::DepoTransform (gen/src/DepoTransform.cxx):
+// configure() takes the same JSON keys, forward() is operator(), and the
+// per-plane window arithmetic is ImpactTransform's (gen/src/ImpactTransform.cxx:83-115).
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/wctb200.h"
+#include "json.hpp"
+#include "kernels.cuh"
+#include "pir.hpp"
+
+namespace wctb200 {
+
+static thread_local std::string g_last_error;
+
+static int fail(int code, const std::string& msg)
+{
+    g_last_error = msg;
+    return code;
+}
+
+#define CUDA_TRY(expr)                                                                                   \
+    do {                                                                                                 \
+        cudaError_t _e = (expr);                                                                         \
+        if (_e != cudaSuccess)                                                                           \
+            return fail(WCT_ERR_CUDA, std::string(#expr ": ") + cudaGetErrorString(_e));                \
+    } while (0)
+
+// ---------------------------------------------------------------------------
+// Device buffer that only grows.
+// ---------------------------------------------------------------------------
+struct DevBuf {
+    void* p{nullptr};
+    size_t n{0};
+    ~DevBuf() { release(); }
+    void release()
+    {
+        if (p) cudaFree(p);
+        p = nullptr;
+        n = 0;
+    }
+    cudaError_t ensure(size_t bytes)
+    {
+        if (bytes <= n) return cudaSuccess;
+        release();
+        size_t b = std::max<size_t>(bytes, 256);
+        cudaError_t e = cudaMalloc(&p, b);
+        if (e == cudaSuccess) n = b;
+        return e;
+    }
+    template <typename T>
+    T* as() const { return reinterpret_cast<T*>(p); }
+};
+
+// ---------------------------------------------------------------------------
+// FFT plans: radices and twiddle tables per complex length M.
+// ---------------------------------------------------------------------------
+struct FftPlanDev {
+    FftDesc desc{};
+    DevBuf tw, twh;
+};
+
+// Radix schedule for M; false if M has a prime factor above 7.
+static bool fft_radices(int M, std::vector<int>& r)
+{
+    r.clear();
+    int m = M;
+    while (m % 8 == 0) { r.push_back(8); m /= 8; }
+    if (m % 4 == 0) { r.push_back(4); m /= 4; }
+    if (m % 2 == 0) { r.push_back(2); m /= 2; }
+    for (int f : {7, 5, 3})
+        while (m % f == 0) { r.push_back(f); m /= f; }
+    return m == 1 && (int)r.size() <= kFftMaxStages;
+}
+
+// Smallest even N >= n whose half has only the factors 2, 3, 5, 7.
+static int gpu_fft_length(int n)
+{
+    std::vector<int> r;
+    int N = n + (n & 1);
+    while (true) {
+        if (fft_radices(N / 2, r)) return N;
+        N += 2;
+    }
+}
+
+static int make_plan(int M, FftPlanDev& p)
+{
+    std::vector<int> r;
+    if (!fft_radices(M, r)) return fail(WCT_ERR_SIZE, "FFT length has a prime factor above 7");
+    p.desc.M = M;
+    p.desc.nst = (int)r.size();
+    for (size_t i = 0; i < r.size(); ++i) p.desc.radix[i] = r[i];
+    std::vector<float2> tw(M), twh(M);
+    const double twopi = 6.283185307179586476925286766559;
+    for (int m = 0; m < M; ++m) {
+        const double a = -twopi * (double)m / (double)M;
+        tw[m] = make_float2((float)std::cos(a), (float)std::sin(a));
+        const double b = -twopi * (double)m / (2.0 * (double)M);
+        twh[m] = make_float2((float)std::cos(b), (float)std::sin(b));
+    }
+    CUDA_TRY(p.tw.ensure(sizeof(float2) * M));
+    CUDA_TRY(p.twh.ensure(sizeof(float2) * M));
+    CUDA_TRY(cudaMemcpy(p.tw.p, tw.data(), sizeof(float2) * M, cudaMemcpyHostToDevice));
+    CUDA_TRY(cudaMemcpy(p.twh.p, twh.data(), sizeof(float2) * M, cudaMemcpyHostToDevice));
+    p.desc.tw = p.tw.as<float2>();
+    p.desc.twh = p.twh.as<float2>();
+    return WCT_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Component state.
+// ---------------------------------------------------------------------------
+struct PlaneState {
+    int face{0}, index{0};
+    wct_plane_desc desc{};
+    std::vector<int> channels;
+    PlaneDev dev{};
+    // response table
+    bool have_resp{false};
+    int G{0}, npad{0}, nresp{0}, ldr{0}, waveform_pad{0};
+    double pitch{0}, impact{0};
+    DevBuf d_table;        // [G][2npad+1][ldr] floats
+    int spec_N{0};
+    DevBuf d_spec;         // [G][2npad+1][M] packed spectra for spec_N
+    int row0{0};           // frame row offset
+};
+
+struct FaceState {
+    bool have_bb{false};
+    double lo[3]{}, hi[3]{};
+    std::vector<int> planes;
+};
+
+struct Core {
+    // configuration (gen/src/DepoTransform.cxx:63-72 defaults)
+    double start_time{0.0};
+    double readout_time{5.0e6};
+    double tick{500.0};
+    double drift_speed{1.0e-3};
+    double nsigma{3.0};
+    bool fluctuate{false};
+    int frame_count{0};
+    int device{0};
+    bool have_drifter{false};
+    DriftDev drifter{};
+    std::vector<FaceState> faces;
+    std::vector<std::unique_ptr<PlaneState>> planes;
+    cudaStream_t own_stream{nullptr};
+    std::map<int, std::unique_ptr<FftPlanDev>> plans;
+    // workspace
+    DevBuf d_drifted, d_valid, d_rec, d_win, d_Q, d_V, d_depos, d_frame;
+    WindowDev* h_win{nullptr};
+    size_t last_n{0};
+    // stage profiling
+    static constexpr int kStages = 6;
+    bool profiling{false};
+    double stage_ms[kStages]{};
+    long stage_launches[kStages]{};
+    long total_launches{0};
+    struct Pending {
+        int stage;
+        cudaEvent_t a, b;
+    };
+    std::vector<Pending> pending;
+    std::vector<cudaEvent_t> event_pool;
+    cudaEvent_t take_event()
+    {
+        if (!event_pool.empty()) {
+            cudaEvent_t e = event_pool.back();
+            event_pool.pop_back();
+            return e;
+        }
+        cudaEvent_t e = nullptr;
+        cudaEventCreate(&e);
+        return e;
+    }
+    // Open a timed stage on stream s; close() records its end.
+    struct StageTimer {
+        Core* c;
+        int stage;
+        cudaStream_t s;
+        cudaEvent_t a{nullptr};
+        StageTimer(Core* c_, int st, cudaStream_t s_) : c(c_), stage(st), s(s_)
+        {
+            if (c->profiling) {
+                a = c->take_event();
+                cudaEventRecord(a, s);
+            }
+        }
+        void close(int launches)
+        {
+            c->total_launches += launches;
+            c->stage_launches[stage] += launches;
+            if (a) {
+                cudaEvent_t b = c->take_event();
+                cudaEventRecord(b, s);
+                c->pending.push_back({stage, a, b});
+                a = nullptr;
+            }
+        }
+    };
+    void harvest()
+    {
+        for (auto& p : pending) {
+            cudaEventSynchronize(p.b);
+            float ms = 0.f;
+            if (cudaEventElapsedTime(&ms, p.a, p.b) == cudaSuccess) stage_ms[p.stage] += ms;
+            event_pool.push_back(p.a);
+            event_pool.push_back(p.b);
+        }
+        pending.clear();
+    }
+    size_t h_win_n{0};
+    std::mutex mtx;
+
+    int nticks() const { return (int)(readout_time / tick); }
+    int nrows() const
+    {
+        int n = 0;
+        for (auto& p : planes) n += p->desc.nwires;
+        return n;
+    }
+    ~Core()
+    {
+        harvest();
+        for (auto e : event_pool) cudaEventDestroy(e);
+        if (h_win) cudaFreeHost(h_win);
+        if (own_stream) cudaStreamDestroy(own_stream);
+    }
+
+    int plan_for(int M, FftDesc& d)
+    {
+        auto it = plans.find(M);
+        if (it == plans.end()) {
+            auto p = std::make_unique<FftPlanDev>();
+            int rc = make_plan(M, *p);
+            if (rc) return rc;
+            it = plans.emplace(M, std::move(p)).first;
+        }
+        d = it->second->desc;
+        return WCT_OK;
+    }
+};
+
+static int configure(Core& c, const std::string& js)
+{
+    json::Value cfg;
+    try {
+        cfg = json::parse(js.empty() ? std::string("{}") : js);
+    }
+    catch (std::exception& e) {
+        return fail(WCT_ERR_CONFIG, e.what());
+    }
+    c.nsigma = cfg["nsigma"].as_number(c.nsigma);
+    c.fluctuate = cfg["fluctuate"].as_bool(false);
+    c.readout_time = cfg["readout_time"].as_number(c.readout_time);
+    c.tick = cfg["tick"].as_number(c.tick);
+    c.start_time = cfg["start_time"].as_number(c.start_time);
+    c.drift_speed = cfg["drift_speed"].as_number(c.drift_speed);
+    c.frame_count = (int)cfg["first_frame_number"].as_number(c.frame_count);
+    c.device = (int)cfg["device"].as_number(0);
+    if (cfg.has("pirs")) {
+        const auto& p = cfg["pirs"];
+        if (p.kind != json::Value::Array || p.arr.empty())
+            return fail(WCT_ERR_CONFIG, "must configure with some plane impact response components");
+    }
+    if (c.fluctuate) return fail(WCT_ERR_CONFIG, "fluctuate=true is not supported by this build of the forward path");
+    if (c.tick <= 0 || c.readout_time <= 0) return fail(WCT_ERR_CONFIG, "tick and readout_time must be positive");
+    if (c.drift_speed <= 0) return fail(WCT_ERR_CONFIG, "illegal drift speed");
+    const auto& dr = cfg["drifter"];
+    if (dr.kind == json::Value::Object) {
+        c.have_drifter = true;
+        DriftDev& d = c.drifter;
+        d.DL = dr["DL"].as_number(7.2e-7);                  // Drifter.cxx:66-71 defaults
+        d.DT = dr["DT"].as_number(12.0e-7);
+        d.lifetime = dr["lifetime"].as_number(8.0e6);
+        d.speed = dr["drift_speed"].as_number(1.6e-3);
+        d.toffset = dr["time_offset"].as_number(0.0);
+        if (dr["fluctuate"].as_bool(false))
+            return fail(WCT_ERR_CONFIG, "drifter fluctuate=true is not supported by this build of the forward path");
+        const auto& xr = dr["xregions"];
+        if (xr.kind != json::Value::Array || xr.arr.empty()) return fail(WCT_ERR_CONFIG, "no xregions given");
+        if (xr.arr.size() > 8) return fail(WCT_ERR_CONFIG, "at most 8 xregions");
+        d.nxr = (int)xr.arr.size();
+        for (int i = 0; i < d.nxr; ++i) {
+            const auto& r = xr.arr[i];
+            // Drifter::Xregion (gen/src/Drifter.cxx:36-52): cathode may be given
+            // directly or as response + drift length is not supported here.
+            d.xr[i][0] = r["anode"].as_number(0.0);
+            d.xr[i][1] = r["response"].as_number(0.0);
+            d.xr[i][2] = r["cathode"].as_number(0.0);
+        }
+        if (d.speed <= 0) return fail(WCT_ERR_CONFIG, "illegal drift speed");
+    }
+    return WCT_OK;
+}
+
+// Per-plane window of ImpactTransform (gen/src/ImpactTransform.cxx:83-115).
+struct PlaneWindow {
+    int start_ch, end_ch, start_tick, end_tick;  // before padding
+    int m_start_ch, m_end_ch, m_start_tick, m_end_tick;
+    int nw_ref, nt_ref, nt_gpu;
+};
+
+static PlaneWindow window_of(const Core& c, const PlaneState& ps, const WindowDev& w)
+{
+    PlaneWindow o{};
+    double pmin = 0, pmax = 0, tmin = 0, tmax = 0;  // gausdesc_range of an empty set
+    if (w.nadded > 0) {
+        pmin = dkey_inv(w.pmin);
+        pmax = dkey_inv(w.pmax);
+        tmin = dkey_inv(w.tmin);
+        tmax = dkey_inv(w.tmax);
+    }
+    const PlaneDev& pl = ps.dev;
+    auto ibin = [&](double v) { return int((v - pl.imp_min) / pl.imp_bs); };
+    const double tbs = (c.start_time + c.readout_time - c.start_time) / (int)(c.readout_time / c.tick);
+    auto tbin = [&](double v) { return int((v - c.start_time) / tbs); };
+    const int nt = c.nticks();
+    const int i0 = std::max(ibin(pmin), 0), i1 = std::min(ibin(pmax) + 1, pl.imp_nbins);
+    const int t0 = std::max(tbin(tmin), 0), t1 = std::min(tbin(tmax) + 1, nt);
+    const int G = ps.G;
+    int start_ch = std::floor(i0 * 1.0 / (G - 1)) - 1;
+    int end_ch = std::ceil(i1 * 1.0 / (G - 1)) + 2;
+    if ((end_ch - start_ch) % 2 == 1) end_ch += 1;
+    int start_tick = t0 - 1;
+    int end_tick = t1 + 2;
+    if ((end_tick - start_tick) % 2 == 1) end_tick += 1;
+    const size_t ntw = fft_best_length(end_ch - start_ch + 2 * ps.npad, true);
+    const int npad_wire = (ntw - end_ch + start_ch) / 2;
+    o.start_ch = start_ch;
+    o.end_ch = end_ch;
+    o.start_tick = start_tick;
+    o.end_tick = end_tick;
+    o.m_start_ch = start_ch - npad_wire;
+    o.m_end_ch = end_ch + npad_wire;
+    const size_t ntt = fft_best_length(end_tick - start_tick + ps.waveform_pad, false);
+    const int npad_time = ntt - end_tick + start_tick;
+    o.m_start_tick = start_tick;
+    o.m_end_tick = end_tick + npad_time;
+    o.nw_ref = end_ch - start_ch + 2 * npad_wire;
+    o.nt_ref = o.m_end_tick - o.m_start_tick;
+    o.nt_gpu = gpu_fft_length(o.nt_ref);
+    return o;
+}
+
+static int ensure_spectra(Core& c, PlaneState& ps, int N)
+{
+    if (ps.spec_N == N) return WCT_OK;
+    FftDesc d;
+    int rc = c.plan_for(N / 2, d);
+    if (rc) return rc;
+    const int rows = ps.G * (2 * ps.npad + 1);
+    CUDA_TRY(ps.d_spec.ensure(sizeof(float2) * (size_t)rows * (N / 2)));
+    launch_rfft_rows(ps.d_table.as<float>(), ps.ldr, std::min(ps.nresp, N), ps.d_spec.as<float2>(), N / 2, rows, d,
+                     c.own_stream);
+    CUDA_TRY(cudaGetLastError());
+    CUDA_TRY(cudaStreamSynchronize(c.own_stream));
+    ps.spec_N = N;
+    return WCT_OK;
+}
+
+__global__ void k_win_init(WindowDev* w, int n)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    w[i].pmin = ~0ull;
+    w[i].tmin = ~0ull;
+    w[i].pmax = 0ull;
+    w[i].tmax = 0ull;
+    w[i].nadded = w[i].out_time = w[i].out_pitch = w[i].oversize = 0;
+}
+
+static int forward_device(Core& c, const double* d_depos, size_t ndepos, float* d_frame, wct_plane_window* wins,
+                          int* frame_ident, cudaStream_t s)
+{
+    if (c.planes.empty()) return fail(WCT_ERR_STATE, "no planes configured");
+    for (auto& p : c.planes)
+        if (!p->have_resp) return fail(WCT_ERR_STATE, "a plane has no response");
+    if (ndepos > (size_t)0x7fffffff) return fail(WCT_ERR_SIZE, "too many depos");
+    CUDA_TRY(cudaSetDevice(c.device));
+    const int n = (int)ndepos;
+    const int np = (int)c.planes.size();
+    const int nticks = c.nticks();
+    TimeDev tb;
+    tb.nbins = nticks;
+    tb.tmin = c.start_time;
+    tb.tmax = c.start_time + c.readout_time;
+    tb.bs = (tb.tmax - tb.tmin) / tb.nbins;
+
+    CUDA_TRY(c.d_drifted.ensure(sizeof(double) * 7 * std::max(n, 1)));
+    CUDA_TRY(c.d_valid.ensure(std::max(n, 1)));
+    CUDA_TRY(c.d_rec.ensure(sizeof(PatchRec) * (size_t)np * std::max(n, 1)));
+    CUDA_TRY(c.d_win.ensure(sizeof(WindowDev) * np));
+    if (c.h_win_n < (size_t)np) {
+        if (c.h_win) cudaFreeHost(c.h_win);
+        CUDA_TRY(cudaMallocHost(&c.h_win, sizeof(WindowDev) * np));
+        c.h_win_n = np;
+    }
+    const double* dep = d_depos;
+    Core::StageTimer t_prep(&c, 0, s);
+    launch_drift(d_depos, n, c.drifter, c.have_drifter ? 1 : 0, c.d_drifted.as<double>(),
+                 c.d_valid.as<unsigned char>(), s);
+    dep = c.d_drifted.as<double>();
+    k_win_init<<<1, 64, 0, s>>>(c.d_win.as<WindowDev>(), np);
+    for (int ip = 0; ip < np; ++ip) {
+        PlaneState& ps = *c.planes[ip];
+        launch_prep(dep, c.d_valid.as<unsigned char>(), n, ps.dev, tb, c.drift_speed, c.nsigma,
+                    c.d_rec.as<PatchRec>() + (size_t)ip * n, c.d_win.as<WindowDev>() + ip, s);
+    }
+    t_prep.close(1 + (n > 0 ? 1 + np : 0));
+    CUDA_TRY(cudaGetLastError());
+    CUDA_TRY(cudaMemcpyAsync(c.h_win, c.d_win.p, sizeof(WindowDev) * np, cudaMemcpyDeviceToHost, s));
+    CUDA_TRY(cudaStreamSynchronize(s));
+    for (int ip = 0; ip < np; ++ip)
+        if (c.h_win[ip].oversize)
+            return fail(WCT_ERR_SIZE, "a diffusion patch exceeds the rasteriser limit (512 ticks x 256 impacts)");
+
+    std::vector<PlaneWindow> pw(np);
+    size_t qbytes = 0, vbytes = 0;
+    for (int ip = 0; ip < np; ++ip) {
+        PlaneState& ps = *c.planes[ip];
+        pw[ip] = window_of(c, ps, c.h_win[ip]);
+        const int nin = pw[ip].end_ch - pw[ip].start_ch;
+        const int nout = nin + 2 * ps.npad;
+        const int N = pw[ip].nt_gpu;
+        if ((double)ps.G * nin * N >= 2147483647.0) return fail(WCT_ERR_SIZE, "charge grid too large");
+        qbytes = std::max(qbytes, sizeof(float) * (size_t)ps.G * nin * N);
+        vbytes = std::max(vbytes, sizeof(float2) * (size_t)nout * (N / 2));
+        int rc = ensure_spectra(c, ps, N);
+        if (rc) return rc;
+    }
+    CUDA_TRY(c.d_Q.ensure(qbytes));
+    CUDA_TRY(c.d_V.ensure(vbytes));
+    CUDA_TRY(cudaMemsetAsync(d_frame, 0, sizeof(float) * (size_t)c.nrows() * nticks, s));
+    for (int ip = 0; ip < np; ++ip) {
+        PlaneState& ps = *c.planes[ip];
+        const PlaneWindow& w = pw[ip];
+        if (wins) {
+            wct_plane_window& o = wins[ip];
+            o.face = ps.face;
+            o.plane = ps.index;
+            o.start_ch = w.m_start_ch;
+            o.end_ch = w.m_end_ch;
+            o.start_tick = w.m_start_tick;
+            o.end_tick = w.m_end_tick;
+            o.nw_fft = w.nw_ref;
+            o.nt_fft = w.nt_ref;
+            o.nt_gpu = w.nt_gpu;
+            o.charge_rows = w.end_ch - w.start_ch;
+            o.npad = ps.npad;
+            o.ndepos_added = c.h_win[ip].nadded;
+            o.outside_time = c.h_win[ip].out_time;
+            o.outside_pitch = c.h_win[ip].out_pitch;
+        }
+        if (c.h_win[ip].nadded == 0) continue;  // no charge: the plane's frame rows stay zero
+        const int nin = w.end_ch - w.start_ch;
+        const int nout = nin + 2 * ps.npad;
+        const int N = w.nt_gpu, M = N / 2;
+        FftDesc d;
+        int rc = c.plan_for(M, d);
+        if (rc) return rc;
+        float* Q = c.d_Q.as<float>();
+        Core::StageTimer t_r(&c, 1, s);
+        CUDA_TRY(cudaMemsetAsync(Q, 0, sizeof(float) * (size_t)ps.G * nin * N, s));
+        launch_raster(c.d_rec.as<PatchRec>() + (size_t)ip * n, n, ps.dev, tb, ps.G, w.start_ch, nin, w.start_tick, N,
+                      Q, nullptr, s);
+        t_r.close(1);
+        Core::StageTimer t_f(&c, 2, s);
+        launch_rfft_rows(Q, N, N, reinterpret_cast<float2*>(Q), M, ps.G * nin, d, s);
+        t_f.close(1);
+        Core::StageTimer t_c(&c, 3, s);
+        launch_wire_conv(reinterpret_cast<const float2*>(Q), ps.d_spec.as<float2>(), c.d_V.as<float2>(), ps.G, ps.npad,
+                         nin, nout, M, s);
+        t_c.close(2);
+        const int wlo = std::max(0, w.m_start_ch), whi = std::min(ps.desc.nwires, w.m_end_ch);
+        Core::StageTimer t_i(&c, 4, s);
+        launch_irfft_rows(c.d_V.as<float2>(), nout, d, w.start_ch - ps.npad, wlo, whi, w.start_tick,
+                          std::min(N, w.nt_ref), nticks, d_frame + (size_t)ps.row0 * nticks, s);
+        t_i.close(1);
+        CUDA_TRY(cudaGetLastError());
+    }
+    if (frame_ident) *frame_ident = c.frame_count;
+    ++c.frame_count;
+    c.last_n = ndepos;
+    return WCT_OK;
+}
+
+}  // namespace wctb200
+
+using namespace wctb200;
+
+struct wct_depotransform {
+    Core core;
+};
+struct wct_pir {
+    Pir pir;
+};
+
+extern "C" {
+
+const char* wct_version(void) { return "wctb200 0.1 (sm_100a)"; }
+const char* wct_last_error(void) { return g_last_error.c_str(); }
+
+int wct_pir_create(const wct_fr_plane* fr, int nshort, const int* short_len, const double* short_wave,
+                   double overall_short_padding, double tick, int nticks, wct_pir** out)
+{
+    if (!fr || !out || !fr->pitchpos || !fr->current || nticks <= 0 || tick <= 0)
+        return fail(WCT_ERR_ARG, "wct_pir_create: bad arguments");
+    try {
+        std::vector<std::vector<double>> shorts;
+        size_t off = 0;
+        for (int i = 0; i < nshort; ++i) {
+            shorts.emplace_back(short_wave + off, short_wave + off + short_len[i]);
+            off += short_len[i];
+        }
+        auto* p = new wct_pir;
+        p->pir = build_pir(fr->npaths, fr->nsamples, fr->pitchpos, fr->current, fr->pitch, fr->tstart, fr->period,
+                           shorts, overall_short_padding, tick, nticks);
+        *out = p;
+        return WCT_OK;
+    }
+    catch (std::exception& e) {
+        return fail(WCT_ERR_CONFIG, e.what());
+    }
+}
+
+int wct_pir_closest(const wct_pir* p, double relpitch, int* path)
+{
+    if (!p || !path) return fail(WCT_ERR_ARG, "wct_pir_closest: bad arguments");
+    int k = p->pir.closest(relpitch);
+    if (k < 0) return fail(WCT_ERR_RESPONSE, "relative pitch outside PIR extent");
+    *path = k;
+    return WCT_OK;
+}
+
+int wct_pir_info(const wct_pir* p, double* pitch, double* impact, double* half_extent, int* nwires,
+                 int* nimp_per_wire, int* npaths, int* nticks, int* waveform_pad)
+{
+    if (!p) return fail(WCT_ERR_ARG, "wct_pir_info: null pir");
+    if (pitch) *pitch = p->pir.pitch;
+    if (impact) *impact = p->pir.impact;
+    if (half_extent) *half_extent = p->pir.half_extent;
+    if (nwires) *nwires = p->pir.nwires();
+    if (nimp_per_wire) *nimp_per_wire = p->pir.nimp_per_wire();
+    if (npaths) *npaths = (int)p->pir.waveform.size();
+    if (nticks) *nticks = p->pir.nticks;
+    if (waveform_pad) *waveform_pad = p->pir.waveform_pad;
+    return WCT_OK;
+}
+
+int wct_pir_waveform(const wct_pir* p, int path, float* out)
+{
+    if (!p || !out || path < 0 || path >= (int)p->pir.waveform.size())
+        return fail(WCT_ERR_ARG, "wct_pir_waveform: bad arguments");
+    std::copy(p->pir.waveform[path].begin(), p->pir.waveform[path].end(), out);
+    return WCT_OK;
+}
+
+int wct_pir_destroy(wct_pir* p)
+{
+    delete p;
+    return WCT_OK;
+}
+
+int wct_dt_create(const char* json_config, wct_depotransform** out)
+{
+    if (!out) return fail(WCT_ERR_ARG, "wct_dt_create: null out");
+    auto* h = new wct_depotransform;
+    int rc = configure(h->core, json_config ? std::string(json_config) : std::string());
+    if (rc) {
+        delete h;
+        return rc;
+    }
+    cudaError_t e = cudaSetDevice(h->core.device);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&h->core.own_stream, cudaStreamNonBlocking);
+    if (e != cudaSuccess) {
+        delete h;
+        return fail(WCT_ERR_CUDA, std::string("wct_dt_create: ") + cudaGetErrorString(e));
+    }
+    *out = h;
+    return WCT_OK;
+}
+
+int wct_dt_default_configuration(char* buf, size_t len)
+{
+    const char* js =
+        "{\"nsigma\": 3.0, \"fluctuate\": false, \"start_time\": 0.0, \"readout_time\": 5000000.0, "
+        "\"tick\": 500.0, \"drift_speed\": 0.001, \"first_frame_number\": 0, \"anode\": \"\", \"rng\": \"\", "
+        "\"pirs\": [], \"dft\": \"FftwDFT\"}";
+    if (!buf || len <= strlen(js)) return fail(WCT_ERR_ARG, "buffer too small");
+    strcpy(buf, js);
+    return WCT_OK;
+}
+
+int wct_dt_add_face(wct_depotransform* h, const double* lo, const double* hi, int* face)
+{
+    if (!h) return fail(WCT_ERR_ARG, "null component");
+    FaceState f;
+    if (lo && hi) {
+        f.have_bb = true;
+        for (int i = 0; i < 3; ++i) {
+            f.lo[i] = lo[i];
+            f.hi[i] = hi[i];
+        }
+    }
+    h->core.faces.push_back(f);
+    if (face) *face = (int)h->core.faces.size() - 1;
+    return WCT_OK;
+}
+
+int wct_dt_add_plane(wct_depotransform* h, int face, const wct_plane_desc* d, int* plane)
+{
+    if (!h || !d || face < 0 || face >= (int)h->core.faces.size())
+        return fail(WCT_ERR_ARG, "wct_dt_add_plane: bad arguments");
+    if (d->nwires < 2 || d->nimpacts < 2 || (d->nimpacts % 2))
+        return fail(WCT_ERR_CONFIG, "need >= 2 wires and an even number of impacts per wire");
+    Core& c = h->core;
+    auto ps = std::make_unique<PlaneState>();
+    ps->face = face;
+    ps->index = (int)c.faces[face].planes.size();
+    ps->desc = *d;
+    if (d->channels) ps->channels.assign(d->channels, d->channels + d->nwires);
+    else {
+        ps->channels.resize(d->nwires);
+        for (int i = 0; i < d->nwires; ++i) ps->channels[i] = i;
+    }
+    ps->desc.channels = nullptr;
+    // Pimpos (util/src/Pimpos.cxx:5-33) with D3Vector::norm (D3Vector.h:147-154)
+    const double* p = d->pitch;
+    const double m = std::sqrt(p[0] * p[0] + p[1] * p[1] + p[2] * p[2]);
+    if (!(m > 0)) return fail(WCT_ERR_CONFIG, "zero pitch direction");
+    PlaneDev& pd = ps->dev;
+    pd.ax = p[0] / m;
+    pd.ay = p[1] / m;
+    pd.az = p[2] / m;
+    pd.ox = d->origin[0];
+    pd.oy = d->origin[1];
+    pd.oz = d->origin[2];
+    pd.nwires = d->nwires;
+    pd.nimp = d->nimpacts;
+    const double regionsize = (d->pitchmax - d->pitchmin) / (d->nwires - 1);
+    pd.imp_min = d->pitchmin - 0.5 * regionsize;
+    pd.imp_max = d->pitchmax + 0.5 * regionsize;
+    pd.imp_nbins = d->nwires * d->nimpacts;
+    pd.imp_bs = (pd.imp_max - pd.imp_min) / pd.imp_nbins;
+    const FaceState& f = c.faces[face];
+    pd.have_bb = f.have_bb ? 1 : 0;
+    for (int i = 0; i < 3; ++i) {
+        pd.bb_lo[i] = f.lo[i];
+        pd.bb_hi[i] = f.hi[i];
+    }
+    ps->row0 = c.nrows();
+    c.faces[face].planes.push_back((int)c.planes.size());
+    c.planes.push_back(std::move(ps));
+    if (plane) *plane = c.faces[face].planes.size() - 1;
+    return WCT_OK;
+}
+
+static PlaneState* find_plane(wct_depotransform* h, int face, int plane)
+{
+    if (!h || face < 0 || face >= (int)h->core.faces.size()) return nullptr;
+    auto& f = h->core.faces[face];
+    if (plane < 0 || plane >= (int)f.planes.size()) return nullptr;
+    return h->core.planes[f.planes[plane]].get();
+}
+
+int wct_dt_set_response_table(wct_depotransform* h, int face, int plane, int ngroups, int npad, int nsamples,
+                              double pitch, double impact, int waveform_pad, const float* table)
+{
+    PlaneState* ps = find_plane(h, face, plane);
+    if (!ps || !table || ngroups < 3 || npad < 0 || nsamples <= 0)
+        return fail(WCT_ERR_ARG, "wct_dt_set_response_table: bad arguments");
+    if (ngroups - 1 != ps->desc.nimpacts)
+        return fail(WCT_ERR_CONFIG, "response impact groups do not match the plane's impact binning");
+    CUDA_TRY(cudaSetDevice(h->core.device));
+    ps->G = ngroups;
+    ps->npad = npad;
+    ps->nresp = nsamples;
+    ps->ldr = nsamples + (nsamples & 1);
+    ps->pitch = pitch;
+    ps->impact = impact;
+    ps->waveform_pad = waveform_pad;
+    const size_t rows = (size_t)ngroups * (2 * npad + 1);
+    std::vector<float> t(rows * ps->ldr, 0.0f);
+    for (size_t r = 0; r < rows; ++r) std::copy(table + r * nsamples, table + (r + 1) * nsamples, t.data() + r * ps->ldr);
+    CUDA_TRY(ps->d_table.ensure(sizeof(float) * t.size()));
+    CUDA_TRY(cudaMemcpy(ps->d_table.p, t.data(), sizeof(float) * t.size(), cudaMemcpyHostToDevice));
+    ps->spec_N = 0;
+    ps->have_resp = true;
+    return WCT_OK;
+}
+
+int wct_dt_set_response_pir(wct_depotransform* h, int face, int plane, const wct_pir* p)
+{
+    PlaneState* ps = find_plane(h, face, plane);
+    if (!ps || !p) return fail(WCT_ERR_ARG, "wct_dt_set_response_pir: bad arguments");
+    const Pir& pir = p->pir;
+    // ImpactTransform.cxx:28-74
+    const int G = std::round(pir.pitch / pir.impact) + 1;
+    const int npad = std::round((pir.nwires() - 1) / 2.);
+    const int ns = std::max(1, std::min(pir.nticks, pir.n_short));
+    std::vector<float> table((size_t)G * (2 * npad + 1) * ns, 0.0f);
+    for (int i = 0; i < G; ++i) {
+        double rel;
+        if (i != G - 1) rel = -pir.pitch / 2. + pir.impact * i + 1e-9;
+        else rel = -pir.pitch / 2. + pir.impact * i - 1e-9;
+        for (int j = 0; j < pir.nwires(); ++j) {
+            const int k = pir.closest(rel - (j - npad) * pir.pitch);
+            if (k < 0) return fail(WCT_ERR_RESPONSE, "ImpactTransform response lookup outside the PIR extent");
+            std::copy(pir.waveform[k].begin(), pir.waveform[k].begin() + ns,
+                      table.begin() + ((size_t)i * (2 * npad + 1) + j) * ns);
+        }
+    }
+    return wct_dt_set_response_table(h, face, plane, G, npad, ns, pir.pitch, pir.impact, pir.waveform_pad,
+                                      table.data());
+}
+
+int wct_dt_frame_shape(const wct_depotransform* h, int* nrows, int* nticks)
+{
+    if (!h) return fail(WCT_ERR_ARG, "null component");
+    if (nrows) *nrows = h->core.nrows();
+    if (nticks) *nticks = h->core.nticks();
+    return WCT_OK;
+}
+
+int wct_dt_forward_device(wct_depotransform* h, const double* d_depos, size_t ndepos, float* d_frame,
+                          wct_plane_window* windows, int* frame_ident, void* stream)
+{
+    if (!h || !d_frame || (ndepos && !d_depos)) return fail(WCT_ERR_ARG, "wct_dt_forward_device: bad arguments");
+    std::lock_guard<std::mutex> lk(h->core.mtx);
+    cudaStream_t s = stream ? (cudaStream_t)stream : h->core.own_stream;
+    return forward_device(h->core, d_depos, ndepos, d_frame, windows, frame_ident, s);
+}
+
+int wct_dt_forward(wct_depotransform* h, const double* depos, size_t ndepos, float* frame, wct_plane_window* windows,
+                   int* frame_ident)
+{
+    if (!h || !frame || (ndepos && !depos)) return fail(WCT_ERR_ARG, "wct_dt_forward: bad arguments");
+    std::lock_guard<std::mutex> lk(h->core.mtx);
+    Core& c = h->core;
+    CUDA_TRY(cudaSetDevice(c.device));
+    cudaStream_t s = c.own_stream;
+    const size_t fbytes = sizeof(float) * (size_t)c.nrows() * c.nticks();
+    CUDA_TRY(c.d_depos.ensure(sizeof(double) * 7 * std::max<size_t>(ndepos, 1)));
+    CUDA_TRY(c.d_frame.ensure(fbytes));
+    if (ndepos)
+        CUDA_TRY(cudaMemcpyAsync(c.d_depos.p, depos, sizeof(double) * 7 * ndepos, cudaMemcpyHostToDevice, s));
+    int rc = forward_device(c, c.d_depos.as<double>(), ndepos, c.d_frame.as<float>(), windows, frame_ident, s);
+    if (rc) return rc;
+    CUDA_TRY(cudaMemcpyAsync(frame, c.d_frame.p, fbytes, cudaMemcpyDeviceToHost, s));
+    CUDA_TRY(cudaStreamSynchronize(s));
+    return WCT_OK;
+}
+
+int wct_dt_eos(wct_depotransform* h)
+{
+    if (!h) return fail(WCT_ERR_ARG, "null component");
+    return WCT_EOS;
+}
+
+int wct_dt_traces(const wct_depotransform* h, const float* frame, int* channel, int* tbin, int* length, long* offset,
+                  int* ntraces)
+{
+    if (!h || !frame || !channel || !tbin || !length || !offset || !ntraces)
+        return fail(WCT_ERR_ARG, "wct_dt_traces: bad arguments");
+    const Core& c = h->core;
+    const int nt = c.nticks();
+    int k = 0;
+    for (auto& ps : c.planes) {
+        for (int w = 0; w < ps->desc.nwires; ++w) {
+            const float* row = frame + (size_t)(ps->row0 + w) * nt;
+            int imin = nt, imax = nt;  // Waveform::edge
+            for (int i = 0; i < nt; ++i) {
+                if (row[i] != 0.0f) {
+                    if (imin == nt) imin = i;
+                    imax = i + 1;
+                }
+            }
+            if (imin == nt) continue;
+            channel[k] = ps->channels[w];
+            tbin[k] = imin;
+            length[k] = imax - imin;
+            offset[k] = (long)(ps->row0 + w) * nt + imin;
+            ++k;
+        }
+    }
+    *ntraces = k;
+    return WCT_OK;
+}
+
+int wct_dt_patch_records(const wct_depotransform* h, int face, int plane, int* out, size_t n)
+{
+    PlaneState* ps = find_plane(const_cast<wct_depotransform*>(h), face, plane);
+    if (!ps || !out) return fail(WCT_ERR_ARG, "wct_dt_patch_records: bad arguments");
+    const Core& c = h->core;
+    if (n != c.last_n) return fail(WCT_ERR_STATE, "depo count differs from the last forward call");
+    if (n == 0) return WCT_OK;
+    int ip = 0;
+    for (; ip < (int)c.planes.size(); ++ip)
+        if (c.planes[ip].get() == ps) break;
+    std::vector<PatchRec> rec(n);
+    CUDA_TRY(cudaSetDevice(c.device));
+    CUDA_TRY(cudaMemcpy(rec.data(), c.d_rec.as<PatchRec>() + (size_t)ip * n, sizeof(PatchRec) * n,
+                        cudaMemcpyDeviceToHost));
+    for (size_t i = 0; i < n; ++i) {
+        out[4 * i + 0] = rec[i].toff;
+        out[4 * i + 1] = rec[i].poff;
+        out[4 * i + 2] = rec[i].nt;
+        out[4 * i + 3] = rec[i].np;
+    }
+    return WCT_OK;
+}
+
+int wct_dt_set_profiling(wct_depotransform* h, int on)
+{
+    if (!h) return fail(WCT_ERR_ARG, "null component");
+    std::lock_guard<std::mutex> lk(h->core.mtx);
+    h->core.profiling = on != 0;
+    return WCT_OK;
+}
+
+int wct_dt_stage_times(wct_depotransform* h, double* ms, long* launches, int nstages, long* total_launches, int reset)
+{
+    if (!h) return fail(WCT_ERR_ARG, "null component");
+    std::lock_guard<std::mutex> lk(h->core.mtx);
+    Core& c = h->core;
+    CUDA_TRY(cudaSetDevice(c.device));
+    c.harvest();
+    for (int i = 0; i < nstages && i < Core::kStages; ++i) {
+        if (ms) ms[i] = c.stage_ms[i];
+        if (launches) launches[i] = c.stage_launches[i];
+    }
+    if (total_launches) *total_launches = c.total_launches;
+    if (reset) {
+        for (int i = 0; i < Core::kStages; ++i) {
+            c.stage_ms[i] = 0;
+            c.stage_launches[i] = 0;
+        }
+        c.total_launches = 0;
+    }
+    return WCT_OK;
+}
+
+int wct_dt_destroy(wct_depotransform* h)
+{
+    if (h) {
+        cudaSetDevice(h->core.device);
+        delete h;
+    }
+    return WCT_OK;
+}
+
+}  // extern "C"

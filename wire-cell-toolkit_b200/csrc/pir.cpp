@@ -1,0 +1,127 @@
+#include "pir.hpp"
+
+#include <algorithm>
+
+namespace wctb200 {
+
+static const size_t kAny[] = {
+    33,   35,   40,   42,   44,   56,   64,   66,   70,   77,   80,   96,   98,   100,  112,  121,  128,
+    140,  143,  160,  168,  169,  200,  224,  256,  280,  320,  400,  448,  512,  560,  640,  686,  768,
+    800,  847,  896,  1024, 1120, 1280, 1331, 1372, 1400, 1536, 1600, 1792, 2048, 2560, 2662, 2744, 3200,
+    3584, 4096, 4116, 4480, 4802, 5120, 5324, 5376, 5544, 5600, 5632, 5929, 6174, 6272, 6292, 6655, 7168,
+    7840, 8192, 8232, 8960, 9317, 10240, 10648, 11979, 14336, 15972, 16384};
+static const size_t kEven[] = {
+    40,   42,   44,   56,   64,   66,   70,   72,   80,   96,   98,   100,  112,  120,  128,  140,  160,
+    168,  200,  224,  256,  280,  320,  400,  448,  512,  560,  640,  686,  768,  800,  896,  1024, 1120,
+    1280, 1372, 1400, 1536, 1600, 1792, 2048, 2560, 2662, 2744, 3200, 3584, 4096, 4116, 4480, 4802, 5120,
+    5324, 5376, 5544, 5600, 5632, 6174, 6272, 6292, 6468, 7168, 7840, 8192, 8232, 8960, 10240, 10648, 11200,
+    11858, 11880, 14336, 15972, 16384};
+static const size_t kOdd[] = {
+    33,   35,   39,   49,   55,   63,   65,   77,   81,   91,   99,   121,  143,  169,  175,  187,  225,
+    231,  245,  275,  297,  343,  363,  375,  385,  405,  441,  455,  495,  539,  605,  637,  693,  735,
+    847,  875,  891,  945,  1001, 1089, 1331, 1573, 1859, 1875, 2197, 2299, 2431, 2541, 2625, 2695, 3025,
+    3267, 3993, 4095, 4125, 4719, 4725, 5005, 5145, 5445, 5929, 6655, 7007, 7623, 7865, 9317, 9801, 11979,
+    14157, 14175, 15379, 16335};
+
+template <size_t N>
+static size_t pick(const size_t (&t)[N], size_t n)
+{
+    if (n <= t[N - 1])
+        for (size_t i = 0; i < N; ++i)
+            if (t[i] >= n) return t[i];
+    return n;
+}
+
+size_t fft_best_length(size_t n, bool keep_odd_even)
+{
+    if (!keep_odd_even) return pick(kAny, n);
+    return (n % 2 == 0) ? pick(kEven, n) : pick(kOdd, n);
+}
+
+std::pair<int, int> Pir::closest_wire_impact(double relpitch) const
+{
+    const int center_wire = nwires() / 2;
+    const int relwire = int(std::round(relpitch / pitch));
+    const int wire_index = center_wire + relwire;
+    const double remainder = relpitch - relwire * pitch;
+    const int impact_index = int(std::round(remainder / impact)) + nimp_per_wire() / 2;
+    return {wire_index, impact_index};
+}
+
+int Pir::closest(double relpitch) const
+{
+    if (relpitch < -half_extent || relpitch > half_extent) return -1;
+    auto wi = closest_wire_impact(relpitch);
+    if (wi.first < 0 || wi.first >= (int)bywire.size()) return -1;
+    const auto& region = bywire[wi.first];
+    if (wi.second < 0 || wi.second >= (int)region.size()) return -1;
+    const int irind = region[wi.second];
+    if (irind < 0 || irind >= (int)waveform.size()) return -1;
+    return irind;
+}
+
+Pir build_pir(int npaths, int nsamples, const double* pitchpos, const double* current, double fr_pitch,
+              double tstart, double period, const std::vector<std::vector<double>>& shorts,
+              double overall_short_padding, double tick, int nticks)
+{
+    const int n_per = 6;  // six paths per wire region (PlaneImpactResponse.cxx:164)
+    if (npaths < n_per || npaths % n_per) throw std::runtime_error("field response must hold 6 paths per wire");
+    Pir p;
+    p.nticks = nticks;
+    p.waveform_pad = (int)(overall_short_padding / tick);
+    const size_t n_short = fft_best_length((size_t)(overall_short_padding / tick), false);
+    p.n_short = (int)n_short;
+    // circular product of the short responses, each cut or zero padded to n_short
+    std::vector<double> kern(n_short, 0.0);
+    kern[0] = 1.0;
+    for (const auto& sw : shorts) {
+        std::vector<double> s(n_short, 0.0);
+        for (size_t i = 0; i < std::min(n_short, sw.size()); ++i) s[i] = sw[i];
+        std::vector<double> out(n_short, 0.0);
+        for (size_t a = 0; a < n_short; ++a) {
+            if (kern[a] == 0.0) continue;
+            for (size_t b = 0; b < n_short; ++b) out[(a + b) % n_short] += kern[a] * s[b];
+        }
+        kern.swap(out);
+    }
+    const int n_wires = npaths / n_per;
+    const int n_wires_half = n_wires / 2;
+    p.impact = std::abs(pitchpos[1] - pitchpos[0]);
+    p.half_extent = std::max(std::abs(pitchpos[0]), std::abs(pitchpos[npaths - 1]));
+    p.pitch = 2.0 * std::abs(pitchpos[n_per - 1] - pitchpos[0]);
+    const double rawmax = tstart + nsamples * period;
+    const double rawbs = (rawmax - tstart) / nsamples;
+    const double oopsilon = 1e-15 * fr_pitch;
+    std::map<int, std::vector<int>> wire_to_ind;
+    p.waveform.assign(npaths, std::vector<float>(nticks, 0.0f));
+    for (int ip = 0; ip < npaths; ++ip) {
+        const int wirenum = int(std::ceil((pitchpos[ip] - oopsilon) / fr_pitch));
+        wire_to_ind[wirenum].push_back(ip);
+        std::vector<double> wave(n_short, 0.0);
+        for (int r = 0; r < nsamples; ++r) {
+            const double time = tstart + (r + 0.5) * rawbs;  // Binning::center
+            const size_t bin = time / tick;
+            if (bin >= n_short) throw std::runtime_error("out of bounds field response");
+            wave[bin] += current[(size_t)ip * nsamples + r] * period;
+        }
+        std::vector<double> wf(n_short, 0.0);
+        if (shorts.empty()) wf = wave;
+        else
+            for (size_t a = 0; a < n_short; ++a) {
+                if (wave[a] == 0.0) continue;
+                for (size_t b = 0; b < n_short; ++b) wf[(a + b) % n_short] += wave[a] * kern[b];
+            }
+        for (int k = 0; k < nticks && k < (int)n_short; ++k) p.waveform[ip][k] = (float)wf[k];
+    }
+    for (int irel = -n_wires_half; irel <= n_wires_half; ++irel) {
+        const auto& direct = wire_to_ind[irel];
+        const auto& other = wire_to_ind[-irel];
+        std::vector<int> idx(direct.begin(), direct.end());
+        if (!other.empty())
+            for (auto it = other.rbegin() + 1; it != other.rend(); ++it) idx.push_back(*it);
+        p.bywire.push_back(idx);
+    }
+    return p;
+}
+
+}  // namespace wctb200
