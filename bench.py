@@ -53,25 +53,42 @@ class ClockSampler:
     def __init__(self, index):
         self.index = index
         self.p = None
+        self.lines = []
 
     def start(self):
         try:
             self.p = subprocess.Popen(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.Q,
                                        "--format=csv,noheader,nounits", "-lms", "200"],
                                       stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.lines = []
+            import threading
+            self.th = threading.Thread(target=self._reader, daemon=True)
+            self.th.start()
         except Exception:
             self.p = None
+
+    def _reader(self):
+        for line in self.p.stdout:
+            self.lines.append(line)
+
+    def wait_first_sample(self, timeout=3.0):
+        t0 = time.perf_counter()
+        while self.p is not None and not self.lines and time.perf_counter() - t0 < timeout:
+            time.sleep(0.01)
+
+    def nsamples(self):
+        return len(self.lines)
 
     def stop(self):
         if self.p is None:
             return None
         self.p.terminate()
         try:
-            out, _ = self.p.communicate(timeout=5)
+            self.p.wait(timeout=5)
         except Exception:
             self.p.kill()
-            out, _ = self.p.communicate()
-        rows = [r for r in csv.reader(io.StringIO(out)) if len(r) >= 9]
+        self.th.join(timeout=5)
+        rows = [[c.strip() for c in r] for r in csv.reader(io.StringIO("".join(self.lines))) if len(r) >= 9]
         if not rows:
             return None
         sm = [float(r[1]) for r in rows if r[1].strip().replace(".", "").isdigit()]
@@ -132,7 +149,9 @@ def run_b200(args):
     depos = synth.apa_depos(seed=2 + rank)
     n = len(depos)
     dt = wct.from_config(cfg, device=local)
-    stream = torch.cuda.current_stream()
+    # a dedicated (non-default) stream: the library and the timing events share it
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
     d_depos = torch.from_numpy(depos).to("cuda")
     nrows, nticks = dt.frame_shape()
     d_frame = torch.empty((nrows, nticks), dtype=torch.float32, device="cuda")
@@ -152,6 +171,7 @@ def run_b200(args):
         torch.distributed.barrier()
     torch.cuda.synchronize()
     clocks.start()
+    clocks.wait_first_sample()
     evs = []
     for k in range(args.steps):
         flush.fill_(float(k))  # L2 flush between timed steps, outside the timed events
@@ -164,8 +184,15 @@ def run_b200(args):
     torch.cuda.synchronize()
     if world > 1:
         torch.distributed.barrier()
-    clk = clocks.stop()
     dt.set_profiling(False)
+    # The timed region is far shorter than the 200 ms sampling period: keep
+    # running identical steps until the sampler has seen the GPU under load.
+    t_load = time.perf_counter()
+    while clocks.nsamples() < 4 and time.perf_counter() - t_load < 5.0:
+        for _ in range(20):
+            step()
+        torch.cuda.synchronize()
+    clk = clocks.stop()
     total_ms = sum(a.elapsed_time(b) for a, b in evs)
     stages, launches = dt.stage_times(reset=True)
     t = torch.tensor([total_ms], dtype=torch.float64, device="cuda")

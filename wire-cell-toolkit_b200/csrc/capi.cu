@@ -85,14 +85,15 @@ static bool fft_radices(int M, std::vector<int>& r)
     return m == 1 && (int)r.size() <= kFftMaxStages;
 }
 
-// Smallest even N >= n whose half has only the factors 2, 3, 5, 7.
+// Smallest N >= n, N a multiple of 4, whose half has only the factors 2, 3, 5, 7
+// (the reference's own length whenever it qualifies).
 static int gpu_fft_length(int n)
 {
     std::vector<int> r;
-    int N = n + (n & 1);
+    int N = (n + 3) & ~3;
     while (true) {
         if (fft_radices(N / 2, r)) return N;
-        N += 2;
+        N += 4;
     }
 }
 
@@ -161,7 +162,7 @@ struct Core {
     cudaStream_t own_stream{nullptr};
     std::map<int, std::unique_ptr<FftPlanDev>> plans;
     // workspace
-    DevBuf d_drifted, d_valid, d_rec, d_win, d_Q, d_V, d_depos, d_frame;
+    DevBuf d_rec, d_win, d_Q, d_V, d_depos, d_frame, d_wcnt, d_woff, d_wcur, d_wlist, d_tprof, d_kbound;
     WindowDev* h_win{nullptr};
     size_t last_n{0};
     // stage profiling
@@ -388,6 +389,7 @@ static int forward_device(Core& c, const double* d_depos, size_t ndepos, float* 
                           int* frame_ident, cudaStream_t s)
 {
     if (c.planes.empty()) return fail(WCT_ERR_STATE, "no planes configured");
+    if ((int)c.planes.size() > kMaxPlanes) return fail(WCT_ERR_CONFIG, "too many planes for one component");
     for (auto& p : c.planes)
         if (!p->have_resp) return fail(WCT_ERR_STATE, "a plane has no response");
     if (ndepos > (size_t)0x7fffffff) return fail(WCT_ERR_SIZE, "too many depos");
@@ -401,54 +403,106 @@ static int forward_device(Core& c, const double* d_depos, size_t ndepos, float* 
     tb.tmax = c.start_time + c.readout_time;
     tb.bs = (tb.tmax - tb.tmin) / tb.nbins;
 
-    CUDA_TRY(c.d_drifted.ensure(sizeof(double) * 7 * std::max(n, 1)));
-    CUDA_TRY(c.d_valid.ensure(std::max(n, 1)));
+    PlaneSet pset{};
+    pset.nplanes = np;
+    int nwt = 0;
+    for (int ip = 0; ip < np; ++ip) {
+        pset.p[ip] = c.planes[ip]->dev;
+        pset.p[ip].wire_base = nwt;
+        nwt += c.planes[ip]->desc.nwires;
+    }
+    pset.nwires_total = nwt;
+    pset.ntiles = (nticks + kTile - 1) / kTile;
+    const int nkeys = nwt * pset.ntiles;
+
     CUDA_TRY(c.d_rec.ensure(sizeof(PatchRec) * (size_t)np * std::max(n, 1)));
+    CUDA_TRY(c.d_tprof.ensure(sizeof(float) * kTprof * (size_t)std::max(n, 1)));
     CUDA_TRY(c.d_win.ensure(sizeof(WindowDev) * np));
+    CUDA_TRY(c.d_wcnt.ensure(sizeof(int) * (nkeys + 1)));
+    CUDA_TRY(c.d_woff.ensure(sizeof(int) * (nkeys + 1)));
+    CUDA_TRY(c.d_wcur.ensure(sizeof(int) * (nkeys + 1)));
     if (c.h_win_n < (size_t)np) {
         if (c.h_win) cudaFreeHost(c.h_win);
-        CUDA_TRY(cudaMallocHost(&c.h_win, sizeof(WindowDev) * np));
+        CUDA_TRY(cudaMallocHost(&c.h_win, sizeof(WindowDev) * np + sizeof(int)));
         c.h_win_n = np;
     }
-    const double* dep = d_depos;
+    int* h_total = reinterpret_cast<int*>(c.h_win + np);
+
     Core::StageTimer t_prep(&c, 0, s);
-    launch_drift(d_depos, n, c.drifter, c.have_drifter ? 1 : 0, c.d_drifted.as<double>(),
-                 c.d_valid.as<unsigned char>(), s);
-    dep = c.d_drifted.as<double>();
+    CUDA_TRY(cudaMemsetAsync(c.d_wcnt.p, 0, sizeof(int) * (nkeys + 1), s));
+    CUDA_TRY(c.d_kbound.ensure(sizeof(float) * (size_t)nkeys * kTileBlocks));
+    CUDA_TRY(cudaMemsetAsync(c.d_kbound.p, 0, sizeof(float) * (size_t)nkeys * kTileBlocks, s));
     k_win_init<<<1, 64, 0, s>>>(c.d_win.as<WindowDev>(), np);
-    for (int ip = 0; ip < np; ++ip) {
-        PlaneState& ps = *c.planes[ip];
-        launch_prep(dep, c.d_valid.as<unsigned char>(), n, ps.dev, tb, c.drift_speed, c.nsigma,
-                    c.d_rec.as<PatchRec>() + (size_t)ip * n, c.d_win.as<WindowDev>() + ip, s);
-    }
-    t_prep.close(1 + (n > 0 ? 1 + np : 0));
+    launch_prep_all(d_depos, n, c.drifter, c.have_drifter ? 1 : 0, pset, tb, c.drift_speed, c.nsigma,
+                    c.d_rec.as<PatchRec>(), c.d_win.as<WindowDev>(), c.d_wcnt.as<int>(), c.d_tprof.as<float>(),
+                    c.d_kbound.as<float>(), s);
+    launch_scan(c.d_wcnt.as<int>(), nkeys, c.d_woff.as<int>(), c.d_wcur.as<int>(), s);
+    t_prep.close(2 + (n > 0 ? 1 : 0));
     CUDA_TRY(cudaGetLastError());
     CUDA_TRY(cudaMemcpyAsync(c.h_win, c.d_win.p, sizeof(WindowDev) * np, cudaMemcpyDeviceToHost, s));
+    CUDA_TRY(cudaMemcpyAsync(h_total, c.d_woff.as<int>() + nkeys, sizeof(int), cudaMemcpyDeviceToHost, s));
     CUDA_TRY(cudaStreamSynchronize(s));
     for (int ip = 0; ip < np; ++ip)
-        if (c.h_win[ip].oversize)
-            return fail(WCT_ERR_SIZE, "a diffusion patch exceeds the rasteriser limit (512 ticks x 256 impacts)");
+        if (c.h_win[ip].oversize) return fail(WCT_ERR_SIZE, "a diffusion patch exceeds 1024 ticks or 1024 impact bins");
+    const int total_visits = *h_total;
 
     std::vector<PlaneWindow> pw(np);
-    size_t qbytes = 0, vbytes = 0;
+    GridSet gset{};
+    gset.nplanes = np;
+    gset.ntiles_abs = pset.ntiles;
+    size_t qfloats = 0, vbytes = 0, smem = 0;
+    int rows = 0;
     for (int ip = 0; ip < np; ++ip) {
         PlaneState& ps = *c.planes[ip];
         pw[ip] = window_of(c, ps, c.h_win[ip]);
-        const int nin = pw[ip].end_ch - pw[ip].start_ch;
-        const int nout = nin + 2 * ps.npad;
-        const int N = pw[ip].nt_gpu;
-        if ((double)ps.G * nin * N >= 2147483647.0) return fail(WCT_ERR_SIZE, "charge grid too large");
-        qbytes = std::max(qbytes, sizeof(float) * (size_t)ps.G * nin * N);
-        vbytes = std::max(vbytes, sizeof(float2) * (size_t)nout * (N / 2));
-        int rc = ensure_spectra(c, ps, N);
-        if (rc) return rc;
+        const PlaneWindow& w = pw[ip];
+        GridPlane& g = gset.p[ip];
+        g.nimp = ps.dev.nimp;
+        g.G = ps.G;
+        g.nwires = ps.desc.nwires;
+        g.wire_base = pset.p[ip].wire_base;
+        g.start_ch = w.start_ch;
+        g.nin = c.h_win[ip].nadded > 0 ? w.end_ch - w.start_ch : 0;
+        g.col0 = w.start_tick;
+        g.ncols = w.end_tick - w.start_tick;
+        g.N = w.nt_gpu;
+        g.tbs = (float)tb.bs;
+        g.pbs = (float)ps.dev.imp_bs;
+        g.qoff = (long long)qfloats;
+        g.recoff = (long long)ip * n;
+        g.row_base = rows;
+        // absolute tick tiles covering grid columns [0, N) (ticks col0 .. col0+N-1), floor division
+        auto fdiv = [](int a, int b) { return a >= 0 ? a / b : -((-a + b - 1) / b); };
+        g.ktile0 = fdiv(g.col0, kTile);
+        g.ntile = fdiv(g.col0 + g.N - 1, kTile) - g.ktile0 + 1;
+        rows += g.nin * g.ntile;
+        qfloats += (size_t)ps.G * g.nin * g.N;
+        vbytes = std::max(vbytes, sizeof(float2) * (size_t)(g.nin + 2 * ps.npad) * (g.N / 2));
+        if (g.nin) {
+            smem = std::max(smem, raster_smem_bytes(g.G));
+            int rc = ensure_spectra(c, ps, g.N);
+            if (rc) return rc;
+        }
     }
-    CUDA_TRY(c.d_Q.ensure(qbytes));
-    CUDA_TRY(c.d_V.ensure(vbytes));
+    gset.nrows_total = rows;
+    if (smem > 227 * 1024) return fail(WCT_ERR_SIZE, "event time window too long for the shared-memory charge grid");
+    if (qfloats >= (size_t)1 << 40) return fail(WCT_ERR_SIZE, "charge grid too large");
+    CUDA_TRY(c.d_Q.ensure(sizeof(float) * std::max<size_t>(qfloats, 1)));
+    CUDA_TRY(c.d_V.ensure(std::max<size_t>(vbytes, 1)));
+    CUDA_TRY(c.d_wlist.ensure(sizeof(Visit) * std::max(total_visits, 1)));
     CUDA_TRY(cudaMemsetAsync(d_frame, 0, sizeof(float) * (size_t)c.nrows() * nticks, s));
+
+    Core::StageTimer t_r(&c, 1, s);
+    launch_fill(c.d_rec.as<PatchRec>(), n, pset, c.d_wcur.as<int>(), c.d_wlist.as<Visit>(), s);
+    launch_raster_wires(c.d_rec.as<PatchRec>(), c.d_tprof.as<float>(), c.d_wcnt.as<int>(), c.d_woff.as<int>(),
+                        c.d_wlist.as<Visit>(), c.d_kbound.as<float>(), gset, c.d_Q.as<float>(), s);
+    t_r.close((n > 0 ? 1 : 0) + (rows > 0 ? 1 : 0));
+    CUDA_TRY(cudaGetLastError());
+
     for (int ip = 0; ip < np; ++ip) {
         PlaneState& ps = *c.planes[ip];
         const PlaneWindow& w = pw[ip];
+        const GridPlane& g = gset.p[ip];
         if (wins) {
             wct_plane_window& o = wins[ip];
             o.face = ps.face;
@@ -466,26 +520,21 @@ static int forward_device(Core& c, const double* d_depos, size_t ndepos, float* 
             o.outside_time = c.h_win[ip].out_time;
             o.outside_pitch = c.h_win[ip].out_pitch;
         }
-        if (c.h_win[ip].nadded == 0) continue;  // no charge: the plane's frame rows stay zero
-        const int nin = w.end_ch - w.start_ch;
+        if (g.nin == 0) continue;  // no charge: the plane's frame rows stay zero
+        const int nin = g.nin;
         const int nout = nin + 2 * ps.npad;
-        const int N = w.nt_gpu, M = N / 2;
+        const int N = g.N, M = N / 2;
         FftDesc d;
         int rc = c.plan_for(M, d);
         if (rc) return rc;
-        float* Q = c.d_Q.as<float>();
-        Core::StageTimer t_r(&c, 1, s);
-        CUDA_TRY(cudaMemsetAsync(Q, 0, sizeof(float) * (size_t)ps.G * nin * N, s));
-        launch_raster(c.d_rec.as<PatchRec>() + (size_t)ip * n, n, ps.dev, tb, ps.G, w.start_ch, nin, w.start_tick, N,
-                      Q, nullptr, s);
-        t_r.close(1);
+        float* Q = c.d_Q.as<float>() + g.qoff;
         Core::StageTimer t_f(&c, 2, s);
         launch_rfft_rows(Q, N, N, reinterpret_cast<float2*>(Q), M, ps.G * nin, d, s);
         t_f.close(1);
         Core::StageTimer t_c(&c, 3, s);
         launch_wire_conv(reinterpret_cast<const float2*>(Q), ps.d_spec.as<float2>(), c.d_V.as<float2>(), ps.G, ps.npad,
                          nin, nout, M, s);
-        t_c.close(2);
+        t_c.close(1);
         const int wlo = std::max(0, w.m_start_ch), whi = std::min(ps.desc.nwires, w.m_end_ch);
         Core::StageTimer t_i(&c, 4, s);
         launch_irfft_rows(c.d_V.as<float2>(), nout, d, w.start_ch - ps.npad, wlo, whi, w.start_tick,
@@ -686,6 +735,7 @@ int wct_dt_set_response_table(wct_depotransform* h, int face, int plane, int ngr
         return fail(WCT_ERR_ARG, "wct_dt_set_response_table: bad arguments");
     if (ngroups - 1 != ps->desc.nimpacts)
         return fail(WCT_ERR_CONFIG, "response impact groups do not match the plane's impact binning");
+    if (ngroups > 12) return fail(WCT_ERR_CONFIG, "at most 12 impact groups (11 impact positions per wire) supported");
     CUDA_TRY(cudaSetDevice(h->core.device));
     ps->G = ngroups;
     ps->npad = npad;

@@ -1,12 +1,13 @@
 // DepoTransform forward kernels for sm_100a.
 //
-// Pipeline for one plane of one event (all on one stream):
-//   k_drift        Drifter::insert per depo               gen/src/Drifter.cxx:127-196
-//   k_prep         BinnedDiffusion_transform::add + the    gen/src/BinnedDiffusion_transform.cxx:37-92
-//                  patch window (sample_bin_range) and     gen/src/GaussianDiffusion.cxx:116-149
-//                  the event window reduction              gen/src/BinnedDiffusion_transform.cxx:416-464
-//   k_raster       erf-integrated patches, linear impact   gen/src/GaussianDiffusion.cxx:30-229
-//                  weights, scatter into impact groups     gen/src/BinnedDiffusion_transform.cxx:227-391
+// Pipeline for one event (all on one stream):
+//   k_prep_all     drift + sensitive cut + BinnedDiffusion_transform::add +
+//                  patch sample ranges + event window reduction + per-wire
+//                  visit counts, all planes, one thread per depo
+//   k_scan/k_fill  per-wire visit lists (CSR)
+//   k_raster_wires erf-integrated patches with linear impact weights,
+//                  accumulated per wire row in shared memory, written as the
+//                  impact-group x tick charge grids       gen/src/BinnedDiffusion_transform.cxx:227-391
 //   k_rfft_rows    real FFT along time of each group row   gen/src/ImpactTransform.cxx:149-151,237
 //   k_wire_conv    wire-direction convolution with the     gen/src/ImpactTransform.cxx:153-212,242-300
 //                  per-group response spectra (direct taps)
@@ -23,6 +24,7 @@
 
 #include "kernels.cuh"
 
+#include <algorithm>
 #include <cfloat>
 
 namespace wctb200 {
@@ -52,207 +54,43 @@ __device__ __forceinline__ T warp_reduce(T v, Op op)
 }
 
 // ---------------------------------------------------------------------------
-// Drift: Drifter::insert without fluctuation (gen/src/Drifter.cxx:127-196).
-// ---------------------------------------------------------------------------
-__global__ void k_drift(const double* __restrict__ in, int n, DriftDev dd, int do_drift, double* __restrict__ out,
-                        unsigned char* __restrict__ valid)
-{
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    const double* p = in + 7 * (size_t)i;
-    double t = p[0], q = p[1], x = p[2], y = p[3], z = p[4], el = p[5], et = p[6];
-    unsigned char ok = 1;
-    if (do_drift) {
-        if (q == 0.0) ok = 0;
-        else {
-            int found = -1;
-            double dir = 0.0;
-            for (int r = 0; r < dd.nxr; ++r) {
-                const double a = dd.xr[r][0], rp = dd.xr[r][1];
-                if ((a < x && x < rp) || (rp < x && x < a)) { found = r; dir = -1.0; break; }
-            }
-            if (found < 0)
-                for (int r = 0; r < dd.nxr; ++r) {
-                    const double rp = dd.xr[r][1], c = dd.xr[r][2];
-                    if ((rp < x && x < c) || (c < x && x < rp)) { found = r; dir = 1.0; break; }
-                }
-            if (found < 0) ok = 0;
-            else {
-                const double respx = dd.xr[found][1];
-                const double dt = fabs(__ddiv_rn(__dsub_rn(respx, x), dd.speed));
-                if (dir > 0) {
-                    const double absorb = __dsub_rn(1.0, exp(__ddiv_rn(-dt, dd.lifetime)));
-                    const double dQ = __dmul_rn(q, absorb);
-                    q = __dsub_rn(q, dQ);
-                    el = __dsqrt_rn(__dadd_rn(__dmul_rn(__dmul_rn(2.0, dd.DL), dt), __dmul_rn(el, el)));
-                    et = __dsqrt_rn(__dadd_rn(__dmul_rn(__dmul_rn(2.0, dd.DT), dt), __dmul_rn(et, et)));
-                }
-                t = __dadd_rn(__dadd_rn(t, __dmul_rn(dir, dt)), dd.toffset);
-                x = respx;
-            }
-        }
-    }
-    double* o = out + 7 * (size_t)i;
-    o[0] = t; o[1] = q; o[2] = x; o[3] = y; o[4] = z; o[5] = el; o[6] = et;
-    valid[i] = ok;
-}
-
-void launch_drift(const double* depos, int n, const DriftDev& dd, int do_drift, double* out, unsigned char* valid,
-                  cudaStream_t s)
-{
-    if (n <= 0) return;
-    k_drift<<<(n + 255) / 256, 256, 0, s>>>(depos, n, dd, do_drift, out, valid);
-}
-
-// ---------------------------------------------------------------------------
-// Prep: sensitive-volume cut (aux/src/DepoTools.cxx:110-123,
-// util/src/BoundingBox.cxx:37-56), BinnedDiffusion_transform::add rejection,
-// GaussianDiffusion sample ranges, and the per-plane window reduction.
-// ---------------------------------------------------------------------------
-__global__ void k_prep(const double* __restrict__ dep, const unsigned char* __restrict__ valid, int n, PlaneDev pl,
-                       TimeDev tb, double drift_speed, double nsigma, PatchRec* __restrict__ rec,
-                       WindowDev* __restrict__ win)
-{
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    unsigned long long kpmin = ~0ull, kpmax = 0ull, ktmin = ~0ull, ktmax = 0ull;
-    int nadd = 0, nout_t = 0, nout_p = 0, nover = 0;
-    if (i < n) {
-        PatchRec r;
-        r.toff = r.poff = 0;
-        r.nt = r.np = 0;
-        r.tcr = r.pcr = r.st = r.sp = r.q = 0.f;
-        if (valid[i]) {
-            const double* p = dep + 7 * (size_t)i;
-            const double t = p[0], q = p[1], x = p[2], y = p[3], z = p[4], el = p[5], et = p[6];
-            bool inbb = true;
-            if (pl.have_bb) {
-                const double pp[3] = {x, y, z};
-#pragma unroll
-                for (int k = 0; k < 3; ++k) {
-                    const double b1 = pl.bb_lo[k], b2 = pl.bb_hi[k];
-                    if (b1 < b2) { if (pp[k] < b1 || pp[k] > b2) inbb = false; }
-                    else if (b2 < b1) { if (pp[k] < b2 || pp[k] > b1) inbb = false; }
-                }
-            }
-            if (inbb) {
-                const double ct = t;
-                const double st = __ddiv_rn(el, drift_speed);                         // DepoTransform.cxx:185
-                const double rx = __dsub_rn(x, pl.ox), ry = __dsub_rn(y, pl.oy), rz = __dsub_rn(z, pl.oz);
-                const double cp = __dadd_rn(__dadd_rn(__dmul_rn(pl.ax, rx), __dmul_rn(pl.ay, ry)),
-                                            __dmul_rn(pl.az, rz));                  // Pimpos.cxx:58
-                const double sp = et;
-                const double eff_t = st > 0 ? nsigma : 0.0;
-                const double eff_p = sp > 0 ? nsigma : 0.0;
-                if (gdistance(tb.tmin, ct, st) > eff_t || gdistance(tb.tmax, ct, st) < -eff_t) {
-                    nout_t = 1;
-                }
-                else if (gdistance(pl.imp_min, cp, sp) > eff_p || gdistance(pl.imp_max, cp, sp) < -eff_p) {
-                    nout_p = 1;
-                }
-                else {
-                    nadd = 1;
-                    const double tlo = __dsub_rn(ct, __dmul_rn(st, nsigma));
-                    const double thi = __dadd_rn(ct, __dmul_rn(st, nsigma));
-                    const double plo = __dsub_rn(cp, __dmul_rn(sp, nsigma));
-                    const double phi = __dadd_rn(cp, __dmul_rn(sp, nsigma));
-                    ktmin = dkey(tlo); ktmax = dkey(thi);
-                    kpmin = dkey(plo); kpmax = dkey(phi);
-                    const int t0 = max(bin_of(tlo, tb.tmin, tb.bs), 0);
-                    const int t1 = min(bin_of(thi, tb.tmin, tb.bs) + 1, tb.nbins);
-                    const int p0 = max(bin_of(plo, pl.imp_min, pl.imp_bs), 0);
-                    const int p1 = min(bin_of(phi, pl.imp_min, pl.imp_bs) + 1, pl.imp_nbins);
-                    if (t1 > t0 && p1 > p0) {
-                        const int nt = t1 - t0, np = p1 - p0;
-                        if (nt > kMaxPatchT || np > kMaxPatchP || (st == 0.0 && nt != 1) ||
-                            (sp == 0.0 && np != 1)) {
-                            nover = 1;
-                        }
-                        else {
-                            r.toff = t0;
-                            r.poff = p0;
-                            r.nt = (unsigned short)nt;
-                            r.np = (unsigned short)np;
-                            r.tcr = (float)__dsub_rn(ct, edge_of(t0, tb.tmin, tb.bs));
-                            r.pcr = (float)__dsub_rn(cp, edge_of(p0, pl.imp_min, pl.imp_bs));
-                            r.st = (float)st;
-                            r.sp = (float)sp;
-                            r.q = (float)q;
-                        }
-                    }
-                }
-            }
-        }
-        rec[i] = r;
-    }
-    // block reduction, one atomic per block per quantity
-    auto umin = [](unsigned long long a, unsigned long long b) { return a < b ? a : b; };
-    auto umax = [](unsigned long long a, unsigned long long b) { return a > b ? a : b; };
-    auto iadd = [](int a, int b) { return a + b; };
-    kpmin = warp_reduce(kpmin, umin);
-    ktmin = warp_reduce(ktmin, umin);
-    kpmax = warp_reduce(kpmax, umax);
-    ktmax = warp_reduce(ktmax, umax);
-    nadd = warp_reduce(nadd, iadd);
-    nout_t = warp_reduce(nout_t, iadd);
-    nout_p = warp_reduce(nout_p, iadd);
-    nover = warp_reduce(nover, iadd);
-    __shared__ unsigned long long s_k[4][32];
-    __shared__ int s_c[4][32];
-    const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
-    if (l == 0) {
-        s_k[0][w] = kpmin; s_k[1][w] = kpmax; s_k[2][w] = ktmin; s_k[3][w] = ktmax;
-        s_c[0][w] = nadd; s_c[1][w] = nout_t; s_c[2][w] = nout_p; s_c[3][w] = nover;
-    }
-    __syncthreads();
-    if (w == 0) {
-        const int nw = blockDim.x >> 5;
-        kpmin = l < nw ? s_k[0][l] : ~0ull;
-        kpmax = l < nw ? s_k[1][l] : 0ull;
-        ktmin = l < nw ? s_k[2][l] : ~0ull;
-        ktmax = l < nw ? s_k[3][l] : 0ull;
-        nadd = l < nw ? s_c[0][l] : 0;
-        nout_t = l < nw ? s_c[1][l] : 0;
-        nout_p = l < nw ? s_c[2][l] : 0;
-        nover = l < nw ? s_c[3][l] : 0;
-        kpmin = warp_reduce(kpmin, umin);
-        ktmin = warp_reduce(ktmin, umin);
-        kpmax = warp_reduce(kpmax, umax);
-        ktmax = warp_reduce(ktmax, umax);
-        nadd = warp_reduce(nadd, iadd);
-        nout_t = warp_reduce(nout_t, iadd);
-        nout_p = warp_reduce(nout_p, iadd);
-        nover = warp_reduce(nover, iadd);
-        if (l == 0 && nadd) {
-            atomicMin(&win->pmin, kpmin);
-            atomicMax(&win->pmax, kpmax);
-            atomicMin(&win->tmin, ktmin);
-            atomicMax(&win->tmax, ktmax);
-            atomicAdd(&win->nadded, nadd);
-        }
-        if (l == 0 && nout_t) atomicAdd(&win->out_time, nout_t);
-        if (l == 0 && nout_p) atomicAdd(&win->out_pitch, nout_p);
-        if (l == 0 && nover) atomicAdd(&win->oversize, nover);
-    }
-}
-
-void launch_prep(const double* depos, const unsigned char* valid, int n, const PlaneDev& pl, const TimeDev& tb,
-                 double drift_speed, double nsigma, PatchRec* rec, WindowDev* win, cudaStream_t s)
-{
-    if (n <= 0) return;
-    k_prep<<<(n + 255) / 256, 256, 0, s>>>(depos, valid, n, pl, tb, drift_speed, nsigma, rec, win);
-}
-
-// ---------------------------------------------------------------------------
-// Raster: one warp per depo patch.
+// Drift, sensitive volume, rejection, patch window and visit counting for
+// every plane, one thread per depo.
+//
+//   Drifter::insert without fluctuation          gen/src/Drifter.cxx:127-196
+//   sensitive-volume cut                          aux/src/DepoTools.cxx:110-123,
+//                                                 util/src/BoundingBox.cxx:37-56
+//   BinnedDiffusion_transform::add rejection      gen/src/BinnedDiffusion_transform.cxx:37-92
+//   GaussianDiffusion sample ranges               gen/src/GaussianDiffusion.cxx:116-149
+//   window reduction (impact/time_bin_range)      gen/src/BinnedDiffusion_transform.cxx:416-464
 //
 // Bin integrals of the unit Gaussian are differences of erfc on the side of
 // the centre the bin lies on, so tail bins keep full FP32 relative accuracy
 // (0.5*(erf(b) - erf(a)) of GaussianDiffusion.cxx:30-56 loses ~4 digits there).
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ float edge_erfc(int k, float bs, float cr, float inv)
+// erfc(z) for z >= 0 by the Chebyshev fit of W. H. Press et al., Numerical
+// Recipes (2nd ed.), section 6.2, function erfcc: fractional error below
+// 1.2e-7 over the whole range (tests check it against FP64 erfc).
+__device__ __forceinline__ float erfc_nr(float z)
 {
-    const float x = ((float)k * bs - cr) * inv;
-    return copysignf(erfcf(fabsf(x)), x);  // sign of x carried on the (non-negative) erfc value
+    const float t = __frcp_rn(fmaf(0.5f, z, 1.0f));
+    float p = 0.17087277f;
+    p = fmaf(t, p, -0.82215223f);
+    p = fmaf(t, p, 1.48851587f);
+    p = fmaf(t, p, -1.13520398f);
+    p = fmaf(t, p, 0.27886807f);
+    p = fmaf(t, p, -0.18628806f);
+    p = fmaf(t, p, 0.09678418f);
+    p = fmaf(t, p, 0.37409196f);
+    p = fmaf(t, p, 1.00002368f);
+    p = fmaf(t, p, -1.26551223f);
+    return t * __expf(fmaf(-z, z, p));
+}
+
+__device__ __forceinline__ float edge_erfc(float k, float bs, float cr, float inv)
+{
+    const float x = (k * bs - cr) * inv;
+    return copysignf(erfc_nr(fabsf(x)), x);  // sign of x carried on the (non-negative) erfc value
 }
 __device__ __forceinline__ float bin_from_edges(float a, float b)
 {
@@ -263,119 +101,569 @@ __device__ __forceinline__ float bin_from_edges(float a, float b)
     return 0.5f * ((2.0f - ea) - eb);         // bin straddles the centre
 }
 
-constexpr int kRasterWarps = 4;
-
-__global__ void __launch_bounds__(kRasterWarps * 32) k_raster(const PatchRec* __restrict__ rec, int n, PlaneDev pl,
-                                                               TimeDev tb, int G, int row0, int nrows, int col0,
-                                                               int ldq, float* __restrict__ Q)
+// Visit keys of one patch: (wire, tick tile) pairs for the wires
+// [w0, w0 + wspan) and tiles [k0, k0 + kspan); key = wire * ntiles + tile.
+// Warp-aggregated increment of the per-key visit counters.
+__device__ __forceinline__ void count_visits(int* cnt, int wbase, int w0, int wspan, int k0, int kspan, int ntiles)
 {
-    __shared__ float s_e[kRasterWarps][kMaxPatchT + 1];
-    __shared__ float s_t[kRasterWarps][kMaxPatchT];
-    __shared__ float s_p[kRasterWarps][kMaxPatchP];
-    __shared__ float s_w[kRasterWarps][kMaxPatchP];
-    __shared__ int s_off[kRasterWarps][kMaxPatchP];
-    const int wib = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int half_g = (G - 1) / 2;
-    const float tbs = (float)tb.bs, pbs = (float)pl.imp_bs;
-    const size_t gstride = (size_t)nrows * ldq;
-    for (int i = blockIdx.x * kRasterWarps + wib; i < n; i += gridDim.x * kRasterWarps) {
-        const PatchRec r = rec[i];
-        const int nt = r.nt, np = r.np;
-        if (np == 0 || nt == 0) continue;
-        // ---- time profile
-        double sum_t = 0.0;
-        if (r.st > 0.f) {
-            const float inv = 1.0f / (1.41421356237309505f * r.st);
-            for (int k = lane; k <= nt; k += 32) s_e[wib][k] = edge_erfc(k, tbs, r.tcr, inv);
-            __syncwarp();
-            for (int k = lane; k < nt; k += 32) {
-                const float v = bin_from_edges(s_e[wib][k], s_e[wib][k + 1]);
-                s_t[wib][k] = v;
-                sum_t += (double)v;
-            }
+    const int span = wspan * kspan;
+    int maxspan = span;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) maxspan = max(maxspan, __shfl_xor_sync(0xffffffffu, maxspan, o));
+    const int lane = threadIdx.x & 31;
+    for (int k = 0; k < maxspan; ++k) {
+        int key = -1;
+        if (k < span) {
+            const int dw = k / kspan, dk = k - dw * kspan;
+            key = (wbase + w0 + dw) * ntiles + k0 + dk;
         }
-        else {
-            if (lane == 0) { s_t[wib][0] = 1.0f; sum_t = 1.0; }
+        const unsigned act = __ballot_sync(0xffffffffu, key >= 0);
+        if (key >= 0) {
+            const unsigned m = __match_any_sync(act, key);
+            if (lane == __ffs(m) - 1) atomicAdd(cnt + key, __popc(m));
         }
-        __syncwarp();
-        // ---- pitch profile and linear weights (GausDesc::weight, GaussianDiffusion.cxx:61-92)
-        double sum_p = 0.0;
-        if (r.sp > 0.f) {
-            const float inv = 1.0f / (1.41421356237309505f * r.sp);
-            for (int k = lane; k <= np; k += 32) s_e[wib][k] = edge_erfc(k, pbs, r.pcr, inv);
-            __syncwarp();
-            const float isg = 1.0f / r.sp;
-            const float c0 = r.sp / (pbs * 2.50662827463100050f);  // sigma / (step*sqrt(2 pi))
-            for (int k = lane; k < np; k += 32) {
-                const float v = bin_from_edges(s_e[wib][k], s_e[wib][k + 1]);
-                const float x1 = (float)k * pbs - r.pcr;
-                const float x2 = (float)(k + 1) * pbs - r.pcr;
-                const float u1 = x1 * isg, u2 = x2 * isg;
-                const float g1 = expf(-0.5f * u1 * u1), g2 = expf(-0.5f * u2 * u2);
-                float w = v > 0.f ? c0 * (g2 - g1) / v + x2 / pbs : 0.0f;
-                s_p[wib][k] = v;
-                s_w[wib][k] = w;
-                sum_p += (double)v;
-            }
-        }
-        else {
-            if (lane == 0) {
-                s_p[wib][0] = 1.0f;
-                s_w[wib][0] = (pbs - r.pcr) / pbs;
-                sum_p = 1.0;
-            }
-        }
-        // ---- impact bin -> (wire row, group) offsets (Pimpos.cxx:41-47)
-        for (int k = lane; k < np; k += 32) {
-            const int kk = r.poff + k;
-            const int w = kk / pl.nimp;
-            const int red = kk - (w * pl.nimp + pl.nimp / 2);
-            const int g0 = red + half_g;
-            s_off[wib][k] = (int)((size_t)g0 * gstride + (size_t)(w - row0) * ldq);
-        }
-        sum_t = warp_reduce(sum_t, [](double a, double b) { return a + b; });
-        sum_p = warp_reduce(sum_p, [](double a, double b) { return a + b; });
-        __syncwarp();
-        const float scale = (float)((double)r.q / (sum_p * sum_t));
-        const int cbase = r.toff - col0;
-        // ---- scatter the patch into the two bracketing impact groups
-        if (nt <= 32) {
-            const int rpp = 32 / nt;
-            const int li = lane / nt, lt = lane - li * nt;
-            if (li < rpp) {
-                const float tv = s_t[wib][lt] * scale;
-                for (int ip = li; ip < np; ip += rpp) {
-                    const float v = s_p[wib][ip] * tv;
-                    const float w = s_w[wib][ip];
-                    float* q0 = Q + s_off[wib][ip] + cbase + lt;
-                    atomicAdd(q0, v * w);
-                    atomicAdd(q0 + gstride, v * (1.0f - w));
+    }
+}
+
+// Magnitude bound of one visit's contribution to any cell: |q| * max bin
+// fraction in pitch * max bin fraction in time * 2 (two bracketing groups).
+__device__ __forceinline__ float visit_bound(float qn, float sp, float st, float pbs, float tbs)
+{
+    const float k = 0.39894228040143268f;  // 1/sqrt(2 pi)
+    const float pm = sp > 0.f ? fminf(1.0f, k * pbs / sp) : 1.0f;
+    const float tm = st > 0.f ? fminf(1.0f, k * tbs / st) : 1.0f;
+    return 2.0f * fabsf(qn) * pm * tm * 1.0001f;
+}
+
+__global__ void __launch_bounds__(256) k_prep_all(const double* __restrict__ dep, int n, DriftDev dd, int do_drift,
+                                                  PlaneSet ps, TimeDev tb, double drift_speed, double nsigma,
+                                                  PatchRec* __restrict__ rec, WindowDev* __restrict__ win,
+                                                  int* __restrict__ wire_cnt, float* __restrict__ tprof,
+                                                  float* __restrict__ key_bound)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    double t = 0, q = 0, x = 0, y = 0, z = 0, el = 0, et = 0;
+    bool ok = false;
+    if (i < n) {
+        const double* p = dep + 7 * (size_t)i;
+        t = p[0]; q = p[1]; x = p[2]; y = p[3]; z = p[4]; el = p[5]; et = p[6];
+        ok = true;
+        if (do_drift) {
+            if (q == 0.0) ok = false;
+            else {
+                int found = -1;
+                double dir = 0.0;
+                for (int r = 0; r < dd.nxr; ++r) {
+                    const double a = dd.xr[r][0], rp = dd.xr[r][1];
+                    if ((a < x && x < rp) || (rp < x && x < a)) { found = r; dir = -1.0; break; }
+                }
+                if (found < 0)
+                    for (int r = 0; r < dd.nxr; ++r) {
+                        const double rp = dd.xr[r][1], c = dd.xr[r][2];
+                        if ((rp < x && x < c) || (c < x && x < rp)) { found = r; dir = 1.0; break; }
+                    }
+                if (found < 0) ok = false;
+                else {
+                    const double respx = dd.xr[found][1];
+                    const double dt = fabs(__ddiv_rn(__dsub_rn(respx, x), dd.speed));
+                    if (dir > 0) {
+                        const double absorb = __dsub_rn(1.0, exp(__ddiv_rn(-dt, dd.lifetime)));
+                        q = __dsub_rn(q, __dmul_rn(q, absorb));
+                        el = __dsqrt_rn(__dadd_rn(__dmul_rn(__dmul_rn(2.0, dd.DL), dt), __dmul_rn(el, el)));
+                        et = __dsqrt_rn(__dadd_rn(__dmul_rn(__dmul_rn(2.0, dd.DT), dt), __dmul_rn(et, et)));
+                    }
+                    t = __dadd_rn(__dadd_rn(t, __dmul_rn(dir, dt)), dd.toffset);
+                    x = respx;
                 }
             }
         }
-        else {
-            for (int ip = 0; ip < np; ++ip) {
-                const float pv = s_p[wib][ip] * scale;
-                const float w = s_w[wib][ip];
-                float* q0 = Q + s_off[wib][ip] + cbase;
-                for (int it = lane; it < nt; it += 32) {
-                    const float v = pv * s_t[wib][it];
-                    atomicAdd(q0 + it, v * w);
-                    atomicAdd(q0 + it + gstride, v * (1.0f - w));
+    }
+    // The time profile depends on the depo only (GaussianDiffusion.cxx:124-136):
+    // compute it once here for every plane's raster.
+    if (ok) {
+        const double st = __ddiv_rn(el, drift_speed);
+        const double tlo = __dsub_rn(t, __dmul_rn(st, nsigma));
+        const double thi = __dadd_rn(t, __dmul_rn(st, nsigma));
+        const int t0 = max(bin_of(tlo, tb.tmin, tb.bs), 0);
+        const int t1 = min(bin_of(thi, tb.tmin, tb.bs) + 1, tb.nbins);
+        const int nt = t1 - t0;
+        if (nt > 0 && nt <= kTprof) {
+            float* tp = tprof + (size_t)i * kTprof;
+            if (st > 0) {
+                const float fst = (float)st;
+                const float tcr = (float)__dsub_rn(t, edge_of(t0, tb.tmin, tb.bs));
+                const float inv = 1.0f / (1.41421356237309505f * fst);
+                const float tbs = (float)tb.bs;
+                float e1 = edge_erfc(0.f, tbs, tcr, inv);
+                for (int k = 0; k < nt; ++k) {
+                    const float e2 = edge_erfc((float)(k + 1), tbs, tcr, inv);
+                    tp[k] = bin_from_edges(e1, e2);
+                    e1 = e2;
+                }
+            }
+            else {
+                tp[0] = 1.0f;
+            }
+        }
+    }
+    __shared__ unsigned long long s_k[4][8];
+    __shared__ int s_c[4][8];
+    const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+    auto umin = [](unsigned long long a, unsigned long long b) { return a < b ? a : b; };
+    auto umax = [](unsigned long long a, unsigned long long b) { return a > b ? a : b; };
+    auto iadd = [](int a, int b) { return a + b; };
+    for (int ip = 0; ip < ps.nplanes; ++ip) {
+        const PlaneDev& pl = ps.p[ip];
+        unsigned long long kpmin = ~0ull, kpmax = 0ull, ktmin = ~0ull, ktmax = 0ull;
+        int nadd = 0, nout_t = 0, nout_p = 0, nover = 0;
+        PatchRec r;
+        r.toff = r.poff = 0;
+        r.nt = r.np = 0;
+        r.tcr = r.pcr = r.st = r.sp = r.qn = 0.f;
+        bool inbb = ok;
+        if (ok && pl.have_bb) {
+            const double pp[3] = {x, y, z};
+#pragma unroll
+            for (int k = 0; k < 3; ++k) {
+                const double b1 = pl.bb_lo[k], b2 = pl.bb_hi[k];
+                if (b1 < b2) { if (pp[k] < b1 || pp[k] > b2) inbb = false; }
+                else if (b2 < b1) { if (pp[k] < b2 || pp[k] > b1) inbb = false; }
+            }
+        }
+        if (inbb) {
+            const double ct = t;
+            const double st = __ddiv_rn(el, drift_speed);                         // DepoTransform.cxx:185
+            const double rx = __dsub_rn(x, pl.ox), ry = __dsub_rn(y, pl.oy), rz = __dsub_rn(z, pl.oz);
+            const double cp = __dadd_rn(__dadd_rn(__dmul_rn(pl.ax, rx), __dmul_rn(pl.ay, ry)),
+                                        __dmul_rn(pl.az, rz));                  // Pimpos.cxx:58
+            const double sp = et;
+            const double eff_t = st > 0 ? nsigma : 0.0;
+            const double eff_p = sp > 0 ? nsigma : 0.0;
+            if (gdistance(tb.tmin, ct, st) > eff_t || gdistance(tb.tmax, ct, st) < -eff_t) {
+                nout_t = 1;
+            }
+            else if (gdistance(pl.imp_min, cp, sp) > eff_p || gdistance(pl.imp_max, cp, sp) < -eff_p) {
+                nout_p = 1;
+            }
+            else {
+                nadd = 1;
+                const double tlo = __dsub_rn(ct, __dmul_rn(st, nsigma));
+                const double thi = __dadd_rn(ct, __dmul_rn(st, nsigma));
+                const double plo = __dsub_rn(cp, __dmul_rn(sp, nsigma));
+                const double phi = __dadd_rn(cp, __dmul_rn(sp, nsigma));
+                ktmin = dkey(tlo); ktmax = dkey(thi);
+                kpmin = dkey(plo); kpmax = dkey(phi);
+                const int t0 = max(bin_of(tlo, tb.tmin, tb.bs), 0);
+                const int t1 = min(bin_of(thi, tb.tmin, tb.bs) + 1, tb.nbins);
+                const int p0 = max(bin_of(plo, pl.imp_min, pl.imp_bs), 0);
+                const int p1 = min(bin_of(phi, pl.imp_min, pl.imp_bs) + 1, pl.imp_nbins);
+                if (t1 > t0 && p1 > p0) {
+                    const int nt = t1 - t0, np = p1 - p0;
+                    if (nt > kMaxPatchT || np > kMaxPatchP || (st == 0.0 && nt != 1) || (sp == 0.0 && np != 1)) {
+                        nover = 1;
+                    }
+                    else {
+                        r.toff = t0;
+                        r.poff = p0;
+                        r.nt = (unsigned short)nt;
+                        r.np = (unsigned short)np;
+                        r.tcr = (float)__dsub_rn(ct, edge_of(t0, tb.tmin, tb.bs));
+                        r.pcr = (float)__dsub_rn(cp, edge_of(p0, pl.imp_min, pl.imp_bs));
+                        r.st = (float)st;
+                        r.sp = (float)sp;
+                        // normalisation to the full charge (GaussianDiffusion.cxx:176-182) with the
+                        // sums of the unit bin integrals taken edge to edge
+                        float sum_t = 1.f, sum_p = 1.f;
+                        if (st > 0) {
+                            const float inv = 1.0f / (1.41421356237309505f * r.st);
+                            sum_t = bin_from_edges(edge_erfc(0.f, (float)tb.bs, r.tcr, inv),
+                                                   edge_erfc((float)nt, (float)tb.bs, r.tcr, inv));
+                        }
+                        if (sp > 0) {
+                            const float inv = 1.0f / (1.41421356237309505f * r.sp);
+                            sum_p = bin_from_edges(edge_erfc(0.f, (float)pl.imp_bs, r.pcr, inv),
+                                                   edge_erfc((float)np, (float)pl.imp_bs, r.pcr, inv));
+                        }
+                        r.qn = (float)(q / ((double)sum_t * (double)sum_p));
+                    }
+                }
+            }
+        }
+        if (i < n) rec[(size_t)ip * n + i] = r;
+        const int w0 = r.np ? r.poff / pl.nimp : 0;
+        const int span = r.np ? (r.poff + r.np - 1) / pl.nimp - w0 + 1 : 0;
+        const int k0 = r.toff / kTile;
+        const int kspan = r.np ? (r.toff + r.nt - 1) / kTile - k0 + 1 : 0;
+        count_visits(wire_cnt, pl.wire_base, w0, span, k0, kspan, ps.ntiles);
+        // fixed-point bounds of the raster: per (wire, tile, 64-tick block)
+        if (r.np) {
+            const float b = visit_bound(r.qn, r.sp, r.st, (float)pl.imp_bs, (float)tb.bs);
+            const int b0 = r.toff / kScaleBlock, b1 = (r.toff + r.nt - 1) / kScaleBlock;
+            for (int ww = 0; ww < span; ++ww) {
+                float* kb = key_bound + (size_t)(pl.wire_base + w0 + ww) * ps.ntiles * kTileBlocks;
+                for (int bb = b0; bb <= b1; ++bb) atomicAdd(kb + bb, b);
+            }
+        }
+        // block reduction, one atomic per block per quantity
+        kpmin = warp_reduce(kpmin, umin);
+        ktmin = warp_reduce(ktmin, umin);
+        kpmax = warp_reduce(kpmax, umax);
+        ktmax = warp_reduce(ktmax, umax);
+        nadd = warp_reduce(nadd, iadd);
+        nout_t = warp_reduce(nout_t, iadd);
+        nout_p = warp_reduce(nout_p, iadd);
+        nover = warp_reduce(nover, iadd);
+        if (l == 0) {
+            s_k[0][w] = kpmin; s_k[1][w] = kpmax; s_k[2][w] = ktmin; s_k[3][w] = ktmax;
+            s_c[0][w] = nadd; s_c[1][w] = nout_t; s_c[2][w] = nout_p; s_c[3][w] = nover;
+        }
+        __syncthreads();
+        if (w == 0) {
+            const int nw = blockDim.x >> 5;
+            kpmin = l < nw ? s_k[0][l] : ~0ull;
+            kpmax = l < nw ? s_k[1][l] : 0ull;
+            ktmin = l < nw ? s_k[2][l] : ~0ull;
+            ktmax = l < nw ? s_k[3][l] : 0ull;
+            nadd = l < nw ? s_c[0][l] : 0;
+            nout_t = l < nw ? s_c[1][l] : 0;
+            nout_p = l < nw ? s_c[2][l] : 0;
+            nover = l < nw ? s_c[3][l] : 0;
+            kpmin = warp_reduce(kpmin, umin);
+            ktmin = warp_reduce(ktmin, umin);
+            kpmax = warp_reduce(kpmax, umax);
+            ktmax = warp_reduce(ktmax, umax);
+            nadd = warp_reduce(nadd, iadd);
+            nout_t = warp_reduce(nout_t, iadd);
+            nout_p = warp_reduce(nout_p, iadd);
+            nover = warp_reduce(nover, iadd);
+            WindowDev* wd = win + ip;
+            if (l == 0 && nadd) {
+                atomicMin(&wd->pmin, kpmin);
+                atomicMax(&wd->pmax, kpmax);
+                atomicMin(&wd->tmin, ktmin);
+                atomicMax(&wd->tmax, ktmax);
+                atomicAdd(&wd->nadded, nadd);
+            }
+            if (l == 0 && nout_t) atomicAdd(&wd->out_time, nout_t);
+            if (l == 0 && nout_p) atomicAdd(&wd->out_pitch, nout_p);
+            if (l == 0 && nover) atomicAdd(&wd->oversize, nover);
+        }
+        __syncthreads();
+    }
+}
+
+void launch_prep_all(const double* depos, int n, const DriftDev& dd, int do_drift, const PlaneSet& ps,
+                     const TimeDev& tb, double drift_speed, double nsigma, PatchRec* rec, WindowDev* win,
+                     int* wire_cnt, float* tprof, float* key_bound, cudaStream_t s)
+{
+    if (n <= 0) return;
+    k_prep_all<<<(n + 255) / 256, 256, 0, s>>>(depos, n, dd, do_drift, ps, tb, drift_speed, nsigma, rec, win,
+                                                 wire_cnt, tprof, key_bound);
+}
+
+// Exclusive scan of the per-wire visit counts (one block).
+__global__ void __launch_bounds__(1024) k_scan(const int* __restrict__ cnt, int n, int* __restrict__ off,
+                                                int* __restrict__ cur)
+{
+    __shared__ int s[1024];
+    const int tid = threadIdx.x;
+    const int chunk = (n + 1023) / 1024;
+    const int b = tid * chunk, e = min(n, b + chunk);
+    int sum = 0;
+    for (int k = b; k < e; ++k) sum += cnt[k];
+    s[tid] = sum;
+    __syncthreads();
+    for (int o = 1; o < 1024; o <<= 1) {
+        const int v = tid >= o ? s[tid - o] : 0;
+        __syncthreads();
+        s[tid] += v;
+        __syncthreads();
+    }
+    int run = s[tid] - sum;
+    for (int k = b; k < e; ++k) {
+        off[k] = run;
+        cur[k] = run;
+        run += cnt[k];
+    }
+    if (tid == 1023) off[n] = s[1023];
+}
+
+void launch_scan(const int* wire_cnt, int nwires_total, int* wire_off, int* wire_cur, cudaStream_t s)
+{
+    k_scan<<<1, 1024, 0, s>>>(wire_cnt, nwires_total, wire_off, wire_cur);
+}
+
+// Per-wire visit lists: wire_list[wire_off[w] ..] holds the depo indices whose
+// patch covers wire w (any order).
+__global__ void __launch_bounds__(256) k_fill(const PatchRec* __restrict__ rec, int n, PlaneSet ps,
+                                              int* __restrict__ cur, Visit* __restrict__ list)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int lane = threadIdx.x & 31;
+    for (int ip = 0; ip < ps.nplanes; ++ip) {
+        const PlaneDev& pl = ps.p[ip];
+        int w0 = 0, span = 0, k0 = 0, kspan = 1;
+        PatchRec r{};
+        if (i < n) {
+            r = rec[(size_t)ip * n + i];
+            if (r.np) {
+                w0 = r.poff / pl.nimp;
+                k0 = r.toff / kTile;
+                kspan = (r.toff + r.nt - 1) / kTile - k0 + 1;
+                span = ((r.poff + r.np - 1) / pl.nimp - w0 + 1) * kspan;
+            }
+        }
+        int maxspan = span;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) maxspan = max(maxspan, __shfl_xor_sync(0xffffffffu, maxspan, o));
+        for (int k = 0; k < maxspan; ++k) {
+            int key = -1;
+            if (k < span) {
+                const int dw = k / kspan, dk = k - dw * kspan;
+                key = (pl.wire_base + w0 + dw) * ps.ntiles + k0 + dk;
+            }
+            const unsigned act = __ballot_sync(0xffffffffu, key >= 0);
+            if (key >= 0) {
+                const unsigned m = __match_any_sync(act, key);
+                const int leader = __ffs(m) - 1;
+                int base = 0;
+                if (lane == leader) base = atomicAdd(cur + key, __popc(m));
+                base = __shfl_sync(m, base, leader);
+                const int rank = __popc(m & ((1u << lane) - 1u));
+                Visit v;
+                v.toff = r.toff;
+                v.poff = r.poff;
+                v.nt_np = ((unsigned)r.nt << 16) | (unsigned)r.np;
+                v.pcr = r.pcr;
+                v.sp = r.sp;
+                v.qn = r.qn;
+                v.d = i;
+                v.pad = 0;
+                list[base + rank] = v;
+            }
+        }
+    }
+}
+
+void launch_fill(const PatchRec* rec, int n, const PlaneSet& ps, int* wire_cur, Visit* visits, cudaStream_t s)
+{
+    if (n <= 0) return;
+    k_fill<<<(n + 255) / 256, 256, 0, s>>>(rec, n, ps, wire_cur, visits);
+}
+
+// ---------------------------------------------------------------------------
+// Charge grids: one block per charge wire row of every plane.  The block
+// accumulates the row's impact-group x tick grid in shared memory (one thread
+// per depo visit of the wire), then writes the G rows of the plane grid with
+// zero padding up to the FFT length.  Each patch bin adds weight*q to the
+// group of its lower impact edge and (1-weight)*q to the next
+// (BinnedDiffusion_transform.cxx:296-367, linear weights of
+// GausDesc::weight, GaussianDiffusion.cxx:61-92).
+//
+// Accumulation is in 32-bit fixed point (native shared-memory integer
+// atomics; FP32 shared atomics are compare-and-swap loops).  Every 64-tick
+// block of the row has its own scale 2^30 / B, where B bounds the magnitude
+// any cell of the block can reach: the sum over the visits touching the block
+// of |q| * max bin fraction in pitch * max bin fraction in time * 2.  Cells
+// cannot overflow and one add is resolved to ~2^-30 of that local bound.
+// Integer sums are order independent, so the grid is bit-reproducible.
+// ---------------------------------------------------------------------------
+constexpr int kRasterThreads = 256;
+constexpr int kStageStride = 13;  // staged coefficients per visit (>= G for G <= 12, plus q; odd: no bank conflicts)
+constexpr int kTileLd = kTile + 8;  // row stride with an 8-word skew between groups
+
+size_t raster_smem_bytes(int G)
+{
+    return sizeof(int) * (size_t)G * kTileLd + sizeof(float) * (size_t)kRasterThreads * kStageStride +
+           sizeof(int4) * (size_t)kRasterThreads;
+}
+
+__global__ void __launch_bounds__(kRasterThreads) k_raster_wires(const PatchRec* __restrict__ rec,
+                                                                 const float* __restrict__ tprof,
+                                                                 const int* __restrict__ wire_cnt,
+                                                                 const int* __restrict__ wire_off,
+                                                                 const Visit* __restrict__ visits,
+                                                                 const float* __restrict__ key_bound, GridSet gs,
+                                                                 float* __restrict__ Q)
+{
+    extern __shared__ int smem_i[];
+    __shared__ float scale[kTileBlocks], iscale[kTileBlocks];
+    int ip = 0;
+    while (ip + 1 < gs.nplanes && (int)blockIdx.x >= gs.p[ip + 1].row_base) ++ip;
+    const GridPlane& P = gs.p[ip];
+    const int rel = blockIdx.x - P.row_base;
+    const int row = rel / P.ntile;
+    const int ktile = P.ktile0 + (rel - row * P.ntile);  // absolute tick tile
+    const int w = P.start_ch + row;
+    const int G = P.G, nimp = P.nimp;
+    const int tick_lo = ktile * kTile;                      // absolute first tick of the tile
+    const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+    int* grid = smem_i;                                       // [G][kTileLd], column = tick - tick_lo
+    float* stage = reinterpret_cast<float*>(smem_i + (size_t)G * kTileLd);
+    int4* stagei = reinterpret_cast<int4*>(stage + (size_t)kRasterThreads * kStageStride);
+    int cnt = 0;
+    const Visit* list = nullptr;
+    int key = -1;
+    if (w >= 0 && w < P.nwires && ktile >= 0 && ktile < gs.ntiles_abs) {
+        key = (P.wire_base + w) * gs.ntiles_abs + ktile;
+        cnt = wire_cnt[key];
+        list = visits + wire_off[key];
+    }
+    {
+        int4* g4 = reinterpret_cast<int4*>(grid);
+        const int n4 = G * kTileLd / 4;
+        for (int k = tid; k < n4; k += kRasterThreads) g4[k] = make_int4(0, 0, 0, 0);
+        if (tid < kTileBlocks) {
+            const float b = key >= 0 ? key_bound[(size_t)key * kTileBlocks + tid] : 0.f;
+            scale[tid] = b > 0.f ? 1073741824.0f / b : 0.f;
+            iscale[tid] = b > 0.f ? b / 1073741824.0f : 0.f;
+        }
+    }
+    __syncthreads();
+    const float pbs = P.pbs, tbs = P.tbs;
+    const int wlo = w * nimp;
+    // pass 2: each lane stages the group coefficients of its own visit, then
+    // the warp scatters the 32 staged visits, two at a time (half-warp per
+    // visit, lanes over ticks, loop over the covered groups).
+    float* my = stage + (size_t)tid * kStageStride;
+    const int wbase = wid * 32;
+    const float inv_pbs = 1.0f / pbs;
+    const int nchunks = (cnt + kRasterThreads - 1) / kRasterThreads;
+    for (int ch = 0; ch < nchunks; ++ch) {
+        const int e = ch * kRasterThreads + tid;
+        int4 si = make_int4(0, 0, 0, 0);  // d, l_lo, ng, (cb << 11) | nt  (cb = toff - tick_lo, ng = 0: none)
+        if (e < cnt) {
+            const Visit r = list[e];
+            const int d = r.d;
+            const int rnp = (int)(r.nt_np & 0xffffu), rnt = (int)(r.nt_np >> 16);
+            const int l_lo = max(r.poff, wlo) - wlo;
+            const int l_hi = min(r.poff + rnp, wlo + nimp) - wlo;
+            if (l_hi > l_lo) {
+                const int ng = l_hi - l_lo + 1;
+                for (int g = 0; g < ng; ++g) my[g] = 0.f;
+                if (r.sp > 0.f) {
+                    const float isg = __frcp_rn(r.sp);
+                    const float inv = 0.70710678118654752f * isg;            // 1/(sqrt2 sigma)
+                    const float c0 = r.sp * inv_pbs * 0.39894228040143268f;  // sigma / (step*sqrt(2 pi))
+                    const int k0 = wlo + l_lo - r.poff;
+                    float x1 = (float)k0 * pbs - r.pcr;
+                    float e1 = copysignf(erfc_nr(fabsf(x1 * inv)), x1);
+                    float u1 = x1 * isg;
+                    float g1 = __expf(-0.5f * u1 * u1);
+                    for (int lb = 0; lb < ng - 1; ++lb) {
+                        const float x2 = (float)(k0 + lb + 1) * pbs - r.pcr;
+                        const float e2 = copysignf(erfc_nr(fabsf(x2 * inv)), x2);
+                        const float u2 = x2 * isg;
+                        const float g2 = __expf(-0.5f * u2 * u2);
+                        const float p = bin_from_edges(e1, e2);
+                        const float wt = p > 0.f ? fmaf(c0 * (g2 - g1), __frcp_rn(p), x2 * inv_pbs) : 0.0f;
+                        my[lb] += p * wt;
+                        my[lb + 1] += p * (1.0f - wt);
+                        e1 = e2;
+                        g1 = g2;
+                    }
+                }
+                else {
+                    const float wt = (pbs - r.pcr) * inv_pbs;
+                    my[0] += wt;
+                    my[1] += 1.0f - wt;
+                }
+                const int cb = r.toff - tick_lo;  // may be negative for patches starting in the previous tile
+                si = make_int4(d, l_lo, ng, ((cb + 1024) << 11) | rnt);
+                my[kStageStride - 1] = r.qn;
+            }
+        }
+        stagei[tid] = si;
+        __syncwarp();
+        const int nv = min(32, cnt - ch * kRasterThreads - wbase);
+        const int half = lane >> 4, hl = lane & 15;
+        for (int v0 = 0; v0 < nv; v0 += 2) {
+            const int v = v0 + half;
+            int4 vi = make_int4(0, 0, 0, 0);
+            if (v < nv) vi = stagei[wbase + v];
+            const int nt = vi.w & 2047;
+            const bool wide = __any_sync(0xffffffffu, nt > 16);
+            if (!wide) {
+                const int ng = vi.z;
+                const int cb = (vi.w >> 11) - 1024;
+                const int c = cb + hl;                  // tile column of this lane's tick
+                const float* vc = stage + (size_t)(wbase + v) * kStageStride;
+                const bool on = ng && hl < nt && c >= 0 && c < kTile;
+                float tq = 0.f;
+                if (on)
+                    tq = __ldg(tprof + (size_t)vi.x * kTprof + hl) * vc[kStageStride - 1] * scale[c / kScaleBlock];
+                const int mg = max(ng, __shfl_xor_sync(0xffffffffu, ng, 16));
+                int* dst = grid + vi.y * kTileLd + c;
+                for (int g = 0; g < mg; ++g) {
+                    if (on && g < ng) atomicAdd(dst, __float2int_rn(vc[g] * tq));
+                    dst += kTileLd;
+                }
+            }
+            else {
+                // at least one of the pair has more than 16 ticks: whole warp per visit
+                for (int hv = 0; hv < 2; ++hv) {
+                    const int vv = v0 + hv;
+                    if (vv >= nv) break;
+                    const int4 wi = stagei[wbase + vv];
+                    const int ng = wi.z;
+                    if (ng == 0) continue;
+                    const int wnt = wi.w & 2047;
+                    const int cb = (wi.w >> 11) - 1024;
+                    const float* vc = stage + (size_t)(wbase + vv) * kStageStride;
+                    const float qn = vc[kStageStride - 1];
+                    const int tstart = max(0, -cb), tend = min(wnt, kTile - cb);  // ticks inside the tile
+                    for (int tc = tstart; tc < tend; tc += 32) {
+                        const int it = tc + lane;
+                        const bool on = it < tend;
+                        float tq = 0.f;
+                        if (on) {
+                            float tv;
+                            if (wnt <= kTprof) tv = __ldg(tprof + (size_t)wi.x * kTprof + it);
+                            else {
+                                const PatchRec r = rec[P.recoff + wi.x];
+                                if (r.st > 0.f) {
+                                    const float inv = 1.0f / (1.41421356237309505f * r.st);
+                                    tv = bin_from_edges(edge_erfc((float)it, tbs, r.tcr, inv),
+                                                        edge_erfc((float)(it + 1), tbs, r.tcr, inv));
+                                }
+                                else tv = 1.0f;
+                            }
+                            tq = tv * qn * scale[(cb + it) / kScaleBlock];
+                        }
+                        int* dst = grid + wi.y * kTileLd + cb + it;
+                        for (int g = 0; g < ng; ++g) {
+                            if (on) atomicAdd(dst, __float2int_rn(vc[g] * tq));
+                            dst += kTileLd;
+                        }
+                    }
                 }
             }
         }
         __syncwarp();
     }
+    __syncthreads();
+    // write the tile's G rows: grid column c is plane column tick_lo + c - col0
+    const int qc0 = tick_lo - P.col0;
+    for (int k = tid; k < G * kTile; k += kRasterThreads) {
+        const int g = k / kTile, c = k - g * kTile;
+        const int qc = qc0 + c;
+        if (qc < 0 || qc >= P.N) continue;
+        const int ccol = tick_lo + c;                  // absolute tick
+        float v = 0.f;
+        if (ccol - P.col0 < P.ncols) v = (float)grid[g * kTileLd + c] * iscale[c / kScaleBlock];
+        Q[P.qoff + ((size_t)g * P.nin + row) * P.N + qc] = v;
+    }
 }
 
-void launch_raster(const PatchRec* rec, int n, const PlaneDev& pl, const TimeDev& tb, int ngroups, int row0,
-                   int nrows, int col0, int ldq, float* Q, WindowDev*, cudaStream_t s)
+void launch_raster_wires(const PatchRec* rec, const float* tprof, const int* wire_cnt, const int* wire_off,
+                         const Visit* visits, const float* key_bound, const GridSet& gs, float* Q, cudaStream_t s)
 {
-    if (n <= 0) return;
-    int blocks = (n + kRasterWarps - 1) / kRasterWarps;
-    if (blocks > 148 * 16) blocks = 148 * 16;
-    k_raster<<<blocks, kRasterWarps * 32, 0, s>>>(rec, n, pl, tb, ngroups, row0, nrows, col0, ldq, Q);
+    if (gs.nrows_total <= 0) return;
+    size_t smem = 0;
+    for (int i = 0; i < gs.nplanes; ++i) smem = std::max(smem, raster_smem_bytes(gs.p[i].G));
+    cudaFuncSetAttribute((const void*)k_raster_wires, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    k_raster_wires<<<gs.nrows_total, kRasterThreads, smem, s>>>(rec, tprof, wire_cnt, wire_off, visits, key_bound,
+                                                                    gs, Q);
 }
 
 // ---------------------------------------------------------------------------
@@ -469,7 +757,7 @@ void launch_irfft_rows(const float2* Vh, int nrows, const FftDesc& d, int wire0,
 // Input row i is wire row0 + i; output row o is wire row0 - P + o.
 // Block: 32 frequencies x 8 row groups, each thread 8 consecutive output
 // rows with a register sliding window over the staged input rows.
-// Bin 0 (packed DC/Nyquist) is redone component-wise by k_wire_conv_dc.
+// Bin 0 (packed DC/Nyquist) is multiplied component-wise.
 // ---------------------------------------------------------------------------
 constexpr int kConvRB = 8;
 constexpr int kConvRG = 8;
@@ -486,6 +774,7 @@ __global__ void __launch_bounds__(32 * kConvRG) k_wire_conv(const float2* __rest
     const int f = blockIdx.x * 32 + lane;
     const int o0 = blockIdx.y * kConvRows;
     const bool fok = f < M;
+    const bool dc = f == 0;
     float2 acc[kConvRB];
 #pragma unroll
     for (int r = 0; r < kConvRB; ++r) acc[r] = make_float2(0.f, 0.f);
@@ -505,10 +794,13 @@ __global__ void __launch_bounds__(32 * kConvRG) k_wire_conv(const float2* __rest
 #pragma unroll
             for (int jj = 0; jj <= 2 * PAD; ++jj) {
                 const float2 rr = __ldg(Rg + (size_t)jj * M);
+                // bin 0 packs two real spectra (DC, Nyquist): multiply component-wise there
+                const float rc = dc ? 0.f : rr.y;
+                const float ry = dc ? rr.y : rr.x;
 #pragma unroll
                 for (int r = 0; r < kConvRB; ++r) {
-                    acc[r].x = fmaf(rr.x, win[r].x, fmaf(-rr.y, win[r].y, acc[r].x));
-                    acc[r].y = fmaf(rr.x, win[r].y, fmaf(rr.y, win[r].x, acc[r].y));
+                    acc[r].x = fmaf(rr.x, win[r].x, fmaf(-rc, win[r].y, acc[r].x));
+                    acc[r].y = fmaf(ry, win[r].y, fmaf(rc, win[r].x, acc[r].y));
                 }
                 if (jj < 2 * PAD) {
 #pragma unroll
@@ -544,14 +836,16 @@ __global__ void __launch_bounds__(32 * kConvRG) k_wire_conv_any(const float2* __
         const float2* Rg = Rh + (size_t)g * (2 * PAD + 1) * M + f;
         for (int jj = 0; jj <= 2 * PAD; ++jj) {
             const float2 rr = Rg[(size_t)jj * M];
+            const float rc = f == 0 ? 0.f : rr.y;
+            const float ry = f == 0 ? rr.y : rr.x;
             const int j = jj - PAD;
 #pragma unroll
             for (int r = 0; r < kConvRB; ++r) {
                 const int i = o0 + rg * kConvRB + r - PAD - j;
                 if (i < 0 || i >= nin) continue;
                 const float2 q = Qh[((size_t)g * nin + i) * M + f];
-                acc[r].x = fmaf(rr.x, q.x, fmaf(-rr.y, q.y, acc[r].x));
-                acc[r].y = fmaf(rr.x, q.y, fmaf(rr.y, q.x, acc[r].y));
+                acc[r].x = fmaf(rr.x, q.x, fmaf(-rc, q.y, acc[r].x));
+                acc[r].y = fmaf(ry, q.y, fmaf(rc, q.x, acc[r].y));
             }
         }
     }
@@ -560,25 +854,6 @@ __global__ void __launch_bounds__(32 * kConvRG) k_wire_conv_any(const float2* __
         const int o = o0 + rg * kConvRB + r;
         if (o < nout) Vh[(size_t)o * M + f] = acc[r];
     }
-}
-
-// Bin 0 holds two real spectra (DC, Nyquist): convolve them component-wise.
-__global__ void k_wire_conv_dc(const float2* __restrict__ Qh, const float2* __restrict__ Rh, float2* __restrict__ Vh,
-                               int G, int PAD, int nin, int nout, int M)
-{
-    const int o = blockIdx.x * blockDim.x + threadIdx.x;
-    if (o >= nout) return;
-    double ax = 0.0, ay = 0.0;
-    for (int g = 0; g < G; ++g)
-        for (int jj = 0; jj <= 2 * PAD; ++jj) {
-            const int i = o - PAD - (jj - PAD);
-            if (i < 0 || i >= nin) continue;
-            const float2 r = Rh[((size_t)g * (2 * PAD + 1) + jj) * M];
-            const float2 q = Qh[((size_t)g * nin + i) * M];
-            ax += (double)r.x * q.x;
-            ay += (double)r.y * q.y;
-        }
-    Vh[(size_t)o * M] = make_float2((float)ax, (float)ay);
 }
 
 void launch_wire_conv(const float2* Qh, const float2* Rh, float2* Vh, int ngroups, int npad, int nrows_in,
@@ -590,7 +865,6 @@ void launch_wire_conv(const float2* Qh, const float2* Rh, float2* Vh, int ngroup
     if (npad == 10) k_wire_conv<10><<<grid, block, 0, s>>>(Qh, Rh, Vh, ngroups, nrows_in, nrows_out, M);
     else if (npad == 21) k_wire_conv<21><<<grid, block, 0, s>>>(Qh, Rh, Vh, ngroups, nrows_in, nrows_out, M);
     else k_wire_conv_any<<<grid, block, 0, s>>>(Qh, Rh, Vh, ngroups, npad, nrows_in, nrows_out, M);
-    k_wire_conv_dc<<<(nrows_out + 127) / 128, 128, 0, s>>>(Qh, Rh, Vh, ngroups, npad, nrows_in, nrows_out, M);
 }
 
 }  // namespace wctb200

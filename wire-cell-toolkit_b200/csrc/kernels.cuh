@@ -9,6 +9,8 @@
 
 namespace wctb200 {
 
+constexpr int kMaxPlanes = 8;
+
 // Drifter configuration (gen/src/Drifter.cxx:62-123).
 struct DriftDev {
     double DL, DT, lifetime, speed, toffset;
@@ -16,9 +18,9 @@ struct DriftDev {
     double xr[8][3];  // anode, response, cathode
 };
 
-// One wire plane as seen by the rasteriser: pitch axis / origin of its
-// Pimpos (util/src/Pimpos.cxx:5-33), its impact binning and the face's
-// sensitive box (gen/src/AnodePlane.cxx:259-290).
+// One wire plane: pitch axis / origin of its Pimpos (util/src/Pimpos.cxx:5-33),
+// its impact binning, the face's sensitive box (gen/src/AnodePlane.cxx:259-290)
+// and the offset of its wires in the event-wide wire arrays.
 struct PlaneDev {
     double ax, ay, az;        // unit pitch axis
     double ox, oy, oz;        // Pimpos origin
@@ -27,7 +29,14 @@ struct PlaneDev {
     double imp_min, imp_max, imp_bs;
     int have_bb;
     double bb_lo[3], bb_hi[3];
-    int depo_slot;            // which drifted-depo flag array applies (face)
+    int wire_base;            // first entry of this plane in per-wire arrays
+};
+
+struct PlaneSet {
+    int nplanes;
+    int nwires_total;
+    int ntiles;               // tick tiles of the readout: ceil(nticks / kTile)
+    PlaneDev p[kMaxPlanes];
 };
 
 // Readout time binning (gen/src/DepoTransform.cxx:180).
@@ -45,9 +54,19 @@ struct PatchRec {
     float pcr;   // center_pitch - edge(poff)
     float st;    // sigma_time
     float sp;    // sigma_pitch
-    float q;     // charge
+    float qn;    // charge / (sum of unit bin integrals in time * in pitch)
 };
 static_assert(sizeof(PatchRec) == 32, "PatchRec layout");
+
+// One depo visit of a (wire, tick tile): what the raster needs of a PatchRec.
+struct Visit {
+    int toff, poff;
+    unsigned int nt_np;  // nt << 16 | np
+    float pcr, sp, qn;
+    int d;               // depo index (time profile, full record)
+    int pad;
+};
+static_assert(sizeof(Visit) == 32, "Visit layout");
 
 // Per-plane window reduction (BinnedDiffusion_transform.cxx:416-464).
 struct WindowDev {
@@ -55,16 +74,43 @@ struct WindowDev {
     int nadded, out_time, out_pitch, oversize;
 };
 
-constexpr int kMaxPatchT = 512;   // raster limit on ticks per patch
-constexpr int kMaxPatchP = 256;   // raster limit on impact bins per patch
+constexpr int kTprof = 16;        // time profiles up to this many ticks are computed once per depo
+constexpr int kTile = 256;        // ticks per charge-grid tile (one raster block per wire x tile)
+constexpr int kScaleBlock = 64;   // ticks sharing one fixed-point scale in the raster
+constexpr int kTileBlocks = kTile / kScaleBlock;
+constexpr int kMaxPatchT = 1024;  // ticks per patch
+constexpr int kMaxPatchP = 1024;  // impact bins per patch
+
+// Per-plane parameters of the charge-grid stage of one event.
+struct GridPlane {
+    int nimp, G;
+    int nwires, wire_base;
+    int start_ch, nin;        // charge rows: wires start_ch .. start_ch+nin-1
+    int col0, ncols;          // charge columns: ticks col0 .. col0+ncols-1
+    int N;                    // row length of the grid (time FFT length)
+    float tbs, pbs;           // tick and impact bin sizes
+    long long qoff;           // offset of this plane's grid [G][nin][N] in floats
+    long long recoff;         // offset of this plane's PatchRecs
+    int row_base;             // first block of this plane in the raster grid
+    int ktile0, ntile;        // absolute tick tiles covering grid columns [0, N)
+};
+
+struct GridSet {
+    int nplanes;
+    int nrows_total;          // raster blocks (wire rows x tiles, all planes)
+    int ntiles_abs;           // tick tiles of the readout (visit-list key stride)
+    GridPlane p[kMaxPlanes];
+};
 
 // ---- launchers (kernels.cu) ----
-void launch_drift(const double* depos, int n, const DriftDev& dd, int do_drift, double* out, unsigned char* valid,
-                  cudaStream_t s);
-void launch_prep(const double* depos, const unsigned char* valid, int n, const PlaneDev& pl, const TimeDev& tb,
-                 double drift_speed, double nsigma, PatchRec* rec, WindowDev* win, cudaStream_t s);
-void launch_raster(const PatchRec* rec, int n, const PlaneDev& pl, const TimeDev& tb, int ngroups, int row0,
-                   int nrows, int col0, int ldq, float* Q, WindowDev* win, cudaStream_t s);
+void launch_prep_all(const double* depos, int n, const DriftDev& dd, int do_drift, const PlaneSet& ps,
+                     const TimeDev& tb, double drift_speed, double nsigma, PatchRec* rec, WindowDev* win,
+                     int* wire_cnt, float* tprof, float* key_bound, cudaStream_t s);
+void launch_scan(const int* wire_cnt, int nwires_total, int* wire_off, int* wire_cur, cudaStream_t s);
+void launch_fill(const PatchRec* rec, int n, const PlaneSet& ps, int* wire_cur, Visit* visits, cudaStream_t s);
+size_t raster_smem_bytes(int G);
+void launch_raster_wires(const PatchRec* rec, const float* tprof, const int* wire_cnt, const int* wire_off,
+                         const Visit* visits, const float* key_bound, const GridSet& gs, float* Q, cudaStream_t s);
 void launch_rfft_rows(const float* in, long in_ld, int in_len, float2* out, long out_ld, int nrows,
                       const FftDesc& d, cudaStream_t s);
 void launch_wire_conv(const float2* Qh, const float2* Rh, float2* Vh, int ngroups, int npad, int nrows_in,
