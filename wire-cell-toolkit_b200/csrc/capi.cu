@@ -132,6 +132,7 @@ struct PlaneState {
     // response table
     bool have_resp{false};
     int G{0}, npad{0}, nresp{0}, ldr{0}, waveform_pad{0};
+    bool mirror{false};    // table[G-1-g][-j] == table[g][j] exactly: pair groups in the convolution
     double pitch{0}, impact{0};
     DevBuf d_table;        // [G][2npad+1][ldr] floats
     int spec_N{0};
@@ -533,7 +534,7 @@ static int forward_device(Core& c, const double* d_depos, size_t ndepos, float* 
         t_f.close(1);
         Core::StageTimer t_c(&c, 3, s);
         launch_wire_conv(reinterpret_cast<const float2*>(Q), ps.d_spec.as<float2>(), c.d_V.as<float2>(), ps.G, ps.npad,
-                         nin, nout, M, s);
+                         nin, nout, M, ps.mirror, s);
         t_c.close(1);
         const int wlo = std::max(0, w.m_start_ch), whi = std::min(ps.desc.nwires, w.m_end_ch);
         Core::StageTimer t_i(&c, 4, s);
@@ -749,6 +750,18 @@ int wct_dt_set_response_table(wct_depotransform* h, int face, int plane, int ngr
     for (size_t r = 0; r < rows; ++r) std::copy(table + r * nsamples, table + (r + 1) * nsamples, t.data() + r * ps->ldr);
     CUDA_TRY(ps->d_table.ensure(sizeof(float) * t.size()));
     CUDA_TRY(cudaMemcpy(ps->d_table.p, t.data(), sizeof(float) * t.size(), cudaMemcpyHostToDevice));
+    // mirror symmetry of the impact groups (gen/src/PlaneImpactResponse.cxx:256-268)
+    bool mirror = true;
+    const int J = 2 * npad + 1;
+    for (int g = 0; g < ngroups && mirror; ++g) {
+        if (2 * g == ngroups - 1) continue;  // the centre group is convolved on its own
+        for (int j = 0; j < J && mirror; ++j) {
+            const float* a = table + ((size_t)g * J + j) * nsamples;
+            const float* b = table + ((size_t)(ngroups - 1 - g) * J + (J - 1 - j)) * nsamples;
+            if (std::memcmp(a, b, sizeof(float) * nsamples) != 0) mirror = false;
+        }
+    }
+    ps->mirror = mirror;
     ps->spec_N = 0;
     ps->have_resp = true;
     return WCT_OK;

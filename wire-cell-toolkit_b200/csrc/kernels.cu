@@ -469,7 +469,10 @@ void launch_fill(const PatchRec* rec, int n, const PlaneSet& ps, int* wire_cur, 
 // Integer sums are order independent, so the grid is bit-reproducible.
 // ---------------------------------------------------------------------------
 constexpr int kRasterThreads = 256;
-constexpr int kStageStride = 13;  // staged coefficients per visit (>= G for G <= 12, plus q; odd: no bank conflicts)
+// staged per visit: 12 group coefficients, q, and 16 scaled tick values (odd stride: no bank conflicts)
+constexpr int kStageQ = 12;
+constexpr int kStageT = 13;
+constexpr int kStageStride = 29;
 constexpr int kTileLd = kTile + 8;  // row stride with an 8-word skew between groups
 
 size_t raster_smem_bytes(int G)
@@ -570,7 +573,18 @@ __global__ void __launch_bounds__(kRasterThreads) k_raster_wires(const PatchRec*
                 }
                 const int cb = r.toff - tick_lo;  // may be negative for patches starting in the previous tile
                 si = make_int4(d, l_lo, ng, ((cb + 1024) << 11) | rnt);
-                my[kStageStride - 1] = r.qn;
+                my[kStageQ] = r.qn;
+                if (rnt <= 16) {
+                    // tick values scaled to the fixed point of their 64-tick block (0 outside the tile)
+                    const float* tp = tprof + (size_t)d * kTprof;
+#pragma unroll
+                    for (int k = 0; k < 16; ++k) {
+                        const int c = cb + k;
+                        float v = 0.f;
+                        if (k < rnt && c >= 0 && c < kTile) v = __ldg(tp + k) * r.qn * scale[c / kScaleBlock];
+                        my[kStageT + k] = v;
+                    }
+                }
             }
         }
         stagei[tid] = si;
@@ -589,14 +603,16 @@ __global__ void __launch_bounds__(kRasterThreads) k_raster_wires(const PatchRec*
                 const int c = cb + hl;                  // tile column of this lane's tick
                 const float* vc = stage + (size_t)(wbase + v) * kStageStride;
                 const bool on = ng && hl < nt && c >= 0 && c < kTile;
-                float tq = 0.f;
-                if (on)
-                    tq = __ldg(tprof + (size_t)vi.x * kTprof + hl) * vc[kStageStride - 1] * scale[c / kScaleBlock];
+                const float tq = on ? vc[kStageT + hl] : 0.f;
                 const int mg = max(ng, __shfl_xor_sync(0xffffffffu, ng, 16));
+                float cf[kStageQ];
+#pragma unroll
+                for (int g = 0; g < kStageQ; ++g) cf[g] = vc[g];
                 int* dst = grid + vi.y * kTileLd + c;
-                for (int g = 0; g < mg; ++g) {
-                    if (on && g < ng) atomicAdd(dst, __float2int_rn(vc[g] * tq));
-                    dst += kTileLd;
+#pragma unroll
+                for (int g = 0; g < kStageQ; ++g) {
+                    if (g >= mg) break;
+                    if (on && g < ng) atomicAdd(dst + g * kTileLd, __float2int_rn(cf[g] * tq));
                 }
             }
             else {
@@ -610,7 +626,7 @@ __global__ void __launch_bounds__(kRasterThreads) k_raster_wires(const PatchRec*
                     const int wnt = wi.w & 2047;
                     const int cb = (wi.w >> 11) - 1024;
                     const float* vc = stage + (size_t)(wbase + vv) * kStageStride;
-                    const float qn = vc[kStageStride - 1];
+                    const float qn = vc[kStageQ];
                     const int tstart = max(0, -cb), tend = min(wnt, kTile - cb);  // ticks inside the tile
                     for (int tc = tstart; tc < tend; tc += 32) {
                         const int it = tc + lane;
@@ -763,13 +779,21 @@ constexpr int kConvRB = 8;
 constexpr int kConvRG = 8;
 constexpr int kConvRows = kConvRB * kConvRG;
 
-template <int PAD>
+template <int PAD, bool PAIR>
 __global__ void __launch_bounds__(32 * kConvRG) k_wire_conv(const float2* __restrict__ Qh,
                                                              const float2* __restrict__ Rh, float2* __restrict__ Vh,
                                                              int G, int nin, int nout, int M)
 {
+    // PAIR: groups g and G-1-g share one response up to a mirror in wire
+    // (R_{G-1-g}[j] = R_g[-j], the symmetrised impact map of
+    // gen/src/PlaneImpactResponse.cxx:256-268), so for each tap the two
+    // mirrored inputs are added before one complex multiply.
     constexpr int SROWS = kConvRows + 2 * PAD;
-    __shared__ float2 Qs[SROWS][32];
+    constexpr int NT = 2 * PAD + 1;
+    extern __shared__ float2 conv_smem[];
+    float2 (*Qs)[32] = reinterpret_cast<float2 (*)[32]>(conv_smem);
+    float2 (*Qs2)[32] = reinterpret_cast<float2 (*)[32]>(conv_smem + SROWS * 32);
+    float2 (*Rs)[32] = reinterpret_cast<float2 (*)[32]>(conv_smem + (PAIR ? 2 : 1) * SROWS * 32);
     const int lane = threadIdx.x, rg = threadIdx.y;
     const int f = blockIdx.x * 32 + lane;
     const int o0 = blockIdx.y * kConvRows;
@@ -779,33 +803,50 @@ __global__ void __launch_bounds__(32 * kConvRG) k_wire_conv(const float2* __rest
 #pragma unroll
     for (int r = 0; r < kConvRB; ++r) acc[r] = make_float2(0.f, 0.f);
     const int rb0 = rg * kConvRB;
-    for (int g = 0; g < G; ++g) {
+    const int ng = PAIR ? (G + 1) / 2 : G;
+    for (int gi = 0; gi < ng; ++gi) {
+        const int g = gi;
+        const int g2 = G - 1 - gi;
+        const bool pair = PAIR && g2 != g;
         __syncthreads();
         for (int s = rg; s < SROWS; s += kConvRG) {
             const int i = o0 - 2 * PAD + s;
-            Qs[s][lane] = (fok && i >= 0 && i < nin) ? Qh[((size_t)g * nin + i) * M + f] : make_float2(0.f, 0.f);
+            const bool ok = fok && i >= 0 && i < nin;
+            Qs[s][lane] = ok ? Qh[((size_t)g * nin + i) * M + f] : make_float2(0.f, 0.f);
+            if (PAIR) Qs2[s][lane] = (ok && pair) ? Qh[((size_t)g2 * nin + i) * M + f] : make_float2(0.f, 0.f);
         }
+        for (int jj = rg; jj < NT; jj += kConvRG)
+            Rs[jj][lane] = fok ? Rh[((size_t)g * NT + jj) * M + f] : make_float2(0.f, 0.f);
         __syncthreads();
         if (fok) {
-            const float2* Rg = Rh + (size_t)g * (2 * PAD + 1) * M + f;
-            float2 win[kConvRB];
+            float2 win[kConvRB], win2[kConvRB];
 #pragma unroll
-            for (int r = 0; r < kConvRB; ++r) win[r] = Qs[rb0 + r + 2 * PAD][lane];
+            for (int r = 0; r < kConvRB; ++r) {
+                win[r] = Qs[rb0 + r + 2 * PAD][lane];       // input row o - PAD - j at j = -PAD
+                if (PAIR) win2[r] = Qs2[rb0 + r][lane];     // input row o - PAD + j at j = -PAD
+            }
 #pragma unroll
-            for (int jj = 0; jj <= 2 * PAD; ++jj) {
-                const float2 rr = __ldg(Rg + (size_t)jj * M);
+            for (int jj = 0; jj < NT; ++jj) {
+                const float2 rr = Rs[jj][lane];
                 // bin 0 packs two real spectra (DC, Nyquist): multiply component-wise there
                 const float rc = dc ? 0.f : rr.y;
                 const float ry = dc ? rr.y : rr.x;
 #pragma unroll
                 for (int r = 0; r < kConvRB; ++r) {
-                    acc[r].x = fmaf(rr.x, win[r].x, fmaf(-rc, win[r].y, acc[r].x));
-                    acc[r].y = fmaf(ry, win[r].y, fmaf(rc, win[r].x, acc[r].y));
+                    float2 q = win[r];
+                    if (PAIR) q = make_float2(q.x + win2[r].x, q.y + win2[r].y);
+                    acc[r].x = fmaf(rr.x, q.x, fmaf(-rc, q.y, acc[r].x));
+                    acc[r].y = fmaf(ry, q.y, fmaf(rc, q.x, acc[r].y));
                 }
-                if (jj < 2 * PAD) {
+                if (jj < NT - 1) {
 #pragma unroll
                     for (int r = kConvRB - 1; r > 0; --r) win[r] = win[r - 1];
                     win[0] = Qs[rb0 + 2 * PAD - jj - 1][lane];
+                    if (PAIR) {
+#pragma unroll
+                        for (int r = 0; r < kConvRB - 1; ++r) win2[r] = win2[r + 1];
+                        win2[kConvRB - 1] = Qs2[rb0 + kConvRB + jj][lane];
+                    }
                 }
             }
         }
@@ -857,13 +898,26 @@ __global__ void __launch_bounds__(32 * kConvRG) k_wire_conv_any(const float2* __
 }
 
 void launch_wire_conv(const float2* Qh, const float2* Rh, float2* Vh, int ngroups, int npad, int nrows_in,
-                      int nrows_out, int M, cudaStream_t s)
+                      int nrows_out, int M, bool pair, cudaStream_t s)
 {
     if (nrows_out <= 0) return;
     dim3 grid((M + 31) / 32, (nrows_out + kConvRows - 1) / kConvRows);
     dim3 block(32, kConvRG);
-    if (npad == 10) k_wire_conv<10><<<grid, block, 0, s>>>(Qh, Rh, Vh, ngroups, nrows_in, nrows_out, M);
-    else if (npad == 21) k_wire_conv<21><<<grid, block, 0, s>>>(Qh, Rh, Vh, ngroups, nrows_in, nrows_out, M);
+    auto smem = [](int pad, bool pr) {
+        return sizeof(float2) * 32 * ((size_t)(pr ? 2 : 1) * (kConvRows + 2 * pad) + (2 * pad + 1));
+    };
+#define WCT_CONV(P, B)                                                                                        \
+    do {                                                                                                      \
+        const size_t sm = smem(P, B);                                                                         \
+        cudaFuncSetAttribute((const void*)k_wire_conv<P, B>, cudaFuncAttributeMaxDynamicSharedMemorySize,    \
+                             (int)sm);                                                                        \
+        k_wire_conv<P, B><<<grid, block, sm, s>>>(Qh, Rh, Vh, ngroups, nrows_in, nrows_out, M);               \
+    } while (0)
+    if (npad == 10 && pair) WCT_CONV(10, true);
+    else if (npad == 10) WCT_CONV(10, false);
+    else if (npad == 21 && pair) WCT_CONV(21, true);
+    else if (npad == 21) WCT_CONV(21, false);
+#undef WCT_CONV
     else k_wire_conv_any<<<grid, block, 0, s>>>(Qh, Rh, Vh, ngroups, npad, nrows_in, nrows_out, M);
 }
 

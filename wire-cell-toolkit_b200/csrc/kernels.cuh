@@ -114,7 +114,7 @@ void launch_raster_wires(const PatchRec* rec, const float* tprof, const int* wir
 void launch_rfft_rows(const float* in, long in_ld, int in_len, float2* out, long out_ld, int nrows,
                       const FftDesc& d, cudaStream_t s);
 void launch_wire_conv(const float2* Qh, const float2* Rh, float2* Vh, int ngroups, int npad, int nrows_in,
-                      int nrows_out, int M, cudaStream_t s);
+                      int nrows_out, int M, bool pair, cudaStream_t s);
 void launch_irfft_rows(const float2* Vh, int nrows, const FftDesc& d, int wire0, int wlo, int whi, int tick0,
                        int ncols, int nticks, float* frame, cudaStream_t s);
 
