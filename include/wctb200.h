@@ -103,6 +103,21 @@ int wct_pir_info(const wct_pir* pir, double* pitch, double* impact, double* half
 int wct_pir_waveform(const wct_pir* pir, int path, float* out);
 int wct_pir_destroy(wct_pir* pir);
 
+/* ---- Batched FFT convolution of rows ---- */
+
+/* Circular convolution of each real row with one real response at FFT length
+ * nfft: out[r][k] = sum_m in[r][m] * resp[(k - m) mod nfft] for k < n_out,
+ * rows and response zero padded to nfft.  nfft = 0 picks the smallest
+ * supported length >= n_in + n_resp - 1 (a linear convolution).  This is
+ * DftTools::convolve (aux/src/DftTools.cxx:145-168) applied to many rows, and
+ * the long-range response step of ImpactTransform::waveform
+ * (gen/src/ImpactTransform.cxx:327-343).  Device pointers, enqueued on stream
+ * (cudaStream_t, NULL = legacy default stream) of the current device; scratch
+ * is taken from the stream-ordered allocator.  Supported nfft: multiples of 4
+ * whose half has no prime factor above 7 (WCT_ERR_SIZE otherwise). */
+int wct_convolve_rows_device(const float* in, long ld_in, int nrows, int n_in, const float* resp, int n_resp,
+                             int nfft, float* out, long ld_out, int n_out, void* stream);
+
 /* ---- DepoTransform (gen/src/DepoTransform.cxx, IDepoFramer) ---- */
 
 /* DepoTransform::configure (gen/src/DepoTransform.cxx:76-113) from JSON with

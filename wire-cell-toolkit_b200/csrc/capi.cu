@@ -549,6 +549,57 @@ static int forward_device(Core& c, const double* d_depos, size_t ndepos, float* 
     return WCT_OK;
 }
 
+// ---------------------------------------------------------------------------
+// Stand-alone operations: per-device FFT plans.
+// ---------------------------------------------------------------------------
+static std::mutex g_ops_mtx;
+static std::map<std::pair<int, int>, std::unique_ptr<FftPlanDev>> g_plans;  // (device, M)
+
+static int device_plan(int M, FftDesc& d)
+{
+    int dev = 0;
+    CUDA_TRY(cudaGetDevice(&dev));
+    std::lock_guard<std::mutex> lk(g_ops_mtx);
+    auto key = std::make_pair(dev, M);
+    auto it = g_plans.find(key);
+    if (it == g_plans.end()) {
+        auto p = std::make_unique<FftPlanDev>();
+        int rc = make_plan(M, *p);
+        if (rc) return rc;
+        it = g_plans.emplace(key, std::move(p)).first;
+    }
+    d = it->second->desc;
+    return WCT_OK;
+}
+
+// Checks shared by the row-convolution entry points; picks the FFT length.
+static int convolve_args(const float* in, long ld_in, int nrows, int n_in, const float* resp, int n_resp, int& nfft,
+                         float* out, long ld_out, int n_out)
+{
+    if (!in || !resp || !out || nrows < 0 || n_in < 0 || n_resp <= 0 || n_out < 0 || ld_in < n_in ||
+        ld_out < n_out)
+        return fail(WCT_ERR_ARG, "convolve rows: bad arguments");
+    if (nfft == 0) nfft = gpu_fft_length(std::max(4, n_in + n_resp - 1));
+    std::vector<int> r;
+    if (nfft <= 0 || nfft % 4 || !fft_radices(nfft / 2, r))
+        return fail(WCT_ERR_SIZE, "convolve rows: unsupported FFT length");
+    if (n_out > nfft) return fail(WCT_ERR_ARG, "convolve rows: n_out exceeds the FFT length");
+    return WCT_OK;
+}
+
+// The convolution itself on caller-provided scratch: X [nrows][M] and R [M].
+static int convolve_on(const float* in, long ld_in, int nrows, int n_in, const float* resp, int n_resp, int nfft,
+                       float* out, long ld_out, int n_out, const FftDesc& d, float2* X, float2* R, cudaStream_t s)
+{
+    const int M = nfft / 2;
+    launch_rfft_rows(resp, n_resp, std::min(n_resp, nfft), R, M, 1, d, s);
+    launch_rfft_rows(in, ld_in, std::min(n_in, nfft), X, M, nrows, d, s);
+    launch_spec_mul(X, M, nrows, M, R, s);
+    launch_irfft_rows(X, nrows, d, 0, 0, nrows, 0, n_out, (int)ld_out, out, s);
+    CUDA_TRY(cudaGetLastError());
+    return WCT_OK;
+}
+
 }  // namespace wctb200
 
 using namespace wctb200;
@@ -623,6 +674,26 @@ int wct_pir_waveform(const wct_pir* p, int path, float* out)
 int wct_pir_destroy(wct_pir* p)
 {
     delete p;
+    return WCT_OK;
+}
+
+int wct_convolve_rows_device(const float* in, long ld_in, int nrows, int n_in, const float* resp, int n_resp,
+                             int nfft, float* out, long ld_out, int n_out, void* stream)
+{
+    int rc = convolve_args(in, ld_in, nrows, n_in, resp, n_resp, nfft, out, ld_out, n_out);
+    if (rc) return rc;
+    if (nrows == 0 || n_out == 0) return WCT_OK;
+    FftDesc d;
+    rc = device_plan(nfft / 2, d);
+    if (rc) return rc;
+    cudaStream_t s = (cudaStream_t)stream;
+    const int M = nfft / 2;
+    float2* scratch = nullptr;
+    CUDA_TRY(cudaMallocAsync(&scratch, sizeof(float2) * (size_t)M * (nrows + 1), s));
+    rc = convolve_on(in, ld_in, nrows, n_in, resp, n_resp, nfft, out, ld_out, n_out, d, scratch + M, scratch, s);
+    cudaError_t e = cudaFreeAsync(scratch, s);
+    if (rc) return rc;
+    if (e != cudaSuccess) return fail(WCT_ERR_CUDA, cudaGetErrorString(e));
     return WCT_OK;
 }
 

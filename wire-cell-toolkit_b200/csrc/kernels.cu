@@ -694,7 +694,7 @@ __global__ void k_rfft_rows(const float* in, long in_ld, int in_len, float2* out
     float2* b = sm + d.M;
     const int M = d.M, tid = threadIdx.x, nth = blockDim.x;
     const float* x = in + (size_t)row * in_ld;
-    if (in_len >= 2 * M) {
+    if (in_len >= 2 * M && ((reinterpret_cast<uintptr_t>(x) & 7) == 0)) {
         const float2* x2 = reinterpret_cast<const float2*>(x);
         for (int m = tid; m < M; m += nth) a[m] = x2[m];
     }
@@ -919,6 +919,45 @@ void launch_wire_conv(const float2* Qh, const float2* Rh, float2* Vh, int ngroup
     else if (npad == 21) WCT_CONV(21, false);
 #undef WCT_CONV
     else k_wire_conv_any<<<grid, block, 0, s>>>(Qh, Rh, Vh, ngroups, npad, nrows_in, nrows_out, M);
+}
+
+// ---------------------------------------------------------------------------
+// Batched row convolution helpers (DftTools::convolve, aux/src/DftTools.cxx:145-168).
+// ---------------------------------------------------------------------------
+// X[row][k] *= R[k] on packed real spectra (bin 0 component-wise).
+__global__ void k_spec_mul(float2* __restrict__ X, long ldx, int nrows, int M, const float2* __restrict__ R)
+{
+    const int row = blockIdx.y;
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < M; k += gridDim.x * blockDim.x) {
+        const float2 r = R[k];
+        float2 x = X[(size_t)row * ldx + k];
+        x = k == 0 ? make_float2(x.x * r.x, x.y * r.y) : cmul(x, r);
+        X[(size_t)row * ldx + k] = x;
+    }
+}
+
+void launch_spec_mul(float2* X, long ldx, int nrows, int M, const float2* R, cudaStream_t s)
+{
+    if (nrows <= 0) return;
+    dim3 grid((M + 255) / 256, nrows);
+    k_spec_mul<<<grid, 256, 0, s>>>(X, ldx, nrows, M, R);
+}
+
+// exp(-2 pi i m / M) and exp(-2 pi i m / (2M)) in double, stored as float.
+__global__ void k_twiddles(float2* __restrict__ tw, float2* __restrict__ twh, int M)
+{
+    for (int m = blockIdx.x * blockDim.x + threadIdx.x; m < M; m += gridDim.x * blockDim.x) {
+        double sa, ca, sb, cb;
+        sincospi(-2.0 * (double)m / (double)M, &sa, &ca);
+        sincospi(-(double)m / (double)M, &sb, &cb);
+        tw[m] = make_float2((float)ca, (float)sa);
+        twh[m] = make_float2((float)cb, (float)sb);
+    }
+}
+
+void launch_twiddles(float2* tw, float2* twh, int M, cudaStream_t s)
+{
+    k_twiddles<<<(M + 255) / 256, 256, 0, s>>>(tw, twh, M);
 }
 
 }  // namespace wctb200

@@ -118,4 +118,7 @@ void launch_wire_conv(const float2* Qh, const float2* Rh, float2* Vh, int ngroup
 void launch_irfft_rows(const float2* Vh, int nrows, const FftDesc& d, int wire0, int wlo, int whi, int tick0,
                        int ncols, int nticks, float* frame, cudaStream_t s);
 
+void launch_spec_mul(float2* X, long ldx, int nrows, int M, const float2* R, cudaStream_t s);
+void launch_twiddles(float2* tw, float2* twh, int M, cudaStream_t s);
+
 }  // namespace wctb200
