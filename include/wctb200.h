@@ -118,6 +118,23 @@ int wct_pir_destroy(wct_pir* pir);
 int wct_convolve_rows_device(const float* in, long ld_in, int nrows, int n_in, const float* resp, int n_resp,
                              int nfft, float* out, long ld_out, int n_out, void* stream);
 
+/* The same convolution without any allocation, for callers that may not
+ * allocate device memory once they are running: an online trigger or DAQ
+ * process whose device-memory budget is fixed at start-up, or a host
+ * framework that owns all device memory through its own pool and forbids
+ * allocations behind its back (an allocation can fail under fragmentation and
+ * can synchronise the device mid-run).  No counterpart in the reference, which
+ * has no device path here.  Scratch is a fixed 32 MiB array in the library's
+ * device image, held by every GPU that loads the library until the process
+ * exits; a call needs (nrows + 3) * nfft / 2 <= 4194304 complex values and
+ * returns WCT_ERR_SIZE beyond that.  The first call on a device looks up the
+ * array's address (cudaGetSymbolAddress) with that device current; make that
+ * first call before any stream capture.  All calls share the array and each
+ * overwrites what it uses: calls that overlap on the GPU (other streams or
+ * threads) race, so serialise them. */
+int wct_convolve_rows_device_noalloc(const float* in, long ld_in, int nrows, int n_in, const float* resp,
+                                     int n_resp, int nfft, float* out, long ld_out, int n_out, void* stream);
+
 /* ---- DepoTransform (gen/src/DepoTransform.cxx, IDepoFramer) ---- */
 
 /* DepoTransform::configure (gen/src/DepoTransform.cxx:76-113) from JSON with

@@ -70,6 +70,8 @@ SIGNATURES = {
     "wct_pir_destroy": (C.c_int, [C.c_void_p]),
     "wct_convolve_rows_device": (C.c_int, [C.c_void_p, C.c_long, C.c_int, C.c_int, C.c_void_p, C.c_int, C.c_int,
                                            C.c_void_p, C.c_long, C.c_int, C.c_void_p]),
+    "wct_convolve_rows_device_noalloc": (C.c_int, [C.c_void_p, C.c_long, C.c_int, C.c_int, C.c_void_p, C.c_int,
+                                                   C.c_int, C.c_void_p, C.c_long, C.c_int, C.c_void_p]),
     "wct_dt_create": (C.c_int, [C.c_char_p, C.POINTER(C.c_void_p)]),
     "wct_dt_default_configuration": (C.c_int, [C.c_char_p, C.c_size_t]),
     "wct_dt_add_face": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(C.c_int)]),
@@ -163,6 +165,14 @@ def convolve_rows(d_in, ld_in, nrows, n_in, d_resp, n_resp, d_out, ld_out, n_out
     """Batched FFT convolution of device rows with one response (pointers as ints)."""
     _check(lib().wct_convolve_rows_device(C.c_void_p(d_in), ld_in, nrows, n_in, C.c_void_p(d_resp), n_resp, nfft,
                                           C.c_void_p(d_out), ld_out, n_out, C.c_void_p(stream) if stream else None))
+
+
+def convolve_rows_noalloc(d_in, ld_in, nrows, n_in, d_resp, n_resp, d_out, ld_out, n_out, nfft=0, stream=None):
+    """Same as convolve_rows with no device allocation: scratch is the library's
+    fixed 32 MiB device array (see wct_convolve_rows_device_noalloc)."""
+    _check(lib().wct_convolve_rows_device_noalloc(C.c_void_p(d_in), ld_in, nrows, n_in, C.c_void_p(d_resp), n_resp,
+                                                  nfft, C.c_void_p(d_out), ld_out, n_out,
+                                                  C.c_void_p(stream) if stream else None))
 
 
 class DepoTransform:

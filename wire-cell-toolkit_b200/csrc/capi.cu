@@ -23,13 +23,15 @@
 
 namespace wctb200 {
 
-static thread_local std::string g_last_error;
+static thread_local char g_last_error[512];
 
-static int fail(int code, const std::string& msg)
+static int fail(int code, const char* msg)
 {
-    g_last_error = msg;
+    std::strncpy(g_last_error, msg, sizeof(g_last_error) - 1);
+    g_last_error[sizeof(g_last_error) - 1] = '\0';
     return code;
 }
+static int fail(int code, const std::string& msg) { return fail(code, msg.c_str()); }
 
 #define CUDA_TRY(expr)                                                                                   \
     do {                                                                                                 \
@@ -72,38 +74,47 @@ struct FftPlanDev {
     DevBuf tw, twh;
 };
 
-// Radix schedule for M; false if M has a prime factor above 7.
-static bool fft_radices(int M, std::vector<int>& r)
+// Radix schedule for M (no heap use); false if M has a prime factor above 7
+// or needs more than kFftMaxStages stages.
+static bool fft_radices(int M, int* r, int& nst)
 {
-    r.clear();
+    nst = 0;
+    if (M < 1) return false;
     int m = M;
-    while (m % 8 == 0) { r.push_back(8); m /= 8; }
-    if (m % 4 == 0) { r.push_back(4); m /= 4; }
-    if (m % 2 == 0) { r.push_back(2); m /= 2; }
+    auto push = [&](int f) {
+        if (nst >= kFftMaxStages) return false;
+        r[nst++] = f;
+        m /= f;
+        return true;
+    };
+    while (m % 8 == 0) if (!push(8)) return false;
+    if (m % 4 == 0 && !push(4)) return false;
+    if (m % 2 == 0 && !push(2)) return false;
     for (int f : {7, 5, 3})
-        while (m % f == 0) { r.push_back(f); m /= f; }
-    return m == 1 && (int)r.size() <= kFftMaxStages;
+        while (m % f == 0) if (!push(f)) return false;
+    return m == 1;
+}
+static bool fft_supported(int M)
+{
+    int r[kFftMaxStages], n = 0;
+    return fft_radices(M, r, n);
 }
 
 // Smallest N >= n, N a multiple of 4, whose half has only the factors 2, 3, 5, 7
 // (the reference's own length whenever it qualifies).
 static int gpu_fft_length(int n)
 {
-    std::vector<int> r;
     int N = (n + 3) & ~3;
-    while (true) {
-        if (fft_radices(N / 2, r)) return N;
-        N += 4;
-    }
+    while (!fft_supported(N / 2)) N += 4;
+    return N;
 }
 
 static int make_plan(int M, FftPlanDev& p)
 {
-    std::vector<int> r;
-    if (!fft_radices(M, r)) return fail(WCT_ERR_SIZE, "FFT length has a prime factor above 7");
+    int nst = 0;
+    if (!fft_radices(M, p.desc.radix, nst)) return fail(WCT_ERR_SIZE, "FFT length has a prime factor above 7");
     p.desc.M = M;
-    p.desc.nst = (int)r.size();
-    for (size_t i = 0; i < r.size(); ++i) p.desc.radix[i] = r[i];
+    p.desc.nst = nst;
     std::vector<float2> tw(M), twh(M);
     const double twopi = 6.283185307179586476925286766559;
     for (int m = 0; m < M; ++m) {
@@ -580,8 +591,7 @@ static int convolve_args(const float* in, long ld_in, int nrows, int n_in, const
         ld_out < n_out)
         return fail(WCT_ERR_ARG, "convolve rows: bad arguments");
     if (nfft == 0) nfft = gpu_fft_length(std::max(4, n_in + n_resp - 1));
-    std::vector<int> r;
-    if (nfft <= 0 || nfft % 4 || !fft_radices(nfft / 2, r))
+    if (nfft <= 0 || nfft % 4 || !fft_supported(nfft / 2))
         return fail(WCT_ERR_SIZE, "convolve rows: unsupported FFT length");
     if (n_out > nfft) return fail(WCT_ERR_ARG, "convolve rows: n_out exceeds the FFT length");
     return WCT_OK;
@@ -600,6 +610,38 @@ static int convolve_on(const float* in, long ld_in, int nrows, int n_in, const f
     return WCT_OK;
 }
 
+// ---------------------------------------------------------------------------
+// Allocation-free row convolution: all scratch (twiddle tables, the response
+// spectrum and the row spectra) lives in this fixed device array, reserved on
+// every GPU that loads the library for as long as the process runs.  Every
+// call overwrites the parts it uses, so nothing needs clearing, and calls that
+// overlap on a GPU (other streams or host threads) race on it.
+// ---------------------------------------------------------------------------
+constexpr size_t kNoAllocComplex = (size_t)4 << 20;  // 4 Mi complex floats = 32 MiB per GPU
+static __device__ __align__(256) float2 g_noalloc_scratch[kNoAllocComplex];
+constexpr int kNoAllocMaxDevices = 64;
+static std::mutex g_noalloc_mtx;
+static float2* g_noalloc_addr[kNoAllocMaxDevices] = {};
+
+// Device address of the scratch array on the current device, looked up once
+// per device (cudaGetSymbolAddress with that device current).
+static int noalloc_scratch(float2** out)
+{
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return fail(WCT_ERR_CUDA, cudaGetErrorString(e));
+    if (dev < 0 || dev >= kNoAllocMaxDevices) return fail(WCT_ERR_ARG, "device ordinal out of range");
+    std::lock_guard<std::mutex> lk(g_noalloc_mtx);
+    if (!g_noalloc_addr[dev]) {
+        void* p = nullptr;
+        e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (e != cudaSuccess) return fail(WCT_ERR_CUDA, cudaGetErrorString(e));
+        g_noalloc_addr[dev] = static_cast<float2*>(p);
+    }
+    *out = g_noalloc_addr[dev];
+    return WCT_OK;
+}
+
 }  // namespace wctb200
 
 using namespace wctb200;
@@ -614,7 +656,7 @@ struct wct_pir {
 extern "C" {
 
 const char* wct_version(void) { return "wctb200 0.1 (sm_100a)"; }
-const char* wct_last_error(void) { return g_last_error.c_str(); }
+const char* wct_last_error(void) { return g_last_error; }
 
 int wct_pir_create(const wct_fr_plane* fr, int nshort, const int* short_len, const double* short_wave,
                    double overall_short_padding, double tick, int nticks, wct_pir** out)
@@ -695,6 +737,33 @@ int wct_convolve_rows_device(const float* in, long ld_in, int nrows, int n_in, c
     if (rc) return rc;
     if (e != cudaSuccess) return fail(WCT_ERR_CUDA, cudaGetErrorString(e));
     return WCT_OK;
+}
+
+int wct_convolve_rows_device_noalloc(const float* in, long ld_in, int nrows, int n_in, const float* resp,
+                                     int n_resp, int nfft, float* out, long ld_out, int n_out, void* stream)
+{
+    int rc = convolve_args(in, ld_in, nrows, n_in, resp, n_resp, nfft, out, ld_out, n_out);
+    if (rc) return rc;
+    const size_t M = (size_t)nfft / 2;
+    if ((3 + (size_t)nrows) * M > kNoAllocComplex)
+        return fail(WCT_ERR_SIZE,
+                    "convolve rows (no allocation): (nrows + 3) * nfft / 2 exceeds the fixed scratch of 4194304 "
+                    "complex values (32 MiB)");
+    if (nrows == 0 || n_out == 0) return WCT_OK;
+    float2* base = nullptr;
+    rc = noalloc_scratch(&base);
+    if (rc) return rc;
+    FftDesc d{};
+    if (!fft_radices((int)M, d.radix, d.nst)) return fail(WCT_ERR_SIZE, "convolve rows: unsupported FFT length");
+    d.M = (int)M;
+    float2* tw = base;
+    float2* twh = base + M;
+    d.tw = tw;
+    d.twh = twh;
+    cudaStream_t s = (cudaStream_t)stream;
+    launch_twiddles(tw, twh, (int)M, s);
+    return convolve_on(in, ld_in, nrows, n_in, resp, n_resp, nfft, out, ld_out, n_out, d, base + 3 * M, base + 2 * M,
+                       s);
 }
 
 int wct_dt_create(const char* json_config, wct_depotransform** out)
