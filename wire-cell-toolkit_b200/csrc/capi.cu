@@ -432,7 +432,7 @@ static int forward_device(Core& c, const double* d_depos, size_t ndepos, float* 
     CUDA_TRY(c.d_win.ensure(sizeof(WindowDev) * np));
     CUDA_TRY(c.d_wcnt.ensure(sizeof(int) * (nkeys + 1)));
     CUDA_TRY(c.d_woff.ensure(sizeof(int) * (nkeys + 1)));
-    CUDA_TRY(c.d_wcur.ensure(sizeof(int) * (nkeys + 1)));
+    CUDA_TRY(c.d_wcur.ensure(sizeof(int) * (nkeys + 1 + (nkeys + 1023) / 1024)));  // + scan block sums
     if (c.h_win_n < (size_t)np) {
         if (c.h_win) cudaFreeHost(c.h_win);
         CUDA_TRY(cudaMallocHost(&c.h_win, sizeof(WindowDev) * np + sizeof(int)));
@@ -449,7 +449,7 @@ static int forward_device(Core& c, const double* d_depos, size_t ndepos, float* 
                     c.d_rec.as<PatchRec>(), c.d_win.as<WindowDev>(), c.d_wcnt.as<int>(), c.d_tprof.as<float>(),
                     c.d_kbound.as<float>(), s);
     launch_scan(c.d_wcnt.as<int>(), nkeys, c.d_woff.as<int>(), c.d_wcur.as<int>(), s);
-    t_prep.close(2 + (n > 0 ? 1 : 0));
+    t_prep.close(4 + (n > 0 ? 1 : 0));
     CUDA_TRY(cudaGetLastError());
     CUDA_TRY(cudaMemcpyAsync(c.h_win, c.d_win.p, sizeof(WindowDev) * np, cudaMemcpyDeviceToHost, s));
     CUDA_TRY(cudaMemcpyAsync(h_total, c.d_woff.as<int>() + nkeys, sizeof(int), cudaMemcpyDeviceToHost, s));

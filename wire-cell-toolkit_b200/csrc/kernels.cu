@@ -361,36 +361,83 @@ void launch_prep_all(const double* depos, int n, const DriftDev& dd, int do_drif
                                                  wire_cnt, tprof, key_bound);
 }
 
-// Exclusive scan of the per-wire visit counts (one block).
-__global__ void __launch_bounds__(1024) k_scan(const int* __restrict__ cnt, int n, int* __restrict__ off,
-                                                int* __restrict__ cur)
+// Exclusive scan of the per-key visit counts: block sums, a scan of the
+// block sums, then per-block scans with their offsets.
+constexpr int kScanBlock = 1024;
+
+__device__ __forceinline__ int block_scan_excl(int v, int* s_warp, int& total)
 {
-    __shared__ int s[1024];
-    const int tid = threadIdx.x;
-    const int chunk = (n + 1023) / 1024;
-    const int b = tid * chunk, e = min(n, b + chunk);
-    int sum = 0;
-    for (int k = b; k < e; ++k) sum += cnt[k];
-    s[tid] = sum;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    int x = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+    }
+    if (lane == 31) s_warp[w] = x;
     __syncthreads();
-    for (int o = 1; o < 1024; o <<= 1) {
-        const int v = tid >= o ? s[tid - o] : 0;
-        __syncthreads();
-        s[tid] += v;
-        __syncthreads();
+    if (w == 0) {
+        int t = lane < (int)(blockDim.x >> 5) ? s_warp[lane] : 0;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int y = __shfl_up_sync(0xffffffffu, t, o);
+            if (lane >= o) t += y;
+        }
+        s_warp[lane] = t;
     }
-    int run = s[tid] - sum;
-    for (int k = b; k < e; ++k) {
-        off[k] = run;
-        cur[k] = run;
-        run += cnt[k];
+    __syncthreads();
+    total = s_warp[(blockDim.x >> 5) - 1];
+    const int before = w ? s_warp[w - 1] : 0;
+    __syncthreads();
+    return before + x - v;
+}
+
+__global__ void __launch_bounds__(kScanBlock) k_scan_sums(const int* __restrict__ cnt, int n, int* __restrict__ sums)
+{
+    __shared__ int s_warp[32];
+    const int i = blockIdx.x * kScanBlock + threadIdx.x;
+    int total = 0;
+    block_scan_excl(i < n ? cnt[i] : 0, s_warp, total);
+    if (threadIdx.x == 0) sums[blockIdx.x] = total;
+}
+
+__global__ void __launch_bounds__(kScanBlock) k_scan_top(int* __restrict__ sums, int nb, int* __restrict__ total_out)
+{
+    __shared__ int s_warp[32];
+    int carry = 0;
+    for (int b0 = 0; b0 < nb; b0 += kScanBlock) {
+        const int i = b0 + threadIdx.x;
+        int total = 0;
+        const int ex = block_scan_excl(i < nb ? sums[i] : 0, s_warp, total);
+        if (i < nb) sums[i] = carry + ex;
+        carry += total;
     }
-    if (tid == 1023) off[n] = s[1023];
+    if (threadIdx.x == 0) *total_out = carry;
+}
+
+__global__ void __launch_bounds__(kScanBlock) k_scan_apply(const int* __restrict__ cnt, int n,
+                                                           const int* __restrict__ sums, int* __restrict__ off,
+                                                           int* __restrict__ cur)
+{
+    __shared__ int s_warp[32];
+    const int i = blockIdx.x * kScanBlock + threadIdx.x;
+    int total = 0;
+    const int ex = block_scan_excl(i < n ? cnt[i] : 0, s_warp, total) + sums[blockIdx.x];
+    if (i < n) {
+        off[i] = ex;
+        cur[i] = ex;
+    }
 }
 
 void launch_scan(const int* wire_cnt, int nwires_total, int* wire_off, int* wire_cur, cudaStream_t s)
 {
-    k_scan<<<1, 1024, 0, s>>>(wire_cnt, nwires_total, wire_off, wire_cur);
+    // wire_cur[nwires_total + 1 ..] holds the block sums (the caller sizes it)
+    const int n = nwires_total;
+    const int nb = (n + kScanBlock - 1) / kScanBlock;
+    int* sums = wire_cur + n + 1;
+    k_scan_sums<<<nb, kScanBlock, 0, s>>>(wire_cnt, n, sums);
+    k_scan_top<<<1, kScanBlock, 0, s>>>(sums, nb, wire_off + n);
+    k_scan_apply<<<nb, kScanBlock, 0, s>>>(wire_cnt, n, sums, wire_off, wire_cur);
 }
 
 // Per-wire visit lists: wire_list[wire_off[w] ..] holds the depo indices whose
