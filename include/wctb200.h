@@ -195,6 +195,26 @@ int wct_dt_patch_records(const wct_depotransform* dt, int face, int plane, int* 
 int wct_dt_set_profiling(wct_depotransform* dt, int on);
 int wct_dt_stage_times(wct_depotransform* dt, double* ms, long* launches, int nstages, long* total_launches,
                        int reset);
+
+/* Reverse-mode derivative of wct_dt_forward (no counterpart in the reference,
+ * whose DepoTransform is forward only).  Given grad_frame = dL/d(frame)
+ * [nrows][nticks] for the same depos, writes grad_depos[i][k] = dL/d(depos[i][k])
+ * for k = t, q, x, y, z, extent_long, extent_tran, and, when grad_drift is not
+ * NULL, dL/d(DL, DT, lifetime) of the drifter (zeros without one).  Patch
+ * placement is recomputed from the depos, and patch windows, rejections and
+ * event windows are held fixed (they are the piecewise-constant part of the
+ * forward).  Outputs are overwritten. */
+int wct_dt_adjoint(wct_depotransform* dt, const double* depos, size_t ndepos, const float* grad_frame,
+                   double* grad_depos, double* grad_drift);
+/* The same on device buffers, enqueued on stream (NULL = the component's own
+ * stream); grad_drift is a device array of 3 doubles or NULL. */
+int wct_dt_adjoint_device(wct_depotransform* dt, const double* d_depos, size_t ndepos, const float* d_grad_frame,
+                          double* d_grad_depos, double* d_grad_drift, void* stream);
+/* Drifter parameters DL, DT (length^2/time) and electron lifetime of a
+ * component configured with a "drifter" (Drifter, gen/src/Drifter.cxx:62-71);
+ * WCT_ERR_STATE without one. */
+int wct_dt_set_drift_params(wct_depotransform* dt, double DL, double DT, double lifetime);
+int wct_dt_get_drift_params(const wct_depotransform* dt, double* DL, double* DT, double* lifetime);
 int wct_dt_destroy(wct_depotransform* dt);
 
 #ifdef __cplusplus

@@ -89,6 +89,12 @@ SIGNATURES = {
     "wct_dt_patch_records": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_size_t]),
     "wct_dt_set_profiling": (C.c_int, [C.c_void_p, C.c_int]),
     "wct_dt_stage_times": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.POINTER(C.c_long), C.c_int]),
+    "wct_dt_adjoint": (C.c_int, [C.c_void_p, C.c_void_p, C.c_size_t, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "wct_dt_adjoint_device": (C.c_int, [C.c_void_p, C.c_void_p, C.c_size_t, C.c_void_p, C.c_void_p, C.c_void_p,
+                                        C.c_void_p]),
+    "wct_dt_set_drift_params": (C.c_int, [C.c_void_p, C.c_double, C.c_double, C.c_double]),
+    "wct_dt_get_drift_params": (C.c_int, [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_double),
+                                          C.POINTER(C.c_double)]),
     "wct_dt_destroy": (C.c_int, [C.c_void_p]),
 }
 
@@ -259,6 +265,35 @@ class DepoTransform:
                                            C.c_void_p(stream) if stream else None))
         return [w.as_dict() for w in wins], ident.value
 
+    def adjoint(self, depos, grad_frame):
+        """Host-buffer adjoint: (dL/d depos [n][7] float64, dL/d (DL, DT, lifetime) [3]) for the
+        frame gradient ``grad_frame`` [nrows][nticks] of the same depos."""
+        d = np.ascontiguousarray(depos, dtype=np.float64).reshape(-1, 7)
+        g = np.ascontiguousarray(grad_frame, dtype=np.float32)
+        nrows, nticks = self.frame_shape()
+        assert g.shape == (nrows, nticks)
+        gd = np.zeros_like(d)
+        gg = np.zeros(3)
+        _check(lib().wct_dt_adjoint(self.h, d.ctypes.data if len(d) else None, len(d), g.ctypes.data,
+                                    gd.ctypes.data if len(d) else None, gg.ctypes.data))
+        return gd, gg
+
+    def adjoint_device(self, d_depos_ptr, ndepos, d_grad_frame_ptr, d_grad_depos_ptr, d_grad_drift_ptr=None,
+                       stream=None):
+        """Device-buffer adjoint (pointers as ints)."""
+        _check(lib().wct_dt_adjoint_device(self.h, C.c_void_p(d_depos_ptr), ndepos, C.c_void_p(d_grad_frame_ptr),
+                                           C.c_void_p(d_grad_depos_ptr),
+                                           C.c_void_p(d_grad_drift_ptr) if d_grad_drift_ptr else None,
+                                           C.c_void_p(stream) if stream else None))
+
+    def set_drift_params(self, DL, DT, lifetime):
+        _check(lib().wct_dt_set_drift_params(self.h, float(DL), float(DT), float(lifetime)))
+
+    def drift_params(self):
+        a, b, c = C.c_double(), C.c_double(), C.c_double()
+        _check(lib().wct_dt_get_drift_params(self.h, C.byref(a), C.byref(b), C.byref(c)))
+        return a.value, b.value, c.value
+
     def patch_records(self, face, plane, n):
         """[n][4] (toffset, poffset, nt, np) per input depo from the last forward call."""
         out = np.zeros((n, 4), dtype=np.int32)
@@ -334,3 +369,32 @@ def from_config(cfg, device=0):
                                   cfg["pir_nticks"])
         dt.set_response_pir(face, p, pir)
     return dt
+
+
+_ag = None
+
+
+def autograd():
+    """The libtorch autograd extension (_wct_autograd, built in-tree on first use)."""
+    global _ag
+    if _ag is None:
+        import importlib
+        import torch  # noqa: F401  (the extension links libtorch)
+        if _build.autograd_stale():
+            _build.build_autograd()
+        lib()
+        _ag = importlib.import_module(__name__ + "._wct_autograd")
+    return _ag
+
+
+def depo_transform(dt, depos, drift_params=None):
+    """Differentiable DepoTransform: the dense frame [nrows][nticks] (float32
+    torch tensor) of ``depos`` ([n][7] float64 CUDA tensor: t, q, x, y, z,
+    extent_long, extent_tran) through the configured component ``dt``, with
+    the drifter's (DL, DT, lifetime) taken from ``drift_params`` (float64 CPU
+    tensor of 3, may require grad) when given.  Backward goes through the
+    hand-written adjoint kernels (torch::autograd::Function in csrc/autograd.cpp)."""
+    import torch
+    if drift_params is None:
+        drift_params = torch.empty(0, dtype=torch.float64)
+    return autograd().depo_transform(depos, drift_params, dt.h.value)

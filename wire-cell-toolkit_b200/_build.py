@@ -6,16 +6,19 @@ import subprocess
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libwctb200.so")
-SOURCES = ["kernels.cu", "capi.cu", "pir.cpp"]
-HEADERS = ["common.cuh", "fft.cuh", "kernels.cuh", "json.hpp", "pir.hpp"]
+SOURCES = ["kernels.cu", "adjoint.cu", "capi.cu", "pir.cpp"]
+HEADERS = ["common.cuh", "fft.cuh", "gauss.cuh", "kernels.cuh", "json.hpp", "pir.hpp"]
 
 NVCC_FLAGS = [
     "-O3", "-std=c++17", "-lineinfo",
     "-gencode", "arch=compute_100a,code=sm_100a",
     "-Xcompiler", "-fPIC", "-Xcompiler", "-ffp-contract=off",
     "--expt-relaxed-constexpr",
-    "-shared",
+    "-shared", "-Xlinker", "-soname=libwctb200.so",
 ]
+
+AUTOGRAD_SRC = os.path.join(CSRC, "autograd.cpp")
+AUTOGRAD_NAME = "_wct_autograd"
 
 
 def nvcc():
@@ -45,5 +48,45 @@ def build(force=False, verbose=False):
     return LIB
 
 
+def autograd_path():
+    import sysconfig
+    return os.path.join(HERE, AUTOGRAD_NAME + sysconfig.get_config_var("EXT_SUFFIX"))
+
+
+def autograd_stale():
+    out = autograd_path()
+    if not os.path.exists(out):
+        return True
+    t = os.path.getmtime(out)
+    inc = os.path.join(os.path.dirname(HERE), "include", "wctb200.h")
+    return any(os.path.getmtime(d) > t for d in (AUTOGRAD_SRC, inc, __file__, LIB) if os.path.exists(d))
+
+
+def build_autograd(force=False, verbose=False):
+    """The libtorch autograd extension (host C++ only; links libwctb200.so)."""
+    out = autograd_path()
+    if not force and not autograd_stale():
+        return out
+    import sysconfig
+    import torch
+    from torch.utils import cpp_extension as ce
+    build(force=False)
+    incs = ce.include_paths(device_type="cuda")
+    libs = ce.library_paths(device_type="cuda")
+    abi = int(torch._C._GLIBCXX_USE_CXX11_ABI)
+    cmd = ["g++", "-O2", "-std=c++17", "-shared", "-fPIC", AUTOGRAD_SRC, "-o", out + ".tmp",
+           "-DTORCH_EXTENSION_NAME=" + AUTOGRAD_NAME, "-DTORCH_API_INCLUDE_EXTENSION_H",
+           "-D_GLIBCXX_USE_CXX11_ABI=%d" % abi, "-I" + sysconfig.get_paths()["include"]]
+    cmd += ["-I" + i for i in incs] + ["-L" + l for l in libs]
+    cmd += ["-L" + HERE, "-lwctb200", "-lc10", "-lc10_cuda", "-ltorch", "-ltorch_cpu", "-ltorch_cuda",
+            "-ltorch_python", "-Wl,-rpath,$ORIGIN"] + ["-Wl,-rpath," + l for l in libs]
+    if verbose:
+        print(" ".join(cmd))
+    subprocess.run(cmd, check=True, cwd=CSRC)
+    os.replace(out + ".tmp", out)
+    return out
+
+
 if __name__ == "__main__":
     build(force=True, verbose=True)
+    build_autograd(force=True, verbose=True)

@@ -175,6 +175,7 @@ struct Core {
     std::map<int, std::unique_ptr<FftPlanDev>> plans;
     // workspace
     DevBuf d_rec, d_win, d_Q, d_V, d_depos, d_frame, d_wcnt, d_woff, d_wcur, d_wlist, d_tprof, d_kbound;
+    DevBuf d_gframe, d_gdep, d_gglob;  // adjoint host entry point
     WindowDev* h_win{nullptr};
     size_t last_n{0};
     // stage profiling
@@ -397,8 +398,19 @@ __global__ void k_win_init(WindowDev* w, int n)
     w[i].nadded = w[i].out_time = w[i].out_pitch = w[i].oversize = 0;
 }
 
-static int forward_device(Core& c, const double* d_depos, size_t ndepos, float* d_frame, wct_plane_window* wins,
-                          int* frame_ident, cudaStream_t s)
+// Drift, patch records, per-plane windows and charge-grid layout of one event:
+// the part of the forward that the adjoint recomputes (patches are never
+// stored between the two).
+struct EventPlan {
+    int n{0}, np{0}, nticks{0};
+    TimeDev tb{};
+    PlaneSet pset{};
+    GridSet gset{};
+    std::vector<PlaneWindow> pw;
+    int total_visits{0};
+};
+
+static int prepare_event(Core& c, const double* d_depos, size_t ndepos, cudaStream_t s, EventPlan& ev)
 {
     if (c.planes.empty()) return fail(WCT_ERR_STATE, "no planes configured");
     if ((int)c.planes.size() > kMaxPlanes) return fail(WCT_ERR_CONFIG, "too many planes for one component");
@@ -409,13 +421,17 @@ static int forward_device(Core& c, const double* d_depos, size_t ndepos, float* 
     const int n = (int)ndepos;
     const int np = (int)c.planes.size();
     const int nticks = c.nticks();
-    TimeDev tb;
+    ev.n = n;
+    ev.np = np;
+    ev.nticks = nticks;
+    TimeDev& tb = ev.tb;
     tb.nbins = nticks;
     tb.tmin = c.start_time;
     tb.tmax = c.start_time + c.readout_time;
     tb.bs = (tb.tmax - tb.tmin) / tb.nbins;
 
-    PlaneSet pset{};
+    PlaneSet& pset = ev.pset;
+    pset = PlaneSet{};
     pset.nplanes = np;
     int nwt = 0;
     for (int ip = 0; ip < np; ++ip) {
@@ -456,10 +472,12 @@ static int forward_device(Core& c, const double* d_depos, size_t ndepos, float* 
     CUDA_TRY(cudaStreamSynchronize(s));
     for (int ip = 0; ip < np; ++ip)
         if (c.h_win[ip].oversize) return fail(WCT_ERR_SIZE, "a diffusion patch exceeds 1024 ticks or 1024 impact bins");
-    const int total_visits = *h_total;
+    ev.total_visits = *h_total;
 
-    std::vector<PlaneWindow> pw(np);
-    GridSet gset{};
+    std::vector<PlaneWindow>& pw = ev.pw;
+    pw.assign(np, PlaneWindow{});
+    GridSet& gset = ev.gset;
+    gset = GridSet{};
     gset.nplanes = np;
     gset.ntiles_abs = pset.ntiles;
     size_t qfloats = 0, vbytes = 0, smem = 0;
@@ -501,6 +519,19 @@ static int forward_device(Core& c, const double* d_depos, size_t ndepos, float* 
     if (qfloats >= (size_t)1 << 40) return fail(WCT_ERR_SIZE, "charge grid too large");
     CUDA_TRY(c.d_Q.ensure(sizeof(float) * std::max<size_t>(qfloats, 1)));
     CUDA_TRY(c.d_V.ensure(std::max<size_t>(vbytes, 1)));
+    return WCT_OK;
+}
+
+static int forward_device(Core& c, const double* d_depos, size_t ndepos, float* d_frame, wct_plane_window* wins,
+                          int* frame_ident, cudaStream_t s)
+{
+    EventPlan ev;
+    int prc = prepare_event(c, d_depos, ndepos, s, ev);
+    if (prc) return prc;
+    const int n = ev.n, np = ev.np, nticks = ev.nticks, total_visits = ev.total_visits, rows = ev.gset.nrows_total;
+    const PlaneSet& pset = ev.pset;
+    const GridSet& gset = ev.gset;
+    const std::vector<PlaneWindow>& pw = ev.pw;
     CUDA_TRY(c.d_wlist.ensure(sizeof(Visit) * std::max(total_visits, 1)));
     CUDA_TRY(cudaMemsetAsync(d_frame, 0, sizeof(float) * (size_t)c.nrows() * nticks, s));
 
@@ -557,6 +588,66 @@ static int forward_device(Core& c, const double* d_depos, size_t ndepos, float* 
     if (frame_ident) *frame_ident = c.frame_count;
     ++c.frame_count;
     c.last_n = ndepos;
+    return WCT_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Adjoint: dL/d(depos) and dL/d(DL, DT, lifetime) from dL/d(frame).
+// Patch records and windows are recomputed (prepare_event), then per plane
+// the frame gradient is correlated with the responses (the transpose of the
+// FFT convolution) into dL/dQ, which the gather kernel reduces per depo.
+// ---------------------------------------------------------------------------
+static int adjoint_device(Core& c, const double* d_depos, size_t ndepos, const float* d_gframe, double* d_gdep,
+                          double* d_gglob, cudaStream_t s)
+{
+    EventPlan ev;
+    int prc = prepare_event(c, d_depos, ndepos, s, ev);
+    if (prc) return prc;
+    const int n = ev.n, np = ev.np, nticks = ev.nticks;
+    if (n) CUDA_TRY(cudaMemsetAsync(d_gdep, 0, sizeof(double) * 7 * (size_t)n, s));
+    if (d_gglob) CUDA_TRY(cudaMemsetAsync(d_gglob, 0, sizeof(double) * 3, s));
+    CUDA_TRY(c.d_gglob.ensure(sizeof(double) * 3));
+    double* gg = d_gglob ? d_gglob : c.d_gglob.as<double>();
+    if (!d_gglob) CUDA_TRY(cudaMemsetAsync(gg, 0, sizeof(double) * 3, s));
+    AdjSet as{};
+    as.nplanes = np;
+    for (int ip = 0; ip < np; ++ip) {
+        PlaneState& ps = *c.planes[ip];
+        const PlaneWindow& w = ev.pw[ip];
+        const GridPlane& g = ev.gset.p[ip];
+        AdjPlane& a = as.p[ip];
+        a.nimp = g.nimp;
+        a.nin = g.nin;
+        a.N = g.N;
+        a.start_ch = g.start_ch;
+        a.col0 = g.col0;
+        a.qoff = g.qoff;
+        a.pbs = g.pbs;
+        a.tbs = g.tbs;
+        a.ax = ps.dev.ax;
+        a.ay = ps.dev.ay;
+        a.az = ps.dev.az;
+        if (g.nin == 0) continue;
+        const int nin = g.nin, nout = nin + 2 * ps.npad, N = g.N, M = N / 2;
+        FftDesc d;
+        int rc = c.plan_for(M, d);
+        if (rc) return rc;
+        float* Gr = c.d_V.as<float>();  // [nout][N] real, then [nout][M] spectra in place
+        const int wlo = std::max(0, w.m_start_ch), whi = std::min(ps.desc.nwires, w.m_end_ch);
+        launch_grad_rows(d_gframe + (size_t)ps.row0 * nticks, nticks, w.start_ch - ps.npad, wlo, whi, w.start_tick,
+                         std::min(N, w.nt_ref), nout, N, Gr, s);
+        launch_rfft_rows(Gr, N, N, reinterpret_cast<float2*>(Gr), M, nout, d, s);
+        float* dQ = c.d_Q.as<float>() + g.qoff;
+        launch_wire_conv_adj(reinterpret_cast<const float2*>(Gr), ps.d_spec.as<float2>(),
+                             reinterpret_cast<float2*>(dQ), ps.G, ps.npad, nin, nout, M, s);
+        launch_irfft_rows(reinterpret_cast<const float2*>(dQ), ps.G * nin, d, 0, 0, ps.G * nin, 0, N, N, dQ, s);
+        c.total_launches += 4;
+        CUDA_TRY(cudaGetLastError());
+    }
+    launch_adj_gather(d_depos, n, c.drifter, c.have_drifter ? 1 : 0, ev.pset, as, c.drift_speed,
+                      c.d_rec.as<PatchRec>(), c.d_Q.as<float>(), d_gdep, gg, s);
+    if (n) c.total_launches += 1;
+    CUDA_TRY(cudaGetLastError());
     return WCT_OK;
 }
 
@@ -966,6 +1057,71 @@ int wct_dt_forward(wct_depotransform* h, const double* depos, size_t ndepos, flo
     if (rc) return rc;
     CUDA_TRY(cudaMemcpyAsync(frame, c.d_frame.p, fbytes, cudaMemcpyDeviceToHost, s));
     CUDA_TRY(cudaStreamSynchronize(s));
+    return WCT_OK;
+}
+
+int wct_dt_adjoint_device(wct_depotransform* h, const double* d_depos, size_t ndepos, const float* d_grad_frame,
+                          double* d_grad_depos, double* d_grad_drift, void* stream)
+{
+    if (!h || !d_grad_frame || (ndepos && (!d_depos || !d_grad_depos)))
+        return fail(WCT_ERR_ARG, "wct_dt_adjoint_device: bad arguments");
+    std::lock_guard<std::mutex> lk(h->core.mtx);
+    cudaStream_t s = stream ? (cudaStream_t)stream : h->core.own_stream;
+    return adjoint_device(h->core, d_depos, ndepos, d_grad_frame, d_grad_depos, d_grad_drift, s);
+}
+
+int wct_dt_adjoint(wct_depotransform* h, const double* depos, size_t ndepos, const float* grad_frame,
+                   double* grad_depos, double* grad_drift)
+{
+    if (!h || !grad_frame || (ndepos && (!depos || !grad_depos)))
+        return fail(WCT_ERR_ARG, "wct_dt_adjoint: bad arguments");
+    std::lock_guard<std::mutex> lk(h->core.mtx);
+    Core& c = h->core;
+    CUDA_TRY(cudaSetDevice(c.device));
+    cudaStream_t s = c.own_stream;
+    const size_t fbytes = sizeof(float) * (size_t)c.nrows() * c.nticks();
+    const size_t dbytes = sizeof(double) * 7 * std::max<size_t>(ndepos, 1);
+    CUDA_TRY(c.d_depos.ensure(dbytes));
+    CUDA_TRY(c.d_gdep.ensure(dbytes));
+    CUDA_TRY(c.d_gframe.ensure(fbytes));
+    CUDA_TRY(c.d_gglob.ensure(sizeof(double) * 3));
+    if (ndepos)
+        CUDA_TRY(cudaMemcpyAsync(c.d_depos.p, depos, sizeof(double) * 7 * ndepos, cudaMemcpyHostToDevice, s));
+    CUDA_TRY(cudaMemcpyAsync(c.d_gframe.p, grad_frame, fbytes, cudaMemcpyHostToDevice, s));
+    int rc = adjoint_device(c, c.d_depos.as<double>(), ndepos, c.d_gframe.as<float>(), c.d_gdep.as<double>(),
+                            c.d_gglob.as<double>(), s);
+    if (rc) return rc;
+    if (ndepos)
+        CUDA_TRY(cudaMemcpyAsync(grad_depos, c.d_gdep.p, sizeof(double) * 7 * ndepos, cudaMemcpyDeviceToHost, s));
+    double gg[3];
+    CUDA_TRY(cudaMemcpyAsync(gg, c.d_gglob.p, sizeof gg, cudaMemcpyDeviceToHost, s));
+    CUDA_TRY(cudaStreamSynchronize(s));
+    if (grad_drift) std::memcpy(grad_drift, gg, sizeof gg);
+    return WCT_OK;
+}
+
+int wct_dt_set_drift_params(wct_depotransform* h, double DL, double DT, double lifetime)
+{
+    if (!h) return fail(WCT_ERR_ARG, "null component");
+    std::lock_guard<std::mutex> lk(h->core.mtx);
+    Core& c = h->core;
+    if (!c.have_drifter) return fail(WCT_ERR_STATE, "no drifter configured");
+    if (!(DL >= 0) || !(DT >= 0) || !(lifetime > 0))
+        return fail(WCT_ERR_ARG, "DL and DT must be non-negative and lifetime positive");
+    c.drifter.DL = DL;
+    c.drifter.DT = DT;
+    c.drifter.lifetime = lifetime;
+    return WCT_OK;
+}
+
+int wct_dt_get_drift_params(const wct_depotransform* h, double* DL, double* DT, double* lifetime)
+{
+    if (!h) return fail(WCT_ERR_ARG, "null component");
+    const Core& c = h->core;
+    if (!c.have_drifter) return fail(WCT_ERR_STATE, "no drifter configured");
+    if (DL) *DL = c.drifter.DL;
+    if (DT) *DT = c.drifter.DT;
+    if (lifetime) *lifetime = c.drifter.lifetime;
     return WCT_OK;
 }
 

@@ -102,6 +102,19 @@ struct GridSet {
     GridPlane p[kMaxPlanes];
 };
 
+// Per-plane parameters of the adjoint's gather (adjoint.cu).
+struct AdjPlane {
+    int nimp, nin, N, start_ch, col0;
+    long long qoff;           // offset of the plane's dL/dQ grid [G][nin][N] in floats
+    float pbs, tbs;
+    double ax, ay, az;        // unit pitch axis
+};
+
+struct AdjSet {
+    int nplanes;
+    AdjPlane p[kMaxPlanes];
+};
+
 // ---- launchers (kernels.cu) ----
 void launch_prep_all(const double* depos, int n, const DriftDev& dd, int do_drift, const PlaneSet& ps,
                      const TimeDev& tb, double drift_speed, double nsigma, PatchRec* rec, WindowDev* win,
@@ -120,5 +133,14 @@ void launch_irfft_rows(const float2* Vh, int nrows, const FftDesc& d, int wire0,
 
 void launch_spec_mul(float2* X, long ldx, int nrows, int M, const float2* R, cudaStream_t s);
 void launch_twiddles(float2* tw, float2* twh, int M, cudaStream_t s);
+
+// ---- adjoint launchers (adjoint.cu) ----
+void launch_grad_rows(const float* gframe, int nticks, int wire0, int wlo, int whi, int tick0, int ncols, int nrows,
+                      int N, float* out, cudaStream_t s);
+void launch_wire_conv_adj(const float2* Gh, const float2* Rh, float2* dQh, int G, int npad, int nin, int nout, int M,
+                          cudaStream_t s);
+void launch_adj_gather(const double* depos, int n, const DriftDev& dd, int do_drift, const PlaneSet& ps,
+                       const AdjSet& as, double drift_speed, const PatchRec* rec, const float* dQ, double* grad,
+                       double* gglob, cudaStream_t s);
 
 }  // namespace wctb200
