@@ -191,7 +191,9 @@ int wct_dt_patch_records(const wct_depotransform* dt, int face, int plane, int* 
  * events around its stages on the launch stream.  wct_dt_stage_times
  * returns, per stage, the accumulated milliseconds and launch count since the
  * last reset (stages: 0 drift+prep, 1 raster, 2 time FFT, 3 wire convolution,
- * 4 inverse FFT + frame, 5 other), and the total number of kernel launches. */
+ * 4 inverse FFT + frame, 5 other; adjoint calls add 6 frame-gradient time FFT,
+ * 7 transposed wire convolution, 8 inverse FFT to dL/dQ, 9 per-depo gather),
+ * and the total number of kernel launches. */
 int wct_dt_set_profiling(wct_depotransform* dt, int on);
 int wct_dt_stage_times(wct_depotransform* dt, double* ms, long* launches, int nstages, long* total_launches,
                        int reset);

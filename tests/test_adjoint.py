@@ -261,10 +261,10 @@ def test_autograd_function_matches_adjoint(wct, synth):
     loss = ((frame - Tt) ** 2).sum()
     loss.backward()
     F, _, _ = dt(d)
-    assert np.array_equal(frame.detach().cpu().numpy(), F)
+    assert np.array_equal(frame.detach().cpu().numpy(), F)  # the forward is bit-reproducible
     gd, gg = dt.adjoint(d, 2.0 * (F - T))
-    assert rel_l2(depos.grad.cpu().numpy(), gd) < 1e-12
-    assert rel_l2(dp.grad.numpy(), gg) < 1e-12
+    assert np.array_equal(depos.grad.cpu().numpy(), gd)     # so is the per-depo gradient
+    assert rel_l2(dp.grad.numpy(), gg) < 1e-12              # global sums: atomics in any order
     # the drift parameters passed in are the ones the forward used
     frame2 = wct.depo_transform(dt, depos.detach(), torch.tensor(_target_glob(glob)))
     assert np.array_equal(frame2.cpu().numpy(), T)

@@ -87,7 +87,8 @@ def test_frame_ident_and_determinism(wct, synth):
     f2, w2, i2 = dt(d)
     assert (i1, i2) == (7, 8)
     assert w1 == w2
-    assert rel_l2(f1, f2) < 1e-6
+    # integer accumulation (charge grid and its fixed-point bounds): bit-reproducible
+    assert np.array_equal(f1, f2)
 
 
 def test_empty_and_rejected_inputs(wct, oracle, synth):

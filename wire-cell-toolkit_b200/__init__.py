@@ -98,7 +98,8 @@ SIGNATURES = {
     "wct_dt_destroy": (C.c_int, [C.c_void_p]),
 }
 
-STAGES = ("drift+prep", "raster", "time_fft", "wire_conv", "inverse_fft+frame", "other")
+STAGES = ("drift+prep", "raster", "time_fft", "wire_conv", "inverse_fft+frame", "other",
+          "adj_time_fft", "adj_wire_conv", "adj_inverse_fft", "adj_gather")
 
 
 def build(force=False):
@@ -117,6 +118,18 @@ def lib():
             f.restype = rt
             f.argtypes = at
     return _lib
+
+
+CUDA_STREAM_LEGACY = 1  # cudaStreamLegacy
+
+
+def _dt_stream(stream):
+    """Stream argument of the component's device entry points: None selects the
+    component's own stream; 0 (the handle of torch's default stream) is passed
+    as the legacy default stream, since the C ABI reads NULL as the former."""
+    if stream is None:
+        return None
+    return C.c_void_p(stream if stream else CUDA_STREAM_LEGACY)
 
 
 def _check(rc):
@@ -262,7 +275,7 @@ class DepoTransform:
         ident = C.c_int()
         _check(lib().wct_dt_forward_device(self.h, C.c_void_p(d_depos_ptr), ndepos, C.c_void_p(d_frame_ptr),
                                            C.cast(wins, C.c_void_p), C.byref(ident),
-                                           C.c_void_p(stream) if stream else None))
+                                           _dt_stream(stream)))
         return [w.as_dict() for w in wins], ident.value
 
     def adjoint(self, depos, grad_frame):
@@ -284,7 +297,7 @@ class DepoTransform:
         _check(lib().wct_dt_adjoint_device(self.h, C.c_void_p(d_depos_ptr), ndepos, C.c_void_p(d_grad_frame_ptr),
                                            C.c_void_p(d_grad_depos_ptr),
                                            C.c_void_p(d_grad_drift_ptr) if d_grad_drift_ptr else None,
-                                           C.c_void_p(stream) if stream else None))
+                                           _dt_stream(stream)))
 
     def set_drift_params(self, DL, DT, lifetime):
         _check(lib().wct_dt_set_drift_params(self.h, float(DL), float(DT), float(lifetime)))
@@ -305,11 +318,12 @@ class DepoTransform:
 
     def stage_times(self, reset=True):
         """{stage: (ms, launches)} accumulated since the last reset, and the total launch count."""
-        ms = np.zeros(6)
-        nl = np.zeros(6, dtype=np.int64)
+        ms = np.zeros(len(STAGES))
+        nl = np.zeros(len(STAGES), dtype=np.int64)
         tot = C.c_long()
-        _check(lib().wct_dt_stage_times(self.h, ms.ctypes.data, nl.ctypes.data, 6, C.byref(tot), 1 if reset else 0))
-        return {STAGES[i]: (float(ms[i]), int(nl[i])) for i in range(6)}, tot.value
+        _check(lib().wct_dt_stage_times(self.h, ms.ctypes.data, nl.ctypes.data, len(STAGES), C.byref(tot),
+                                        1 if reset else 0))
+        return {STAGES[i]: (float(ms[i]), int(nl[i])) for i in range(len(STAGES))}, tot.value
 
     def eos(self):
         return lib().wct_dt_eos(self.h)

@@ -121,9 +121,10 @@ void launch_wire_conv_adj(const float2* Gh, const float2* Rh, float2* dQh, int G
 }
 
 // ---------------------------------------------------------------------------
-// Per (plane, depo): gather the patch cells of dL/dQ and form the gradients.
-// One warp per depo-plane: lanes over ticks, a loop over the impact bins,
-// which are tabulated in shared memory in chunks of kGatherChunk bins.
+// Per depo: gather the patch cells of dL/dQ on every plane and form the
+// gradients.  One warp per depo; the patch is tabulated in shared memory in
+// chunks (impact bins x ticks) and the chunk's cells are spread over the 32
+// lanes, so every lane is busy whatever the patch shape.
 //
 // With x_k = edge_k - c (c the pitch centre, k = 0..np), u_k = x_k / s,
 // phi the unit normal density and bs the impact bin size:
@@ -135,10 +136,21 @@ void launch_wire_conv_adj(const float2* Gh, const float2* Rh, float2* dQh, int G
 //   da/ds    = [phi_{k+1} - phi_k + (u^2 phi)_{k+1} - (u^2 phi)_k + x_{k+1} dp/ds] / bs
 // and the same bin integrals and derivatives in time.  The patch adds
 // qn t_tau a_k to group l and qn t_tau (p_k - a_k) to group l + 1 of its wire,
-// qn = q / (sum_k p_k * sum_tau t_tau) (sums over the clipped patch).
+// qn = q / (sum_k p_k * sum_tau t_tau) (sums over the clipped patch).  Every
+// accumulated quantity is a sum over cells (k, tau) of a bin factor times a
+// tick factor times dL/dQ, e.g. dL/dqn = sum tv_tau (a_k D0 + (p_k - a_k) D1).
 // ---------------------------------------------------------------------------
 constexpr int kGatherWarps = 4;
-constexpr int kGatherChunk = 256;  // impact bins tabulated at once
+constexpr int kChunkP = 128;  // impact bins per table chunk
+constexpr int kChunkT = 128;  // ticks per table chunk
+constexpr int kUnroll = 4;    // cells per lane with loads in flight together
+
+struct __align__(16) BinTab {
+    float a, p, dadc, dpdc;
+    float dads, dpds;
+    int base;  // offset of (group l, charge row) of this bin in the plane grid, plus the patch's first column
+    int pad;
+};
 
 __device__ __forceinline__ double warp_sum_d(double v)
 {
@@ -147,8 +159,8 @@ __device__ __forceinline__ double warp_sum_d(double v)
     return v;
 }
 
-// Derivatives of the unit bin integral between edges at distances x1 < x2
-// from the centre, for sigma s > 0: returns p; dc, ds receive dp/dc, dp/ds.
+// Unit bin integral between edges at distances x1 < x2 from the centre
+// (sigma s > 0, inv = 1 / (sqrt(2) s)) and its derivatives in centre and sigma.
 __device__ __forceinline__ float bin_and_derivs(float x1, float x2, float s, float inv, float& dc, float& ds)
 {
     const float u1 = x1 / s, u2 = x2 / s;
@@ -159,26 +171,25 @@ __device__ __forceinline__ float bin_and_derivs(float x1, float x2, float s, flo
     return bin_from_edges(e1, e2);
 }
 
-__global__ void __launch_bounds__(kGatherWarps * 32) k_adj_gather(const double* __restrict__ dep, int n, DriftDev dd,
-                                                                  int do_drift, PlaneSet ps, AdjSet as,
-                                                                  double drift_speed,
+__global__ void __launch_bounds__(kGatherWarps * 32, 5) k_adj_gather(int n, PlaneSet ps, AdjSet as, double drift_speed,
                                                                   const PatchRec* __restrict__ rec,
                                                                   const float* __restrict__ dQ,
-                                                                  double* __restrict__ grad,
-                                                                  double* __restrict__ gglob)
+                                                                  double* __restrict__ grad)
 {
-    __shared__ float s_bin[kGatherWarps][kGatherChunk][6];  // a, p, da/dc, dp/dc, da/ds, dp/ds
-    __shared__ double s_glob[kGatherWarps][3];
+    __shared__ BinTab s_p[kGatherWarps][kChunkP];
+    __shared__ float4 s_t[kGatherWarps][kChunkT];
     const int wib = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const long long gw = (long long)blockIdx.x * kGatherWarps + wib;
-    const long long total = (long long)ps.nplanes * n;
-    double gDL = 0.0, gDT = 0.0, gTau = 0.0;
-    if (gw < total) {
-        const int ip = (int)(gw / n), i = (int)(gw - (long long)ip * n);
-        const PatchRec r = rec[(size_t)ip * n + i];
-        const AdjPlane& A = as.p[ip];
-        const int np = r.np, nt = r.nt;
-        if (np > 0 && nt > 0 && A.nin > 0) {
+    const int i = blockIdx.x * kGatherWarps + wib;
+    if (i < n) {
+        // per-depo sums over planes: dL/dt', dL/dq', dL/dsL, dL/dsT, dL/d(x', y, z) through the pitch
+        double s_ct = 0.0, s_qf = 0.0, s_sL = 0.0, s_sT = 0.0, s_px = 0.0, s_py = 0.0, s_pz = 0.0;
+        bool any = false;
+        for (int ip = 0; ip < ps.nplanes; ++ip) {
+            const PatchRec r = rec[(size_t)ip * n + i];
+            const AdjPlane& A = as.p[ip];
+            const int np = r.np, nt = r.nt;
+            if (np == 0 || nt == 0 || A.nin == 0) continue;
+            any = true;
             const float pbs = A.pbs, tbs = A.tbs;
             const float sp = r.sp, st = r.st;
             const float invp = sp > 0.f ? 1.0f / (1.41421356237309505f * sp) : 0.f;
@@ -189,76 +200,90 @@ __global__ void __launch_bounds__(kGatherWarps * 32) k_adj_gather(const double* 
             float St = 1.f, dSt_c = 0.f, dSt_s = 0.f;
             if (st > 0.f) St = bin_and_derivs(-r.tcr, (float)nt * tbs - r.tcr, st, invt, dSt_c, dSt_s);
             double acc_qn = 0.0, acc_cp = 0.0, acc_sp = 0.0, acc_ct = 0.0, acc_st = 0.0;
-            const int nimp = A.nimp;
             const size_t gstride = (size_t)A.nin * A.N;
-            for (int k0 = 0; k0 < np; k0 += kGatherChunk) {
-                const int nk = min(kGatherChunk, np - k0);
+            const float* dQp = dQ + A.qoff;
+            const int col = r.toff - A.col0;
+            for (int t0 = 0; t0 < nt; t0 += kChunkT) {
+                const int ntc = min(kChunkT, nt - t0);
                 __syncwarp();
-                for (int kk = lane; kk < nk; kk += 32) {
-                    const int k = k0 + kk;
-                    float a, p, dadc, dpdc, dads, dpds;
-                    if (sp > 0.f) {
-                        const float x1 = (float)k * pbs - r.pcr, x2 = (float)(k + 1) * pbs - r.pcr;
-                        p = bin_and_derivs(x1, x2, sp, invp, dpdc, dpds);
-                        const float u1 = x1 / sp, u2 = x2 / sp;
-                        const float f1 = norm_pdf(u1), f2 = norm_pdf(u2);
-                        a = (sp * (f2 - f1) + x2 * p) / pbs;
-                        dadc = ((u2 * f2 - u1 * f1) - p + x2 * dpdc) / pbs;
-                        dads = ((f2 - f1) + (u2 * u2 * f2 - u1 * u1 * f1) + x2 * dpds) / pbs;
-                    }
-                    else {  // point in pitch: one bin, weight (edge_{k+1} - c) / bs
-                        p = 1.f;
-                        a = (pbs - r.pcr) / pbs;
-                        dpdc = dpds = dads = 0.f;
-                        dadc = -1.0f / pbs;
-                    }
-                    float* sb = s_bin[wib][kk];
-                    sb[0] = a;
-                    sb[1] = p;
-                    sb[2] = dadc;
-                    sb[3] = dpdc;
-                    sb[4] = dads;
-                    sb[5] = dpds;
+                for (int tt = lane; tt < ntc; tt += 32) {
+                    const int tau = t0 + tt;
+                    float tv = 1.f, dtc = 0.f, dts = 0.f;
+                    if (st > 0.f)
+                        tv = bin_and_derivs((float)tau * tbs - r.tcr, (float)(tau + 1) * tbs - r.tcr, st, invt, dtc,
+                                            dts);
+                    s_t[wib][tt] = make_float4(tv, dtc, dts, 0.f);
                 }
-                __syncwarp();
-                for (int tc = 0; tc < nt; tc += 32) {
-                    const int tau = tc + lane;
-                    const bool on = tau < nt;
-                    float tv = 0.f, dtc = 0.f, dts = 0.f;
-                    if (on) {
-                        if (st > 0.f)
-                            tv = bin_and_derivs((float)tau * tbs - r.tcr, (float)(tau + 1) * tbs - r.tcr, st, invt, dtc,
-                                                dts);
-                        else tv = 1.f;
-                    }
-                    float U = 0.f, ac = 0.f, as_ = 0.f;
-                    const int col = r.toff + tau - A.col0;
-                    int kabs = r.poff + k0;
-                    int wire = kabs / nimp;
-                    int l = kabs - wire * nimp;
-                    for (int kk = 0; kk < nk; ++kk) {
-                        float D0 = 0.f, D1 = 0.f;
-                        if (on) {
-                            const float* b0 = dQ + A.qoff + ((size_t)l * A.nin + (wire - A.start_ch)) * A.N + col;
-                            D0 = __ldg(b0);
-                            D1 = __ldg(b0 + gstride);
+                for (int k0 = 0; k0 < np; k0 += kChunkP) {
+                    const int nk = min(kChunkP, np - k0);
+                    __syncwarp();
+                    for (int kk = lane; kk < nk; kk += 32) {
+                        const int k = k0 + kk;
+                        BinTab b;
+                        if (sp > 0.f) {
+                            const float x1 = (float)k * pbs - r.pcr, x2 = (float)(k + 1) * pbs - r.pcr;
+                            b.p = bin_and_derivs(x1, x2, sp, invp, b.dpdc, b.dpds);
+                            const float u1 = x1 / sp, u2 = x2 / sp;
+                            const float f1 = norm_pdf(u1), f2 = norm_pdf(u2);
+                            b.a = (sp * (f2 - f1) + x2 * b.p) / pbs;
+                            b.dadc = ((u2 * f2 - u1 * f1) - b.p + x2 * b.dpdc) / pbs;
+                            b.dads = ((f2 - f1) + (u2 * u2 * f2 - u1 * u1 * f1) + x2 * b.dpds) / pbs;
                         }
-                        const float* sb = s_bin[wib][kk];
-                        const float a = sb[0], p = sb[1];
-                        const float dd0 = D0 - D1;
-                        U = fmaf(a, dd0, fmaf(p, D1, U));
-                        ac = fmaf(dd0, sb[2], fmaf(D1, sb[3], ac));
-                        as_ = fmaf(dd0, sb[4], fmaf(D1, sb[5], as_));
-                        if (++l == nimp) {
-                            l = 0;
-                            ++wire;
+                        else {  // point in pitch: one bin, weight (edge_{k+1} - c) / bs
+                            b.p = 1.f;
+                            b.a = (pbs - r.pcr) / pbs;
+                            b.dpdc = b.dpds = b.dads = 0.f;
+                            b.dadc = -1.0f / pbs;
+                        }
+                        const int kabs = r.poff + k;
+                        const int wire = kabs / A.nimp;
+                        const int l = kabs - wire * A.nimp;
+                        b.base = (l * A.nin + (wire - A.start_ch)) * A.N + col + t0;
+                        b.pad = 0;
+                        s_p[wib][kk] = b;
+                    }
+                    __syncwarp();
+                    // cells c = lane + 32 m of the nk x ntc chunk, (k, tau) advanced
+                    // incrementally; kUnroll cells per lane have their loads in flight at once
+                    const int ncell = nk * ntc;
+                    const int dk = 32 / ntc, dt = 32 - dk * ntc;
+                    int k = lane / ntc, tau = lane - k * ntc;
+                    for (int c0 = 0; c0 < ncell; c0 += 32 * kUnroll) {
+                        float D0[kUnroll], D1[kUnroll];
+                        int kk[kUnroll], tt[kUnroll];
+#pragma unroll
+                        for (int u = 0; u < kUnroll; ++u) {
+                            kk[u] = k;
+                            tt[u] = tau;
+                            D0[u] = D1[u] = 0.f;
+                            if (c0 + lane + 32 * u < ncell) {
+                                const float* q = dQp + s_p[wib][k].base + tau;
+                                D0[u] = __ldg(q);
+                                D1[u] = __ldg(q + gstride);
+                            }
+                            tau += dt;
+                            k += dk;
+                            if (tau >= ntc) {
+                                tau -= ntc;
+                                ++k;
+                            }
+                        }
+#pragma unroll
+                        for (int u = 0; u < kUnroll; ++u) {
+                            // cells past the end loaded zeros: they add nothing (kk, tt stay in the tables)
+                            const BinTab b = s_p[wib][min(kk[u], nk - 1)];
+                            const float4 tq = s_t[wib][tt[u]];  // tt < ntc always
+                            const float dd0 = D0[u] - D1[u];
+                            const float uu = fmaf(b.a, dd0, b.p * D1[u]);
+                            const float vc = fmaf(b.dadc, dd0, b.dpdc * D1[u]);
+                            const float vs = fmaf(b.dads, dd0, b.dpds * D1[u]);
+                            acc_qn = fma((double)tq.x, (double)uu, acc_qn);
+                            acc_cp = fma((double)tq.x, (double)vc, acc_cp);
+                            acc_sp = fma((double)tq.x, (double)vs, acc_sp);
+                            acc_ct = fma((double)tq.y, (double)uu, acc_ct);
+                            acc_st = fma((double)tq.z, (double)uu, acc_st);
                         }
                     }
-                    acc_qn += (double)(tv * U);
-                    acc_cp += (double)(tv * ac);
-                    acc_sp += (double)(tv * as_);
-                    acc_ct += (double)(U * dtc);
-                    acc_st += (double)(U * dts);
                 }
             }
             acc_qn = warp_sum_d(acc_qn);
@@ -266,83 +291,100 @@ __global__ void __launch_bounds__(kGatherWarps * 32) k_adj_gather(const double* 
             acc_sp = warp_sum_d(acc_sp);
             acc_ct = warp_sum_d(acc_ct);
             acc_st = warp_sum_d(acc_st);
-            if (lane == 0) {
-                const double qn = r.qn;
-                const double gqn = acc_qn;
-                // centres and widths, through qn = q / (Sp * St) as well
-                const double gcp = qn * acc_cp - gqn * (qn / Sp) * dSp_c;
-                const double gsp = qn * acc_sp - gqn * (qn / Sp) * dSp_s;
-                const double gct = qn * acc_ct - gqn * (qn / St) * dSt_c;
-                const double gst = qn * acc_st - gqn * (qn / St) * dSt_s;
-                const double gqf = gqn / ((double)Sp * (double)St);
-                const double gsL = gst / drift_speed;  // sigma_time = extent_long / drift_speed
-                const double gsT = gsp;                // sigma_pitch = extent_tran
-                // back through the drift (Drifter::insert, gen/src/Drifter.cxx:164-192)
-                const double* pd = dep + 7 * (size_t)i;
-                const double q0 = pd[1], x0 = pd[2], el0 = pd[5], et0 = pd[6];
-                double gq = gqf, gx = 0.0, gel = gsL, get = gsT;
-                if (do_drift) {
-                    int found = -1;
-                    double dir = 0.0;
-                    for (int k = 0; k < dd.nxr; ++k) {
-                        const double a = dd.xr[k][0], rp = dd.xr[k][1];
-                        if ((a < x0 && x0 < rp) || (rp < x0 && x0 < a)) { found = k; dir = -1.0; break; }
-                    }
-                    if (found < 0)
-                        for (int k = 0; k < dd.nxr; ++k) {
-                            const double rp = dd.xr[k][1], c = dd.xr[k][2];
-                            if ((rp < x0 && x0 < c) || (c < x0 && x0 < rp)) { found = k; dir = 1.0; break; }
-                        }
-                    if (found >= 0) {
-                        const double respx = dd.xr[found][1];
-                        const double dt = fabs((respx - x0) / dd.speed);
-                        const double dtdx = (x0 > respx ? 1.0 : -1.0) / dd.speed;  // d(dt)/dx
-                        if (dir > 0) {
-                            // t' = t + dt, q' = q exp(-dt/lifetime), sL^2 = 2 DL dt + el^2, sT^2 = 2 DT dt + et^2
-                            const double ex = exp(-dt / dd.lifetime);
-                            const double qd = q0 * ex;
-                            const double sL = sqrt(2.0 * dd.DL * dt + el0 * el0);
-                            const double sT = sqrt(2.0 * dd.DT * dt + et0 * et0);
-                            const double hL = sL > 0.0 ? gsL / sL : 0.0;  // dL/d(sL^2) * 2
-                            const double hT = sT > 0.0 ? gsT / sT : 0.0;
-                            const double gdt = gct - gqf * qd / dd.lifetime + hL * dd.DL + hT * dd.DT;
-                            gx = gdt * dtdx;
-                            gq = gqf * ex;
-                            gel = hL * el0;
-                            get = hT * et0;
-                            gDL = hL * dt;
-                            gDT = hT * dt;
-                            gTau = gqf * qd * dt / (dd.lifetime * dd.lifetime);
-                        }
-                        else {
-                            gx = -gct * dtdx;  // t' = t - dt in the response region
-                        }
-                    }
-                }
-                else {
-                    gx = gcp * A.ax;
-                }
-                double* gd = grad + 7 * (size_t)i;
-                atomicAdd(gd + 0, gct);
-                atomicAdd(gd + 1, gq);
-                atomicAdd(gd + 2, gx);
-                atomicAdd(gd + 3, gcp * A.ay);
-                atomicAdd(gd + 4, gcp * A.az);
-                atomicAdd(gd + 5, gel);
-                atomicAdd(gd + 6, get);
-                (void)q0;
-            }
+            const double qn = r.qn;
+            const double gqn = acc_qn;
+            // centres and widths, through qn = q / (Sp * St) as well
+            const double gcp = qn * acc_cp - gqn * (qn / Sp) * dSp_c;
+            const double gsp = qn * acc_sp - gqn * (qn / Sp) * dSp_s;
+            s_ct += qn * acc_ct - gqn * (qn / St) * dSt_c;
+            s_sL += (qn * acc_st - gqn * (qn / St) * dSt_s) / drift_speed;  // sigma_time = extent_long / v
+            s_sT += gsp;                                                       // sigma_pitch = extent_tran
+            s_qf += gqn / ((double)Sp * (double)St);
+            s_px += gcp * A.ax;
+            s_py += gcp * A.ay;
+            s_pz += gcp * A.az;
+        }
+        if (any && lane == 0) {
+            // sums over planes; k_adj_drift takes them back through the drift in place
+            double* gd = grad + 7 * (size_t)i;
+            gd[0] = s_ct;
+            gd[1] = s_qf;
+            gd[2] = s_px;
+            gd[3] = s_py;
+            gd[4] = s_pz;
+            gd[5] = s_sL;
+            gd[6] = s_sT;
         }
     }
-    if (lane == 0) {
-        s_glob[wib][0] = gDL;
-        s_glob[wib][1] = gDT;
-        s_glob[wib][2] = gTau;
+}
+
+// Back through the drift (Drifter::insert, gen/src/Drifter.cxx:164-192), one
+// thread per depo, in place on the per-depo sums of k_adj_gather
+// (dL/dt', dL/dq', dL/d(x', y, z) through the pitch, dL/dsigma_L, dL/dsigma_T),
+// plus the block sums of dL/d(DL, DT, lifetime).
+__global__ void __launch_bounds__(256) k_adj_drift(const double* __restrict__ dep, int n, DriftDev dd,
+                                                    double* __restrict__ grad, double* __restrict__ gglob)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    double gDL = 0.0, gDT = 0.0, gTau = 0.0;
+    if (i < n) {
+        double* gd = grad + 7 * (size_t)i;
+        const double s_ct = gd[0], s_qf = gd[1], s_sL = gd[5], s_sT = gd[6];
+        const double* pd = dep + 7 * (size_t)i;
+        const double q0 = pd[1], x0 = pd[2], el0 = pd[5], et0 = pd[6];
+        int found = -1;
+        double dir = 0.0;
+        for (int k = 0; k < dd.nxr; ++k) {
+            const double a = dd.xr[k][0], rp = dd.xr[k][1];
+            if ((a < x0 && x0 < rp) || (rp < x0 && x0 < a)) { found = k; dir = -1.0; break; }
+        }
+        if (found < 0)
+            for (int k = 0; k < dd.nxr; ++k) {
+                const double rp = dd.xr[k][1], c = dd.xr[k][2];
+                if ((rp < x0 && x0 < c) || (c < x0 && x0 < rp)) { found = k; dir = 1.0; break; }
+            }
+        double gx = 0.0;  // x' = x_response: x enters through the drift time only
+        if (found >= 0) {
+            const double respx = dd.xr[found][1];
+            const double dtm = fabs((respx - x0) / dd.speed);
+            const double dtdx = (x0 > respx ? 1.0 : -1.0) / dd.speed;  // d(dt)/dx
+            if (dir > 0) {
+                // t' = t + dt, q' = q exp(-dt/lifetime), sL^2 = 2 DL dt + el^2, sT^2 = 2 DT dt + et^2
+                const double ex = exp(-dtm / dd.lifetime);
+                const double qd = q0 * ex;
+                const double sL = sqrt(2.0 * dd.DL * dtm + el0 * el0);
+                const double sT = sqrt(2.0 * dd.DT * dtm + et0 * et0);
+                const double hL = sL > 0.0 ? s_sL / sL : 0.0;
+                const double hT = sT > 0.0 ? s_sT / sT : 0.0;
+                const double gdt = s_ct - s_qf * qd / dd.lifetime + hL * dd.DL + hT * dd.DT;
+                gx = gdt * dtdx;
+                gd[1] = s_qf * ex;
+                gd[5] = hL * el0;
+                gd[6] = hT * et0;
+                gDL = hL * dtm;
+                gDT = hT * dtm;
+                gTau = s_qf * qd * dtm / (dd.lifetime * dd.lifetime);
+            }
+            else {
+                gx = -s_ct * dtdx;  // t' = t - dt in the response region
+            }
+        }
+        gd[2] = gx;
+    }
+    __shared__ double s_glob[8][3];
+    gDL = warp_sum_d(gDL);
+    gDT = warp_sum_d(gDT);
+    gTau = warp_sum_d(gTau);
+    const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+    if (l == 0) {
+        s_glob[w][0] = gDL;
+        s_glob[w][1] = gDT;
+        s_glob[w][2] = gTau;
     }
     __syncthreads();
     if (threadIdx.x < 3) {
         double v = 0.0;
-        for (int k = 0; k < kGatherWarps; ++k) v += s_glob[k][threadIdx.x];
+        for (int k = 0; k < (int)(blockDim.x >> 5); ++k) v += s_glob[k][threadIdx.x];
         if (v != 0.0) atomicAdd(gglob + threadIdx.x, v);
     }
 }
@@ -351,11 +393,10 @@ void launch_adj_gather(const double* depos, int n, const DriftDev& dd, int do_dr
                        const AdjSet& as, double drift_speed, const PatchRec* rec, const float* dQ, double* grad,
                        double* gglob, cudaStream_t s)
 {
-    const long long warps = (long long)ps.nplanes * n;
-    if (warps <= 0) return;
-    const long long blocks = (warps + kGatherWarps - 1) / kGatherWarps;
-    k_adj_gather<<<(unsigned)blocks, kGatherWarps * 32, 0, s>>>(depos, n, dd, do_drift, ps, as, drift_speed, rec, dQ,
-                                                                grad, gglob);
+    if (n <= 0) return;
+    const int blocks = (n + kGatherWarps - 1) / kGatherWarps;
+    k_adj_gather<<<blocks, kGatherWarps * 32, 0, s>>>(n, ps, as, drift_speed, rec, dQ, grad);
+    if (do_drift) k_adj_drift<<<(n + 255) / 256, 256, 0, s>>>(depos, n, dd, grad, gglob);
 }
 
 }  // namespace wctb200

@@ -42,6 +42,15 @@ void set_params(wct_depotransform* h, const torch::Tensor& dp)
     check(wct_dt_set_drift_params(h, v[0], v[1], v[2]));
 }
 
+// The launch stream: torch's current stream.  Torch's default stream has the
+// handle 0, which the C ABI reads as "the component's own stream", so it is
+// passed as the explicit legacy default-stream handle instead.
+cudaStream_t launch_stream(const torch::Tensor& t)
+{
+    cudaStream_t s = c10::cuda::getCurrentCUDAStream(t.device().index()).stream();
+    return s ? s : cudaStreamLegacy;
+}
+
 void check_depos(const torch::Tensor& d)
 {
     TORCH_CHECK(d.is_cuda(), "depos must be a CUDA tensor");
@@ -61,9 +70,8 @@ struct DepoTransformFn : public torch::autograd::Function<DepoTransformFn> {
         int nrows = 0, nticks = 0;
         check(wct_dt_frame_shape(h, &nrows, &nticks));
         auto frame = torch::empty({nrows, nticks}, d.options().dtype(torch::kFloat32));
-        auto stream = c10::cuda::getCurrentCUDAStream(d.device().index());
         check(wct_dt_forward_device(h, d.data_ptr<double>(), (size_t)d.size(0), frame.data_ptr<float>(), nullptr,
-                                    nullptr, stream.stream()));
+                                    nullptr, launch_stream(d)));
         ctx->save_for_backward({d, drift_params});
         ctx->saved_data["handle"] = handle;
         return frame;
@@ -81,10 +89,9 @@ struct DepoTransformFn : public torch::autograd::Function<DepoTransformFn> {
         TORCH_CHECK(g.is_cuda() && g.device() == d.device(), "frame gradient on another device");
         auto gd = torch::empty_like(d);
         auto gg = torch::zeros({3}, d.options());
-        auto stream = c10::cuda::getCurrentCUDAStream(d.device().index());
         check(wct_dt_adjoint_device(h, d.data_ptr<double>(), (size_t)d.size(0), g.data_ptr<float>(),
                                     d.size(0) ? gd.data_ptr<double>() : nullptr, gg.data_ptr<double>(),
-                                    stream.stream()));
+                                    launch_stream(d)));
         torch::Tensor gdp;
         if (dp.defined() && dp.numel() == 3) gdp = gg.to(dp.device()).reshape(dp.sizes());
         return {gd, gdp, torch::Tensor()};

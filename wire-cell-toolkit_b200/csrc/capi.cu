@@ -179,7 +179,7 @@ struct Core {
     WindowDev* h_win{nullptr};
     size_t last_n{0};
     // stage profiling
-    static constexpr int kStages = 6;
+    static constexpr int kStages = 10;
     bool profiling{false};
     double stage_ms[kStages]{};
     long stage_launches[kStages]{};
@@ -395,7 +395,7 @@ __global__ void k_win_init(WindowDev* w, int n)
     w[i].tmin = ~0ull;
     w[i].pmax = 0ull;
     w[i].tmax = 0ull;
-    w[i].nadded = w[i].out_time = w[i].out_pitch = w[i].oversize = 0;
+    w[i].nadded = w[i].out_time = w[i].out_pitch = w[i].oversize = w[i].bigcharge = 0;
 }
 
 // Drift, patch records, per-plane windows and charge-grid layout of one event:
@@ -458,12 +458,12 @@ static int prepare_event(Core& c, const double* d_depos, size_t ndepos, cudaStre
 
     Core::StageTimer t_prep(&c, 0, s);
     CUDA_TRY(cudaMemsetAsync(c.d_wcnt.p, 0, sizeof(int) * (nkeys + 1), s));
-    CUDA_TRY(c.d_kbound.ensure(sizeof(float) * (size_t)nkeys * kTileBlocks));
-    CUDA_TRY(cudaMemsetAsync(c.d_kbound.p, 0, sizeof(float) * (size_t)nkeys * kTileBlocks, s));
+    CUDA_TRY(c.d_kbound.ensure(sizeof(unsigned long long) * (size_t)nkeys * kTileBlocks));
+    CUDA_TRY(cudaMemsetAsync(c.d_kbound.p, 0, sizeof(unsigned long long) * (size_t)nkeys * kTileBlocks, s));
     k_win_init<<<1, 64, 0, s>>>(c.d_win.as<WindowDev>(), np);
     launch_prep_all(d_depos, n, c.drifter, c.have_drifter ? 1 : 0, pset, tb, c.drift_speed, c.nsigma,
                     c.d_rec.as<PatchRec>(), c.d_win.as<WindowDev>(), c.d_wcnt.as<int>(), c.d_tprof.as<float>(),
-                    c.d_kbound.as<float>(), s);
+                    c.d_kbound.as<unsigned long long>(), s);
     launch_scan(c.d_wcnt.as<int>(), nkeys, c.d_woff.as<int>(), c.d_wcur.as<int>(), s);
     t_prep.close(4 + (n > 0 ? 1 : 0));
     CUDA_TRY(cudaGetLastError());
@@ -472,6 +472,8 @@ static int prepare_event(Core& c, const double* d_depos, size_t ndepos, cudaStre
     CUDA_TRY(cudaStreamSynchronize(s));
     for (int ip = 0; ip < np; ++ip)
         if (c.h_win[ip].oversize) return fail(WCT_ERR_SIZE, "a diffusion patch exceeds 1024 ticks or 1024 impact bins");
+    for (int ip = 0; ip < np; ++ip)
+        if (c.h_win[ip].bigcharge) return fail(WCT_ERR_SIZE, "a depo charge exceeds 5e11 electrons");
     ev.total_visits = *h_total;
 
     std::vector<PlaneWindow>& pw = ev.pw;
@@ -538,7 +540,7 @@ static int forward_device(Core& c, const double* d_depos, size_t ndepos, float* 
     Core::StageTimer t_r(&c, 1, s);
     launch_fill(c.d_rec.as<PatchRec>(), n, pset, c.d_wcur.as<int>(), c.d_wlist.as<Visit>(), s);
     launch_raster_wires(c.d_rec.as<PatchRec>(), c.d_tprof.as<float>(), c.d_wcnt.as<int>(), c.d_woff.as<int>(),
-                        c.d_wlist.as<Visit>(), c.d_kbound.as<float>(), gset, c.d_Q.as<float>(), s);
+                        c.d_wlist.as<Visit>(), c.d_kbound.as<unsigned long long>(), gset, c.d_Q.as<float>(), s);
     t_r.close((n > 0 ? 1 : 0) + (rows > 0 ? 1 : 0));
     CUDA_TRY(cudaGetLastError());
 
@@ -634,19 +636,25 @@ static int adjoint_device(Core& c, const double* d_depos, size_t ndepos, const f
         if (rc) return rc;
         float* Gr = c.d_V.as<float>();  // [nout][N] real, then [nout][M] spectra in place
         const int wlo = std::max(0, w.m_start_ch), whi = std::min(ps.desc.nwires, w.m_end_ch);
+        Core::StageTimer t_f(&c, 6, s);
         launch_grad_rows(d_gframe + (size_t)ps.row0 * nticks, nticks, w.start_ch - ps.npad, wlo, whi, w.start_tick,
                          std::min(N, w.nt_ref), nout, N, Gr, s);
         launch_rfft_rows(Gr, N, N, reinterpret_cast<float2*>(Gr), M, nout, d, s);
+        t_f.close(2);
         float* dQ = c.d_Q.as<float>() + g.qoff;
+        Core::StageTimer t_c(&c, 7, s);
         launch_wire_conv_adj(reinterpret_cast<const float2*>(Gr), ps.d_spec.as<float2>(),
                              reinterpret_cast<float2*>(dQ), ps.G, ps.npad, nin, nout, M, s);
+        t_c.close(1);
+        Core::StageTimer t_i(&c, 8, s);
         launch_irfft_rows(reinterpret_cast<const float2*>(dQ), ps.G * nin, d, 0, 0, ps.G * nin, 0, N, N, dQ, s);
-        c.total_launches += 4;
+        t_i.close(1);
         CUDA_TRY(cudaGetLastError());
     }
+    Core::StageTimer t_g(&c, 9, s);
     launch_adj_gather(d_depos, n, c.drifter, c.have_drifter ? 1 : 0, ev.pset, as, c.drift_speed,
                       c.d_rec.as<PatchRec>(), c.d_Q.as<float>(), d_gdep, gg, s);
-    if (n) c.total_launches += 1;
+    t_g.close(n ? (c.have_drifter ? 2 : 1) : 0);
     CUDA_TRY(cudaGetLastError());
     return WCT_OK;
 }

@@ -107,7 +107,7 @@ __global__ void __launch_bounds__(256) k_prep_all(const double* __restrict__ dep
                                                   PlaneSet ps, TimeDev tb, double drift_speed, double nsigma,
                                                   PatchRec* __restrict__ rec, WindowDev* __restrict__ win,
                                                   int* __restrict__ wire_cnt, float* __restrict__ tprof,
-                                                  float* __restrict__ key_bound)
+                                                  unsigned long long* __restrict__ key_bound)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     double t = 0, q = 0, x = 0, y = 0, z = 0, el = 0, et = 0;
@@ -175,7 +175,7 @@ __global__ void __launch_bounds__(256) k_prep_all(const double* __restrict__ dep
         }
     }
     __shared__ unsigned long long s_k[4][8];
-    __shared__ int s_c[4][8];
+    __shared__ int s_c[5][8];
     const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
     auto umin = [](unsigned long long a, unsigned long long b) { return a < b ? a : b; };
     auto umax = [](unsigned long long a, unsigned long long b) { return a > b ? a : b; };
@@ -183,7 +183,7 @@ __global__ void __launch_bounds__(256) k_prep_all(const double* __restrict__ dep
     for (int ip = 0; ip < ps.nplanes; ++ip) {
         const PlaneDev& pl = ps.p[ip];
         unsigned long long kpmin = ~0ull, kpmax = 0ull, ktmin = ~0ull, ktmax = 0ull;
-        int nadd = 0, nout_t = 0, nout_p = 0, nover = 0;
+        int nadd = 0, nout_t = 0, nout_p = 0, nover = 0, nbig = 0;
         PatchRec r;
         r.toff = r.poff = 0;
         r.nt = r.np = 0;
@@ -263,13 +263,17 @@ __global__ void __launch_bounds__(256) k_prep_all(const double* __restrict__ dep
         const int k0 = r.toff / kTile;
         const int kspan = r.np ? (r.toff + r.nt - 1) / kTile - k0 + 1 : 0;
         count_visits(wire_cnt, pl.wire_base, w0, span, k0, kspan, ps.ntiles);
-        // fixed-point bounds of the raster: per (wire, tile, 64-tick block)
+        // fixed-point bounds of the raster: per (wire, tile, 64-tick block), summed
+        // as integers in units of 2^-16 (each term rounded up), so the bound --
+        // and with it the raster's scale -- does not depend on the order of the adds
         if (r.np) {
             const float b = visit_bound(r.qn, r.sp, r.st, (float)pl.imp_bs, (float)tb.bs);
+            if (b > kMaxVisitBound) nbig = 1;
+            const unsigned long long bu = __float2ull_ru(fminf(b, kMaxVisitBound) * 65536.0f);
             const int b0 = r.toff / kScaleBlock, b1 = (r.toff + r.nt - 1) / kScaleBlock;
             for (int ww = 0; ww < span; ++ww) {
-                float* kb = key_bound + (size_t)(pl.wire_base + w0 + ww) * ps.ntiles * kTileBlocks;
-                for (int bb = b0; bb <= b1; ++bb) atomicAdd(kb + bb, b);
+                unsigned long long* kb = key_bound + (size_t)(pl.wire_base + w0 + ww) * ps.ntiles * kTileBlocks;
+                for (int bb = b0; bb <= b1; ++bb) atomicAdd(kb + bb, bu);
             }
         }
         // block reduction, one atomic per block per quantity
@@ -281,9 +285,10 @@ __global__ void __launch_bounds__(256) k_prep_all(const double* __restrict__ dep
         nout_t = warp_reduce(nout_t, iadd);
         nout_p = warp_reduce(nout_p, iadd);
         nover = warp_reduce(nover, iadd);
+        nbig = warp_reduce(nbig, iadd);
         if (l == 0) {
             s_k[0][w] = kpmin; s_k[1][w] = kpmax; s_k[2][w] = ktmin; s_k[3][w] = ktmax;
-            s_c[0][w] = nadd; s_c[1][w] = nout_t; s_c[2][w] = nout_p; s_c[3][w] = nover;
+            s_c[0][w] = nadd; s_c[1][w] = nout_t; s_c[2][w] = nout_p; s_c[3][w] = nover; s_c[4][w] = nbig;
         }
         __syncthreads();
         if (w == 0) {
@@ -296,6 +301,7 @@ __global__ void __launch_bounds__(256) k_prep_all(const double* __restrict__ dep
             nout_t = l < nw ? s_c[1][l] : 0;
             nout_p = l < nw ? s_c[2][l] : 0;
             nover = l < nw ? s_c[3][l] : 0;
+            nbig = l < nw ? s_c[4][l] : 0;
             kpmin = warp_reduce(kpmin, umin);
             ktmin = warp_reduce(ktmin, umin);
             kpmax = warp_reduce(kpmax, umax);
@@ -304,6 +310,7 @@ __global__ void __launch_bounds__(256) k_prep_all(const double* __restrict__ dep
             nout_t = warp_reduce(nout_t, iadd);
             nout_p = warp_reduce(nout_p, iadd);
             nover = warp_reduce(nover, iadd);
+            nbig = warp_reduce(nbig, iadd);
             WindowDev* wd = win + ip;
             if (l == 0 && nadd) {
                 atomicMin(&wd->pmin, kpmin);
@@ -315,6 +322,7 @@ __global__ void __launch_bounds__(256) k_prep_all(const double* __restrict__ dep
             if (l == 0 && nout_t) atomicAdd(&wd->out_time, nout_t);
             if (l == 0 && nout_p) atomicAdd(&wd->out_pitch, nout_p);
             if (l == 0 && nover) atomicAdd(&wd->oversize, nover);
+            if (l == 0 && nbig) atomicAdd(&wd->bigcharge, nbig);
         }
         __syncthreads();
     }
@@ -322,7 +330,7 @@ __global__ void __launch_bounds__(256) k_prep_all(const double* __restrict__ dep
 
 void launch_prep_all(const double* depos, int n, const DriftDev& dd, int do_drift, const PlaneSet& ps,
                      const TimeDev& tb, double drift_speed, double nsigma, PatchRec* rec, WindowDev* win,
-                     int* wire_cnt, float* tprof, float* key_bound, cudaStream_t s)
+                     int* wire_cnt, float* tprof, unsigned long long* key_bound, cudaStream_t s)
 {
     if (n <= 0) return;
     k_prep_all<<<(n + 255) / 256, 256, 0, s>>>(depos, n, dd, do_drift, ps, tb, drift_speed, nsigma, rec, win,
@@ -481,7 +489,8 @@ void launch_fill(const PatchRec* rec, int n, const PlaneSet& ps, int* wire_cur, 
 // any cell of the block can reach: the sum over the visits touching the block
 // of |q| * max bin fraction in pitch * max bin fraction in time * 2.  Cells
 // cannot overflow and one add is resolved to ~2^-30 of that local bound.
-// Integer sums are order independent, so the grid is bit-reproducible.
+// Integer sums are order independent (the bounds too are integer sums), so
+// the grid is bit-reproducible.
 // ---------------------------------------------------------------------------
 constexpr int kRasterThreads = 256;
 // staged per visit: 12 group coefficients, q, and 16 scaled tick values (odd stride: no bank conflicts)
@@ -501,7 +510,8 @@ __global__ void __launch_bounds__(kRasterThreads) k_raster_wires(const PatchRec*
                                                                  const int* __restrict__ wire_cnt,
                                                                  const int* __restrict__ wire_off,
                                                                  const Visit* __restrict__ visits,
-                                                                 const float* __restrict__ key_bound, GridSet gs,
+                                                                 const unsigned long long* __restrict__ key_bound,
+                                                                 GridSet gs,
                                                                  float* __restrict__ Q)
 {
     extern __shared__ int smem_i[];
@@ -532,7 +542,8 @@ __global__ void __launch_bounds__(kRasterThreads) k_raster_wires(const PatchRec*
         const int n4 = G * kTileLd / 4;
         for (int k = tid; k < n4; k += kRasterThreads) g4[k] = make_int4(0, 0, 0, 0);
         if (tid < kTileBlocks) {
-            const float b = key >= 0 ? key_bound[(size_t)key * kTileBlocks + tid] : 0.f;
+            const float b = key >= 0 ? __ull2float_ru(key_bound[(size_t)key * kTileBlocks + tid]) * (1.0f / 65536.0f)
+                                     : 0.f;
             scale[tid] = b > 0.f ? 1073741824.0f / b : 0.f;
             iscale[tid] = b > 0.f ? b / 1073741824.0f : 0.f;
         }
@@ -687,7 +698,8 @@ __global__ void __launch_bounds__(kRasterThreads) k_raster_wires(const PatchRec*
 }
 
 void launch_raster_wires(const PatchRec* rec, const float* tprof, const int* wire_cnt, const int* wire_off,
-                         const Visit* visits, const float* key_bound, const GridSet& gs, float* Q, cudaStream_t s)
+                         const Visit* visits, const unsigned long long* key_bound, const GridSet& gs, float* Q,
+                         cudaStream_t s)
 {
     if (gs.nrows_total <= 0) return;
     size_t smem = 0;

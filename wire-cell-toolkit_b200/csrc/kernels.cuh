@@ -72,6 +72,7 @@ static_assert(sizeof(Visit) == 32, "Visit layout");
 struct WindowDev {
     unsigned long long pmin, pmax, tmin, tmax;  // order-preserving double keys
     int nadded, out_time, out_pitch, oversize;
+    int bigcharge;  // patches whose raster bound exceeds kMaxVisitBound
 };
 
 constexpr int kTprof = 16;        // time profiles up to this many ticks are computed once per depo
@@ -80,6 +81,9 @@ constexpr int kScaleBlock = 64;   // ticks sharing one fixed-point scale in the 
 constexpr int kTileBlocks = kTile / kScaleBlock;
 constexpr int kMaxPatchT = 1024;  // ticks per patch
 constexpr int kMaxPatchP = 1024;  // impact bins per patch
+// Largest per-visit bound (2 |q| x peak bin fractions, in electrons) of the
+// raster's integer bound sums (units of 2^-16 in 64 bits).
+constexpr float kMaxVisitBound = 1.0e12f;
 
 // Per-plane parameters of the charge-grid stage of one event.
 struct GridPlane {
@@ -118,12 +122,13 @@ struct AdjSet {
 // ---- launchers (kernels.cu) ----
 void launch_prep_all(const double* depos, int n, const DriftDev& dd, int do_drift, const PlaneSet& ps,
                      const TimeDev& tb, double drift_speed, double nsigma, PatchRec* rec, WindowDev* win,
-                     int* wire_cnt, float* tprof, float* key_bound, cudaStream_t s);
+                     int* wire_cnt, float* tprof, unsigned long long* key_bound, cudaStream_t s);
 void launch_scan(const int* wire_cnt, int nwires_total, int* wire_off, int* wire_cur, cudaStream_t s);
 void launch_fill(const PatchRec* rec, int n, const PlaneSet& ps, int* wire_cur, Visit* visits, cudaStream_t s);
 size_t raster_smem_bytes(int G);
 void launch_raster_wires(const PatchRec* rec, const float* tprof, const int* wire_cnt, const int* wire_off,
-                         const Visit* visits, const float* key_bound, const GridSet& gs, float* Q, cudaStream_t s);
+                         const Visit* visits, const unsigned long long* key_bound, const GridSet& gs, float* Q,
+                         cudaStream_t s);
 void launch_rfft_rows(const float* in, long in_ld, int in_len, float2* out, long out_ld, int nrows,
                       const FftDesc& d, cudaStream_t s);
 void launch_wire_conv(const float2* Qh, const float2* Rh, float2* Vh, int ngroups, int npad, int nrows_in,
