@@ -159,162 +159,206 @@ __device__ __forceinline__ double warp_sum_d(double v)
     return v;
 }
 
-// Unit bin integral between edges at distances x1 < x2 from the centre
-// (sigma s > 0, inv = 1 / (sqrt(2) s)) and its derivatives in centre and sigma.
-__device__ __forceinline__ float bin_and_derivs(float x1, float x2, float s, float inv, float& dc, float& ds)
+// Quantities of one bin edge at distance x from the centre (sigma s > 0,
+// is = 1/s, inv = 1/(sqrt(2) s)): the signed erfc of the forward's bin
+// integrals, the density phi(u), u phi(u) and u^2 phi(u) with u = x/s.
+__device__ __forceinline__ void edge_terms(float x, float is, float inv, float& E, float& f, float& uf, float& uuf)
 {
-    const float u1 = x1 / s, u2 = x2 / s;
-    const float f1 = norm_pdf(u1), f2 = norm_pdf(u2);
-    dc = -(f2 - f1) / s;
-    ds = -(u2 * f2 - u1 * f1) / s;
-    const float e1 = copysignf(erfc_nr(fabsf(x1 * inv)), x1), e2 = copysignf(erfc_nr(fabsf(x2 * inv)), x2);
-    return bin_from_edges(e1, e2);
+    const float u = x * is;
+    E = copysignf(erfc_nr(fabsf(x * inv)), x);
+    f = norm_pdf(u);
+    uf = u * f;
+    uuf = u * uf;
 }
 
-__global__ void __launch_bounds__(kGatherWarps * 32, 5) k_adj_gather(int n, PlaneSet ps, AdjSet as, double drift_speed,
-                                                                  const PatchRec* __restrict__ rec,
-                                                                  const float* __restrict__ dQ,
-                                                                  double* __restrict__ grad)
+__device__ __forceinline__ float warp_sum_f(float v)
+{
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+__global__ void __launch_bounds__(kGatherWarps * 32, 5) k_adj_gather(int n, PlaneSet ps, AdjSet as, double inv_vd,
+                                                                     const PatchRec* __restrict__ rec,
+                                                                     const float* __restrict__ dQ,
+                                                                     double* __restrict__ grad)
 {
     __shared__ BinTab s_p[kGatherWarps][kChunkP];
     __shared__ float4 s_t[kGatherWarps][kChunkT];
+    const unsigned full = 0xffffffffu;
     const int wib = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int i = blockIdx.x * kGatherWarps + wib;
-    if (i < n) {
-        // per-depo sums over planes: dL/dt', dL/dq', dL/dsL, dL/dsT, dL/d(x', y, z) through the pitch
-        double s_ct = 0.0, s_qf = 0.0, s_sL = 0.0, s_sT = 0.0, s_px = 0.0, s_py = 0.0, s_pz = 0.0;
-        bool any = false;
-        for (int ip = 0; ip < ps.nplanes; ++ip) {
-            const PatchRec r = rec[(size_t)ip * n + i];
-            const AdjPlane& A = as.p[ip];
-            const int np = r.np, nt = r.nt;
-            if (np == 0 || nt == 0 || A.nin == 0) continue;
-            any = true;
-            const float pbs = A.pbs, tbs = A.tbs;
-            const float sp = r.sp, st = r.st;
-            const float invp = sp > 0.f ? 1.0f / (1.41421356237309505f * sp) : 0.f;
-            const float invt = st > 0.f ? 1.0f / (1.41421356237309505f * st) : 0.f;
-            // normalisation sums over the clipped patch and their derivatives
-            float Sp = 1.f, dSp_c = 0.f, dSp_s = 0.f;
-            if (sp > 0.f) Sp = bin_and_derivs(-r.pcr, (float)np * pbs - r.pcr, sp, invp, dSp_c, dSp_s);
-            float St = 1.f, dSt_c = 0.f, dSt_s = 0.f;
-            if (st > 0.f) St = bin_and_derivs(-r.tcr, (float)nt * tbs - r.tcr, st, invt, dSt_c, dSt_s);
-            double acc_qn = 0.0, acc_cp = 0.0, acc_sp = 0.0, acc_ct = 0.0, acc_st = 0.0;
-            const size_t gstride = (size_t)A.nin * A.N;
-            const float* dQp = dQ + A.qoff;
-            const int col = r.toff - A.col0;
-            for (int t0 = 0; t0 < nt; t0 += kChunkT) {
-                const int ntc = min(kChunkT, nt - t0);
-                __syncwarp();
-                for (int tt = lane; tt < ntc; tt += 32) {
-                    const int tau = t0 + tt;
-                    float tv = 1.f, dtc = 0.f, dts = 0.f;
-                    if (st > 0.f)
-                        tv = bin_and_derivs((float)tau * tbs - r.tcr, (float)(tau + 1) * tbs - r.tcr, st, invt, dtc,
-                                            dts);
-                    s_t[wib][tt] = make_float4(tv, dtc, dts, 0.f);
+    if (i >= n) return;  // whole warps only: no block-level barrier follows
+    // per-depo sums over planes: dL/dt', dL/dq', dL/dsL, dL/dsT, dL/d(x', y, z) through the pitch
+    double s_ct = 0.0, s_qf = 0.0, s_sL = 0.0, s_sT = 0.0, s_px = 0.0, s_py = 0.0, s_pz = 0.0;
+    bool any = false;
+    for (int ip = 0; ip < ps.nplanes; ++ip) {
+        const PatchRec r = rec[(size_t)ip * n + i];
+        const AdjPlane& A = as.p[ip];
+        const int np = r.np, nt = r.nt;
+        if (np == 0 || nt == 0 || A.nin == 0) continue;
+        any = true;
+        const float pbs = A.pbs, tbs = A.tbs, ipbs = 1.0f / pbs;
+        const float sp = r.sp, st = r.st;
+        const float isp = sp > 0.f ? 1.0f / sp : 0.f, invp = 0.70710678118654752f * isp;
+        const float ist = st > 0.f ? 1.0f / st : 0.f, invt = 0.70710678118654752f * ist;
+        // lane partial sums of the bin integrals and their derivatives (normalisation)
+        float pS = 0.f, pSc = 0.f, pSs = 0.f, tS = 0.f, tSc = 0.f, tSs = 0.f;
+        double acc_qn = 0.0, acc_cp = 0.0, acc_sp = 0.0, acc_ct = 0.0, acc_st = 0.0;
+        const size_t gstride = (size_t)A.nin * A.N;
+        const float* dQp = dQ + A.qoff;
+        const int col = r.toff - A.col0;
+        for (int t0 = 0; t0 < nt; t0 += kChunkT) {
+            const int ntc = min(kChunkT, nt - t0);
+            __syncwarp();
+            if (st > 0.f) {
+                // one edge per lane, bins from neighbouring lanes (31 bins per round)
+                for (int tb = t0; tb < t0 + ntc; tb += 31) {
+                    const int e = tb + lane;
+                    const float x = (float)e * tbs - r.tcr;
+                    float E = 0.f, f = 0.f, uf = 0.f, uuf = 0.f;
+                    if (e <= nt) edge_terms(x, ist, invt, E, f, uf, uuf);
+                    const float E2 = __shfl_down_sync(full, E, 1), f2 = __shfl_down_sync(full, f, 1);
+                    const float uf2 = __shfl_down_sync(full, uf, 1);
+                    if (lane < 31 && e < t0 + ntc) {
+                        const float tv = bin_from_edges(E, E2);
+                        const float dtc = -(f2 - f) * ist, dts = -(uf2 - uf) * ist;
+                        s_t[wib][e - t0] = make_float4(tv, dtc, dts, 0.f);
+                        tS += tv;
+                        tSc += dtc;
+                        tSs += dts;
+                    }
+                    (void)uuf;
                 }
-                for (int k0 = 0; k0 < np; k0 += kChunkP) {
-                    const int nk = min(kChunkP, np - k0);
-                    __syncwarp();
-                    for (int kk = lane; kk < nk; kk += 32) {
-                        const int k = k0 + kk;
+            }
+            else if (lane == 0) {  // point in time: one tick
+                s_t[wib][0] = make_float4(1.f, 0.f, 0.f, 0.f);
+                tS = 1.f;
+            }
+            for (int k0 = 0; k0 < np; k0 += kChunkP) {
+                const int nk = min(kChunkP, np - k0);
+                __syncwarp();
+                for (int kb = k0; kb < k0 + nk; kb += 31) {
+                    const int e = kb + lane;
+                    float E = 0.f, f = 0.f, uf = 0.f, uuf = 0.f;
+                    if (sp > 0.f && e <= np) edge_terms((float)e * pbs - r.pcr, isp, invp, E, f, uf, uuf);
+                    const float E2 = __shfl_down_sync(full, E, 1), f2 = __shfl_down_sync(full, f, 1);
+                    const float uf2 = __shfl_down_sync(full, uf, 1), uuf2 = __shfl_down_sync(full, uuf, 1);
+                    if (lane < 31 && e < k0 + nk) {
                         BinTab b;
                         if (sp > 0.f) {
-                            const float x1 = (float)k * pbs - r.pcr, x2 = (float)(k + 1) * pbs - r.pcr;
-                            b.p = bin_and_derivs(x1, x2, sp, invp, b.dpdc, b.dpds);
-                            const float u1 = x1 / sp, u2 = x2 / sp;
-                            const float f1 = norm_pdf(u1), f2 = norm_pdf(u2);
-                            b.a = (sp * (f2 - f1) + x2 * b.p) / pbs;
-                            b.dadc = ((u2 * f2 - u1 * f1) - b.p + x2 * b.dpdc) / pbs;
-                            b.dads = ((f2 - f1) + (u2 * u2 * f2 - u1 * u1 * f1) + x2 * b.dpds) / pbs;
+                            const float x2 = (float)(e + 1) * pbs - r.pcr;
+                            b.p = bin_from_edges(E, E2);
+                            b.dpdc = -(f2 - f) * isp;
+                            b.dpds = -(uf2 - uf) * isp;
+                            b.a = fmaf(sp, f2 - f, x2 * b.p) * ipbs;
+                            b.dadc = (((uf2 - uf) - b.p) + x2 * b.dpdc) * ipbs;
+                            b.dads = (((f2 - f) + (uuf2 - uuf)) + x2 * b.dpds) * ipbs;
                         }
                         else {  // point in pitch: one bin, weight (edge_{k+1} - c) / bs
                             b.p = 1.f;
-                            b.a = (pbs - r.pcr) / pbs;
+                            b.a = (pbs - r.pcr) * ipbs;
                             b.dpdc = b.dpds = b.dads = 0.f;
-                            b.dadc = -1.0f / pbs;
+                            b.dadc = -ipbs;
                         }
-                        const int kabs = r.poff + k;
+                        const int kabs = r.poff + e;
                         const int wire = kabs / A.nimp;
                         const int l = kabs - wire * A.nimp;
                         b.base = (l * A.nin + (wire - A.start_ch)) * A.N + col + t0;
                         b.pad = 0;
-                        s_p[wib][kk] = b;
-                    }
-                    __syncwarp();
-                    // cells c = lane + 32 m of the nk x ntc chunk, (k, tau) advanced
-                    // incrementally; kUnroll cells per lane have their loads in flight at once
-                    const int ncell = nk * ntc;
-                    const int dk = 32 / ntc, dt = 32 - dk * ntc;
-                    int k = lane / ntc, tau = lane - k * ntc;
-                    for (int c0 = 0; c0 < ncell; c0 += 32 * kUnroll) {
-                        float D0[kUnroll], D1[kUnroll];
-                        int kk[kUnroll], tt[kUnroll];
-#pragma unroll
-                        for (int u = 0; u < kUnroll; ++u) {
-                            kk[u] = k;
-                            tt[u] = tau;
-                            D0[u] = D1[u] = 0.f;
-                            if (c0 + lane + 32 * u < ncell) {
-                                const float* q = dQp + s_p[wib][k].base + tau;
-                                D0[u] = __ldg(q);
-                                D1[u] = __ldg(q + gstride);
-                            }
-                            tau += dt;
-                            k += dk;
-                            if (tau >= ntc) {
-                                tau -= ntc;
-                                ++k;
-                            }
-                        }
-#pragma unroll
-                        for (int u = 0; u < kUnroll; ++u) {
-                            // cells past the end loaded zeros: they add nothing (kk, tt stay in the tables)
-                            const BinTab b = s_p[wib][min(kk[u], nk - 1)];
-                            const float4 tq = s_t[wib][tt[u]];  // tt < ntc always
-                            const float dd0 = D0[u] - D1[u];
-                            const float uu = fmaf(b.a, dd0, b.p * D1[u]);
-                            const float vc = fmaf(b.dadc, dd0, b.dpdc * D1[u]);
-                            const float vs = fmaf(b.dads, dd0, b.dpds * D1[u]);
-                            acc_qn = fma((double)tq.x, (double)uu, acc_qn);
-                            acc_cp = fma((double)tq.x, (double)vc, acc_cp);
-                            acc_sp = fma((double)tq.x, (double)vs, acc_sp);
-                            acc_ct = fma((double)tq.y, (double)uu, acc_ct);
-                            acc_st = fma((double)tq.z, (double)uu, acc_st);
+                        s_p[wib][e - k0] = b;
+                        if (t0 == 0) {
+                            pS += b.p;
+                            pSc += b.dpdc;
+                            pSs += b.dpds;
                         }
                     }
                 }
+                __syncwarp();
+                // cells c = lane + 32 m of the nk x ntc chunk, (k, tau) advanced
+                // incrementally; kUnroll cells per lane have their loads in flight at once
+                const int ncell = nk * ntc;
+                const int dk = 32 / ntc, dt = 32 - dk * ntc;
+                int k = lane / ntc, tau = lane - k * ntc;
+                for (int c0 = 0; c0 < ncell; c0 += 32 * kUnroll) {
+                    float D0[kUnroll], D1[kUnroll];
+                    int kk[kUnroll], tt[kUnroll];
+#pragma unroll
+                    for (int u = 0; u < kUnroll; ++u) {
+                        kk[u] = min(k, nk - 1);
+                        tt[u] = tau;
+                        D0[u] = D1[u] = 0.f;
+                        if (c0 + lane + 32 * u < ncell) {
+                            const float* q = dQp + s_p[wib][k].base + tau;
+                            D0[u] = __ldg(q);
+                            D1[u] = __ldg(q + gstride);
+                        }
+                        tau += dt;
+                        k += dk;
+                        if (tau >= ntc) {
+                            tau -= ntc;
+                            ++k;
+                        }
+                    }
+                    // cells past the end loaded zeros and add nothing
+                    float pq = 0.f, pc = 0.f, pss = 0.f, pct = 0.f, pst = 0.f;
+#pragma unroll
+                    for (int u = 0; u < kUnroll; ++u) {
+                        const BinTab b = s_p[wib][kk[u]];
+                        const float4 tq = s_t[wib][tt[u]];
+                        const float dd0 = D0[u] - D1[u];
+                        const float uu = fmaf(b.a, dd0, b.p * D1[u]);
+                        const float vc = fmaf(b.dadc, dd0, b.dpdc * D1[u]);
+                        const float vs = fmaf(b.dads, dd0, b.dpds * D1[u]);
+                        pq = fmaf(tq.x, uu, pq);
+                        pc = fmaf(tq.x, vc, pc);
+                        pss = fmaf(tq.x, vs, pss);
+                        pct = fmaf(tq.y, uu, pct);
+                        pst = fmaf(tq.z, uu, pst);
+                    }
+                    acc_qn += (double)pq;
+                    acc_cp += (double)pc;
+                    acc_sp += (double)pss;
+                    acc_ct += (double)pct;
+                    acc_st += (double)pst;
+                }
             }
-            acc_qn = warp_sum_d(acc_qn);
-            acc_cp = warp_sum_d(acc_cp);
-            acc_sp = warp_sum_d(acc_sp);
-            acc_ct = warp_sum_d(acc_ct);
-            acc_st = warp_sum_d(acc_st);
-            const double qn = r.qn;
-            const double gqn = acc_qn;
-            // centres and widths, through qn = q / (Sp * St) as well
-            const double gcp = qn * acc_cp - gqn * (qn / Sp) * dSp_c;
-            const double gsp = qn * acc_sp - gqn * (qn / Sp) * dSp_s;
-            s_ct += qn * acc_ct - gqn * (qn / St) * dSt_c;
-            s_sL += (qn * acc_st - gqn * (qn / St) * dSt_s) / drift_speed;  // sigma_time = extent_long / v
-            s_sT += gsp;                                                       // sigma_pitch = extent_tran
-            s_qf += gqn / ((double)Sp * (double)St);
-            s_px += gcp * A.ax;
-            s_py += gcp * A.ay;
-            s_pz += gcp * A.az;
         }
-        if (any && lane == 0) {
-            // sums over planes; k_adj_drift takes them back through the drift in place
-            double* gd = grad + 7 * (size_t)i;
-            gd[0] = s_ct;
-            gd[1] = s_qf;
-            gd[2] = s_px;
-            gd[3] = s_py;
-            gd[4] = s_pz;
-            gd[5] = s_sL;
-            gd[6] = s_sT;
-        }
+        // normalisation sums (whole warp), then this lane's share of the gradients:
+        // every term is linear in the lane's partial sums, so the warp reduction
+        // waits until all planes are done
+        const float Sp = warp_sum_f(pS), dSp_c = warp_sum_f(pSc), dSp_s = warp_sum_f(pSs);
+        const float St = warp_sum_f(tS), dSt_c = warp_sum_f(tSc), dSt_s = warp_sum_f(tSs);
+        const float iSp = 1.0f / Sp, iSt = 1.0f / St;
+        const double qn = r.qn;
+        // centres and widths, through qn = q / (Sp * St) as well
+        const double gcp = qn * acc_cp - acc_qn * (double)(r.qn * iSp * dSp_c);
+        s_sT += qn * acc_sp - acc_qn * (double)(r.qn * iSp * dSp_s);                  // sigma_pitch = extent_tran
+        s_ct += qn * acc_ct - acc_qn * (double)(r.qn * iSt * dSt_c);
+        s_sL += (qn * acc_st - acc_qn * (double)(r.qn * iSt * dSt_s)) * inv_vd;      // sigma_time = extent_long / v
+        s_qf += acc_qn * (double)(iSp * iSt);
+        s_px += gcp * A.ax;
+        s_py += gcp * A.ay;
+        s_pz += gcp * A.az;
+    }
+    if (!any) return;
+    s_ct = warp_sum_d(s_ct);
+    s_qf = warp_sum_d(s_qf);
+    s_px = warp_sum_d(s_px);
+    s_py = warp_sum_d(s_py);
+    s_pz = warp_sum_d(s_pz);
+    s_sL = warp_sum_d(s_sL);
+    s_sT = warp_sum_d(s_sT);
+    if (lane == 0) {
+        // sums over planes; k_adj_drift takes them back through the drift in place
+        double* gd = grad + 7 * (size_t)i;
+        gd[0] = s_ct;
+        gd[1] = s_qf;
+        gd[2] = s_px;
+        gd[3] = s_py;
+        gd[4] = s_pz;
+        gd[5] = s_sL;
+        gd[6] = s_sT;
     }
 }
 
@@ -395,7 +439,7 @@ void launch_adj_gather(const double* depos, int n, const DriftDev& dd, int do_dr
 {
     if (n <= 0) return;
     const int blocks = (n + kGatherWarps - 1) / kGatherWarps;
-    k_adj_gather<<<blocks, kGatherWarps * 32, 0, s>>>(n, ps, as, drift_speed, rec, dQ, grad);
+    k_adj_gather<<<blocks, kGatherWarps * 32, 0, s>>>(n, ps, as, 1.0 / drift_speed, rec, dQ, grad);
     if (do_drift) k_adj_drift<<<(n + 255) / 256, 256, 0, s>>>(depos, n, dd, grad, gglob);
 }
 
