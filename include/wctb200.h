@@ -198,6 +198,37 @@ int wct_dt_set_profiling(wct_depotransform* dt, int on);
 int wct_dt_stage_times(wct_depotransform* dt, double* ms, long* launches, int nstages, long* total_launches,
                        int reset);
 
+/* ---- Batched events (no counterpart in the reference, which frames one
+ * event per DepoTransform call) ----
+ *
+ * DepoTransform::operator() over nevents events at once: event e holds depos
+ * [offsets[e], offsets[e+1]) of d_depos ([offsets[nevents]][7], device) and
+ * its frame is d_frames + e * nrows * nticks (device).  Each frame equals the
+ * frame of wct_dt_forward_device for that event within floating-point
+ * rounding (time FFT lengths come from a fixed ladder instead of each
+ * window's own length).  The windows of all events are planned on the device,
+ * so the whole batch runs as one CUDA graph, captured on the first call and
+ * replayed while the offsets, buffers, stream, launch shapes and drift
+ * parameters stay the same.  windows: [nevents][nplanes] or NULL; frame
+ * idents are first_ident .. first_ident + nevents - 1.  Returns after the
+ * batch completes.  offsets is a host array of nevents + 1 values with
+ * offsets[0] = 0. */
+int wct_dt_forward_batch_device(wct_depotransform* dt, const double* d_depos, const long long* offsets, int nevents,
+                                float* d_frames, wct_plane_window* windows, int* first_ident, void* stream);
+/* The same on host buffers (frames [nevents][nrows][nticks]). */
+int wct_dt_forward_batch(wct_depotransform* dt, const double* depos, const long long* offsets, int nevents,
+                         float* frames, wct_plane_window* windows, int* first_ident);
+/* Launch shapes of the batched path: params[5] = {events per pass, persistent
+ * raster blocks per SM, threads per time-FFT row (128..1024, power of 2),
+ * time-FFT blocks per SM, wire-convolution blocks per SM}; set != 0 sets them,
+ * otherwise they are read. */
+int wct_dt_batch_tune(wct_depotransform* dt, int* params, int set);
+/* Autotuner: times candidate launch shapes on the given batch (device
+ * buffers as for wct_dt_forward_batch_device), keeps the fastest and writes a
+ * JSON report of every candidate and its time to report (may be NULL). */
+int wct_dt_autotune_batch(wct_depotransform* dt, const double* d_depos, const long long* offsets, int nevents,
+                          float* d_frames, void* stream, char* report, size_t len);
+
 /* Reverse-mode derivative of wct_dt_forward (no counterpart in the reference,
  * whose DepoTransform is forward only).  Given grad_frame = dL/d(frame)
  * [nrows][nticks] for the same depos, writes grad_depos[i][k] = dL/d(depos[i][k])

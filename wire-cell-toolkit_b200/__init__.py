@@ -95,6 +95,13 @@ SIGNATURES = {
     "wct_dt_set_drift_params": (C.c_int, [C.c_void_p, C.c_double, C.c_double, C.c_double]),
     "wct_dt_get_drift_params": (C.c_int, [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_double),
                                           C.POINTER(C.c_double)]),
+    "wct_dt_forward_batch_device": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p,
+                                              C.POINTER(C.c_int), C.c_void_p]),
+    "wct_dt_forward_batch": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p,
+                                       C.POINTER(C.c_int)]),
+    "wct_dt_batch_tune": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int]),
+    "wct_dt_autotune_batch": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p,
+                                        C.c_char_p, C.c_size_t]),
     "wct_dt_destroy": (C.c_int, [C.c_void_p]),
 }
 
@@ -298,6 +305,62 @@ class DepoTransform:
                                            C.c_void_p(d_grad_depos_ptr),
                                            C.c_void_p(d_grad_drift_ptr) if d_grad_drift_ptr else None,
                                            _dt_stream(stream)))
+
+    def forward_batch(self, events, out=None):
+        """Host-buffer batch: ``events`` is a list of [n_e][7] depo arrays.  Returns
+        (frames [nevents][nrows][nticks] float32, windows per event, first ident)."""
+        evs = [np.ascontiguousarray(e, dtype=np.float64).reshape(-1, 7) for e in events]
+        offsets = np.zeros(len(evs) + 1, dtype=np.int64)
+        offsets[1:] = np.cumsum([len(e) for e in evs])
+        d = np.concatenate(evs) if offsets[-1] else np.zeros((1, 7))
+        nrows, nticks = self.frame_shape()
+        if out is None:
+            out = np.empty((len(evs), nrows, nticks), dtype=np.float32)
+        assert out.shape == (len(evs), nrows, nticks) and out.dtype == np.float32 and out.flags.c_contiguous
+        wins = (PlaneWindow * max(1, len(evs) * len(self.planes)))()
+        ident = C.c_int()
+        _check(lib().wct_dt_forward_batch(self.h, d.ctypes.data, offsets.ctypes.data, len(evs), out.ctypes.data,
+                                          C.cast(wins, C.c_void_p), C.byref(ident)))
+        npl = len(self.planes)
+        w = [[wins[e * npl + i].as_dict() for i in range(npl)] for e in range(len(evs))]
+        return out, w, ident.value
+
+    def forward_batch_device(self, d_depos_ptr, offsets, d_frames_ptr, stream=None, windows=False):
+        """Device-buffer batch (one CUDA graph); ``offsets`` host int64 [nevents + 1]."""
+        off = np.ascontiguousarray(offsets, dtype=np.int64)
+        nev = len(off) - 1
+        npl = len(self.planes)
+        wins = (PlaneWindow * max(1, nev * npl))() if windows else None
+        ident = C.c_int()
+        _check(lib().wct_dt_forward_batch_device(self.h, C.c_void_p(d_depos_ptr), off.ctypes.data, nev,
+                                                 C.c_void_p(d_frames_ptr),
+                                                 C.cast(wins, C.c_void_p) if windows else None, C.byref(ident),
+                                                 _dt_stream(stream)))
+        if windows:
+            return [[wins[e * npl + i].as_dict() for i in range(npl)] for e in range(nev)], ident.value
+        return None, ident.value
+
+    BATCH_TUNE_KEYS = ("slots", "raster_per_sm", "fft_threads", "fft_per_sm", "conv_per_sm")
+
+    def batch_tune(self, **kw):
+        """Read (no arguments) or change the launch shapes of the batched path."""
+        p = (C.c_int * 5)()
+        _check(lib().wct_dt_batch_tune(self.h, p, 0))
+        cur = dict(zip(self.BATCH_TUNE_KEYS, list(p)))
+        if kw:
+            cur.update(kw)
+            for i, k in enumerate(self.BATCH_TUNE_KEYS):
+                p[i] = int(cur[k])
+            _check(lib().wct_dt_batch_tune(self.h, p, 1))
+        return cur
+
+    def autotune_batch(self, d_depos_ptr, offsets, d_frames_ptr, stream=None):
+        """Autotune the batched path on this batch; returns the report (dict)."""
+        off = np.ascontiguousarray(offsets, dtype=np.int64)
+        buf = C.create_string_buffer(1 << 16)
+        _check(lib().wct_dt_autotune_batch(self.h, C.c_void_p(d_depos_ptr), off.ctypes.data, len(off) - 1,
+                                           C.c_void_p(d_frames_ptr), _dt_stream(stream), buf, len(buf)))
+        return json.loads(buf.value.decode())
 
     def set_drift_params(self, DL, DT, lifetime):
         _check(lib().wct_dt_set_drift_params(self.h, float(DL), float(DT), float(lifetime)))

@@ -10,6 +10,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <functional>
 #include <map>
 #include <memory>
 #include <mutex>
@@ -176,6 +177,8 @@ struct Core {
     // workspace
     DevBuf d_rec, d_win, d_Q, d_V, d_depos, d_frame, d_wcnt, d_woff, d_wcur, d_wlist, d_tprof, d_kbound;
     DevBuf d_gframe, d_gdep, d_gglob;  // adjoint host entry point
+    int config_gen{0};                 // bumped by every change of planes or responses
+    std::unique_ptr<struct BatchState> batch;
     WindowDev* h_win{nullptr};
     size_t last_n{0};
     // stage profiling
@@ -247,7 +250,8 @@ struct Core {
         for (auto& p : planes) n += p->desc.nwires;
         return n;
     }
-    ~Core()
+    ~Core();
+    void destroy()
     {
         harvest();
         for (auto e : event_pool) cudaEventDestroy(e);
@@ -403,6 +407,8 @@ __global__ void k_win_init(WindowDev* w, int n)
 // stored between the two).
 struct EventPlan {
     int n{0}, np{0}, nticks{0};
+    int nkeys{0};
+    EventTable et{};
     TimeDev tb{};
     PlaneSet pset{};
     GridSet gset{};
@@ -442,6 +448,7 @@ static int prepare_event(Core& c, const double* d_depos, size_t ndepos, cudaStre
     pset.nwires_total = nwt;
     pset.ntiles = (nticks + kTile - 1) / kTile;
     const int nkeys = nwt * pset.ntiles;
+    ev.nkeys = nkeys;
 
     CUDA_TRY(c.d_rec.ensure(sizeof(PatchRec) * (size_t)np * std::max(n, 1)));
     CUDA_TRY(c.d_tprof.ensure(sizeof(float) * kTprof * (size_t)std::max(n, 1)));
@@ -461,7 +468,13 @@ static int prepare_event(Core& c, const double* d_depos, size_t ndepos, cudaStre
     CUDA_TRY(c.d_kbound.ensure(sizeof(unsigned long long) * (size_t)nkeys * kTileBlocks));
     CUDA_TRY(cudaMemsetAsync(c.d_kbound.p, 0, sizeof(unsigned long long) * (size_t)nkeys * kTileBlocks, s));
     k_win_init<<<1, 64, 0, s>>>(c.d_win.as<WindowDev>(), np);
-    launch_prep_all(d_depos, n, c.drifter, c.have_drifter ? 1 : 0, pset, tb, c.drift_speed, c.nsigma,
+    EventTable& et = ev.et;
+    et.nev = 1;
+    et.dep0[0] = 0;
+    et.dep0[1] = n;
+    et.blk0[0] = 0;
+    et.blk0[1] = (n + 255) / 256;
+    launch_prep_all(d_depos, et, nkeys, c.drifter, c.have_drifter ? 1 : 0, pset, tb, c.drift_speed, c.nsigma,
                     c.d_rec.as<PatchRec>(), c.d_win.as<WindowDev>(), c.d_wcnt.as<int>(), c.d_tprof.as<float>(),
                     c.d_kbound.as<unsigned long long>(), s);
     launch_scan(c.d_wcnt.as<int>(), nkeys, c.d_woff.as<int>(), c.d_wcur.as<int>(), s);
@@ -538,9 +551,11 @@ static int forward_device(Core& c, const double* d_depos, size_t ndepos, float* 
     CUDA_TRY(cudaMemsetAsync(d_frame, 0, sizeof(float) * (size_t)c.nrows() * nticks, s));
 
     Core::StageTimer t_r(&c, 1, s);
-    launch_fill(c.d_rec.as<PatchRec>(), n, pset, c.d_wcur.as<int>(), c.d_wlist.as<Visit>(), s);
+    launch_fill(c.d_rec.as<PatchRec>(), ev.et, ev.nkeys, pset, c.d_wcur.as<int>(), c.d_wlist.as<Visit>(),
+                (long long)std::max(total_visits, 1), s);
     launch_raster_wires(c.d_rec.as<PatchRec>(), c.d_tprof.as<float>(), c.d_wcnt.as<int>(), c.d_woff.as<int>(),
-                        c.d_wlist.as<Visit>(), c.d_kbound.as<unsigned long long>(), gset, c.d_Q.as<float>(), s);
+                        c.d_wlist.as<Visit>(), (long long)std::max(total_visits, 1),
+                        c.d_kbound.as<unsigned long long>(), gset, c.d_Q.as<float>(), s);
     t_r.close((n > 0 ? 1 : 0) + (rows > 0 ? 1 : 0));
     CUDA_TRY(cudaGetLastError());
 
@@ -741,6 +756,449 @@ static int noalloc_scratch(float2** out)
     return WCT_OK;
 }
 
+// ---------------------------------------------------------------------------
+// Batched events.  The whole batch -- every pass of up to `slots` events
+// through prep, scan, device planning, fill and the persistent raster,
+// time-FFT, wire-convolution and inverse kernels -- is captured once as a
+// CUDA graph and replayed while the batch shape, buffers and drift
+// parameters stay the same.  Time FFTs use a fixed ladder of lengths (about
+// 10% apart) so that the response spectra of every length are ready before
+// the graph runs.
+// ---------------------------------------------------------------------------
+struct BatchState {
+    int gen{-1};  // Core::config_gen of the setup
+    BatchStatic bs{};
+    std::vector<std::unique_ptr<FftPlanDev>> cls_plans;
+    DevBuf d_descs;
+    std::vector<std::unique_ptr<DevBuf>> spec;  // [plane * ncls + cls]
+    DevBuf d_spec_tab;                          // const float2* [plane][ncls]
+    int maxM{0}, maxG{0}, nsm{148};
+    DevBuf d_Q, d_V, d_rec, d_tprof, d_win, d_wcnt, d_woff, d_wcur, d_kbound, d_wlist, d_plans;
+    long long vcap{0};
+    BatchPlan* h_plans{nullptr};
+    size_t h_plans_n{0};
+    BatchTune tune{16, 3, 512, 3, 3};
+    // the instantiated graph and what it was captured for
+    cudaGraphExec_t exec{nullptr};
+    const void* g_depos{nullptr};
+    void* g_frames{nullptr};
+    std::vector<long long> g_offsets;
+    BatchTune g_tune{};
+    long long g_vcap{0};
+    cudaStream_t g_stream{nullptr};
+    DriftDev g_drift{};
+    std::vector<void*> g_bufs;
+    void drop_graph()
+    {
+        if (exec) cudaGraphExecDestroy(exec);
+        exec = nullptr;
+    }
+    ~BatchState()
+    {
+        drop_graph();
+        if (h_plans) cudaFreeHost(h_plans);
+    }
+};
+
+Core::~Core()
+{
+    batch.reset();
+    destroy();
+}
+
+static int batch_setup(Core& c)
+{
+    if (!c.batch) c.batch = std::make_unique<BatchState>();
+    BatchState& b = *c.batch;
+    if (b.gen == c.config_gen) return WCT_OK;
+    b.drop_graph();
+    const int np = (int)c.planes.size();
+    BatchStatic& bs = b.bs;
+    bs = BatchStatic{};
+    bs.np = np;
+    bs.nticks = c.nticks();
+    bs.ntiles = (bs.nticks + kTile - 1) / kTile;
+    int nwt = 0, minpad = 1 << 30;
+    size_t nneed = 0;
+    for (auto& ps : c.planes) {
+        nwt += ps->desc.nwires;
+        minpad = std::min(minpad, ps->waveform_pad);
+        // longest reference time window: end_tick - start_tick <= nticks + 4
+        nneed = std::max(nneed, fft_best_length((size_t)bs.nticks + 4 + ps->waveform_pad, false));
+    }
+    bs.nkeys = nwt * bs.ntiles;
+    bs.start_time = c.start_time;
+    bs.tbs = (c.start_time + c.readout_time - c.start_time) / (int)(c.readout_time / c.tick);
+    // ladder of time-FFT lengths from the shortest possible window up
+    std::vector<int> cls;
+    const int nfirst = gpu_fft_length(std::max(64, (int)fft_best_length((size_t)4 + std::max(minpad, 0), false)));
+    for (double ratio = 1.1;; ratio *= 1.05) {
+        cls.clear();
+        int N = nfirst;
+        for (;;) {
+            cls.push_back(N);
+            if ((size_t)N >= nneed) break;
+            N = gpu_fft_length(std::max((int)std::ceil(N * ratio), N + 4));
+        }
+        if ((int)cls.size() <= kMaxClasses) break;
+    }
+    bs.ncls = (int)cls.size();
+    for (int k = 0; k < bs.ncls; ++k) bs.cls_N[k] = cls[k];
+    b.maxM = cls.back() / 2;
+    b.cls_plans.clear();
+    std::vector<FftDesc> descs;
+    for (int N : cls) {
+        auto pl = std::make_unique<FftPlanDev>();
+        int rc = make_plan(N / 2, *pl);
+        if (rc) return rc;
+        descs.push_back(pl->desc);
+        b.cls_plans.push_back(std::move(pl));
+    }
+    CUDA_TRY(b.d_descs.ensure(sizeof(FftDesc) * descs.size()));
+    CUDA_TRY(cudaMemcpy(b.d_descs.p, descs.data(), sizeof(FftDesc) * descs.size(), cudaMemcpyHostToDevice));
+    long long q = 0, v = 0;
+    b.maxG = 0;
+    b.spec.clear();
+    std::vector<const float2*> tab((size_t)np * bs.ncls);
+    for (int ip = 0; ip < np; ++ip) {
+        PlaneState& ps = *c.planes[ip];
+        BatchPlaneStatic& pl = bs.pl[ip];
+        pl.G = ps.G;
+        pl.npad = ps.npad;
+        pl.waveform_pad = ps.waveform_pad;
+        pl.nwires = ps.desc.nwires;
+        pl.imp_nbins = ps.dev.imp_nbins;
+        pl.row0 = ps.row0;
+        pl.nin_max = ps.desc.nwires + 4;  // end_ch - start_ch of any window
+        pl.imp_min = ps.dev.imp_min;
+        pl.imp_bs = ps.dev.imp_bs;
+        pl.qslot = q;
+        pl.vslot = v;
+        q += (long long)ps.G * pl.nin_max * cls.back();
+        v += (long long)(pl.nin_max + 2 * ps.npad) * b.maxM;
+        b.maxG = std::max(b.maxG, ps.G);
+        const int rows = ps.G * (2 * ps.npad + 1);
+        for (int k = 0; k < bs.ncls; ++k) {
+            const int N = cls[k];
+            auto sp = std::make_unique<DevBuf>();
+            CUDA_TRY(sp->ensure(sizeof(float2) * (size_t)rows * (N / 2)));
+            launch_rfft_rows(ps.d_table.as<float>(), ps.ldr, std::min(ps.nresp, N), sp->as<float2>(), N / 2, rows,
+                             b.cls_plans[k]->desc, c.own_stream);
+            CUDA_TRY(cudaGetLastError());
+            tab[(size_t)ip * bs.ncls + k] = sp->as<float2>();
+            b.spec.push_back(std::move(sp));
+        }
+    }
+    bs.qslot_total = q;
+    bs.vslot_total = v;
+    CUDA_TRY(b.d_spec_tab.ensure(sizeof(const float2*) * tab.size()));
+    CUDA_TRY(cudaMemcpyAsync(b.d_spec_tab.p, tab.data(), sizeof(const float2*) * tab.size(), cudaMemcpyHostToDevice,
+                             c.own_stream));
+    CUDA_TRY(cudaStreamSynchronize(c.own_stream));
+    CUDA_TRY(cudaDeviceGetAttribute(&b.nsm, cudaDevAttrMultiProcessorCount, c.device));
+    batch_kernel_attributes(b.maxG, b.maxM);
+    CUDA_TRY(cudaGetLastError());
+    b.gen = c.config_gen;
+    return WCT_OK;
+}
+
+// Device bytes of one event slot (charge grids, V rows, per-event keys).
+static size_t batch_slot_bytes(const BatchState& b)
+{
+    const BatchStatic& bs = b.bs;
+    return sizeof(float) * (size_t)bs.qslot_total + sizeof(float2) * (size_t)bs.vslot_total +
+           (sizeof(int) * 3 + sizeof(unsigned long long) * kTileBlocks) * (size_t)bs.nkeys;
+}
+
+static int batch_slots(Core& c, int nev)
+{
+    BatchState& b = *c.batch;
+    int K = std::max(1, std::min({b.tune.slots, kMaxBatch, nev}));
+    size_t fre = 0, tot = 0;
+    if (cudaMemGetInfo(&fre, &tot) == cudaSuccess) {
+        // keep the arenas within about half of what is free (plus what they hold already)
+        const size_t held = b.d_Q.n + b.d_V.n;
+        const size_t budget = (fre + held) / 2;
+        const size_t per = std::max<size_t>(batch_slot_bytes(b), 1);
+        K = std::max(1, std::min<int>(K, (int)(budget / per)));
+    }
+    return K;
+}
+
+static int forward_batch_device(Core& c, const double* d_depos, const long long* offsets, int nev, float* d_frames,
+                                wct_plane_window* wins, int* first_ident, cudaStream_t s)
+{
+    if (c.planes.empty()) return fail(WCT_ERR_STATE, "no planes configured");
+    if ((int)c.planes.size() > kMaxPlanes) return fail(WCT_ERR_CONFIG, "too many planes for one component");
+    for (auto& p : c.planes)
+        if (!p->have_resp) return fail(WCT_ERR_STATE, "a plane has no response");
+    if (nev < 0 || !offsets || (nev > 0 && !d_frames)) return fail(WCT_ERR_ARG, "forward batch: bad arguments");
+    if (offsets[0] != 0) return fail(WCT_ERR_ARG, "forward batch: offsets[0] must be 0");
+    for (int e = 0; e < nev; ++e)
+        if (offsets[e + 1] < offsets[e]) return fail(WCT_ERR_ARG, "forward batch: offsets must not decrease");
+    if (nev > 0 && offsets[nev] > 0 && !d_depos) return fail(WCT_ERR_ARG, "forward batch: null depos");
+    if (first_ident) *first_ident = c.frame_count;
+    if (nev == 0) return WCT_OK;
+    CUDA_TRY(cudaSetDevice(c.device));
+    int rc = batch_setup(c);
+    if (rc) return rc;
+    BatchState& b = *c.batch;
+    const BatchStatic& bs = b.bs;
+    const int np = bs.np;
+    const int K = batch_slots(c, nev);
+    const int nch = (nev + K - 1) / K;
+    long long maxdep = 1;
+    for (int c0 = 0; c0 < nev; c0 += K) {
+        const int c1 = std::min(nev, c0 + K);
+        maxdep = std::max(maxdep, offsets[c1] - offsets[c0]);
+    }
+    if (maxdep > 0x7fffff00LL) return fail(WCT_ERR_SIZE, "forward batch: too many depos in one pass");
+    const long long fstride = (long long)c.nrows() * bs.nticks;
+    const long long est = 6LL * np * maxdep + 4096;
+    if (b.vcap < est) b.vcap = est;
+    PlaneSet pset{};
+    pset.nplanes = np;
+    {
+        int nwt = 0;
+        for (int ip = 0; ip < np; ++ip) {
+            pset.p[ip] = c.planes[ip]->dev;
+            pset.p[ip].wire_base = nwt;
+            nwt += c.planes[ip]->desc.nwires;
+        }
+        pset.nwires_total = nwt;
+        pset.ntiles = bs.ntiles;
+    }
+    TimeDev tb;
+    tb.nbins = bs.nticks;
+    tb.tmin = c.start_time;
+    tb.tmax = c.start_time + c.readout_time;
+    tb.bs = (tb.tmax - tb.tmin) / tb.nbins;
+    const long long nkeysK = (long long)K * bs.nkeys;
+
+    for (int attempt = 0; attempt < 3; ++attempt) {
+        std::vector<void*> before = {b.d_Q.p, b.d_V.p, b.d_rec.p, b.d_tprof.p, b.d_win.p, b.d_wcnt.p, b.d_woff.p,
+                                     b.d_wcur.p, b.d_kbound.p, b.d_wlist.p, b.d_plans.p};
+        CUDA_TRY(b.d_Q.ensure(sizeof(float) * (size_t)bs.qslot_total * K));
+        CUDA_TRY(b.d_V.ensure(sizeof(float2) * (size_t)bs.vslot_total * K));
+        CUDA_TRY(b.d_rec.ensure(sizeof(PatchRec) * (size_t)np * maxdep));
+        CUDA_TRY(b.d_tprof.ensure(sizeof(float) * kTprof * (size_t)maxdep));
+        CUDA_TRY(b.d_win.ensure(sizeof(WindowDev) * (size_t)K * np));
+        CUDA_TRY(b.d_wcnt.ensure(sizeof(int) * (size_t)(nkeysK + 1)));
+        CUDA_TRY(b.d_woff.ensure(sizeof(int) * (size_t)(nkeysK + 1)));
+        CUDA_TRY(b.d_wcur.ensure(sizeof(int) * (size_t)(nkeysK + 1 + (nkeysK + 1023) / 1024)));
+        CUDA_TRY(b.d_kbound.ensure(sizeof(unsigned long long) * (size_t)nkeysK * kTileBlocks));
+        CUDA_TRY(b.d_wlist.ensure(sizeof(Visit) * (size_t)b.vcap));
+        CUDA_TRY(b.d_plans.ensure(sizeof(BatchPlan) * (size_t)nch));
+        std::vector<void*> after = {b.d_Q.p, b.d_V.p, b.d_rec.p, b.d_tprof.p, b.d_win.p, b.d_wcnt.p, b.d_woff.p,
+                                    b.d_wcur.p, b.d_kbound.p, b.d_wlist.p, b.d_plans.p};
+        if (b.h_plans_n < (size_t)nch) {
+            if (b.h_plans) cudaFreeHost(b.h_plans);
+            b.h_plans = nullptr;
+            CUDA_TRY(cudaMallocHost(&b.h_plans, sizeof(BatchPlan) * (size_t)nch));
+            b.h_plans_n = nch;
+        }
+        const bool same = b.exec && before == after && after == b.g_bufs && b.g_depos == d_depos &&
+                          b.g_frames == d_frames && b.g_stream == s && b.g_vcap == b.vcap &&
+                          std::memcmp(&b.g_tune, &b.tune, sizeof(BatchTune)) == 0 &&
+                          std::memcmp(&b.g_drift, &c.drifter, sizeof(DriftDev)) == 0 &&
+                          b.g_offsets.size() == (size_t)nev + 1 &&
+                          std::equal(b.g_offsets.begin(), b.g_offsets.end(), offsets);
+        if (!same) {
+            b.drop_graph();
+            cudaGraph_t graph = nullptr;
+            CUDA_TRY(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+            BatchPlan* plans = b.d_plans.as<BatchPlan>();
+            const int nb_r = std::max(1, b.nsm * b.tune.raster_per_sm);
+            const int nb_f = std::max(1, b.nsm * b.tune.fft_per_sm);
+            const int nb_c = std::max(1, b.nsm * b.tune.conv_per_sm);
+            for (int ch = 0; ch < nch; ++ch) {
+                const int c0 = ch * K, c1 = std::min(nev, c0 + K), ne = c1 - c0;
+                EventTable et{};
+                et.nev = ne;
+                int blk = 0;
+                for (int j = 0; j <= ne; ++j) {
+                    et.dep0[j] = (int)(offsets[c0 + j] - offsets[c0]);
+                    et.blk0[j] = blk;
+                    if (j < ne) blk += (int)((offsets[c0 + j + 1] - offsets[c0 + j] + 255) / 256);
+                }
+                const long long nk = (long long)ne * bs.nkeys;
+                const double* dep = d_depos ? d_depos + 7 * offsets[c0] : nullptr;
+                cudaMemsetAsync(b.d_wcnt.p, 0, sizeof(int) * (size_t)(nk + 1), s);
+                cudaMemsetAsync(b.d_kbound.p, 0, sizeof(unsigned long long) * (size_t)nk * kTileBlocks, s);
+                k_win_init<<<(ne * np + 63) / 64, 64, 0, s>>>(b.d_win.as<WindowDev>(), ne * np);
+                launch_prep_all(dep, et, bs.nkeys, c.drifter, c.have_drifter ? 1 : 0, pset, tb, c.drift_speed,
+                                c.nsigma, b.d_rec.as<PatchRec>(), b.d_win.as<WindowDev>(), b.d_wcnt.as<int>(),
+                                b.d_tprof.as<float>(), b.d_kbound.as<unsigned long long>(), s);
+                launch_scan(b.d_wcnt.as<int>(), (int)nk, b.d_woff.as<int>(), b.d_wcur.as<int>(), s);
+                launch_plan_batch(plans + ch, bs, ne, b.d_win.as<WindowDev>(), b.d_woff.as<int>() + nk, b.vcap, s);
+                launch_fill(b.d_rec.as<PatchRec>(), et, bs.nkeys, pset, b.d_wcur.as<int>(), b.d_wlist.as<Visit>(),
+                            b.vcap, s);
+                cudaMemsetAsync(d_frames + c0 * fstride, 0, sizeof(float) * (size_t)(ne * fstride), s);
+                launch_raster_batch(plans + ch, bs, pset, b.d_rec.as<PatchRec>(), et.dep0[ne], b.d_tprof.as<float>(),
+                                    b.d_wcnt.as<int>(), b.d_woff.as<int>(), b.d_wlist.as<Visit>(), b.vcap,
+                                    b.d_kbound.as<unsigned long long>(), b.d_Q.as<float>(), nb_r, b.maxG, s);
+                launch_rfft_batch(plans + ch, b.d_descs.as<FftDesc>(), b.d_Q.as<float>(), nb_f, b.tune.fft_threads,
+                                  b.maxM, s);
+                for (int ip = 0; ip < np; ++ip)
+                    launch_conv_batch(plans + ch, bs, ip, c.planes[ip]->mirror,
+                                      b.d_spec_tab.as<const float2*>() + (size_t)ip * bs.ncls, b.d_Q.as<float>(),
+                                      b.d_V.as<float2>(), nb_c, s);
+                launch_irfft_batch(plans + ch, bs, b.d_descs.as<FftDesc>(), b.d_V.as<float2>(), d_frames + c0 * fstride,
+                                   fstride, nb_f, b.tune.fft_threads, b.maxM, s);
+            }
+            cudaError_t ce = cudaStreamEndCapture(s, &graph);
+            if (ce != cudaSuccess) {
+                if (graph) cudaGraphDestroy(graph);
+                return fail(WCT_ERR_CUDA, std::string("forward batch: graph capture: ") + cudaGetErrorString(ce));
+            }
+            ce = cudaGraphInstantiate(&b.exec, graph, 0);
+            cudaGraphDestroy(graph);
+            if (ce != cudaSuccess) {
+                b.exec = nullptr;
+                return fail(WCT_ERR_CUDA, std::string("forward batch: graph instantiate: ") + cudaGetErrorString(ce));
+            }
+            b.g_bufs = after;
+            b.g_depos = d_depos;
+            b.g_frames = d_frames;
+            b.g_stream = s;
+            b.g_vcap = b.vcap;
+            b.g_tune = b.tune;
+            b.g_drift = c.drifter;
+            b.g_offsets.assign(offsets, offsets + nev + 1);
+        }
+        CUDA_TRY(cudaGraphLaunch(b.exec, s));
+        // statuses (and windows when asked for) of every pass
+        const size_t head = offsetof(BatchPlan, pre_raster);
+        for (int ch = 0; ch < nch; ++ch) {
+            const size_t bytes = wins ? sizeof(BatchPlan) : head;
+            CUDA_TRY(cudaMemcpyAsync(b.h_plans + ch, b.d_plans.as<BatchPlan>() + ch, bytes, cudaMemcpyDeviceToHost, s));
+        }
+        CUDA_TRY(cudaStreamSynchronize(s));
+        int st = 0;
+        long long need = 0;
+        for (int ch = 0; ch < nch; ++ch) {
+            st |= b.h_plans[ch].status;
+            need = std::max<long long>(need, b.h_plans[ch].total_visits);
+        }
+        if (st & kBatchVisitOverflow) {
+            b.vcap = need + need / 4 + 4096;  // grow the visit list and run again
+            continue;
+        }
+        if (st & kBatchOversize) return fail(WCT_ERR_SIZE, "a diffusion patch exceeds 1024 ticks or 1024 impact bins");
+        if (st & kBatchBigCharge) return fail(WCT_ERR_SIZE, "a depo charge exceeds 5e11 electrons");
+        if (st & kBatchNoClass) return fail(WCT_ERR_SIZE, "forward batch: a window exceeds the time-FFT ladder");
+        if (wins) {
+            for (int e = 0; e < nev; ++e) {
+                const BatchPlan& P = b.h_plans[e / K];
+                for (int ip = 0; ip < np; ++ip) {
+                    const EvPlane& E = P.ep[(e % K) * np + ip];
+                    const PlaneState& ps = *c.planes[ip];
+                    wct_plane_window& o = wins[(size_t)e * np + ip];
+                    o.face = ps.face;
+                    o.plane = ps.index;
+                    o.start_ch = E.m_start_ch;
+                    o.end_ch = E.m_end_ch;
+                    o.start_tick = E.m_start_tick;
+                    o.end_tick = E.m_end_tick;
+                    o.nw_fft = E.nw_ref;
+                    o.nt_fft = E.nt_ref;
+                    o.nt_gpu = E.N;
+                    o.charge_rows = E.end_ch - E.start_ch;
+                    o.npad = ps.npad;
+                    o.ndepos_added = E.ndepos_added;
+                    o.outside_time = E.outside_time;
+                    o.outside_pitch = E.outside_pitch;
+                }
+            }
+        }
+        c.frame_count += nev;
+        return WCT_OK;
+    }
+    return fail(WCT_ERR_SIZE, "forward batch: visit lists kept overflowing");
+}
+
+// Coordinate search over the launch shapes of the batched path on the
+// caller's batch: each candidate is captured, run once, then timed over three
+// graph replays (CUDA events on the stream); the fastest is kept.
+static int autotune_batch(Core& c, const double* d_depos, const long long* offsets, int nev, float* d_frames,
+                          cudaStream_t s, std::string& report)
+{
+    if (nev <= 0) return fail(WCT_ERR_ARG, "autotune: empty batch");
+    int rc = batch_setup(c);
+    if (rc) return rc;
+    BatchState& b = *c.batch;
+    cudaEvent_t e0, e1;
+    CUDA_TRY(cudaEventCreate(&e0));
+    CUDA_TRY(cudaEventCreate(&e1));
+    auto measure = [&](float& ms) -> int {
+        int r = forward_batch_device(c, d_depos, offsets, nev, d_frames, nullptr, nullptr, s);
+        if (r) return r;
+        float best = 1e30f;
+        for (int k = 0; k < 3; ++k) {
+            cudaEventRecord(e0, s);
+            r = forward_batch_device(c, d_depos, offsets, nev, d_frames, nullptr, nullptr, s);
+            if (r) return r;
+            cudaEventRecord(e1, s);
+            cudaEventSynchronize(e1);
+            float t = 0.f;
+            cudaEventElapsedTime(&t, e0, e1);
+            best = std::min(best, t);
+        }
+        ms = best;
+        return WCT_OK;
+    };
+    std::string rows;
+    auto note = [&](const BatchTune& t, float ms) {
+        char buf[200];
+        std::snprintf(buf, sizeof buf,
+                      "%s{\"slots\": %d, \"raster_per_sm\": %d, \"fft_threads\": %d, \"fft_per_sm\": %d, "
+                      "\"conv_per_sm\": %d, \"ms\": %.4f}",
+                      rows.empty() ? "" : ", ", t.slots, t.raster_per_sm, t.fft_threads, t.fft_per_sm, t.conv_per_sm,
+                      ms);
+        rows += buf;
+    };
+    BatchTune best = b.tune;
+    float best_ms = 0.f;
+    rc = measure(best_ms);
+    if (rc) return rc;
+    note(best, best_ms);
+    const std::vector<std::vector<int>> cand = {
+        {4, 8, 16, 32, 64}, {2, 3, 4, 6}, {256, 512}, {2, 3, 4}, {2, 3, 4}};
+    for (int par = 0; par < 5; ++par) {
+        for (int v : cand[par]) {
+            BatchTune t = best;
+            int* f[5] = {&t.slots, &t.raster_per_sm, &t.fft_threads, &t.fft_per_sm, &t.conv_per_sm};
+            if (*f[par] == v) continue;
+            if (par == 0 && v > std::max(nev, 4)) continue;
+            *f[par] = v;
+            b.tune = t;
+            float ms = 0.f;
+            rc = measure(ms);
+            if (rc) {
+                b.tune = best;
+                cudaEventDestroy(e0);
+                cudaEventDestroy(e1);
+                return rc;
+            }
+            note(t, ms);
+            if (ms < best_ms) {
+                best_ms = ms;
+                best = t;
+            }
+        }
+    }
+    b.tune = best;
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    char buf[200];
+    std::snprintf(buf, sizeof buf,
+                  "{\"best\": {\"slots\": %d, \"raster_per_sm\": %d, \"fft_threads\": %d, \"fft_per_sm\": %d, "
+                  "\"conv_per_sm\": %d, \"ms\": %.4f}, \"tried\": [",
+                  best.slots, best.raster_per_sm, best.fft_threads, best.fft_per_sm, best.conv_per_sm, best_ms);
+    report = std::string(buf) + rows + "]}";
+    return WCT_OK;
+}
+
 }  // namespace wctb200
 
 using namespace wctb200;
@@ -918,6 +1376,7 @@ int wct_dt_add_plane(wct_depotransform* h, int face, const wct_plane_desc* d, in
     if (d->nwires < 2 || d->nimpacts < 2 || (d->nimpacts % 2))
         return fail(WCT_ERR_CONFIG, "need >= 2 wires and an even number of impacts per wire");
     Core& c = h->core;
+    ++c.config_gen;
     auto ps = std::make_unique<PlaneState>();
     ps->face = face;
     ps->index = (int)c.faces[face].planes.size();
@@ -1003,6 +1462,7 @@ int wct_dt_set_response_table(wct_depotransform* h, int face, int plane, int ngr
     ps->mirror = mirror;
     ps->spec_N = 0;
     ps->have_resp = true;
+    ++h->core.config_gen;
     return WCT_OK;
 }
 
@@ -1130,6 +1590,101 @@ int wct_dt_get_drift_params(const wct_depotransform* h, double* DL, double* DT, 
     if (DL) *DL = c.drifter.DL;
     if (DT) *DT = c.drifter.DT;
     if (lifetime) *lifetime = c.drifter.lifetime;
+    return WCT_OK;
+}
+
+// Graphs cannot be captured on the legacy or per-thread default stream: run
+// on the component's own stream, ordered after and before the caller's.
+static int on_capturable_stream(Core& c, cudaStream_t s, const std::function<int(cudaStream_t)>& f)
+{
+    if (s != nullptr && s != cudaStreamLegacy && s != cudaStreamPerThread) return f(s);
+    CUDA_TRY(cudaSetDevice(c.device));
+    cudaEvent_t a = c.take_event(), b = c.take_event();
+    CUDA_TRY(cudaEventRecord(a, s));
+    CUDA_TRY(cudaStreamWaitEvent(c.own_stream, a, 0));
+    const int rc = f(c.own_stream);
+    cudaEventRecord(b, c.own_stream);
+    cudaStreamWaitEvent(s, b, 0);
+    c.event_pool.push_back(a);
+    c.event_pool.push_back(b);
+    return rc;
+}
+
+int wct_dt_forward_batch_device(wct_depotransform* h, const double* d_depos, const long long* offsets, int nevents,
+                                float* d_frames, wct_plane_window* windows, int* first_ident, void* stream)
+{
+    if (!h) return fail(WCT_ERR_ARG, "null component");
+    std::lock_guard<std::mutex> lk(h->core.mtx);
+    cudaStream_t s = stream ? (cudaStream_t)stream : h->core.own_stream;
+    return on_capturable_stream(h->core, s, [&](cudaStream_t r) {
+        return forward_batch_device(h->core, d_depos, offsets, nevents, d_frames, windows, first_ident, r);
+    });
+}
+
+int wct_dt_forward_batch(wct_depotransform* h, const double* depos, const long long* offsets, int nevents,
+                         float* frames, wct_plane_window* windows, int* first_ident)
+{
+    if (!h || !offsets || nevents < 0 || (nevents > 0 && !frames)) return fail(WCT_ERR_ARG, "wct_dt_forward_batch: bad arguments");
+    if (nevents == 0) return WCT_OK;
+    std::lock_guard<std::mutex> lk(h->core.mtx);
+    Core& c = h->core;
+    CUDA_TRY(cudaSetDevice(c.device));
+    cudaStream_t s = c.own_stream;
+    const long long ndep = offsets[nevents];
+    if (ndep < 0 || (ndep > 0 && !depos)) return fail(WCT_ERR_ARG, "wct_dt_forward_batch: bad depos");
+    const size_t fbytes = sizeof(float) * (size_t)c.nrows() * c.nticks() * (size_t)nevents;
+    CUDA_TRY(c.d_depos.ensure(sizeof(double) * 7 * std::max<long long>(ndep, 1)));
+    CUDA_TRY(c.d_frame.ensure(fbytes));
+    if (ndep)
+        CUDA_TRY(cudaMemcpyAsync(c.d_depos.p, depos, sizeof(double) * 7 * (size_t)ndep, cudaMemcpyHostToDevice, s));
+    int rc = forward_batch_device(c, c.d_depos.as<double>(), offsets, nevents, c.d_frame.as<float>(), windows,
+                                  first_ident, s);
+    if (rc) return rc;
+    CUDA_TRY(cudaMemcpyAsync(frames, c.d_frame.p, fbytes, cudaMemcpyDeviceToHost, s));
+    CUDA_TRY(cudaStreamSynchronize(s));
+    return WCT_OK;
+}
+
+int wct_dt_autotune_batch(wct_depotransform* h, const double* d_depos, const long long* offsets, int nevents,
+                          float* d_frames, void* stream, char* report, size_t len)
+{
+    if (!h) return fail(WCT_ERR_ARG, "null component");
+    std::lock_guard<std::mutex> lk(h->core.mtx);
+    cudaStream_t s = stream ? (cudaStream_t)stream : h->core.own_stream;
+    std::string rep;
+    int rc = on_capturable_stream(h->core, s, [&](cudaStream_t r) {
+        return autotune_batch(h->core, d_depos, offsets, nevents, d_frames, r, rep);
+    });
+    if (rc) return rc;
+    if (report && len) {
+        std::strncpy(report, rep.c_str(), len - 1);
+        report[len - 1] = '\0';
+        if (rep.size() >= len) return fail(WCT_ERR_SIZE, "autotune report truncated");
+    }
+    return WCT_OK;
+}
+
+int wct_dt_batch_tune(wct_depotransform* h, int* params, int set)
+{
+    if (!h || !params) return fail(WCT_ERR_ARG, "wct_dt_batch_tune: bad arguments");
+    std::lock_guard<std::mutex> lk(h->core.mtx);
+    Core& c = h->core;
+    if (!c.batch) c.batch = std::make_unique<BatchState>();
+    BatchTune& t = c.batch->tune;
+    if (set) {
+        if (params[0] < 1 || params[0] > kMaxBatch || params[1] < 1 || params[1] > 64 ||
+            (params[2] != 128 && params[2] != 256 && params[2] != 512 && params[2] != 1024) || params[3] < 1 ||
+            params[3] > 64 || params[4] < 1 || params[4] > 64)
+            return fail(WCT_ERR_ARG, "wct_dt_batch_tune: value out of range");
+        t = BatchTune{params[0], params[1], params[2], params[3], params[4]};
+    }
+    else {
+        params[0] = t.slots;
+        params[1] = t.raster_per_sm;
+        params[2] = t.fft_threads;
+        params[3] = t.fft_per_sm;
+        params[4] = t.conv_per_sm;
+    }
     return WCT_OK;
 }
 

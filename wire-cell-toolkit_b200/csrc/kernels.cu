@@ -103,16 +103,38 @@ __device__ __forceinline__ float visit_bound(float qn, float sp, float st, float
     return 2.0f * fabsf(qn) * pm * tm * 1.0001f;
 }
 
-__global__ void __launch_bounds__(256) k_prep_all(const double* __restrict__ dep, int n, DriftDev dd, int do_drift,
-                                                  PlaneSet ps, TimeDev tb, double drift_speed, double nsigma,
-                                                  PatchRec* __restrict__ rec, WindowDev* __restrict__ win,
-                                                  int* __restrict__ wire_cnt, float* __restrict__ tprof,
-                                                  unsigned long long* __restrict__ key_bound)
+// Event of a prep/fill block: blocks never straddle events.
+__device__ __forceinline__ int event_of_block(const EventTable& et, int b)
 {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    int lo = 0, hi = et.nev - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (et.blk0[mid] <= b) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
+}
+
+// One thread per depo of every event of the table; per-event window
+// statistics, visit counters and bounds (nkeys keys per event); patch
+// records [plane][depo] and time profiles indexed by the depo's position in
+// the concatenated depo array.
+__global__ void __launch_bounds__(256) k_prep_all(const double* __restrict__ dep, EventTable evt, int nkeys,
+                                                  DriftDev dd, int do_drift, PlaneSet ps, TimeDev tb,
+                                                  double drift_speed, double nsigma, PatchRec* __restrict__ rec,
+                                                  WindowDev* __restrict__ win_all, int* __restrict__ cnt_all,
+                                                  float* __restrict__ tprof, unsigned long long* __restrict__ kb_all)
+{
+    const int ev = event_of_block(evt, blockIdx.x);
+    const int i = evt.dep0[ev] + (blockIdx.x - evt.blk0[ev]) * blockDim.x + threadIdx.x;
+    const int n = evt.dep0[evt.nev];  // record stride: all depos of the table
+    const bool in = i < evt.dep0[ev + 1];
+    WindowDev* win = win_all + (size_t)ev * ps.nplanes;
+    int* wire_cnt = cnt_all + (size_t)ev * nkeys;
+    unsigned long long* key_bound = kb_all + (size_t)ev * nkeys * kTileBlocks;
     double t = 0, q = 0, x = 0, y = 0, z = 0, el = 0, et = 0;
     bool ok = false;
-    if (i < n) {
+    if (in) {
         const double* p = dep + 7 * (size_t)i;
         t = p[0]; q = p[1]; x = p[2]; y = p[3]; z = p[4]; el = p[5]; et = p[6];
         ok = true;
@@ -257,7 +279,7 @@ __global__ void __launch_bounds__(256) k_prep_all(const double* __restrict__ dep
                 }
             }
         }
-        if (i < n) rec[(size_t)ip * n + i] = r;
+        if (in) rec[(size_t)ip * n + i] = r;
         const int w0 = r.np ? r.poff / pl.nimp : 0;
         const int span = r.np ? (r.poff + r.np - 1) / pl.nimp - w0 + 1 : 0;
         const int k0 = r.toff / kTile;
@@ -328,13 +350,14 @@ __global__ void __launch_bounds__(256) k_prep_all(const double* __restrict__ dep
     }
 }
 
-void launch_prep_all(const double* depos, int n, const DriftDev& dd, int do_drift, const PlaneSet& ps,
-                     const TimeDev& tb, double drift_speed, double nsigma, PatchRec* rec, WindowDev* win,
-                     int* wire_cnt, float* tprof, unsigned long long* key_bound, cudaStream_t s)
+void launch_prep_all(const double* depos, const EventTable& et, int nkeys, const DriftDev& dd, int do_drift,
+                     const PlaneSet& ps, const TimeDev& tb, double drift_speed, double nsigma, PatchRec* rec,
+                     WindowDev* win, int* wire_cnt, float* tprof, unsigned long long* key_bound, cudaStream_t s)
 {
-    if (n <= 0) return;
-    k_prep_all<<<(n + 255) / 256, 256, 0, s>>>(depos, n, dd, do_drift, ps, tb, drift_speed, nsigma, rec, win,
-                                                 wire_cnt, tprof, key_bound);
+    const int nblocks = et.blk0[et.nev];
+    if (nblocks <= 0) return;
+    k_prep_all<<<nblocks, 256, 0, s>>>(depos, et, nkeys, dd, do_drift, ps, tb, drift_speed, nsigma, rec, win,
+                                       wire_cnt, tprof, key_bound);
 }
 
 // Exclusive scan of the per-key visit counts: block sums, a scan of the
@@ -418,16 +441,21 @@ void launch_scan(const int* wire_cnt, int nwires_total, int* wire_off, int* wire
 
 // Per-wire visit lists: wire_list[wire_off[w] ..] holds the depo indices whose
 // patch covers wire w (any order).
-__global__ void __launch_bounds__(256) k_fill(const PatchRec* __restrict__ rec, int n, PlaneSet ps,
-                                              int* __restrict__ cur, Visit* __restrict__ list)
+__global__ void __launch_bounds__(256) k_fill(const PatchRec* __restrict__ rec, EventTable evt, int nkeys,
+                                              PlaneSet ps, int* __restrict__ cur, Visit* __restrict__ list,
+                                              long long cap)
 {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int ev = event_of_block(evt, blockIdx.x);
+    const int i = evt.dep0[ev] + (blockIdx.x - evt.blk0[ev]) * blockDim.x + threadIdx.x;
+    const int n = evt.dep0[evt.nev];
+    const bool in = i < evt.dep0[ev + 1];
+    const int key0 = ev * nkeys;
     const int lane = threadIdx.x & 31;
     for (int ip = 0; ip < ps.nplanes; ++ip) {
         const PlaneDev& pl = ps.p[ip];
         int w0 = 0, span = 0, k0 = 0, kspan = 1;
         PatchRec r{};
-        if (i < n) {
+        if (in) {
             r = rec[(size_t)ip * n + i];
             if (r.np) {
                 w0 = r.poff / pl.nimp;
@@ -443,7 +471,7 @@ __global__ void __launch_bounds__(256) k_fill(const PatchRec* __restrict__ rec, 
             int key = -1;
             if (k < span) {
                 const int dw = k / kspan, dk = k - dw * kspan;
-                key = (pl.wire_base + w0 + dw) * ps.ntiles + k0 + dk;
+                key = key0 + (pl.wire_base + w0 + dw) * ps.ntiles + k0 + dk;
             }
             const unsigned act = __ballot_sync(0xffffffffu, key >= 0);
             if (key >= 0) {
@@ -462,16 +490,18 @@ __global__ void __launch_bounds__(256) k_fill(const PatchRec* __restrict__ rec, 
                 v.qn = r.qn;
                 v.d = i;
                 v.pad = 0;
-                list[base + rank] = v;
+                if (base + rank < cap) list[base + rank] = v;  // beyond cap: the caller reports an overflow
             }
         }
     }
 }
 
-void launch_fill(const PatchRec* rec, int n, const PlaneSet& ps, int* wire_cur, Visit* visits, cudaStream_t s)
+void launch_fill(const PatchRec* rec, const EventTable& et, int nkeys, const PlaneSet& ps, int* wire_cur,
+                 Visit* visits, long long cap, cudaStream_t s)
 {
-    if (n <= 0) return;
-    k_fill<<<(n + 255) / 256, 256, 0, s>>>(rec, n, ps, wire_cur, visits);
+    const int nblocks = et.blk0[et.nev];
+    if (nblocks <= 0) return;
+    k_fill<<<nblocks, 256, 0, s>>>(rec, et, nkeys, ps, wire_cur, visits, cap);
 }
 
 // ---------------------------------------------------------------------------
@@ -505,23 +535,18 @@ size_t raster_smem_bytes(int G)
            sizeof(int4) * (size_t)kRasterThreads;
 }
 
-__global__ void __launch_bounds__(kRasterThreads) k_raster_wires(const PatchRec* __restrict__ rec,
-                                                                 const float* __restrict__ tprof,
-                                                                 const int* __restrict__ wire_cnt,
-                                                                 const int* __restrict__ wire_off,
-                                                                 const Visit* __restrict__ visits,
-                                                                 const unsigned long long* __restrict__ key_bound,
-                                                                 GridSet gs,
-                                                                 float* __restrict__ Q)
+// One raster work item: charge row `row` (wire start_ch + row) of plane P and
+// absolute tick tile ktile.  Visit keys are key_base + wire * ntiles_abs +
+// tile; at most vcap visits exist.  Called by all threads of the block;
+// smem_i holds the dynamic shared memory of raster_smem_bytes(P.G).
+__device__ __forceinline__ void raster_tile(const GridPlane& P, int row, int ktile, int key_base, int ntiles_abs,
+                                            const PatchRec* __restrict__ rec, const float* __restrict__ tprof,
+                                            const int* __restrict__ wire_cnt, const int* __restrict__ wire_off,
+                                            const Visit* __restrict__ visits, long long vcap,
+                                            const unsigned long long* __restrict__ key_bound,
+                                            float* __restrict__ Q, int* smem_i, float* scale, float* iscale)
 {
-    extern __shared__ int smem_i[];
-    __shared__ float scale[kTileBlocks], iscale[kTileBlocks];
-    int ip = 0;
-    while (ip + 1 < gs.nplanes && (int)blockIdx.x >= gs.p[ip + 1].row_base) ++ip;
-    const GridPlane& P = gs.p[ip];
-    const int rel = blockIdx.x - P.row_base;
-    const int row = rel / P.ntile;
-    const int ktile = P.ktile0 + (rel - row * P.ntile);  // absolute tick tile
+    __syncthreads();  // the previous item of a persistent block is done with the shared arrays
     const int w = P.start_ch + row;
     const int G = P.G, nimp = P.nimp;
     const int tick_lo = ktile * kTile;                      // absolute first tick of the tile
@@ -532,10 +557,11 @@ __global__ void __launch_bounds__(kRasterThreads) k_raster_wires(const PatchRec*
     int cnt = 0;
     const Visit* list = nullptr;
     int key = -1;
-    if (w >= 0 && w < P.nwires && ktile >= 0 && ktile < gs.ntiles_abs) {
-        key = (P.wire_base + w) * gs.ntiles_abs + ktile;
-        cnt = wire_cnt[key];
-        list = visits + wire_off[key];
+    if (w >= 0 && w < P.nwires && ktile >= 0 && ktile < ntiles_abs) {
+        key = key_base + (P.wire_base + w) * ntiles_abs + ktile;
+        const int off = wire_off[key];
+        cnt = (int)min((long long)wire_cnt[key], max(0ll, vcap - off));  // no reads past an overflowed list
+        list = visits + off;
     }
     {
         int4* g4 = reinterpret_cast<int4*>(grid);
@@ -697,30 +723,49 @@ __global__ void __launch_bounds__(kRasterThreads) k_raster_wires(const PatchRec*
     }
 }
 
+__global__ void __launch_bounds__(kRasterThreads) k_raster_wires(const PatchRec* __restrict__ rec,
+                                                                 const float* __restrict__ tprof,
+                                                                 const int* __restrict__ wire_cnt,
+                                                                 const int* __restrict__ wire_off,
+                                                                 const Visit* __restrict__ visits, long long vcap,
+                                                                 const unsigned long long* __restrict__ key_bound,
+                                                                 GridSet gs, float* __restrict__ Q)
+{
+    extern __shared__ int smem_i[];
+    __shared__ float scale[kTileBlocks], iscale[kTileBlocks];
+    int ip = 0;
+    while (ip + 1 < gs.nplanes && (int)blockIdx.x >= gs.p[ip + 1].row_base) ++ip;
+    const GridPlane& P = gs.p[ip];
+    const int rel = blockIdx.x - P.row_base;
+    const int row = rel / P.ntile;
+    const int ktile = P.ktile0 + (rel - row * P.ntile);  // absolute tick tile
+    raster_tile(P, row, ktile, 0, gs.ntiles_abs, rec, tprof, wire_cnt, wire_off, visits, vcap, key_bound, Q, smem_i,
+                scale, iscale);
+}
+
 void launch_raster_wires(const PatchRec* rec, const float* tprof, const int* wire_cnt, const int* wire_off,
-                         const Visit* visits, const unsigned long long* key_bound, const GridSet& gs, float* Q,
-                         cudaStream_t s)
+                         const Visit* visits, long long vcap, const unsigned long long* key_bound, const GridSet& gs,
+                         float* Q, cudaStream_t s)
 {
     if (gs.nrows_total <= 0) return;
     size_t smem = 0;
     for (int i = 0; i < gs.nplanes; ++i) smem = std::max(smem, raster_smem_bytes(gs.p[i].G));
     cudaFuncSetAttribute((const void*)k_raster_wires, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    k_raster_wires<<<gs.nrows_total, kRasterThreads, smem, s>>>(rec, tprof, wire_cnt, wire_off, visits, key_bound,
-                                                                    gs, Q);
+    k_raster_wires<<<gs.nrows_total, kRasterThreads, smem, s>>>(rec, tprof, wire_cnt, wire_off, visits, vcap,
+                                                                    key_bound, gs, Q);
 }
 
 // ---------------------------------------------------------------------------
 // Real FFT of rows (forward), packed output.  One row per block.
 // ---------------------------------------------------------------------------
-__global__ void k_rfft_rows(const float* in, long in_ld, int in_len, float2* out, long out_ld, int nrows, FftDesc d)
+// One row: x (in_len real values, zero padded to 2M) -> o (M packed bins).
+// Called by all threads of the block; sm holds 2M complex values.
+__device__ __forceinline__ void rfft_row(const float* x, int in_len, float2* o, const FftDesc& d, float2* sm)
 {
-    extern __shared__ float2 sm[];
-    const int row = blockIdx.x;
-    if (row >= nrows) return;
+    __syncthreads();  // the previous row of a persistent block is done with sm
     float2* a = sm;
     float2* b = sm + d.M;
     const int M = d.M, tid = threadIdx.x, nth = blockDim.x;
-    const float* x = in + (size_t)row * in_ld;
     if (in_len >= 2 * M && ((reinterpret_cast<uintptr_t>(x) & 7) == 0)) {
         const float2* x2 = reinterpret_cast<const float2*>(x);
         for (int m = tid; m < M; m += nth) a[m] = x2[m];
@@ -733,8 +778,15 @@ __global__ void k_rfft_rows(const float* in, long in_ld, int in_len, float2* out
     }
     __syncthreads();
     float2* Z = fft_c2c<-1>(a, b, d, tid, nth);
-    float2* o = out + (size_t)row * out_ld;
     for (int k = tid; k < M; k += nth) o[k] = r2c_bin(Z, k, M, d.twh);
+}
+
+__global__ void k_rfft_rows(const float* in, long in_ld, int in_len, float2* out, long out_ld, int nrows, FftDesc d)
+{
+    extern __shared__ float2 sm[];
+    const int row = blockIdx.x;
+    if (row >= nrows) return;
+    rfft_row(in + (size_t)row * in_ld, in_len, out + (size_t)row * out_ld, d, sm);
 }
 
 // Two complex rows of M bins in dynamic shared memory; raise the opt-in limit
@@ -757,24 +809,21 @@ void launch_rfft_rows(const float* in, long in_ld, int in_len, float2* out, long
 // Inverse real FFT of rows + frame write (ImpactTransform.cxx:303-347).
 // Row r of Vh is wire wire0 + r; ticks are tick0 + column.
 // ---------------------------------------------------------------------------
-__global__ void k_irfft_rows(const float2* __restrict__ Vh, int nrows, FftDesc d, int wire0, int wlo, int whi,
-                             int tick0, int ncols, int nticks, float* __restrict__ frame)
+// One row: v (M packed bins) -> real values written to f[tick0 + c] for
+// c < ncols, 0 <= tick0 + c < nticks.  Called by all threads of the block.
+__device__ __forceinline__ void irfft_row(const float2* __restrict__ v, const FftDesc& d, float* __restrict__ f,
+                                          int tick0, int ncols, int nticks, float2* sm)
 {
-    extern __shared__ float2 sm[];
-    const int row = blockIdx.x;
-    const int W = wire0 + row;
-    if (row >= nrows || W < wlo || W >= whi) return;
+    __syncthreads();  // the previous row of a persistent block is done with sm
     float2* a = sm;
     float2* b = sm + d.M;
     const int M = d.M, tid = threadIdx.x, nth = blockDim.x;
-    const float2* v = Vh + (size_t)row * M;
     for (int k = tid; k < M; k += nth) b[k] = v[k];
     __syncthreads();
     for (int k = tid; k < M; k += nth) a[k] = c2r_bin(b, k, M, d.twh);
     __syncthreads();
     float2* z = fft_c2c<+1>(a, b, d, tid, nth);
     const float sc = 1.0f / (float)M;
-    float* f = frame + (size_t)W * nticks;
     for (int m = tid; m < M; m += nth) {
         const float2 zz = z[m];
         const int c0 = 2 * m;
@@ -782,6 +831,16 @@ __global__ void k_irfft_rows(const float2* __restrict__ Vh, int nrows, FftDesc d
         if (c0 < ncols && t0 >= 0 && t0 < nticks) f[t0] = zz.x * sc;
         if (c0 + 1 < ncols && t0 + 1 >= 0 && t0 + 1 < nticks) f[t0 + 1] = zz.y * sc;
     }
+}
+
+__global__ void k_irfft_rows(const float2* __restrict__ Vh, int nrows, FftDesc d, int wire0, int wlo, int whi,
+                             int tick0, int ncols, int nticks, float* __restrict__ frame)
+{
+    extern __shared__ float2 sm[];
+    const int row = blockIdx.x;
+    const int W = wire0 + row;
+    if (row >= nrows || W < wlo || W >= whi) return;
+    irfft_row(Vh + (size_t)row * d.M, d, frame + (size_t)W * nticks, tick0, ncols, nticks, sm);
 }
 
 void launch_irfft_rows(const float2* Vh, int nrows, const FftDesc& d, int wire0, int wlo, int whi, int tick0,
@@ -806,24 +865,25 @@ constexpr int kConvRB = 8;
 constexpr int kConvRG = 8;
 constexpr int kConvRows = kConvRB * kConvRG;
 
+// One tile of the wire convolution: frequencies fblk*32 .. +31, output rows
+// oblk*64 .. +63.  Called by all threads of a (32, kConvRG) block.
+// PAIR: groups g and G-1-g share one response up to a mirror in wire
+// (R_{G-1-g}[j] = R_g[-j], the symmetrised impact map of
+// gen/src/PlaneImpactResponse.cxx:256-268), so for each tap the two
+// mirrored inputs are added before one complex multiply.
 template <int PAD, bool PAIR>
-__global__ void __launch_bounds__(32 * kConvRG) k_wire_conv(const float2* __restrict__ Qh,
-                                                             const float2* __restrict__ Rh, float2* __restrict__ Vh,
-                                                             int G, int nin, int nout, int M)
+__device__ __forceinline__ void wire_conv_tile(const float2* __restrict__ Qh, const float2* __restrict__ Rh,
+                                               float2* __restrict__ Vh, int G, int nin, int nout, int M, int fblk,
+                                               int oblk, float2* conv_smem)
 {
-    // PAIR: groups g and G-1-g share one response up to a mirror in wire
-    // (R_{G-1-g}[j] = R_g[-j], the symmetrised impact map of
-    // gen/src/PlaneImpactResponse.cxx:256-268), so for each tap the two
-    // mirrored inputs are added before one complex multiply.
     constexpr int SROWS = kConvRows + 2 * PAD;
     constexpr int NT = 2 * PAD + 1;
-    extern __shared__ float2 conv_smem[];
     float2 (*Qs)[32] = reinterpret_cast<float2 (*)[32]>(conv_smem);
     float2 (*Qs2)[32] = reinterpret_cast<float2 (*)[32]>(conv_smem + SROWS * 32);
     float2 (*Rs)[32] = reinterpret_cast<float2 (*)[32]>(conv_smem + (PAIR ? 2 : 1) * SROWS * 32);
     const int lane = threadIdx.x, rg = threadIdx.y;
-    const int f = blockIdx.x * 32 + lane;
-    const int o0 = blockIdx.y * kConvRows;
+    const int f = fblk * 32 + lane;
+    const int o0 = oblk * kConvRows;
     const bool fok = f < M;
     const bool dc = f == 0;
     float2 acc[kConvRB];
@@ -885,6 +945,15 @@ __global__ void __launch_bounds__(32 * kConvRG) k_wire_conv(const float2* __rest
             if (o < nout) Vh[(size_t)o * M + f] = acc[r];
         }
     }
+}
+
+template <int PAD, bool PAIR>
+__global__ void __launch_bounds__(32 * kConvRG) k_wire_conv(const float2* __restrict__ Qh,
+                                                             const float2* __restrict__ Rh, float2* __restrict__ Vh,
+                                                             int G, int nin, int nout, int M)
+{
+    extern __shared__ float2 conv_smem[];
+    wire_conv_tile<PAD, PAIR>(Qh, Rh, Vh, G, nin, nout, M, blockIdx.x, blockIdx.y, conv_smem);
 }
 
 // Same convolution with a run-time pad (any response width).
@@ -985,6 +1054,394 @@ __global__ void k_twiddles(float2* __restrict__ tw, float2* __restrict__ twh, in
 void launch_twiddles(float2* tw, float2* twh, int M, cudaStream_t s)
 {
     k_twiddles<<<(M + 255) / 256, 256, 0, s>>>(tw, twh, M);
+}
+
+// ===========================================================================
+// Batched events: a device-planned pipeline with no host round trip, so a
+// whole batch is one captured CUDA graph.  After the prep/scan/fill kernels
+// (the event-table forms of the single-event ones), k_plan_batch computes
+// every (event, plane) window on the device -- ImpactTransform's window
+// arithmetic (gen/src/ImpactTransform.cxx:83-115) with the reference's FFT
+// length tables -- picks the time-FFT length class, places the event's grids
+// in fixed event slots, and writes the work-item prefixes that the persistent
+// raster, time-FFT, wire-convolution and inverse kernels walk.
+// ===========================================================================
+}  // namespace wctb200
+
+#include "fft_lengths.h"
+
+namespace wctb200 {
+
+__constant__ int c_fbl_any[] = {WCT_FFT_LENGTHS_ANY};
+__constant__ int c_fbl_even[] = {WCT_FFT_LENGTHS_EVEN};
+__constant__ int c_fbl_odd[] = {WCT_FFT_LENGTHS_ODD};
+
+template <int N>
+__device__ __forceinline__ int fbl_pick(const int (&t)[N], int n)
+{
+    if (n <= t[N - 1])
+        for (int i = 0; i < N; ++i)
+            if (t[i] >= n) return t[i];
+    return n;
+}
+
+// fft_best_length (util/src/FFTBestLength.cxx:12-59)
+__device__ int fft_best_length_dev(int n, bool keep_odd_even)
+{
+    if (!keep_odd_even) return fbl_pick(c_fbl_any, n);
+    return (n % 2 == 0) ? fbl_pick(c_fbl_even, n) : fbl_pick(c_fbl_odd, n);
+}
+
+// The window of one (event, plane) from its reduced depo extents: the same
+// arithmetic, in the same double operations, as the host path.
+__device__ void window_dev(const BatchStatic& bs, int ip, const WindowDev& w, EvPlane& o)
+{
+    const BatchPlaneStatic& pl = bs.pl[ip];
+    double pmin = 0, pmax = 0, tmin = 0, tmax = 0;  // gausdesc_range of an empty set
+    if (w.nadded > 0) {
+        pmin = dkey_inv(w.pmin);
+        pmax = dkey_inv(w.pmax);
+        tmin = dkey_inv(w.tmin);
+        tmax = dkey_inv(w.tmax);
+    }
+    auto ibin = [&](double v) { return __double2int_rz(__ddiv_rn(__dsub_rn(v, pl.imp_min), pl.imp_bs)); };
+    auto tbin = [&](double v) { return __double2int_rz(__ddiv_rn(__dsub_rn(v, bs.start_time), bs.tbs)); };
+    const int i0 = max(ibin(pmin), 0), i1 = min(ibin(pmax) + 1, pl.imp_nbins);
+    const int t0 = max(tbin(tmin), 0), t1 = min(tbin(tmax) + 1, bs.nticks);
+    const int G = pl.G;
+    int start_ch = (int)floor(__ddiv_rn((double)i0, (double)(G - 1))) - 1;
+    int end_ch = (int)ceil(__ddiv_rn((double)i1, (double)(G - 1))) + 2;
+    if ((end_ch - start_ch) % 2 == 1) end_ch += 1;
+    int start_tick = t0 - 1;
+    int end_tick = t1 + 2;
+    if ((end_tick - start_tick) % 2 == 1) end_tick += 1;
+    const int ntw = fft_best_length_dev(end_ch - start_ch + 2 * pl.npad, true);
+    const int npad_wire = (ntw - end_ch + start_ch) / 2;
+    const int ntt = fft_best_length_dev(end_tick - start_tick + pl.waveform_pad, false);
+    const int npad_time = ntt - end_tick + start_tick;
+    o.start_ch = start_ch;
+    o.end_ch = end_ch;
+    o.start_tick = start_tick;
+    o.end_tick = end_tick;
+    o.m_start_ch = start_ch - npad_wire;
+    o.m_end_ch = end_ch + npad_wire;
+    o.m_start_tick = start_tick;
+    o.m_end_tick = end_tick + npad_time;
+    o.nw_ref = end_ch - start_ch + 2 * npad_wire;
+    o.nt_ref = o.m_end_tick - o.m_start_tick;
+    o.ndepos_added = w.nadded;
+    o.outside_time = w.out_time;
+    o.outside_pitch = w.out_pitch;
+}
+
+__device__ __forceinline__ int fdiv_floor(int a, int b) { return a >= 0 ? a / b : -((-a + b - 1) / b); }
+
+// One block of 256 threads: windows and work counts per (event, plane), then
+// the prefixes (thread 0; at most kMaxBatch * kMaxPlanes entries).
+__global__ void __launch_bounds__(256) k_plan_batch(BatchPlan* __restrict__ plan, BatchStatic bs, int nev,
+                                                    const WindowDev* __restrict__ win,
+                                                    const int* __restrict__ total_visits, long long vcap)
+{
+    __shared__ int s_status;
+    __shared__ int c_raster[kMaxBatch * kMaxPlanes], c_rows[kMaxBatch * kMaxPlanes],
+        c_orows[kMaxBatch * kMaxPlanes], c_conv[kMaxBatch * kMaxPlanes];
+    const int np = bs.np, ne = nev * np;
+    if (threadIdx.x == 0) s_status = 0;
+    __syncthreads();
+    for (int k = threadIdx.x; k < ne; k += blockDim.x) {
+        const int e = k / np, ip = k - e * np;
+        const WindowDev& w = win[k];
+        EvPlane o{};
+        window_dev(bs, ip, w, o);
+        const BatchPlaneStatic& pl = bs.pl[ip];
+        int st = 0;
+        if (w.oversize) st |= kBatchOversize;
+        if (w.bigcharge) st |= kBatchBigCharge;
+        o.nin = w.nadded > 0 ? o.end_ch - o.start_ch : 0;
+        o.nout = o.nin ? o.nin + 2 * pl.npad : 0;
+        o.ncols = o.end_tick - o.start_tick;
+        int cls = -1;
+        for (int c = 0; c < bs.ncls; ++c)
+            if (bs.cls_N[c] >= o.nt_ref) {
+                cls = c;
+                break;
+            }
+        if (cls < 0 || o.nin > pl.nin_max) {
+            if (o.nin) st |= kBatchNoClass;
+            o.nin = o.nout = 0;
+            cls = 0;
+        }
+        o.cls = cls;
+        o.N = bs.cls_N[cls];
+        o.M = o.N / 2;
+        o.ktile0 = fdiv_floor(o.start_tick, kTile);
+        o.ntile = fdiv_floor(o.start_tick + o.N - 1, kTile) - o.ktile0 + 1;
+        o.qoff = (long long)e * bs.qslot_total + pl.qslot;
+        o.voff = (long long)e * bs.vslot_total + pl.vslot;
+        plan->ep[k] = o;
+        c_raster[k] = o.nin * o.ntile;
+        c_rows[k] = pl.G * o.nin;
+        c_orows[k] = o.nout;
+        c_conv[k] = o.nin ? ((o.M + 31) / 32) * ((o.nout + kConvRows - 1) / kConvRows) : 0;
+        if (st) atomicOr(&s_status, st);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int a = 0, b = 0, c = 0;
+        for (int k = 0; k < ne; ++k) {
+            plan->pre_raster[k] = a;
+            plan->pre_rows[k] = b;
+            plan->pre_orows[k] = c;
+            a += c_raster[k];
+            b += c_rows[k];
+            c += c_orows[k];
+        }
+        plan->pre_raster[ne] = a;
+        plan->pre_rows[ne] = b;
+        plan->pre_orows[ne] = c;
+        for (int ip = 0; ip < np; ++ip) {
+            int t = 0;
+            for (int e = 0; e < nev; ++e) {
+                plan->pre_conv[ip][e] = t;
+                t += c_conv[e * np + ip];
+            }
+            plan->pre_conv[ip][nev] = t;
+        }
+        const int tv = *total_visits;
+        plan->total_visits = tv;
+        plan->nev = nev;
+        plan->np = np;
+        plan->status = s_status | ((long long)tv > vcap ? kBatchVisitOverflow : 0);
+    }
+}
+
+void launch_plan_batch(BatchPlan* plan, const BatchStatic& bs, int nev, const WindowDev* win, const int* total_visits,
+                       long long vcap, cudaStream_t s)
+{
+    k_plan_batch<<<1, 256, 0, s>>>(plan, bs, nev, win, total_visits, vcap);
+}
+
+// Index of the (event, plane) entry whose item range holds `item`: the last
+// k in [0, n) with pre[k] <= item (entries with no items are skipped).
+__device__ __forceinline__ int find_entry(const int* __restrict__ pre, int n, int item)
+{
+    int lo = 0, hi = n - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (pre[mid] <= item) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
+}
+
+__global__ void __launch_bounds__(kRasterThreads) k_raster_batch(const BatchPlan* __restrict__ plan, BatchStatic bs,
+                                                                 PlaneSet ps, const PatchRec* __restrict__ rec,
+                                                                 long long recstride,
+                                                                 const float* __restrict__ tprof,
+                                                                 const int* __restrict__ wire_cnt,
+                                                                 const int* __restrict__ wire_off,
+                                                                 const Visit* __restrict__ visits, long long vcap,
+                                                                 const unsigned long long* __restrict__ key_bound,
+                                                                 float* __restrict__ Q)
+{
+    extern __shared__ int smem_i[];
+    __shared__ float scale[kTileBlocks], iscale[kTileBlocks];
+    if (plan->status & kBatchVisitOverflow) return;
+    const int ne = plan->nev * plan->np;
+    const int total = plan->pre_raster[ne];
+    for (int item = blockIdx.x; item < total; item += gridDim.x) {
+        const int k = find_entry(plan->pre_raster, ne, item);
+        const int e = k / plan->np, ip = k - e * plan->np;
+        const EvPlane& E = plan->ep[k];
+        GridPlane P;
+        P.nimp = ps.p[ip].nimp;
+        P.G = bs.pl[ip].G;
+        P.nwires = ps.p[ip].nwires;
+        P.wire_base = ps.p[ip].wire_base;
+        P.start_ch = E.start_ch;
+        P.nin = E.nin;
+        P.col0 = E.start_tick;
+        P.ncols = E.ncols;
+        P.N = E.N;
+        P.tbs = (float)bs.tbs;
+        P.pbs = (float)ps.p[ip].imp_bs;
+        P.qoff = E.qoff;
+        P.recoff = (long long)ip * recstride;
+        P.row_base = 0;
+        P.ktile0 = E.ktile0;
+        P.ntile = E.ntile;
+        const int rel = item - plan->pre_raster[k];
+        const int row = rel / E.ntile;
+        raster_tile(P, row, E.ktile0 + (rel - row * E.ntile), e * bs.nkeys, bs.ntiles, rec, tprof, wire_cnt, wire_off,
+                    visits, vcap, key_bound, Q, smem_i, scale, iscale);
+    }
+}
+
+void launch_raster_batch(const BatchPlan* plan, const BatchStatic& bs, const PlaneSet& ps, const PatchRec* rec,
+                         long long recstride, const float* tprof, const int* wire_cnt, const int* wire_off,
+                         const Visit* visits, long long vcap, const unsigned long long* key_bound, float* Q,
+                         int nblocks, int maxG, cudaStream_t s)
+{
+    const size_t smem = raster_smem_bytes(maxG);
+    k_raster_batch<<<nblocks, kRasterThreads, smem, s>>>(plan, bs, ps, rec, recstride, tprof, wire_cnt, wire_off,
+                                                          visits, vcap, key_bound, Q);
+}
+
+// Time FFT of every charge-grid row of the pass, in place (rows of N reals
+// become M packed bins), whatever their length class.
+__global__ void k_rfft_batch(const BatchPlan* __restrict__ plan, const FftDesc* __restrict__ descs,
+                             float* __restrict__ Q)
+{
+    extern __shared__ float2 sm[];
+    if (plan->status & kBatchVisitOverflow) return;
+    const int ne = plan->nev * plan->np;
+    const int total = plan->pre_rows[ne];
+    for (int item = blockIdx.x; item < total; item += gridDim.x) {
+        const int k = find_entry(plan->pre_rows, ne, item);
+        const EvPlane& E = plan->ep[k];
+        const FftDesc d = descs[E.cls];
+        float* x = Q + E.qoff + (size_t)(item - plan->pre_rows[k]) * E.N;
+        rfft_row(x, E.N, reinterpret_cast<float2*>(x), d, sm);
+    }
+}
+
+void launch_rfft_batch(const BatchPlan* plan, const FftDesc* descs, float* Q, int nblocks, int nthreads, int maxM,
+                       cudaStream_t s)
+{
+    const size_t smem = 2 * (size_t)maxM * sizeof(float2);
+    k_rfft_batch<<<nblocks, nthreads, smem, s>>>(plan, descs, Q);
+}
+
+// Wire convolution with a run-time pad, one tile (generic response widths).
+__device__ __forceinline__ void wire_conv_tile_any(const float2* __restrict__ Qh, const float2* __restrict__ Rh,
+                                                   float2* __restrict__ Vh, int G, int PAD, int nin, int nout, int M,
+                                                   int fblk, int oblk)
+{
+    const int lane = threadIdx.x, rg = threadIdx.y;
+    const int f = fblk * 32 + lane;
+    const int o0 = oblk * kConvRows;
+    if (f >= M) return;
+    float2 acc[kConvRB];
+#pragma unroll
+    for (int r = 0; r < kConvRB; ++r) acc[r] = make_float2(0.f, 0.f);
+    for (int g = 0; g < G; ++g) {
+        const float2* Rg = Rh + (size_t)g * (2 * PAD + 1) * M + f;
+        for (int jj = 0; jj <= 2 * PAD; ++jj) {
+            const float2 rr = Rg[(size_t)jj * M];
+            const float rc = f == 0 ? 0.f : rr.y;
+            const float ry = f == 0 ? rr.y : rr.x;
+            const int j = jj - PAD;
+#pragma unroll
+            for (int r = 0; r < kConvRB; ++r) {
+                const int i = o0 + rg * kConvRB + r - PAD - j;
+                if (i < 0 || i >= nin) continue;
+                const float2 q = Qh[((size_t)g * nin + i) * M + f];
+                acc[r].x = fmaf(rr.x, q.x, fmaf(-rc, q.y, acc[r].x));
+                acc[r].y = fmaf(ry, q.y, fmaf(rc, q.x, acc[r].y));
+            }
+        }
+    }
+#pragma unroll
+    for (int r = 0; r < kConvRB; ++r) {
+        const int o = o0 + rg * kConvRB + r;
+        if (o < nout) Vh[(size_t)o * M + f] = acc[r];
+    }
+}
+
+// PAD < 0: run-time pad (bs.pl[ip].npad) without shared-memory staging.
+template <int PAD, bool PAIR>
+__global__ void __launch_bounds__(32 * kConvRG) k_conv_batch(const BatchPlan* __restrict__ plan, BatchStatic bs,
+                                                             int ip, const float2* const* __restrict__ spec,
+                                                             const float* __restrict__ Q, float2* __restrict__ V)
+{
+    extern __shared__ float2 conv_smem[];
+    if (plan->status & kBatchVisitOverflow) return;
+    const int nev = plan->nev, np = plan->np;
+    const int* pre = plan->pre_conv[ip];
+    const int total = pre[nev];
+    const int G = bs.pl[ip].G;
+    for (int item = blockIdx.x; item < total; item += gridDim.x) {
+        const int e = find_entry(pre, nev, item);
+        const EvPlane& E = plan->ep[e * np + ip];
+        const int rel = item - pre[e];
+        const int nfb = (E.M + 31) / 32;
+        const int oblk = rel / nfb, fblk = rel - oblk * nfb;
+        const float2* Qh = reinterpret_cast<const float2*>(Q + E.qoff);
+        if constexpr (PAD >= 0)
+            wire_conv_tile<PAD, PAIR>(Qh, spec[E.cls], V + E.voff, G, E.nin, E.nout, E.M, fblk, oblk, conv_smem);
+        else
+            wire_conv_tile_any(Qh, spec[E.cls], V + E.voff, G, bs.pl[ip].npad, E.nin, E.nout, E.M, fblk, oblk);
+    }
+}
+
+size_t conv_smem_bytes(int npad, bool pair)
+{
+    if (npad != 10 && npad != 21) return 0;
+    return sizeof(float2) * 32 * ((size_t)(pair ? 2 : 1) * (kConvRows + 2 * npad) + (2 * npad + 1));
+}
+
+void launch_conv_batch(const BatchPlan* plan, const BatchStatic& bs, int ip, bool pair, const float2* const* spec,
+                       const float* Q, float2* V, int nblocks, cudaStream_t s)
+{
+    const int npad = bs.pl[ip].npad;
+    dim3 block(32, kConvRG);
+    const size_t sm = conv_smem_bytes(npad, pair);
+#define WCT_CONVB(P, B) k_conv_batch<P, B><<<nblocks, block, sm, s>>>(plan, bs, ip, spec, Q, V)
+    if (npad == 10 && pair) WCT_CONVB(10, true);
+    else if (npad == 10) WCT_CONVB(10, false);
+    else if (npad == 21 && pair) WCT_CONVB(21, true);
+    else if (npad == 21) WCT_CONVB(21, false);
+#undef WCT_CONVB
+    else k_conv_batch<-1, false><<<nblocks, block, 0, s>>>(plan, bs, ip, spec, Q, V);
+}
+
+// Inverse time FFT of every V row of the pass and the frame write of its event.
+__global__ void k_irfft_batch(const BatchPlan* __restrict__ plan, BatchStatic bs, const FftDesc* __restrict__ descs,
+                              const float2* __restrict__ V, float* __restrict__ frames, long long frame_stride)
+{
+    extern __shared__ float2 sm[];
+    if (plan->status & kBatchVisitOverflow) return;
+    const int ne = plan->nev * plan->np;
+    const int total = plan->pre_orows[ne];
+    for (int item = blockIdx.x; item < total; item += gridDim.x) {
+        const int k = find_entry(plan->pre_orows, ne, item);
+        const int e = k / plan->np, ip = k - e * plan->np;
+        const EvPlane& E = plan->ep[k];
+        const BatchPlaneStatic& pl = bs.pl[ip];
+        const int o = item - plan->pre_orows[k];
+        const int W = E.start_ch - pl.npad + o;
+        const int wlo = max(0, E.m_start_ch), whi = min(pl.nwires, E.m_end_ch);
+        if (W < wlo || W >= whi) continue;  // uniform over the block
+        const FftDesc d = descs[E.cls];
+        irfft_row(V + E.voff + (size_t)o * E.M, d, frames + (size_t)e * frame_stride + (size_t)(pl.row0 + W) * bs.nticks,
+                  E.start_tick, min(E.N, E.nt_ref), bs.nticks, sm);
+    }
+}
+
+void launch_irfft_batch(const BatchPlan* plan, const BatchStatic& bs, const FftDesc* descs, const float2* V,
+                        float* frames, long long frame_stride, int nblocks, int nthreads, int maxM, cudaStream_t s)
+{
+    const size_t smem = 2 * (size_t)maxM * sizeof(float2);
+    k_irfft_batch<<<nblocks, nthreads, smem, s>>>(plan, bs, descs, V, frames, frame_stride);
+}
+
+// Shared-memory opt-ins of the batched kernels, set before a graph capture
+// (the launchers themselves only enqueue).
+void batch_kernel_attributes(int maxG, int maxM)
+{
+    const int sr = (int)raster_smem_bytes(maxG);
+    const int sf = (int)(2 * (size_t)maxM * sizeof(float2));
+    cudaFuncSetAttribute((const void*)k_raster_batch, cudaFuncAttributeMaxDynamicSharedMemorySize, sr);
+    cudaFuncSetAttribute((const void*)k_rfft_batch, cudaFuncAttributeMaxDynamicSharedMemorySize, sf);
+    cudaFuncSetAttribute((const void*)k_irfft_batch, cudaFuncAttributeMaxDynamicSharedMemorySize, sf);
+    cudaFuncSetAttribute((const void*)k_conv_batch<10, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)conv_smem_bytes(10, true));
+    cudaFuncSetAttribute((const void*)k_conv_batch<10, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)conv_smem_bytes(10, false));
+    cudaFuncSetAttribute((const void*)k_conv_batch<21, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)conv_smem_bytes(21, true));
+    cudaFuncSetAttribute((const void*)k_conv_batch<21, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)conv_smem_bytes(21, false));
 }
 
 }  // namespace wctb200

@@ -119,16 +119,88 @@ struct AdjSet {
     AdjPlane p[kMaxPlanes];
 };
 
+// Events of one launch of the prep and fill kernels: depo ranges in the
+// concatenated depo array and the first 256-thread block of each event
+// (blocks never straddle events).  A single event is a table of one.
+constexpr int kMaxBatch = 64;
+struct EventTable {
+    int nev;
+    int dep0[kMaxBatch + 1];
+    int blk0[kMaxBatch + 1];
+};
+
+// ---- batched events: device-planned pipeline ----
+constexpr int kMaxClasses = 48;  // time-FFT length classes of the batched path
+
+// Static description of the batched path (a kernel parameter): the window
+// arithmetic inputs of every plane and the layout of one event slot in the
+// charge-grid (Q, floats) and wire-convolution (V, complex) arenas.
+struct BatchPlaneStatic {
+    int G, npad, waveform_pad, nwires, imp_nbins, row0, nin_max;
+    double imp_min, imp_bs;
+    long long qslot;  // offset of the plane's grid within an event slot (floats)
+    long long vslot;  // offset of the plane's V rows within an event slot (complex values)
+};
+
+struct BatchStatic {
+    int np, nticks, nkeys, ntiles;
+    double start_time, tbs;   // tick binning of the window arithmetic (ImpactTransform)
+    int ncls;
+    int cls_N[kMaxClasses];   // ascending time-FFT lengths
+    long long qslot_total, vslot_total;
+    BatchPlaneStatic pl[kMaxPlanes];
+};
+
+// Per (event, plane) plan, written on the device by the planner.
+struct EvPlane {
+    int start_ch, end_ch, start_tick, end_tick;           // window before padding
+    int m_start_ch, m_end_ch, m_start_tick, m_end_tick;   // ImpactTransform's padded window
+    int nw_ref, nt_ref;
+    int nin, nout, ncols, N, M, cls;
+    int ktile0, ntile;
+    int ndepos_added, outside_time, outside_pitch;
+    long long qoff;  // grid offset in the Q arena (floats)
+    long long voff;  // V offset in the V arena (complex values)
+};
+
+// One pass of the batched pipeline over up to kMaxBatch events: the plan of
+// every (event, plane) and the work-item prefixes of the persistent kernels
+// (index e * np + ip, events major).
+struct BatchPlan {
+    int nev, np;
+    int status;        // kBatch* bits
+    int total_visits;
+    int pre_raster[kMaxBatch * kMaxPlanes + 1];
+    int pre_rows[kMaxBatch * kMaxPlanes + 1];   // time-FFT rows: G * nin
+    int pre_orows[kMaxBatch * kMaxPlanes + 1];  // inverse-FFT rows: nout
+    int pre_conv[kMaxPlanes][kMaxBatch + 1];    // wire-convolution tiles of plane ip over events
+    EvPlane ep[kMaxBatch * kMaxPlanes];
+};
+constexpr int kBatchVisitOverflow = 1;
+constexpr int kBatchOversize = 2;
+constexpr int kBatchBigCharge = 4;
+constexpr int kBatchNoClass = 8;
+
+// Launch shapes of the persistent kernels (chosen by the autotuner).
+struct BatchTune {
+    int slots;            // events per pass (event slots in the arenas)
+    int raster_per_sm;    // persistent raster blocks per SM
+    int fft_threads;      // threads per time-FFT row
+    int fft_per_sm;       // persistent time-FFT blocks per SM
+    int conv_per_sm;      // persistent wire-convolution blocks per SM
+};
+
 // ---- launchers (kernels.cu) ----
-void launch_prep_all(const double* depos, int n, const DriftDev& dd, int do_drift, const PlaneSet& ps,
-                     const TimeDev& tb, double drift_speed, double nsigma, PatchRec* rec, WindowDev* win,
-                     int* wire_cnt, float* tprof, unsigned long long* key_bound, cudaStream_t s);
+void launch_prep_all(const double* depos, const EventTable& et, int nkeys, const DriftDev& dd, int do_drift,
+                     const PlaneSet& ps, const TimeDev& tb, double drift_speed, double nsigma, PatchRec* rec,
+                     WindowDev* win, int* wire_cnt, float* tprof, unsigned long long* key_bound, cudaStream_t s);
 void launch_scan(const int* wire_cnt, int nwires_total, int* wire_off, int* wire_cur, cudaStream_t s);
-void launch_fill(const PatchRec* rec, int n, const PlaneSet& ps, int* wire_cur, Visit* visits, cudaStream_t s);
+void launch_fill(const PatchRec* rec, const EventTable& et, int nkeys, const PlaneSet& ps, int* wire_cur,
+                 Visit* visits, long long cap, cudaStream_t s);
 size_t raster_smem_bytes(int G);
 void launch_raster_wires(const PatchRec* rec, const float* tprof, const int* wire_cnt, const int* wire_off,
-                         const Visit* visits, const unsigned long long* key_bound, const GridSet& gs, float* Q,
-                         cudaStream_t s);
+                         const Visit* visits, long long vcap, const unsigned long long* key_bound, const GridSet& gs,
+                         float* Q, cudaStream_t s);
 void launch_rfft_rows(const float* in, long in_ld, int in_len, float2* out, long out_ld, int nrows,
                       const FftDesc& d, cudaStream_t s);
 void launch_wire_conv(const float2* Qh, const float2* Rh, float2* Vh, int ngroups, int npad, int nrows_in,
@@ -138,6 +210,22 @@ void launch_irfft_rows(const float2* Vh, int nrows, const FftDesc& d, int wire0,
 
 void launch_spec_mul(float2* X, long ldx, int nrows, int M, const float2* R, cudaStream_t s);
 void launch_twiddles(float2* tw, float2* twh, int M, cudaStream_t s);
+
+// ---- batched-path launchers (kernels.cu) ----
+void launch_plan_batch(BatchPlan* plan, const BatchStatic& bs, int nev, const WindowDev* win, const int* total_visits,
+                       long long vcap, cudaStream_t s);
+void launch_raster_batch(const BatchPlan* plan, const BatchStatic& bs, const PlaneSet& ps, const PatchRec* rec,
+                         long long recstride, const float* tprof, const int* wire_cnt, const int* wire_off,
+                         const Visit* visits, long long vcap, const unsigned long long* key_bound, float* Q,
+                         int nblocks, int maxG, cudaStream_t s);
+void launch_rfft_batch(const BatchPlan* plan, const FftDesc* descs, float* Q, int nblocks, int nthreads, int maxM,
+                       cudaStream_t s);
+void launch_conv_batch(const BatchPlan* plan, const BatchStatic& bs, int ip, bool pair, const float2* const* spec,
+                       const float* Q, float2* V, int nblocks, cudaStream_t s);
+void launch_irfft_batch(const BatchPlan* plan, const BatchStatic& bs, const FftDesc* descs, const float2* V,
+                        float* frames, long long frame_stride, int nblocks, int nthreads, int maxM, cudaStream_t s);
+size_t conv_smem_bytes(int npad, bool pair);
+void batch_kernel_attributes(int maxG, int maxM);
 
 // ---- adjoint launchers (adjoint.cu) ----
 void launch_grad_rows(const float* gframe, int nticks, int wire0, int wlo, int whi, int tick0, int ncols, int nrows,
