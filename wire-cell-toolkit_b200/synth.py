@@ -190,10 +190,12 @@ def apa_depos(seed=2, ntracks=20):
     return track_depos(rng, ntracks=ntracks)
 
 
-def shower_depos(rng, n, center=None, radius=300.0 * mm, energy_mev=1000.0, ext_max=25.0 * mm):
-    """A Gaussian blob of n depos around ``center`` carrying ``energy_mev`` with
-    initial longitudinal/transverse extents up to ``ext_max`` (so patch sizes
-    reach tens of impact bins and up to ~200 ticks)."""
+def shower_depos(rng, n, center=None, radius=300.0 * mm, energy_mev=1000.0, ext_long_max=26.0 * mm,
+                 ext_tran_max=2.4 * mm):
+    """A Gaussian blob of n depos around ``center`` carrying ``energy_mev``, with
+    initial extents uniform up to ``ext_long_max`` along the drift and
+    ``ext_tran_max`` across it: with diffusion over 0-2.5 m of drift the patches
+    span from ~3 x 10 up to ~40 impact bins x ~200 ticks."""
     if center is None:
         center = np.array([RESPONSE_X + rng.uniform(200, 2300), rng.uniform(-2500, 2500), rng.uniform(-900, 900)])
     pos = center[None, :] + rng.normal(0.0, radius / 3.0, (n, 3))
@@ -203,8 +205,8 @@ def shower_depos(rng, n, center=None, radius=300.0 * mm, energy_mev=1000.0, ext_
     d = np.zeros((n, 7))
     d[:, 1] = -(e / 23.6e-6) * 0.7
     d[:, 2:5] = pos
-    d[:, 5] = rng.uniform(0.0, ext_max, n)
-    d[:, 6] = rng.uniform(0.0, ext_max, n)
+    d[:, 5] = rng.uniform(0.0, ext_long_max, n)
+    d[:, 6] = rng.uniform(0.0, ext_tran_max, n)
     return d
 
 
