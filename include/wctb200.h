@@ -140,9 +140,11 @@ int wct_convolve_rows_device_noalloc(const float* in, long ld_in, int nrows, int
 /* DepoTransform::configure (gen/src/DepoTransform.cxx:76-113) from JSON with
  * the reference keys: anode, pirs, dft, rng, fluctuate, nsigma, start_time,
  * readout_time, tick, drift_speed, first_frame_number.  Optional extra keys:
- * "drifter" {DL, DT, lifetime, drift_speed, time_offset, xregions:[{anode,
- * response, cathode}]} to drift depos on the device before the transform
- * (Drifter, gen/src/Drifter.cxx:94-123), and "device" (CUDA ordinal). */
+ * "drifter" {DL, DT, lifetime, drift_speed, time_offset, fluctuate,
+ * xregions:[{anode, response, cathode}]} to drift depos on the device before
+ * the transform (Drifter, gen/src/Drifter.cxx:94-123; fluctuate defaults to
+ * false here), "device" (CUDA ordinal) and "seed" (key of the random streams
+ * that "fluctuate" draws from, in place of the reference's "rng" component). */
 int wct_dt_create(const char* json_config, wct_depotransform** out);
 /* DepoTransform::default_configuration (gen/src/DepoTransform.cxx:114-153) as JSON. */
 int wct_dt_default_configuration(char* buf, size_t len);
@@ -228,6 +230,21 @@ int wct_dt_batch_tune(wct_depotransform* dt, int* params, int set);
  * JSON report of every candidate and its time to report (may be NULL). */
 int wct_dt_autotune_batch(wct_depotransform* dt, const double* d_depos, const long long* offsets, int nevents,
                           float* d_frames, void* stream, char* report, size_t len);
+
+/* ---- Random numbers of the fluctuated forward ----
+ *
+ * With "fluctuate": true (DepoTransform, gen/src/DepoTransform.cxx:82-87) every
+ * patch cell is redrawn as Binomial(|Q|, cell fraction) and the patch rescaled
+ * to Q (gen/src/GaussianDiffusion.cxx:184-213); with a drifter "fluctuate":
+ * true the absorbed electrons are Binomial(|Q|, 1 - exp(-dt / lifetime))
+ * (gen/src/Drifter.cxx:177-185).  The draws come from counter-based streams
+ * (Philox-4x32-10) keyed by the configuration's "seed" and each event's frame
+ * ident, so a call is reproducible and successive frames draw afresh.
+ * IRandom::binomial (iface/inc/WireCellIface/IRandom.h) in bulk: count
+ * independent Binomial(n, p) draws of the stream (seed, ident) into d_out
+ * (device), enqueued on stream (NULL = legacy default stream). */
+int wct_random_binomial_device(unsigned long long seed, int ident, int n, double p, long count, int* d_out,
+                               void* stream);
 
 /* Reverse-mode derivative of wct_dt_forward (no counterpart in the reference,
  * whose DepoTransform is forward only).  Given grad_frame = dL/d(frame)

@@ -54,6 +54,7 @@ def lib():
         _lib.orc_run.restype = C.c_int
         _lib.orc_run.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
         _lib.orc_edge.argtypes = [C.c_void_p, C.c_int, C.c_void_p]
+        _lib.orc_binomial_samples.argtypes = [C.c_ulonglong, C.c_int, C.c_double, C.c_long, C.c_void_p]
     return _lib
 
 
@@ -105,6 +106,7 @@ class OrcJob(C.Structure):
         ("nplanes", C.c_int), ("planes", C.c_void_p),
         ("ndepos", C.c_int), ("depos", C.c_void_p),
         ("fp64", C.c_int), ("nthreads", C.c_int),
+        ("fluctuate", C.c_int), ("drift_fluctuate", C.c_int), ("seed", C.c_ulonglong),
     ]
 
 
@@ -116,9 +118,13 @@ class OrcPlaneOut(C.Structure):
 class Job:
     """Owns the numpy buffers an OrcJob points into."""
 
-    def __init__(self, cfg, depos, drift=True, fp64=False, nthreads=1):
+    def __init__(self, cfg, depos, drift=True, fp64=False, nthreads=1, fluctuate=False, drift_fluctuate=False,
+                 seed=0):
         self.keep = []
         j = OrcJob()
+        j.fluctuate = 1 if fluctuate else 0
+        j.drift_fluctuate = 1 if drift_fluctuate else 0
+        j.seed = int(seed)
         j.start_time = cfg["start_time"]
         j.readout_time = cfg["readout_time"]
         j.tick = cfg["tick"]
@@ -187,10 +193,14 @@ def fft_best_length(n, keep=False):
     return lib().orc_fft_best_length(int(n), 1 if keep else 0)
 
 
-def run(cfg, depos, drift=True, fp64=False, nthreads=1, records=False):
+def run(cfg, depos, drift=True, fp64=False, nthreads=1, records=False, fluctuate=False, drift_fluctuate=False,
+        seed=0):
     """Run the restated DepoTransform. Returns dict(frames=[per-plane
-    [nwires][nticks]], windows=[OrcPlaneOut as dict], records=optional)."""
-    job = Job(cfg, depos, drift=drift, fp64=fp64, nthreads=nthreads)
+    [nwires][nticks]], windows=[OrcPlaneOut as dict], records=optional).
+    ``fluctuate`` / ``drift_fluctuate`` draw the reference's binomial
+    fluctuations with std::mt19937 streams seeded from ``seed``."""
+    job = Job(cfg, depos, drift=drift, fp64=fp64, nthreads=nthreads, fluctuate=fluctuate,
+              drift_fluctuate=drift_fluctuate, seed=seed)
     nticks = int(cfg["readout_time"] / cfg["tick"])
     nw = [pl["nwires"] for pl in cfg["planes"]]
     dt = np.float64 if fp64 else np.float32
@@ -210,6 +220,13 @@ def run(cfg, depos, drift=True, fp64=False, nthreads=1, records=False):
         r0 += n
     wins = [{f: getattr(p, f) for f, _ in OrcPlaneOut._fields_} for p in pouts]
     return dict(frames=frames, windows=wins, records=rec)
+
+
+def binomial_samples(n, p, count, seed=1):
+    """``count`` draws of std::binomial_distribution<int>(n, p) over std::mt19937."""
+    out = np.zeros(count, dtype=np.int32)
+    lib().orc_binomial_samples(int(seed), int(n), float(p), int(count), out.ctypes.data)
+    return out
 
 
 def drift(cfg, depos):

@@ -35,6 +35,7 @@
 #include <map>
 #include <memory>
 #include <mutex>
+#include <random>
 #include <stdexcept>
 #include <thread>
 #include <unordered_map>
@@ -336,7 +337,7 @@ struct Depo {
 };
 
 // ---------------------------------------------------------------------------
-// Drifter::insert (no fluctuation) -- gen/src/Drifter.cxx:127-196,
+// Drifter::insert -- gen/src/Drifter.cxx:127-196,
 // Xregion tests gen/src/Drifter.cxx:53-60.
 // ---------------------------------------------------------------------------
 struct XRegion {
@@ -348,6 +349,7 @@ struct XRegion {
 struct DriftParams {
     double DL, DT, lifetime, speed, toffset;
     std::vector<XRegion> xregions;
+    std::mt19937* rng{nullptr};  // Drifter "fluctuate": binomial absorption (Drifter.cxx:177-185)
 };
 
 static bool drift_one(const DriftParams& dp, const Depo& in, Depo& out)
@@ -371,6 +373,11 @@ static bool drift_one(const DriftParams& dp, const Depo& in, Depo& out)
     if (direction > 0) {
         const double absorbprob = 1 - exp(-dt / dp.lifetime);
         double dQ = Qi * absorbprob;
+        if (dp.rng) {
+            const double sign = Qi < 0 ? -1.0 : 1.0;
+            std::binomial_distribution<int> bin((int)std::abs(Qi), absorbprob);
+            dQ = sign * bin(*dp.rng);
+        }
         Qf = Qi - dQ;
         dL = sqrt(2.0 * dp.DL * dt + dL * dL);
         dT = sqrt(2.0 * dp.DT * dt + dT * dT);
@@ -488,7 +495,7 @@ struct Patch {
 
 template <typename T>
 static void set_sampling(const Depo& depo, const GausDesc& td, const GausDesc& pd, const Binning& tb,
-                         const Binning& pb, double nsigma, Patch<T>& out)
+                         const Binning& pb, double nsigma, Patch<T>& out, std::mt19937* fluctuate = nullptr)
 {
     out.toffset = out.poffset = -1;
     out.nt = out.np = 0;
@@ -523,6 +530,31 @@ static void set_sampling(const Depo& depo, const GausDesc& td, const GausDesc& p
     const double depo_charge = depo.q;
     const T scale = (T)(depo_charge / raw_sum);  // Eigen float array *= double scalar
     for (auto& v : out.val) v *= scale;
+    // GaussianDiffusion.cxx:184-213: every cell redrawn as Binomial(|Q|, cell / Q),
+    // the patch rescaled to the depo charge; a patch whose draws are all zero is
+    // not kept (the depo adds nothing)
+    if (fluctuate) {
+        const double charge_sign = depo_charge < 0 ? -1 : 1;
+        double fluc_sum = 0;
+        for (auto& v : out.val) {
+            const double relval = (double)v / depo_charge;
+            double number;
+            if (relval >= 1.0) number = (int)std::abs(depo_charge);
+            else {
+                std::binomial_distribution<int> bin((int)std::abs(depo_charge), relval);
+                number = bin(*fluctuate);
+            }
+            number *= charge_sign;
+            fluc_sum += number;
+            v = (T)number;
+        }
+        if (fluc_sum == 0) {
+            out.val.assign(out.val.size(), (T)0);
+            return;
+        }
+        const T f = (T)(depo_charge / fluc_sum);
+        for (auto& v : out.val) v *= f;
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -655,6 +687,7 @@ struct BinnedDiffusion {
     double nsigma;
     std::vector<Diff> diffs;
     int outside_time{0}, outside_pitch{0};
+    std::mt19937* fluctuate{nullptr};
     BinnedDiffusion(const Pimpos& p, const Binning& tb, double ns) : pimpos(p), tbins(tb), nsigma(ns) {}
 
     // BinnedDiffusion_transform.cxx:37-92
@@ -703,7 +736,7 @@ struct BinnedDiffusion {
         int counter = 0;
         Patch<T> patch;
         for (auto& d : diffs) {
-            set_sampling<T>(d.depo, d.td, d.pd, tbins, ib, nsigma, patch);
+            set_sampling<T>(d.depo, d.td, d.pd, tbins, ib, nsigma, patch, fluctuate);
             counter++;
             if (rec) {
                 auto& r = (*rec)[d.depo.index];
@@ -964,6 +997,12 @@ struct OrcJob {
     const double* depos;  // [n][7] t, q, x, y, z, extent_long, extent_tran
     int fp64;
     int nthreads;
+    // fluctuation (reference distribution): DepoTransform "fluctuate" and the
+    // Drifter's, drawn with std::mt19937 and std::binomial_distribution as
+    // gen/src/Random.cxx does; seed of the streams (one per plane, one for the drift)
+    int fluctuate;
+    int drift_fluctuate;
+    unsigned long long seed;
 };
 
 struct OrcPlaneOut {
@@ -972,6 +1011,17 @@ struct OrcPlaneOut {
 };
 
 int orc_fft_best_length(long n, int keep) { return (int)orc::fft_best_length((size_t)n, keep != 0); }
+
+// Binomial draws of the reference's generator (gen/src/Random.cxx:55-58 with
+// the "twister" engine): std::binomial_distribution<int> over std::mt19937.
+void orc_binomial_samples(unsigned long long seed, int n, double p, long count, int* out)
+{
+    std::mt19937 g((std::uint32_t)seed);
+    for (long i = 0; i < count; ++i) {
+        std::binomial_distribution<int> bin(n, p);
+        out[i] = bin(g);
+    }
+}
 
 int orc_binning_bin(int nbins, double lo, double hi, double v) { return orc::Binning(nbins, lo, hi).bin(v); }
 
@@ -1103,6 +1153,8 @@ int orc_run(const OrcJob* job, void* frame, OrcPlaneOut* pout, int* rec)
             orc::DriftParams dp{job->DL, job->DT, job->lifetime, job->drifter_speed, job->toffset, {}};
             for (int i = 0; i < job->nxregions; ++i)
                 dp.xregions.push_back({job->xregions[3 * i], job->xregions[3 * i + 1], job->xregions[3 * i + 2]});
+            std::mt19937 drng((std::uint32_t)(job->seed * 2654435761ull + 977));
+            if (job->drift_fluctuate) dp.rng = &drng;
             depos = orc::drift_all(dp, depos);  // keeps each depo's input index
         }
         // face sensitive volume: DepoTools.cxx:110-123
@@ -1133,6 +1185,8 @@ int orc_run(const OrcJob* job, void* frame, OrcPlaneOut* pout, int* rec)
                               job->pir_nticks, pir);
             orc::Binning tbins(job->readout_time / job->tick, job->start_time, job->start_time + job->readout_time);
             orc::BinnedDiffusion<T> bd(pim, tbins, job->nsigma);
+            std::mt19937 prng((std::uint32_t)(job->seed * 2654435761ull + 31 * (unsigned long long)ip + 1));
+            if (job->fluctuate) bd.fluctuate = &prng;
             std::vector<orc::PlaneRecord> precs(ndep_rec);
             for (auto& d : face) {
                 bool ok = bd.add(d, d.el / job->drift_speed, d.et);

@@ -102,6 +102,8 @@ SIGNATURES = {
     "wct_dt_batch_tune": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int]),
     "wct_dt_autotune_batch": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p,
                                         C.c_char_p, C.c_size_t]),
+    "wct_random_binomial_device": (C.c_int, [C.c_ulonglong, C.c_int, C.c_int, C.c_double, C.c_long, C.c_void_p,
+                                             C.c_void_p]),
     "wct_dt_destroy": (C.c_int, [C.c_void_p]),
 }
 
@@ -209,7 +211,7 @@ class DepoTransform:
     depos on the device first."""
 
     CONFIG_KEYS = ("anode", "pirs", "dft", "rng", "fluctuate", "nsigma", "start_time", "readout_time", "tick",
-                   "drift_speed", "first_frame_number", "drifter", "device")
+                   "drift_speed", "first_frame_number", "drifter", "device", "seed")
 
     def __init__(self, cfg=None):
         L = lib()
@@ -423,6 +425,12 @@ def _jsonable(o):
     return o
 
 
+def binomial_device(seed, ident, n, p, count, d_out_ptr, stream=None):
+    """``count`` Binomial(n, p) draws of the stream (seed, ident) into device memory."""
+    _check(lib().wct_random_binomial_device(int(seed), int(ident), int(n), float(p), int(count),
+                                            C.c_void_p(d_out_ptr), C.c_void_p(stream) if stream else None))
+
+
 def drifter_json(dr):
     """Drifter configuration with xregions as objects (gen/src/Drifter.cxx:36-52)."""
     d = dict(dr)
@@ -434,7 +442,7 @@ def from_config(cfg, device=0):
     """Build a DepoTransform for a synthetic workload description (see synth.py):
     one face with cfg["planes"], PIRs from cfg["fr"] and the short responses."""
     dcfg = {k: cfg[k] for k in ("tick", "start_time", "readout_time", "drift_speed", "nsigma", "fluctuate",
-                                 "first_frame_number") if k in cfg}
+                                 "seed", "first_frame_number") if k in cfg}
     if cfg.get("drifter"):
         dcfg["drifter"] = drifter_json(cfg["drifter"])
     dcfg["device"] = device

@@ -166,6 +166,8 @@ struct Core {
     double drift_speed{1.0e-3};
     double nsigma{3.0};
     bool fluctuate{false};
+    bool drift_fluctuate{false};
+    unsigned long long seed{0};  // key of the counter-based random streams
     int frame_count{0};
     int device{0};
     bool have_drifter{false};
@@ -177,6 +179,7 @@ struct Core {
     // workspace
     DevBuf d_rec, d_win, d_Q, d_V, d_depos, d_frame, d_wcnt, d_woff, d_wcur, d_wlist, d_tprof, d_kbound;
     DevBuf d_gframe, d_gdep, d_gglob;  // adjoint host entry point
+    DevBuf d_fq, d_fluc;               // fluctuation: drifted charges, per (plane, depo) draw sums
     int config_gen{0};                 // bumped by every change of planes or responses
     std::unique_ptr<struct BatchState> batch;
     WindowDev* h_win{nullptr};
@@ -284,6 +287,7 @@ static int configure(Core& c, const std::string& js)
     }
     c.nsigma = cfg["nsigma"].as_number(c.nsigma);
     c.fluctuate = cfg["fluctuate"].as_bool(false);
+    c.seed = (unsigned long long)cfg["seed"].as_number(0.0);
     c.readout_time = cfg["readout_time"].as_number(c.readout_time);
     c.tick = cfg["tick"].as_number(c.tick);
     c.start_time = cfg["start_time"].as_number(c.start_time);
@@ -295,7 +299,6 @@ static int configure(Core& c, const std::string& js)
         if (p.kind != json::Value::Array || p.arr.empty())
             return fail(WCT_ERR_CONFIG, "must configure with some plane impact response components");
     }
-    if (c.fluctuate) return fail(WCT_ERR_CONFIG, "fluctuate=true is not supported by this build of the forward path");
     if (c.tick <= 0 || c.readout_time <= 0) return fail(WCT_ERR_CONFIG, "tick and readout_time must be positive");
     if (c.drift_speed <= 0) return fail(WCT_ERR_CONFIG, "illegal drift speed");
     const auto& dr = cfg["drifter"];
@@ -307,8 +310,7 @@ static int configure(Core& c, const std::string& js)
         d.lifetime = dr["lifetime"].as_number(8.0e6);
         d.speed = dr["drift_speed"].as_number(1.6e-3);
         d.toffset = dr["time_offset"].as_number(0.0);
-        if (dr["fluctuate"].as_bool(false))
-            return fail(WCT_ERR_CONFIG, "drifter fluctuate=true is not supported by this build of the forward path");
+        c.drift_fluctuate = dr["fluctuate"].as_bool(false);
         const auto& xr = dr["xregions"];
         if (xr.kind != json::Value::Array || xr.arr.empty()) return fail(WCT_ERR_CONFIG, "no xregions given");
         if (xr.arr.size() > 8) return fail(WCT_ERR_CONFIG, "at most 8 xregions");
@@ -409,6 +411,7 @@ struct EventPlan {
     int n{0}, np{0}, nticks{0};
     int nkeys{0};
     EventTable et{};
+    FlucParams fp{};
     TimeDev tb{};
     PlaneSet pset{};
     GridSet gset{};
@@ -416,7 +419,21 @@ struct EventPlan {
     int total_visits{0};
 };
 
-static int prepare_event(Core& c, const double* d_depos, size_t ndepos, cudaStream_t s, EventPlan& ev)
+// Random-stream parameters of one call (fluct = false: the mean model, as the adjoint needs).
+static FlucParams fluc_params(const Core& c, bool fluct, int ident0, const int* ident_base)
+{
+    FlucParams fp{};
+    fp.on_patch = fluct && c.fluctuate ? 1 : 0;
+    fp.on_drift = fluct && c.drift_fluctuate && c.have_drifter ? 1 : 0;
+    fp.key0 = (unsigned)(c.seed & 0xffffffffull);
+    fp.key1 = (unsigned)(c.seed >> 32);
+    fp.ident0 = ident0;
+    fp.ident_base = ident_base;
+    return fp;
+}
+
+static int prepare_event(Core& c, const double* d_depos, size_t ndepos, cudaStream_t s, EventPlan& ev,
+                         bool fluct = true)
 {
     if (c.planes.empty()) return fail(WCT_ERR_STATE, "no planes configured");
     if ((int)c.planes.size() > kMaxPlanes) return fail(WCT_ERR_CONFIG, "too many planes for one component");
@@ -474,9 +491,14 @@ static int prepare_event(Core& c, const double* d_depos, size_t ndepos, cudaStre
     et.dep0[1] = n;
     et.blk0[0] = 0;
     et.blk0[1] = (n + 255) / 256;
+    ev.fp = fluc_params(c, fluct, c.frame_count, nullptr);
+    if (ev.fp.on_patch) {
+        CUDA_TRY(c.d_fq.ensure(sizeof(double) * (size_t)std::max(n, 1)));
+        CUDA_TRY(c.d_fluc.ensure(sizeof(FlucRec) * (size_t)np * std::max(n, 1)));
+    }
     launch_prep_all(d_depos, et, nkeys, c.drifter, c.have_drifter ? 1 : 0, pset, tb, c.drift_speed, c.nsigma,
                     c.d_rec.as<PatchRec>(), c.d_win.as<WindowDev>(), c.d_wcnt.as<int>(), c.d_tprof.as<float>(),
-                    c.d_kbound.as<unsigned long long>(), s);
+                    c.d_kbound.as<unsigned long long>(), ev.fp, ev.fp.on_patch ? c.d_fq.as<double>() : nullptr, s);
     launch_scan(c.d_wcnt.as<int>(), nkeys, c.d_woff.as<int>(), c.d_wcur.as<int>(), s);
     t_prep.close(4 + (n > 0 ? 1 : 0));
     CUDA_TRY(cudaGetLastError());
@@ -553,10 +575,18 @@ static int forward_device(Core& c, const double* d_depos, size_t ndepos, float* 
     Core::StageTimer t_r(&c, 1, s);
     launch_fill(c.d_rec.as<PatchRec>(), ev.et, ev.nkeys, pset, c.d_wcur.as<int>(), c.d_wlist.as<Visit>(),
                 (long long)std::max(total_visits, 1), s);
-    launch_raster_wires(c.d_rec.as<PatchRec>(), c.d_tprof.as<float>(), c.d_wcnt.as<int>(), c.d_woff.as<int>(),
-                        c.d_wlist.as<Visit>(), (long long)std::max(total_visits, 1),
-                        c.d_kbound.as<unsigned long long>(), gset, c.d_Q.as<float>(), s);
-    t_r.close((n > 0 ? 1 : 0) + (rows > 0 ? 1 : 0));
+    if (ev.fp.on_patch) {
+        launch_fluc_sums(c.d_rec.as<PatchRec>(), ev.et, pset, (float)ev.tb.bs, ev.fp, c.d_fq.as<double>(),
+                         c.d_fluc.as<FlucRec>(), s);
+        launch_raster_fluc(c.d_rec.as<PatchRec>(), c.d_fluc.as<FlucRec>(), ev.fp, ev.et, c.d_wcnt.as<int>(),
+                           c.d_woff.as<int>(), c.d_wlist.as<Visit>(), (long long)std::max(total_visits, 1), gset,
+                           c.d_Q.as<float>(), s);
+    }
+    else
+        launch_raster_wires(c.d_rec.as<PatchRec>(), c.d_tprof.as<float>(), c.d_wcnt.as<int>(), c.d_woff.as<int>(),
+                            c.d_wlist.as<Visit>(), (long long)std::max(total_visits, 1),
+                            c.d_kbound.as<unsigned long long>(), gset, c.d_Q.as<float>(), s);
+    t_r.close((n > 0 ? 1 : 0) + (rows > 0 ? 1 : 0) + (ev.fp.on_patch && n > 0 ? 1 : 0));
     CUDA_TRY(cudaGetLastError());
 
     for (int ip = 0; ip < np; ++ip) {
@@ -618,7 +648,7 @@ static int adjoint_device(Core& c, const double* d_depos, size_t ndepos, const f
                           double* d_gglob, cudaStream_t s)
 {
     EventPlan ev;
-    int prc = prepare_event(c, d_depos, ndepos, s, ev);
+    int prc = prepare_event(c, d_depos, ndepos, s, ev, false);  // the mean model
     if (prc) return prc;
     const int n = ev.n, np = ev.np, nticks = ev.nticks;
     if (n) CUDA_TRY(cudaMemsetAsync(d_gdep, 0, sizeof(double) * 7 * (size_t)n, s));
@@ -774,6 +804,8 @@ struct BatchState {
     DevBuf d_spec_tab;                          // const float2* [plane][ncls]
     int maxM{0}, maxG{0}, nsm{148};
     DevBuf d_Q, d_V, d_rec, d_tprof, d_win, d_wcnt, d_woff, d_wcur, d_kbound, d_wlist, d_plans;
+    DevBuf d_fq, d_fluc, d_ident;  // fluctuation: drifted charges, draw sums, first frame ident of the call
+    int* h_ident{nullptr};         // pinned source of d_ident
     long long vcap{0};
     BatchPlan* h_plans{nullptr};
     size_t h_plans_n{0};
@@ -787,6 +819,8 @@ struct BatchState {
     long long g_vcap{0};
     cudaStream_t g_stream{nullptr};
     DriftDev g_drift{};
+    int g_fluc[2]{0, 0};
+    unsigned long long g_seed{0};
     std::vector<void*> g_bufs;
     void drop_graph()
     {
@@ -797,6 +831,7 @@ struct BatchState {
     {
         drop_graph();
         if (h_plans) cudaFreeHost(h_plans);
+        if (h_ident) cudaFreeHost(h_ident);
     }
 };
 
@@ -977,7 +1012,8 @@ static int forward_batch_device(Core& c, const double* d_depos, const long long*
 
     for (int attempt = 0; attempt < 3; ++attempt) {
         std::vector<void*> before = {b.d_Q.p, b.d_V.p, b.d_rec.p, b.d_tprof.p, b.d_win.p, b.d_wcnt.p, b.d_woff.p,
-                                     b.d_wcur.p, b.d_kbound.p, b.d_wlist.p, b.d_plans.p};
+                                     b.d_wcur.p, b.d_kbound.p, b.d_wlist.p, b.d_plans.p, b.d_fq.p, b.d_fluc.p,
+                                     b.d_ident.p};
         CUDA_TRY(b.d_Q.ensure(sizeof(float) * (size_t)bs.qslot_total * K));
         CUDA_TRY(b.d_V.ensure(sizeof(float2) * (size_t)bs.vslot_total * K));
         CUDA_TRY(b.d_rec.ensure(sizeof(PatchRec) * (size_t)np * maxdep));
@@ -989,8 +1025,15 @@ static int forward_batch_device(Core& c, const double* d_depos, const long long*
         CUDA_TRY(b.d_kbound.ensure(sizeof(unsigned long long) * (size_t)nkeysK * kTileBlocks));
         CUDA_TRY(b.d_wlist.ensure(sizeof(Visit) * (size_t)b.vcap));
         CUDA_TRY(b.d_plans.ensure(sizeof(BatchPlan) * (size_t)nch));
+        CUDA_TRY(b.d_ident.ensure(sizeof(int)));
+        if (c.fluctuate) {
+            CUDA_TRY(b.d_fq.ensure(sizeof(double) * (size_t)maxdep));
+            CUDA_TRY(b.d_fluc.ensure(sizeof(FlucRec) * (size_t)np * maxdep));
+        }
+        if (!b.h_ident) CUDA_TRY(cudaMallocHost(&b.h_ident, sizeof(int)));
         std::vector<void*> after = {b.d_Q.p, b.d_V.p, b.d_rec.p, b.d_tprof.p, b.d_win.p, b.d_wcnt.p, b.d_woff.p,
-                                    b.d_wcur.p, b.d_kbound.p, b.d_wlist.p, b.d_plans.p};
+                                    b.d_wcur.p, b.d_kbound.p, b.d_wlist.p, b.d_plans.p, b.d_fq.p, b.d_fluc.p,
+                                    b.d_ident.p};
         if (b.h_plans_n < (size_t)nch) {
             if (b.h_plans) cudaFreeHost(b.h_plans);
             b.h_plans = nullptr;
@@ -1001,6 +1044,8 @@ static int forward_batch_device(Core& c, const double* d_depos, const long long*
                           b.g_frames == d_frames && b.g_stream == s && b.g_vcap == b.vcap &&
                           std::memcmp(&b.g_tune, &b.tune, sizeof(BatchTune)) == 0 &&
                           std::memcmp(&b.g_drift, &c.drifter, sizeof(DriftDev)) == 0 &&
+                          b.g_fluc[0] == (int)c.fluctuate && b.g_fluc[1] == (int)c.drift_fluctuate &&
+                          b.g_seed == c.seed &&
                           b.g_offsets.size() == (size_t)nev + 1 &&
                           std::equal(b.g_offsets.begin(), b.g_offsets.end(), offsets);
         if (!same) {
@@ -1026,17 +1071,25 @@ static int forward_batch_device(Core& c, const double* d_depos, const long long*
                 cudaMemsetAsync(b.d_wcnt.p, 0, sizeof(int) * (size_t)(nk + 1), s);
                 cudaMemsetAsync(b.d_kbound.p, 0, sizeof(unsigned long long) * (size_t)nk * kTileBlocks, s);
                 k_win_init<<<(ne * np + 63) / 64, 64, 0, s>>>(b.d_win.as<WindowDev>(), ne * np);
+                // random streams keyed by the frame ident of each event: base (a device
+                // value written before every launch of the graph) + c0 + event
+                const FlucParams fp = fluc_params(c, true, c0, b.d_ident.as<int>());
                 launch_prep_all(dep, et, bs.nkeys, c.drifter, c.have_drifter ? 1 : 0, pset, tb, c.drift_speed,
                                 c.nsigma, b.d_rec.as<PatchRec>(), b.d_win.as<WindowDev>(), b.d_wcnt.as<int>(),
-                                b.d_tprof.as<float>(), b.d_kbound.as<unsigned long long>(), s);
+                                b.d_tprof.as<float>(), b.d_kbound.as<unsigned long long>(), fp,
+                                fp.on_patch ? b.d_fq.as<double>() : nullptr, s);
                 launch_scan(b.d_wcnt.as<int>(), (int)nk, b.d_woff.as<int>(), b.d_wcur.as<int>(), s);
                 launch_plan_batch(plans + ch, bs, ne, b.d_win.as<WindowDev>(), b.d_woff.as<int>() + nk, b.vcap, s);
                 launch_fill(b.d_rec.as<PatchRec>(), et, bs.nkeys, pset, b.d_wcur.as<int>(), b.d_wlist.as<Visit>(),
                             b.vcap, s);
                 cudaMemsetAsync(d_frames + c0 * fstride, 0, sizeof(float) * (size_t)(ne * fstride), s);
+                if (fp.on_patch)
+                    launch_fluc_sums(b.d_rec.as<PatchRec>(), et, pset, (float)tb.bs, fp, b.d_fq.as<double>(),
+                                     b.d_fluc.as<FlucRec>(), s);
                 launch_raster_batch(plans + ch, bs, pset, b.d_rec.as<PatchRec>(), et.dep0[ne], b.d_tprof.as<float>(),
                                     b.d_wcnt.as<int>(), b.d_woff.as<int>(), b.d_wlist.as<Visit>(), b.vcap,
-                                    b.d_kbound.as<unsigned long long>(), b.d_Q.as<float>(), nb_r, b.maxG, s);
+                                    b.d_kbound.as<unsigned long long>(), b.d_Q.as<float>(), nb_r, b.maxG, et, fp,
+                                    b.d_fluc.as<FlucRec>(), s);
                 launch_rfft_batch(plans + ch, b.d_descs.as<FftDesc>(), b.d_Q.as<float>(), nb_f, b.tune.fft_threads,
                                   b.maxM, s);
                 for (int ip = 0; ip < np; ++ip)
@@ -1064,8 +1117,13 @@ static int forward_batch_device(Core& c, const double* d_depos, const long long*
             b.g_vcap = b.vcap;
             b.g_tune = b.tune;
             b.g_drift = c.drifter;
+            b.g_fluc[0] = (int)c.fluctuate;
+            b.g_fluc[1] = (int)c.drift_fluctuate;
+            b.g_seed = c.seed;
             b.g_offsets.assign(offsets, offsets + nev + 1);
         }
+        *b.h_ident = c.frame_count;
+        CUDA_TRY(cudaMemcpyAsync(b.d_ident.p, b.h_ident, sizeof(int), cudaMemcpyHostToDevice, s));
         CUDA_TRY(cudaGraphLaunch(b.exec, s));
         // statuses (and windows when asked for) of every pass
         const size_t head = offsetof(BatchPlan, pre_raster);
@@ -1685,6 +1743,16 @@ int wct_dt_batch_tune(wct_depotransform* h, int* params, int set)
         params[3] = t.fft_per_sm;
         params[4] = t.conv_per_sm;
     }
+    return WCT_OK;
+}
+
+int wct_random_binomial_device(unsigned long long seed, int ident, int n, double p, long count, int* d_out,
+                               void* stream)
+{
+    if (n < 0 || count < 0 || (count > 0 && !d_out) || !(p >= 0.0 && p <= 1.0))
+        return fail(WCT_ERR_ARG, "wct_random_binomial_device: bad arguments");
+    launch_binomial_samples(seed, ident, n, p, count, d_out, (cudaStream_t)stream);
+    CUDA_TRY(cudaGetLastError());
     return WCT_OK;
 }
 

@@ -24,6 +24,7 @@
 
 #include "kernels.cuh"
 #include "gauss.cuh"
+#include "rng.cuh"
 
 #include <algorithm>
 #include <cfloat>
@@ -115,6 +116,12 @@ __device__ __forceinline__ int event_of_block(const EventTable& et, int b)
     return lo;
 }
 
+// Frame ident of event ev of the launch: the key of its random streams.
+__device__ __forceinline__ int fluc_ident(const FlucParams& fp, int ev)
+{
+    return (fp.ident_base ? *fp.ident_base : 0) + fp.ident0 + ev;
+}
+
 // One thread per depo of every event of the table; per-event window
 // statistics, visit counters and bounds (nkeys keys per event); patch
 // records [plane][depo] and time profiles indexed by the depo's position in
@@ -123,7 +130,8 @@ __global__ void __launch_bounds__(256) k_prep_all(const double* __restrict__ dep
                                                   DriftDev dd, int do_drift, PlaneSet ps, TimeDev tb,
                                                   double drift_speed, double nsigma, PatchRec* __restrict__ rec,
                                                   WindowDev* __restrict__ win_all, int* __restrict__ cnt_all,
-                                                  float* __restrict__ tprof, unsigned long long* __restrict__ kb_all)
+                                                  float* __restrict__ tprof, unsigned long long* __restrict__ kb_all,
+                                                  FlucParams fp, double* __restrict__ fq)
 {
     const int ev = event_of_block(evt, blockIdx.x);
     const int i = evt.dep0[ev] + (blockIdx.x - evt.blk0[ev]) * blockDim.x + threadIdx.x;
@@ -158,7 +166,15 @@ __global__ void __launch_bounds__(256) k_prep_all(const double* __restrict__ dep
                     const double dt = fabs(__ddiv_rn(__dsub_rn(respx, x), dd.speed));
                     if (dir > 0) {
                         const double absorb = __dsub_rn(1.0, exp(__ddiv_rn(-dt, dd.lifetime)));
-                        q = __dsub_rn(q, __dmul_rn(q, absorb));
+                        if (fp.on_drift) {
+                            // Binomial(|Q|, absorb) electrons absorbed (Drifter.cxx:179-185)
+                            Philox g;
+                            g.init(fp.key0, fp.key1 + 0x9E3779B9u * (unsigned)fluc_ident(fp, ev),
+                                   (unsigned)(i - evt.dep0[ev]), kRngDriftTag, 0u);
+                            const int nabs = binomial((int)fabs(q), absorb, g);
+                            q = __dsub_rn(q, q < 0 ? -(double)nabs : (double)nabs);
+                        }
+                        else q = __dsub_rn(q, __dmul_rn(q, absorb));
                         el = __dsqrt_rn(__dadd_rn(__dmul_rn(__dmul_rn(2.0, dd.DL), dt), __dmul_rn(el, el)));
                         et = __dsqrt_rn(__dadd_rn(__dmul_rn(__dmul_rn(2.0, dd.DT), dt), __dmul_rn(et, et)));
                     }
@@ -168,6 +184,7 @@ __global__ void __launch_bounds__(256) k_prep_all(const double* __restrict__ dep
             }
         }
     }
+    if (fq && in) fq[i] = q;  // drifted charge, the trial count of fluctuated patches
     // The time profile depends on the depo only (GaussianDiffusion.cxx:124-136):
     // compute it once here for every plane's raster.
     if (ok) {
@@ -352,12 +369,13 @@ __global__ void __launch_bounds__(256) k_prep_all(const double* __restrict__ dep
 
 void launch_prep_all(const double* depos, const EventTable& et, int nkeys, const DriftDev& dd, int do_drift,
                      const PlaneSet& ps, const TimeDev& tb, double drift_speed, double nsigma, PatchRec* rec,
-                     WindowDev* win, int* wire_cnt, float* tprof, unsigned long long* key_bound, cudaStream_t s)
+                     WindowDev* win, int* wire_cnt, float* tprof, unsigned long long* key_bound,
+                     const FlucParams& fp, double* fq, cudaStream_t s)
 {
     const int nblocks = et.blk0[et.nev];
     if (nblocks <= 0) return;
     k_prep_all<<<nblocks, 256, 0, s>>>(depos, et, nkeys, dd, do_drift, ps, tb, drift_speed, nsigma, rec, win,
-                                       wire_cnt, tprof, key_bound);
+                                       wire_cnt, tprof, key_bound, fp, fq);
 }
 
 // Exclusive scan of the per-key visit counts: block sums, a scan of the
@@ -753,6 +771,271 @@ void launch_raster_wires(const PatchRec* rec, const float* tprof, const int* wir
     cudaFuncSetAttribute((const void*)k_raster_wires, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     k_raster_wires<<<gs.nrows_total, kRasterThreads, smem, s>>>(rec, tprof, wire_cnt, wire_off, visits, vcap,
                                                                     key_bound, gs, Q);
+}
+
+// ---------------------------------------------------------------------------
+// Fluctuated patches (GaussianDiffusion::set_sampling with an IRandom,
+// gen/src/GaussianDiffusion.cxx:184-213): every cell (k, tau) of a patch is
+// redrawn as N ~ Binomial((int)|Q|, p_k t_tau / (sum p * sum t)) and the
+// patch is rescaled by Q / sum N; a patch whose draws are all zero adds
+// nothing.  The draws are counter-based: k_fluc_sums draws every cell to get
+// sum N, and the fluctuated raster draws the same cells again.  The unit bin
+// integrals that set each cell's probability come from one non-inlined
+// function with explicitly rounded operations, so both passes see the same
+// probabilities bit for bit and therefore the same draws.
+// ---------------------------------------------------------------------------
+__device__ __noinline__ float unit_bin(int k, float bs, float cr, float sigma)
+{
+    if (!(sigma > 0.f)) return 1.0f;  // point: its single bin holds everything
+    const float inv = __frcp_rn(__fmul_rn(1.41421356237309505f, sigma));
+    const float x1 = __fmul_rn(__fsub_rn(__fmul_rn((float)k, bs), cr), inv);
+    const float x2 = __fmul_rn(__fsub_rn(__fmul_rn((float)(k + 1), bs), cr), inv);
+    return bin_from_edges(copysignf(erfc_nr(fabsf(x1)), x1), copysignf(erfc_nr(fabsf(x2)), x2));
+}
+
+// 1 / (sum of the patch's unit bin integrals in pitch * in time), edge to edge.
+__device__ __noinline__ float patch_inv_norm(const PatchRec& r, float pbs, float tbs)
+{
+    float sp = 1.f, st = 1.f;
+    if (r.sp > 0.f) {
+        const float inv = __frcp_rn(__fmul_rn(1.41421356237309505f, r.sp));
+        const float x1 = __fmul_rn(__fsub_rn(0.f, r.pcr), inv);
+        const float x2 = __fmul_rn(__fsub_rn(__fmul_rn((float)r.np, pbs), r.pcr), inv);
+        sp = bin_from_edges(copysignf(erfc_nr(fabsf(x1)), x1), copysignf(erfc_nr(fabsf(x2)), x2));
+    }
+    if (r.st > 0.f) {
+        const float inv = __frcp_rn(__fmul_rn(1.41421356237309505f, r.st));
+        const float x1 = __fmul_rn(__fsub_rn(0.f, r.tcr), inv);
+        const float x2 = __fmul_rn(__fsub_rn(__fmul_rn((float)r.nt, tbs), r.tcr), inv);
+        st = bin_from_edges(copysignf(erfc_nr(fabsf(x1)), x1), copysignf(erfc_nr(fabsf(x2)), x2));
+    }
+    return __frcp_rn(__fmul_rn(sp, st));
+}
+
+__device__ __forceinline__ int event_of_depo(const EventTable& et, int i)
+{
+    int lo = 0, hi = et.nev - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (et.dep0[mid] <= i) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
+}
+
+// The draw of cell (k, tau) of depo i_ev (index within its event) on plane ip.
+__device__ __forceinline__ int cell_draw(const FlucParams& fp, int ident, int i_ev, int ip, int cell, int nq,
+                                         float relval)
+{
+    Philox g;
+    g.init(fp.key0, fp.key1 + 0x9E3779B9u * (unsigned)ident, (unsigned)i_ev, (unsigned)ip, (unsigned)cell);
+    return binomial(nq, (double)relval, g);
+}
+
+constexpr int kFlucWarps = 4;
+constexpr int kFlucTab = 1024;  // patches hold at most kMaxPatchT ticks and kMaxPatchP bins
+
+// One warp per (plane, depo): the sum of the cell draws.
+__global__ void __launch_bounds__(kFlucWarps * 32) k_fluc_sums(const PatchRec* __restrict__ rec, EventTable evt,
+                                                               PlaneSet ps, float tbs, FlucParams fp,
+                                                               const double* __restrict__ fq,
+                                                               FlucRec* __restrict__ fluc)
+{
+    __shared__ float s_p[kFlucWarps][kFlucTab], s_t[kFlucWarps][kFlucTab];
+    const int wib = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int n = evt.dep0[evt.nev];
+    const long long gw = (long long)blockIdx.x * kFlucWarps + wib;
+    if (gw >= (long long)n * ps.nplanes) return;  // whole warps only; no block barrier follows
+    const int ip = (int)(gw / n), i = (int)(gw - (long long)ip * n);
+    const PatchRec r = rec[(size_t)ip * n + i];
+    FlucRec out{0, 0.f, 0.f, 0};
+    if (r.np > 0 && r.nt > 0) {
+        const float pbs = (float)ps.p[ip].imp_bs;
+        const int np = r.np, nt = r.nt;
+        for (int k = lane; k < np; k += 32) s_p[wib][k] = unit_bin(k, pbs, r.pcr, r.sp);
+        for (int t = lane; t < nt; t += 32) s_t[wib][t] = unit_bin(t, tbs, r.tcr, r.st);
+        __syncwarp();
+        const float invS = patch_inv_norm(r, pbs, tbs);
+        const double Q = fq[i];
+        const int nq = (int)fabs(Q);
+        const int ev = event_of_depo(evt, i);
+        const int ident = fluc_ident(fp, ev), i_ev = i - evt.dep0[ev];
+        long long sum = 0;
+        for (int c = lane; c < np * nt; c += 32) {
+            const int k = c / nt, t = c - k * nt;
+            const float relval = __fmul_rn(__fmul_rn(s_p[wib][k], s_t[wib][t]), invS);
+            sum += cell_draw(fp, ident, i_ev, ip, c, nq, relval);
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);
+        out.nq = nq;
+        out.invS = invS;
+        out.scale = sum > 0 ? (float)(Q / (double)sum) : 0.f;
+    }
+    if (lane == 0) fluc[(size_t)ip * n + i] = out;
+}
+
+void launch_fluc_sums(const PatchRec* rec, const EventTable& et, const PlaneSet& ps, float tbs, const FlucParams& fp,
+                      const double* fq, FlucRec* fluc, cudaStream_t s)
+{
+    const long long warps = (long long)et.dep0[et.nev] * ps.nplanes;
+    if (warps <= 0) return;
+    const long long blocks = (warps + kFlucWarps - 1) / kFlucWarps;
+    k_fluc_sums<<<(unsigned)blocks, kFlucWarps * 32, 0, s>>>(rec, et, ps, tbs, fp, fq, fluc);
+}
+
+// Fluctuated raster of one (charge row, tick tile) item: one warp per visit,
+// lanes over the visit's ticks in the tile, a loop over the patch bins of the
+// row's wire; cell charges N * Q / sum N split between the two impact groups
+// of the bin by its linear weight (BinnedDiffusion_transform.cxx:296-367).
+// Accumulation in 64-bit fixed point (2^-16 electron), so the grid does not
+// depend on the order of the adds.
+constexpr int kFlucRasterThreads = 256;
+constexpr float kFlucFix = 65536.0f;
+
+size_t raster_fluc_smem_bytes(int G) { return sizeof(long long) * (size_t)G * kTileLd; }
+
+__device__ __forceinline__ void raster_tile_fluc(const GridPlane& P, int ip, int row, int ktile, int key_base,
+                                                 int ntiles_abs, const EventTable& evt, const FlucParams& fp,
+                                                 const PatchRec* __restrict__ rec, const FlucRec* __restrict__ fluc,
+                                                 const int* __restrict__ wire_cnt, const int* __restrict__ wire_off,
+                                                 const Visit* __restrict__ visits, long long vcap,
+                                                 float* __restrict__ Q, long long* grid)
+{
+    __syncthreads();  // the previous item of a persistent block is done with the grid
+    __shared__ float s_p[kFlucRasterThreads / 32][16], s_w[kFlucRasterThreads / 32][16];
+    const int w = P.start_ch + row;
+    const int G = P.G, nimp = P.nimp;
+    const int tick_lo = ktile * kTile;
+    const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+    const int nwarps = blockDim.x >> 5;
+    int cnt = 0;
+    const Visit* list = nullptr;
+    if (w >= 0 && w < P.nwires && ktile >= 0 && ktile < ntiles_abs) {
+        const int key = key_base + (P.wire_base + w) * ntiles_abs + ktile;
+        const int off = wire_off[key];
+        cnt = (int)min((long long)wire_cnt[key], max(0ll, vcap - off));
+        list = visits + off;
+    }
+    for (int k = tid; k < G * kTileLd; k += blockDim.x) grid[k] = 0;
+    __syncthreads();
+    const float pbs = P.pbs, tbs = P.tbs, inv_pbs = 1.0f / pbs;
+    const int wlo = w * nimp;
+    for (int e = wid; e < cnt; e += nwarps) {
+        const Visit v = list[e];
+        const int d = v.d;
+        const FlucRec fr = fluc[P.recoff + d];
+        const int rnp = (int)(v.nt_np & 0xffffu), rnt = (int)(v.nt_np >> 16);
+        const int l_lo = max(v.poff, wlo) - wlo, l_hi = min(v.poff + rnp, wlo + nimp) - wlo;
+        if (fr.scale == 0.f || l_hi <= l_lo) continue;  // warp-uniform
+        const PatchRec r = rec[P.recoff + d];
+        const int nb = l_hi - l_lo;
+        const int k0 = wlo + l_lo - v.poff;  // first patch bin on this wire
+        if (lane < nb) {
+            const int k = k0 + lane;
+            const float p = unit_bin(k, pbs, r.pcr, r.sp);
+            float wt;
+            if (r.sp > 0.f) {
+                const float isg = __frcp_rn(r.sp);
+                const float x1 = (float)k * pbs - r.pcr, x2 = (float)(k + 1) * pbs - r.pcr;
+                const float g1 = __expf(-0.5f * (x1 * isg) * (x1 * isg)), g2 = __expf(-0.5f * (x2 * isg) * (x2 * isg));
+                const float c0 = r.sp * inv_pbs * 0.39894228040143268f;
+                wt = p > 0.f ? fmaf(c0 * (g2 - g1), __frcp_rn(p), x2 * inv_pbs) : 0.f;
+            }
+            else wt = (pbs - r.pcr) * inv_pbs;
+            s_p[wid][lane] = p;
+            s_w[wid][lane] = wt;
+        }
+        __syncwarp();
+        const int ev = event_of_depo(evt, d);
+        const int ident = fluc_ident(fp, ev), i_ev = d - evt.dep0[ev];
+        const int cb = v.toff - tick_lo;
+        const int tstart = max(0, -cb), tend = min(rnt, kTile - cb);
+        for (int tc = tstart; tc < tend; tc += 32) {
+            const int t = tc + lane;
+            if (t < tend) {
+                const float tv = unit_bin(t, tbs, r.tcr, r.st);
+                long long* dst = grid + (size_t)l_lo * kTileLd + cb + t;
+                for (int b = 0; b < nb; ++b) {
+                    const int k = k0 + b;
+                    const float relval = __fmul_rn(__fmul_rn(s_p[wid][b], tv), fr.invS);
+                    const int N = cell_draw(fp, ident, i_ev, ip, k * rnt + t, fr.nq, relval);
+                    if (N) {
+                        const float c = (float)N * fr.scale;
+                        const float a = c * s_w[wid][b];
+                        atomicAdd(reinterpret_cast<unsigned long long*>(dst + (size_t)b * kTileLd),
+                                  (unsigned long long)__float2ll_rn(a * kFlucFix));
+                        atomicAdd(reinterpret_cast<unsigned long long*>(dst + (size_t)(b + 1) * kTileLd),
+                                  (unsigned long long)__float2ll_rn((c - a) * kFlucFix));
+                    }
+                }
+            }
+        }
+        __syncwarp();
+    }
+    __syncthreads();
+    const int qc0 = tick_lo - P.col0;
+    for (int k = tid; k < G * kTile; k += blockDim.x) {
+        const int g = k / kTile, c = k - g * kTile;
+        const int qc = qc0 + c;
+        if (qc < 0 || qc >= P.N) continue;
+        float val = 0.f;
+        if (tick_lo + c - P.col0 < P.ncols) val = (float)((double)grid[g * kTileLd + c] * (1.0 / 65536.0));
+        Q[P.qoff + ((size_t)g * P.nin + row) * P.N + qc] = val;
+    }
+}
+
+__global__ void __launch_bounds__(kFlucRasterThreads) k_raster_fluc(const PatchRec* __restrict__ rec,
+                                                                    const FlucRec* __restrict__ fluc, FlucParams fp,
+                                                                    EventTable evt,
+                                                                    const int* __restrict__ wire_cnt,
+                                                                    const int* __restrict__ wire_off,
+                                                                    const Visit* __restrict__ visits, long long vcap,
+                                                                    GridSet gs, float* __restrict__ Q)
+{
+    extern __shared__ long long grid64[];
+    int ip = 0;
+    while (ip + 1 < gs.nplanes && (int)blockIdx.x >= gs.p[ip + 1].row_base) ++ip;
+    const GridPlane& P = gs.p[ip];
+    const int rel = blockIdx.x - P.row_base;
+    const int row = rel / P.ntile;
+    const int ktile = P.ktile0 + (rel - row * P.ntile);
+    raster_tile_fluc(P, ip, row, ktile, 0, gs.ntiles_abs, evt, fp, rec, fluc, wire_cnt, wire_off, visits, vcap, Q,
+                     grid64);
+}
+
+void launch_raster_fluc(const PatchRec* rec, const FlucRec* fluc, const FlucParams& fp, const EventTable& evt,
+                        const int* wire_cnt, const int* wire_off, const Visit* visits, long long vcap,
+                        const GridSet& gs, float* Q, cudaStream_t s)
+{
+    if (gs.nrows_total <= 0) return;
+    size_t smem = 0;
+    for (int i = 0; i < gs.nplanes; ++i) smem = std::max(smem, raster_fluc_smem_bytes(gs.p[i].G));
+    cudaFuncSetAttribute((const void*)k_raster_fluc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    k_raster_fluc<<<gs.nrows_total, kFlucRasterThreads, smem, s>>>(rec, fluc, fp, evt, wire_cnt, wire_off, visits,
+                                                                     vcap, gs, Q);
+}
+
+// Independent Binomial(n, p) draws: out[i] from the stream of key (seed,
+// ident) and counter (i, kRngSampleTag, 0) -- IRandom::binomial in bulk.
+__global__ void k_binomial_samples(unsigned int key0, unsigned int key1, int n, double p, long long count,
+                                   int* __restrict__ out)
+{
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < count; i += (long long)gridDim.x * blockDim.x) {
+        Philox g;
+        g.init(key0, key1, (unsigned)(i & 0xffffffffll), kRngSampleTag, (unsigned)(i >> 32));
+        out[i] = binomial(n, p, g);
+    }
+}
+
+void launch_binomial_samples(unsigned long long seed, int ident, int n, double p, long long count, int* out,
+                             cudaStream_t s)
+{
+    if (count <= 0) return;
+    const unsigned key0 = (unsigned)(seed & 0xffffffffull);
+    const unsigned key1 = (unsigned)(seed >> 32) + 0x9E3779B9u * (unsigned)ident;
+    const long long blocks = std::min<long long>((count + 255) / 256, 148LL * 32);
+    k_binomial_samples<<<(unsigned)blocks, 256, 0, s>>>(key0, key1, n, p, count, out);
 }
 
 // ---------------------------------------------------------------------------
@@ -1234,6 +1517,7 @@ __device__ __forceinline__ int find_entry(const int* __restrict__ pre, int n, in
     return lo;
 }
 
+template <bool FLUC>
 __global__ void __launch_bounds__(kRasterThreads) k_raster_batch(const BatchPlan* __restrict__ plan, BatchStatic bs,
                                                                  PlaneSet ps, const PatchRec* __restrict__ rec,
                                                                  long long recstride,
@@ -1242,7 +1526,8 @@ __global__ void __launch_bounds__(kRasterThreads) k_raster_batch(const BatchPlan
                                                                  const int* __restrict__ wire_off,
                                                                  const Visit* __restrict__ visits, long long vcap,
                                                                  const unsigned long long* __restrict__ key_bound,
-                                                                 float* __restrict__ Q)
+                                                                 float* __restrict__ Q, EventTable evt, FlucParams fp,
+                                                                 const FlucRec* __restrict__ fluc)
 {
     extern __shared__ int smem_i[];
     __shared__ float scale[kTileBlocks], iscale[kTileBlocks];
@@ -1272,19 +1557,30 @@ __global__ void __launch_bounds__(kRasterThreads) k_raster_batch(const BatchPlan
         P.ntile = E.ntile;
         const int rel = item - plan->pre_raster[k];
         const int row = rel / E.ntile;
-        raster_tile(P, row, E.ktile0 + (rel - row * E.ntile), e * bs.nkeys, bs.ntiles, rec, tprof, wire_cnt, wire_off,
-                    visits, vcap, key_bound, Q, smem_i, scale, iscale);
+        if constexpr (FLUC)
+            raster_tile_fluc(P, ip, row, E.ktile0 + (rel - row * E.ntile), e * bs.nkeys, bs.ntiles, evt, fp, rec,
+                             fluc, wire_cnt, wire_off, visits, vcap, Q, reinterpret_cast<long long*>(smem_i));
+        else
+            raster_tile(P, row, E.ktile0 + (rel - row * E.ntile), e * bs.nkeys, bs.ntiles, rec, tprof, wire_cnt,
+                        wire_off, visits, vcap, key_bound, Q, smem_i, scale, iscale);
     }
 }
 
 void launch_raster_batch(const BatchPlan* plan, const BatchStatic& bs, const PlaneSet& ps, const PatchRec* rec,
                          long long recstride, const float* tprof, const int* wire_cnt, const int* wire_off,
                          const Visit* visits, long long vcap, const unsigned long long* key_bound, float* Q,
-                         int nblocks, int maxG, cudaStream_t s)
+                         int nblocks, int maxG, const EventTable& evt, const FlucParams& fp, const FlucRec* fluc,
+                         cudaStream_t s)
 {
-    const size_t smem = raster_smem_bytes(maxG);
-    k_raster_batch<<<nblocks, kRasterThreads, smem, s>>>(plan, bs, ps, rec, recstride, tprof, wire_cnt, wire_off,
-                                                          visits, vcap, key_bound, Q);
+    const size_t smem = std::max(raster_smem_bytes(maxG), raster_fluc_smem_bytes(maxG));
+    if (fp.on_patch)
+        k_raster_batch<true><<<nblocks, kRasterThreads, smem, s>>>(plan, bs, ps, rec, recstride, tprof, wire_cnt,
+                                                                    wire_off, visits, vcap, key_bound, Q, evt, fp,
+                                                                    fluc);
+    else
+        k_raster_batch<false><<<nblocks, kRasterThreads, smem, s>>>(plan, bs, ps, rec, recstride, tprof, wire_cnt,
+                                                                     wire_off, visits, vcap, key_bound, Q, evt, fp,
+                                                                     fluc);
 }
 
 // Time FFT of every charge-grid row of the pass, in place (rows of N reals
@@ -1429,9 +1725,10 @@ void launch_irfft_batch(const BatchPlan* plan, const BatchStatic& bs, const FftD
 // (the launchers themselves only enqueue).
 void batch_kernel_attributes(int maxG, int maxM)
 {
-    const int sr = (int)raster_smem_bytes(maxG);
+    const int sr = (int)std::max(raster_smem_bytes(maxG), raster_fluc_smem_bytes(maxG));
     const int sf = (int)(2 * (size_t)maxM * sizeof(float2));
-    cudaFuncSetAttribute((const void*)k_raster_batch, cudaFuncAttributeMaxDynamicSharedMemorySize, sr);
+    cudaFuncSetAttribute((const void*)k_raster_batch<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, sr);
+    cudaFuncSetAttribute((const void*)k_raster_batch<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, sr);
     cudaFuncSetAttribute((const void*)k_rfft_batch, cudaFuncAttributeMaxDynamicSharedMemorySize, sf);
     cudaFuncSetAttribute((const void*)k_irfft_batch, cudaFuncAttributeMaxDynamicSharedMemorySize, sf);
     cudaFuncSetAttribute((const void*)k_conv_batch<10, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,

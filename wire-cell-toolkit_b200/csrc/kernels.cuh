@@ -190,10 +190,37 @@ struct BatchTune {
     int conv_per_sm;      // persistent wire-convolution blocks per SM
 };
 
+// ---- fluctuation (counter-based binomial draws, rng.cuh) ----
+// Streams: key (key0, key1 + 0x9E3779B9 * ident) with ident the frame ident of
+// the event; counter (depo index within its event, plane or drift tag, cell).
+struct FlucParams {
+    int on_patch;           // DepoTransform "fluctuate": patch cells (GaussianDiffusion.cxx:184-213)
+    int on_drift;           // Drifter "fluctuate": absorbed electrons (Drifter.cxx:177-185)
+    unsigned int key0, key1;
+    int ident0;             // frame ident of the launch's first event, relative to *ident_base
+    const int* ident_base;  // device value added to ident0 (lets a replayed graph draw afresh), or null
+};
+
+// Per (plane, depo) normalisation of a fluctuated patch.
+struct FlucRec {
+    int nq;          // (int)|Q|, the binomial trial count of every cell
+    float scale;     // Q / (sum of the cell draws), 0 when every draw is 0
+    float invS;      // 1 / (sum of unit bin integrals in pitch * in time)
+    int pad;
+};
+
 // ---- launchers (kernels.cu) ----
 void launch_prep_all(const double* depos, const EventTable& et, int nkeys, const DriftDev& dd, int do_drift,
                      const PlaneSet& ps, const TimeDev& tb, double drift_speed, double nsigma, PatchRec* rec,
-                     WindowDev* win, int* wire_cnt, float* tprof, unsigned long long* key_bound, cudaStream_t s);
+                     WindowDev* win, int* wire_cnt, float* tprof, unsigned long long* key_bound,
+                     const FlucParams& fp, double* fq, cudaStream_t s);
+void launch_binomial_samples(unsigned long long seed, int ident, int n, double p, long long count, int* out,
+                             cudaStream_t s);
+void launch_fluc_sums(const PatchRec* rec, const EventTable& et, const PlaneSet& ps, float tbs, const FlucParams& fp,
+                      const double* fq, FlucRec* fluc, cudaStream_t s);
+void launch_raster_fluc(const PatchRec* rec, const FlucRec* fluc, const FlucParams& fp, const EventTable& evt,
+                        const int* wire_cnt, const int* wire_off, const Visit* visits, long long vcap,
+                        const GridSet& gs, float* Q, cudaStream_t s);
 void launch_scan(const int* wire_cnt, int nwires_total, int* wire_off, int* wire_cur, cudaStream_t s);
 void launch_fill(const PatchRec* rec, const EventTable& et, int nkeys, const PlaneSet& ps, int* wire_cur,
                  Visit* visits, long long cap, cudaStream_t s);
@@ -217,7 +244,8 @@ void launch_plan_batch(BatchPlan* plan, const BatchStatic& bs, int nev, const Wi
 void launch_raster_batch(const BatchPlan* plan, const BatchStatic& bs, const PlaneSet& ps, const PatchRec* rec,
                          long long recstride, const float* tprof, const int* wire_cnt, const int* wire_off,
                          const Visit* visits, long long vcap, const unsigned long long* key_bound, float* Q,
-                         int nblocks, int maxG, cudaStream_t s);
+                         int nblocks, int maxG, const EventTable& evt, const FlucParams& fp, const FlucRec* fluc,
+                         cudaStream_t s);
 void launch_rfft_batch(const BatchPlan* plan, const FftDesc* descs, float* Q, int nblocks, int nthreads, int maxM,
                        cudaStream_t s);
 void launch_conv_batch(const BatchPlan* plan, const BatchStatic& bs, int ip, bool pair, const float2* const* spec,
