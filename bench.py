@@ -11,6 +11,12 @@ Output: one JSON line (rank 0).  Multi-GPU: one process per GPU (torchrun),
 every rank simulates its own event (events are independent: weak scaling, no
 data-path collective).
 
+On one GPU the line also carries "patterns": forward + adjoint on 20k track
+depos (full-APA geometry), a batch of 64 uneven full-APA events through one
+captured CUDA graph against per-event calls (and a batch of small events),
+and a full-APA event with fluctuation on -- each timed with CUDA events on
+the launch stream (skip with --no-patterns).
+
 ``--impl reference`` times the CPU restatement of the reference (oracle/,
 FP32, one event per step) on the host cores instead.
 """
@@ -282,12 +288,106 @@ def run_b200(args):
         "gpu_launches": launches,
         "clocks": clk,
     }
+    result["frame_ticks_per_s"] = world * nrows * nticks * args.steps / (max_ms / 1e3)
+    if rank == 0 and world == 1 and not args.no_patterns:
+        result["patterns"] = patterns(wct, synth, torch, stream, local)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         result["cpu_baseline"] = cpu_baseline(cfg, depos, nthreads=1)
     if rank == 0:
         print(json.dumps(result), flush=True)
     if world > 1:
         torch.distributed.destroy_process_group()
+
+
+def _time_ms(torch, stream, fn, reps=5, warm=2):
+    """Median milliseconds of fn() (device time, CUDA events on the launch stream)."""
+    for _ in range(warm):
+        fn()
+    torch.cuda.synchronize()
+    ts = []
+    for _ in range(reps):
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        fn()
+        b.record(stream)
+        b.synchronize()
+        ts.append(a.elapsed_time(b))
+    return float(statistics.median(ts))
+
+
+def patterns(wct, synth, torch, stream, local):
+    """The two patterns beside the plain forward, and the fluctuated forward:
+    forward + adjoint on 20k track depos (full-APA geometry), a batch of 64
+    uneven events through one captured graph against per-event calls (and the
+    same for a batch of small events), and one full-APA event with
+    fluctuation on."""
+    out = {}
+    cfg = synth.apa_config()
+    nrows, nticks = wct.from_config(cfg, device=local).frame_shape()
+
+    # forward + adjoint (gradients of every depo coordinate and of DL, DT, lifetime)
+    d = synth.adjoint_depos(n=20_000)
+    dt = wct.from_config(cfg, device=local)
+    dd = torch.from_numpy(d).cuda()
+    fr = torch.zeros((nrows, nticks), dtype=torch.float32, device="cuda")
+    gf = torch.randn((nrows, nticks), dtype=torch.float32, device="cuda")
+    gd = torch.zeros_like(dd)
+    gg = torch.zeros(3, dtype=torch.float64, device="cuda")
+    sid = stream.cuda_stream
+    fwd = lambda: dt.forward_device(dd.data_ptr(), len(d), fr.data_ptr(), sid)  # noqa: E731
+    adj = lambda: dt.adjoint_device(dd.data_ptr(), len(d), gf.data_ptr(), gd.data_ptr(), gg.data_ptr(), sid)  # noqa
+    t_f = _time_ms(torch, stream, fwd)
+    t_fa = _time_ms(torch, stream, lambda: (fwd(), adj()))
+    out["fwd_adjoint"] = {
+        "workload": "full-APA geometry, 6000 ticks, 20000 track depos; adjoint of every depo coordinate and of "
+                    "DL, DT, lifetime with patches recomputed",
+        "fwd_ms": t_f, "fwd_adj_ms": t_fa, "ratio_fwd_adj_over_fwd": t_fa / t_f,
+        "depos_per_s_fwd_adj": len(d) / (t_fa / 1e3), "target_ratio": "<= 3"}
+    del dd, fr, gf, gd, gg
+
+    def batch_case(events, label):
+        dtb = wct.from_config(cfg, device=local)
+        off = np.zeros(len(events) + 1, dtype=np.int64)
+        off[1:] = np.cumsum([len(e) for e in events])
+        db = torch.from_numpy(np.concatenate(events)).cuda()
+        frames = torch.zeros((len(events), nrows, nticks), dtype=torch.float32, device="cuda")
+
+        def per_event():
+            for k in range(len(events)):
+                if off[k + 1] > off[k]:
+                    dtb.forward_device(db[off[k]:off[k + 1]].data_ptr(), int(off[k + 1] - off[k]),
+                                       frames[k].data_ptr(), sid)
+        t_pe = _time_ms(torch, stream, per_event, reps=3, warm=1)
+        rep = dtb.autotune_batch(db.data_ptr(), off, frames.data_ptr(), stream=sid)
+        t_b = _time_ms(torch, stream, lambda: dtb.forward_batch_device(db.data_ptr(), off, frames.data_ptr(), sid),
+                       reps=3, warm=1)
+        nd = int(off[-1])
+        r = {"workload": label, "events": len(events), "depos": nd, "per_event_ms": t_pe, "batched_ms": t_b,
+             "speedup_batched_over_per_event": t_pe / t_b, "depos_per_s_batched": nd / (t_b / 1e3),
+             "frame_ticks_per_s_batched": len(events) * nrows * nticks / (t_b / 1e3),
+             "autotuned": rep["best"], "target_speedup": ">= 2"}
+        del db, frames
+        torch.cuda.empty_cache()
+        return r
+
+    out["batched"] = batch_case(synth.batch_events(64),
+                                "64 full-APA events, depo counts log-uniform in [10k, 500k], tracks + shower blobs, "
+                                "patches 3x10 .. 40x200 bins; one captured graph, autotuned launch shapes")
+    out["batched_small"] = batch_case(synth.batch_events(64, seed=5, lo=500, hi=5000),
+                                      "64 full-APA events, depo counts log-uniform in [500, 5000] (launch-bound "
+                                      "regime)")
+
+    # fluctuated forward (patch cells and drift), one full-APA event
+    dfl = wct.from_config(dict(cfg, fluctuate=True, seed=1, drifter=dict(cfg["drifter"], fluctuate=True)),
+                          device=local)
+    d = synth.apa_depos(seed=2)
+    dd = torch.from_numpy(d).cuda()
+    fr = torch.zeros((nrows, nticks), dtype=torch.float32, device="cuda")
+    t_fl = _time_ms(torch, stream, lambda: dfl.forward_device(dd.data_ptr(), len(d), fr.data_ptr(), sid))
+    out["fluctuated"] = {"workload": "full-APA event (%d depos), patch-cell and drift fluctuation on" % len(d),
+                         "ms": t_fl, "depos_per_s": len(d) / (t_fl / 1e3)}
+    return out
 
 
 def cpu_baseline(cfg, depos, nthreads=1):
@@ -339,6 +439,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-patterns", action="store_true", help="skip the adjoint / batched / fluctuated lines")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
