@@ -809,7 +809,7 @@ struct BatchState {
     long long vcap{0};
     BatchPlan* h_plans{nullptr};
     size_t h_plans_n{0};
-    BatchTune tune{16, 3, 512, 3, 3};
+    BatchTune tune{16, 6, 256, 4, 4};  // autotuned on a 64-event full-APA batch
     // the instantiated graph and what it was captured for
     cudaGraphExec_t exec{nullptr};
     const void* g_depos{nullptr};
@@ -1092,10 +1092,17 @@ static int forward_batch_device(Core& c, const double* d_depos, const long long*
                                     b.d_fluc.as<FlucRec>(), s);
                 launch_rfft_batch(plans + ch, b.d_descs.as<FftDesc>(), b.d_Q.as<float>(), nb_f, b.tune.fft_threads,
                                   b.maxM, s);
-                for (int ip = 0; ip < np; ++ip)
-                    launch_conv_batch(plans + ch, bs, ip, c.planes[ip]->mirror,
-                                      b.d_spec_tab.as<const float2*>() + (size_t)ip * bs.ncls, b.d_Q.as<float>(),
-                                      b.d_V.as<float2>(), nb_c, s);
+                // one launch per run of planes that share the pad and the group pairing
+                // (the launches use one work counter, so they must not overlap: same stream)
+                for (int ip0 = 0; ip0 < np;) {
+                    int ip1 = ip0 + 1;
+                    while (ip1 < np && c.planes[ip1]->npad == c.planes[ip0]->npad &&
+                           c.planes[ip1]->mirror == c.planes[ip0]->mirror)
+                        ++ip1;
+                    launch_conv_batch(plans + ch, bs, ip0, ip1, c.planes[ip0]->mirror,
+                                      b.d_spec_tab.as<const float2*>(), b.d_Q.as<float>(), b.d_V.as<float2>(), nb_c, s);
+                    ip0 = ip1;
+                }
                 launch_irfft_batch(plans + ch, bs, b.d_descs.as<FftDesc>(), b.d_V.as<float2>(), d_frames + c0 * fstride,
                                    fstride, nb_f, b.tune.fft_threads, b.maxM, s);
             }

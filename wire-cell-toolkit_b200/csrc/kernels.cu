@@ -1495,6 +1495,7 @@ __global__ void __launch_bounds__(256) k_plan_batch(BatchPlan* __restrict__ plan
         plan->nev = nev;
         plan->np = np;
         plan->status = s_status | ((long long)tv > vcap ? kBatchVisitOverflow : 0);
+        for (int k = 0; k < 3 + kMaxPlanes; ++k) plan->next[k] = 0;
     }
 }
 
@@ -1502,6 +1503,18 @@ void launch_plan_batch(BatchPlan* plan, const BatchStatic& bs, int nev, const Wi
                        long long vcap, cudaStream_t s)
 {
     k_plan_batch<<<1, 256, 0, s>>>(plan, bs, nev, win, total_visits, vcap);
+}
+
+// Next work item of a persistent block (all threads get the same value):
+// blocks take items from a shared counter, so a block that drew a heavy item
+// does not hold back the rest.
+__device__ __forceinline__ int next_item(int* counter, int* s_item)
+{
+    if (threadIdx.x == 0 && threadIdx.y == 0) *s_item = atomicAdd(counter, 1);
+    __syncthreads();
+    const int item = *s_item;
+    __syncthreads();  // every thread has read it before the next draw overwrites it
+    return item;
 }
 
 // Index of the (event, plane) entry whose item range holds `item`: the last
@@ -1532,9 +1545,11 @@ __global__ void __launch_bounds__(kRasterThreads) k_raster_batch(const BatchPlan
     extern __shared__ int smem_i[];
     __shared__ float scale[kTileBlocks], iscale[kTileBlocks];
     if (plan->status & kBatchVisitOverflow) return;
+    __shared__ int s_item;
     const int ne = plan->nev * plan->np;
     const int total = plan->pre_raster[ne];
-    for (int item = blockIdx.x; item < total; item += gridDim.x) {
+    int* ctr = const_cast<int*>(&plan->next[0]);
+    for (int item = next_item(ctr, &s_item); item < total; item = next_item(ctr, &s_item)) {
         const int k = find_entry(plan->pre_raster, ne, item);
         const int e = k / plan->np, ip = k - e * plan->np;
         const EvPlane& E = plan->ep[k];
@@ -1590,9 +1605,11 @@ __global__ void k_rfft_batch(const BatchPlan* __restrict__ plan, const FftDesc* 
 {
     extern __shared__ float2 sm[];
     if (plan->status & kBatchVisitOverflow) return;
+    __shared__ int s_item;
     const int ne = plan->nev * plan->np;
     const int total = plan->pre_rows[ne];
-    for (int item = blockIdx.x; item < total; item += gridDim.x) {
+    int* ctr = const_cast<int*>(&plan->next[1]);
+    for (int item = next_item(ctr, &s_item); item < total; item = next_item(ctr, &s_item)) {
         const int k = find_entry(plan->pre_rows, ne, item);
         const EvPlane& E = plan->ep[k];
         const FftDesc d = descs[E.cls];
@@ -1645,28 +1662,37 @@ __device__ __forceinline__ void wire_conv_tile_any(const float2* __restrict__ Qh
 }
 
 // PAD < 0: run-time pad (bs.pl[ip].npad) without shared-memory staging.
+// Items of planes ip0 .. ip1-1 in order; within a plane, events in order.
 template <int PAD, bool PAIR>
 __global__ void __launch_bounds__(32 * kConvRG) k_conv_batch(const BatchPlan* __restrict__ plan, BatchStatic bs,
-                                                             int ip, const float2* const* __restrict__ spec,
+                                                             int ip0, int ip1, const float2* const* __restrict__ spec,
                                                              const float* __restrict__ Q, float2* __restrict__ V)
 {
     extern __shared__ float2 conv_smem[];
+    __shared__ int s_item;
     if (plan->status & kBatchVisitOverflow) return;
     const int nev = plan->nev, np = plan->np;
-    const int* pre = plan->pre_conv[ip];
-    const int total = pre[nev];
-    const int G = bs.pl[ip].G;
-    for (int item = blockIdx.x; item < total; item += gridDim.x) {
-        const int e = find_entry(pre, nev, item);
+    int total = 0;
+    for (int ip = ip0; ip < ip1; ++ip) total += plan->pre_conv[ip][nev];
+    int* ctr = const_cast<int*>(&plan->next[3 + ip0]);
+    for (int item = next_item(ctr, &s_item); item < total; item = next_item(ctr, &s_item)) {
+        int ip = ip0, rel = item;
+        while (rel >= plan->pre_conv[ip][nev]) {
+            rel -= plan->pre_conv[ip][nev];
+            ++ip;
+        }
+        const int* pre = plan->pre_conv[ip];
+        const int e = find_entry(pre, nev, rel);
         const EvPlane& E = plan->ep[e * np + ip];
-        const int rel = item - pre[e];
+        rel -= pre[e];
         const int nfb = (E.M + 31) / 32;
         const int oblk = rel / nfb, fblk = rel - oblk * nfb;
         const float2* Qh = reinterpret_cast<const float2*>(Q + E.qoff);
+        const float2* R = spec[(size_t)ip * bs.ncls + E.cls];
         if constexpr (PAD >= 0)
-            wire_conv_tile<PAD, PAIR>(Qh, spec[E.cls], V + E.voff, G, E.nin, E.nout, E.M, fblk, oblk, conv_smem);
+            wire_conv_tile<PAD, PAIR>(Qh, R, V + E.voff, bs.pl[ip].G, E.nin, E.nout, E.M, fblk, oblk, conv_smem);
         else
-            wire_conv_tile_any(Qh, spec[E.cls], V + E.voff, G, bs.pl[ip].npad, E.nin, E.nout, E.M, fblk, oblk);
+            wire_conv_tile_any(Qh, R, V + E.voff, bs.pl[ip].G, bs.pl[ip].npad, E.nin, E.nout, E.M, fblk, oblk);
     }
 }
 
@@ -1676,19 +1702,19 @@ size_t conv_smem_bytes(int npad, bool pair)
     return sizeof(float2) * 32 * ((size_t)(pair ? 2 : 1) * (kConvRows + 2 * npad) + (2 * npad + 1));
 }
 
-void launch_conv_batch(const BatchPlan* plan, const BatchStatic& bs, int ip, bool pair, const float2* const* spec,
-                       const float* Q, float2* V, int nblocks, cudaStream_t s)
+void launch_conv_batch(const BatchPlan* plan, const BatchStatic& bs, int ip0, int ip1, bool pair,
+                       const float2* const* spec, const float* Q, float2* V, int nblocks, cudaStream_t s)
 {
-    const int npad = bs.pl[ip].npad;
+    const int npad = bs.pl[ip0].npad;
     dim3 block(32, kConvRG);
     const size_t sm = conv_smem_bytes(npad, pair);
-#define WCT_CONVB(P, B) k_conv_batch<P, B><<<nblocks, block, sm, s>>>(plan, bs, ip, spec, Q, V)
+#define WCT_CONVB(P, B) k_conv_batch<P, B><<<nblocks, block, sm, s>>>(plan, bs, ip0, ip1, spec, Q, V)
     if (npad == 10 && pair) WCT_CONVB(10, true);
     else if (npad == 10) WCT_CONVB(10, false);
     else if (npad == 21 && pair) WCT_CONVB(21, true);
     else if (npad == 21) WCT_CONVB(21, false);
 #undef WCT_CONVB
-    else k_conv_batch<-1, false><<<nblocks, block, 0, s>>>(plan, bs, ip, spec, Q, V);
+    else k_conv_batch<-1, false><<<nblocks, block, 0, s>>>(plan, bs, ip0, ip1, spec, Q, V);
 }
 
 // Inverse time FFT of every V row of the pass and the frame write of its event.
@@ -1697,9 +1723,11 @@ __global__ void k_irfft_batch(const BatchPlan* __restrict__ plan, BatchStatic bs
 {
     extern __shared__ float2 sm[];
     if (plan->status & kBatchVisitOverflow) return;
+    __shared__ int s_item;
     const int ne = plan->nev * plan->np;
     const int total = plan->pre_orows[ne];
-    for (int item = blockIdx.x; item < total; item += gridDim.x) {
+    int* ctr = const_cast<int*>(&plan->next[2]);
+    for (int item = next_item(ctr, &s_item); item < total; item = next_item(ctr, &s_item)) {
         const int k = find_entry(plan->pre_orows, ne, item);
         const int e = k / plan->np, ip = k - e * plan->np;
         const EvPlane& E = plan->ep[k];

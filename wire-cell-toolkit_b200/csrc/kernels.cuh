@@ -174,6 +174,7 @@ struct BatchPlan {
     int pre_rows[kMaxBatch * kMaxPlanes + 1];   // time-FFT rows: G * nin
     int pre_orows[kMaxBatch * kMaxPlanes + 1];  // inverse-FFT rows: nout
     int pre_conv[kMaxPlanes][kMaxBatch + 1];    // wire-convolution tiles of plane ip over events
+    int next[3 + kMaxPlanes];                   // work-stealing counters: raster, rfft, irfft, conv from plane ip0
     EvPlane ep[kMaxBatch * kMaxPlanes];
 };
 constexpr int kBatchVisitOverflow = 1;
@@ -248,8 +249,9 @@ void launch_raster_batch(const BatchPlan* plan, const BatchStatic& bs, const Pla
                          cudaStream_t s);
 void launch_rfft_batch(const BatchPlan* plan, const FftDesc* descs, float* Q, int nblocks, int nthreads, int maxM,
                        cudaStream_t s);
-void launch_conv_batch(const BatchPlan* plan, const BatchStatic& bs, int ip, bool pair, const float2* const* spec,
-                       const float* Q, float2* V, int nblocks, cudaStream_t s);
+// Wire convolution of planes [ip0, ip1) (all with the same pad and pairing) in one launch.
+void launch_conv_batch(const BatchPlan* plan, const BatchStatic& bs, int ip0, int ip1, bool pair,
+                       const float2* const* spec, const float* Q, float2* V, int nblocks, cudaStream_t s);
 void launch_irfft_batch(const BatchPlan* plan, const BatchStatic& bs, const FftDesc* descs, const float2* V,
                         float* frames, long long frame_stride, int nblocks, int nthreads, int maxM, cudaStream_t s);
 size_t conv_smem_bytes(int npad, bool pair);
