@@ -180,6 +180,8 @@ struct Core {
     DevBuf d_rec, d_win, d_Q, d_V, d_depos, d_frame, d_wcnt, d_woff, d_wcur, d_wlist, d_tprof, d_kbound;
     DevBuf d_gframe, d_gdep, d_gglob;  // adjoint host entry point
     DevBuf d_fq, d_fluc;               // fluctuation: drifted charges, per (plane, depo) draw sums
+    DevBuf d_pool, d_pool_off, d_pool_used;  // time profiles of long patches
+    DevBuf d_wide;                           // per visit key: holds a long patch
     int config_gen{0};                 // bumped by every change of planes or responses
     std::unique_ptr<struct BatchState> batch;
     WindowDev* h_win{nullptr};
@@ -401,7 +403,7 @@ __global__ void k_win_init(WindowDev* w, int n)
     w[i].tmin = ~0ull;
     w[i].pmax = 0ull;
     w[i].tmax = 0ull;
-    w[i].nadded = w[i].out_time = w[i].out_pitch = w[i].oversize = w[i].bigcharge = 0;
+    w[i].nadded = w[i].out_time = w[i].out_pitch = w[i].oversize = w[i].bigcharge = w[i].wide_ticks = 0;
 }
 
 // Drift, patch records, per-plane windows and charge-grid layout of one event:
@@ -483,6 +485,8 @@ static int prepare_event(Core& c, const double* d_depos, size_t ndepos, cudaStre
     Core::StageTimer t_prep(&c, 0, s);
     CUDA_TRY(cudaMemsetAsync(c.d_wcnt.p, 0, sizeof(int) * (nkeys + 1), s));
     CUDA_TRY(c.d_kbound.ensure(sizeof(unsigned long long) * (size_t)nkeys * kTileBlocks));
+    CUDA_TRY(c.d_wide.ensure((size_t)nkeys));
+    CUDA_TRY(cudaMemsetAsync(c.d_wide.p, 0, (size_t)nkeys, s));
     CUDA_TRY(cudaMemsetAsync(c.d_kbound.p, 0, sizeof(unsigned long long) * (size_t)nkeys * kTileBlocks, s));
     k_win_init<<<1, 64, 0, s>>>(c.d_win.as<WindowDev>(), np);
     EventTable& et = ev.et;
@@ -498,7 +502,8 @@ static int prepare_event(Core& c, const double* d_depos, size_t ndepos, cudaStre
     }
     launch_prep_all(d_depos, et, nkeys, c.drifter, c.have_drifter ? 1 : 0, pset, tb, c.drift_speed, c.nsigma,
                     c.d_rec.as<PatchRec>(), c.d_win.as<WindowDev>(), c.d_wcnt.as<int>(), c.d_tprof.as<float>(),
-                    c.d_kbound.as<unsigned long long>(), ev.fp, ev.fp.on_patch ? c.d_fq.as<double>() : nullptr, s);
+                    c.d_kbound.as<unsigned long long>(), ev.fp, ev.fp.on_patch ? c.d_fq.as<double>() : nullptr,
+                    c.d_wide.as<unsigned char>(), s);
     launch_scan(c.d_wcnt.as<int>(), nkeys, c.d_woff.as<int>(), c.d_wcur.as<int>(), s);
     t_prep.close(4 + (n > 0 ? 1 : 0));
     CUDA_TRY(cudaGetLastError());
@@ -572,9 +577,19 @@ static int forward_device(Core& c, const double* d_depos, size_t ndepos, float* 
     CUDA_TRY(c.d_wlist.ensure(sizeof(Visit) * std::max(total_visits, 1)));
     CUDA_TRY(cudaMemsetAsync(d_frame, 0, sizeof(float) * (size_t)c.nrows() * nticks, s));
 
+    // time profiles of the long patches: exactly the room counted by the prep kernel
+    const long long wide = c.h_win[0].wide_ticks;
+    CUDA_TRY(c.d_pool.ensure(sizeof(float) * (size_t)std::max<long long>(wide, 1)));
+    CUDA_TRY(c.d_pool_off.ensure(sizeof(int) * (size_t)std::max(n, 1)));
+    CUDA_TRY(c.d_pool_used.ensure(sizeof(int)));
+    CUDA_TRY(cudaMemsetAsync(c.d_pool_used.p, 0, sizeof(int), s));
+    const TprofPool pool{c.d_pool.as<float>(), c.d_pool_off.as<int>(), c.d_pool_used.as<int>(), wide};
+
     Core::StageTimer t_r(&c, 1, s);
     launch_fill(c.d_rec.as<PatchRec>(), ev.et, ev.nkeys, pset, c.d_wcur.as<int>(), c.d_wlist.as<Visit>(),
                 (long long)std::max(total_visits, 1), s);
+    if (!ev.fp.on_patch && wide > 0)
+        launch_tprof_pool(c.d_rec.as<PatchRec>(), ev.et, np, (float)ev.tb.bs, pool, nullptr, s);
     if (ev.fp.on_patch) {
         launch_fluc_sums(c.d_rec.as<PatchRec>(), ev.et, pset, (float)ev.tb.bs, ev.fp, c.d_fq.as<double>(),
                          c.d_fluc.as<FlucRec>(), s);
@@ -583,10 +598,12 @@ static int forward_device(Core& c, const double* d_depos, size_t ndepos, float* 
                            c.d_Q.as<float>(), s);
     }
     else
-        launch_raster_wires(c.d_rec.as<PatchRec>(), c.d_tprof.as<float>(), c.d_wcnt.as<int>(), c.d_woff.as<int>(),
-                            c.d_wlist.as<Visit>(), (long long)std::max(total_visits, 1),
+        launch_raster_wires(c.d_rec.as<PatchRec>(), c.d_tprof.as<float>(), pool, c.d_wide.as<unsigned char>(),
+                            c.d_wcnt.as<int>(),
+                            c.d_woff.as<int>(), c.d_wlist.as<Visit>(), (long long)std::max(total_visits, 1),
                             c.d_kbound.as<unsigned long long>(), gset, c.d_Q.as<float>(), s);
-    t_r.close((n > 0 ? 1 : 0) + (rows > 0 ? 1 : 0) + (ev.fp.on_patch && n > 0 ? 1 : 0));
+    t_r.close((n > 0 ? 1 : 0) + (ev.fp.on_patch && n > 0 ? 1 : 0) + (!ev.fp.on_patch && wide > 0 ? 1 : 0) +
+              (rows > 0 ? 1 : 0));
     CUDA_TRY(cudaGetLastError());
 
     for (int ip = 0; ip < np; ++ip) {
@@ -805,6 +822,9 @@ struct BatchState {
     int maxM{0}, maxG{0}, nsm{148};
     DevBuf d_Q, d_V, d_rec, d_tprof, d_win, d_wcnt, d_woff, d_wcur, d_kbound, d_wlist, d_plans;
     DevBuf d_fq, d_fluc, d_ident;  // fluctuation: drifted charges, draw sums, first frame ident of the call
+    DevBuf d_pool, d_pool_off, d_pool_used;  // time profiles of long patches
+    DevBuf d_wide;                           // per key: holds a long patch
+    long long pool_cap{0};
     int* h_ident{nullptr};         // pinned source of d_ident
     long long vcap{0};
     BatchPlan* h_plans{nullptr};
@@ -821,6 +841,7 @@ struct BatchState {
     DriftDev g_drift{};
     int g_fluc[2]{0, 0};
     unsigned long long g_seed{0};
+    long long g_pool_cap{0};
     std::vector<void*> g_bufs;
     void drop_graph()
     {
@@ -1013,7 +1034,7 @@ static int forward_batch_device(Core& c, const double* d_depos, const long long*
     for (int attempt = 0; attempt < 3; ++attempt) {
         std::vector<void*> before = {b.d_Q.p, b.d_V.p, b.d_rec.p, b.d_tprof.p, b.d_win.p, b.d_wcnt.p, b.d_woff.p,
                                      b.d_wcur.p, b.d_kbound.p, b.d_wlist.p, b.d_plans.p, b.d_fq.p, b.d_fluc.p,
-                                     b.d_ident.p};
+                                     b.d_ident.p, b.d_pool.p, b.d_pool_off.p, b.d_pool_used.p, b.d_wide.p};
         CUDA_TRY(b.d_Q.ensure(sizeof(float) * (size_t)bs.qslot_total * K));
         CUDA_TRY(b.d_V.ensure(sizeof(float2) * (size_t)bs.vslot_total * K));
         CUDA_TRY(b.d_rec.ensure(sizeof(PatchRec) * (size_t)np * maxdep));
@@ -1023,9 +1044,14 @@ static int forward_batch_device(Core& c, const double* d_depos, const long long*
         CUDA_TRY(b.d_woff.ensure(sizeof(int) * (size_t)(nkeysK + 1)));
         CUDA_TRY(b.d_wcur.ensure(sizeof(int) * (size_t)(nkeysK + 1 + (nkeysK + 1023) / 1024)));
         CUDA_TRY(b.d_kbound.ensure(sizeof(unsigned long long) * (size_t)nkeysK * kTileBlocks));
+        CUDA_TRY(b.d_wide.ensure((size_t)nkeysK));
         CUDA_TRY(b.d_wlist.ensure(sizeof(Visit) * (size_t)b.vcap));
         CUDA_TRY(b.d_plans.ensure(sizeof(BatchPlan) * (size_t)nch));
         CUDA_TRY(b.d_ident.ensure(sizeof(int)));
+        if (b.pool_cap < 32 * maxdep) b.pool_cap = 32 * maxdep;
+        CUDA_TRY(b.d_pool.ensure(sizeof(float) * (size_t)b.pool_cap));
+        CUDA_TRY(b.d_pool_off.ensure(sizeof(int) * (size_t)maxdep));
+        CUDA_TRY(b.d_pool_used.ensure(sizeof(int)));
         if (c.fluctuate) {
             CUDA_TRY(b.d_fq.ensure(sizeof(double) * (size_t)maxdep));
             CUDA_TRY(b.d_fluc.ensure(sizeof(FlucRec) * (size_t)np * maxdep));
@@ -1033,7 +1059,7 @@ static int forward_batch_device(Core& c, const double* d_depos, const long long*
         if (!b.h_ident) CUDA_TRY(cudaMallocHost(&b.h_ident, sizeof(int)));
         std::vector<void*> after = {b.d_Q.p, b.d_V.p, b.d_rec.p, b.d_tprof.p, b.d_win.p, b.d_wcnt.p, b.d_woff.p,
                                     b.d_wcur.p, b.d_kbound.p, b.d_wlist.p, b.d_plans.p, b.d_fq.p, b.d_fluc.p,
-                                    b.d_ident.p};
+                                    b.d_ident.p, b.d_pool.p, b.d_pool_off.p, b.d_pool_used.p, b.d_wide.p};
         if (b.h_plans_n < (size_t)nch) {
             if (b.h_plans) cudaFreeHost(b.h_plans);
             b.h_plans = nullptr;
@@ -1045,7 +1071,7 @@ static int forward_batch_device(Core& c, const double* d_depos, const long long*
                           std::memcmp(&b.g_tune, &b.tune, sizeof(BatchTune)) == 0 &&
                           std::memcmp(&b.g_drift, &c.drifter, sizeof(DriftDev)) == 0 &&
                           b.g_fluc[0] == (int)c.fluctuate && b.g_fluc[1] == (int)c.drift_fluctuate &&
-                          b.g_seed == c.seed &&
+                          b.g_seed == c.seed && b.g_pool_cap == b.pool_cap &&
                           b.g_offsets.size() == (size_t)nev + 1 &&
                           std::equal(b.g_offsets.begin(), b.g_offsets.end(), offsets);
         if (!same) {
@@ -1070,6 +1096,7 @@ static int forward_batch_device(Core& c, const double* d_depos, const long long*
                 const double* dep = d_depos ? d_depos + 7 * offsets[c0] : nullptr;
                 cudaMemsetAsync(b.d_wcnt.p, 0, sizeof(int) * (size_t)(nk + 1), s);
                 cudaMemsetAsync(b.d_kbound.p, 0, sizeof(unsigned long long) * (size_t)nk * kTileBlocks, s);
+                cudaMemsetAsync(b.d_wide.p, 0, (size_t)nk, s);
                 k_win_init<<<(ne * np + 63) / 64, 64, 0, s>>>(b.d_win.as<WindowDev>(), ne * np);
                 // random streams keyed by the frame ident of each event: base (a device
                 // value written before every launch of the graph) + c0 + event
@@ -1077,17 +1104,23 @@ static int forward_batch_device(Core& c, const double* d_depos, const long long*
                 launch_prep_all(dep, et, bs.nkeys, c.drifter, c.have_drifter ? 1 : 0, pset, tb, c.drift_speed,
                                 c.nsigma, b.d_rec.as<PatchRec>(), b.d_win.as<WindowDev>(), b.d_wcnt.as<int>(),
                                 b.d_tprof.as<float>(), b.d_kbound.as<unsigned long long>(), fp,
-                                fp.on_patch ? b.d_fq.as<double>() : nullptr, s);
+                                fp.on_patch ? b.d_fq.as<double>() : nullptr, b.d_wide.as<unsigned char>(), s);
                 launch_scan(b.d_wcnt.as<int>(), (int)nk, b.d_woff.as<int>(), b.d_wcur.as<int>(), s);
                 launch_plan_batch(plans + ch, bs, ne, b.d_win.as<WindowDev>(), b.d_woff.as<int>() + nk, b.vcap, s);
                 launch_fill(b.d_rec.as<PatchRec>(), et, bs.nkeys, pset, b.d_wcur.as<int>(), b.d_wlist.as<Visit>(),
                             b.vcap, s);
                 cudaMemsetAsync(d_frames + c0 * fstride, 0, sizeof(float) * (size_t)(ne * fstride), s);
+                const TprofPool pool{b.d_pool.as<float>(), b.d_pool_off.as<int>(), b.d_pool_used.as<int>(),
+                                     b.pool_cap};
                 if (fp.on_patch)
                     launch_fluc_sums(b.d_rec.as<PatchRec>(), et, pset, (float)tb.bs, fp, b.d_fq.as<double>(),
                                      b.d_fluc.as<FlucRec>(), s);
+                else {
+                    cudaMemsetAsync(b.d_pool_used.p, 0, sizeof(int), s);
+                    launch_tprof_pool(b.d_rec.as<PatchRec>(), et, np, (float)tb.bs, pool, &plans[ch].status, s);
+                }
                 launch_raster_batch(plans + ch, bs, pset, b.d_rec.as<PatchRec>(), et.dep0[ne], b.d_tprof.as<float>(),
-                                    b.d_wcnt.as<int>(), b.d_woff.as<int>(), b.d_wlist.as<Visit>(), b.vcap,
+                                    pool, b.d_wide.as<unsigned char>(), b.d_wcnt.as<int>(), b.d_woff.as<int>(), b.d_wlist.as<Visit>(), b.vcap,
                                     b.d_kbound.as<unsigned long long>(), b.d_Q.as<float>(), nb_r, b.maxG, et, fp,
                                     b.d_fluc.as<FlucRec>(), s);
                 launch_rfft_batch(plans + ch, b.d_descs.as<FftDesc>(), b.d_Q.as<float>(), nb_f, b.tune.fft_threads,
@@ -1127,6 +1160,7 @@ static int forward_batch_device(Core& c, const double* d_depos, const long long*
             b.g_fluc[0] = (int)c.fluctuate;
             b.g_fluc[1] = (int)c.drift_fluctuate;
             b.g_seed = c.seed;
+            b.g_pool_cap = b.pool_cap;
             b.g_offsets.assign(offsets, offsets + nev + 1);
         }
         *b.h_ident = c.frame_count;
@@ -1145,6 +1179,7 @@ static int forward_batch_device(Core& c, const double* d_depos, const long long*
             st |= b.h_plans[ch].status;
             need = std::max<long long>(need, b.h_plans[ch].total_visits);
         }
+        if (st & kBatchPoolShort) b.pool_cap *= 2;  // frames are right; the next call gets more room
         if (st & kBatchVisitOverflow) {
             b.vcap = need + need / 4 + 4096;  // grow the visit list and run again
             continue;

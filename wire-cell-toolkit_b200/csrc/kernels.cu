@@ -104,6 +104,37 @@ __device__ __forceinline__ float visit_bound(float qn, float sp, float st, float
     return 2.0f * fabsf(qn) * pm * tm * 1.0001f;
 }
 
+// Unit bin integral of bin k of a patch (edges at k*bs - cr and (k+1)*bs - cr
+// from the centre), with explicitly rounded operations and not inlined, so
+// every kernel that calls it gets the same value bit for bit.
+__device__ __noinline__ float unit_bin(int k, float bs, float cr, float sigma)
+{
+    if (!(sigma > 0.f)) return 1.0f;  // point: its single bin holds everything
+    const float inv = __frcp_rn(__fmul_rn(1.41421356237309505f, sigma));
+    const float x1 = __fmul_rn(__fsub_rn(__fmul_rn((float)k, bs), cr), inv);
+    const float x2 = __fmul_rn(__fsub_rn(__fmul_rn((float)(k + 1), bs), cr), inv);
+    return bin_from_edges(copysignf(erfc_nr(fabsf(x1)), x1), copysignf(erfc_nr(fabsf(x2)), x2));
+}
+
+// 1 / (sum of the patch's unit bin integrals in pitch * in time), edge to edge.
+__device__ __noinline__ float patch_inv_norm(const PatchRec& r, float pbs, float tbs)
+{
+    float sp = 1.f, st = 1.f;
+    if (r.sp > 0.f) {
+        const float inv = __frcp_rn(__fmul_rn(1.41421356237309505f, r.sp));
+        const float x1 = __fmul_rn(__fsub_rn(0.f, r.pcr), inv);
+        const float x2 = __fmul_rn(__fsub_rn(__fmul_rn((float)r.np, pbs), r.pcr), inv);
+        sp = bin_from_edges(copysignf(erfc_nr(fabsf(x1)), x1), copysignf(erfc_nr(fabsf(x2)), x2));
+    }
+    if (r.st > 0.f) {
+        const float inv = __frcp_rn(__fmul_rn(1.41421356237309505f, r.st));
+        const float x1 = __fmul_rn(__fsub_rn(0.f, r.tcr), inv);
+        const float x2 = __fmul_rn(__fsub_rn(__fmul_rn((float)r.nt, tbs), r.tcr), inv);
+        st = bin_from_edges(copysignf(erfc_nr(fabsf(x1)), x1), copysignf(erfc_nr(fabsf(x2)), x2));
+    }
+    return __frcp_rn(__fmul_rn(sp, st));
+}
+
 // Event of a prep/fill block: blocks never straddle events.
 __device__ __forceinline__ int event_of_block(const EventTable& et, int b)
 {
@@ -131,7 +162,8 @@ __global__ void __launch_bounds__(256) k_prep_all(const double* __restrict__ dep
                                                   double drift_speed, double nsigma, PatchRec* __restrict__ rec,
                                                   WindowDev* __restrict__ win_all, int* __restrict__ cnt_all,
                                                   float* __restrict__ tprof, unsigned long long* __restrict__ kb_all,
-                                                  FlucParams fp, double* __restrict__ fq)
+                                                  FlucParams fp, double* __restrict__ fq,
+                                                  unsigned char* __restrict__ wide_all)
 {
     const int ev = event_of_block(evt, blockIdx.x);
     const int i = evt.dep0[ev] + (blockIdx.x - evt.blk0[ev]) * blockDim.x + threadIdx.x;
@@ -194,6 +226,7 @@ __global__ void __launch_bounds__(256) k_prep_all(const double* __restrict__ dep
         const int t0 = max(bin_of(tlo, tb.tmin, tb.bs), 0);
         const int t1 = min(bin_of(thi, tb.tmin, tb.bs) + 1, tb.nbins);
         const int nt = t1 - t0;
+        if (nt > kTprof) atomicAdd(&win[0].wide_ticks, nt);
         if (nt > 0 && nt <= kTprof) {
             float* tp = tprof + (size_t)i * kTprof;
             if (st > 0) {
@@ -302,6 +335,11 @@ __global__ void __launch_bounds__(256) k_prep_all(const double* __restrict__ dep
         const int k0 = r.toff / kTile;
         const int kspan = r.np ? (r.toff + r.nt - 1) / kTile - k0 + 1 : 0;
         count_visits(wire_cnt, pl.wire_base, w0, span, k0, kspan, ps.ntiles);
+        if (r.nt > kTprof) {  // keys that hold a long patch: their raster block spreads visits over warps
+            unsigned char* wk = wide_all + (size_t)ev * nkeys;
+            for (int ww = 0; ww < span; ++ww)
+                for (int kk = 0; kk < kspan; ++kk) wk[(pl.wire_base + w0 + ww) * ps.ntiles + k0 + kk] = 1;
+        }
         // fixed-point bounds of the raster: per (wire, tile, 64-tick block), summed
         // as integers in units of 2^-16 (each term rounded up), so the bound --
         // and with it the raster's scale -- does not depend on the order of the adds
@@ -370,12 +408,12 @@ __global__ void __launch_bounds__(256) k_prep_all(const double* __restrict__ dep
 void launch_prep_all(const double* depos, const EventTable& et, int nkeys, const DriftDev& dd, int do_drift,
                      const PlaneSet& ps, const TimeDev& tb, double drift_speed, double nsigma, PatchRec* rec,
                      WindowDev* win, int* wire_cnt, float* tprof, unsigned long long* key_bound,
-                     const FlucParams& fp, double* fq, cudaStream_t s)
+                     const FlucParams& fp, double* fq, unsigned char* wide, cudaStream_t s)
 {
     const int nblocks = et.blk0[et.nev];
     if (nblocks <= 0) return;
     k_prep_all<<<nblocks, 256, 0, s>>>(depos, et, nkeys, dd, do_drift, ps, tb, drift_speed, nsigma, rec, win,
-                                       wire_cnt, tprof, key_bound, fp, fq);
+                                       wire_cnt, tprof, key_bound, fp, fq, wide);
 }
 
 // Exclusive scan of the per-key visit counts: block sums, a scan of the
@@ -455,6 +493,42 @@ void launch_scan(const int* wire_cnt, int nwires_total, int* wire_off, int* wire
     k_scan_sums<<<nb, kScanBlock, 0, s>>>(wire_cnt, n, sums);
     k_scan_top<<<1, kScanBlock, 0, s>>>(sums, nb, wire_off + n);
     k_scan_apply<<<nb, kScanBlock, 0, s>>>(wire_cnt, n, sums, wire_off, wire_cur);
+}
+
+// Time profiles of the long patches, one warp per depo (its first plane with a
+// patch: the time profile does not depend on the plane).
+__global__ void __launch_bounds__(256) k_tprof_pool(const PatchRec* __restrict__ rec, EventTable evt, int nplanes,
+                                                   float tbs, TprofPool pool, int* status)
+{
+    const int lane = threadIdx.x & 31;
+    const int n = evt.dep0[evt.nev];
+    const int i = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    if (i >= n) return;  // whole warps
+    PatchRec r{};
+    for (int ip = 0; ip < nplanes; ++ip) {
+        r = rec[(size_t)ip * n + i];
+        if (r.np) break;
+    }
+    int off = -1;
+    if (r.np && r.nt > kTprof) {
+        if (lane == 0) off = atomicAdd(pool.used, (int)r.nt);
+        off = __shfl_sync(0xffffffffu, off, 0);
+        if ((long long)off + r.nt > pool.cap) {
+            off = -1;
+            if (lane == 0 && status) atomicOr(status, kBatchPoolShort);
+        }
+        else
+            for (int t = lane; t < r.nt; t += 32) pool.val[off + t] = unit_bin(t, tbs, r.tcr, r.st);
+    }
+    if (lane == 0) pool.off[i] = off;
+}
+
+void launch_tprof_pool(const PatchRec* rec, const EventTable& et, int nplanes, float tbs, const TprofPool& pool,
+                       int* status, cudaStream_t s)
+{
+    const int n = et.dep0[et.nev];
+    if (n <= 0) return;
+    k_tprof_pool<<<(n + 7) / 8, 256, 0, s>>>(rec, et, nplanes, tbs, pool, status);
 }
 
 // Per-wire visit lists: wire_list[wire_off[w] ..] holds the depo indices whose
@@ -559,6 +633,7 @@ size_t raster_smem_bytes(int G)
 // smem_i holds the dynamic shared memory of raster_smem_bytes(P.G).
 __device__ __forceinline__ void raster_tile(const GridPlane& P, int row, int ktile, int key_base, int ntiles_abs,
                                             const PatchRec* __restrict__ rec, const float* __restrict__ tprof,
+                                            const TprofPool& pool, const unsigned char* __restrict__ wide_key,
                                             const int* __restrict__ wire_cnt, const int* __restrict__ wire_off,
                                             const Visit* __restrict__ visits, long long vcap,
                                             const unsigned long long* __restrict__ key_bound,
@@ -581,6 +656,7 @@ __device__ __forceinline__ void raster_tile(const GridPlane& P, int row, int kti
         cnt = (int)min((long long)wire_cnt[key], max(0ll, vcap - off));  // no reads past an overflowed list
         list = visits + off;
     }
+    const bool spread = key >= 0 && wide_key[key];
     {
         int4* g4 = reinterpret_cast<int4*>(grid);
         const int n4 = G * kTileLd / 4;
@@ -595,15 +671,22 @@ __device__ __forceinline__ void raster_tile(const GridPlane& P, int row, int kti
     __syncthreads();
     const float pbs = P.pbs, tbs = P.tbs;
     const int wlo = w * nimp;
-    // pass 2: each lane stages the group coefficients of its own visit, then
-    // the warp scatters the 32 staged visits, two at a time (half-warp per
-    // visit, lanes over ticks, loop over the covered groups).
+    // pass 2: each lane stages the group coefficients of one visit, then the
+    // warp scatters its 32 staged visits, two at a time (half-warp per visit,
+    // lanes over ticks, loop over the covered groups; whole warp for a pair
+    // with a visit longer than 16 ticks).
     float* my = stage + (size_t)tid * kStageStride;
     const int wbase = wid * 32;
     const float inv_pbs = 1.0f / pbs;
     const int nchunks = (cnt + kRasterThreads - 1) / kRasterThreads;
     for (int ch = 0; ch < nchunks; ++ch) {
-        const int e = ch * kRasterThreads + tid;
+        // visit of this thread: in blocks with long patches, lanes 2k, 2k+1
+        // hold consecutive visits (a pair) and consecutive pairs go to
+        // different warps (the lists hold one depo kind in runs: long patches
+        // would otherwise pile up on a few warps); elsewhere visits stay in
+        // list order (coalesced reads, alike neighbours along a track)
+        const int e = ch * kRasterThreads +
+                      (spread ? (lane >> 1) * (kRasterThreads / 16) + wid * 2 + (lane & 1) : tid);
         int4 si = make_int4(0, 0, 0, 0);  // d, l_lo, ng, (cb << 11) | nt  (cb = toff - tick_lo, ng = 0: none)
         if (e < cnt) {
             const Visit r = list[e];
@@ -659,7 +742,8 @@ __device__ __forceinline__ void raster_tile(const GridPlane& P, int row, int kti
         }
         stagei[tid] = si;
         __syncwarp();
-        const int nv = min(32, cnt - ch * kRasterThreads - wbase);
+        // lanes 0 .. nv-1 of this warp hold visits (e grows with the lane)
+        const int nv = __popc(__ballot_sync(0xffffffffu, e < cnt));
         const int half = lane >> 4, hl = lane & 15;
         for (int v0 = 0; v0 < nv; v0 += 2) {
             const int v = v0 + half;
@@ -698,6 +782,13 @@ __device__ __forceinline__ void raster_tile(const GridPlane& P, int row, int kti
                     const float* vc = stage + (size_t)(wbase + vv) * kStageStride;
                     const float qn = vc[kStageQ];
                     const int tstart = max(0, -cb), tend = min(wnt, kTile - cb);  // ticks inside the tile
+                    const int poff = wnt > kTprof ? __ldg(pool.off + wi.x) : -1;
+                    float rtcr = 0.f, rst = 0.f;
+                    if (wnt > kTprof && poff < 0) {
+                        const PatchRec r = rec[P.recoff + wi.x];
+                        rtcr = r.tcr;
+                        rst = r.st;
+                    }
                     for (int tc = tstart; tc < tend; tc += 32) {
                         const int it = tc + lane;
                         const bool on = it < tend;
@@ -705,15 +796,8 @@ __device__ __forceinline__ void raster_tile(const GridPlane& P, int row, int kti
                         if (on) {
                             float tv;
                             if (wnt <= kTprof) tv = __ldg(tprof + (size_t)wi.x * kTprof + it);
-                            else {
-                                const PatchRec r = rec[P.recoff + wi.x];
-                                if (r.st > 0.f) {
-                                    const float inv = 1.0f / (1.41421356237309505f * r.st);
-                                    tv = bin_from_edges(edge_erfc((float)it, tbs, r.tcr, inv),
-                                                        edge_erfc((float)(it + 1), tbs, r.tcr, inv));
-                                }
-                                else tv = 1.0f;
-                            }
+                            else if (poff >= 0) tv = __ldg(pool.val + poff + it);
+                            else tv = unit_bin(it, tbs, rtcr, rst);
                             tq = tv * qn * scale[(cb + it) / kScaleBlock];
                         }
                         int* dst = grid + wi.y * kTileLd + cb + it;
@@ -747,7 +831,8 @@ __global__ void __launch_bounds__(kRasterThreads) k_raster_wires(const PatchRec*
                                                                  const int* __restrict__ wire_off,
                                                                  const Visit* __restrict__ visits, long long vcap,
                                                                  const unsigned long long* __restrict__ key_bound,
-                                                                 GridSet gs, float* __restrict__ Q)
+                                                                 GridSet gs, float* __restrict__ Q, TprofPool pool,
+                                                                 const unsigned char* __restrict__ wide_key)
 {
     extern __shared__ int smem_i[];
     __shared__ float scale[kTileBlocks], iscale[kTileBlocks];
@@ -757,20 +842,21 @@ __global__ void __launch_bounds__(kRasterThreads) k_raster_wires(const PatchRec*
     const int rel = blockIdx.x - P.row_base;
     const int row = rel / P.ntile;
     const int ktile = P.ktile0 + (rel - row * P.ntile);  // absolute tick tile
-    raster_tile(P, row, ktile, 0, gs.ntiles_abs, rec, tprof, wire_cnt, wire_off, visits, vcap, key_bound, Q, smem_i,
-                scale, iscale);
+    raster_tile(P, row, ktile, 0, gs.ntiles_abs, rec, tprof, pool, wide_key, wire_cnt, wire_off, visits, vcap,
+                key_bound, Q, smem_i, scale, iscale);
 }
 
-void launch_raster_wires(const PatchRec* rec, const float* tprof, const int* wire_cnt, const int* wire_off,
-                         const Visit* visits, long long vcap, const unsigned long long* key_bound, const GridSet& gs,
-                         float* Q, cudaStream_t s)
+void launch_raster_wires(const PatchRec* rec, const float* tprof, const TprofPool& pool, const unsigned char* wide_key,
+                         const int* wire_cnt,
+                         const int* wire_off, const Visit* visits, long long vcap,
+                         const unsigned long long* key_bound, const GridSet& gs, float* Q, cudaStream_t s)
 {
     if (gs.nrows_total <= 0) return;
     size_t smem = 0;
     for (int i = 0; i < gs.nplanes; ++i) smem = std::max(smem, raster_smem_bytes(gs.p[i].G));
     cudaFuncSetAttribute((const void*)k_raster_wires, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     k_raster_wires<<<gs.nrows_total, kRasterThreads, smem, s>>>(rec, tprof, wire_cnt, wire_off, visits, vcap,
-                                                                    key_bound, gs, Q);
+                                                                    key_bound, gs, Q, pool, wide_key);
 }
 
 // ---------------------------------------------------------------------------
@@ -784,34 +870,6 @@ void launch_raster_wires(const PatchRec* rec, const float* tprof, const int* wir
 // function with explicitly rounded operations, so both passes see the same
 // probabilities bit for bit and therefore the same draws.
 // ---------------------------------------------------------------------------
-__device__ __noinline__ float unit_bin(int k, float bs, float cr, float sigma)
-{
-    if (!(sigma > 0.f)) return 1.0f;  // point: its single bin holds everything
-    const float inv = __frcp_rn(__fmul_rn(1.41421356237309505f, sigma));
-    const float x1 = __fmul_rn(__fsub_rn(__fmul_rn((float)k, bs), cr), inv);
-    const float x2 = __fmul_rn(__fsub_rn(__fmul_rn((float)(k + 1), bs), cr), inv);
-    return bin_from_edges(copysignf(erfc_nr(fabsf(x1)), x1), copysignf(erfc_nr(fabsf(x2)), x2));
-}
-
-// 1 / (sum of the patch's unit bin integrals in pitch * in time), edge to edge.
-__device__ __noinline__ float patch_inv_norm(const PatchRec& r, float pbs, float tbs)
-{
-    float sp = 1.f, st = 1.f;
-    if (r.sp > 0.f) {
-        const float inv = __frcp_rn(__fmul_rn(1.41421356237309505f, r.sp));
-        const float x1 = __fmul_rn(__fsub_rn(0.f, r.pcr), inv);
-        const float x2 = __fmul_rn(__fsub_rn(__fmul_rn((float)r.np, pbs), r.pcr), inv);
-        sp = bin_from_edges(copysignf(erfc_nr(fabsf(x1)), x1), copysignf(erfc_nr(fabsf(x2)), x2));
-    }
-    if (r.st > 0.f) {
-        const float inv = __frcp_rn(__fmul_rn(1.41421356237309505f, r.st));
-        const float x1 = __fmul_rn(__fsub_rn(0.f, r.tcr), inv);
-        const float x2 = __fmul_rn(__fsub_rn(__fmul_rn((float)r.nt, tbs), r.tcr), inv);
-        st = bin_from_edges(copysignf(erfc_nr(fabsf(x1)), x1), copysignf(erfc_nr(fabsf(x2)), x2));
-    }
-    return __frcp_rn(__fmul_rn(sp, st));
-}
-
 __device__ __forceinline__ int event_of_depo(const EventTable& et, int i)
 {
     int lo = 0, hi = et.nev - 1;
@@ -1534,7 +1592,8 @@ template <bool FLUC>
 __global__ void __launch_bounds__(kRasterThreads) k_raster_batch(const BatchPlan* __restrict__ plan, BatchStatic bs,
                                                                  PlaneSet ps, const PatchRec* __restrict__ rec,
                                                                  long long recstride,
-                                                                 const float* __restrict__ tprof,
+                                                                 const float* __restrict__ tprof, TprofPool pool,
+                                                                 const unsigned char* __restrict__ wide_key,
                                                                  const int* __restrict__ wire_cnt,
                                                                  const int* __restrict__ wire_off,
                                                                  const Visit* __restrict__ visits, long long vcap,
@@ -1576,24 +1635,27 @@ __global__ void __launch_bounds__(kRasterThreads) k_raster_batch(const BatchPlan
             raster_tile_fluc(P, ip, row, E.ktile0 + (rel - row * E.ntile), e * bs.nkeys, bs.ntiles, evt, fp, rec,
                              fluc, wire_cnt, wire_off, visits, vcap, Q, reinterpret_cast<long long*>(smem_i));
         else
-            raster_tile(P, row, E.ktile0 + (rel - row * E.ntile), e * bs.nkeys, bs.ntiles, rec, tprof, wire_cnt,
-                        wire_off, visits, vcap, key_bound, Q, smem_i, scale, iscale);
+            raster_tile(P, row, E.ktile0 + (rel - row * E.ntile), e * bs.nkeys, bs.ntiles, rec, tprof, pool,
+                        wide_key, wire_cnt, wire_off, visits, vcap, key_bound, Q, smem_i, scale, iscale);
     }
 }
 
 void launch_raster_batch(const BatchPlan* plan, const BatchStatic& bs, const PlaneSet& ps, const PatchRec* rec,
-                         long long recstride, const float* tprof, const int* wire_cnt, const int* wire_off,
+                         long long recstride, const float* tprof, const TprofPool& pool,
+                         const unsigned char* wide_key, const int* wire_cnt, const int* wire_off,
                          const Visit* visits, long long vcap, const unsigned long long* key_bound, float* Q,
                          int nblocks, int maxG, const EventTable& evt, const FlucParams& fp, const FlucRec* fluc,
                          cudaStream_t s)
 {
     const size_t smem = std::max(raster_smem_bytes(maxG), raster_fluc_smem_bytes(maxG));
     if (fp.on_patch)
-        k_raster_batch<true><<<nblocks, kRasterThreads, smem, s>>>(plan, bs, ps, rec, recstride, tprof, wire_cnt,
+        k_raster_batch<true><<<nblocks, kRasterThreads, smem, s>>>(plan, bs, ps, rec, recstride, tprof, pool, wide_key,
+                                                                    wire_cnt,
                                                                     wire_off, visits, vcap, key_bound, Q, evt, fp,
                                                                     fluc);
     else
-        k_raster_batch<false><<<nblocks, kRasterThreads, smem, s>>>(plan, bs, ps, rec, recstride, tprof, wire_cnt,
+        k_raster_batch<false><<<nblocks, kRasterThreads, smem, s>>>(plan, bs, ps, rec, recstride, tprof, pool,
+                                                                     wide_key, wire_cnt,
                                                                      wire_off, visits, vcap, key_bound, Q, evt, fp,
                                                                      fluc);
 }

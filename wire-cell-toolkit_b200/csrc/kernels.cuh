@@ -73,6 +73,7 @@ struct WindowDev {
     unsigned long long pmin, pmax, tmin, tmax;  // order-preserving double keys
     int nadded, out_time, out_pitch, oversize;
     int bigcharge;  // patches whose raster bound exceeds kMaxVisitBound
+    int wide_ticks; // (plane 0 entry of an event) ticks of the event's patches longer than kTprof
 };
 
 constexpr int kTprof = 16;        // time profiles up to this many ticks are computed once per depo
@@ -181,6 +182,7 @@ constexpr int kBatchVisitOverflow = 1;
 constexpr int kBatchOversize = 2;
 constexpr int kBatchBigCharge = 4;
 constexpr int kBatchNoClass = 8;
+constexpr int kBatchPoolShort = 16;  // not an error: some time profiles were computed in the raster
 
 // Launch shapes of the persistent kernels (chosen by the autotuner).
 struct BatchTune {
@@ -210,11 +212,22 @@ struct FlucRec {
     int pad;
 };
 
+// Time profiles of patches longer than kTprof ticks, computed once per depo
+// (the raster would otherwise recompute them on every wire it visits).
+// off[i] < 0: no room in the pool, the raster computes the values itself
+// with the same function, so the frame does not depend on the pool.
+struct TprofPool {
+    float* val;
+    int* off;     // per depo
+    int* used;    // allocation counter
+    long long cap;
+};
+
 // ---- launchers (kernels.cu) ----
 void launch_prep_all(const double* depos, const EventTable& et, int nkeys, const DriftDev& dd, int do_drift,
                      const PlaneSet& ps, const TimeDev& tb, double drift_speed, double nsigma, PatchRec* rec,
                      WindowDev* win, int* wire_cnt, float* tprof, unsigned long long* key_bound,
-                     const FlucParams& fp, double* fq, cudaStream_t s);
+                     const FlucParams& fp, double* fq, unsigned char* wide, cudaStream_t s);
 void launch_binomial_samples(unsigned long long seed, int ident, int n, double p, long long count, int* out,
                              cudaStream_t s);
 void launch_fluc_sums(const PatchRec* rec, const EventTable& et, const PlaneSet& ps, float tbs, const FlucParams& fp,
@@ -223,12 +236,15 @@ void launch_raster_fluc(const PatchRec* rec, const FlucRec* fluc, const FlucPara
                         const int* wire_cnt, const int* wire_off, const Visit* visits, long long vcap,
                         const GridSet& gs, float* Q, cudaStream_t s);
 void launch_scan(const int* wire_cnt, int nwires_total, int* wire_off, int* wire_cur, cudaStream_t s);
+void launch_tprof_pool(const PatchRec* rec, const EventTable& et, int nplanes, float tbs, const TprofPool& pool,
+                       int* status, cudaStream_t s);
 void launch_fill(const PatchRec* rec, const EventTable& et, int nkeys, const PlaneSet& ps, int* wire_cur,
                  Visit* visits, long long cap, cudaStream_t s);
 size_t raster_smem_bytes(int G);
-void launch_raster_wires(const PatchRec* rec, const float* tprof, const int* wire_cnt, const int* wire_off,
-                         const Visit* visits, long long vcap, const unsigned long long* key_bound, const GridSet& gs,
-                         float* Q, cudaStream_t s);
+void launch_raster_wires(const PatchRec* rec, const float* tprof, const TprofPool& pool, const unsigned char* wide_key,
+                         const int* wire_cnt,
+                         const int* wire_off, const Visit* visits, long long vcap,
+                         const unsigned long long* key_bound, const GridSet& gs, float* Q, cudaStream_t s);
 void launch_rfft_rows(const float* in, long in_ld, int in_len, float2* out, long out_ld, int nrows,
                       const FftDesc& d, cudaStream_t s);
 void launch_wire_conv(const float2* Qh, const float2* Rh, float2* Vh, int ngroups, int npad, int nrows_in,
@@ -243,7 +259,8 @@ void launch_twiddles(float2* tw, float2* twh, int M, cudaStream_t s);
 void launch_plan_batch(BatchPlan* plan, const BatchStatic& bs, int nev, const WindowDev* win, const int* total_visits,
                        long long vcap, cudaStream_t s);
 void launch_raster_batch(const BatchPlan* plan, const BatchStatic& bs, const PlaneSet& ps, const PatchRec* rec,
-                         long long recstride, const float* tprof, const int* wire_cnt, const int* wire_off,
+                         long long recstride, const float* tprof, const TprofPool& pool,
+                         const unsigned char* wide_key, const int* wire_cnt, const int* wire_off,
                          const Visit* visits, long long vcap, const unsigned long long* key_bound, float* Q,
                          int nblocks, int maxG, const EventTable& evt, const FlucParams& fp, const FlucRec* fluc,
                          cudaStream_t s);
