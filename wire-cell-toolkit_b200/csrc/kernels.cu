@@ -962,6 +962,7 @@ __device__ __forceinline__ void raster_tile_fluc(const GridPlane& P, int ip, int
 {
     __syncthreads();  // the previous item of a persistent block is done with the grid
     __shared__ float s_p[kFlucRasterThreads / 32][16], s_w[kFlucRasterThreads / 32][16];
+    __shared__ float s_tv[kFlucRasterThreads / 32][kTile];  // unit time bins of the current visit
     const int w = P.start_ch + row;
     const int G = P.G, nimp = P.nimp;
     const int tick_lo = ktile * kTile;
@@ -1009,24 +1010,24 @@ __device__ __forceinline__ void raster_tile_fluc(const GridPlane& P, int ip, int
         const int ident = fluc_ident(fp, ev), i_ev = d - evt.dep0[ev];
         const int cb = v.toff - tick_lo;
         const int tstart = max(0, -cb), tend = min(rnt, kTile - cb);
-        for (int tc = tstart; tc < tend; tc += 32) {
-            const int t = tc + lane;
-            if (t < tend) {
-                const float tv = unit_bin(t, tbs, r.tcr, r.st);
-                long long* dst = grid + (size_t)l_lo * kTileLd + cb + t;
-                for (int b = 0; b < nb; ++b) {
-                    const int k = k0 + b;
-                    const float relval = __fmul_rn(__fmul_rn(s_p[wid][b], tv), fr.invS);
-                    const int N = cell_draw(fp, ident, i_ev, ip, k * rnt + t, fr.nq, relval);
-                    if (N) {
-                        const float c = (float)N * fr.scale;
-                        const float a = c * s_w[wid][b];
-                        atomicAdd(reinterpret_cast<unsigned long long*>(dst + (size_t)b * kTileLd),
-                                  (unsigned long long)__float2ll_rn(a * kFlucFix));
-                        atomicAdd(reinterpret_cast<unsigned long long*>(dst + (size_t)(b + 1) * kTileLd),
-                                  (unsigned long long)__float2ll_rn((c - a) * kFlucFix));
-                    }
-                }
+        const int ntt = tend - tstart;
+        if (ntt <= 0) continue;  // warp-uniform
+        for (int t = lane; t < ntt; t += 32) s_tv[wid][t] = unit_bin(tstart + t, tbs, r.tcr, r.st);
+        __syncwarp();
+        // cells (bin b, tick t) of the visit in this tile, spread over the lanes
+        for (int cell = lane; cell < nb * ntt; cell += 32) {
+            const int b = cell / ntt, tt = cell - b * ntt;
+            const int t = tstart + tt;
+            const int k = k0 + b;
+            const float relval = __fmul_rn(__fmul_rn(s_p[wid][b], s_tv[wid][tt]), fr.invS);
+            const int N = cell_draw(fp, ident, i_ev, ip, k * rnt + t, fr.nq, relval);
+            if (N) {
+                const float c = (float)N * fr.scale;
+                const float a = c * s_w[wid][b];
+                long long* dst = grid + (size_t)(l_lo + b) * kTileLd + cb + t;
+                atomicAdd(reinterpret_cast<unsigned long long*>(dst), (unsigned long long)__float2ll_rn(a * kFlucFix));
+                atomicAdd(reinterpret_cast<unsigned long long*>(dst + kTileLd),
+                          (unsigned long long)__float2ll_rn((c - a) * kFlucFix));
             }
         }
         __syncwarp();

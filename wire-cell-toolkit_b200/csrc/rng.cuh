@@ -11,9 +11,11 @@
 //     f(x+1) = f(x) * (n - x) / (x + 1) * p / (1 - p);
 //   * otherwise: transformed rejection with squeeze, algorithm BTRS of
 //     W. Hormann, "The generation of binomial random variates", J. Statist.
-//     Comput. Simul. 46 (1993) 101-110, with its acceptance test written with
-//     log-gamma: accept k when log(v * alpha / (a / us^2 + b)) <=
-//     log f(k) - log f(m), m the mode.
+//     Comput. Simul. 46 (1993) 101-110: accept k when
+//     log(v * alpha / (a / us^2 + b)) <= log f(k) - log f(m), m the mode,
+//     with log x! = (x + 1/2) log(x + 1) - (x + 1) + log(2 pi) / 2 + fc(x),
+//     fc the Stirling correction (exact values below 10, the series
+//     1/12 (x+1)^-1 - 1/360 (x+1)^-3 + 1/1260 (x+1)^-5 above).
 // Both are exact samplers (up to floating-point rounding).
 #pragma once
 
@@ -75,6 +77,26 @@ struct Philox {
     }
 };
 
+// Stirling correction fc(x) = log x! - [(x + 1/2) log(x + 1) - (x + 1) + log(2 pi)/2].
+__device__ __forceinline__ double stirling_fc(int x)
+{
+    if (x < 10) {
+        const double t[10] = {0.08106146679532733,  0.041340695955409457, 0.027677925684997717,
+                              0.020790672103765839, 0.016644691189821259, 0.013876128823072875,
+                              0.011896709945893313, 0.010411265261973668, 0.0092554621827094508,
+                              0.0083305634333594725};
+        return t[x];
+    }
+    const double r = 1.0 / ((double)x + 1.0), r2 = r * r;
+    return r * (1.0 / 12.0 - r2 * (1.0 / 360.0 - r2 * (1.0 / 1260.0)));
+}
+
+// log x! up to the terms that cancel in the ratios below: (x + 1/2) log(x + 1) + fc(x).
+__device__ __forceinline__ double logfact_part(int x)
+{
+    return ((double)x + 0.5) * log((double)x + 1.0) + stirling_fc(x);
+}
+
 // Binomial(n, p) for 0 <= p <= 1/2.
 __device__ __forceinline__ int binomial_low(int n, double p, Philox& g)
 {
@@ -108,7 +130,7 @@ __device__ __forceinline__ int binomial_low(int n, double p, Philox& g)
     const double alpha = (2.83 + 5.1 / b) * spq;
     const double lpq = log(p / q);
     const int m = (int)floor((double)(n + 1) * p);
-    const double lfm = lgamma((double)m + 1.0) + lgamma((double)(n - m) + 1.0);
+    const double lfm = logfact_part(m) + logfact_part(n - m);
     for (int attempt = 0; attempt < 1000; ++attempt) {
         const double u = g.uniform() - 0.5;
         const double v = g.uniform();
@@ -117,7 +139,8 @@ __device__ __forceinline__ int binomial_low(int n, double p, Philox& g)
         if (k < 0 || k > n) continue;
         if (us >= 0.07 && v <= vr) return k;  // squeeze
         const double lv = log(v * alpha / (a / (us * us) + b));
-        const double lratio = lfm - lgamma((double)k + 1.0) - lgamma((double)(n - k) + 1.0) + (double)(k - m) * lpq;
+        // log f(k) - log f(m); the -(x+1) and log(2 pi)/2 terms of the four factorials cancel
+        const double lratio = lfm - logfact_part(k) - logfact_part(n - k) + (double)(k - m) * lpq;
         if (lv <= lratio) return k;
     }
     return m;  // not reached in practice (acceptance probability per try is above 0.5)
