@@ -14,8 +14,10 @@ data-path collective).
 On one GPU the line also carries "patterns": forward + adjoint on 20k track
 depos (full-APA geometry), a batch of 64 uneven full-APA events through one
 captured CUDA graph against per-event calls (and a batch of small events),
-and a full-APA event with fluctuation on -- each timed with CUDA events on
-the launch stream (skip with --no-patterns).
+a full-APA event with fluctuation on, and the large batched calibration (16
+events x 4M depos, fluctuated targets, DL/DT/lifetime fit steps) -- each timed
+with CUDA events on the launch stream (skip with --no-patterns,
+--no-calibration).
 
 ``--impl reference`` times the CPU restatement of the reference (oracle/,
 FP32, one event per step) on the host cores instead.
@@ -290,7 +292,15 @@ def run_b200(args):
     }
     result["frame_ticks_per_s"] = world * nrows * nticks * args.steps / (max_ms / 1e3)
     if rank == 0 and world == 1 and not args.no_patterns:
-        result["patterns"] = patterns(wct, synth, torch, stream, local)
+        try:
+            result["patterns"] = patterns(wct, synth, torch, stream, local)
+        except Exception as e:  # the headline line must print whatever happens here
+            result["patterns"] = {"error": repr(e)[:300]}
+        if not args.no_calibration:
+            try:
+                result["patterns"]["calibration"] = calibration(wct, synth, torch, local)
+            except Exception as e:
+                result["patterns"]["calibration"] = {"error": repr(e)[:300]}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         result["cpu_baseline"] = cpu_baseline(cfg, depos, nthreads=1)
     if rank == 0:
@@ -390,6 +400,64 @@ def patterns(wct, synth, torch, stream, local):
     return out
 
 
+def calibration(wct, synth, torch, local, nevents=16, ndepos=4_000_000, steps=20):
+    """Large batched calibration: nevents events of ndepos depos (cosmic muons +
+    exponential-spectrum showers, mean 1 GeV), targets drawn with fluctuation
+    on (patch cells and drift) at DL x 0.9, DT x 1.1, lifetime 8 ms, then
+    gradient-descent steps of DL, DT, lifetime (batched mean forward + adjoint
+    of every event per step), timed with CUDA events."""
+    cal = importlib.import_module("wire-cell-toolkit_b200.calibrate")
+    cfg = synth.apa_config()
+    dr = cfg["drifter"]
+    truth = (dr["DL"] * 0.9, dr["DT"] * 1.1, 8.0e6)
+    t0 = time.perf_counter()
+    events = synth.calibration_events(nevents, ndepos)
+    t_gen = time.perf_counter() - t0
+    off = np.zeros(nevents + 1, dtype=np.int64)
+    off[1:] = np.cumsum([len(e) for e in events])
+    d = torch.from_numpy(np.concatenate(events)).to("cuda")
+    del events
+    gen = wct.from_config(dict(cfg, fluctuate=True, seed=5, drifter=dict(dr, fluctuate=True)), device=local)
+    gen.set_drift_params(*truth)
+    nrows, nticks = gen.frame_shape()
+    targets = torch.zeros((nevents, nrows, nticks), dtype=torch.float32, device="cuda")
+    s = torch.cuda.Stream()
+    a = torch.cuda.Event(enable_timing=True)
+    b = torch.cuda.Event(enable_timing=True)
+    a.record(s)
+    gen.forward_batch_device(d.data_ptr(), off, targets.data_ptr(), stream=s.cuda_stream)
+    b.record(s)
+    b.synchronize()
+    t_target = a.elapsed_time(b)
+    del gen
+    model = wct.from_config(cfg, device=local)
+    marks = []
+
+    def cb(it, p, loss, g):
+        ev = torch.cuda.Event(enable_timing=True)
+        ev.record(s)
+        marks.append(ev)
+
+    hist, final = cal.fit_drift_params(model, d, off, targets, steps=steps, lr=0.05, stream=s, callback=cb)
+    torch.cuda.synchronize()
+    per_step = [marks[k].elapsed_time(marks[k + 1]) for k in range(len(marks) - 1)]
+    ms_step = float(statistics.median(per_step)) if per_step else None
+    ndep = int(off[-1])
+    out = {
+        "workload": "%d full-APA events x %d depos (cosmic muons + showers, exponential spectrum of mean 1 GeV); "
+                    "targets with patch and drift fluctuation at DL x 0.9, DT x 1.1, lifetime 8 ms; fit of "
+                    "DL, DT, lifetime by batched forward + per-event adjoint, Adam in log space" % (nevents, ndepos),
+        "depos": ndep, "generation_s": t_gen, "fluctuated_target_ms": t_target,
+        "fluctuated_depos_per_s": ndep / (t_target / 1e3),
+        "ms_per_fit_step": ms_step,
+        "fwd_adj_depos_per_s": ndep / (ms_step / 1e3) if ms_step else None,
+        "loss_first": hist[0][2], "loss_last": hist[-1][2],
+        "params_start": list(hist[0][1]), "params_final": list(final), "params_truth": list(truth)}
+    del d, targets
+    torch.cuda.empty_cache()
+    return out
+
+
 def cpu_baseline(cfg, depos, nthreads=1):
     """The oracle (FP32 restatement of the reference) on one full event."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
@@ -440,6 +508,7 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-patterns", action="store_true", help="skip the adjoint / batched / fluctuated lines")
+    ap.add_argument("--no-calibration", action="store_true", help="skip the large batched calibration")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

@@ -403,7 +403,8 @@ __global__ void k_win_init(WindowDev* w, int n)
     w[i].tmin = ~0ull;
     w[i].pmax = 0ull;
     w[i].tmax = 0ull;
-    w[i].nadded = w[i].out_time = w[i].out_pitch = w[i].oversize = w[i].bigcharge = w[i].wide_ticks = 0;
+    w[i].nadded = w[i].out_time = w[i].out_pitch = w[i].oversize = w[i].bigcharge = 0;
+    w[i].wide_ticks = w[i].nvisits = 0;
 }
 
 // Drift, patch records, per-plane windows and charge-grid layout of one event:
@@ -514,6 +515,8 @@ static int prepare_event(Core& c, const double* d_depos, size_t ndepos, cudaStre
         if (c.h_win[ip].oversize) return fail(WCT_ERR_SIZE, "a diffusion patch exceeds 1024 ticks or 1024 impact bins");
     for (int ip = 0; ip < np; ++ip)
         if (c.h_win[ip].bigcharge) return fail(WCT_ERR_SIZE, "a depo charge exceeds 5e11 electrons");
+    if (c.h_win[0].nvisits >= 0x7fffffffull)
+        return fail(WCT_ERR_SIZE, "an event holds 2^31 or more patch visits (wire x 256-tick tile); split it");
     ev.total_visits = *h_total;
 
     std::vector<PlaneWindow>& pw = ev.pw;
@@ -578,12 +581,14 @@ static int forward_device(Core& c, const double* d_depos, size_t ndepos, float* 
     CUDA_TRY(cudaMemsetAsync(d_frame, 0, sizeof(float) * (size_t)c.nrows() * nticks, s));
 
     // time profiles of the long patches: exactly the room counted by the prep kernel
-    const long long wide = c.h_win[0].wide_ticks;
+    // (int offsets: beyond 2^31 - 2 ticks the rest is computed in the raster)
+    const long long wide = (long long)std::min<unsigned long long>(c.h_win[0].wide_ticks, 0x7ffffffeull);
     CUDA_TRY(c.d_pool.ensure(sizeof(float) * (size_t)std::max<long long>(wide, 1)));
     CUDA_TRY(c.d_pool_off.ensure(sizeof(int) * (size_t)std::max(n, 1)));
-    CUDA_TRY(c.d_pool_used.ensure(sizeof(int)));
-    CUDA_TRY(cudaMemsetAsync(c.d_pool_used.p, 0, sizeof(int), s));
-    const TprofPool pool{c.d_pool.as<float>(), c.d_pool_off.as<int>(), c.d_pool_used.as<int>(), wide};
+    CUDA_TRY(c.d_pool_used.ensure(sizeof(unsigned long long)));
+    CUDA_TRY(cudaMemsetAsync(c.d_pool_used.p, 0, sizeof(unsigned long long), s));
+    const TprofPool pool{c.d_pool.as<float>(), c.d_pool_off.as<int>(), c.d_pool_used.as<unsigned long long>(),
+                         wide};
 
     Core::StageTimer t_r(&c, 1, s);
     launch_fill(c.d_rec.as<PatchRec>(), ev.et, ev.nkeys, pset, c.d_wcur.as<int>(), c.d_wlist.as<Visit>(),
@@ -959,6 +964,8 @@ static int batch_setup(Core& c)
 }
 
 // Device bytes of one event slot (charge grids, V rows, per-event keys).
+constexpr long long kMaxPassDepos = 16LL << 20;  // depos per pass of the batched path
+
 static size_t batch_slot_bytes(const BatchState& b)
 {
     const BatchStatic& bs = b.bs;
@@ -1001,14 +1008,23 @@ static int forward_batch_device(Core& c, const double* d_depos, const long long*
     BatchState& b = *c.batch;
     const BatchStatic& bs = b.bs;
     const int np = bs.np;
-    const int K = batch_slots(c, nev);
-    const int nch = (nev + K - 1) / K;
+    int K = batch_slots(c, nev);
+    int nch = 1;
     long long maxdep = 1;
-    for (int c0 = 0; c0 < nev; c0 += K) {
-        const int c1 = std::min(nev, c0 + K);
-        maxdep = std::max(maxdep, offsets[c1] - offsets[c0]);
-    }
-    if (maxdep > 0x7fffff00LL) return fail(WCT_ERR_SIZE, "forward batch: too many depos in one pass");
+    // events per pass: K, fewer while a pass would hold more than kMaxPassDepos
+    // depos (bounded work arrays; their visit lists keep int offsets)
+    auto layout = [&]() {
+        for (;;) {
+            nch = (nev + K - 1) / K;
+            maxdep = 1;
+            for (int c0 = 0; c0 < nev; c0 += K)
+                maxdep = std::max(maxdep, offsets[std::min(nev, c0 + K)] - offsets[c0]);
+            if (K == 1 || maxdep <= kMaxPassDepos) return;
+            K = std::max(1, K / 2);
+        }
+    };
+    layout();
+    if (maxdep > 0x7fffff00LL) return fail(WCT_ERR_SIZE, "forward batch: too many depos in one event");
     const long long fstride = (long long)c.nrows() * bs.nticks;
     const long long est = 6LL * np * maxdep + 4096;
     if (b.vcap < est) b.vcap = est;
@@ -1029,9 +1045,8 @@ static int forward_batch_device(Core& c, const double* d_depos, const long long*
     tb.tmin = c.start_time;
     tb.tmax = c.start_time + c.readout_time;
     tb.bs = (tb.tmax - tb.tmin) / tb.nbins;
-    const long long nkeysK = (long long)K * bs.nkeys;
-
-    for (int attempt = 0; attempt < 3; ++attempt) {
+    for (int attempt = 0; attempt < 8; ++attempt) {
+        const long long nkeysK = (long long)K * bs.nkeys;
         std::vector<void*> before = {b.d_Q.p, b.d_V.p, b.d_rec.p, b.d_tprof.p, b.d_win.p, b.d_wcnt.p, b.d_woff.p,
                                      b.d_wcur.p, b.d_kbound.p, b.d_wlist.p, b.d_plans.p, b.d_fq.p, b.d_fluc.p,
                                      b.d_ident.p, b.d_pool.p, b.d_pool_off.p, b.d_pool_used.p, b.d_wide.p};
@@ -1049,9 +1064,10 @@ static int forward_batch_device(Core& c, const double* d_depos, const long long*
         CUDA_TRY(b.d_plans.ensure(sizeof(BatchPlan) * (size_t)nch));
         CUDA_TRY(b.d_ident.ensure(sizeof(int)));
         if (b.pool_cap < 32 * maxdep) b.pool_cap = 32 * maxdep;
+        b.pool_cap = std::min<long long>(b.pool_cap, 0x7ffffffeLL);  // int offsets
         CUDA_TRY(b.d_pool.ensure(sizeof(float) * (size_t)b.pool_cap));
         CUDA_TRY(b.d_pool_off.ensure(sizeof(int) * (size_t)maxdep));
-        CUDA_TRY(b.d_pool_used.ensure(sizeof(int)));
+        CUDA_TRY(b.d_pool_used.ensure(sizeof(unsigned long long)));
         if (c.fluctuate) {
             CUDA_TRY(b.d_fq.ensure(sizeof(double) * (size_t)maxdep));
             CUDA_TRY(b.d_fluc.ensure(sizeof(FlucRec) * (size_t)np * maxdep));
@@ -1106,17 +1122,17 @@ static int forward_batch_device(Core& c, const double* d_depos, const long long*
                                 b.d_tprof.as<float>(), b.d_kbound.as<unsigned long long>(), fp,
                                 fp.on_patch ? b.d_fq.as<double>() : nullptr, b.d_wide.as<unsigned char>(), s);
                 launch_scan(b.d_wcnt.as<int>(), (int)nk, b.d_woff.as<int>(), b.d_wcur.as<int>(), s);
-                launch_plan_batch(plans + ch, bs, ne, b.d_win.as<WindowDev>(), b.d_woff.as<int>() + nk, b.vcap, s);
+                launch_plan_batch(plans + ch, bs, ne, b.d_win.as<WindowDev>(), b.vcap, s);
                 launch_fill(b.d_rec.as<PatchRec>(), et, bs.nkeys, pset, b.d_wcur.as<int>(), b.d_wlist.as<Visit>(),
                             b.vcap, s);
                 cudaMemsetAsync(d_frames + c0 * fstride, 0, sizeof(float) * (size_t)(ne * fstride), s);
-                const TprofPool pool{b.d_pool.as<float>(), b.d_pool_off.as<int>(), b.d_pool_used.as<int>(),
-                                     b.pool_cap};
+                const TprofPool pool{b.d_pool.as<float>(), b.d_pool_off.as<int>(),
+                                     b.d_pool_used.as<unsigned long long>(), b.pool_cap};
                 if (fp.on_patch)
                     launch_fluc_sums(b.d_rec.as<PatchRec>(), et, pset, (float)tb.bs, fp, b.d_fq.as<double>(),
                                      b.d_fluc.as<FlucRec>(), s);
                 else {
-                    cudaMemsetAsync(b.d_pool_used.p, 0, sizeof(int), s);
+                    cudaMemsetAsync(b.d_pool_used.p, 0, sizeof(unsigned long long), s);
                     launch_tprof_pool(b.d_rec.as<PatchRec>(), et, np, (float)tb.bs, pool, &plans[ch].status, s);
                 }
                 launch_raster_batch(plans + ch, bs, pset, b.d_rec.as<PatchRec>(), et.dep0[ne], b.d_tprof.as<float>(),
@@ -1180,6 +1196,13 @@ static int forward_batch_device(Core& c, const double* d_depos, const long long*
             need = std::max<long long>(need, b.h_plans[ch].total_visits);
         }
         if (st & kBatchPoolShort) b.pool_cap *= 2;  // frames are right; the next call gets more room
+        if (st & kBatchTooBig) {  // 2^31 visits in a pass: fewer events per pass
+            if (K == 1) return fail(WCT_ERR_SIZE, "an event holds 2^31 or more patch visits; split it");
+            K = std::max(1, K / 2);
+            layout();
+            b.drop_graph();
+            continue;
+        }
         if (st & kBatchVisitOverflow) {
             b.vcap = need + need / 4 + 4096;  // grow the visit list and run again
             continue;

@@ -226,7 +226,7 @@ __global__ void __launch_bounds__(256) k_prep_all(const double* __restrict__ dep
         const int t0 = max(bin_of(tlo, tb.tmin, tb.bs), 0);
         const int t1 = min(bin_of(thi, tb.tmin, tb.bs) + 1, tb.nbins);
         const int nt = t1 - t0;
-        if (nt > kTprof) atomicAdd(&win[0].wide_ticks, nt);
+        if (nt > kTprof) atomicAdd(&win[0].wide_ticks, (unsigned long long)nt);
         if (nt > 0 && nt <= kTprof) {
             float* tp = tprof + (size_t)i * kTprof;
             if (st > 0) {
@@ -252,6 +252,7 @@ __global__ void __launch_bounds__(256) k_prep_all(const double* __restrict__ dep
     auto umin = [](unsigned long long a, unsigned long long b) { return a < b ? a : b; };
     auto umax = [](unsigned long long a, unsigned long long b) { return a > b ? a : b; };
     auto iadd = [](int a, int b) { return a + b; };
+    unsigned long long myvis = 0;
     for (int ip = 0; ip < ps.nplanes; ++ip) {
         const PlaneDev& pl = ps.p[ip];
         unsigned long long kpmin = ~0ull, kpmax = 0ull, ktmin = ~0ull, ktmax = 0ull;
@@ -335,6 +336,7 @@ __global__ void __launch_bounds__(256) k_prep_all(const double* __restrict__ dep
         const int k0 = r.toff / kTile;
         const int kspan = r.np ? (r.toff + r.nt - 1) / kTile - k0 + 1 : 0;
         count_visits(wire_cnt, pl.wire_base, w0, span, k0, kspan, ps.ntiles);
+        myvis += (unsigned long long)span * (unsigned long long)kspan;
         if (r.nt > kTprof) {  // keys that hold a long patch: their raster block spreads visits over warps
             unsigned char* wk = wide_all + (size_t)ev * nkeys;
             for (int ww = 0; ww < span; ++ww)
@@ -403,6 +405,10 @@ __global__ void __launch_bounds__(256) k_prep_all(const double* __restrict__ dep
         }
         __syncthreads();
     }
+    // 64-bit visit total of the event (the visit lists use int offsets)
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) myvis += __shfl_xor_sync(0xffffffffu, myvis, o);
+    if (l == 0 && myvis) atomicAdd(&win[0].nvisits, myvis);
 }
 
 void launch_prep_all(const double* depos, const EventTable& et, int nkeys, const DriftDev& dd, int do_drift,
@@ -511,9 +517,11 @@ __global__ void __launch_bounds__(256) k_tprof_pool(const PatchRec* __restrict__
     }
     int off = -1;
     if (r.np && r.nt > kTprof) {
-        if (lane == 0) off = atomicAdd(pool.used, (int)r.nt);
-        off = __shfl_sync(0xffffffffu, off, 0);
-        if ((long long)off + r.nt > pool.cap) {
+        long long off64 = 0;
+        if (lane == 0) off64 = (long long)atomicAdd(pool.used, (unsigned long long)r.nt);
+        off64 = __shfl_sync(0xffffffffu, off64, 0);
+        off = off64 + r.nt > pool.cap ? -1 : (int)off64;  // 64-bit counter: no wrap
+        if (off < 0) {
             off = -1;
             if (lane == 0 && status) atomicOr(status, kBatchPoolShort);
         }
@@ -582,7 +590,8 @@ __global__ void __launch_bounds__(256) k_fill(const PatchRec* __restrict__ rec, 
                 v.qn = r.qn;
                 v.d = i;
                 v.pad = 0;
-                if (base + rank < cap) list[base + rank] = v;  // beyond cap: the caller reports an overflow
+                const long long at = (long long)base + rank;
+                if (at >= 0 && at < cap) list[at] = v;  // outside: the caller reports an overflow
             }
         }
     }
@@ -653,8 +662,8 @@ __device__ __forceinline__ void raster_tile(const GridPlane& P, int row, int kti
     if (w >= 0 && w < P.nwires && ktile >= 0 && ktile < ntiles_abs) {
         key = key_base + (P.wire_base + w) * ntiles_abs + ktile;
         const int off = wire_off[key];
-        cnt = (int)min((long long)wire_cnt[key], max(0ll, vcap - off));  // no reads past an overflowed list
-        list = visits + off;
+        cnt = off < 0 ? 0 : (int)min((long long)wire_cnt[key], max(0ll, vcap - off));  // no reads past the list
+        list = visits + max(off, 0);
     }
     const bool spread = key >= 0 && wide_key[key];
     {
@@ -973,8 +982,8 @@ __device__ __forceinline__ void raster_tile_fluc(const GridPlane& P, int ip, int
     if (w >= 0 && w < P.nwires && ktile >= 0 && ktile < ntiles_abs) {
         const int key = key_base + (P.wire_base + w) * ntiles_abs + ktile;
         const int off = wire_off[key];
-        cnt = (int)min((long long)wire_cnt[key], max(0ll, vcap - off));
-        list = visits + off;
+        cnt = off < 0 ? 0 : (int)min((long long)wire_cnt[key], max(0ll, vcap - off));
+        list = visits + max(off, 0);
     }
     for (int k = tid; k < G * kTileLd; k += blockDim.x) grid[k] = 0;
     __syncthreads();
@@ -1482,7 +1491,7 @@ __device__ __forceinline__ int fdiv_floor(int a, int b) { return a >= 0 ? a / b 
 // the prefixes (thread 0; at most kMaxBatch * kMaxPlanes entries).
 __global__ void __launch_bounds__(256) k_plan_batch(BatchPlan* __restrict__ plan, BatchStatic bs, int nev,
                                                     const WindowDev* __restrict__ win,
-                                                    const int* __restrict__ total_visits, long long vcap)
+                                                    long long vcap)
 {
     __shared__ int s_status;
     __shared__ int c_raster[kMaxBatch * kMaxPlanes], c_rows[kMaxBatch * kMaxPlanes],
@@ -1549,19 +1558,21 @@ __global__ void __launch_bounds__(256) k_plan_batch(BatchPlan* __restrict__ plan
             }
             plan->pre_conv[ip][nev] = t;
         }
-        const int tv = *total_visits;
-        plan->total_visits = tv;
+        unsigned long long tv = 0;  // visits of the pass, 64-bit (the list offsets are int)
+        for (int e = 0; e < nev; ++e) tv += win[(size_t)e * np].nvisits;
+        plan->total_visits = (long long)tv;
         plan->nev = nev;
         plan->np = np;
-        plan->status = s_status | ((long long)tv > vcap ? kBatchVisitOverflow : 0);
+        plan->status = s_status | (tv > (unsigned long long)vcap ? kBatchVisitOverflow : 0) |
+                       (tv >= 0x7fffffffull ? kBatchTooBig : 0);
         for (int k = 0; k < 3 + kMaxPlanes; ++k) plan->next[k] = 0;
     }
 }
 
-void launch_plan_batch(BatchPlan* plan, const BatchStatic& bs, int nev, const WindowDev* win, const int* total_visits,
-                       long long vcap, cudaStream_t s)
+void launch_plan_batch(BatchPlan* plan, const BatchStatic& bs, int nev, const WindowDev* win, long long vcap,
+                       cudaStream_t s)
 {
-    k_plan_batch<<<1, 256, 0, s>>>(plan, bs, nev, win, total_visits, vcap);
+    k_plan_batch<<<1, 256, 0, s>>>(plan, bs, nev, win, vcap);
 }
 
 // Next work item of a persistent block (all threads get the same value):
@@ -1604,7 +1615,7 @@ __global__ void __launch_bounds__(kRasterThreads) k_raster_batch(const BatchPlan
 {
     extern __shared__ int smem_i[];
     __shared__ float scale[kTileBlocks], iscale[kTileBlocks];
-    if (plan->status & kBatchVisitOverflow) return;
+    if (plan->status & kBatchSkip) return;
     __shared__ int s_item;
     const int ne = plan->nev * plan->np;
     const int total = plan->pre_raster[ne];
@@ -1667,7 +1678,7 @@ __global__ void k_rfft_batch(const BatchPlan* __restrict__ plan, const FftDesc* 
                              float* __restrict__ Q)
 {
     extern __shared__ float2 sm[];
-    if (plan->status & kBatchVisitOverflow) return;
+    if (plan->status & kBatchSkip) return;
     __shared__ int s_item;
     const int ne = plan->nev * plan->np;
     const int total = plan->pre_rows[ne];
@@ -1733,7 +1744,7 @@ __global__ void __launch_bounds__(32 * kConvRG) k_conv_batch(const BatchPlan* __
 {
     extern __shared__ float2 conv_smem[];
     __shared__ int s_item;
-    if (plan->status & kBatchVisitOverflow) return;
+    if (plan->status & kBatchSkip) return;
     const int nev = plan->nev, np = plan->np;
     int total = 0;
     for (int ip = ip0; ip < ip1; ++ip) total += plan->pre_conv[ip][nev];
@@ -1785,7 +1796,7 @@ __global__ void k_irfft_batch(const BatchPlan* __restrict__ plan, BatchStatic bs
                               const float2* __restrict__ V, float* __restrict__ frames, long long frame_stride)
 {
     extern __shared__ float2 sm[];
-    if (plan->status & kBatchVisitOverflow) return;
+    if (plan->status & kBatchSkip) return;
     __shared__ int s_item;
     const int ne = plan->nev * plan->np;
     const int total = plan->pre_orows[ne];

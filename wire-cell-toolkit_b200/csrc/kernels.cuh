@@ -71,9 +71,11 @@ static_assert(sizeof(Visit) == 32, "Visit layout");
 // Per-plane window reduction (BinnedDiffusion_transform.cxx:416-464).
 struct WindowDev {
     unsigned long long pmin, pmax, tmin, tmax;  // order-preserving double keys
+    // (plane 0 entry of an event only) 64-bit totals of the event: ticks of
+    // its patches longer than kTprof, and raster visits of all its patches
+    unsigned long long wide_ticks, nvisits;
     int nadded, out_time, out_pitch, oversize;
     int bigcharge;  // patches whose raster bound exceeds kMaxVisitBound
-    int wide_ticks; // (plane 0 entry of an event) ticks of the event's patches longer than kTprof
 };
 
 constexpr int kTprof = 16;        // time profiles up to this many ticks are computed once per depo
@@ -170,7 +172,8 @@ struct EvPlane {
 struct BatchPlan {
     int nev, np;
     int status;        // kBatch* bits
-    int total_visits;
+    int pad_;
+    long long total_visits;
     int pre_raster[kMaxBatch * kMaxPlanes + 1];
     int pre_rows[kMaxBatch * kMaxPlanes + 1];   // time-FFT rows: G * nin
     int pre_orows[kMaxBatch * kMaxPlanes + 1];  // inverse-FFT rows: nout
@@ -183,6 +186,8 @@ constexpr int kBatchOversize = 2;
 constexpr int kBatchBigCharge = 4;
 constexpr int kBatchNoClass = 8;
 constexpr int kBatchPoolShort = 16;  // not an error: some time profiles were computed in the raster
+constexpr int kBatchTooBig = 32;     // a pass holds 2^31 or more visits: fewer events per pass
+constexpr int kBatchSkip = kBatchVisitOverflow | kBatchTooBig;  // the raster and later stages skip the pass
 
 // Launch shapes of the persistent kernels (chosen by the autotuner).
 struct BatchTune {
@@ -218,9 +223,9 @@ struct FlucRec {
 // with the same function, so the frame does not depend on the pool.
 struct TprofPool {
     float* val;
-    int* off;     // per depo
-    int* used;    // allocation counter
-    long long cap;
+    int* off;                  // per depo
+    unsigned long long* used;  // allocation counter
+    long long cap;             // at most INT_MAX - 1 (offsets are int)
 };
 
 // ---- launchers (kernels.cu) ----
@@ -256,8 +261,8 @@ void launch_spec_mul(float2* X, long ldx, int nrows, int M, const float2* R, cud
 void launch_twiddles(float2* tw, float2* twh, int M, cudaStream_t s);
 
 // ---- batched-path launchers (kernels.cu) ----
-void launch_plan_batch(BatchPlan* plan, const BatchStatic& bs, int nev, const WindowDev* win, const int* total_visits,
-                       long long vcap, cudaStream_t s);
+void launch_plan_batch(BatchPlan* plan, const BatchStatic& bs, int nev, const WindowDev* win, long long vcap,
+                       cudaStream_t s);
 void launch_raster_batch(const BatchPlan* plan, const BatchStatic& bs, const PlaneSet& ps, const PatchRec* rec,
                          long long recstride, const float* tprof, const TprofPool& pool,
                          const unsigned char* wide_key, const int* wire_cnt, const int* wire_off,

@@ -245,3 +245,48 @@ def adjoint_depos(seed=4, n=20_000, ntracks=20):
     step = total / n
     d = track_depos(rng, ntracks=ntracks, step=step, lo=lo, hi=hi)
     return d[:n]
+
+
+def cosmic_depos(rng, ntracks, step=0.1 * mm, t0_spread=0.0):
+    """Cosmic-ray muons crossing the volume from top (y = +3 m) to bottom
+    (y = -3 m), entry and exit x, z uniform; Moyal dE/dx as track_depos."""
+    out = []
+    for _ in range(ntracks):
+        a = np.array((RESPONSE_X + 2500.0 * rng.random(), 3000.0, -1150.0 + 2300.0 * rng.random()))
+        b = np.array((RESPONSE_X + 2500.0 * rng.random(), -3000.0, -1150.0 + 2300.0 * rng.random()))
+        t0 = float(rng.uniform(0.0, t0_spread)) if t0_spread else 0.0
+        out.append(_segment(rng, a, b, step, t0))
+    return np.concatenate(out, axis=0)
+
+
+def _segment(rng, a, b, step, t0, dedx_mpv=2.1, dedx_width=0.1, wion=23.6e-6, recomb=0.7):
+    length = float(np.linalg.norm(b - a))
+    n = max(1, int(length / step))
+    s = (np.arange(n) + 0.5) / n
+    d = np.zeros((n, 7))
+    d[:, 0] = t0
+    d[:, 2:5] = a[None, :] + s[:, None] * (b - a)[None, :]
+    dedx = np.clip(dedx_mpv + dedx_width * moyal(rng, n), 0.2, 200.0)
+    d[:, 1] = -(dedx * (step / cm) / wion) * recomb
+    return d
+
+
+def calibration_events(nevents=16, ndepos=4_000_000, seed=9, depos_per_gev=40_000):
+    """Events of about ``ndepos`` depos: half cosmic-ray muons, half EM shower
+    blobs with energies drawn from an exponential spectrum of mean 1 GeV (a
+    shower of E GeV holds depos_per_gev * E depos)."""
+    rng = np.random.default_rng(seed)
+    events = []
+    for _ in range(nevents):
+        parts, n = [], 0
+        while n < ndepos // 2:
+            c = cosmic_depos(rng, 1)
+            parts.append(c)
+            n += len(c)
+        while n < ndepos:
+            e_gev = float(rng.exponential(1.0)) + 0.01
+            k = min(ndepos - n, max(10, int(depos_per_gev * e_gev)))
+            parts.append(shower_depos(rng, k, energy_mev=1000.0 * e_gev))
+            n += k
+        events.append(np.ascontiguousarray(np.concatenate(parts, axis=0)[:ndepos]))
+    return events
