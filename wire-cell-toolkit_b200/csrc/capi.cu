@@ -175,6 +175,7 @@ struct Core {
     std::vector<FaceState> faces;
     std::vector<std::unique_ptr<PlaneState>> planes;
     cudaStream_t own_stream{nullptr};
+    cudaStream_t copy_stream{nullptr};  // frame downloads of the host API, overlapped with later planes
     std::map<int, std::unique_ptr<FftPlanDev>> plans;
     // workspace
     DevBuf d_rec, d_win, d_Q, d_V, d_depos, d_frame, d_wcnt, d_woff, d_wcur, d_wlist, d_tprof, d_kbound;
@@ -262,6 +263,7 @@ struct Core {
         for (auto e : event_pool) cudaEventDestroy(e);
         if (h_win) cudaFreeHost(h_win);
         if (own_stream) cudaStreamDestroy(own_stream);
+        if (copy_stream) cudaStreamDestroy(copy_stream);
     }
 
     int plan_for(int M, FftDesc& d)
@@ -567,8 +569,10 @@ static int prepare_event(Core& c, const double* d_depos, size_t ndepos, cudaStre
     return WCT_OK;
 }
 
+// plane_done (optional, one event per plane): recorded on s once the plane's
+// frame rows are final, so a caller can download them while later planes run.
 static int forward_device(Core& c, const double* d_depos, size_t ndepos, float* d_frame, wct_plane_window* wins,
-                          int* frame_ident, cudaStream_t s)
+                          int* frame_ident, cudaStream_t s, cudaEvent_t* plane_done = nullptr)
 {
     EventPlan ev;
     int prc = prepare_event(c, d_depos, ndepos, s, ev);
@@ -632,7 +636,10 @@ static int forward_device(Core& c, const double* d_depos, size_t ndepos, float* 
             o.outside_time = c.h_win[ip].out_time;
             o.outside_pitch = c.h_win[ip].out_pitch;
         }
-        if (g.nin == 0) continue;  // no charge: the plane's frame rows stay zero
+        if (g.nin == 0) {  // no charge: the plane's frame rows stay zero
+            if (plane_done) CUDA_TRY(cudaEventRecord(plane_done[ip], s));
+            continue;
+        }
         const int nin = g.nin;
         const int nout = nin + 2 * ps.npad;
         const int N = g.N, M = N / 2;
@@ -653,6 +660,7 @@ static int forward_device(Core& c, const double* d_depos, size_t ndepos, float* 
                           std::min(N, w.nt_ref), nticks, d_frame + (size_t)ps.row0 * nticks, s);
         t_i.close(1);
         CUDA_TRY(cudaGetLastError());
+        if (plane_done) CUDA_TRY(cudaEventRecord(plane_done[ip], s));
     }
     if (frame_ident) *frame_ident = c.frame_count;
     ++c.frame_count;
@@ -1457,6 +1465,7 @@ int wct_dt_create(const char* json_config, wct_depotransform** out)
     }
     cudaError_t e = cudaSetDevice(h->core.device);
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&h->core.own_stream, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&h->core.copy_stream, cudaStreamNonBlocking);
     if (e != cudaSuccess) {
         delete h;
         return fail(WCT_ERR_CUDA, std::string("wct_dt_create: ") + cudaGetErrorString(e));
@@ -1644,10 +1653,35 @@ int wct_dt_forward(wct_depotransform* h, const double* depos, size_t ndepos, flo
     CUDA_TRY(c.d_frame.ensure(fbytes));
     if (ndepos)
         CUDA_TRY(cudaMemcpyAsync(c.d_depos.p, depos, sizeof(double) * 7 * ndepos, cudaMemcpyHostToDevice, s));
-    int rc = forward_device(c, c.d_depos.as<double>(), ndepos, c.d_frame.as<float>(), windows, frame_ident, s);
+    // each plane's rows go back as soon as they are final (copy stream), while
+    // the next planes are still transformed
+    const int np = (int)c.planes.size();
+    std::vector<cudaEvent_t> done(np);
+    for (auto& ev : done) ev = c.take_event();
+    int rc = forward_device(c, c.d_depos.as<double>(), ndepos, c.d_frame.as<float>(), windows, frame_ident, s,
+                            done.data());
+    if (rc == WCT_OK) {
+        const int nt = c.nticks();
+        for (int ip = 0; ip < np; ++ip) {
+            const PlaneState& ps = *c.planes[ip];
+            const size_t off = (size_t)ps.row0 * nt, bytes = sizeof(float) * (size_t)ps.desc.nwires * nt;
+            cudaError_t e = cudaStreamWaitEvent(c.copy_stream, done[ip], 0);
+            if (e == cudaSuccess)
+                e = cudaMemcpyAsync(frame + off, c.d_frame.as<float>() + off, bytes, cudaMemcpyDeviceToHost,
+                                    c.copy_stream);
+            if (e != cudaSuccess) {
+                rc = fail(WCT_ERR_CUDA, std::string("wct_dt_forward: frame download: ") + cudaGetErrorString(e));
+                break;
+            }
+        }
+    }
+    cudaError_t e1 = cudaStreamSynchronize(c.copy_stream);
+    cudaError_t e2 = cudaStreamSynchronize(s);
+    for (auto& ev : done) c.event_pool.push_back(ev);
     if (rc) return rc;
-    CUDA_TRY(cudaMemcpyAsync(frame, c.d_frame.p, fbytes, cudaMemcpyDeviceToHost, s));
-    CUDA_TRY(cudaStreamSynchronize(s));
+    if (e1 != cudaSuccess || e2 != cudaSuccess)
+        return fail(WCT_ERR_CUDA, std::string("wct_dt_forward: ") + cudaGetErrorString(e1 != cudaSuccess ? e1 : e2));
+    (void)fbytes;
     return WCT_OK;
 }
 
