@@ -737,13 +737,25 @@ __device__ __forceinline__ void raster_tile(const GridPlane& P, int row, int kti
                 si = make_int4(d, l_lo, ng, ((cb + 1024) << 11) | rnt);
                 my[kStageQ] = r.qn;
                 if (rnt <= 16) {
-                    // tick values scaled to the fixed point of their 64-tick block (0 outside the tile)
-                    const float* tp = tprof + (size_t)d * kTprof;
+                    // tick values scaled to the fixed point of their 64-tick block (0 outside the tile);
+                    // the whole 16-value profile row in four 128-bit loads (one L1 wavefront per
+                    // lane each, against one per value with scalar loads)
+                    static_assert(kTprof == 16, "profile rows are four float4");
+                    const float4* tp4 = reinterpret_cast<const float4*>(tprof + (size_t)d * kTprof);
+                    float tv[16];
+#pragma unroll
+                    for (int k4 = 0; k4 < 4; ++k4) {
+                        const float4 x = __ldg(tp4 + k4);
+                        tv[4 * k4] = x.x;
+                        tv[4 * k4 + 1] = x.y;
+                        tv[4 * k4 + 2] = x.z;
+                        tv[4 * k4 + 3] = x.w;
+                    }
 #pragma unroll
                     for (int k = 0; k < 16; ++k) {
                         const int c = cb + k;
                         float v = 0.f;
-                        if (k < rnt && c >= 0 && c < kTile) v = __ldg(tp + k) * r.qn * scale[c / kScaleBlock];
+                        if (k < rnt && c >= 0 && c < kTile) v = tv[k] * r.qn * scale[c / kScaleBlock];
                         my[kStageT + k] = v;
                     }
                 }

@@ -47,7 +47,7 @@ struct TimeDev {
 
 // Per (plane, depo) patch description, written by the prep kernel.
 // np == 0 marks a depo that does not contribute to the plane.
-struct PatchRec {
+struct __align__(16) PatchRec {  // 16-byte aligned: two 128-bit loads per record
     int toff, poff;
     unsigned short nt, np;
     float tcr;   // center_time - edge(toff)
@@ -59,7 +59,7 @@ struct PatchRec {
 static_assert(sizeof(PatchRec) == 32, "PatchRec layout");
 
 // One depo visit of a (wire, tick tile): what the raster needs of a PatchRec.
-struct Visit {
+struct __align__(16) Visit {
     int toff, poff;
     unsigned int nt_np;  // nt << 16 | np
     float pcr, sp, qn;
