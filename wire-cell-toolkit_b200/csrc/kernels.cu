@@ -153,10 +153,13 @@ __device__ __forceinline__ int fluc_ident(const FlucParams& fp, int ev)
     return (fp.ident_base ? *fp.ident_base : 0) + fp.ident0 + ev;
 }
 
-// One thread per depo of every event of the table; per-event window
+// One thread per (depo, plane) of every event of the table (plane =
+// blockIdx.y; each plane's threads drift the depo again, which is cheaper
+// than serialising the planes' FP64 chains in one thread); per-event window
 // statistics, visit counters and bounds (nkeys keys per event); patch
-// records [plane][depo] and time profiles indexed by the depo's position in
-// the concatenated depo array.
+// records [plane][depo]; plane 0's threads also write the drifted charge and
+// the time profiles indexed by the depo's position in the concatenated depo
+// array.
 __global__ void __launch_bounds__(256) k_prep_all(const double* __restrict__ dep, EventTable evt, int nkeys,
                                                   DriftDev dd, int do_drift, PlaneSet ps, TimeDev tb,
                                                   double drift_speed, double nsigma, PatchRec* __restrict__ rec,
@@ -216,10 +219,11 @@ __global__ void __launch_bounds__(256) k_prep_all(const double* __restrict__ dep
             }
         }
     }
-    if (fq && in) fq[i] = q;  // drifted charge, the trial count of fluctuated patches
+    const int ip = blockIdx.y;
+    if (fq && in && ip == 0) fq[i] = q;  // drifted charge, the trial count of fluctuated patches
     // The time profile depends on the depo only (GaussianDiffusion.cxx:124-136):
     // compute it once here for every plane's raster.
-    if (ok) {
+    if (ok && ip == 0) {
         const double st = __ddiv_rn(el, drift_speed);
         const double tlo = __dsub_rn(t, __dmul_rn(st, nsigma));
         const double thi = __dadd_rn(t, __dmul_rn(st, nsigma));
@@ -253,7 +257,7 @@ __global__ void __launch_bounds__(256) k_prep_all(const double* __restrict__ dep
     auto umax = [](unsigned long long a, unsigned long long b) { return a > b ? a : b; };
     auto iadd = [](int a, int b) { return a + b; };
     unsigned long long myvis = 0;
-    for (int ip = 0; ip < ps.nplanes; ++ip) {
+    {
         const PlaneDev& pl = ps.p[ip];
         unsigned long long kpmin = ~0ull, kpmax = 0ull, ktmin = ~0ull, ktmax = 0ull;
         int nadd = 0, nout_t = 0, nout_p = 0, nover = 0, nbig = 0;
@@ -403,7 +407,6 @@ __global__ void __launch_bounds__(256) k_prep_all(const double* __restrict__ dep
             if (l == 0 && nover) atomicAdd(&wd->oversize, nover);
             if (l == 0 && nbig) atomicAdd(&wd->bigcharge, nbig);
         }
-        __syncthreads();
     }
     // 64-bit visit total of the event (the visit lists use int offsets)
 #pragma unroll
@@ -418,7 +421,8 @@ void launch_prep_all(const double* depos, const EventTable& et, int nkeys, const
 {
     const int nblocks = et.blk0[et.nev];
     if (nblocks <= 0) return;
-    k_prep_all<<<nblocks, 256, 0, s>>>(depos, et, nkeys, dd, do_drift, ps, tb, drift_speed, nsigma, rec, win,
+    k_prep_all<<<dim3(nblocks, ps.nplanes), 256, 0, s>>>(depos, et, nkeys, dd, do_drift, ps, tb, drift_speed,
+                                                         nsigma, rec, win,
                                        wire_cnt, tprof, key_bound, fp, fq, wide);
 }
 
@@ -664,6 +668,16 @@ __device__ __forceinline__ void raster_tile(const GridPlane& P, int row, int kti
         const int off = wire_off[key];
         cnt = off < 0 ? 0 : (int)min((long long)wire_cnt[key], max(0ll, vcap - off));  // no reads past the list
         list = visits + max(off, 0);
+    }
+    if (cnt == 0) {
+        // no visit (block-uniform): the tile's G rows are zero
+        const int qc0 = tick_lo - P.col0;
+        for (int k = tid; k < G * kTile; k += kRasterThreads) {
+            const int g = k / kTile, c = k - g * kTile;
+            const int qc = qc0 + c;
+            if (qc >= 0 && qc < P.N) Q[P.qoff + ((size_t)g * P.nin + row) * P.N + qc] = 0.f;
+        }
+        return;
     }
     const bool spread = key >= 0 && wide_key[key];
     {
