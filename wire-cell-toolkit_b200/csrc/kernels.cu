@@ -160,7 +160,7 @@ __device__ __forceinline__ int fluc_ident(const FlucParams& fp, int ev)
 // records [plane][depo]; plane 0's threads also write the drifted charge and
 // the time profiles indexed by the depo's position in the concatenated depo
 // array.
-__global__ void __launch_bounds__(256) k_prep_all(const double* __restrict__ dep, EventTable evt, int nkeys,
+__global__ void __launch_bounds__(256, 3) k_prep_all(const double* __restrict__ dep, EventTable evt, int nkeys,
                                                   DriftDev dd, int do_drift, PlaneSet ps, TimeDev tb,
                                                   double drift_speed, double nsigma, PatchRec* __restrict__ rec,
                                                   WindowDev* __restrict__ win_all, int* __restrict__ cnt_all,
@@ -779,34 +779,35 @@ __device__ __forceinline__ void raster_tile(const GridPlane& P, int row, int kti
         __syncwarp();
         // lanes 0 .. nv-1 of this warp hold visits (e grows with the lane)
         const int nv = __popc(__ballot_sync(0xffffffffu, e < cnt));
-        const int half = lane >> 4, hl = lane & 15;
-        for (int v0 = 0; v0 < nv; v0 += 2) {
-            const int v = v0 + half;
+        // four visits at a time: a quarter warp per visit, each lane two ticks (hl, hl + 8)
+        const int qv = lane >> 3, hl = lane & 7;
+        for (int v0 = 0; v0 < nv; v0 += 4) {
+            const int v = v0 + qv;
             int4 vi = make_int4(0, 0, 0, 0);
             if (v < nv) vi = stagei[wbase + v];
             const int nt = vi.w & 2047;
             const bool wide = __any_sync(0xffffffffu, nt > 16);
             if (!wide) {
                 const int ng = vi.z;
-                const int cb = (vi.w >> 11) - 1024;
-                const int c = cb + hl;                  // tile column of this lane's tick
-                const float* vc = stage + (size_t)(wbase + v) * kStageStride;
-                const bool on = ng && hl < nt && c >= 0 && c < kTile;
-                const float tq = on ? vc[kStageT + hl] : 0.f;
-                const int mg = max(ng, __shfl_xor_sync(0xffffffffu, ng, 16));
-                float cf[kStageQ];
-#pragma unroll
-                for (int g = 0; g < kStageQ; ++g) cf[g] = vc[g];
-                int* dst = grid + vi.y * kTileLd + c;
-#pragma unroll
-                for (int g = 0; g < kStageQ; ++g) {
-                    if (g >= mg) break;
-                    if (on && g < ng) atomicAdd(dst + g * kTileLd, __float2int_rn(cf[g] * tq));
+                const int c0 = (vi.w >> 11) - 1024 + hl;  // tile columns of this lane's ticks: c0, c0 + 8
+                const float* vc = stage + (size_t)(wbase + min(v, 31)) * kStageStride;
+                const bool on0 = hl < nt && c0 >= 0 && c0 < kTile;
+                const bool on1 = hl + 8 < nt && c0 + 8 >= 0 && c0 + 8 < kTile;
+                const float tq0 = on0 ? vc[kStageT + hl] : 0.f;
+                const float tq1 = on1 ? vc[kStageT + hl + 8] : 0.f;
+                const int g0 = on0 ? ng : 0, g1 = on1 ? ng : 0;
+                const int mg = __reduce_max_sync(0xffffffffu, max(g0, g1));
+                int* dst = grid + vi.y * kTileLd + c0;
+                for (int g = 0; g < mg; ++g) {
+                    const float cf = vc[g];
+                    if (g < g0) atomicAdd(dst, __float2int_rn(cf * tq0));
+                    if (g < g1) atomicAdd(dst + 8, __float2int_rn(cf * tq1));
+                    dst += kTileLd;
                 }
             }
             else {
-                // at least one of the pair has more than 16 ticks: whole warp per visit
-                for (int hv = 0; hv < 2; ++hv) {
+                // at least one of the four has more than 16 ticks: whole warp per visit
+                for (int hv = 0; hv < 4; ++hv) {
                     const int vv = v0 + hv;
                     if (vv >= nv) break;
                     const int4 wi = stagei[wbase + vv];
@@ -860,7 +861,7 @@ __device__ __forceinline__ void raster_tile(const GridPlane& P, int row, int kti
     }
 }
 
-__global__ void __launch_bounds__(kRasterThreads) k_raster_wires(const PatchRec* __restrict__ rec,
+__global__ void __launch_bounds__(kRasterThreads, 4) k_raster_wires(const PatchRec* __restrict__ rec,
                                                                  const float* __restrict__ tprof,
                                                                  const int* __restrict__ wire_cnt,
                                                                  const int* __restrict__ wire_off,
@@ -1627,7 +1628,7 @@ __device__ __forceinline__ int find_entry(const int* __restrict__ pre, int n, in
 }
 
 template <bool FLUC>
-__global__ void __launch_bounds__(kRasterThreads) k_raster_batch(const BatchPlan* __restrict__ plan, BatchStatic bs,
+__global__ void __launch_bounds__(kRasterThreads, FLUC ? 1 : 4) k_raster_batch(const BatchPlan* __restrict__ plan, BatchStatic bs,
                                                                  PlaneSet ps, const PatchRec* __restrict__ rec,
                                                                  long long recstride,
                                                                  const float* __restrict__ tprof, TprofPool pool,
