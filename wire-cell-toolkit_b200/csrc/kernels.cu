@@ -735,7 +735,7 @@ __device__ __forceinline__ void raster_tile(const GridPlane& P, int row, int kti
                         const float u2 = x2 * isg;
                         const float g2 = __expf(-0.5f * u2 * u2);
                         const float p = bin_from_edges(e1, e2);
-                        const float wt = p > 0.f ? fmaf(c0 * (g2 - g1), __frcp_rn(p), x2 * inv_pbs) : 0.0f;
+                        const float wt = p > 0.f ? fmaf(c0 * (g2 - g1), __fdividef(1.0f, p), x2 * inv_pbs) : 0.0f;
                         my[lb] += p * wt;
                         my[lb + 1] += p * (1.0f - wt);
                         e1 = e2;
@@ -779,9 +779,9 @@ __device__ __forceinline__ void raster_tile(const GridPlane& P, int row, int kti
         __syncwarp();
         // lanes 0 .. nv-1 of this warp hold visits (e grows with the lane)
         const int nv = __popc(__ballot_sync(0xffffffffu, e < cnt));
-        // four visits at a time: a quarter warp per visit, each lane two ticks (hl, hl + 8)
-        const int qv = lane >> 3, hl = lane & 7;
-        for (int v0 = 0; v0 < nv; v0 += 4) {
+        // eight visits at a time: four lanes per visit, each lane four ticks (hl + 4k)
+        const int qv = lane >> 2, hl = lane & 3;
+        for (int v0 = 0; v0 < nv; v0 += 8) {
             const int v = v0 + qv;
             int4 vi = make_int4(0, 0, 0, 0);
             if (v < nv) vi = stagei[wbase + v];
@@ -789,25 +789,32 @@ __device__ __forceinline__ void raster_tile(const GridPlane& P, int row, int kti
             const bool wide = __any_sync(0xffffffffu, nt > 16);
             if (!wide) {
                 const int ng = vi.z;
-                const int c0 = (vi.w >> 11) - 1024 + hl;  // tile columns of this lane's ticks: c0, c0 + 8
+                const int c0 = (vi.w >> 11) - 1024 + hl;  // tile column of this lane's first tick
                 const float* vc = stage + (size_t)(wbase + min(v, 31)) * kStageStride;
-                const bool on0 = hl < nt && c0 >= 0 && c0 < kTile;
-                const bool on1 = hl + 8 < nt && c0 + 8 >= 0 && c0 + 8 < kTile;
-                const float tq0 = on0 ? vc[kStageT + hl] : 0.f;
-                const float tq1 = on1 ? vc[kStageT + hl + 8] : 0.f;
-                const int g0 = on0 ? ng : 0, g1 = on1 ? ng : 0;
-                const int mg = __reduce_max_sync(0xffffffffu, max(g0, g1));
+                float tq[4];
+                int gl[4];  // groups this lane adds at tick hl + 4k (0: tick outside the patch or tile)
+                int mgl = 0;
+#pragma unroll
+                for (int k = 0; k < 4; ++k) {
+                    const int c = c0 + 4 * k;
+                    const bool on = hl + 4 * k < nt && c >= 0 && c < kTile;
+                    tq[k] = on ? vc[kStageT + hl + 4 * k] : 0.f;
+                    gl[k] = on ? ng : 0;
+                    mgl = max(mgl, gl[k]);
+                }
+                const int mg = __reduce_max_sync(0xffffffffu, mgl);
                 int* dst = grid + vi.y * kTileLd + c0;
                 for (int g = 0; g < mg; ++g) {
                     const float cf = vc[g];
-                    if (g < g0) atomicAdd(dst, __float2int_rn(cf * tq0));
-                    if (g < g1) atomicAdd(dst + 8, __float2int_rn(cf * tq1));
+#pragma unroll
+                    for (int k = 0; k < 4; ++k)
+                        if (g < gl[k]) atomicAdd(dst + 4 * k, __float2int_rn(cf * tq[k]));
                     dst += kTileLd;
                 }
             }
             else {
-                // at least one of the four has more than 16 ticks: whole warp per visit
-                for (int hv = 0; hv < 4; ++hv) {
+                // at least one of the eight has more than 16 ticks: whole warp per visit
+                for (int hv = 0; hv < 8; ++hv) {
                     const int vv = v0 + hv;
                     if (vv >= nv) break;
                     const int4 wi = stagei[wbase + vv];
