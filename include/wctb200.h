@@ -135,6 +135,41 @@ int wct_convolve_rows_device(const float* in, long ld_in, int nrows, int n_in, c
 int wct_convolve_rows_device_noalloc(const float* in, long ld_in, int nrows, int n_in, const float* resp,
                                      int n_resp, int nfft, float* out, long ld_out, int n_out, void* stream);
 
+/* ---- GPU IDFT (iface/inc/WireCellIface/IDFT.h) ---- */
+
+/* The IDFT interface on the GPU: the cuFftDFT plugin that
+ * cuda/test/test_idft_cufftdft.bats names (the reference has no GPU
+ * implementation; FftwDFT, aux/src/FftwDFT.cxx:149-217, and TorchDFT,
+ * pytorch/src/DFT.cxx:80-123, are its CPU ones).  Arrays are single
+ * precision complex values stored as interleaved (re, im) float pairs in C
+ * (row-major) order; in and out may be the same array.  Forward transforms
+ * are unnormalised, inverse transforms carry 1/n (1/(nrows*ncols) for 2d).
+ * 1b: axis = 1 transforms each of the nrows rows (length ncols), axis = 0
+ * each column (length nrows), as numpy.fft.  Any length from 1 up: lengths
+ * whose prime factors are at most 7 run directly up to 14336; any other
+ * length up to 7168 runs through Bluestein's chirp-z transform; beyond
+ * that WCT_ERR_SIZE.  The host-pointer calls (IDFT::fwd1d, inv1d, fwd1b,
+ * inv1b, fwd2d, inv2d, transpose) copy through the current device and
+ * return when the result is in out; they may be called from several
+ * threads at once (IDFT.h: "safe concurrent calls"). */
+int wct_dft_fwd1d(const float* in, float* out, int size);
+int wct_dft_inv1d(const float* in, float* out, int size);
+int wct_dft_fwd1b(const float* in, float* out, int nrows, int ncols, int axis);
+int wct_dft_inv1b(const float* in, float* out, int nrows, int ncols, int axis);
+int wct_dft_fwd2d(const float* in, float* out, int nrows, int ncols);
+int wct_dft_inv2d(const float* in, float* out, int nrows, int ncols);
+/* IDFT::transpose: out[c][r] = in[r][c] for an nrows x ncols input, real or
+ * complex elements. */
+int wct_dft_transpose_real(const float* in, float* out, int nrows, int ncols);
+int wct_dft_transpose_complex(const float* in, float* out, int nrows, int ncols);
+/* The same on device arrays, enqueued on stream (cudaStream_t, NULL = legacy
+ * default stream) of the current device; inverse != 0 selects the inverse.
+ * Column transforms and in-place transposes take scratch from the
+ * stream-ordered allocator. */
+int wct_dft_1b_device(const float* in, float* out, int nrows, int ncols, int axis, int inverse, void* stream);
+int wct_dft_2d_device(const float* in, float* out, int nrows, int ncols, int inverse, void* stream);
+int wct_dft_transpose_device(const float* in, float* out, int nrows, int ncols, int is_complex, void* stream);
+
 /* ---- DepoTransform (gen/src/DepoTransform.cxx, IDepoFramer) ---- */
 
 /* DepoTransform::configure (gen/src/DepoTransform.cxx:76-113) from JSON with

@@ -70,6 +70,17 @@ SIGNATURES = {
     "wct_pir_destroy": (C.c_int, [C.c_void_p]),
     "wct_convolve_rows_device": (C.c_int, [C.c_void_p, C.c_long, C.c_int, C.c_int, C.c_void_p, C.c_int, C.c_int,
                                            C.c_void_p, C.c_long, C.c_int, C.c_void_p]),
+    "wct_dft_fwd1d": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int]),
+    "wct_dft_inv1d": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int]),
+    "wct_dft_fwd1b": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int]),
+    "wct_dft_inv1b": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int]),
+    "wct_dft_fwd2d": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_int]),
+    "wct_dft_inv2d": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_int]),
+    "wct_dft_transpose_real": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_int]),
+    "wct_dft_transpose_complex": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_int]),
+    "wct_dft_1b_device": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_void_p]),
+    "wct_dft_2d_device": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_void_p]),
+    "wct_dft_transpose_device": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_void_p]),
     "wct_convolve_rows_device_noalloc": (C.c_int, [C.c_void_p, C.c_long, C.c_int, C.c_int, C.c_void_p, C.c_int,
                                                    C.c_int, C.c_void_p, C.c_long, C.c_int, C.c_void_p]),
     "wct_dt_create": (C.c_int, [C.c_char_p, C.POINTER(C.c_void_p)]),
@@ -193,6 +204,71 @@ def convolve_rows(d_in, ld_in, nrows, n_in, d_resp, n_resp, d_out, ld_out, n_out
     """Batched FFT convolution of device rows with one response (pointers as ints)."""
     _check(lib().wct_convolve_rows_device(C.c_void_p(d_in), ld_in, nrows, n_in, C.c_void_p(d_resp), n_resp, nfft,
                                           C.c_void_p(d_out), ld_out, n_out, C.c_void_p(stream) if stream else None))
+
+
+class IDFT:
+    """The IDFT interface (iface/inc/WireCellIface/IDFT.h) on the GPU, for
+    numpy arrays: complex64 in and out (converted if needed), C order, forward
+    unnormalised, inverse with 1/n; 1b axis as numpy.fft (1: along rows).
+    Each call copies through the current device and returns the result."""
+
+    @staticmethod
+    def _c(a):
+        return np.ascontiguousarray(a, dtype=np.complex64)
+
+    def _run(self, fn, x, *shape):
+        x = self._c(x)
+        out = np.empty_like(x)
+        _check(fn(x.ctypes.data, out.ctypes.data, *shape))
+        return out
+
+    def fwd1d(self, x):
+        x = self._c(x).reshape(-1)
+        return self._run(lib().wct_dft_fwd1d, x, x.size)
+
+    def inv1d(self, x):
+        x = self._c(x).reshape(-1)
+        return self._run(lib().wct_dft_inv1d, x, x.size)
+
+    def fwd1b(self, x, axis):
+        x = self._c(x)
+        return self._run(lib().wct_dft_fwd1b, x, x.shape[0], x.shape[1], int(axis))
+
+    def inv1b(self, x, axis):
+        x = self._c(x)
+        return self._run(lib().wct_dft_inv1b, x, x.shape[0], x.shape[1], int(axis))
+
+    def fwd2d(self, x):
+        x = self._c(x)
+        return self._run(lib().wct_dft_fwd2d, x, x.shape[0], x.shape[1])
+
+    def inv2d(self, x):
+        x = self._c(x)
+        return self._run(lib().wct_dft_inv2d, x, x.shape[0], x.shape[1])
+
+    def transpose(self, x):
+        """IDFT::transpose of a 2-D float32 or complex64 array."""
+        if np.iscomplexobj(x):
+            x = self._c(x)
+            out = np.empty((x.shape[1], x.shape[0]), dtype=np.complex64)
+            _check(lib().wct_dft_transpose_complex(x.ctypes.data, out.ctypes.data, x.shape[0], x.shape[1]))
+        else:
+            x = np.ascontiguousarray(x, dtype=np.float32)
+            out = np.empty((x.shape[1], x.shape[0]), dtype=np.float32)
+            _check(lib().wct_dft_transpose_real(x.ctypes.data, out.ctypes.data, x.shape[0], x.shape[1]))
+        return out
+
+
+def dft_1b_device(d_in, d_out, nrows, ncols, axis, inverse=False, stream=None):
+    """IDFT 1b transform of a device complex64 array (pointers as ints)."""
+    _check(lib().wct_dft_1b_device(C.c_void_p(d_in), C.c_void_p(d_out), nrows, ncols, int(axis), int(bool(inverse)),
+                                   C.c_void_p(stream) if stream else None))
+
+
+def dft_2d_device(d_in, d_out, nrows, ncols, inverse=False, stream=None):
+    """IDFT 2d transform of a device complex64 array (pointers as ints)."""
+    _check(lib().wct_dft_2d_device(C.c_void_p(d_in), C.c_void_p(d_out), nrows, ncols, int(bool(inverse)),
+                                   C.c_void_p(stream) if stream else None))
 
 
 def convolve_rows_noalloc(d_in, ld_in, nrows, n_in, d_resp, n_resp, d_out, ld_out, n_out, nfft=0, stream=None):

@@ -1330,6 +1330,190 @@ static int autotune_batch(Core& c, const double* d_depos, const long long* offse
     return WCT_OK;
 }
 
+// ---------------------------------------------------------------------------
+// GPU IDFT (iface/inc/WireCellIface/IDFT.h; the cuFftDFT plugin that
+// cuda/test/test_idft_cufftdft.bats expects): complex single-precision
+// transforms, forward unnormalised, inverse with 1/n, C (row-major) order,
+// in place allowed.  Lengths whose prime factors are at most 7 use the
+// shared-memory FFT directly; any other length goes through Bluestein's
+// chirp-z transform with a 7-smooth FFT length >= 2n - 1.  Column transforms
+// (axis 0 of the 1b methods, the second pass of the 2d methods) are row
+// transforms between two transposes.  Host-pointer calls copy through the
+// current device on the per-thread default stream and return when done, so
+// several threads may call at once.
+// ---------------------------------------------------------------------------
+constexpr int kDftMaxFft = 14336;  // longest shared-memory FFT: two buffers of 14336 complex = 224 KB
+
+static bool dft_smooth(int n)
+{
+    int r[kFftMaxStages], ns = 0;
+    return fft_radices(n, r, ns);
+}
+
+static int dft_bluestein_length(int n)
+{
+    for (long long P = 2LL * n - 1; P <= kDftMaxFft; ++P)
+        if (dft_smooth((int)P)) return (int)P;
+    return 0;
+}
+
+struct BluesteinDev {
+    int N{0}, P{0};
+    DevBuf chirp, bhat;
+};
+static std::map<std::pair<int, int>, std::unique_ptr<BluesteinDev>> g_bluestein;  // (device, N)
+
+// Chirp c_n = exp(-pi i n^2 / N) (phase from n^2 mod 2N, exact in integers)
+// and the spectrum of the chirp filter, built once per device and length.
+static int bluestein_plan(int N, FftDesc& dP, const float2*& chirp, const float2*& bhat)
+{
+    int dev = 0;
+    CUDA_TRY(cudaGetDevice(&dev));
+    const int P = dft_bluestein_length(N);
+    if (!P)
+        return fail(WCT_ERR_SIZE, "DFT length " + std::to_string(N) + " needs a Bluestein FFT longer than " +
+                                      std::to_string(kDftMaxFft));
+    int rc = device_plan(P, dP);
+    if (rc) return rc;
+    std::lock_guard<std::mutex> lk(g_ops_mtx);
+    auto key = std::make_pair(dev, N);
+    auto it = g_bluestein.find(key);
+    if (it == g_bluestein.end()) {
+        auto b = std::make_unique<BluesteinDev>();
+        b->N = N;
+        b->P = P;
+        std::vector<float2> c(N);
+        const double pi = 3.14159265358979323846;
+        for (int n = 0; n < N; ++n) {
+            const long long q = ((long long)n * n) % (2LL * N);
+            const double ph = pi * (double)q / (double)N;
+            c[n] = make_float2((float)std::cos(ph), (float)-std::sin(ph));
+        }
+        CUDA_TRY(b->chirp.ensure(sizeof(float2) * N));
+        CUDA_TRY(b->bhat.ensure(sizeof(float2) * P));
+        cudaStream_t s = cudaStreamPerThread;
+        CUDA_TRY(cudaMemcpyAsync(b->chirp.p, c.data(), sizeof(float2) * N, cudaMemcpyHostToDevice, s));
+        launch_bluestein_b(b->chirp.as<float2>(), b->bhat.as<float2>(), N, P, s);
+        launch_c2c_rows(b->bhat.as<float2>(), P, b->bhat.as<float2>(), P, 1, dP, -1, 1.0f, s);
+        CUDA_TRY(cudaGetLastError());
+        CUDA_TRY(cudaStreamSynchronize(s));
+        it = g_bluestein.emplace(key, std::move(b)).first;
+    }
+    chirp = it->second->chirp.as<float2>();
+    bhat = it->second->bhat.as<float2>();
+    return WCT_OK;
+}
+
+// nrows transforms of length n along rows (row strides ld_in, ld_out).
+static int dft_rows(const float2* in, long ld_in, float2* out, long ld_out, int nrows, int n, int sign, cudaStream_t s)
+{
+    if (nrows <= 0 || n <= 0) return WCT_OK;
+    const float scale = sign > 0 ? 1.0f / (float)n : 1.0f;
+    if (n <= kDftMaxFft && dft_smooth(n)) {
+        FftDesc d;
+        int rc = device_plan(n, d);
+        if (rc) return rc;
+        launch_c2c_rows(in, ld_in, out, ld_out, nrows, d, sign, scale, s);
+    }
+    else {
+        FftDesc dP;
+        const float2 *chirp = nullptr, *bhat = nullptr;
+        int rc = bluestein_plan(n, dP, chirp, bhat);
+        if (rc) return rc;
+        launch_bluestein_rows(in, ld_in, out, ld_out, nrows, n, dP, chirp, bhat, sign, scale, s);
+    }
+    CUDA_TRY(cudaGetLastError());
+    return WCT_OK;
+}
+
+// Stream-ordered scratch freed when it goes out of scope.
+struct AsyncBuf {
+    void* p{nullptr};
+    cudaStream_t s{nullptr};
+    ~AsyncBuf()
+    {
+        if (p) cudaFreeAsync(p, s);
+    }
+};
+
+static int dft_check(const void* in, const void* out, int nrows, int ncols)
+{
+    if (!in || !out || nrows < 0 || ncols < 0) return fail(WCT_ERR_ARG, "DFT: null array or negative size");
+    if (nrows > 65535 * 32 || ncols > 65535 * 32 || (long long)nrows * ncols > (1LL << 31))
+        return fail(WCT_ERR_SIZE, "DFT: array too large");
+    return WCT_OK;
+}
+
+// Transforms along axis 1 (rows) or 0 (columns) of a row-major nrows x ncols array.
+static int dft_1b_dev(const float2* in, float2* out, int nrows, int ncols, int axis, int sign, cudaStream_t s)
+{
+    if (axis != 0 && axis != 1) return fail(WCT_ERR_ARG, "DFT: axis must be 0 or 1");
+    if (nrows == 0 || ncols == 0) return WCT_OK;
+    if (axis == 1) return dft_rows(in, ncols, out, ncols, nrows, ncols, sign, s);
+    AsyncBuf t;
+    t.s = s;
+    CUDA_TRY(cudaMallocAsync(&t.p, sizeof(float2) * (size_t)nrows * ncols, s));
+    float2* tp = static_cast<float2*>(t.p);
+    launch_transpose_c(in, tp, nrows, ncols, s);
+    int rc = dft_rows(tp, nrows, tp, nrows, ncols, nrows, sign, s);
+    if (rc) return rc;
+    launch_transpose_c(tp, out, ncols, nrows, s);
+    CUDA_TRY(cudaGetLastError());
+    return WCT_OK;
+}
+
+static int dft_2d_dev(const float2* in, float2* out, int nrows, int ncols, int sign, cudaStream_t s)
+{
+    int rc = dft_1b_dev(in, out, nrows, ncols, 1, sign, s);
+    if (rc) return rc;
+    return dft_1b_dev(out, out, nrows, ncols, 0, sign, s);
+}
+
+static int dft_transpose_dev(const float* in, float* out, int nrows, int ncols, bool cplx, cudaStream_t s)
+{
+    if (nrows == 0 || ncols == 0) return WCT_OK;
+    const size_t bytes = (cplx ? sizeof(float2) : sizeof(float)) * (size_t)nrows * ncols;
+    AsyncBuf t;
+    t.s = s;
+    void* dst = out;
+    if (in == out) {  // through scratch
+        CUDA_TRY(cudaMallocAsync(&t.p, bytes, s));
+        dst = t.p;
+    }
+    if (cplx)
+        launch_transpose_c(reinterpret_cast<const float2*>(in), static_cast<float2*>(dst), nrows, ncols, s);
+    else
+        launch_transpose_r(in, static_cast<float*>(dst), nrows, ncols, s);
+    CUDA_TRY(cudaGetLastError());
+    if (dst != out) CUDA_TRY(cudaMemcpyAsync(out, dst, bytes, cudaMemcpyDeviceToDevice, s));
+    return WCT_OK;
+}
+
+// Host arrays: copy in, transform on the current device, copy out.
+// kind 0: 1b (axis), 1: 2d, 2: transpose (cplx).
+static int dft_host(const float* in, float* out, int nrows, int ncols, int kind, int axis, int sign, bool cplx)
+{
+    int rc = dft_check(in, out, nrows, ncols);
+    if (rc) return rc;
+    if (nrows == 0 || ncols == 0) return WCT_OK;
+    cudaStream_t s = cudaStreamPerThread;
+    const size_t bytes = (cplx ? sizeof(float2) : sizeof(float)) * (size_t)nrows * ncols;
+    {
+        AsyncBuf d;
+        d.s = s;
+        CUDA_TRY(cudaMallocAsync(&d.p, bytes, s));
+        CUDA_TRY(cudaMemcpyAsync(d.p, in, bytes, cudaMemcpyHostToDevice, s));
+        float2* dp = static_cast<float2*>(d.p);
+        if (kind == 0) rc = dft_1b_dev(dp, dp, nrows, ncols, axis, sign, s);
+        else if (kind == 1) rc = dft_2d_dev(dp, dp, nrows, ncols, sign, s);
+        else rc = dft_transpose_dev(static_cast<float*>(d.p), static_cast<float*>(d.p), nrows, ncols, cplx, s);
+        if (rc) return rc;
+        CUDA_TRY(cudaMemcpyAsync(out, d.p, bytes, cudaMemcpyDeviceToHost, s));
+    }
+    CUDA_TRY(cudaStreamSynchronize(s));
+    return WCT_OK;
+}
+
 }  // namespace wctb200
 
 using namespace wctb200;
@@ -1951,6 +2135,56 @@ int wct_dt_destroy(wct_depotransform* h)
         delete h;
     }
     return WCT_OK;
+}
+
+/* ---- GPU IDFT ---- */
+
+int wct_dft_fwd1d(const float* in, float* out, int size) { return dft_host(in, out, 1, size, 0, 1, -1, true); }
+int wct_dft_inv1d(const float* in, float* out, int size) { return dft_host(in, out, 1, size, 0, 1, +1, true); }
+int wct_dft_fwd1b(const float* in, float* out, int nrows, int ncols, int axis)
+{
+    return dft_host(in, out, nrows, ncols, 0, axis, -1, true);
+}
+int wct_dft_inv1b(const float* in, float* out, int nrows, int ncols, int axis)
+{
+    return dft_host(in, out, nrows, ncols, 0, axis, +1, true);
+}
+int wct_dft_fwd2d(const float* in, float* out, int nrows, int ncols)
+{
+    return dft_host(in, out, nrows, ncols, 1, 1, -1, true);
+}
+int wct_dft_inv2d(const float* in, float* out, int nrows, int ncols)
+{
+    return dft_host(in, out, nrows, ncols, 1, 1, +1, true);
+}
+int wct_dft_transpose_real(const float* in, float* out, int nrows, int ncols)
+{
+    return dft_host(in, out, nrows, ncols, 2, 1, -1, false);
+}
+int wct_dft_transpose_complex(const float* in, float* out, int nrows, int ncols)
+{
+    return dft_host(in, out, nrows, ncols, 2, 1, -1, true);
+}
+int wct_dft_1b_device(const float* in, float* out, int nrows, int ncols, int axis, int inverse, void* stream)
+{
+    int rc = dft_check(in, out, nrows, ncols);
+    if (rc) return rc;
+    return dft_1b_dev(reinterpret_cast<const float2*>(in), reinterpret_cast<float2*>(out), nrows, ncols, axis,
+                      inverse ? +1 : -1, (cudaStream_t)stream);
+}
+int wct_dft_2d_device(const float* in, float* out, int nrows, int ncols, int inverse, void* stream)
+{
+    int rc = dft_check(in, out, nrows, ncols);
+    if (rc) return rc;
+    if (nrows == 0 || ncols == 0) return WCT_OK;
+    return dft_2d_dev(reinterpret_cast<const float2*>(in), reinterpret_cast<float2*>(out), nrows, ncols,
+                      inverse ? +1 : -1, (cudaStream_t)stream);
+}
+int wct_dft_transpose_device(const float* in, float* out, int nrows, int ncols, int is_complex, void* stream)
+{
+    int rc = dft_check(in, out, nrows, ncols);
+    if (rc) return rc;
+    return dft_transpose_dev(in, out, nrows, ncols, is_complex != 0, (cudaStream_t)stream);
 }
 
 }  // extern "C"

@@ -258,6 +258,18 @@ void launch_irfft_rows(const float2* Vh, int nrows, const FftDesc& d, int wire0,
                        int ncols, int nticks, float* frame, cudaStream_t s);
 
 void launch_spec_mul(float2* X, long ldx, int nrows, int M, const float2* R, cudaStream_t s);
+
+// GPU IDFT (dft.cu): complex row transforms (sign -1 forward, +1 inverse,
+// result times scale), Bluestein rows for any length N (FFT length dP.M >=
+// 2N - 1, chirp c_n = exp(-pi i n^2 / N), bhat = FFT of the chirp filter
+// built by launch_bluestein_b), and transposes of row-major matrices.
+void launch_c2c_rows(const float2* in, long ld_in, float2* out, long ld_out, int nrows, const FftDesc& d, int sign,
+                     float scale, cudaStream_t s);
+void launch_bluestein_rows(const float2* in, long ld_in, float2* out, long ld_out, int nrows, int N, const FftDesc& dP,
+                           const float2* chirp, const float2* bhat, int sign, float scale, cudaStream_t s);
+void launch_bluestein_b(const float2* chirp, float2* b, int N, int P, cudaStream_t s);
+void launch_transpose_c(const float2* in, float2* out, int nrows, int ncols, cudaStream_t s);
+void launch_transpose_r(const float* in, float* out, int nrows, int ncols, cudaStream_t s);
 void launch_twiddles(float2* tw, float2* twh, int M, cudaStream_t s);
 
 // ---- batched-path launchers (kernels.cu) ----
