@@ -101,6 +101,18 @@ int wct_pir_info(const wct_pir* pir, double* pitch, double* impact, double* half
                  int* nimp_per_wire, int* npaths, int* nticks, int* waveform_pad);
 /* IImpactResponse::waveform() of one path: nticks floats. */
 int wct_pir_waveform(const wct_pir* pir, int path, float* out);
+/* PlaneImpactResponse "long_responses" and "long_padding"
+ * (gen/src/PlaneImpactResponse.cxx:46-47,121-150): the long-range response
+ * is the circular convolution, at fft_best_length(nticks), of the nlong
+ * waveforms (concatenated in long_wave, lengths long_len; each cut or zero
+ * padded to that length); its pad is long_padding / tick ticks
+ * (IImpactResponse::long_aux_waveform, long_aux_waveform_pad).  nlong = 0
+ * removes it. */
+int wct_pir_set_long_responses(wct_pir* pir, int nlong, const int* long_len, const double* long_wave,
+                               double long_padding);
+/* Length (0: no long-range response) and pad of the long-range response, and its samples. */
+int wct_pir_long_info(const wct_pir* pir, int* nsamples, int* pad);
+int wct_pir_long_waveform(const wct_pir* pir, float* out);
 int wct_pir_destroy(wct_pir* pir);
 
 /* ---- Batched FFT convolution of rows ---- */
@@ -146,9 +158,11 @@ int wct_convolve_rows_device_noalloc(const float* in, long ld_in, int nrows, int
  * are unnormalised, inverse transforms carry 1/n (1/(nrows*ncols) for 2d).
  * 1b: axis = 1 transforms each of the nrows rows (length ncols), axis = 0
  * each column (length nrows), as numpy.fft.  Any length from 1 up: lengths
- * whose prime factors are at most 7 run directly up to 14336; any other
- * length up to 7168 runs through Bluestein's chirp-z transform; beyond
- * that WCT_ERR_SIZE.  The host-pointer calls (IDFT::fwd1d, inv1d, fwd1b,
+ * whose prime factors are at most 7 run in shared memory up to 14336 and as
+ * four-step transforms (two passes of shorter ones) above; any other length
+ * runs through Bluestein's chirp-z transform on such a length.  Arrays hold
+ * at most 2^30 values, and the column transforms and transposes at most
+ * 2097120 per side (WCT_ERR_SIZE beyond).  The host-pointer calls (IDFT::fwd1d, inv1d, fwd1b,
  * inv1b, fwd2d, inv2d, transpose) copy through the current device and
  * return when the result is in out; they may be called from several
  * threads at once (IDFT.h: "safe concurrent calls"). */
@@ -191,6 +205,13 @@ int wct_dt_add_plane(wct_depotransform* dt, int face, const wct_plane_desc* desc
 /* Use a PIR for a plane: ImpactTransform's response selection
  * (gen/src/ImpactTransform.cxx:26-74) over pirs[plane]. */
 int wct_dt_set_response_pir(wct_depotransform* dt, int face, int plane, const wct_pir* pir);
+/* The plane's long-range response (set by wct_dt_set_response_pir from the
+ * PIR; nsamples = 0: none): every frame row inside the plane's window is
+ * circularly convolved with wave, both zero padded to
+ * fft_best_length(nticks + pad), and cut back to nticks
+ * (ImpactTransform::waveform, gen/src/ImpactTransform.cxx:327-343); the
+ * adjoint applies the transposed step. */
+int wct_dt_set_long_response(wct_depotransform* dt, int face, int plane, int nsamples, const float* wave, int pad);
 /* Same from a ready table: table[g][j][k] for impact group g < ngroups, wire
  * offset j - npad in [-npad, npad], tick k < nsamples (the closest() waveform
  * for that group and offset). */

@@ -107,6 +107,7 @@ class OrcJob(C.Structure):
         ("ndepos", C.c_int), ("depos", C.c_void_p),
         ("fp64", C.c_int), ("nthreads", C.c_int),
         ("fluctuate", C.c_int), ("drift_fluctuate", C.c_int), ("seed", C.c_ulonglong),
+        ("nlong", C.c_int), ("long_len", C.c_void_p), ("long_wave", C.c_void_p), ("long_padding", C.c_double),
     ]
 
 
@@ -155,6 +156,14 @@ class Job:
             j.short_wave = sw.ctypes.data
         j.overall_short_padding = cfg["overall_short_padding"]
         j.pir_nticks = cfg["pir_nticks"]
+        longs = [np.asarray(w, dtype=np.float64) for w in cfg.get("long_responses", [])]
+        j.nlong = len(longs)
+        j.long_padding = cfg.get("long_padding", 1.5e6)
+        if longs:
+            ll = self._arr(np.array([len(w) for w in longs], dtype=np.int32))
+            lw = self._arr(np.concatenate(longs))
+            j.long_len = ll.ctypes.data
+            j.long_wave = lw.ctypes.data
         planes = (OrcPlane * len(cfg["planes"]))()
         for i, (pl, fr) in enumerate(zip(cfg["planes"], cfg["fr"])):
             p = planes[i]

@@ -572,6 +572,9 @@ struct PIR {
     std::vector<ImpactResp<T>> ir;
     std::vector<std::vector<int>> bywire;
     double half_extent{0}, pitch{0}, impact{0};
+    // long_aux_waveform / long_aux_waveform_pad of every path (PlaneImpactResponse.cxx:121-150,252)
+    std::vector<T> long_wf;
+    int long_pad{0};
     int nwires() const { return (int)bywire.size(); }
     int nimp_per_wire() const { return (int)bywire[0].size(); }
 
@@ -606,12 +609,28 @@ struct FRPlane {
     double pitch;            // PlaneResponse::pitch
 };
 
-// PlaneImpactResponse::build_responses, gen/src/PlaneImpactResponse.cxx:89-269
-// (no long responses: they are empty in every configuration handled here).
+// PlaneImpactResponse::build_responses, gen/src/PlaneImpactResponse.cxx:89-269,
+// long responses included (:121-150): the product of their spectra at
+// fft_best_length(nbins), back in time.
 template <typename T>
 static void build_pir(const FRPlane& fr, double tstart, double period, const std::vector<std::vector<double>>& shorts,
-                      double overall_short_padding, double tick, int nbins, PIR<T>& pir)
+                      double overall_short_padding, double tick, int nbins, PIR<T>& pir,
+                      const std::vector<std::vector<double>>& longs = {}, double long_padding = 0.0)
 {
+    pir.long_wf.clear();
+    pir.long_pad = 0;
+    if (!longs.empty()) {
+        const size_t n_long = fft_best_length((size_t)nbins, false);
+        std::vector<std::complex<T>> long_spec(n_long, std::complex<T>(1.0, 0.0));
+        for (auto& lw : longs) {
+            std::vector<T> wave(lw.begin(), lw.end());
+            wave.resize(n_long, 0);
+            auto spec = fwd_r2c<T>(wave);
+            for (size_t i = 0; i < n_long; ++i) long_spec[i] *= spec[i];
+        }
+        pir.long_wf = inv_c2r<T>(long_spec);
+        pir.long_pad = (int)(long_padding / tick);
+    }
     using C = std::complex<T>;
     const size_t n_short = fft_best_length((size_t)(overall_short_padding / tick), false);
     std::vector<C> short_spec(n_short, C(1.0, 0.0));
@@ -839,7 +858,11 @@ struct ImpactTransform {
         return fwd_r2c<T>(red);
     }
 
-    ImpactTransform(const PIR<T>& pir, BinnedDiffusion<T>& bd, std::vector<PlaneRecord>* rec)
+    const PIR<T>* m_pir{nullptr};
+    mutable int long_n{0};
+    mutable std::vector<C> long_spec;  // spectrum of the long waveform at long_n
+
+    ImpactTransform(const PIR<T>& pir, BinnedDiffusion<T>& bd, std::vector<PlaneRecord>* rec) : m_pir(&pir)
     {
         const int G = std::round(pir.pitch / pir.impact) + 1;
         const int npad = std::round((pir.nwires() - 1) / 2.);
@@ -943,7 +966,8 @@ struct ImpactTransform {
                                              std::imag(acc[(size_t)(NW - 1 - r) * NT + c2]);
     }
 
-    // ImpactTransform::waveform, ImpactTransform.cxx:312-347 (no long response).
+    // ImpactTransform::waveform, ImpactTransform.cxx:312-347, with the
+    // long-range step (:327-343) when the PIR has a long response.
     void waveform(int iwire, int nsamples, T* out) const
     {
         std::fill(out, out + nsamples, (T)0);
@@ -951,6 +975,21 @@ struct ImpactTransform {
         for (int i = 0; i != nsamples; i++)
             if (i >= win.start_tick && i < win.end_tick)
                 out[i] = decon[(size_t)(iwire - win.start_ch) * win.nt + (i - win.start_tick)];
+        if (m_pir && !m_pir->long_wf.empty()) {
+            const int nlength = (int)fft_best_length((size_t)nsamples + m_pir->long_pad, false);
+            if (long_n != nlength) {
+                std::vector<T> lr(m_pir->long_wf.begin(), m_pir->long_wf.end());
+                lr.resize(nlength, 0);
+                long_spec = fwd_r2c<T>(lr);
+                long_n = nlength;
+            }
+            std::vector<T> wf(out, out + nsamples);
+            wf.resize(nlength, 0);
+            auto spec = fwd_r2c<T>(wf);
+            for (int i = 0; i < nlength; ++i) spec[i] *= long_spec[i];
+            wf = inv_c2r<T>(spec);
+            for (int i = 0; i < nsamples; ++i) out[i] = wf[i];
+        }
     }
 };
 
@@ -1003,7 +1042,23 @@ struct OrcJob {
     int fluctuate;
     int drift_fluctuate;
     unsigned long long seed;
+    // PlaneImpactResponse "long_responses" (concatenated) and "long_padding"
+    int nlong;
+    const int* long_len;
+    const double* long_wave;
+    double long_padding;
 };
+
+static std::vector<std::vector<double>> job_longs(const OrcJob* job)
+{
+    std::vector<std::vector<double>> longs;
+    size_t off = 0;
+    for (int s = 0; s < job->nlong; ++s) {
+        longs.emplace_back(job->long_wave + off, job->long_wave + off + job->long_len[s]);
+        off += job->long_len[s];
+    }
+    return longs;
+}
 
 struct OrcPlaneOut {
     int start_ch, end_ch, start_tick, end_tick, nw, nt;
@@ -1112,7 +1167,7 @@ int orc_pir_build(const OrcJob* job, int iplane, double* waveforms, int* bywire,
         orc::FRPlane fr{pl.npaths, pl.nfr, pl.pitchpos, pl.current, pl.fr_pitch};
         orc::PIR<T> pir;
         orc::build_pir<T>(fr, job->fr_tstart, job->fr_period, shorts, job->overall_short_padding, job->tick,
-                          job->pir_nticks, pir);
+                          job->pir_nticks, pir, job_longs(job), job->long_padding);
         for (size_t p = 0; p < pir.ir.size(); ++p)
             for (int k = 0; k < job->pir_nticks; ++k)
                 waveforms[p * job->pir_nticks + k] = pir.ir[p].waveform[k];
@@ -1173,6 +1228,7 @@ int orc_run(const OrcJob* job, void* frame, OrcPlaneOut* pout, int* rec)
         for (int p = 0; p < job->nplanes; ++p) row0[p + 1] = row0[p] + job->planes[p].nwires;
         const size_t ndep_rec = (size_t)job->ndepos;
 
+        const std::vector<std::vector<double>> longs = job_longs(job);
         auto do_plane = [&](int ip, auto tag) {
             using T = decltype(tag);
             const OrcPlane& pl = job->planes[ip];
@@ -1182,7 +1238,7 @@ int orc_run(const OrcJob* job, void* frame, OrcPlaneOut* pout, int* rec)
             orc::FRPlane fr{pl.npaths, pl.nfr, pl.pitchpos, pl.current, pl.fr_pitch};
             orc::PIR<T> pir;
             orc::build_pir<T>(fr, job->fr_tstart, job->fr_period, shorts, job->overall_short_padding, job->tick,
-                              job->pir_nticks, pir);
+                              job->pir_nticks, pir, longs, job->long_padding);
             orc::Binning tbins(job->readout_time / job->tick, job->start_time, job->start_time + job->readout_time);
             orc::BinnedDiffusion<T> bd(pim, tbins, job->nsigma);
             std::mt19937 prng((std::uint32_t)(job->seed * 2654435761ull + 31 * (unsigned long long)ip + 1));

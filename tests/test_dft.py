@@ -11,8 +11,8 @@ import pytest
 
 from conftest import rel_l2
 
-SMOOTH = [1, 2, 7, 64, 1000, 1024, 3200, 6000, 14336]
-OTHER = [11, 13, 97, 1009, 4097, 7001]
+SMOOTH = [1, 2, 7, 64, 1000, 1024, 3200, 6000, 14336, 16384, 100000]   # above 14336: four steps
+OTHER = [11, 13, 97, 1009, 4097, 7001, 7177, 9317, 20011]              # above 7168: Bluestein in global memory
 
 
 def _rand(rng, *shape):
@@ -31,7 +31,7 @@ def test_1d_against_numpy(dft, n):
     x = _rand(rng, n)
     X = dft.fwd1d(x)
     ref = np.fft.fft(x.astype(np.complex128))
-    tol = 2e-6 if n in SMOOTH else 1e-5
+    tol = (2e-6 if n <= 14336 else 5e-6) if n in SMOOTH else 2e-5
     assert rel_l2(X, ref) < tol
     back = dft.inv1d(X)
     assert rel_l2(back, x) < 2 * tol
@@ -142,8 +142,6 @@ def test_device_2d_matches_host(wct, dft):
 @pytest.mark.gpu
 def test_errors(wct, dft):
     with pytest.raises(wct.WctError) as e:
-        dft.fwd1d(np.zeros(7177, np.complex64))  # 7177 = 7177 (prime): Bluestein beyond 14336
-    assert e.value.code == 6
-    with pytest.raises(wct.WctError):
         dft.fwd1b(np.zeros((4, 4), np.complex64), 2)
+    assert e.value.code == 1
     assert dft.fwd1d(np.zeros(0, np.complex64)).size == 0

@@ -68,6 +68,9 @@ SIGNATURES = {
     "wct_pir_info": (C.c_int, [C.c_void_p] + [C.c_void_p] * 8),
     "wct_pir_waveform": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p]),
     "wct_pir_destroy": (C.c_int, [C.c_void_p]),
+    "wct_pir_set_long_responses": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_double]),
+    "wct_pir_long_info": (C.c_int, [C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
+    "wct_pir_long_waveform": (C.c_int, [C.c_void_p, C.c_void_p]),
     "wct_convolve_rows_device": (C.c_int, [C.c_void_p, C.c_long, C.c_int, C.c_int, C.c_void_p, C.c_int, C.c_int,
                                            C.c_void_p, C.c_long, C.c_int, C.c_void_p]),
     "wct_dft_fwd1d": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int]),
@@ -88,6 +91,7 @@ SIGNATURES = {
     "wct_dt_add_face": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(C.c_int)]),
     "wct_dt_add_plane": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.POINTER(C.c_int)]),
     "wct_dt_set_response_pir": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_void_p]),
+    "wct_dt_set_long_response": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_int]),
     "wct_dt_set_response_table": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_double,
                                             C.c_double, C.c_int, C.c_void_p]),
     "wct_dt_frame_shape": (C.c_int, [C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
@@ -159,10 +163,12 @@ def _check(rc):
 
 
 class PlaneImpactResponse:
-    """Gen::PlaneImpactResponse built from a Response::Schema plane and short
-    responses (gen/src/PlaneImpactResponse.cxx:56-269)."""
+    """Gen::PlaneImpactResponse built from a Response::Schema plane, short
+    responses and optional long responses with their padding
+    (gen/src/PlaneImpactResponse.cxx:56-269)."""
 
-    def __init__(self, fr, short_responses, overall_short_padding, tick, nticks):
+    def __init__(self, fr, short_responses, overall_short_padding, tick, nticks, long_responses=(),
+                 long_padding=1.5e6):
         L = lib()
         pp = np.ascontiguousarray(fr["pitchpos"], dtype=np.float64)
         cur = np.ascontiguousarray(fr["current"], dtype=np.float64)
@@ -175,6 +181,20 @@ class PlaneImpactResponse:
         _check(L.wct_pir_create(C.byref(d), len(shorts), sl.ctypes.data, sw.ctypes.data, overall_short_padding,
                                 tick, nticks, C.byref(h)))
         self.h = h
+        longs = [np.asarray(w, dtype=np.float64) for w in long_responses]
+        if longs:
+            ll = np.array([len(w) for w in longs], dtype=np.int32)
+            lw = np.concatenate(longs)
+            _check(L.wct_pir_set_long_responses(h, len(longs), ll.ctypes.data, lw.ctypes.data, long_padding))
+
+    def long_waveform(self):
+        """(long-range response samples, pad in ticks); an empty array without one."""
+        n, pad = C.c_int(), C.c_int()
+        _check(lib().wct_pir_long_info(self.h, C.byref(n), C.byref(pad)))
+        out = np.zeros(n.value, dtype=np.float32)
+        if n.value:
+            _check(lib().wct_pir_long_waveform(self.h, out.ctypes.data))
+        return out, pad.value
 
     def info(self):
         pitch, impact, he = C.c_double(), C.c_double(), C.c_double()
@@ -527,7 +547,7 @@ def from_config(cfg, device=0):
     for pl, fr in zip(cfg["planes"], cfg["fr"]):
         p = dt.add_plane(face, pl)
         pir = PlaneImpactResponse(fr, cfg.get("short_responses", []), cfg["overall_short_padding"], cfg["tick"],
-                                  cfg["pir_nticks"])
+                                  cfg["pir_nticks"], cfg.get("long_responses", []), cfg.get("long_padding", 1.5e6))
         dt.set_response_pir(face, p, pir)
     return dt
 

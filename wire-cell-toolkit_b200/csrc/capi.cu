@@ -149,6 +149,11 @@ struct PlaneState {
     DevBuf d_table;        // [G][2npad+1][ldr] floats
     int spec_N{0};
     DevBuf d_spec;         // [G][2npad+1][M] packed spectra for spec_N
+    // long-range response (ImpactTransform::waveform, gen/src/ImpactTransform.cxx:327-343); empty: none
+    std::vector<float> long_wf;
+    int long_pad{0};
+    int long_nfft{0};
+    DevBuf d_long_spec;    // [long_nfft] spectrum of long_wf cut or zero padded to long_nfft
     int row0{0};           // frame row offset
 };
 
@@ -179,6 +184,7 @@ struct Core {
     std::map<int, std::unique_ptr<FftPlanDev>> plans;
     // workspace
     DevBuf d_rec, d_win, d_Q, d_V, d_depos, d_frame, d_wcnt, d_woff, d_wcur, d_wlist, d_tprof, d_kbound;
+    DevBuf d_long_z, d_glong;  // long-range step: packed row spectra; adjoint's frame-gradient rows
     DevBuf d_gframe, d_gdep, d_gglob;  // adjoint host entry point
     DevBuf d_fq, d_fluc;               // fluctuation: drifted charges, per (plane, depo) draw sums
     DevBuf d_pool, d_pool_off, d_pool_used;  // time profiles of long patches
@@ -569,6 +575,46 @@ static int prepare_event(Core& c, const double* d_depos, size_t ndepos, cudaStre
     return WCT_OK;
 }
 
+static int dft_rows(const float2* in, long ld_in, float2* out, long ld_out, int nrows, int n, int sign,
+                    cudaStream_t s);
+
+// The long-range step of ImpactTransform::waveform
+// (gen/src/ImpactTransform.cxx:327-343) on nrows frame rows of nticks
+// samples (row stride ld): each row, zero padded to nfft =
+// fft_best_length(nticks + long_pad), is circularly convolved with the long
+// waveform cut or zero padded to nfft, and cut back to nticks.  Rows go two
+// per complex transform (the kernel is real); any nfft of the reference's
+// tables (7-smooth directly, others through Bluestein).  transpose: the
+// adjoint (correlation, conjugate spectrum).
+static int long_conv_rows(Core& c, PlaneState& ps, float* rows, long ld, int nrows, int nticks, bool transpose,
+                          cudaStream_t s)
+{
+    if (ps.long_wf.empty() || nrows <= 0 || nticks <= 0) return WCT_OK;
+    const int nfft = (int)fft_best_length((size_t)nticks + (size_t)ps.long_pad, false);
+    if (ps.long_nfft != nfft) {
+        std::vector<float2> lw(nfft, make_float2(0.f, 0.f));
+        for (int k = 0; k < nfft && k < (int)ps.long_wf.size(); ++k) lw[k].x = ps.long_wf[k];
+        CUDA_TRY(ps.d_long_spec.ensure(sizeof(float2) * nfft));
+        CUDA_TRY(cudaMemcpyAsync(ps.d_long_spec.p, lw.data(), sizeof(float2) * nfft, cudaMemcpyHostToDevice, s));
+        int rc = dft_rows(ps.d_long_spec.as<float2>(), nfft, ps.d_long_spec.as<float2>(), nfft, 1, nfft, -1, s);
+        if (rc) return rc;
+        CUDA_TRY(cudaStreamSynchronize(s));  // lw goes out of scope
+        ps.long_nfft = nfft;
+    }
+    const int nz = (nrows + 1) / 2;
+    CUDA_TRY(c.d_long_z.ensure(sizeof(float2) * (size_t)nz * nfft));
+    float2* Z = c.d_long_z.as<float2>();
+    launch_pack_rows(rows, ld, nrows, nticks, Z, nfft, s);
+    int rc = dft_rows(Z, nfft, Z, nfft, nz, nfft, -1, s);
+    if (rc) return rc;
+    launch_cmul_rows(Z, nfft, nz, ps.d_long_spec.as<float2>(), transpose, s);
+    rc = dft_rows(Z, nfft, Z, nfft, nz, nfft, +1, s);
+    if (rc) return rc;
+    launch_unpack_rows(Z, nfft, rows, ld, nrows, nticks, s);
+    CUDA_TRY(cudaGetLastError());
+    return WCT_OK;
+}
+
 // plane_done (optional, one event per plane): recorded on s once the plane's
 // frame rows are final, so a caller can download them while later planes run.
 static int forward_device(Core& c, const double* d_depos, size_t ndepos, float* d_frame, wct_plane_window* wins,
@@ -658,7 +704,11 @@ static int forward_device(Core& c, const double* d_depos, size_t ndepos, float* 
         Core::StageTimer t_i(&c, 4, s);
         launch_irfft_rows(c.d_V.as<float2>(), nout, d, w.start_ch - ps.npad, wlo, whi, w.start_tick,
                           std::min(N, w.nt_ref), nticks, d_frame + (size_t)ps.row0 * nticks, s);
-        t_i.close(1);
+        if (!ps.long_wf.empty() && whi > wlo) {
+            rc = long_conv_rows(c, ps, d_frame + ((size_t)ps.row0 + wlo) * nticks, nticks, whi - wlo, nticks, false, s);
+            if (rc) return rc;
+        }
+        t_i.close(ps.long_wf.empty() || whi <= wlo ? 1 : 6);
         CUDA_TRY(cudaGetLastError());
         if (plane_done) CUDA_TRY(cudaEventRecord(plane_done[ip], s));
     }
@@ -712,8 +762,19 @@ static int adjoint_device(Core& c, const double* d_depos, size_t ndepos, const f
         float* Gr = c.d_V.as<float>();  // [nout][N] real, then [nout][M] spectra in place
         const int wlo = std::max(0, w.m_start_ch), whi = std::min(ps.desc.nwires, w.m_end_ch);
         Core::StageTimer t_f(&c, 6, s);
-        launch_grad_rows(d_gframe + (size_t)ps.row0 * nticks, nticks, w.start_ch - ps.npad, wlo, whi, w.start_tick,
-                         std::min(N, w.nt_ref), nout, N, Gr, s);
+        const float* gplane = d_gframe + (size_t)ps.row0 * nticks;
+        if (!ps.long_wf.empty() && whi > wlo) {
+            // the long-range step's transpose on a copy of the window rows (same row indices)
+            CUDA_TRY(c.d_glong.ensure(sizeof(float) * (size_t)whi * nticks));
+            float* gl = c.d_glong.as<float>();
+            CUDA_TRY(cudaMemcpyAsync(gl + (size_t)wlo * nticks, gplane + (size_t)wlo * nticks,
+                                     sizeof(float) * (size_t)(whi - wlo) * nticks, cudaMemcpyDeviceToDevice, s));
+            rc = long_conv_rows(c, ps, gl + (size_t)wlo * nticks, nticks, whi - wlo, nticks, true, s);
+            if (rc) return rc;
+            gplane = gl;
+        }
+        launch_grad_rows(gplane, nticks, w.start_ch - ps.npad, wlo, whi, w.start_tick, std::min(N, w.nt_ref), nout,
+                         N, Gr, s);
         launch_rfft_rows(Gr, N, N, reinterpret_cast<float2*>(Gr), M, nout, d, s);
         t_f.close(2);
         float* dQ = c.d_Q.as<float>() + g.qoff;
@@ -1218,6 +1279,17 @@ static int forward_batch_device(Core& c, const double* d_depos, const long long*
         if (st & kBatchOversize) return fail(WCT_ERR_SIZE, "a diffusion patch exceeds 1024 ticks or 1024 impact bins");
         if (st & kBatchBigCharge) return fail(WCT_ERR_SIZE, "a depo charge exceeds 5e11 electrons");
         if (st & kBatchNoClass) return fail(WCT_ERR_SIZE, "forward batch: a window exceeds the time-FFT ladder");
+        // long-range step on every plane with one (rows outside an event's window are zero and stay zero)
+        for (int ip = 0; ip < np; ++ip) {
+            PlaneState& ps = *c.planes[ip];
+            if (ps.long_wf.empty()) continue;
+            const int nticks = c.nticks();
+            for (int e = 0; e < nev; ++e) {
+                int rc2 = long_conv_rows(c, ps, d_frames + (size_t)e * c.nrows() * nticks + (size_t)ps.row0 * nticks,
+                                         nticks, ps.desc.nwires, nticks, false, s);
+                if (rc2) return rc2;
+            }
+        }
         if (wins) {
             for (int e = 0; e < nev; ++e) {
                 const BatchPlan& P = b.h_plans[e / K];
@@ -1344,38 +1416,63 @@ static int autotune_batch(Core& c, const double* d_depos, const long long* offse
 // ---------------------------------------------------------------------------
 constexpr int kDftMaxFft = 14336;  // longest shared-memory FFT: two buffers of 14336 complex = 224 KB
 
-static bool dft_smooth(int n)
+static bool dft_smooth(long long n)
 {
-    int r[kFftMaxStages], ns = 0;
-    return fft_radices(n, r, ns);
+    if (n < 1) return false;
+    for (int p : {2, 3, 5, 7})
+        while (n % p == 0) n /= p;
+    return n == 1;
 }
 
 static int dft_bluestein_length(int n)
 {
-    for (long long P = 2LL * n - 1; P <= kDftMaxFft; ++P)
-        if (dft_smooth((int)P)) return (int)P;
+    for (long long P = 2LL * n - 1; P < (1LL << 30); ++P)
+        if (dft_smooth(P)) return (int)P;
     return 0;
 }
+
+// Four-step split of a 7-smooth N > kDftMaxFft: N = N1 * N2, both <= kDftMaxFft,
+// N1 the largest such divisor not above sqrt(N).
+static bool four_step_split(int N, int& N1, int& N2)
+{
+    for (int d = (int)std::sqrt((double)N) + 1; d >= 1; --d) {
+        if (N % d || d > kDftMaxFft || N / d > kDftMaxFft || (long long)d * d > N) continue;
+        N1 = d;
+        N2 = N / d;
+        return true;
+    }
+    return false;
+}
+
+// Stream-ordered scratch freed when it goes out of scope.
+struct AsyncBuf {
+    void* p{nullptr};
+    cudaStream_t s{nullptr};
+    ~AsyncBuf()
+    {
+        if (p) cudaFreeAsync(p, s);
+    }
+};
 
 struct BluesteinDev {
     int N{0}, P{0};
     DevBuf chirp, bhat;
 };
+static std::mutex g_blue_mtx;
 static std::map<std::pair<int, int>, std::unique_ptr<BluesteinDev>> g_bluestein;  // (device, N)
+
+static int dft_rows(const float2* in, long ld_in, float2* out, long ld_out, int nrows, int n, int sign,
+                    cudaStream_t s);
 
 // Chirp c_n = exp(-pi i n^2 / N) (phase from n^2 mod 2N, exact in integers)
 // and the spectrum of the chirp filter, built once per device and length.
-static int bluestein_plan(int N, FftDesc& dP, const float2*& chirp, const float2*& bhat)
+static int bluestein_plan(int N, int& P, const float2*& chirp, const float2*& bhat)
 {
     int dev = 0;
     CUDA_TRY(cudaGetDevice(&dev));
-    const int P = dft_bluestein_length(N);
-    if (!P)
-        return fail(WCT_ERR_SIZE, "DFT length " + std::to_string(N) + " needs a Bluestein FFT longer than " +
-                                      std::to_string(kDftMaxFft));
-    int rc = device_plan(P, dP);
-    if (rc) return rc;
-    std::lock_guard<std::mutex> lk(g_ops_mtx);
+    P = dft_bluestein_length(N);
+    if (!P) return fail(WCT_ERR_SIZE, "DFT length " + std::to_string(N) + " too long");
+    std::lock_guard<std::mutex> lk(g_blue_mtx);
     auto key = std::make_pair(dev, N);
     auto it = g_bluestein.find(key);
     if (it == g_bluestein.end()) {
@@ -1391,12 +1488,13 @@ static int bluestein_plan(int N, FftDesc& dP, const float2*& chirp, const float2
         }
         CUDA_TRY(b->chirp.ensure(sizeof(float2) * N));
         CUDA_TRY(b->bhat.ensure(sizeof(float2) * P));
-        cudaStream_t s = cudaStreamPerThread;
-        CUDA_TRY(cudaMemcpyAsync(b->chirp.p, c.data(), sizeof(float2) * N, cudaMemcpyHostToDevice, s));
-        launch_bluestein_b(b->chirp.as<float2>(), b->bhat.as<float2>(), N, P, s);
-        launch_c2c_rows(b->bhat.as<float2>(), P, b->bhat.as<float2>(), P, 1, dP, -1, 1.0f, s);
+        cudaStream_t st = cudaStreamPerThread;
+        CUDA_TRY(cudaMemcpyAsync(b->chirp.p, c.data(), sizeof(float2) * N, cudaMemcpyHostToDevice, st));
+        launch_bluestein_b(b->chirp.as<float2>(), b->bhat.as<float2>(), N, P, st);
+        int rc = dft_rows(b->bhat.as<float2>(), P, b->bhat.as<float2>(), P, 1, P, -1, st);
+        if (rc) return rc;
         CUDA_TRY(cudaGetLastError());
-        CUDA_TRY(cudaStreamSynchronize(s));
+        CUDA_TRY(cudaStreamSynchronize(st));
         it = g_bluestein.emplace(key, std::move(b)).first;
     }
     chirp = it->second->chirp.as<float2>();
@@ -1404,43 +1502,96 @@ static int bluestein_plan(int N, FftDesc& dP, const float2*& chirp, const float2
     return WCT_OK;
 }
 
-// nrows transforms of length n along rows (row strides ld_in, ld_out).
-static int dft_rows(const float2* in, long ld_in, float2* out, long ld_out, int nrows, int n, int sign, cudaStream_t s)
+// Four-step FFT of contiguous rows of a 7-smooth length N = N1 * N2: column
+// transforms of the N1 x N2 view (transpose, rows of N1), twiddles, rows of
+// N2, transpose back.  Inverse scales by 1/N (1/N1 * 1/N2).
+static int four_step_rows(const float2* in, float2* out, int nrows, int N, int sign, cudaStream_t s)
 {
-    if (nrows <= 0 || n <= 0) return WCT_OK;
-    const float scale = sign > 0 ? 1.0f / (float)n : 1.0f;
-    if (n <= kDftMaxFft && dft_smooth(n)) {
-        FftDesc d;
-        int rc = device_plan(n, d);
+    int N1 = 0, N2 = 0;
+    if (!four_step_split(N, N1, N2)) return fail(WCT_ERR_SIZE, "DFT length " + std::to_string(N) + " too long");
+    const int chunk = std::max(1, std::min(65535, (int)std::min<long long>(nrows, (1LL << 28) / N)));
+    AsyncBuf w;
+    w.s = s;
+    CUDA_TRY(cudaMallocAsync(&w.p, sizeof(float2) * (size_t)chunk * N, s));
+    float2* W = static_cast<float2*>(w.p);
+    for (int r0 = 0; r0 < nrows; r0 += chunk) {
+        const int nb = std::min(chunk, nrows - r0);
+        const float2* src = in + (size_t)r0 * N;
+        float2* dst = out + (size_t)r0 * N;
+        launch_transpose_c(src, W, N1, N2, s, nb);                       // [N2][N1]
+        int rc = dft_rows(W, N1, W, N1, nb * N2, N1, sign, s);          // along n1
         if (rc) return rc;
-        launch_c2c_rows(in, ld_in, out, ld_out, nrows, d, sign, scale, s);
-    }
-    else {
-        FftDesc dP;
-        const float2 *chirp = nullptr, *bhat = nullptr;
-        int rc = bluestein_plan(n, dP, chirp, bhat);
+        launch_twiddle4(W, (long long)nb * N, N1, N2, sign, s);
+        launch_transpose_c(W, dst, N2, N1, s, nb);                      // [N1][N2]
+        rc = dft_rows(dst, N2, dst, N2, nb * N1, N2, sign, s);          // along n2
         if (rc) return rc;
-        launch_bluestein_rows(in, ld_in, out, ld_out, nrows, n, dP, chirp, bhat, sign, scale, s);
+        launch_transpose_c(dst, W, N1, N2, s, nb);                      // X[k2 * N1 + k1]
+        CUDA_TRY(cudaMemcpyAsync(dst, W, sizeof(float2) * (size_t)nb * N, cudaMemcpyDeviceToDevice, s));
     }
     CUDA_TRY(cudaGetLastError());
     return WCT_OK;
 }
 
-// Stream-ordered scratch freed when it goes out of scope.
-struct AsyncBuf {
-    void* p{nullptr};
-    cudaStream_t s{nullptr};
-    ~AsyncBuf()
-    {
-        if (p) cudaFreeAsync(p, s);
+// nrows transforms of length n along rows (row strides ld_in, ld_out; the
+// four-step and long Bluestein paths take contiguous rows).
+static int dft_rows(const float2* in, long ld_in, float2* out, long ld_out, int nrows, int n, int sign, cudaStream_t s)
+{
+    if (nrows <= 0 || n <= 0) return WCT_OK;
+    const float scale = sign > 0 ? 1.0f / (float)n : 1.0f;
+    if (dft_smooth(n) && n <= kDftMaxFft) {
+        FftDesc d;
+        int rc = device_plan(n, d);
+        if (rc) return rc;
+        launch_c2c_rows(in, ld_in, out, ld_out, nrows, d, sign, scale, s);
     }
-};
+    else if (dft_smooth(n)) {
+        if (ld_in != n || ld_out != n) return fail(WCT_ERR_ARG, "DFT: long rows must be contiguous");
+        return four_step_rows(in, out, nrows, n, sign, s);
+    }
+    else {
+        int P = 0;
+        const float2 *chirp = nullptr, *bhat = nullptr;
+        int rc = bluestein_plan(n, P, chirp, bhat);
+        if (rc) return rc;
+        if (P <= kDftMaxFft) {
+            FftDesc dP;
+            rc = device_plan(P, dP);
+            if (rc) return rc;
+            launch_bluestein_rows(in, ld_in, out, ld_out, nrows, n, dP, chirp, bhat, sign, scale, s);
+        }
+        else {  // through global memory, the length-P transforms by four steps
+            const int chunk = std::max(1, std::min(nrows, (int)std::min<long long>(65535, (1LL << 28) / P)));
+            AsyncBuf z;
+            z.s = s;
+            CUDA_TRY(cudaMallocAsync(&z.p, sizeof(float2) * (size_t)chunk * P, s));
+            float2* Z = static_cast<float2*>(z.p);
+            for (int r0 = 0; r0 < nrows; r0 += chunk) {
+                const int nb = std::min(chunk, nrows - r0);
+                launch_blue_pre(in + (size_t)r0 * ld_in, ld_in, Z, nb, n, P, chirp, sign > 0, s);
+                rc = dft_rows(Z, P, Z, P, nb, P, -1, s);
+                if (rc) return rc;
+                launch_cmul_rows(Z, P, nb, bhat, false, s);
+                rc = dft_rows(Z, P, Z, P, nb, P, +1, s);  // carries 1/P
+                if (rc) return rc;
+                launch_blue_post(Z, P, out + (size_t)r0 * ld_out, ld_out, nb, n, chirp, sign > 0, scale, s);
+            }
+        }
+    }
+    CUDA_TRY(cudaGetLastError());
+    return WCT_OK;
+}
 
 static int dft_check(const void* in, const void* out, int nrows, int ncols)
 {
     if (!in || !out || nrows < 0 || ncols < 0) return fail(WCT_ERR_ARG, "DFT: null array or negative size");
-    if (nrows > 65535 * 32 || ncols > 65535 * 32 || (long long)nrows * ncols > (1LL << 31))
-        return fail(WCT_ERR_SIZE, "DFT: array too large");
+    if ((long long)nrows * ncols > (1LL << 30)) return fail(WCT_ERR_SIZE, "DFT: array too large");
+    return WCT_OK;
+}
+
+// Transposes tile the matrix with a grid of 32 x 32 blocks (at most 65535 tiles per side).
+static int dft_check_transpose(int nrows, int ncols)
+{
+    if (nrows > 65535 * 32 || ncols > 65535 * 32) return fail(WCT_ERR_SIZE, "DFT: a side longer than 2097120");
     return WCT_OK;
 }
 
@@ -1450,6 +1601,8 @@ static int dft_1b_dev(const float2* in, float2* out, int nrows, int ncols, int a
     if (axis != 0 && axis != 1) return fail(WCT_ERR_ARG, "DFT: axis must be 0 or 1");
     if (nrows == 0 || ncols == 0) return WCT_OK;
     if (axis == 1) return dft_rows(in, ncols, out, ncols, nrows, ncols, sign, s);
+    int rc0 = dft_check_transpose(nrows, ncols);
+    if (rc0) return rc0;
     AsyncBuf t;
     t.s = s;
     CUDA_TRY(cudaMallocAsync(&t.p, sizeof(float2) * (size_t)nrows * ncols, s));
@@ -1472,6 +1625,8 @@ static int dft_2d_dev(const float2* in, float2* out, int nrows, int ncols, int s
 static int dft_transpose_dev(const float* in, float* out, int nrows, int ncols, bool cplx, cudaStream_t s)
 {
     if (nrows == 0 || ncols == 0) return WCT_OK;
+    int rc0 = dft_check_transpose(nrows, ncols);
+    if (rc0) return rc0;
     const size_t bytes = (cplx ? sizeof(float2) : sizeof(float)) * (size_t)nrows * ncols;
     AsyncBuf t;
     t.s = s;
@@ -1551,6 +1706,37 @@ int wct_pir_create(const wct_fr_plane* fr, int nshort, const int* short_len, con
     catch (std::exception& e) {
         return fail(WCT_ERR_CONFIG, e.what());
     }
+}
+
+int wct_pir_set_long_responses(wct_pir* p, int nlong, const int* long_len, const double* long_wave,
+                               double long_padding)
+{
+    if (!p || nlong < 0 || (nlong && (!long_len || !long_wave)) || long_padding < 0)
+        return fail(WCT_ERR_ARG, "wct_pir_set_long_responses: bad arguments");
+    std::vector<std::vector<double>> longs;
+    size_t off = 0;
+    for (int i = 0; i < nlong; ++i) {
+        if (long_len[i] < 0) return fail(WCT_ERR_ARG, "wct_pir_set_long_responses: negative length");
+        longs.emplace_back(long_wave + off, long_wave + off + long_len[i]);
+        off += long_len[i];
+    }
+    set_long_responses(p->pir, longs, long_padding);
+    return WCT_OK;
+}
+
+int wct_pir_long_info(const wct_pir* p, int* nsamples, int* pad)
+{
+    if (!p) return fail(WCT_ERR_ARG, "wct_pir_long_info: null pir");
+    if (nsamples) *nsamples = (int)p->pir.long_wf.size();
+    if (pad) *pad = p->pir.long_pad;
+    return WCT_OK;
+}
+
+int wct_pir_long_waveform(const wct_pir* p, float* out)
+{
+    if (!p || (!out && !p->pir.long_wf.empty())) return fail(WCT_ERR_ARG, "wct_pir_long_waveform: bad arguments");
+    std::copy(p->pir.long_wf.begin(), p->pir.long_wf.end(), out);
+    return WCT_OK;
 }
 
 int wct_pir_closest(const wct_pir* p, double relpitch, int* path)
@@ -1803,8 +1989,22 @@ int wct_dt_set_response_pir(wct_depotransform* h, int face, int plane, const wct
                       table.begin() + ((size_t)i * (2 * npad + 1) + j) * ns);
         }
     }
-    return wct_dt_set_response_table(h, face, plane, G, npad, ns, pir.pitch, pir.impact, pir.waveform_pad,
-                                      table.data());
+    int rc = wct_dt_set_response_table(h, face, plane, G, npad, ns, pir.pitch, pir.impact, pir.waveform_pad,
+                                        table.data());
+    if (rc) return rc;
+    return wct_dt_set_long_response(h, face, plane, (int)pir.long_wf.size(), pir.long_wf.data(), pir.long_pad);
+}
+
+int wct_dt_set_long_response(wct_depotransform* h, int face, int plane, int nsamples, const float* wave, int pad)
+{
+    PlaneState* ps = find_plane(h, face, plane);
+    if (!ps || nsamples < 0 || (nsamples && !wave) || pad < 0)
+        return fail(WCT_ERR_ARG, "wct_dt_set_long_response: bad arguments");
+    std::lock_guard<std::mutex> lk(h->core.mtx);
+    ps->long_wf.assign(wave, wave + nsamples);
+    ps->long_pad = pad;
+    ps->long_nfft = 0;  // spectrum rebuilt at the next use
+    return WCT_OK;
 }
 
 int wct_dt_frame_shape(const wct_depotransform* h, int* nrows, int* nticks)

@@ -82,11 +82,15 @@ __global__ void k_bluestein_b(const float2* __restrict__ chirp, float2* __restri
     }
 }
 
-// out[c][r] = in[r][c] for an nrows x ncols input (32 x 32 tiles).
+// out[c][r] = in[r][c] for an nrows x ncols input (32 x 32 tiles); a batch
+// of matrices along blockIdx.z, each nrows * ncols elements apart.
 template <typename T>
 __global__ void k_transpose(const T* __restrict__ in, T* __restrict__ out, int nrows, int ncols)
 {
     __shared__ T tile[32][33];
+    const size_t boff = (size_t)blockIdx.z * nrows * ncols;
+    in += boff;
+    out += boff;
     const int c0 = blockIdx.x * 32, r0 = blockIdx.y * 32;
     for (int k = threadIdx.y; k < 32; k += blockDim.y) {
         const int r = r0 + k, c = c0 + threadIdx.x;
@@ -97,6 +101,136 @@ __global__ void k_transpose(const T* __restrict__ in, T* __restrict__ out, int n
         const int c = c0 + k, r = r0 + threadIdx.x;
         if (r < nrows && c < ncols) out[(size_t)c * nrows + r] = tile[threadIdx.x][k];
     }
+}
+
+// Real rows (n values, row stride ld) packed two per complex row of length
+// nfft: Z[p][k] = rows[2p][k] + i rows[2p+1][k] for k < n, zero beyond.
+__global__ void k_pack_rows(const float* __restrict__ rows, long ld, int nrows, int n, float2* __restrict__ Z,
+                            int nfft)
+{
+    const int p = blockIdx.y;
+    const float* r0 = rows + (size_t)(2 * p) * ld;
+    const bool has1 = 2 * p + 1 < nrows;
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < nfft; k += gridDim.x * blockDim.x) {
+        float2 v = make_float2(0.f, 0.f);
+        if (k < n) v = make_float2(r0[k], has1 ? r0[ld + k] : 0.f);
+        Z[(size_t)p * nfft + k] = v;
+    }
+}
+
+// The inverse of k_pack_rows for the first n values of each row.
+__global__ void k_unpack_rows(const float2* __restrict__ Z, int nfft, float* __restrict__ rows, long ld, int nrows,
+                              int n)
+{
+    const int p = blockIdx.y;
+    float* r0 = rows + (size_t)(2 * p) * ld;
+    const bool has1 = 2 * p + 1 < nrows;
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+        const float2 v = Z[(size_t)p * nfft + k];
+        r0[k] = v.x;
+        if (has1) r0[ld + k] = v.y;
+    }
+}
+
+// Z[p][k] *= L[k] (or conj(L[k])).
+__global__ void k_cmul_rows(float2* __restrict__ Z, int nfft, const float2* __restrict__ L, int conj)
+{
+    const int p = blockIdx.y;
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < nfft; k += gridDim.x * blockDim.x) {
+        float2 l = L[k];
+        if (conj) l.y = -l.y;
+        Z[(size_t)p * nfft + k] = cmul(Z[(size_t)p * nfft + k], l);
+    }
+}
+
+void launch_pack_rows(const float* rows, long ld, int nrows, int n, float2* Z, int nfft, cudaStream_t s)
+{
+    if (nrows <= 0) return;
+    const dim3 grid(std::min((nfft + 255) / 256, 64), (nrows + 1) / 2);
+    k_pack_rows<<<grid, 256, 0, s>>>(rows, ld, nrows, n, Z, nfft);
+}
+
+void launch_unpack_rows(const float2* Z, int nfft, float* rows, long ld, int nrows, int n, cudaStream_t s)
+{
+    if (nrows <= 0) return;
+    const dim3 grid(std::min((n + 255) / 256, 64), (nrows + 1) / 2);
+    k_unpack_rows<<<grid, 256, 0, s>>>(Z, nfft, rows, ld, nrows, n);
+}
+
+void launch_cmul_rows(float2* Z, int nfft, int nz, const float2* L, bool conj, cudaStream_t s)
+{
+    if (nz <= 0) return;
+    const dim3 grid(std::min((nfft + 255) / 256, 64), nz);
+    k_cmul_rows<<<grid, 256, 0, s>>>(Z, nfft, L, conj ? 1 : 0);
+}
+
+// Four-step FFT twiddles: Z[b][n2][k1] *= exp(sign 2 pi i n2 k1 / (N1 N2)),
+// the phase reduced in integers and evaluated in double precision.
+__global__ void k_twiddle4(float2* __restrict__ Z, long long count, int N1, int N2, int sign)
+{
+    const long long N = (long long)N1 * N2;
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < count;
+         e += (long long)gridDim.x * blockDim.x) {
+        const long long in_b = e % N;
+        const int n2 = (int)(in_b / N1), k1 = (int)(in_b - (long long)n2 * N1);
+        const long long q = ((long long)n2 * k1) % N;
+        double sn, cs;
+        sincospi(2.0 * (double)q / (double)N, &sn, &cs);
+        const float2 w = make_float2((float)cs, (float)(sign * sn));
+        Z[e] = cmul(Z[e], w);
+    }
+}
+
+// Bluestein in global memory (lengths whose FFT exceeds shared memory):
+// Z[r][m] = x_m c_m (conjugated input for the inverse) for m < N, 0 up to P;
+// then out[r][k] = scale * c_k Z[r][k] (conjugated for the inverse).
+__global__ void k_blue_pre(const float2* __restrict__ in, long ld_in, float2* __restrict__ Z, int N, int P,
+                           const float2* __restrict__ chirp, int inv)
+{
+    const int r = blockIdx.y;
+    for (int m = blockIdx.x * blockDim.x + threadIdx.x; m < P; m += gridDim.x * blockDim.x) {
+        float2 v = make_float2(0.f, 0.f);
+        if (m < N) {
+            float2 x = in[(size_t)r * ld_in + m];
+            if (inv) x.y = -x.y;
+            v = cmul(x, chirp[m]);
+        }
+        Z[(size_t)r * P + m] = v;
+    }
+}
+
+__global__ void k_blue_post(const float2* __restrict__ Z, int P, float2* __restrict__ out, long ld_out, int N,
+                            const float2* __restrict__ chirp, int inv, float scale)
+{
+    const int r = blockIdx.y;
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < N; k += gridDim.x * blockDim.x) {
+        float2 v = cmul(Z[(size_t)r * P + k], chirp[k]);
+        if (inv) v.y = -v.y;
+        out[(size_t)r * ld_out + k] = make_float2(v.x * scale, v.y * scale);
+    }
+}
+
+void launch_twiddle4(float2* Z, long long count, int N1, int N2, int sign, cudaStream_t s)
+{
+    if (count <= 0) return;
+    const long long blocks = std::min<long long>((count + 255) / 256, 148LL * 16);
+    k_twiddle4<<<(unsigned)blocks, 256, 0, s>>>(Z, count, N1, N2, sign);
+}
+
+void launch_blue_pre(const float2* in, long ld_in, float2* Z, int nrows, int N, int P, const float2* chirp, bool inv,
+                     cudaStream_t s)
+{
+    if (nrows <= 0) return;
+    const dim3 grid(std::min((P + 255) / 256, 64), nrows);
+    k_blue_pre<<<grid, 256, 0, s>>>(in, ld_in, Z, N, P, chirp, inv ? 1 : 0);
+}
+
+void launch_blue_post(const float2* Z, int P, float2* out, long ld_out, int nrows, int N, const float2* chirp,
+                      bool inv, float scale, cudaStream_t s)
+{
+    if (nrows <= 0) return;
+    const dim3 grid(std::min((N + 255) / 256, 64), nrows);
+    k_blue_post<<<grid, 256, 0, s>>>(Z, P, out, ld_out, N, chirp, inv ? 1 : 0, scale);
 }
 
 static int dft_threads(int M) { return M >= 2048 ? 512 : 256; }
@@ -140,10 +274,10 @@ void launch_bluestein_b(const float2* chirp, float2* b, int N, int P, cudaStream
     k_bluestein_b<<<std::min((P + 255) / 256, 1024), 256, 0, s>>>(chirp, b, N, P);
 }
 
-void launch_transpose_c(const float2* in, float2* out, int nrows, int ncols, cudaStream_t s)
+void launch_transpose_c(const float2* in, float2* out, int nrows, int ncols, cudaStream_t s, int batch)
 {
-    if (nrows <= 0 || ncols <= 0) return;
-    const dim3 grid((ncols + 31) / 32, (nrows + 31) / 32), block(32, 8);
+    if (nrows <= 0 || ncols <= 0 || batch <= 0) return;
+    const dim3 grid((ncols + 31) / 32, (nrows + 31) / 32, batch), block(32, 8);
     k_transpose<float2><<<grid, block, 0, s>>>(in, out, nrows, ncols);
 }
 

@@ -268,8 +268,23 @@ void launch_c2c_rows(const float2* in, long ld_in, float2* out, long ld_out, int
 void launch_bluestein_rows(const float2* in, long ld_in, float2* out, long ld_out, int nrows, int N, const FftDesc& dP,
                            const float2* chirp, const float2* bhat, int sign, float scale, cudaStream_t s);
 void launch_bluestein_b(const float2* chirp, float2* b, int N, int P, cudaStream_t s);
-void launch_transpose_c(const float2* in, float2* out, int nrows, int ncols, cudaStream_t s);
+// batch: that many nrows x ncols matrices back to back (at most 65535)
+void launch_transpose_c(const float2* in, float2* out, int nrows, int ncols, cudaStream_t s, int batch = 1);
+// Four-step FFT twiddles on count elements of [b][n2][k1] blocks (N1 x N2 = N):
+// times exp(sign 2 pi i n2 k1 / N).
+void launch_twiddle4(float2* Z, long long count, int N1, int N2, int sign, cudaStream_t s);
+// Bluestein through global memory: chirp-multiplied, zero-padded rows of
+// length P, and the chirp-multiplied first N values back (scaled).
+void launch_blue_pre(const float2* in, long ld_in, float2* Z, int nrows, int N, int P, const float2* chirp, bool inv,
+                     cudaStream_t s);
+void launch_blue_post(const float2* Z, int P, float2* out, long ld_out, int nrows, int N, const float2* chirp,
+                      bool inv, float scale, cudaStream_t s);
 void launch_transpose_r(const float* in, float* out, int nrows, int ncols, cudaStream_t s);
+// Real rows packed two per complex row of length nfft (zero padded beyond n),
+// the unpacking of the first n values, and a product with one spectrum.
+void launch_pack_rows(const float* rows, long ld, int nrows, int n, float2* Z, int nfft, cudaStream_t s);
+void launch_unpack_rows(const float2* Z, int nfft, float* rows, long ld, int nrows, int n, cudaStream_t s);
+void launch_cmul_rows(float2* Z, int nfft, int nz, const float2* L, bool conj, cudaStream_t s);
 void launch_twiddles(float2* tw, float2* twh, int M, cudaStream_t s);
 
 // ---- batched-path launchers (kernels.cu) ----

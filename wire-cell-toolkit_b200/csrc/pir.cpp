@@ -55,6 +55,7 @@ Pir build_pir(int npaths, int nsamples, const double* pitchpos, const double* cu
     if (npaths < n_per || npaths % n_per) throw std::runtime_error("field response must hold 6 paths per wire");
     Pir p;
     p.nticks = nticks;
+    p.tick = tick;
     p.waveform_pad = (int)(overall_short_padding / tick);
     const size_t n_short = fft_best_length((size_t)(overall_short_padding / tick), false);
     p.n_short = (int)n_short;
@@ -109,6 +110,31 @@ Pir build_pir(int npaths, int nsamples, const double* pitchpos, const double* cu
         p.bywire.push_back(idx);
     }
     return p;
+}
+
+void set_long_responses(Pir& p, const std::vector<std::vector<double>>& longs, double long_padding)
+{
+    p.long_wf.clear();
+    p.long_pad = 0;
+    if (longs.empty()) return;
+    const size_t n = fft_best_length((size_t)p.nticks, false);
+    std::vector<double> acc(n, 0.0);
+    acc[0] = 1.0;
+    for (const auto& lw : longs) {
+        std::vector<double> w(n, 0.0);
+        for (size_t i = 0; i < std::min(n, lw.size()); ++i) w[i] = lw[i];
+        std::vector<double> out(n, 0.0);
+        for (size_t a = 0; a < n; ++a) {
+            if (acc[a] == 0.0) continue;
+            for (size_t b = 0; b < n; ++b) {
+                if (w[b] == 0.0) continue;
+                out[(a + b) % n] += acc[a] * w[b];
+            }
+        }
+        acc.swap(out);
+    }
+    p.long_wf.assign(acc.begin(), acc.end());
+    p.long_pad = (int)(long_padding / p.tick);
 }
 
 }  // namespace wctb200

@@ -23,6 +23,11 @@ struct Pir {
     int nticks{0};
     int waveform_pad{0};
     int n_short{0};
+    double tick{0};
+    // long-range response (IImpactResponse::long_aux_waveform and
+    // long_aux_waveform_pad, PlaneImpactResponse.cxx:121-150,252); empty: none
+    std::vector<float> long_wf;
+    int long_pad{0};
 
     int nwires() const { return (int)bywire.size(); }
     int nimp_per_wire() const { return bywire.empty() ? 0 : (int)bywire[0].size(); }
@@ -40,5 +45,12 @@ struct Pir {
 Pir build_pir(int npaths, int nsamples, const double* pitchpos, const double* current, double fr_pitch,
               double tstart, double period, const std::vector<std::vector<double>>& shorts,
               double overall_short_padding, double tick, int nticks);
+
+// The long-range response of PlaneImpactResponse::build_responses
+// (:121-150): the circular convolution, at length fft_best_length(nticks),
+// of the long responses (each cut or zero padded to that length; the
+// reference multiplies their single-precision spectra), computed directly in
+// double precision; long_pad = long_padding / tick.  No responses: none.
+void set_long_responses(Pir& p, const std::vector<std::vector<double>>& longs, double long_padding);
 
 }  // namespace wctb200
