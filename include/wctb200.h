@@ -184,6 +184,49 @@ int wct_dft_1b_device(const float* in, float* out, int nrows, int ncols, int axi
 int wct_dft_2d_device(const float* in, float* out, int nrows, int ncols, int inverse, void* stream);
 int wct_dft_transpose_device(const float* in, float* out, int nrows, int ncols, int is_complex, void* stream);
 
+/* ---- Noise (gen/src/AddNoise.cxx, IFrameFilter) ---- */
+
+/* IncoherentAddNoise / CoherentAddNoise (gen/src/AddNoise.cxx:44-160) with
+ * the waveform of GeneratorN (aux/src/NoiseTools.cxx: sigma_k = S_k *
+ * sqrt(2/3.141592); bins 0 .. N/2 drawn as sigma_k (n_k, n_{k+N/2}), DC and
+ * Nyquist by modulus, Hermitian, inverse DFT with 1/N) added to each frame
+ * row's first min(N, ncols) samples.  Row r uses spectrum row_spec[r] of
+ * spectra [nspectra][nspec] (the model's channel_spectrum or group_spectrum;
+ * -1: the row gets no noise) and the random stream row_stream[r]: the
+ * channel number for incoherent noise, the group id for coherent noise (so
+ * every channel of a group gets the same waveform).  Normals are
+ * counter-based (key: seed, ident = frame ident; counter: stream, model,
+ * normal index), so a frame's noise is reproducible and independent of the
+ * launch; the reference's generator (std::mt19937 with recycled normals) is
+ * matched in distribution, not in values.  nspec even with a 7-smooth half
+ * up to 14336.  Device version on the current device and stream; host
+ * version on host arrays (frame updated in place). */
+int wct_add_noise_device(float* frame, long ld, int nrows, int ncols, const float* spectra, int nspec,
+                         const int* row_spec, const int* row_stream, unsigned long long seed, int ident, int model,
+                         void* stream);
+int wct_add_noise(float* frame, int nrows, int ncols, const float* spectra, int nspectra, int nspec,
+                  const int* row_spec, const int* row_stream, unsigned long long seed, int ident, int model);
+
+/* ---- Digitizer (gen/src/Digitizer.cxx, IFrameFilter) ---- */
+
+/* Digitizer's per-sample arithmetic (gen/src/Digitizer.cxx:82-141) on a
+ * dense frame: voltage = gain * value + row_baseline[row] (the baseline of
+ * the row's plane, a float as the reference reads it), then ADC = 0 at or
+ * below fs_lo, 2^resolution - 1 at or above fs_hi, otherwise
+ * (voltage - fs_lo) / (fs_hi - fs_lo) * (2^resolution - 1), rounded (half
+ * away from zero) when round_adc, else floored; in double precision, bit
+ * for bit the reference's values.  The reference emits these for the
+ * channels and tick range of its input traces; the dense result holds them
+ * at the same rows and ticks.  Configuration keys map as resolution,
+ * gain, fullscale = [fs_lo, fs_hi], baselines (per plane), round.
+ * Device version: frame and adc (may be the same array) and row_baseline on
+ * the current device, enqueued on stream; host version: host arrays. */
+int wct_digitize_device(const float* frame, long ld_in, int nrows, int ncols, const float* row_baseline, double gain,
+                        double fs_lo, double fs_hi, int resolution, int round_adc, float* adc, long ld_out,
+                        void* stream);
+int wct_digitize(const float* frame, int nrows, int ncols, const float* row_baseline, double gain, double fs_lo,
+                 double fs_hi, int resolution, int round_adc, float* adc);
+
 /* ---- DepoTransform (gen/src/DepoTransform.cxx, IDepoFramer) ---- */
 
 /* DepoTransform::configure (gen/src/DepoTransform.cxx:76-113) from JSON with

@@ -376,3 +376,45 @@ def cround(x):
 def drift_fn(cfg, depos):
     o = drift(cfg, depos)
     return o[:, :7]
+
+
+def digitize(frame, row_baseline, gain=1.0, fullscale=(0.0, 2.0e-6), resolution=12, round_adc=False):
+    """Gen::Digitizer's per-sample arithmetic (gen/src/Digitizer.cxx:82-141)
+    in float64, vectorised: voltage = gain * value + baseline (a float32, as
+    the reference reads m_baselines into a float), then digitize (:82-97):
+    0 at or below fullscale[0], 2^resolution - 1 at or above fullscale[1],
+    otherwise (v - fs0) / (fs1 - fs0) * max, rounded half away from zero
+    (C round; the values are positive here) or floored; returned as float32."""
+    f = np.asarray(frame, dtype=np.float32).astype(np.float64)
+    base = np.asarray(row_baseline, dtype=np.float32).astype(np.float64)[:, None]
+    maxv = float((1 << resolution) - 1)
+    v = gain * f + base
+    with np.errstate(invalid="ignore"):
+        fp = ((v - fullscale[0]) / (fullscale[1] - fullscale[0])) * maxv
+        fl = np.floor(fp)
+        adc = fl + ((fp - fl) >= 0.5) if round_adc else fl
+    adc = np.where(v <= fullscale[0], 0.0, np.where(v >= fullscale[1], maxv, adc))
+    return adc.astype(np.float32)
+
+
+def noise_wave(spectrum, normals):
+    """One noise waveform as IncoherentAddNoise makes it
+    (gen/src/AddNoise.cxx:79-84 and aux/src/NoiseTools.cxx GeneratorN::spec,
+    ::wave), float64: sigma_k = S_k * sqrt(2 / 3.141592); for k <= N/2 +
+    (N even) the bin is sigma_k (n_k, n_{k + N/2}); DC and (N even) Nyquist
+    become their modulus; the spectrum is made Hermitian and inverted with
+    1/N.  ``normals`` holds at least 2 (N/2 + (N even)) + 1 standard normals."""
+    S = np.asarray(spectrum, dtype=np.float64)
+    n = S.size
+    nextra = (n + 1) % 2
+    nhalf = n // 2
+    sig = S * np.sqrt(2.0 / 3.141592)
+    spec = np.zeros(n, dtype=np.complex128)
+    for ind in range(min(nhalf + nextra, n - 1) + 1):
+        spec[ind] = sig[ind] * complex(normals[ind], normals[ind + nhalf])
+    spec[0] = abs(spec[0])
+    if nextra:
+        spec[nhalf] = abs(spec[nhalf])
+    for k in range(1, (n + 1) // 2):  # Hermitian mirror
+        spec[n - k] = np.conj(spec[k])
+    return np.real(np.fft.ifft(spec))

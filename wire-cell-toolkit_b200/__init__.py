@@ -73,6 +73,14 @@ SIGNATURES = {
     "wct_pir_long_waveform": (C.c_int, [C.c_void_p, C.c_void_p]),
     "wct_convolve_rows_device": (C.c_int, [C.c_void_p, C.c_long, C.c_int, C.c_int, C.c_void_p, C.c_int, C.c_int,
                                            C.c_void_p, C.c_long, C.c_int, C.c_void_p]),
+    "wct_add_noise_device": (C.c_int, [C.c_void_p, C.c_long, C.c_int, C.c_int, C.c_void_p, C.c_int, C.c_void_p,
+                                       C.c_void_p, C.c_ulonglong, C.c_int, C.c_int, C.c_void_p]),
+    "wct_add_noise": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_void_p,
+                                C.c_ulonglong, C.c_int, C.c_int]),
+    "wct_digitize_device": (C.c_int, [C.c_void_p, C.c_long, C.c_int, C.c_int, C.c_void_p, C.c_double, C.c_double,
+                                      C.c_double, C.c_int, C.c_int, C.c_void_p, C.c_long, C.c_void_p]),
+    "wct_digitize": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_double, C.c_double, C.c_double, C.c_int,
+                               C.c_int, C.c_void_p]),
     "wct_dft_fwd1d": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int]),
     "wct_dft_inv1d": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int]),
     "wct_dft_fwd1b": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int]),
@@ -224,6 +232,55 @@ def convolve_rows(d_in, ld_in, nrows, n_in, d_resp, n_resp, d_out, ld_out, n_out
     """Batched FFT convolution of device rows with one response (pointers as ints)."""
     _check(lib().wct_convolve_rows_device(C.c_void_p(d_in), ld_in, nrows, n_in, C.c_void_p(d_resp), n_resp, nfft,
                                           C.c_void_p(d_out), ld_out, n_out, C.c_void_p(stream) if stream else None))
+
+
+def add_noise(frame, spectra, row_spec, row_stream, seed=0, ident=0, model=0):
+    """IncoherentAddNoise / CoherentAddNoise on a host frame [nrows][ncols]
+    float32 (updated in place and returned): spectra [nspectra][nspec]
+    amplitude spectra, row_spec[r] the spectrum of row r (-1: none),
+    row_stream[r] its random stream (channel number, or group id for
+    coherent noise)."""
+    f = frame if (isinstance(frame, np.ndarray) and frame.dtype == np.float32 and frame.flags.c_contiguous) \
+        else np.ascontiguousarray(frame, dtype=np.float32)
+    sp = np.ascontiguousarray(spectra, dtype=np.float32)
+    rs = np.ascontiguousarray(row_spec, dtype=np.int32)
+    rt = np.ascontiguousarray(row_stream, dtype=np.int32)
+    _check(lib().wct_add_noise(f.ctypes.data, f.shape[0], f.shape[1], sp.ctypes.data, sp.shape[0], sp.shape[1],
+                               rs.ctypes.data, rt.ctypes.data, int(seed), int(ident), int(model)))
+    return f
+
+
+class Digitizer:
+    """Gen::Digitizer (gen/src/Digitizer.cxx) on a dense frame: configuration
+    keys resolution, gain, fullscale, baselines (per plane), round with the
+    reference's defaults; ``rows_per_plane`` gives the frame's row count of
+    each plane in order (the DepoTransform frame layout)."""
+
+    VOLT = 1.0e-6  # the toolkit's system of units (WireCellUtil/Units.h)
+
+    def __init__(self, rows_per_plane, resolution=12, gain=1.0, fullscale=(0.0, 2.0 * VOLT), baselines=None,
+                 round=False):
+        # reference defaults: 12 bits, gain 1, 0 .. 2 V, baselines 900, 900, 200 mV
+        self.rows_per_plane = list(rows_per_plane)
+        if baselines is None:
+            baselines = [0.9 * self.VOLT, 0.9 * self.VOLT, 0.2 * self.VOLT][:len(self.rows_per_plane)]
+        self.resolution, self.gain, self.fullscale, self.round = int(resolution), float(gain), fullscale, bool(round)
+        self.row_baseline = np.concatenate([np.full(n, b, dtype=np.float32)
+                                            for n, b in zip(self.rows_per_plane, baselines)])
+
+    def __call__(self, frame, out=None):
+        f = np.ascontiguousarray(frame, dtype=np.float32)
+        out = np.empty_like(f) if out is None else out
+        _check(lib().wct_digitize(f.ctypes.data, f.shape[0], f.shape[1], self.row_baseline.ctypes.data, self.gain,
+                                  self.fullscale[0], self.fullscale[1], self.resolution, int(self.round),
+                                  out.ctypes.data))
+        return out
+
+    def device(self, d_frame, ld_in, nrows, ncols, d_row_baseline, d_adc, ld_out, stream=None):
+        _check(lib().wct_digitize_device(C.c_void_p(d_frame), ld_in, nrows, ncols, C.c_void_p(d_row_baseline),
+                                         self.gain, self.fullscale[0], self.fullscale[1], self.resolution,
+                                         int(self.round), C.c_void_p(d_adc), ld_out,
+                                         C.c_void_p(stream) if stream else None))
 
 
 class IDFT:

@@ -2387,4 +2387,117 @@ int wct_dft_transpose_device(const float* in, float* out, int nrows, int ncols, 
     return dft_transpose_dev(in, out, nrows, ncols, is_complex != 0, (cudaStream_t)stream);
 }
 
+/* ---- Noise ---- */
+
+static int noise_args(const void* frame, int nrows, int ncols, const void* spectra, int nspec, const void* row_spec,
+                      const void* row_stream, FftDesc& d)
+{
+    if (!frame || !spectra || !row_spec || !row_stream || nrows < 0 || ncols < 0 || nspec <= 0)
+        return fail(WCT_ERR_ARG, "add noise: bad arguments");
+    if (nspec % 2 || nspec / 2 > kDftMaxFft || !dft_smooth(nspec / 2))
+        return fail(WCT_ERR_SIZE, "add noise: the spectrum length must be even with a 7-smooth half up to 14336");
+    return device_plan(nspec / 2, d);
+}
+
+int wct_add_noise_device(float* frame, long ld, int nrows, int ncols, const float* spectra, int nspec,
+                         const int* row_spec, const int* row_stream, unsigned long long seed, int ident, int model,
+                         void* stream)
+{
+    FftDesc d;
+    int rc = noise_args(frame, nrows, ncols, spectra, nspec, row_spec, row_stream, d);
+    if (rc) return rc;
+    if (ld < ncols) return fail(WCT_ERR_ARG, "add noise: row stride below the row length");
+    const unsigned k0 = (unsigned)(seed & 0xffffffffull);
+    const unsigned k1 = (unsigned)(seed >> 32) + 0x9E3779B9u * (unsigned)ident;
+    launch_add_noise(frame, ld, nrows, ncols, spectra, nspec, row_spec, row_stream, k0, k1, (unsigned)model, d,
+                     (cudaStream_t)stream);
+    CUDA_TRY(cudaGetLastError());
+    return WCT_OK;
+}
+
+int wct_add_noise(float* frame, int nrows, int ncols, const float* spectra, int nspectra, int nspec,
+                  const int* row_spec, const int* row_stream, unsigned long long seed, int ident, int model)
+{
+    FftDesc d;
+    int rc = noise_args(frame, nrows, ncols, spectra, nspec, row_spec, row_stream, d);
+    if (rc) return rc;
+    if (nspectra < 0) return fail(WCT_ERR_ARG, "add noise: bad arguments");
+    for (int r = 0; r < nrows; ++r)
+        if (row_spec[r] >= nspectra) return fail(WCT_ERR_ARG, "add noise: spectrum index out of range");
+    if (!nrows || !ncols) return WCT_OK;
+    cudaStream_t s = cudaStreamPerThread;
+    const size_t fb = sizeof(float) * (size_t)nrows * ncols;
+    const size_t sb = sizeof(float) * (size_t)std::max(nspectra, 1) * nspec;
+    {
+        AsyncBuf f, sp, rs, rt;
+        f.s = sp.s = rs.s = rt.s = s;
+        CUDA_TRY(cudaMallocAsync(&f.p, fb, s));
+        CUDA_TRY(cudaMallocAsync(&sp.p, sb, s));
+        CUDA_TRY(cudaMallocAsync(&rs.p, sizeof(int) * (size_t)nrows, s));
+        CUDA_TRY(cudaMallocAsync(&rt.p, sizeof(int) * (size_t)nrows, s));
+        CUDA_TRY(cudaMemcpyAsync(f.p, frame, fb, cudaMemcpyHostToDevice, s));
+        if (nspectra)
+            CUDA_TRY(cudaMemcpyAsync(sp.p, spectra, sizeof(float) * (size_t)nspectra * nspec, cudaMemcpyHostToDevice,
+                                     s));
+        CUDA_TRY(cudaMemcpyAsync(rs.p, row_spec, sizeof(int) * (size_t)nrows, cudaMemcpyHostToDevice, s));
+        CUDA_TRY(cudaMemcpyAsync(rt.p, row_stream, sizeof(int) * (size_t)nrows, cudaMemcpyHostToDevice, s));
+        rc = wct_add_noise_device(static_cast<float*>(f.p), ncols, nrows, ncols, static_cast<const float*>(sp.p),
+                                  nspec, static_cast<const int*>(rs.p), static_cast<const int*>(rt.p), seed, ident,
+                                  model, s);
+        if (rc) return rc;
+        CUDA_TRY(cudaMemcpyAsync(frame, f.p, fb, cudaMemcpyDeviceToHost, s));
+    }
+    CUDA_TRY(cudaStreamSynchronize(s));
+    return WCT_OK;
+}
+
+/* ---- Digitizer ---- */
+
+static int digitize_args(const void* in, int nrows, int ncols, const void* base, double fs_lo, double fs_hi,
+                         int resolution, const void* out)
+{
+    if (!in || !out || !base || nrows < 0 || ncols < 0) return fail(WCT_ERR_ARG, "digitize: bad arguments");
+    if (resolution < 1 || resolution > 30) return fail(WCT_ERR_ARG, "digitize: resolution must be 1..30 bits");
+    if (!(fs_hi > fs_lo)) return fail(WCT_ERR_ARG, "digitize: fullscale[1] must exceed fullscale[0]");
+    return WCT_OK;
+}
+
+int wct_digitize_device(const float* frame, long ld_in, int nrows, int ncols, const float* row_baseline, double gain,
+                        double fs_lo, double fs_hi, int resolution, int round_adc, float* adc, long ld_out,
+                        void* stream)
+{
+    int rc = digitize_args(frame, nrows, ncols, row_baseline, fs_lo, fs_hi, resolution, adc);
+    if (rc) return rc;
+    if (ld_in < ncols || ld_out < ncols) return fail(WCT_ERR_ARG, "digitize: row stride below the row length");
+    launch_digitize(frame, ld_in, adc, ld_out, nrows, ncols, row_baseline, gain, fs_lo, fs_hi, resolution,
+                    round_adc != 0, (cudaStream_t)stream);
+    CUDA_TRY(cudaGetLastError());
+    return WCT_OK;
+}
+
+int wct_digitize(const float* frame, int nrows, int ncols, const float* row_baseline, double gain, double fs_lo,
+                 double fs_hi, int resolution, int round_adc, float* adc)
+{
+    int rc = digitize_args(frame, nrows, ncols, row_baseline, fs_lo, fs_hi, resolution, adc);
+    if (rc) return rc;
+    if (!nrows || !ncols) return WCT_OK;
+    cudaStream_t s = cudaStreamPerThread;
+    const size_t bytes = sizeof(float) * (size_t)nrows * ncols;
+    {
+        AsyncBuf d, b;
+        d.s = b.s = s;
+        CUDA_TRY(cudaMallocAsync(&d.p, bytes, s));
+        CUDA_TRY(cudaMallocAsync(&b.p, sizeof(float) * (size_t)nrows, s));
+        CUDA_TRY(cudaMemcpyAsync(d.p, frame, bytes, cudaMemcpyHostToDevice, s));
+        CUDA_TRY(cudaMemcpyAsync(b.p, row_baseline, sizeof(float) * (size_t)nrows, cudaMemcpyHostToDevice, s));
+        float* dp = static_cast<float*>(d.p);
+        launch_digitize(dp, ncols, dp, ncols, nrows, ncols, static_cast<const float*>(b.p), gain, fs_lo, fs_hi,
+                        resolution, round_adc != 0, s);
+        CUDA_TRY(cudaGetLastError());
+        CUDA_TRY(cudaMemcpyAsync(adc, d.p, bytes, cudaMemcpyDeviceToHost, s));
+    }
+    CUDA_TRY(cudaStreamSynchronize(s));
+    return WCT_OK;
+}
+
 }  // extern "C"

@@ -14,6 +14,7 @@
 #include <algorithm>
 
 #include "kernels.cuh"
+#include "rng.cuh"
 
 namespace wctb200 {
 
@@ -286,6 +287,126 @@ void launch_transpose_r(const float* in, float* out, int nrows, int ncols, cudaS
     if (nrows <= 0 || ncols <= 0) return;
     const dim3 grid((ncols + 31) / 32, (nrows + 31) / 32), block(32, 8);
     k_transpose<float><<<grid, block, 0, s>>>(in, out, nrows, ncols);
+}
+
+// ---------------------------------------------------------------------------
+// Digitizer (gen/src/Digitizer.cxx:82-141): per sample, voltage = gain * value
+// + baseline of the row's plane (a float, as the reference reads it), then
+// Digitizer::digitize (:82-97): 0 at or below fullscale[0], 2^resolution - 1
+// at or above fullscale[1], otherwise (v - fs0) / (fs1 - fs0) * max rounded
+// (half away from zero) or floored.  Double arithmetic with explicit
+// rounding (no fused multiply-add), as the reference computes it on the CPU.
+// ---------------------------------------------------------------------------
+__global__ void k_digitize(const float* __restrict__ in, long ld_in, float* __restrict__ out, long ld_out, int nrows,
+                           int ncols, const float* __restrict__ row_baseline, double gain, double fs0, double fs1,
+                           int resolution, int rnd)
+{
+    const int r = blockIdx.y;
+    if (r >= nrows) return;
+    const double maxv = (double)((1 << resolution) - 1);
+    const double base = (double)row_baseline[r];
+    const double span = __dsub_rn(fs1, fs0);
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < ncols; c += gridDim.x * blockDim.x) {
+        const double v = __dadd_rn(__dmul_rn(gain, (double)in[(size_t)r * ld_in + c]), base);
+        double adc;
+        if (v <= fs0) adc = 0.0;
+        else if (v >= fs1) adc = maxv;
+        else {
+            const double fp = __dmul_rn(__ddiv_rn(__dsub_rn(v, fs0), span), maxv);
+            adc = rnd ? round(fp) : floor(fp);
+        }
+        out[(size_t)r * ld_out + c] = (float)adc;
+    }
+}
+
+void launch_digitize(const float* in, long ld_in, float* out, long ld_out, int nrows, int ncols,
+                     const float* row_baseline, double gain, double fs0, double fs1, int resolution, bool rnd,
+                     cudaStream_t s)
+{
+    if (nrows <= 0 || ncols <= 0) return;
+    const dim3 grid(std::min((ncols + 255) / 256, 32), nrows);
+    k_digitize<<<grid, 256, 0, s>>>(in, ld_in, out, ld_out, nrows, ncols, row_baseline, gain, fs0, fs1, resolution,
+                                    rnd ? 1 : 0);
+}
+
+// ---------------------------------------------------------------------------
+// Noise (gen/src/AddNoise.cxx:44-100 IncoherentAddNoise, :102-160
+// CoherentAddNoise; the waveform of aux/src/NoiseTools.cxx GeneratorN::spec
+// and ::wave): for a channel spectrum S of N bins, sigma_k = S_k *
+// sqrt(2 / 3.141592) (the reference's constant), bins 0 .. N/2 get
+// sigma_k (n_k, n_{k + N/2}) from one list of normals n (the two index
+// ranges overlap as in the reference), DC and Nyquist take their modulus,
+// the spectrum is made Hermitian and transformed back (1/N): the noise
+// waveform, added to the row's first min(N, ncols) samples.  Normals come
+// from a counter-based stream per row: the channel's (incoherent) or the
+// group's (coherent, so every channel of a group gets the same waveform).
+// One row per block; N even, N/2 a supported FFT length.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ float noise_normal(unsigned k0, unsigned k1, unsigned stream, unsigned model, int i)
+{
+    Philox g;
+    g.init(k0, k1, stream, model, (unsigned)i);
+    const double u1 = g.uniform(), u2 = g.uniform();
+    double sn, cs;
+    sincospi(2.0 * u2, &sn, &cs);
+    return (float)(sqrt(-2.0 * log(u1)) * cs);  // Box-Muller
+}
+
+__global__ void k_add_noise(float* frame, long ld, int ncols, const float* __restrict__ spectra, int nspec,
+                            const int* __restrict__ row_spec, const int* __restrict__ row_stream, unsigned k0,
+                            unsigned k1, unsigned model, FftDesc d)
+{
+    extern __shared__ float2 nsm[];
+    const int row = blockIdx.x;
+    const int sp = row_spec[row];
+    if (sp < 0) return;
+    const unsigned stream = (unsigned)row_stream[row];
+    const float* S = spectra + (size_t)sp * nspec;
+    const int M = d.M, N = 2 * M, nhalf = M;
+    const int tid = threadIdx.x, nth = blockDim.x;
+    const float s2opi = sqrtf(2.0f / 3.141592f);
+    float2* a = nsm;
+    float2* b = nsm + M;
+    // packed half spectrum: bin 0 = (|X_0|, |X_M|), bins 1 .. M-1 = X_k
+    for (int k = tid; k < M; k += nth) {
+        float2 v;
+        if (k == 0) {
+            const float m0 = S[0] * s2opi, mh = S[nhalf] * s2opi;
+            const float2 x0 = make_float2(m0 * noise_normal(k0, k1, stream, model, 0),
+                                          m0 * noise_normal(k0, k1, stream, model, nhalf));
+            const float2 xh = make_float2(mh * noise_normal(k0, k1, stream, model, nhalf),
+                                          mh * noise_normal(k0, k1, stream, model, 2 * nhalf));
+            v = make_float2(sqrtf(x0.x * x0.x + x0.y * x0.y), sqrtf(xh.x * xh.x + xh.y * xh.y));
+        }
+        else {
+            const float m = S[k] * s2opi;
+            v = make_float2(m * noise_normal(k0, k1, stream, model, k),
+                            m * noise_normal(k0, k1, stream, model, k + nhalf));
+        }
+        b[k] = v;
+    }
+    __syncthreads();
+    for (int k = tid; k < M; k += nth) a[k] = c2r_bin(b, k, M, d.twh);
+    __syncthreads();
+    const float2* z = fft_c2c<+1>(a, b, d, tid, nth);
+    const float sc = 1.0f / (float)M;  // with the halves of c2r_bin: the inverse's 1/N
+    float* f = frame + (size_t)row * ld;
+    for (int m = tid; m < M; m += nth) {
+        const int c0 = 2 * m;
+        if (c0 < ncols && c0 < N) f[c0] += z[m].x * sc;
+        if (c0 + 1 < ncols && c0 + 1 < N) f[c0 + 1] += z[m].y * sc;
+    }
+}
+
+void launch_add_noise(float* frame, long ld, int nrows, int ncols, const float* spectra, int nspec,
+                      const int* row_spec, const int* row_stream, unsigned k0, unsigned k1, unsigned model,
+                      const FftDesc& d, cudaStream_t s)
+{
+    if (nrows <= 0) return;
+    const size_t sm = 2 * sizeof(float2) * (size_t)d.M;
+    cudaFuncSetAttribute((const void*)k_add_noise, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    k_add_noise<<<nrows, dft_threads(d.M), sm, s>>>(frame, ld, ncols, spectra, nspec, row_spec, row_stream, k0, k1,
+                                                     model, d);
 }
 
 }  // namespace wctb200

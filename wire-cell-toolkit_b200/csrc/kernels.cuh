@@ -285,6 +285,16 @@ void launch_transpose_r(const float* in, float* out, int nrows, int ncols, cudaS
 void launch_pack_rows(const float* rows, long ld, int nrows, int n, float2* Z, int nfft, cudaStream_t s);
 void launch_unpack_rows(const float2* Z, int nfft, float* rows, long ld, int nrows, int n, cudaStream_t s);
 void launch_cmul_rows(float2* Z, int nfft, int nz, const float2* L, bool conj, cudaStream_t s);
+// Digitizer::digitize of every sample (one baseline per row, in the frame's units).
+void launch_digitize(const float* in, long ld_in, float* out, long ld_out, int nrows, int ncols,
+                     const float* row_baseline, double gain, double fs0, double fs1, int resolution, bool rnd,
+                     cudaStream_t s);
+// Noise waveforms of GeneratorN (aux/src/NoiseTools.cxx) from per-row channel
+// spectra (row_spec: spectrum index, -1 none) on random streams row_stream,
+// added to the frame rows; d: plan of length nspec / 2.
+void launch_add_noise(float* frame, long ld, int nrows, int ncols, const float* spectra, int nspec,
+                      const int* row_spec, const int* row_stream, unsigned k0, unsigned k1, unsigned model,
+                      const FftDesc& d, cudaStream_t s);
 void launch_twiddles(float2* tw, float2* twh, int M, cudaStream_t s);
 
 // ---- batched-path launchers (kernels.cu) ----
