@@ -184,6 +184,32 @@ int wct_dft_1b_device(const float* in, float* out, int nrows, int ncols, int axi
 int wct_dft_2d_device(const float* in, float* out, int nrows, int ncols, int inverse, void* stream);
 int wct_dft_transpose_device(const float* in, float* out, int nrows, int ncols, int is_complex, void* stream);
 
+/* ---- DepoFluxSplat (gen/src/DepoFluxSplat.cxx, IDepoFramer) ---- */
+
+/* DepoFluxSplat's configuration keys (gen/src/DepoFluxSplat.cxx:81-128):
+ * tick, window_start, window_duration (frame ticks = (int)(duration / tick)),
+ * nsigma, drift_speed, response_plane (depo times are shifted by
+ * response_plane / drift_speed), time_offsets (per plane, in time), and the
+ * extra smearing per plane: smear_long in ticks, smear_tran in wire pitches. */
+typedef struct {
+    double tick, window_start, window_duration, nsigma, drift_speed, response_plane;
+    double time_offsets[3], smear_long[3], smear_tran[3];
+} wct_splat_config;
+
+/* The dense truth frame of DepoFluxSplat::operator() (:247-390) for drifted
+ * depos ([n][7] t, q, x, y, z, extent_long, extent_tran, as at the response
+ * plane) over the component's faces and planes: each depo's erf-integrated
+ * Gaussian patch on (wire, tick), |charge| added; frame rows are the
+ * component's wires (as the DepoTransform frame), columns the window's ticks;
+ * samples that time_offsets move outside the window are dropped (the
+ * reference keeps them in its traces).  wct_dt_splat_shape gives the frame
+ * shape; the device version takes device depos and frame on stream (NULL:
+ * the component's stream). */
+int wct_dt_splat_shape(const wct_depotransform* dt, const wct_splat_config* cfg, int* nrows, int* nticks);
+int wct_dt_splat_device(wct_depotransform* dt, const wct_splat_config* cfg, const double* depos, size_t ndepos,
+                        float* frame, void* stream);
+int wct_dt_splat(wct_depotransform* dt, const wct_splat_config* cfg, const double* depos, size_t ndepos, float* frame);
+
 /* ---- Noise (gen/src/AddNoise.cxx, IFrameFilter) ---- */
 
 /* IncoherentAddNoise / CoherentAddNoise (gen/src/AddNoise.cxx:44-160) with

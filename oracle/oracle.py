@@ -418,3 +418,33 @@ def noise_wave(spectrum, normals):
     for k in range(1, (n + 1) // 2):  # Hermitian mirror
         spec[n - k] = np.conj(spec[k])
     return np.real(np.fft.ifft(spec))
+
+
+class OrcSplat(C.Structure):
+    _fields_ = [(n, C.c_double) for n in ("tick", "window_start", "window_duration", "nsigma", "drift_speed",
+                                          "response_plane")] + \
+        [("time_offsets", C.c_double * 3), ("smear_long", C.c_double * 3), ("smear_tran", C.c_double * 3)]
+
+
+def splat(cfg, depos, scfg):
+    """DepoFluxSplat's dense truth frame (gen/src/DepoFluxSplat.cxx:247-390) of
+    drifted depos for the planes of ``cfg`` (its face cut included):
+    [sum of nwires][nbins] float64.  ``scfg``: tick, window_start,
+    window_duration, nsigma, drift_speed, response_plane, and optional
+    3-lists time_offsets, smear_long, smear_tran."""
+    job = Job(cfg, depos, drift=False)
+    sp = OrcSplat()
+    for k in ("tick", "window_start", "window_duration", "nsigma", "drift_speed", "response_plane"):
+        setattr(sp, k, float(scfg[k]))
+    for k in ("time_offsets", "smear_long", "smear_tran"):
+        v = scfg.get(k) or [0.0, 0.0, 0.0]
+        for i in range(3):
+            getattr(sp, k)[i] = float(v[i])
+    nbins = int(scfg["window_duration"] / scfg["tick"])
+    nrows = sum(p["nwires"] for p in cfg["planes"])
+    out = np.zeros((nrows, nbins))
+    L = lib()
+    L.orc_splat.argtypes = [C.POINTER(OrcJob), C.POINTER(OrcSplat), C.c_void_p]
+    if L.orc_splat(C.byref(job.job), C.byref(sp), out.ctypes.data) != 0:
+        raise RuntimeError("orc_splat failed")
+    return out

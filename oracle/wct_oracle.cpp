@@ -1303,6 +1303,80 @@ int orc_run(const OrcJob* job, void* frame, OrcPlaneOut* pout, int* rec)
 }
 
 // Waveform::edge (util/src/Waveform.cxx:136-153) over a float row.
+// DepoFluxSplat (gen/src/DepoFluxSplat.cxx:81-135 configuration,
+// :247-390 operator()): for each depo in the face (DepoTools sensitive
+// cut here) and each plane in order, a GaussianDiffusion with time
+// t + response_plane / drift_speed, time sigma extent_long (smeared by
+// smear_long ticks) / speed and pitch sigma extent_tran (smeared by
+// smear_tran wire pitches), sampled on the window's tick binning and the
+// plane's wire (region) binning; a depo whose time span misses the window
+// skips the plane, one whose pitch span misses the wire plane skips the
+// remaining planes (the reference's `break`).  |patch| is added at
+// tick (int)(toffset + time_offset / tick) + k.  Dense accumulation in
+// double; frame [sum of nwires][nbins], nbins = (int)(window_duration / tick).
+struct OrcSplat {
+    double tick, window_start, window_duration, nsigma, drift_speed, response_plane;
+    double time_offsets[3], smear_long[3], smear_tran[3];
+};
+
+int orc_splat(const OrcJob* job, const OrcSplat* sp, double* frame)
+{
+    try {
+        const int nbins = (int)(sp->window_duration / sp->tick);
+        orc::Binning tb(nbins, sp->window_start, sp->window_start + nbins * sp->tick);
+        std::vector<size_t> row0(job->nplanes + 1, 0);
+        for (int p = 0; p < job->nplanes; ++p) row0[p + 1] = row0[p] + job->planes[p].nwires;
+        std::fill(frame, frame + row0[job->nplanes] * (size_t)nbins, 0.0);
+        for (int i = 0; i < job->ndepos; ++i) {
+            const double* q = job->depos + 7 * (size_t)i;
+            orc::Depo d{q[0], q[1], q[2], q[3], q[4], q[5], q[6], i};
+            if (job->have_bb && !orc::bb_inside(job->bb_lo, job->bb_hi, d)) continue;
+            const double nominal = d.t + sp->response_plane / sp->drift_speed;
+            for (int ip = 0; ip < job->nplanes && ip < 3; ++ip) {
+                const OrcPlane& pl = job->planes[ip];
+                double sigma_L = d.el;
+                if (sp->smear_long[ip] > 0) {
+                    const double extra = sp->smear_long[ip] * tb.binsize * sp->drift_speed;
+                    sigma_L = std::sqrt(sigma_L * sigma_L + extra * extra);
+                }
+                orc::GausDesc td{nominal, sigma_L / sp->drift_speed};
+                const double eff_t = d.el > 0 ? sp->nsigma : 0;
+                if (td.distance(tb.minv) > eff_t || td.distance(tb.maxv) < -eff_t) continue;
+                orc::Pimpos pim(pl.nwires, pl.pitchmin, pl.pitchmax, orc::V3{pl.wire[0], pl.wire[1], pl.wire[2]},
+                                orc::V3{pl.pitch[0], pl.pitch[1], pl.pitch[2]},
+                                orc::V3{pl.origin[0], pl.origin[1], pl.origin[2]}, pl.nimp);
+                const orc::Binning& wb = pim.region;
+                double sigma_T = d.et;
+                if (sp->smear_tran[ip] > 0) {
+                    const double extra = sp->smear_tran[ip] * wb.binsize;
+                    sigma_T = std::sqrt(sigma_T * sigma_T + extra * extra);
+                }
+                orc::GausDesc pd{pim.distance(orc::V3{d.x, d.y, d.z}), sigma_T};
+                const double eff_p = d.et > 0 ? sp->nsigma : 0;
+                if (pd.distance(wb.minv) > eff_p || pd.distance(wb.maxv) < -eff_p) break;
+                orc::Patch<float> patch;
+                orc::set_sampling(d, td, pd, tb, wb, sp->nsigma, patch);
+                if (!patch.np || !patch.nt) continue;
+                const int tstart = (int)(patch.toffset + sp->time_offsets[ip] / sp->tick);
+                for (int a = 0; a < patch.np; ++a) {
+                    const int pbin = patch.poffset + a;
+                    if (pbin < 0 || pbin >= pl.nwires) continue;
+                    for (int k = 0; k < patch.nt; ++k) {
+                        const int tick = tstart + k;
+                        if (tick < 0 || tick >= nbins) continue;
+                        frame[(row0[ip] + pbin) * (size_t)nbins + tick] +=
+                            std::abs(patch.val[(size_t)a * patch.nt + k]);
+                    }
+                }
+            }
+        }
+        return 0;
+    }
+    catch (...) {
+        return -1;
+    }
+}
+
 void orc_edge(const float* wave, int size, int* out)
 {
     int imin = size, imax = size;

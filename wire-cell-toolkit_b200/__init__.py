@@ -49,6 +49,23 @@ class FrPlane(C.Structure):
     ]
 
 
+class SplatConfig(C.Structure):
+    """wct_splat_config: DepoFluxSplat's configuration keys (gen/src/DepoFluxSplat.cxx:81-128)."""
+    _fields_ = [(n, C.c_double) for n in ("tick", "window_start", "window_duration", "nsigma", "drift_speed",
+                                          "response_plane")] + \
+        [("time_offsets", C.c_double * 3), ("smear_long", C.c_double * 3), ("smear_tran", C.c_double * 3)]
+
+    @classmethod
+    def make(cls, tick=500.0, window_start=0.0, window_duration=8096 * 500.0, nsigma=3.0, drift_speed=1.6e-3,
+             response_plane=100.0, time_offsets=None, smear_long=None, smear_tran=None):
+        c = cls(tick, window_start, window_duration, nsigma, drift_speed, response_plane)
+        for name, v in (("time_offsets", time_offsets), ("smear_long", smear_long), ("smear_tran", smear_tran)):
+            v = v or [0.0, 0.0, 0.0]
+            for i in range(3):
+                getattr(c, name)[i] = float(v[i])
+        return c
+
+
 class PlaneWindow(C.Structure):
     _fields_ = [(n, C.c_int) for n in (
         "face", "plane", "start_ch", "end_ch", "start_tick", "end_tick", "nw_fft", "nt_fft", "nt_gpu",
@@ -73,6 +90,9 @@ SIGNATURES = {
     "wct_pir_long_waveform": (C.c_int, [C.c_void_p, C.c_void_p]),
     "wct_convolve_rows_device": (C.c_int, [C.c_void_p, C.c_long, C.c_int, C.c_int, C.c_void_p, C.c_int, C.c_int,
                                            C.c_void_p, C.c_long, C.c_int, C.c_void_p]),
+    "wct_dt_splat_shape": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
+    "wct_dt_splat_device": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_size_t, C.c_void_p, C.c_void_p]),
+    "wct_dt_splat": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_size_t, C.c_void_p]),
     "wct_add_noise_device": (C.c_int, [C.c_void_p, C.c_long, C.c_int, C.c_int, C.c_void_p, C.c_int, C.c_void_p,
                                        C.c_void_p, C.c_ulonglong, C.c_int, C.c_int, C.c_void_p]),
     "wct_add_noise": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_void_p,
@@ -460,6 +480,18 @@ class DepoTransform:
                                            C.c_void_p(d_grad_depos_ptr),
                                            C.c_void_p(d_grad_drift_ptr) if d_grad_drift_ptr else None,
                                            _dt_stream(stream)))
+
+    def splat(self, depos, **cfg):
+        """DepoFluxSplat truth frame [nrows][ticks] float32 of drifted depos
+        (keys as SplatConfig.make: tick, window_start, window_duration, nsigma,
+        drift_speed, response_plane, time_offsets, smear_long, smear_tran)."""
+        sc = SplatConfig.make(**cfg)
+        nr, nt = C.c_int(), C.c_int()
+        _check(lib().wct_dt_splat_shape(self.h, C.byref(sc), C.byref(nr), C.byref(nt)))
+        d = np.ascontiguousarray(depos, dtype=np.float64).reshape(-1, 7)
+        out = np.zeros((nr.value, nt.value), dtype=np.float32)
+        _check(lib().wct_dt_splat(self.h, C.byref(sc), d.ctypes.data if len(d) else None, len(d), out.ctypes.data))
+        return out
 
     def forward_batch(self, events, out=None):
         """Host-buffer batch: ``events`` is a list of [n_e][7] depo arrays.  Returns

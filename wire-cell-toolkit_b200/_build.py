@@ -6,7 +6,7 @@ import subprocess
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libwctb200.so")
-SOURCES = ["kernels.cu", "adjoint.cu", "dft.cu", "capi.cu", "pir.cpp"]
+SOURCES = ["kernels.cu", "adjoint.cu", "dft.cu", "splat.cu", "capi.cu", "pir.cpp"]
 HEADERS = ["common.cuh", "fft.cuh", "gauss.cuh", "kernels.cuh", "rng.cuh", "fft_lengths.h", "json.hpp", "pir.hpp"]
 
 NVCC_FLAGS = [

@@ -185,6 +185,7 @@ struct Core {
     // workspace
     DevBuf d_rec, d_win, d_Q, d_V, d_depos, d_frame, d_wcnt, d_woff, d_wcur, d_wlist, d_tprof, d_kbound;
     DevBuf d_long_z, d_glong;  // long-range step: packed row spectra; adjoint's frame-gradient rows
+    DevBuf d_splat;            // DepoFluxSplat accumulator (doubles)
     DevBuf d_gframe, d_gdep, d_gglob;  // adjoint host entry point
     DevBuf d_fq, d_fluc;               // fluctuation: drifted charges, per (plane, depo) draw sums
     DevBuf d_pool, d_pool_off, d_pool_used;  // time profiles of long patches
@@ -2496,6 +2497,106 @@ int wct_digitize(const float* frame, int nrows, int ncols, const float* row_base
         CUDA_TRY(cudaGetLastError());
         CUDA_TRY(cudaMemcpyAsync(adc, d.p, bytes, cudaMemcpyDeviceToHost, s));
     }
+    CUDA_TRY(cudaStreamSynchronize(s));
+    return WCT_OK;
+}
+
+/* ---- DepoFluxSplat ---- */
+
+static int splat_setup(const wct_depotransform* h, const wct_splat_config* cfg, SplatParams& sp, int& nrows)
+{
+    if (!h || !cfg) return fail(WCT_ERR_ARG, "splat: bad arguments");
+    if (!(cfg->tick > 0) || !(cfg->window_duration >= 0) || !(cfg->drift_speed > 0) || !(cfg->nsigma >= 0))
+        return fail(WCT_ERR_CONFIG, "splat: tick and drift_speed must be positive, window_duration and nsigma not negative");
+    sp = SplatParams{};
+    const int nbins = (int)(cfg->window_duration / cfg->tick);
+    sp.tb.nbins = nbins;
+    sp.tb.tmin = cfg->window_start;
+    sp.tb.tmax = cfg->window_start + nbins * cfg->tick;
+    sp.tb.bs = (sp.tb.tmax - sp.tb.tmin) / nbins;
+    sp.nsigma = cfg->nsigma;
+    sp.speed = cfg->drift_speed;
+    sp.time_shift = cfg->response_plane / cfg->drift_speed;
+    for (int k = 0; k < 3; ++k) {
+        sp.pl[k].smear_long = cfg->smear_long[k];
+        sp.pl[k].smear_tran = cfg->smear_tran[k];
+        sp.pl[k].tick_offset = cfg->time_offsets[k] / cfg->tick;
+    }
+    nrows = h->core.nrows();
+    return WCT_OK;
+}
+
+int wct_dt_splat_shape(const wct_depotransform* h, const wct_splat_config* cfg, int* nrows, int* nticks)
+{
+    SplatParams sp;
+    int nr = 0;
+    int rc = splat_setup(h, cfg, sp, nr);
+    if (rc) return rc;
+    if (nrows) *nrows = nr;
+    if (nticks) *nticks = sp.tb.nbins;
+    return WCT_OK;
+}
+
+int wct_dt_splat_device(wct_depotransform* h, const wct_splat_config* cfg, const double* d_depos, size_t ndepos,
+                        float* d_frame, void* stream)
+{
+    SplatParams sp;
+    int nrows = 0;
+    int rc = splat_setup(h, cfg, sp, nrows);
+    if (rc) return rc;
+    if (!d_frame || (ndepos && !d_depos)) return fail(WCT_ERR_ARG, "splat: bad arguments");
+    if (ndepos > (size_t)0x7fffffff) return fail(WCT_ERR_SIZE, "splat: more than 2^31 - 1 depos");
+    std::lock_guard<std::mutex> lk(h->core.mtx);
+    Core& c = h->core;
+    CUDA_TRY(cudaSetDevice(c.device));
+    cudaStream_t s = stream ? (cudaStream_t)stream : c.own_stream;
+    const long long count = (long long)nrows * sp.tb.nbins;
+    if (count <= 0) return WCT_OK;
+    CUDA_TRY(c.d_splat.ensure(sizeof(double) * (size_t)count));
+    CUDA_TRY(cudaMemsetAsync(c.d_splat.p, 0, sizeof(double) * (size_t)count, s));
+    for (const FaceState& f : c.faces) {
+        PlaneSet ps{};
+        ps.nplanes = std::min((int)f.planes.size(), kMaxPlanes);
+        for (int k = 0; k < ps.nplanes; ++k) {
+            const PlaneState& pl = *c.planes[f.planes[k]];
+            ps.p[k] = pl.dev;
+            ps.p[k].wire_base = pl.row0;
+            ps.nwires_total += pl.desc.nwires;
+        }
+        SplatParams fsp = sp;
+        for (int k = 3; k < kMaxPlanes; ++k) fsp.pl[k] = SplatPlane{};
+        launch_splat_face(d_depos, (int)ndepos, ps, fsp, c.d_splat.as<double>(), s);
+    }
+    launch_splat_finish(c.d_splat.as<double>(), d_frame, count, s);
+    CUDA_TRY(cudaGetLastError());
+    return WCT_OK;
+}
+
+int wct_dt_splat(wct_depotransform* h, const wct_splat_config* cfg, const double* depos, size_t ndepos, float* frame)
+{
+    SplatParams sp;
+    int nrows = 0;
+    int rc = splat_setup(h, cfg, sp, nrows);
+    if (rc) return rc;
+    if (!frame || (ndepos && !depos)) return fail(WCT_ERR_ARG, "splat: bad arguments");
+    const size_t fbytes = sizeof(float) * (size_t)nrows * sp.tb.nbins;
+    if (!fbytes) return WCT_OK;
+    cudaStream_t s = nullptr;
+    {
+        std::lock_guard<std::mutex> lk(h->core.mtx);
+        CUDA_TRY(cudaSetDevice(h->core.device));
+        s = h->core.own_stream;
+    }
+    AsyncBuf dd, df;
+    dd.s = df.s = s;
+    if (ndepos) {
+        CUDA_TRY(cudaMallocAsync(&dd.p, sizeof(double) * 7 * ndepos, s));
+        CUDA_TRY(cudaMemcpyAsync(dd.p, depos, sizeof(double) * 7 * ndepos, cudaMemcpyHostToDevice, s));
+    }
+    CUDA_TRY(cudaMallocAsync(&df.p, fbytes, s));
+    rc = wct_dt_splat_device(h, cfg, static_cast<const double*>(dd.p), ndepos, static_cast<float*>(df.p), s);
+    if (rc) return rc;
+    CUDA_TRY(cudaMemcpyAsync(frame, df.p, fbytes, cudaMemcpyDeviceToHost, s));
     CUDA_TRY(cudaStreamSynchronize(s));
     return WCT_OK;
 }

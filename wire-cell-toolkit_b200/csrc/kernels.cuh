@@ -285,6 +285,23 @@ void launch_transpose_r(const float* in, float* out, int nrows, int ncols, cudaS
 void launch_pack_rows(const float* rows, long ld, int nrows, int n, float2* Z, int nfft, cudaStream_t s);
 void launch_unpack_rows(const float2* Z, int nfft, float* rows, long ld, int nrows, int n, cudaStream_t s);
 void launch_cmul_rows(float2* Z, int nfft, int nz, const float2* L, bool conj, cudaStream_t s);
+// DepoFluxSplat (splat.cu): per plane the smear (ticks, wire pitches) and the
+// time offset in ticks; the window binning, nsigma, drift speed and the time
+// shift response_plane / drift_speed.
+struct SplatPlane {
+    double smear_long, smear_tran, tick_offset;
+};
+struct SplatParams {
+    TimeDev tb;
+    double nsigma, speed, time_shift;
+    SplatPlane pl[kMaxPlanes];
+};
+// The planes of one face (wire_base = frame row of each plane's first wire)
+// added into acc [rows][tb.nbins] doubles (zeroed by the caller); then the
+// float frame from acc.
+void launch_splat_face(const double* depos, int n, const PlaneSet& ps, const SplatParams& sp, double* acc,
+                       cudaStream_t s);
+void launch_splat_finish(const double* acc, float* frame, long long count, cudaStream_t s);
 // Digitizer::digitize of every sample (one baseline per row, in the frame's units).
 void launch_digitize(const float* in, long ld_in, float* out, long ld_out, int nrows, int ncols,
                      const float* row_baseline, double gain, double fs0, double fs1, int resolution, bool rnd,
