@@ -1,0 +1,83 @@
+"""EmpiricalNoiseModel's channel spectra (gen/src/EmpiricalNoiseModel.cxx):
+frequency grid, resampling (sqrt(L / n) scale, clamped linear
+interpolation), wire-length interpolation and clamping, gain scaling, the
+constant added in quadrature, and the spectra handed to add_noise."""
+
+import importlib
+
+import numpy as np
+import pytest
+
+noise = importlib.import_module("wire-cell-toolkit_b200.noise")
+CM = 10.0
+US = 1000.0
+
+
+def _entries(nsamples=256, period=0.5 * US, lengths=(100 * CM, 300 * CM, 600 * CM)):
+    out = []
+    freqs = np.linspace(0.0, 1.0 / (2 * period), 65)  # up to Nyquist
+    for k, wl in enumerate(lengths):
+        out.append(dict(plane=0, gain=14.0, shaping=2.0 * US, wirelen=wl, const=0.01 * (k + 1), nsamples=nsamples,
+                        period=period, freqs=list(freqs), amps=list(1.0 + (k + 1) * freqs * period)))
+    return out
+
+
+def test_grid_and_resampling(wct):
+    ents = _entries()
+    m = noise.EmpiricalNoiseModel(ents, nsamples=6000, period=0.5 * US)
+    L = wct.fft_best_length(6000)
+    assert m.L == L and m.freq.size == L
+    assert m.freq[1] == pytest.approx(1.0 / (L * 0.5 * US)) and m.freq[L - 1] == m.freq[1]
+    # the entries' amplitudes are linear in frequency: resampling keeps the line, times sqrt(L / 256)
+    s = np.sqrt(L / 256.0)
+    k = 0
+    want = s * (1.0 + (k + 1) * np.minimum(m.freq, 1.0 / (2 * 0.5 * US)) * 0.5 * US)
+    np.testing.assert_allclose(m.planes[0][0]["amps"], want, rtol=2e-6)
+    assert m.planes[0][0]["const"] == pytest.approx(0.01 * s)
+
+
+def test_no_resampling_at_the_model_grid(wct):
+    L = wct.fft_best_length(6000)
+    ents = _entries(nsamples=L)
+    ents[0]["amps"] = list(np.arange(L, dtype=np.float64))  # kept as is
+    ents[0]["freqs"] = list(np.arange(L, dtype=np.float64))
+    for e in ents[1:]:
+        e["amps"], e["freqs"] = list(np.ones(L)), list(np.arange(L, dtype=np.float64))
+    m = noise.EmpiricalNoiseModel(ents, nsamples=6000, period=0.5 * US)
+    assert np.array_equal(m.planes[0][0]["amps"], np.arange(L, dtype=np.float32))
+
+
+def test_wire_length_interpolation_and_channel_spectrum():
+    m = noise.EmpiricalNoiseModel(_entries(), nsamples=6000, period=0.5 * US)
+    a, b = m.planes[0][0], m.planes[0][1]
+    c, amp = m.interpolate_wire_length(0, 200 * CM)  # halfway between 100 and 300 cm
+    np.testing.assert_allclose(amp, 0.5 * (a["amps"] + b["amps"]), rtol=1e-6)
+    assert c == pytest.approx(0.5 * (a["const"] + b["const"]))
+    c0, amp0 = m.interpolate_wire_length(0, 10 * CM)    # clamped at the shortest
+    assert c0 == a["const"] and np.array_equal(amp0, a["amps"])
+    s = m.channel_spectrum(0, 200.7 * CM)              # 200.7 cm rounds down to 200 cm steps
+    np.testing.assert_allclose(s, np.sqrt(amp * amp + c * c), rtol=1e-6)
+    sg = m.channel_spectrum(0, 200 * CM, gain=28.0)    # twice the spectra's gain
+    np.testing.assert_allclose(sg, np.sqrt((2 * amp) ** 2 + c * c), rtol=1e-6)
+    assert np.array_equal(m.channel_spectrum(0, 200 * CM, gain=14.05), s)  # within 1%: unchanged
+
+
+def test_frame_spectra_groups_rows():
+    m = noise.EmpiricalNoiseModel(_entries(), nsamples=6000, period=0.5 * US)
+    spectra, row_spec = m.frame_spectra([0, 0, 0, 0], [150 * CM, 150.4 * CM, 400 * CM, 150 * CM])
+    assert spectra.shape == (2, m.L) and list(row_spec) == [0, 0, 1, 0]
+
+
+@pytest.mark.gpu
+def test_model_noise_power(wct):
+    """add_noise with the model's spectrum: mean power per bin 2 sigma_k^2."""
+    m = noise.EmpiricalNoiseModel(_entries(), nsamples=6000, period=0.5 * US)
+    rows = 1500
+    spectra, row_spec = m.frame_spectra([0] * rows, [250 * CM] * rows)
+    if m.L % 2:
+        pytest.skip("odd model length")
+    frame = np.zeros((rows, m.L), np.float32)
+    wct.add_noise(frame, spectra, row_spec, np.arange(rows, dtype=np.int32), seed=3)
+    P = (np.abs(np.fft.fft(frame.astype(np.float64), axis=1)) ** 2).mean(axis=0)
+    sig2 = 2.0 * (spectra[0].astype(np.float64) * np.sqrt(2.0 / 3.141592)) ** 2
+    assert abs((P[: m.L // 2 + 1] / sig2[: m.L // 2 + 1]).mean() - 1.0) < 0.01

@@ -90,6 +90,7 @@ SIGNATURES = {
     "wct_pir_long_waveform": (C.c_int, [C.c_void_p, C.c_void_p]),
     "wct_convolve_rows_device": (C.c_int, [C.c_void_p, C.c_long, C.c_int, C.c_int, C.c_void_p, C.c_int, C.c_int,
                                            C.c_void_p, C.c_long, C.c_int, C.c_void_p]),
+    "wct_fft_best_length": (C.c_long, [C.c_long, C.c_int]),
     "wct_dt_splat_shape": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
     "wct_dt_splat_device": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_size_t, C.c_void_p, C.c_void_p]),
     "wct_dt_splat": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_size_t, C.c_void_p]),
@@ -252,6 +253,11 @@ def convolve_rows(d_in, ld_in, nrows, n_in, d_resp, n_resp, d_out, ld_out, n_out
     """Batched FFT convolution of device rows with one response (pointers as ints)."""
     _check(lib().wct_convolve_rows_device(C.c_void_p(d_in), ld_in, nrows, n_in, C.c_void_p(d_resp), n_resp, nfft,
                                           C.c_void_p(d_out), ld_out, n_out, C.c_void_p(stream) if stream else None))
+
+
+def fft_best_length(n, keep_odd_even=False):
+    """util/src/FFTBestLength.cxx: smallest fast FFT length >= n of the reference's tables."""
+    return int(lib().wct_fft_best_length(int(n), 1 if keep_odd_even else 0))
 
 
 def add_noise(frame, spectra, row_spec, row_stream, seed=0, ident=0, model=0):

@@ -1740,6 +1740,12 @@ int wct_pir_long_waveform(const wct_pir* p, float* out)
     return WCT_OK;
 }
 
+long wct_fft_best_length(long n, int keep_odd_even)
+{
+    if (n <= 0) return 0;
+    return (long)fft_best_length((size_t)n, keep_odd_even != 0);
+}
+
 int wct_pir_closest(const wct_pir* p, double relpitch, int* path)
 {
     if (!p || !path) return fail(WCT_ERR_ARG, "wct_pir_closest: bad arguments");

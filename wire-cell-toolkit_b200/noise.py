@@ -1,0 +1,107 @@
+"""Channel noise spectra of the empirical noise model, for ``add_noise``.
+
+EmpiricalNoiseModel (gen/src/EmpiricalNoiseModel.cxx) holds measured
+amplitude spectra per plane at several wire lengths (its "spectra_file":
+entries with plane, gain, shaping, wirelen, const, nsamples, period, freqs,
+amps).  At configuration (:96-175) every entry is resampled onto the model's
+frequency grid of L = fft_best_length(nsamples) bins (:58-70: bin i holds
+i / (L period) up to L/2, mirrored above), its amplitudes and constant scaled
+by sqrt(L / entry nsamples), by linear interpolation between the entry's
+frequencies (clamped at both ends).  A channel's spectrum (:250-330) is the
+linear interpolation between the plane's entries bracketing the channel's
+total wire length (rounded down to wire_length_scale steps; clamped at the
+shortest and longest), scaled by the channel's gain over the entries' gain
+when they differ by more than 1%, and combined with the interpolated
+constant as sqrt(amp^2 + const^2).  The shaping-time correction, which
+needs the channel-status component and the cold-electronics response, is
+not restated here.
+"""
+
+import numpy as np
+
+from . import fft_best_length
+
+CM = 10.0  # the toolkit's length unit is the mm
+
+
+class EmpiricalNoiseModel:
+    def __init__(self, spectra, nsamples, period, wire_length_scale=1.0 * CM):
+        self.nsamples = int(nsamples)
+        self.period = float(period)
+        self.wlres = float(wire_length_scale)
+        self.L = fft_best_length(self.nsamples)
+        L = self.L
+        i = np.arange(L)
+        self.freq = np.where(i <= L / 2.0, i / (L * 1.0) / self.period, (L - i) / (L * 1.0) / self.period)
+        self.planes = {}
+        for e in spectra:  # file order: by wire length within a plane
+            ent = dict(plane=int(e["plane"]), gain=float(np.float32(e["gain"])),
+                       shaping=float(np.float32(e["shaping"])), wirelen=float(np.float32(e["wirelen"])),
+                       const=float(e.get("const", 0.0)), nsamples=int(e["nsamples"]),
+                       period=float(np.float32(e["period"])),
+                       freqs=np.asarray(e["freqs"], dtype=np.float32).astype(np.float64),
+                       amps=np.asarray(e["amps"], dtype=np.float32).astype(np.float64))
+            self._resample(ent)
+            self.planes.setdefault(ent["plane"], []).append(ent)
+
+    def _resample(self, s):
+        """EmpiricalNoiseModel::resample (:96-136)."""
+        if s["nsamples"] == self.L and s["period"] == self.period:
+            return
+        scale = np.sqrt(self.L / (s["nsamples"] * 1.0))
+        s["const"] *= scale
+        amps = (s["amps"] * scale).astype(np.float32).astype(np.float64)  # amplitude_t holds floats
+        fr = s["freqs"]
+        out = np.empty(self.L)
+        for i, f in enumerate(self.freq):
+            if f <= fr[0]:
+                lo, hi, mu = 0, 1, 0.0
+            elif f >= fr[-1]:
+                lo, hi, mu = len(fr) - 2, len(fr) - 1, 1.0
+            else:
+                lo = int(np.searchsorted(fr, f, side="left")) - 1  # last j with f > fr[j]
+                hi = lo + 1
+                mu = (f - fr[lo]) / (fr[hi] - fr[lo])
+            out[i] = (1 - mu) * amps[lo] + mu * amps[hi]
+        s["amps"] = out.astype(np.float32).astype(np.float64)
+
+    def interpolate_wire_length(self, plane, wire_length):
+        """(constant, amplitudes) at a wire length (:175-210)."""
+        sp = self.planes[plane]
+        if wire_length <= sp[0]["wirelen"]:
+            return sp[0]["const"], sp[0]["amps"].copy()
+        if wire_length >= sp[-1]["wirelen"]:
+            return sp[-1]["const"], sp[-1]["amps"].copy()
+        for k in range(1, len(sp)):
+            hi = sp[k]
+            if hi["wirelen"] < wire_length:
+                continue
+            lo = sp[k - 1]
+            mu = (wire_length - lo["wirelen"]) / (hi["wirelen"] - lo["wirelen"])
+            amp = (lo["amps"] * (1 - mu) + hi["amps"] * mu).astype(np.float32).astype(np.float64)
+            return lo["const"] * (1 - mu) + hi["const"] * mu, amp
+        raise ValueError("EmpiricalNoiseModel: data corruption")
+
+    def channel_spectrum(self, plane, wire_length, gain=None):
+        """The amplitude spectrum (L float32 values) of a channel of ``plane``
+        whose wires total ``wire_length``; ``gain``: the channel's preamplifier
+        gain when it deviates from the spectra's."""
+        ilen = int(wire_length / self.wlres)
+        const, amp = self.interpolate_wire_length(plane, ilen * self.wlres)
+        db_gain = self.planes[plane][0]["gain"]
+        if gain is not None and abs(gain - db_gain) > 0.01 * gain:
+            amp = (amp * (gain / db_gain)).astype(np.float32).astype(np.float64)
+        return np.sqrt(amp * amp + const * const).astype(np.float32)
+
+    def frame_spectra(self, row_plane, row_wire_length, row_gain=None):
+        """Spectra for ``add_noise``: (spectra [k][L] float32, row_spec [rows])
+        with one spectrum per distinct (plane, length step, gain) of the rows."""
+        keys, spectra, row_spec = {}, [], np.empty(len(row_plane), dtype=np.int32)
+        for r, (p, wl) in enumerate(zip(row_plane, row_wire_length)):
+            g = None if row_gain is None else float(row_gain[r])
+            key = (int(p), int(wl / self.wlres), g)
+            if key not in keys:
+                keys[key] = len(spectra)
+                spectra.append(self.channel_spectrum(int(p), wl, g))
+            row_spec[r] = keys[key]
+        return np.stack(spectra) if spectra else np.zeros((0, self.L), np.float32), row_spec
