@@ -177,6 +177,40 @@ def test_device_api_matches_host_api(wct, synth):
     assert rel_l2(fd.cpu().numpy(), fh) < 1e-6
 
 
+@pytest.mark.parametrize("case", ["apa", "one_plane_empty", "long_response"])
+def test_host_frame_fully_written(wct, synth, case):
+    """The host forward downloads each plane's zero rest early and its
+    written block after the plane: every element of the caller's buffer is
+    set (a NaN-filled buffer), and bit for bit the device frame."""
+    import torch
+    cfg = synth.apa_config(nticks=6000)
+    d = synth.apa_depos(seed=6)[:40000]
+    if case == "one_plane_empty":  # a 10-wire second plane that no depo reaches: its rows hold no window
+        planes = list(cfg["planes"])
+        planes[1] = synth._plane(10, 4.67 * synth.mm, -35.7, 1, 800, synth.RESPONSE_X)
+        cfg = dict(cfg, planes=planes)
+        d = d.copy()
+        d[:, 3] = -2500.0  # its pitch coordinate is then above 500 mm, beyond the 10 wires
+    if case == "long_response":
+        k = -0.004 * np.exp(-np.arange(3000) / 400.0)
+        k[0] = 1.0
+        cfg = dict(cfg, long_responses=[k], long_padding=100e3)
+    dt = wct.from_config(cfg)
+    nrows, nticks = dt.frame_shape()
+    out = np.full((nrows, nticks), np.nan, dtype=np.float32)
+    fh, _, _ = dt(d, out=out)
+    assert not np.isnan(fh).any()
+    dd = torch.from_numpy(np.ascontiguousarray(d)).cuda()
+    fd = torch.empty((nrows, nticks), dtype=torch.float32, device="cuda")
+    dt.forward_device(dd.data_ptr(), len(d), fd.data_ptr(), torch.cuda.current_stream().cuda_stream)
+    torch.cuda.synchronize()
+    assert np.array_equal(fd.cpu().numpy(), fh)
+    empty = synth.apa_depos(seed=6)[:0]
+    out2 = np.full((nrows, nticks), np.nan, dtype=np.float32)
+    f0, _, _ = dt(empty, out=out2)
+    assert np.all(f0 == 0)
+
+
 def test_traces_follow_waveform_edge(wct, oracle, synth):
     """Trace assembly (gen/src/DepoTransform.cxx:193-208): every non-zero wire
     becomes one trace spanning its first..last non-zero tick."""

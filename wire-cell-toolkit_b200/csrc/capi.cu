@@ -616,10 +616,19 @@ static int long_conv_rows(Core& c, PlaneState& ps, float* rows, long ld, int nro
     return WCT_OK;
 }
 
+// The part of a plane's frame rows that the forward writes (plane rows
+// [rlo, rhi), ticks [tlo, thi)); the rest of the plane stays zero.
+struct FrameRegion {
+    int rlo{0}, rhi{0}, tlo{0}, thi{0};
+};
+
 // plane_done (optional, one event per plane): recorded on s once the plane's
-// frame rows are final, so a caller can download them while later planes run.
+// frame rows are final, so a caller can download them while later planes run;
+// zeroed (optional): recorded once the frame is cleared; regions (optional):
+// each plane's written block, so the zero rest can go first.
 static int forward_device(Core& c, const double* d_depos, size_t ndepos, float* d_frame, wct_plane_window* wins,
-                          int* frame_ident, cudaStream_t s, cudaEvent_t* plane_done = nullptr)
+                          int* frame_ident, cudaStream_t s, cudaEvent_t* plane_done = nullptr,
+                          cudaEvent_t zeroed = nullptr, std::vector<FrameRegion>* regions = nullptr)
 {
     EventPlan ev;
     int prc = prepare_event(c, d_depos, ndepos, s, ev);
@@ -630,6 +639,8 @@ static int forward_device(Core& c, const double* d_depos, size_t ndepos, float* 
     const std::vector<PlaneWindow>& pw = ev.pw;
     CUDA_TRY(c.d_wlist.ensure(sizeof(Visit) * std::max(total_visits, 1)));
     CUDA_TRY(cudaMemsetAsync(d_frame, 0, sizeof(float) * (size_t)c.nrows() * nticks, s));
+    if (zeroed) CUDA_TRY(cudaEventRecord(zeroed, s));
+    if (regions) regions->assign(np, FrameRegion{});
 
     // time profiles of the long patches: exactly the room counted by the prep kernel
     // (int offsets: beyond 2^31 - 2 ticks the rest is computed in the raster)
@@ -708,6 +719,14 @@ static int forward_device(Core& c, const double* d_depos, size_t ndepos, float* 
         if (!ps.long_wf.empty() && whi > wlo) {
             rc = long_conv_rows(c, ps, d_frame + ((size_t)ps.row0 + wlo) * nticks, nticks, whi - wlo, nticks, false, s);
             if (rc) return rc;
+        }
+        if (regions && whi > wlo) {  // what the inverse (and the long-range step) wrote
+            FrameRegion& r = (*regions)[ip];
+            r.rlo = wlo;
+            r.rhi = whi;
+            r.tlo = ps.long_wf.empty() ? std::max(0, w.start_tick) : 0;
+            r.thi = ps.long_wf.empty() ? std::min(nticks, w.start_tick + std::min(N, w.nt_ref)) : nticks;
+            if (r.thi < r.tlo) r.thi = r.tlo;
         }
         t_i.close(ps.long_wf.empty() || whi <= wlo ? 1 : 6);
         CUDA_TRY(cudaGetLastError());
@@ -2046,29 +2065,59 @@ int wct_dt_forward(wct_depotransform* h, const double* depos, size_t ndepos, flo
         CUDA_TRY(cudaMemcpyAsync(c.d_depos.p, depos, sizeof(double) * 7 * ndepos, cudaMemcpyHostToDevice, s));
     // each plane's rows go back as soon as they are final (copy stream), while
     // the next planes are still transformed
+    // the frame goes back on the copy stream in two parts: first the zero
+    // rest of every plane (as soon as the frame is cleared, while the
+    // kernels run), then each plane's written block once the plane is final
     const int np = (int)c.planes.size();
     std::vector<cudaEvent_t> done(np);
     for (auto& ev : done) ev = c.take_event();
+    cudaEvent_t zeroed = c.take_event();
+    std::vector<FrameRegion> reg;
     int rc = forward_device(c, c.d_depos.as<double>(), ndepos, c.d_frame.as<float>(), windows, frame_ident, s,
-                            done.data());
+                            done.data(), zeroed, &reg);
     if (rc == WCT_OK) {
         const int nt = c.nticks();
-        for (int ip = 0; ip < np; ++ip) {
+        const float* df = c.d_frame.as<float>();
+        const size_t rowb = sizeof(float) * (size_t)nt;
+        auto rows = [&](int r0, int r1) {  // whole rows [r0, r1) of the frame
+            if (r1 <= r0) return cudaSuccess;
+            return cudaMemcpyAsync(frame + (size_t)r0 * nt, df + (size_t)r0 * nt, rowb * (r1 - r0),
+                                   cudaMemcpyDeviceToHost, c.copy_stream);
+        };
+        auto block = [&](int r0, int r1, int t0, int t1) {  // rows [r0, r1), ticks [t0, t1)
+            if (r1 <= r0 || t1 <= t0) return cudaSuccess;
+            return cudaMemcpy2DAsync(frame + (size_t)r0 * nt + t0, rowb, df + (size_t)r0 * nt + t0, rowb,
+                                     sizeof(float) * (size_t)(t1 - t0), r1 - r0, cudaMemcpyDeviceToHost,
+                                     c.copy_stream);
+        };
+        cudaError_t e = cudaStreamWaitEvent(c.copy_stream, zeroed, 0);
+        for (int ip = 0; ip < np && e == cudaSuccess; ++ip) {
             const PlaneState& ps = *c.planes[ip];
-            const size_t off = (size_t)ps.row0 * nt, bytes = sizeof(float) * (size_t)ps.desc.nwires * nt;
-            cudaError_t e = cudaStreamWaitEvent(c.copy_stream, done[ip], 0);
-            if (e == cudaSuccess)
-                e = cudaMemcpyAsync(frame + off, c.d_frame.as<float>() + off, bytes, cudaMemcpyDeviceToHost,
-                                    c.copy_stream);
-            if (e != cudaSuccess) {
-                rc = fail(WCT_ERR_CUDA, std::string("wct_dt_forward: frame download: ") + cudaGetErrorString(e));
-                break;
+            const int base = ps.row0, nw = ps.desc.nwires;
+            const FrameRegion& r = reg[ip];
+            if (r.rhi <= r.rlo) {
+                e = rows(base, base + nw);
+                continue;
             }
+            e = rows(base, base + r.rlo);
+            if (e == cudaSuccess) e = rows(base + r.rhi, base + nw);
+            if (e == cudaSuccess) e = block(base + r.rlo, base + r.rhi, 0, r.tlo);
+            if (e == cudaSuccess) e = block(base + r.rlo, base + r.rhi, r.thi, nt);
         }
+        for (int ip = 0; ip < np && e == cudaSuccess; ++ip) {
+            const FrameRegion& r = reg[ip];
+            if (r.rhi <= r.rlo) continue;
+            const int base = c.planes[ip]->row0;
+            e = cudaStreamWaitEvent(c.copy_stream, done[ip], 0);
+            if (e == cudaSuccess) e = block(base + r.rlo, base + r.rhi, r.tlo, r.thi);
+        }
+        if (e != cudaSuccess)
+            rc = fail(WCT_ERR_CUDA, std::string("wct_dt_forward: frame download: ") + cudaGetErrorString(e));
     }
     cudaError_t e1 = cudaStreamSynchronize(c.copy_stream);
     cudaError_t e2 = cudaStreamSynchronize(s);
     for (auto& ev : done) c.event_pool.push_back(ev);
+    c.event_pool.push_back(zeroed);
     if (rc) return rc;
     if (e1 != cudaSuccess || e2 != cudaSuccess)
         return fail(WCT_ERR_CUDA, std::string("wct_dt_forward: ") + cudaGetErrorString(e1 != cudaSuccess ? e1 : e2));
