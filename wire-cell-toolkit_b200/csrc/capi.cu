@@ -444,8 +444,11 @@ static FlucParams fluc_params(const Core& c, bool fluct, int ident0, const int* 
     return fp;
 }
 
+// h_depos (optional): the depos in host memory, uploaded into d_depos here
+// in chunks on the copy stream, each chunk's prep blocks launched as soon as
+// it has arrived.
 static int prepare_event(Core& c, const double* d_depos, size_t ndepos, cudaStream_t s, EventPlan& ev,
-                         bool fluct = true)
+                         bool fluct = true, const double* h_depos = nullptr)
 {
     if (c.planes.empty()) return fail(WCT_ERR_STATE, "no planes configured");
     if ((int)c.planes.size() > kMaxPlanes) return fail(WCT_ERR_CONFIG, "too many planes for one component");
@@ -510,10 +513,34 @@ static int prepare_event(Core& c, const double* d_depos, size_t ndepos, cudaStre
         CUDA_TRY(c.d_fq.ensure(sizeof(double) * (size_t)std::max(n, 1)));
         CUDA_TRY(c.d_fluc.ensure(sizeof(FlucRec) * (size_t)np * std::max(n, 1)));
     }
-    launch_prep_all(d_depos, et, nkeys, c.drifter, c.have_drifter ? 1 : 0, pset, tb, c.drift_speed, c.nsigma,
-                    c.d_rec.as<PatchRec>(), c.d_win.as<WindowDev>(), c.d_wcnt.as<int>(), c.d_tprof.as<float>(),
-                    c.d_kbound.as<unsigned long long>(), ev.fp, ev.fp.on_patch ? c.d_fq.as<double>() : nullptr,
-                    c.d_wide.as<unsigned char>(), s);
+    auto prep = [&](int b0, int b1) {
+        launch_prep_all(d_depos, et, nkeys, c.drifter, c.have_drifter ? 1 : 0, pset, tb, c.drift_speed, c.nsigma,
+                        c.d_rec.as<PatchRec>(), c.d_win.as<WindowDev>(), c.d_wcnt.as<int>(), c.d_tprof.as<float>(),
+                        c.d_kbound.as<unsigned long long>(), ev.fp, ev.fp.on_patch ? c.d_fq.as<double>() : nullptr,
+                        c.d_wide.as<unsigned char>(), s, b0, b1);
+    };
+    if (h_depos && n > 0) {
+        // 4 chunks (whole 256-depo blocks): upload k + 1 runs while the prep of chunk k does
+        const int nb = et.blk0[1], per = (nb + 3) / 4;
+        std::vector<cudaEvent_t> up;
+        int rc = WCT_OK;
+        for (int b0 = 0; b0 < nb && rc == WCT_OK; b0 += per) {
+            const int b1 = std::min(nb, b0 + per);
+            const size_t d0 = (size_t)b0 * 256, d1 = std::min((size_t)b1 * 256, (size_t)n);
+            cudaEvent_t e = c.take_event();
+            up.push_back(e);
+            cudaError_t ce = cudaMemcpyAsync(const_cast<double*>(d_depos) + 7 * d0, h_depos + 7 * d0,
+                                             sizeof(double) * 7 * (d1 - d0), cudaMemcpyHostToDevice, c.copy_stream);
+            if (ce == cudaSuccess) ce = cudaEventRecord(e, c.copy_stream);
+            if (ce == cudaSuccess) ce = cudaStreamWaitEvent(s, e, 0);
+            if (ce != cudaSuccess) rc = fail(WCT_ERR_CUDA, std::string("depo upload: ") + cudaGetErrorString(ce));
+            else prep(b0, b1);
+        }
+        for (auto e : up) c.event_pool.push_back(e);  // reusable once s has passed its wait
+        if (rc) return rc;
+    }
+    else
+        prep(0, -1);
     launch_scan(c.d_wcnt.as<int>(), nkeys, c.d_woff.as<int>(), c.d_wcur.as<int>(), s);
     t_prep.close(4 + (n > 0 ? 1 : 0));
     CUDA_TRY(cudaGetLastError());
@@ -628,10 +655,11 @@ struct FrameRegion {
 // each plane's written block, so the zero rest can go first.
 static int forward_device(Core& c, const double* d_depos, size_t ndepos, float* d_frame, wct_plane_window* wins,
                           int* frame_ident, cudaStream_t s, cudaEvent_t* plane_done = nullptr,
-                          cudaEvent_t zeroed = nullptr, std::vector<FrameRegion>* regions = nullptr)
+                          cudaEvent_t zeroed = nullptr, std::vector<FrameRegion>* regions = nullptr,
+                          const double* h_depos = nullptr)
 {
     EventPlan ev;
-    int prc = prepare_event(c, d_depos, ndepos, s, ev);
+    int prc = prepare_event(c, d_depos, ndepos, s, ev, true, h_depos);
     if (prc) return prc;
     const int n = ev.n, np = ev.np, nticks = ev.nticks, total_visits = ev.total_visits, rows = ev.gset.nrows_total;
     const PlaneSet& pset = ev.pset;
@@ -2061,8 +2089,7 @@ int wct_dt_forward(wct_depotransform* h, const double* depos, size_t ndepos, flo
     const size_t fbytes = sizeof(float) * (size_t)c.nrows() * c.nticks();
     CUDA_TRY(c.d_depos.ensure(sizeof(double) * 7 * std::max<size_t>(ndepos, 1)));
     CUDA_TRY(c.d_frame.ensure(fbytes));
-    if (ndepos)
-        CUDA_TRY(cudaMemcpyAsync(c.d_depos.p, depos, sizeof(double) * 7 * ndepos, cudaMemcpyHostToDevice, s));
+    // the depos go up in chunks on the copy stream, each chunk's prep starting as it arrives
     // each plane's rows go back as soon as they are final (copy stream), while
     // the next planes are still transformed
     // the frame goes back on the copy stream in two parts: first the zero
@@ -2074,7 +2101,7 @@ int wct_dt_forward(wct_depotransform* h, const double* depos, size_t ndepos, flo
     cudaEvent_t zeroed = c.take_event();
     std::vector<FrameRegion> reg;
     int rc = forward_device(c, c.d_depos.as<double>(), ndepos, c.d_frame.as<float>(), windows, frame_ident, s,
-                            done.data(), zeroed, &reg);
+                            done.data(), zeroed, &reg, ndepos ? depos : nullptr);
     if (rc == WCT_OK) {
         const int nt = c.nticks();
         const float* df = c.d_frame.as<float>();

@@ -166,10 +166,11 @@ __global__ void __launch_bounds__(256, 3) k_prep_all(const double* __restrict__ 
                                                   WindowDev* __restrict__ win_all, int* __restrict__ cnt_all,
                                                   float* __restrict__ tprof, unsigned long long* __restrict__ kb_all,
                                                   FlucParams fp, double* __restrict__ fq,
-                                                  unsigned char* __restrict__ wide_all)
+                                                  unsigned char* __restrict__ wide_all, int blk_offset)
 {
-    const int ev = event_of_block(evt, blockIdx.x);
-    const int i = evt.dep0[ev] + (blockIdx.x - evt.blk0[ev]) * blockDim.x + threadIdx.x;
+    const int bid = blockIdx.x + blk_offset;  // a launch may cover a range of the table's blocks
+    const int ev = event_of_block(evt, bid);
+    const int i = evt.dep0[ev] + (bid - evt.blk0[ev]) * blockDim.x + threadIdx.x;
     const int n = evt.dep0[evt.nev];  // record stride: all depos of the table
     const bool in = i < evt.dep0[ev + 1];
     WindowDev* win = win_all + (size_t)ev * ps.nplanes;
@@ -417,13 +418,15 @@ __global__ void __launch_bounds__(256, 3) k_prep_all(const double* __restrict__ 
 void launch_prep_all(const double* depos, const EventTable& et, int nkeys, const DriftDev& dd, int do_drift,
                      const PlaneSet& ps, const TimeDev& tb, double drift_speed, double nsigma, PatchRec* rec,
                      WindowDev* win, int* wire_cnt, float* tprof, unsigned long long* key_bound,
-                     const FlucParams& fp, double* fq, unsigned char* wide, cudaStream_t s)
+                     const FlucParams& fp, double* fq, unsigned char* wide, cudaStream_t s, int blk_begin,
+                     int blk_end)
 {
-    const int nblocks = et.blk0[et.nev];
-    if (nblocks <= 0) return;
-    k_prep_all<<<dim3(nblocks, ps.nplanes), 256, 0, s>>>(depos, et, nkeys, dd, do_drift, ps, tb, drift_speed,
-                                                         nsigma, rec, win,
-                                       wire_cnt, tprof, key_bound, fp, fq, wide);
+    const int nb = et.blk0[et.nev];
+    const int b0 = std::max(0, blk_begin), b1 = blk_end < 0 ? nb : std::min(blk_end, nb);
+    if (b1 <= b0) return;
+    k_prep_all<<<dim3(b1 - b0, ps.nplanes), 256, 0, s>>>(depos, et, nkeys, dd, do_drift, ps, tb, drift_speed,
+                                                         nsigma, rec, win, wire_cnt, tprof, key_bound, fp, fq, wide,
+                                                         b0);
 }
 
 // Exclusive scan of the per-key visit counts: block sums, a scan of the

@@ -232,7 +232,8 @@ struct TprofPool {
 void launch_prep_all(const double* depos, const EventTable& et, int nkeys, const DriftDev& dd, int do_drift,
                      const PlaneSet& ps, const TimeDev& tb, double drift_speed, double nsigma, PatchRec* rec,
                      WindowDev* win, int* wire_cnt, float* tprof, unsigned long long* key_bound,
-                     const FlucParams& fp, double* fq, unsigned char* wide, cudaStream_t s);
+                     const FlucParams& fp, double* fq, unsigned char* wide, cudaStream_t s, int blk_begin = 0,
+                     int blk_end = -1);  // blocks [blk_begin, blk_end) of the table (-1: to the end)
 void launch_binomial_samples(unsigned long long seed, int ident, int n, double p, long long count, int* out,
                              cudaStream_t s);
 void launch_fluc_sums(const PatchRec* rec, const EventTable& et, const PlaneSet& ps, float tbs, const FlucParams& fp,
