@@ -296,6 +296,10 @@ def run_b200(args):
             result["patterns"] = patterns(wct, synth, torch, stream, local)
         except Exception as e:  # the headline line must print whatever happens here
             result["patterns"] = {"error": repr(e)[:300]}
+        try:
+            result["patterns"]["downstream"] = downstream(wct, synth, torch, stream, local)
+        except Exception as e:
+            result["patterns"]["downstream"] = {"error": repr(e)[:300]}
         if not args.no_calibration:
             try:
                 result["patterns"]["calibration"] = calibration(wct, synth, torch, local)
@@ -397,6 +401,66 @@ def patterns(wct, synth, torch, stream, local):
     t_fl = _time_ms(torch, stream, lambda: dfl.forward_device(dd.data_ptr(), len(d), fr.data_ptr(), sid))
     out["fluctuated"] = {"workload": "full-APA event (%d depos), patch-cell and drift fluctuation on" % len(d),
                          "ms": t_fl, "depos_per_s": len(d) / (t_fl / 1e3)}
+    return out
+
+
+def downstream(wct, synth, torch, stream, local):
+    """The components beside the DepoTransform path, device-timed (CUDA events
+    on the launch stream, median of 5): the DepoFluxSplat truth frame of a
+    full-APA event's depos at the response plane, noise (three plane spectra)
+    and digitization of the full-APA frame, and IDFT 2-D transforms."""
+    peak, kind = load_peaks()
+    out = {}
+    sid = stream.cuda_stream
+    cfg = synth.apa_config()
+    dt = wct.from_config(cfg, device=local)
+    nrows, nticks = dt.frame_shape()
+    # splat: depos as the drifter leaves them (times and extents of their drift distance)
+    d = synth.apa_depos(seed=2).copy()
+    drift = np.abs(d[:, 2] - synth.RESPONSE_X)
+    d[:, 0] = drift / (1.6 * synth.mm / synth.us)
+    d[:, 2] = synth.RESPONSE_X
+    d[:, 5] = np.sqrt(2 * cfg["drifter"]["DL"] * d[:, 0])
+    d[:, 6] = np.sqrt(2 * cfg["drifter"]["DT"] * d[:, 0])
+    sc = dict(tick=cfg["tick"], window_start=0.0, window_duration=nticks * cfg["tick"], nsigma=3.0,
+              drift_speed=1.6 * synth.mm / synth.us, response_plane=synth.RESPONSE_X)
+    sr, st = dt.splat_shape(**sc)
+    dd = torch.from_numpy(d).cuda()
+    sf = torch.empty((sr, st), dtype=torch.float32, device="cuda")
+    t = _time_ms(torch, stream, lambda: dt.splat_device(dd.data_ptr(), len(d), sf.data_ptr(), sid, **sc))
+    out["splat"] = {"workload": "DepoFluxSplat frame of %d depos, %d x %d" % (len(d), sr, st), "ms": t,
+                    "depos_per_s": len(d) / (t / 1e3)}
+    # noise + digitizer on the full frame
+    frame = torch.zeros((nrows, nticks), dtype=torch.float32, device="cuda")
+    k = np.arange(nticks)
+    f = np.minimum(k, nticks - k).astype(np.float64)
+    spec = np.stack([(0.02 + 0.05 * np.exp(-((f - 300.0 * (p + 1)) / 400.0) ** 2)) * 1e-6 for p in range(3)])
+    dspec = torch.from_numpy(spec.astype(np.float32)).cuda()
+    row_spec = torch.from_numpy(np.concatenate([np.full(p["nwires"], i, np.int32)
+                                                for i, p in enumerate(cfg["planes"])])).cuda()
+    row_stream = torch.arange(nrows, dtype=torch.int32, device="cuda")
+    t_n = _time_ms(torch, stream, lambda: wct.add_noise_device(frame.data_ptr(), nticks, nrows, nticks,
+                                                               dspec.data_ptr(), nticks, row_spec.data_ptr(),
+                                                               row_stream.data_ptr(), seed=1, stream=sid))
+    dz = wct.Digitizer([p["nwires"] for p in cfg["planes"]], round=True)
+    base = torch.from_numpy(dz.row_baseline).cuda()
+    adc = torch.empty_like(frame)
+    t_d = _time_ms(torch, stream, lambda: dz.device(frame.data_ptr(), nticks, nrows, nticks, base.data_ptr(),
+                                                    adc.data_ptr(), nticks, stream=sid))
+    fb = nrows * nticks * 4
+    out["noise"] = {"workload": "incoherent noise on %d x %d" % (nrows, nticks), "ms": t_n,
+                    "gbs": 2 * fb / (t_n / 1e3) / 1e9, "peak_gbs": peak, "peak_kind": kind}
+    out["digitizer"] = {"workload": "Digitizer on %d x %d" % (nrows, nticks), "ms": t_d,
+                        "gbs": 2 * fb / (t_d / 1e3) / 1e9, "frac": 2 * fb / (t_d / 1e3) / 1e9 / peak,
+                        "peak_gbs": peak, "peak_kind": kind}
+    # IDFT: 2-D forward transforms
+    for (nr, nc) in ((1024, 1024), (2560, 6000)):
+        x = torch.randn((nr, nc), dtype=torch.complex64, device="cuda")
+        y = torch.empty_like(x)
+        t2 = _time_ms(torch, stream, lambda: wct.dft_2d_device(x.data_ptr(), y.data_ptr(), nr, nc, stream=sid))
+        n = nr * nc
+        out["idft_2d_%dx%d" % (nr, nc)] = {"ms": t2, "gflops_5nlog2n": 5 * n * np.log2(n) / (t2 / 1e3) / 1e9}
+        del x, y
     return out
 
 

@@ -260,6 +260,14 @@ def fft_best_length(n, keep_odd_even=False):
     return int(lib().wct_fft_best_length(int(n), 1 if keep_odd_even else 0))
 
 
+def add_noise_device(d_frame, ld, nrows, ncols, d_spectra, nspec, d_row_spec, d_row_stream, seed=0, ident=0, model=0,
+                     stream=None):
+    """add_noise on device arrays (pointers as ints), enqueued on stream."""
+    _check(lib().wct_add_noise_device(C.c_void_p(d_frame), ld, nrows, ncols, C.c_void_p(d_spectra), nspec,
+                                      C.c_void_p(d_row_spec), C.c_void_p(d_row_stream), int(seed), int(ident),
+                                      int(model), C.c_void_p(stream) if stream else None))
+
+
 def add_noise(frame, spectra, row_spec, row_stream, seed=0, ident=0, model=0):
     """IncoherentAddNoise / CoherentAddNoise on a host frame [nrows][ncols]
     float32 (updated in place and returned): spectra [nspectra][nspec]
@@ -498,6 +506,18 @@ class DepoTransform:
         out = np.zeros((nr.value, nt.value), dtype=np.float32)
         _check(lib().wct_dt_splat(self.h, C.byref(sc), d.ctypes.data if len(d) else None, len(d), out.ctypes.data))
         return out
+
+    def splat_device(self, d_depos_ptr, ndepos, d_frame_ptr, stream=None, **cfg):
+        """DepoFluxSplat on device buffers (frame of splat_shape(**cfg))."""
+        sc = SplatConfig.make(**cfg)
+        _check(lib().wct_dt_splat_device(self.h, C.byref(sc), C.c_void_p(d_depos_ptr), ndepos, C.c_void_p(d_frame_ptr),
+                                          C.c_void_p(stream) if stream else None))
+
+    def splat_shape(self, **cfg):
+        sc = SplatConfig.make(**cfg)
+        nr, nt = C.c_int(), C.c_int()
+        _check(lib().wct_dt_splat_shape(self.h, C.byref(sc), C.byref(nr), C.byref(nt)))
+        return nr.value, nt.value
 
     def forward_batch(self, events, out=None):
         """Host-buffer batch: ``events`` is a list of [n_e][7] depo arrays.  Returns
