@@ -62,6 +62,24 @@ def test_wire_length_interpolation_and_channel_spectrum():
     assert np.array_equal(m.channel_spectrum(0, 200 * CM, gain=14.05), s)  # within 1%: unchanged
 
 
+def test_coldelec_and_shaping_correction():
+    t = np.arange(0, 12 * US, 10.0)
+    r = noise.coldelec(t, 10.0, 2.0 * US)
+    assert r[0] == 0 and np.all(r[t >= 10 * US] == 0)
+    assert 1.0 * US < t[np.argmax(r)] < 3.0 * US          # peaks after about the shaping time
+    m = noise.EmpiricalNoiseModel(_entries(), nsamples=6000, period=0.5 * US)
+    base = m.channel_spectrum(0, 200 * CM)
+    assert np.array_equal(m.channel_spectrum(0, 200 * CM, shaping=2.01 * US), base)  # within 1%
+    s1 = m.channel_spectrum(0, 200 * CM, shaping=1.0 * US)
+    c, amp = m.interpolate_wire_length(0, 200 * CM)
+    tt = np.arange(m.L) * 0.5 * US
+    ratio = (np.abs(np.fft.fft(noise.coldelec(tt, 10.0, 1.0 * US).astype(np.float32).astype(np.float64)))
+             / np.abs(np.fft.fft(noise.coldelec(tt, 10.0, 2.0 * US).astype(np.float32).astype(np.float64))))
+    np.testing.assert_allclose(s1, np.sqrt((amp * ratio) ** 2 + c * c), rtol=1e-5)
+    # responses cached per 0.1 us step: 1.03 us reuses the 1.0 us response
+    assert np.array_equal(m.channel_spectrum(0, 200 * CM, shaping=1.03 * US), s1)
+
+
 def test_frame_spectra_groups_rows():
     m = noise.EmpiricalNoiseModel(_entries(), nsamples=6000, period=0.5 * US)
     spectra, row_spec = m.frame_spectra([0, 0, 0, 0], [150 * CM, 150.4 * CM, 400 * CM, 150 * CM])

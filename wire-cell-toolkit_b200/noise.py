@@ -12,9 +12,12 @@ linear interpolation between the plane's entries bracketing the channel's
 total wire length (rounded down to wire_length_scale steps; clamped at the
 shortest and longest), scaled by the channel's gain over the entries' gain
 when they differ by more than 1%, and combined with the interpolated
-constant as sqrt(amp^2 + const^2).  The shaping-time correction, which
-needs the channel-status component and the cold-electronics response, is
-not restated here.
+constant as sqrt(amp^2 + const^2).  A channel whose shaping time differs
+from the entries' by more than 1% has its amplitudes scaled by the ratio of
+the cold-electronics response magnitudes (util/src/Response.cxx:311-340,
+sampled at i * period for i < L) at the two shaping times; responses are
+cached by shaping time in 0.1 us steps, the first channel of a step setting
+it (as the reference caches them).
 """
 
 import numpy as np
@@ -22,6 +25,25 @@ import numpy as np
 from . import fft_best_length
 
 CM = 10.0  # the toolkit's length unit is the mm
+US = 1000.0  # and its time unit the ns
+
+
+def coldelec(time, gain, shaping):
+    """Response::coldelec (util/src/Response.cxx:311-340): the cold
+    electronics response at ``time`` (array), zero outside (0, 10 us)."""
+    t = np.asarray(time, dtype=np.float64)
+    r = t / shaping
+    g = gain * 10 * 1.012
+    e1, e2, e3 = np.exp(-2.94809 * r), np.exp(-2.82833 * r), np.exp(-2.40318 * r)
+    c1, s1 = np.cos(1.19361 * r), np.sin(1.19361 * r)
+    c2, s2 = np.cos(2.38722 * r), np.sin(2.38722 * r)
+    c3, s3 = np.cos(2.5928 * r), np.sin(2.5928 * r)
+    c4, s4 = np.cos(5.18561 * r), np.sin(5.18561 * r)
+    v = (4.31054 * e1 * g - 2.6202 * e2 * c1 * g - 2.6202 * e2 * c1 * c2 * g + 0.464924 * e3 * c3 * g
+         + 0.464924 * e3 * c3 * c4 * g + 0.762456 * e2 * s1 * g - 0.762456 * e2 * c2 * s1 * g
+         + 0.762456 * e2 * c1 * s2 * g - 2.620200 * e2 * s1 * s2 * g - 0.327684 * e3 * s3 * g
+         + 0.327684 * e3 * c4 * s3 * g - 0.327684 * e3 * c3 * s4 * g + 0.464924 * e3 * s3 * s4 * g)
+    return np.where((t <= 0) | (t >= 10 * US), 0.0, v)
 
 
 class EmpiricalNoiseModel:
@@ -34,6 +56,7 @@ class EmpiricalNoiseModel:
         i = np.arange(L)
         self.freq = np.where(i <= L / 2.0, i / (L * 1.0) / self.period, (L - i) / (L * 1.0) / self.period)
         self.planes = {}
+        self._resp = {}  # shaping step -> response magnitude (L values)
         for e in spectra:  # file order: by wire length within a plane
             ent = dict(plane=int(e["plane"]), gain=float(np.float32(e["gain"])),
                        shaping=float(np.float32(e["shaping"])), wirelen=float(np.float32(e["wirelen"])),
@@ -82,26 +105,41 @@ class EmpiricalNoiseModel:
             return lo["const"] * (1 - mu) + hi["const"] * mu, amp
         raise ValueError("EmpiricalNoiseModel: data corruption")
 
-    def channel_spectrum(self, plane, wire_length, gain=None):
+    def _response(self, shaping):
+        """|DFT| of ColdElec(10, shaping) sampled at i * period, i < L (float
+        samples), cached per 0.1 us step of the shaping time."""
+        key = int(shaping / US / 0.1)
+        if key not in self._resp:
+            sig = coldelec(np.arange(self.L) * self.period, 10.0, shaping).astype(np.float32)
+            self._resp[key] = np.abs(np.fft.fft(sig.astype(np.float64))).astype(np.float32).astype(np.float64)
+        return self._resp[key]
+
+    def channel_spectrum(self, plane, wire_length, gain=None, shaping=None):
         """The amplitude spectrum (L float32 values) of a channel of ``plane``
-        whose wires total ``wire_length``; ``gain``: the channel's preamplifier
-        gain when it deviates from the spectra's."""
+        whose wires total ``wire_length``; ``gain`` and ``shaping``: the
+        channel's preamplifier gain and shaping time when they deviate from
+        the spectra's (the channel-status values)."""
         ilen = int(wire_length / self.wlres)
         const, amp = self.interpolate_wire_length(plane, ilen * self.wlres)
         db_gain = self.planes[plane][0]["gain"]
+        db_shaping = self.planes[plane][0]["shaping"]
         if gain is not None and abs(gain - db_gain) > 0.01 * gain:
             amp = (amp * (gain / db_gain)).astype(np.float32).astype(np.float64)
+        if shaping is not None and abs(shaping - db_shaping) > 0.01 * shaping:
+            r1, r2 = self._response(shaping), self._response(db_shaping)
+            amp = (amp * (r1 / r2)).astype(np.float32).astype(np.float64)
         return np.sqrt(amp * amp + const * const).astype(np.float32)
 
-    def frame_spectra(self, row_plane, row_wire_length, row_gain=None):
+    def frame_spectra(self, row_plane, row_wire_length, row_gain=None, row_shaping=None):
         """Spectra for ``add_noise``: (spectra [k][L] float32, row_spec [rows])
-        with one spectrum per distinct (plane, length step, gain) of the rows."""
+        with one spectrum per distinct (plane, length step, gain, shaping) of the rows."""
         keys, spectra, row_spec = {}, [], np.empty(len(row_plane), dtype=np.int32)
         for r, (p, wl) in enumerate(zip(row_plane, row_wire_length)):
             g = None if row_gain is None else float(row_gain[r])
-            key = (int(p), int(wl / self.wlres), g)
+            sh = None if row_shaping is None else float(row_shaping[r])
+            key = (int(p), int(wl / self.wlres), g, sh)
             if key not in keys:
                 keys[key] = len(spectra)
-                spectra.append(self.channel_spectrum(int(p), wl, g))
+                spectra.append(self.channel_spectrum(int(p), wl, g, sh))
             row_spec[r] = keys[key]
         return np.stack(spectra) if spectra else np.zeros((0, self.L), np.float32), row_spec
