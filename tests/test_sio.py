@@ -88,3 +88,14 @@ def test_tar_streams(tmp_path, ext):
     m = sio.read_tar(q)
     assert sorted(m) == ["channels_sim_3", "frame_sim_3", "tickinfo_sim_3"]
     assert np.array_equal(m["frame_sim_3"], sio.frame_arrays(_frame(), np.arange(6), 500.0)[0])
+
+
+def test_frame_stream_back_to_dense(tmp_path):
+    f = _frame()
+    chans = np.array([100, 105, 101, 102, 104, 103])
+    q = str(tmp_path / "frames.tar.bz2")
+    sio.save_frame_stream(q, [(3, f, chans, 500.0, 2.0e3)], tag="sim")
+    (ident, tag, arr, ch, ti), = sio.load_frame_stream(q)
+    assert (ident, tag) == (3, "sim") and list(ti) == [2.0e3, 500.0, 3.0]
+    rows = {int(c): r for r, c in enumerate(chans)}
+    assert np.array_equal(sio.dense_frame(arr, ch, ti, rows, 40), f)

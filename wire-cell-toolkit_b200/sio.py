@@ -209,3 +209,34 @@ def save_frame_stream(path, frames, tag=""):
         members["channels_%s_%d" % (tag, ident)] = a[1]
         members["tickinfo_%s_%d" % (tag, ident)] = a[2]
     write_tar(path, members)
+
+
+def load_frame_stream(path):
+    """FrameFileSource: [(ident, tag, frame, channels, tickinfo)] of the
+    frames in a tar stream, in stream order."""
+    m = read_tar(path)
+    out = []
+    for name in m:
+        if not name.startswith("frame_"):
+            continue
+        tag, ident = name[len("frame_"):].rsplit("_", 1)
+        out.append((int(ident), tag, m[name], m["channels_%s_%s" % (tag, ident)],
+                    m["tickinfo_%s_%s" % (tag, ident)]))
+    return out
+
+
+def dense_frame(frame, channels, tickinfo, channel_rows, nticks, baseline=0.0, scale=1.0, offset=0.0):
+    """A saved frame put back on a dense [rows][nticks] float32 array:
+    ``channel_rows`` maps channel number -> row (the component's frame rows);
+    the saved (value - offset) / scale - baseline lands at ticks
+    tickinfo[2] + k; ticks outside [0, nticks) and unknown channels are dropped."""
+    nrows = max(channel_rows.values()) + 1 if channel_rows else 0
+    out = np.zeros((nrows, nticks), dtype=np.float32)
+    t0 = int(tickinfo[2])
+    vals = (np.asarray(frame, dtype=np.float32) - np.float32(offset)) / np.float32(scale) - np.float32(baseline)
+    lo, hi = max(0, t0), min(nticks, t0 + vals.shape[1])
+    for k, ch in enumerate(channels):
+        r = channel_rows.get(int(ch))
+        if r is not None and hi > lo:
+            out[r, lo:hi] = vals[k, lo - t0:hi - t0]
+    return out
