@@ -4,6 +4,8 @@ plane's wire bins and the window's ticks, |charge| added; per-plane smearing
 and time offsets; depos outside the window in time skip a plane, depos
 outside the wire plane in pitch skip the remaining planes."""
 
+import math
+
 import numpy as np
 import pytest
 
@@ -65,3 +67,77 @@ def test_splat_window_edges(wct, synth, oracle):
     o = oracle.splat(cfg, d, sc)
     assert rel_l2(f, o) < 1e-6
     assert wct.from_config(cfg).splat(d[:0], **sc).sum() == 0
+
+
+def _scalar_splat(cfg, depos, sc):
+    """DepoFluxSplat::operator() (gen/src/DepoFluxSplat.cxx:247-390) with
+    GaussianDiffusion::set_sampling and GausDesc::binint
+    (gen/src/GaussianDiffusion.cxx:30-56,116-182) one depo and cell at a
+    time in plain Python, for a single face without a bounding box."""
+    tick, nb = sc["tick"], int(sc["window_duration"] / sc["tick"])
+    tmin, tbs = sc["window_start"], (nb * tick) / nb
+    tmax = tmin + nb * tick
+    rows0 = np.cumsum([0] + [p["nwires"] for p in cfg["planes"]])
+    out = np.zeros((rows0[-1], nb))
+
+    def binint(start, step, n, c, s):
+        if s == 0:
+            return [1.0]
+        e = [0.5 * math.erf((start + step * k - c) / (math.sqrt(2.0) * s)) for k in range(n + 1)]
+        return [e[k + 1] - e[k] for k in range(n)]
+
+    def dist(x, c, s):
+        return (x - c) / s if s else x - c
+
+    for d in depos:
+        t, q, x, y, z, el, et = d
+        nominal = t + sc["response_plane"] / sc["drift_speed"]
+        for ip, pl in enumerate(cfg["planes"]):
+            st = el / sc["drift_speed"]
+            eff = sc["nsigma"] if el > 0 else 0
+            if dist(tmin, nominal, st) > eff or dist(tmax, nominal, st) < -eff:
+                continue
+            region = (pl["pitchmax"] - pl["pitchmin"]) / (pl["nwires"] - 1)
+            pmin, pmax = pl["pitchmin"] - 0.5 * region, pl["pitchmax"] + 0.5 * region
+            pbs = (pmax - pmin) / pl["nwires"]
+            cp = sum(pl["pitch"][k] * ((x, y, z)[k] - pl["origin"][k]) for k in range(3))
+            effp = sc["nsigma"] if et > 0 else 0
+            if dist(pmin, cp, et) > effp or dist(pmax, cp, et) < -effp:
+                break
+            t0 = max(int((nominal - st * sc["nsigma"] - tmin) / tbs), 0)
+            t1 = min(int((nominal + st * sc["nsigma"] - tmin) / tbs) + 1, nb)
+            p0 = max(int((cp - et * sc["nsigma"] - pmin) / pbs), 0)
+            p1 = min(int((cp + et * sc["nsigma"] - pmin) / pbs) + 1, pl["nwires"])
+            if t1 <= t0 or p1 <= p0:
+                continue
+            tv = binint(tmin + t0 * tbs, tbs, t1 - t0, nominal, st)
+            pv = binint(pmin + p0 * pbs, pbs, p1 - p0, cp, et)
+            raw = sum(a * b for a in pv for b in tv)
+            scale = np.float32(q / raw)
+            for a, pa in enumerate(pv):
+                for k, tb in enumerate(tv):
+                    out[rows0[ip] + p0 + a, t0 + k] += abs(float(np.float32(pa * tb) * scale))
+    return out
+
+
+def test_oracle_splat_matches_scalar_restatement(synth, oracle):
+    cfg = dict(synth.plane1_config(nticks=600), face_bb=None)
+    cfg["planes"] = [dict(cfg["planes"][0], nwires=120, pitchmin=-0.5 * 4.79 * 119, pitchmax=0.5 * 4.79 * 119)]
+    rng = np.random.default_rng(8)
+    n = 60
+    d = np.zeros((n, 7))
+    d[:, 0] = rng.uniform(0, 2.5e5, n)
+    d[:, 1] = -rng.uniform(1e3, 6e3, n)
+    d[:, 2] = 100.0
+    d[:, 4] = rng.uniform(-300, 300, n)
+    d[:, 5] = rng.uniform(0.0, 1.5, n)
+    d[:, 6] = rng.uniform(0.0, 2.0, n)
+    d[::7, 5] = 0.0
+    d[::5, 6] = 0.0
+    d[-3:, 4] = 2000.0  # beyond the wires: skipped
+    sc = dict(tick=500.0, window_start=0.0, window_duration=600 * 500.0, nsigma=3.0, drift_speed=1.6e-3,
+              response_plane=100.0)
+    o = oracle.splat(cfg, d, sc)
+    r = _scalar_splat(cfg, d, sc)
+    np.testing.assert_allclose(o, r, rtol=0, atol=1e-9 * np.abs(r).max())
+    assert r.sum() > 0
