@@ -99,3 +99,36 @@ def test_model_noise_power(wct):
     P = (np.abs(np.fft.fft(frame.astype(np.float64), axis=1)) ** 2).mean(axis=0)
     sig2 = 2.0 * (spectra[0].astype(np.float64) * np.sqrt(2.0 / 3.141592)) ** 2
     assert abs((P[: m.L // 2 + 1] / sig2[: m.L // 2 + 1]).mean() - 1.0) < 0.01
+
+
+def _scalar_resample(freq_grid, nsamples_model, ent):
+    """EmpiricalNoiseModel::resample (gen/src/EmpiricalNoiseModel.cxx:96-136) line by line."""
+    scale = np.sqrt(nsamples_model / (ent["nsamples"] * 1.0))
+    amps = [float(np.float32(a * scale)) for a in np.asarray(ent["amps"], np.float32)]
+    freqs = [float(f) for f in np.asarray(ent["freqs"], np.float32)]
+    out = []
+    for frequency in freq_grid:
+        if frequency <= freqs[0]:
+            lo, hi, mu = 0, 1, 0.0
+        elif frequency >= freqs[-1]:
+            lo, hi, mu = len(freqs) - 2, len(freqs) - 1, 1.0
+        else:
+            lo, hi = 0, 1
+            for j in range(len(freqs)):
+                if frequency > freqs[j]:
+                    lo, hi = j, j + 1
+                else:
+                    break
+            mu = (frequency - freqs[lo]) / (freqs[hi] - freqs[lo])
+        out.append(float(np.float32((1 - mu) * amps[lo] + mu * amps[hi])))
+    return np.array(out)
+
+
+def test_resample_matches_scalar_loop():
+    rng = np.random.default_rng(4)
+    ents = _entries()
+    ents[1]["freqs"] = list(np.sort(rng.uniform(0, 1.0 / (2 * 0.5 * US), 40)))
+    ents[1]["amps"] = list(rng.uniform(0.5, 2.0, 40))
+    m = noise.EmpiricalNoiseModel(ents, nsamples=6000, period=0.5 * US)
+    for k in range(3):
+        np.testing.assert_array_equal(m.planes[0][k]["amps"], _scalar_resample(m.freq, m.L, ents[k]))
