@@ -295,7 +295,12 @@ int wct_dt_frame_shape(const wct_depotransform* dt, int* nrows, int* nticks);
 
 /* DepoTransform::operator() (gen/src/DepoTransform.cxx:155-224) on host
  * buffers: depos [ndepos][7] in, dense frame [nrows][nticks] out, one window
- * per plane (may be NULL), frame ident out (may be NULL). */
+ * per plane (may be NULL), frame ident out (may be NULL).  The transfers
+ * overlap the kernels: the depos go up in chunks that the first kernel takes
+ * as they arrive, each plane's zero rows and ticks come back while the
+ * kernels run and its window block once the plane is done; every element of
+ * frame is written.  Page-locked host buffers let the copies run alongside
+ * the kernels. */
 int wct_dt_forward(wct_depotransform* dt, const double* depos, size_t ndepos, float* frame,
                    wct_plane_window* windows, int* frame_ident);
 /* The same on device buffers, enqueued on stream (cudaStream_t, NULL = the
