@@ -116,7 +116,8 @@ int wct_pir_long_waveform(const wct_pir* pir, float* out);
 int wct_pir_destroy(wct_pir* pir);
 
 /* fft_best_length (util/src/FFTBestLength.cxx:12-59): the smallest length
- * >= n of the reference's fast-size tables (keep_odd_even: of n's parity). */
+ * >= n of the reference's fast-size tables (keep_odd_even: of n's parity),
+ * n itself above the tables; 0 for a negative n. */
 long wct_fft_best_length(long n, int keep_odd_even);
 
 /* ---- Batched FFT convolution of rows ---- */

@@ -71,6 +71,40 @@ def test_fft_best_length_known_sizes(oracle):
     assert oracle.fft_best_length(846, True) == 896
 
 
+def _fft_tables():
+    with open(os.path.join(os.path.dirname(GOLDEN), "fft_lengths_ref.json")) as f:
+        return json.load(f)
+
+
+def test_fft_length_tables_are_the_references():
+    """The three tables of util/src/FFTBestLength.cxx:16-50 (extracted from
+    the source text by tests/golden/make_fft_lengths.py) equal csrc/fft_lengths.h,
+    which the host window arithmetic and the device batch planner share."""
+    g = _fft_tables()
+    hdr = open(os.path.join(os.path.dirname(os.path.dirname(os.path.dirname(GOLDEN))), "wire-cell-toolkit_b200", "csrc",
+                            "fft_lengths.h")).read()
+    for key, macro in (("any", "WCT_FFT_LENGTHS_ANY"), ("even", "WCT_FFT_LENGTHS_EVEN"), ("odd", "WCT_FFT_LENGTHS_ODD")):
+        line = next(ln for ln in hdr.splitlines() if ln.startswith("#define " + macro + " "))
+        assert [int(x) for x in line.split(None, 2)[2].split(",")] == g[key]
+
+
+def test_fft_best_length_every_size(oracle, wct):
+    """util/src/FFTBestLength.cxx:52-58: the first table entry >= n while n is
+    within the table, else n itself; the even or odd table by n's parity when
+    keep_odd_even.  Every n up to past the tables' end, oracle and product."""
+    g = _fft_tables()
+
+    def expect(n, keep):
+        t = g["any"] if not keep else (g["even"] if n % 2 == 0 else g["odd"])
+        return next((e for e in t if e >= n), n)
+
+    for keep in (False, True):
+        for n in range(0, 17001):
+            e = expect(n, keep)
+            assert oracle.fft_best_length(n, keep) == e, (n, keep)
+            assert wct.fft_best_length(n, keep) == e, (n, keep)
+
+
 def test_pimpos_known_answers(oracle):
     """util/test/test_pimpos.cxx:47-70: 2001 wires at 3 mm."""
     pitch = 3.0

@@ -1789,7 +1789,7 @@ int wct_pir_long_waveform(const wct_pir* p, float* out)
 
 long wct_fft_best_length(long n, int keep_odd_even)
 {
-    if (n <= 0) return 0;
+    if (n < 0) return 0;
     return (long)fft_best_length((size_t)n, keep_odd_even != 0);
 }
 
