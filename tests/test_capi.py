@@ -71,6 +71,33 @@ def test_null_arguments_are_rejected(wct):
     assert L.wct_pir_closest(None, 0.0, C.byref(k)) == wct.WCT_ERR_ARG
 
 
+def test_pir_create_argument_checks(wct, synth):
+    """Inconsistent response arguments are status codes: short responses
+    announced but not given, a negative length, a non-positive field-response
+    pitch (PlaneImpactResponse's wire numbering divides by it), and a field
+    response sampled before t = 0 (the reference's bin index would not exist)."""
+    import ctypes as C
+    L = wct.lib()
+    fr = synth.plane1_config(nticks=1000, nwire_half=10)["fr"][0]
+    pp = np.ascontiguousarray(fr["pitchpos"], dtype=np.float64)
+    cur = np.ascontiguousarray(fr["current"], dtype=np.float64)
+    h = C.c_void_p()
+
+    def create(pitch=fr["pitch"], tstart=fr["tstart"], nshort=0, sl=None, sw=None):
+        d = wct.FrPlane(pp.shape[0], cur.shape[1], pp.ctypes.data, cur.ctypes.data, pitch, tstart, fr["period"])
+        return L.wct_pir_create(C.byref(d), nshort, sl, sw, 100e3, 500.0, 1000, C.byref(h))
+
+    assert create(nshort=1) == wct.WCT_ERR_ARG
+    neg = np.array([-5], dtype=np.int32)
+    wave = np.zeros(4)
+    assert create(nshort=1, sl=neg.ctypes.data, sw=wave.ctypes.data) == wct.WCT_ERR_ARG
+    assert create(pitch=0.0) == wct.WCT_ERR_CONFIG
+    assert create(tstart=-10e3) == wct.WCT_ERR_CONFIG
+    assert create() == wct.WCT_OK
+    L.wct_pir_destroy(h)
+    assert L.wct_pir_set_long_responses(None, 0, None, None, 0.0) == wct.WCT_ERR_ARG
+
+
 @pytest.mark.parametrize("nwire_half", [10, 21])
 def test_pir_build_matches_oracle(wct, oracle, synth, nwire_half):
     """PlaneImpactResponse::build_responses (gen/src/PlaneImpactResponse.cxx:89-269):

@@ -1736,8 +1736,11 @@ const char* wct_last_error(void) { return g_last_error; }
 int wct_pir_create(const wct_fr_plane* fr, int nshort, const int* short_len, const double* short_wave,
                    double overall_short_padding, double tick, int nticks, wct_pir** out)
 {
-    if (!fr || !out || !fr->pitchpos || !fr->current || nticks <= 0 || tick <= 0)
+    if (!fr || !out || !fr->pitchpos || !fr->current || fr->npaths <= 0 || fr->nsamples <= 0 || nticks <= 0 ||
+        tick <= 0 || nshort < 0 || (nshort && (!short_len || !short_wave)))
         return fail(WCT_ERR_ARG, "wct_pir_create: bad arguments");
+    for (int i = 0; i < nshort; ++i)
+        if (short_len[i] < 0) return fail(WCT_ERR_ARG, "wct_pir_create: negative short response length");
     try {
         std::vector<std::vector<double>> shorts;
         size_t off = 0;
@@ -1745,10 +1748,10 @@ int wct_pir_create(const wct_fr_plane* fr, int nshort, const int* short_len, con
             shorts.emplace_back(short_wave + off, short_wave + off + short_len[i]);
             off += short_len[i];
         }
-        auto* p = new wct_pir;
+        auto p = std::make_unique<wct_pir>();
         p->pir = build_pir(fr->npaths, fr->nsamples, fr->pitchpos, fr->current, fr->pitch, fr->tstart, fr->period,
                            shorts, overall_short_padding, tick, nticks);
-        *out = p;
+        *out = p.release();
         return WCT_OK;
     }
     catch (std::exception& e) {
@@ -1761,15 +1764,21 @@ int wct_pir_set_long_responses(wct_pir* p, int nlong, const int* long_len, const
 {
     if (!p || nlong < 0 || (nlong && (!long_len || !long_wave)) || long_padding < 0)
         return fail(WCT_ERR_ARG, "wct_pir_set_long_responses: bad arguments");
-    std::vector<std::vector<double>> longs;
-    size_t off = 0;
-    for (int i = 0; i < nlong; ++i) {
+    for (int i = 0; i < nlong; ++i)
         if (long_len[i] < 0) return fail(WCT_ERR_ARG, "wct_pir_set_long_responses: negative length");
-        longs.emplace_back(long_wave + off, long_wave + off + long_len[i]);
-        off += long_len[i];
+    try {
+        std::vector<std::vector<double>> longs;
+        size_t off = 0;
+        for (int i = 0; i < nlong; ++i) {
+            longs.emplace_back(long_wave + off, long_wave + off + long_len[i]);
+            off += long_len[i];
+        }
+        set_long_responses(p->pir, longs, long_padding);
+        return WCT_OK;
     }
-    set_long_responses(p->pir, longs, long_padding);
-    return WCT_OK;
+    catch (std::exception& e) {
+        return fail(WCT_ERR_CONFIG, e.what());
+    }
 }
 
 int wct_pir_long_info(const wct_pir* p, int* nsamples, int* pad)

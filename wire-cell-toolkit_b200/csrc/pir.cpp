@@ -53,6 +53,8 @@ Pir build_pir(int npaths, int nsamples, const double* pitchpos, const double* cu
 {
     const int n_per = 6;  // six paths per wire region (PlaneImpactResponse.cxx:164)
     if (npaths < n_per || npaths % n_per) throw std::runtime_error("field response must hold 6 paths per wire");
+    if (!(fr_pitch > 0.0) || !(period > 0.0) || !(tick > 0.0))
+        throw std::runtime_error("field response pitch, period and tick must be positive");
     Pir p;
     p.nticks = nticks;
     p.tick = tick;
@@ -88,6 +90,7 @@ Pir build_pir(int npaths, int nsamples, const double* pitchpos, const double* cu
         std::vector<double> wave(n_short, 0.0);
         for (int r = 0; r < nsamples; ++r) {
             const double time = tstart + (r + 0.5) * rawbs;  // Binning::center
+            if (!(time >= 0.0)) throw std::runtime_error("out of bounds field response (sample before t = 0)");
             const size_t bin = time / tick;
             if (bin >= n_short) throw std::runtime_error("out of bounds field response");
             wave[bin] += current[(size_t)ip * nsamples + r] * period;
