@@ -269,12 +269,16 @@ int wct_digitize(const float* frame, int nrows, int ncols, const float* row_base
  * false here), "device" (CUDA ordinal) and "seed" (key of the random streams
  * that "fluctuate" draws from, in place of the reference's "rng" component). */
 int wct_dt_create(const char* json_config, wct_depotransform** out);
+/* The calls below that take a component are serialised on it: configuration
+ * calls and forwards from several host threads take turns (as the
+ * reference's single-threaded node); separate components run concurrently. */
 /* DepoTransform::default_configuration (gen/src/DepoTransform.cxx:114-153) as JSON. */
 int wct_dt_default_configuration(char* buf, size_t len);
 /* Add an anode face with its sensitive volume (IAnodeFace::sensitive,
  * gen/src/AnodePlane.cxx:259-290); bb_lo == NULL means no volume cut. */
 int wct_dt_add_face(wct_depotransform* dt, const double* bb_lo, const double* bb_hi, int* face);
-/* Add a wire plane to a face (IAnodeFace::planes order). */
+/* Add a wire plane to a face (IAnodeFace::planes order); WCT_ERR_CONFIG
+ * unless nwires >= 2, nimpacts even and >= 2, and pitchmax > pitchmin. */
 int wct_dt_add_plane(wct_depotransform* dt, int face, const wct_plane_desc* desc, int* plane);
 /* Use a PIR for a plane: ImpactTransform's response selection
  * (gen/src/ImpactTransform.cxx:26-74) over pirs[plane]. */
@@ -321,7 +325,10 @@ int wct_dt_traces(const wct_depotransform* dt, const float* frame, int* channel,
  * call: out[i] = {toffset, poffset, nt, np} of GaussianDiffusion::set_sampling
  * (gen/src/GaussianDiffusion.cxx:116-149); nt = np = 0 where the depo adds no
  * patch (dropped by the drift, the sensitive volume, BinnedDiffusion_transform::add
- * or an empty sample range).  n must equal the last call's depo count. */
+ * or an empty sample range).  n must equal the last call's depo count.  The
+ * records are read with a blocking copy on the legacy default stream, which
+ * does not wait for the component's streams: after wct_dt_forward_device,
+ * synchronise its stream first (wct_dt_forward returns complete). */
 int wct_dt_patch_records(const wct_depotransform* dt, int face, int plane, int* out, size_t n);
 /* Stage profiling (the engine-level timers of pgraph/src/Graph.cxx:118-122,
  * here per device stage): when enabled, every forward call records CUDA

@@ -1921,6 +1921,7 @@ int wct_dt_default_configuration(char* buf, size_t len)
 int wct_dt_add_face(wct_depotransform* h, const double* lo, const double* hi, int* face)
 {
     if (!h) return fail(WCT_ERR_ARG, "null component");
+    std::lock_guard<std::mutex> lk(h->core.mtx);
     FaceState f;
     if (lo && hi) {
         f.have_bb = true;
@@ -1936,10 +1937,12 @@ int wct_dt_add_face(wct_depotransform* h, const double* lo, const double* hi, in
 
 int wct_dt_add_plane(wct_depotransform* h, int face, const wct_plane_desc* d, int* plane)
 {
-    if (!h || !d || face < 0 || face >= (int)h->core.faces.size())
-        return fail(WCT_ERR_ARG, "wct_dt_add_plane: bad arguments");
+    if (!h || !d) return fail(WCT_ERR_ARG, "wct_dt_add_plane: bad arguments");
+    std::lock_guard<std::mutex> lk(h->core.mtx);
+    if (face < 0 || face >= (int)h->core.faces.size()) return fail(WCT_ERR_ARG, "wct_dt_add_plane: bad face");
     if (d->nwires < 2 || d->nimpacts < 2 || (d->nimpacts % 2))
         return fail(WCT_ERR_CONFIG, "need >= 2 wires and an even number of impacts per wire");
+    if (!(d->pitchmax > d->pitchmin)) return fail(WCT_ERR_CONFIG, "pitchmax must exceed pitchmin");
     Core& c = h->core;
     ++c.config_gen;
     auto ps = std::make_unique<PlaneState>();
@@ -1994,6 +1997,8 @@ static PlaneState* find_plane(wct_depotransform* h, int face, int plane)
 int wct_dt_set_response_table(wct_depotransform* h, int face, int plane, int ngroups, int npad, int nsamples,
                               double pitch, double impact, int waveform_pad, const float* table)
 {
+    if (!h) return fail(WCT_ERR_ARG, "wct_dt_set_response_table: null component");
+    std::lock_guard<std::mutex> lk(h->core.mtx);
     PlaneState* ps = find_plane(h, face, plane);
     if (!ps || !table || ngroups < 3 || npad < 0 || nsamples <= 0)
         return fail(WCT_ERR_ARG, "wct_dt_set_response_table: bad arguments");
@@ -2033,8 +2038,12 @@ int wct_dt_set_response_table(wct_depotransform* h, int face, int plane, int ngr
 
 int wct_dt_set_response_pir(wct_depotransform* h, int face, int plane, const wct_pir* p)
 {
-    PlaneState* ps = find_plane(h, face, plane);
-    if (!ps || !p) return fail(WCT_ERR_ARG, "wct_dt_set_response_pir: bad arguments");
+    bool have_plane = false;
+    if (h) {
+        std::lock_guard<std::mutex> lk(h->core.mtx);
+        have_plane = find_plane(h, face, plane) != nullptr;
+    }
+    if (!have_plane || !p) return fail(WCT_ERR_ARG, "wct_dt_set_response_pir: bad arguments");
     const Pir& pir = p->pir;
     // ImpactTransform.cxx:28-74
     const int G = std::round(pir.pitch / pir.impact) + 1;
@@ -2060,10 +2069,11 @@ int wct_dt_set_response_pir(wct_depotransform* h, int face, int plane, const wct
 
 int wct_dt_set_long_response(wct_depotransform* h, int face, int plane, int nsamples, const float* wave, int pad)
 {
+    if (!h) return fail(WCT_ERR_ARG, "wct_dt_set_long_response: null component");
+    std::lock_guard<std::mutex> lk(h->core.mtx);
     PlaneState* ps = find_plane(h, face, plane);
     if (!ps || nsamples < 0 || (nsamples && !wave) || pad < 0)
         return fail(WCT_ERR_ARG, "wct_dt_set_long_response: bad arguments");
-    std::lock_guard<std::mutex> lk(h->core.mtx);
     ps->long_wf.assign(wave, wave + nsamples);
     ps->long_pad = pad;
     ps->long_nfft = 0;  // spectrum rebuilt at the next use
