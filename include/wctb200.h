@@ -230,8 +230,10 @@ int wct_dt_splat(wct_depotransform* dt, const wct_splat_config* cfg, const doubl
  * normal index), so a frame's noise is reproducible and independent of the
  * launch; the reference's generator (std::mt19937 with recycled normals) is
  * matched in distribution, not in values.  nspec even with a 7-smooth half
- * up to 14336.  Device version on the current device and stream; host
- * version on host arrays (frame updated in place). */
+ * up to 14336.  Device version on the current device and stream, the
+ * spectrum indices unchecked (each below the number of spectra the caller
+ * holds on the device); host version on host arrays (frame updated in place,
+ * indices checked against nspectra). */
 int wct_add_noise_device(float* frame, long ld, int nrows, int ncols, const float* spectra, int nspec,
                          const int* row_spec, const int* row_stream, unsigned long long seed, int ident, int model,
                          void* stream);

@@ -2609,6 +2609,7 @@ static int splat_setup(const wct_depotransform* h, const wct_splat_config* cfg, 
     if (!h || !cfg) return fail(WCT_ERR_ARG, "splat: bad arguments");
     if (!(cfg->tick > 0) || !(cfg->window_duration >= 0) || !(cfg->drift_speed > 0) || !(cfg->nsigma >= 0))
         return fail(WCT_ERR_CONFIG, "splat: tick and drift_speed must be positive, window_duration and nsigma not negative");
+    if (cfg->window_duration / cfg->tick >= 2147483647.0) return fail(WCT_ERR_SIZE, "splat: more than 2^31 - 1 ticks");
     sp = SplatParams{};
     const int nbins = (int)(cfg->window_duration / cfg->tick);
     sp.tb.nbins = nbins;
