@@ -1,10 +1,14 @@
 // Minimal JSON reader for component configuration (the subset produced by
 // Jsonnet -> JSON in Wire-Cell configurations: objects, arrays, strings,
-// numbers, booleans, null).
+// numbers, booleans, null).  Numbers follow the JSON grammar and convert
+// independently of the process locale (a host framework may set LC_NUMERIC);
+// nesting deeper than kMaxDepth is refused instead of exhausting the stack.
 #pragma once
 
 #include <cctype>
+#include <charconv>
 #include <cstdlib>
+#include <system_error>
 #include <map>
 #include <memory>
 #include <stdexcept>
@@ -57,9 +61,12 @@ class Parser {
         return v;
     }
 
+    static constexpr int kMaxDepth = 256;
+
    private:
     const std::string& s_;
     size_t i_{0};
+    int depth_{0};
     [[noreturn]] void fail(const char* what)
     {
         throw std::runtime_error(std::string("json: ") + what + " at offset " + std::to_string(i_));
@@ -89,11 +96,30 @@ class Parser {
     }
     Value number()
     {
-        const char* b = s_.c_str() + i_;
-        char* e = nullptr;
-        double d = std::strtod(b, &e);
-        if (e == b) fail("bad value");
-        i_ += (size_t)(e - b);
+        // -?(0|[1-9][0-9]*)(.[0-9]+)?([eE][+-]?[0-9]+)?
+        const size_t n = s_.size();
+        size_t j = i_;
+        auto digits = [&]() {
+            const size_t k = j;
+            while (j < n && s_[j] >= '0' && s_[j] <= '9') ++j;
+            return j > k;
+        };
+        if (j < n && s_[j] == '-') ++j;
+        if (j < n && s_[j] == '0') ++j;
+        else if (!digits()) fail("bad value");
+        if (j < n && s_[j] == '.') {
+            ++j;
+            if (!digits()) fail("bad number");
+        }
+        if (j < n && (s_[j] == 'e' || s_[j] == 'E')) {
+            ++j;
+            if (j < n && (s_[j] == '+' || s_[j] == '-')) ++j;
+            if (!digits()) fail("bad number");
+        }
+        double d = 0.0;
+        const auto r = std::from_chars(s_.data() + i_, s_.data() + j, d);
+        if (r.ec != std::errc() || r.ptr != s_.data() + j) fail("number out of range");
+        i_ = j;
         Value v;
         v.kind = Value::Number;
         v.num = d;
@@ -139,27 +165,33 @@ class Parser {
     }
     Value array()
     {
+        if (++depth_ > kMaxDepth) fail("nesting too deep");
         Value v;
         v.kind = Value::Array;
         eat('[');
-        if (eat(']')) return v;
-        do { v.arr.push_back(value()); } while (eat(','));
-        if (!eat(']')) fail("expected ]");
+        if (!eat(']')) {
+            do { v.arr.push_back(value()); } while (eat(','));
+            if (!eat(']')) fail("expected ]");
+        }
+        --depth_;
         return v;
     }
     Value object()
     {
+        if (++depth_ > kMaxDepth) fail("nesting too deep");
         Value v;
         v.kind = Value::Object;
         eat('{');
-        if (eat('}')) return v;
-        do {
-            ws();
-            std::string k = string();
-            if (!eat(':')) fail("expected :");
-            v.obj[k] = value();
-        } while (eat(','));
-        if (!eat('}')) fail("expected }");
+        if (!eat('}')) {
+            do {
+                ws();
+                std::string k = string();
+                if (!eat(':')) fail("expected :");
+                v.obj[k] = value();
+            } while (eat(','));
+            if (!eat('}')) fail("expected }");
+        }
+        --depth_;
         return v;
     }
 };
