@@ -10,7 +10,9 @@
  * units (util/inc/WireCellUtil/Units.h): mm = 1, ns = 1, positron charge = 1.
  *
  * Depo layout (IDepo, iface/inc/WireCellIface/IDepo.h:14-51): 7 doubles per
- * depo: time, charge, x, y, z, extent_long, extent_tran.
+ * depo: time, charge, x, y, z, extent_long, extent_tran.  The transform drops
+ * a depo with a NaN or infinite value, as it drops one outside the drift
+ * volume (the reference's result is undefined for such a depo).
  *
  * Frame layout: dense float32 rows, one row per wire of every plane (faces in
  * the order added, planes in the order added within a face), nticks columns

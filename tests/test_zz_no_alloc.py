@@ -8,8 +8,8 @@ check that it gives the same rows as the allocating entry point on two calls
 in a row -- the second call finds the first call's data in the scratch -- and
 that sizes beyond the fixed array are refused before any device work.
 
-This file is collected last (test_zz_*) so a run that stops at the first
-failure has already run every other test."""
+This file is collected at the end (test_zz_*) so a run that stops at the
+first failure has already run the other tests."""
 
 import ctypes as C
 

@@ -181,8 +181,11 @@ __global__ void __launch_bounds__(256, 3) k_prep_all(const double* __restrict__ 
     if (in) {
         const double* p = dep + 7 * (size_t)i;
         t = p[0]; q = p[1]; x = p[2]; y = p[3]; z = p[4]; el = p[5]; et = p[6];
-        ok = true;
-        if (do_drift) {
+        // a depo with a NaN or infinite value is dropped: the reference's
+        // bin-index arithmetic is undefined for it, and its extents would
+        // otherwise reach the event window's min/max reduction
+        ok = isfinite(t) && isfinite(q) && isfinite(x) && isfinite(y) && isfinite(z) && isfinite(el) && isfinite(et);
+        if (ok && do_drift) {
             if (q == 0.0) ok = false;
             else {
                 int found = -1;
