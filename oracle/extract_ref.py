@@ -1,0 +1,73 @@
+"""TEST INFRASTRUCTURE ONLY.
+
+Cuts self-contained pieces out of the reference source tree, as they are,
+into oracle/_ref/ (git-ignored build output) so that oracle/Makefile can
+compile them with ref_funcs_harness.cpp.  The surrounding reference files
+cannot be compiled here (they include Boost, Eigen, jsoncpp or spdlog
+headers); the pieces themselves need only the standard library and the
+reference's own header-only Units.h and Waveform.h.
+
+  gausdesc_struct.inc  struct GausDesc       gen/inc/WireCellGen/GaussianDiffusion.h
+  gausdesc_fns.inc     GausDesc::sample, binint, weight
+                                             gen/src/GaussianDiffusion.cxx
+  waveform_edge.inc    Waveform::edge        util/src/Waveform.cxx
+  coldelec.inc         Response::coldelec    util/src/Response.cxx
+
+Each piece is found by its declaration (not by line number) and ends at the
+brace that closes it.
+
+Usage: python extract_ref.py REFERENCE_TREE OUT_DIR"""
+
+import os
+import re
+import sys
+
+PIECES = {
+    "gausdesc_struct.inc": [("gen/inc/WireCellGen/GaussianDiffusion.h", r"^\s*struct GausDesc\s*\{")],
+    "gausdesc_fns.inc": [
+        ("gen/src/GaussianDiffusion.cxx", r"^std::vector<double> Gen::GausDesc::sample\("),
+        ("gen/src/GaussianDiffusion.cxx", r"^std::vector<double> Gen::GausDesc::binint\("),
+        ("gen/src/GaussianDiffusion.cxx", r"^std::vector<double> Gen::GausDesc::weight\("),
+    ],
+    "waveform_edge.inc": [("util/src/Waveform.cxx", r"^std::pair<int, int> WireCell::Waveform::edge\(")],
+    "coldelec.inc": [("util/src/Response.cxx", r"^double Response::coldelec\(")],
+}
+
+
+def block(text, start):
+    """The text from the first line matching ``start`` to the brace closing
+    the first brace opened at or after it (and a ';' right after it)."""
+    m = re.search(start, text, flags=re.M)
+    if m is None:
+        raise SystemExit("not found: " + start)
+    i = m.start()
+    depth, opened = 0, False
+    for j in range(text.index("{", m.start()), len(text)):
+        c = text[j]
+        if c == "{":
+            depth += 1
+            opened = True
+        elif c == "}":
+            depth -= 1
+            if opened and depth == 0:
+                end = j + 1
+                if text[end:end + 1] == ";":
+                    end += 1
+                return text[i:end] + "\n"
+    raise SystemExit("unbalanced braces after: " + start)
+
+
+def main():
+    ref, out = sys.argv[1], sys.argv[2]
+    os.makedirs(out, exist_ok=True)
+    for name, parts in PIECES.items():
+        chunks = []
+        for path, start in parts:
+            with open(os.path.join(ref, path)) as f:
+                chunks.append("// %s\n" % path + block(f.read(), start))
+        with open(os.path.join(out, name), "w") as f:
+            f.write("\n".join(chunks))
+
+
+if __name__ == "__main__":
+    main()

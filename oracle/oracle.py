@@ -18,9 +18,11 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "liboracle.so")
 REF_PATH = os.path.join(HERE, "_ref", "libref_binning.so")
+REF_FUNCS_PATH = os.path.join(HERE, "_ref", "libref_funcs.so")
 
 _lib = None
 _ref = None
+_ref_funcs = None
 
 
 def build():
@@ -35,6 +37,7 @@ def lib():
         if not os.path.exists(LIB_PATH):
             build()
         _lib = C.CDLL(LIB_PATH)
+        _sig(_lib, "orc")
         _lib.orc_fft_best_length.restype = C.c_int
         _lib.orc_fft_best_length.argtypes = [C.c_long, C.c_int]
         _lib.orc_binning_bin.restype = C.c_int
@@ -79,6 +82,48 @@ def ref():
         _ref.ref_sample_bin_range.argtypes = [C.c_int, C.c_double, C.c_double, C.c_double, C.c_double,
                                               C.POINTER(C.c_int)]
     return _ref
+
+
+def ref_funcs():
+    """The harness of reference-compiled GausDesc, Waveform::edge and
+    Response::coldelec (oracle/ref_funcs_harness.cpp), or None when it was
+    not built."""
+    global _ref_funcs
+    if _ref_funcs is None and os.path.exists(REF_FUNCS_PATH):
+        _ref_funcs = C.CDLL(REF_FUNCS_PATH)
+        _sig(_ref_funcs, "ref")
+    return _ref_funcs
+
+
+def _sig(L, prefix):
+    d, i, p = C.c_double, C.c_int, C.c_void_p
+    for n, rt, at in [("_gd_binint", i, [d, d, d, d, i, p]), ("_gd_weight", i, [d, d, d, d, i, p, p]),
+                      ("_gd_distance", d, [d, d, d])]:
+        f = getattr(L, prefix + n)
+        f.restype = rt
+        f.argtypes = at
+    if prefix == "ref":
+        L.ref_gd_sigma_range.restype = None
+        L.ref_gd_sigma_range.argtypes = [d, d, d, p]
+        L.ref_wave_edge.restype = None
+        L.ref_wave_edge.argtypes = [p, i, p]
+        L.ref_coldelec.restype = d
+        L.ref_coldelec.argtypes = [d, d, d]
+
+
+def gd_binint(L, prefix, center, sigma, start, step, nbins):
+    """GausDesc(center, sigma).binint(start, step, nbins) through library L
+    (the oracle with prefix "orc", the reference harness with "ref")."""
+    out = np.zeros(max(nbins, 1))
+    n = getattr(L, prefix + "_gd_binint")(center, sigma, start, step, nbins, out.ctypes.data)
+    return out[:n]
+
+
+def gd_weight(L, prefix, center, sigma, start, step, nbins, pvec):
+    pv = np.ascontiguousarray(pvec, dtype=np.float64)
+    out = np.zeros(max(nbins, 1))
+    n = getattr(L, prefix + "_gd_weight")(center, sigma, start, step, nbins, pv.ctypes.data, out.ctypes.data)
+    return out[:n]
 
 
 class OrcPlane(C.Structure):

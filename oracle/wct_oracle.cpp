@@ -1390,4 +1390,23 @@ void orc_edge(const float* wave, int size, int* out)
     out[1] = imax;
 }
 
+// GausDesc::binint / weight / distance of the restatement, for the pins
+// against the reference-compiled functions.  Return the result length; out
+// holds max(nbins, 1) values.
+int orc_gd_binint(double center, double sigma, double start, double step, int nbins, double* out)
+{
+    auto v = orc::GausDesc{center, sigma}.binint(start, step, nbins);
+    for (size_t i = 0; i < v.size(); ++i) out[i] = v[i];
+    return (int)v.size();
+}
+int orc_gd_weight(double center, double sigma, double start, double step, int nbins, const double* pvec,
+                  double* out)
+{
+    std::vector<double> p(pvec, pvec + nbins);
+    auto v = orc::GausDesc{center, sigma}.weight(start, step, nbins, p);
+    for (size_t i = 0; i < v.size(); ++i) out[i] = v[i];
+    return (int)v.size();
+}
+double orc_gd_distance(double center, double sigma, double x) { return orc::GausDesc{center, sigma}.distance(x); }
+
 }  // extern "C"

@@ -1,0 +1,88 @@
+"""Generate tests/golden/ref_funcs.json from reference code compiled here:
+GausDesc::binint / weight / distance (gen/src/GaussianDiffusion.cxx:30-92,
+gen/inc/WireCellGen/GaussianDiffusion.h:33-49), Waveform::edge
+(util/src/Waveform.cxx:136-153) and Response::coldelec
+(util/src/Response.cxx:311-340), from oracle/_ref/libref_funcs.so (built by
+oracle/Makefile with extract_ref.py and ref_funcs_harness.cpp).
+
+Run from the repository root:  python tests/golden/make_ref_funcs.py"""
+
+import json
+import os
+import sys
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+sys.path.insert(0, os.path.join(ROOT, "oracle"))
+import oracle as O  # noqa: E402
+
+US = 1000.0  # ns
+
+
+def gausdesc_cases(rng, n):
+    """Bin ranges as GaussianDiffusion::set_sampling takes them: the bins
+    covering +-nsigma around the centre on a grid of the given step."""
+    out = []
+    for k in range(n):
+        center = float(rng.uniform(-100.0, 100.0))
+        step = float(rng.uniform(0.1, 5.0))
+        if k % 10 == 0:
+            sigma, nbins = 0.0, 1
+            start = center - float(rng.uniform(0.0, step))
+        else:
+            sigma = float(np.exp(rng.uniform(np.log(1e-2), np.log(50.0))))
+            nsig = float(rng.choice([1.0, 3.0, 5.0]))
+            lo = center - nsig * sigma
+            start = np.floor(lo / step) * step
+            nbins = int(np.ceil((center + nsig * sigma - start) / step))
+            nbins = max(1, min(nbins, 120))
+        out.append(dict(center=center, sigma=sigma, start=float(start), step=step, nbins=nbins,
+                        x=float(center + rng.normal() * (sigma or 1.0))))
+    return out
+
+
+def main():
+    O.build()
+    R = O.ref_funcs()
+    if R is None:
+        raise SystemExit("reference function harness not built (reference tree absent)")
+    rng = np.random.default_rng(2024)
+    gd = []
+    for c in gausdesc_cases(rng, 200):
+        b = O.gd_binint(R, "ref", c["center"], c["sigma"], c["start"], c["step"], c["nbins"])
+        w = O.gd_weight(R, "ref", c["center"], c["sigma"], c["start"], c["step"], len(b), b)
+        d = R.ref_gd_distance(c["center"], c["sigma"], c["x"])
+        gd.append(dict(c, binint=[float(v) for v in b], weight=[float(v) for v in w], distance=d))
+
+    edges = []
+    for k in range(60):
+        n = int(rng.integers(0, 120))
+        w = rng.normal(size=n).astype(np.float32)
+        w[rng.random(n) < rng.uniform(0.0, 1.0)] = 0.0
+        if n and k % 3 == 0:
+            a, b = sorted(rng.integers(0, n, 2))
+            w[:a] = 0.0
+            w[b:] = 0.0
+        if n and k % 7 == 0:
+            w[rng.random(n) < 0.3] = -0.0
+        out = np.zeros(2, dtype=np.int32)
+        R.ref_wave_edge(w.ctypes.data, n, out.ctypes.data)
+        edges.append(dict(wave=[float(v) for v in w], edge=[int(out[0]), int(out[1])]))
+
+    cold = []
+    times = list(np.linspace(-1.0, 12.0, 131) * US) + [0.0, 10.0 * US, 10.0 * US - 1e-9]
+    for gain in (7.8, 14.0):
+        for shaping in (0.5 * US, 1.0 * US, 2.0 * US, 3.0 * US):
+            cold.append(dict(gain=gain, shaping=shaping, time=[float(t) for t in times],
+                             value=[R.ref_coldelec(float(t), gain, shaping) for t in times]))
+
+    out = {"source": ["gen/src/GaussianDiffusion.cxx", "util/src/Waveform.cxx", "util/src/Response.cxx"],
+           "gausdesc": gd, "edge": edges, "coldelec": cold}
+    with open(os.path.join(ROOT, "tests", "golden", "ref_funcs.json"), "w") as f:
+        json.dump(out, f)
+    print("%d GausDesc cases, %d edges, %d coldelec curves" % (len(gd), len(edges), len(cold)))
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,87 @@
+"""Pins against reference functions compiled here from the reference's own
+source (oracle/extract_ref.py + oracle/ref_funcs_harness.cpp): GausDesc bin
+integrals, impact weights and distance (gen/src/GaussianDiffusion.cxx:30-92,
+gen/inc/WireCellGen/GaussianDiffusion.h:33-49), Waveform::edge
+(util/src/Waveform.cxx:136-153) and Response::coldelec
+(util/src/Response.cxx:311-340).  Against the committed vectors
+(tests/golden/ref_funcs.json, written by tests/golden/make_ref_funcs.py) and,
+where the harness was built, live on fresh random cases.  CPU only."""
+
+import json
+import os
+
+import numpy as np
+import pytest
+
+from conftest import ROOT
+
+GOLDEN = os.path.join(ROOT, "tests", "golden", "ref_funcs.json")
+
+
+@pytest.fixture(scope="module")
+def golden():
+    with open(GOLDEN) as f:
+        return json.load(f)
+
+
+def test_gausdesc_against_reference_vectors(oracle, golden):
+    """The oracle's GausDesc (FP64, the arithmetic of the patch bins and the
+    linear impact weights) is bit for bit the reference's."""
+    L = oracle.lib()
+    for c in golden["gausdesc"]:
+        b = oracle.gd_binint(L, "orc", c["center"], c["sigma"], c["start"], c["step"], c["nbins"])
+        assert b.tolist() == c["binint"], c
+        w = oracle.gd_weight(L, "orc", c["center"], c["sigma"], c["start"], c["step"], len(b), b)
+        assert w.tolist() == c["weight"], c
+        assert L.orc_gd_distance(c["center"], c["sigma"], c["x"]) == c["distance"]
+
+
+def test_gausdesc_against_compiled_reference(oracle):
+    R = oracle.ref_funcs()
+    if R is None:
+        pytest.skip("reference function harness not built")
+    L = oracle.lib()
+    rng = np.random.default_rng(99)
+    for _ in range(3000):
+        center = rng.uniform(-3000.0, 3000.0)
+        sigma = 0.0 if rng.random() < 0.05 else np.exp(rng.uniform(np.log(1e-3), np.log(100.0)))
+        step = rng.uniform(0.05, 10.0)
+        start = center - rng.uniform(0.0, 6.0 * (sigma or step))
+        nbins = 1 if sigma == 0.0 else int(rng.integers(1, 80))
+        a = oracle.gd_binint(L, "orc", center, sigma, start, step, nbins)
+        b = oracle.gd_binint(R, "ref", center, sigma, start, step, nbins)
+        assert np.array_equal(a, b)
+        if np.all(a > 0):
+            assert np.array_equal(oracle.gd_weight(L, "orc", center, sigma, start, step, len(a), a),
+                                  oracle.gd_weight(R, "ref", center, sigma, start, step, len(b), b))
+
+
+def test_trace_edges_against_reference(oracle, golden):
+    """Waveform::edge: first non-zero sample and one past the last (-0.0 is zero)."""
+    for e in golden["edge"]:
+        w = np.array(e["wave"], dtype=np.float32)
+        assert list(oracle.edge(w)) == e["edge"]
+    R = oracle.ref_funcs()
+    if R is not None:
+        rng = np.random.default_rng(5)
+        for n in range(0, 64):
+            w = rng.normal(size=n).astype(np.float32)
+            w[rng.random(n) < 0.7] = 0.0
+            out = np.zeros(2, dtype=np.int32)
+            R.ref_wave_edge(w.ctypes.data, n, out.ctypes.data)
+            assert list(oracle.edge(w)) == out.tolist()
+
+
+def test_coldelec_against_reference(golden):
+    """The noise model's cold-electronics response (noise.coldelec, NumPy)
+    against the reference's compiled Response::coldelec: the same terms
+    summed in another order, so equal to rounding (1e-12 of the peak); zero
+    outside (0, 10 us) exactly as the reference."""
+    import importlib
+    noise = importlib.import_module("wire-cell-toolkit_b200.noise")
+    for c in golden["coldelec"]:
+        t = np.array(c["time"])
+        want = np.array(c["value"])
+        got = noise.coldelec(t, c["gain"], c["shaping"])
+        assert np.array_equal(got == 0.0, want == 0.0)
+        assert np.max(np.abs(got - want)) <= 1e-12 * np.max(np.abs(want))
