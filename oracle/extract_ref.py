@@ -5,16 +5,18 @@ into oracle/_ref/ (git-ignored build output) so that oracle/Makefile can
 compile them with ref_funcs_harness.cpp.  The surrounding reference files
 cannot be compiled here (they include Boost, Eigen, jsoncpp or spdlog
 headers); the pieces themselves need only the standard library and the
-reference's own header-only Units.h and Waveform.h.
+reference's own header-only Units.h, Waveform.h, Binning.h and D3Vector.h.
 
   gausdesc_struct.inc  struct GausDesc       gen/inc/WireCellGen/GaussianDiffusion.h
   gausdesc_fns.inc     GausDesc::sample, binint, weight
                                              gen/src/GaussianDiffusion.cxx
   waveform_edge.inc    Waveform::edge        util/src/Waveform.cxx
   coldelec.inc         Response::coldelec    util/src/Response.cxx
+  pimpos_class.inc     class Pimpos          util/inc/WireCellUtil/Pimpos.h
+  pimpos_fns.inc       Pimpos methods        util/src/Pimpos.cxx (all but its #include)
 
 Each piece is found by its declaration (not by line number) and ends at the
-brace that closes it.
+brace that closes it, or at the end of the file for "rest" pieces.
 
 Usage: python extract_ref.py REFERENCE_TREE OUT_DIR"""
 
@@ -31,6 +33,9 @@ PIECES = {
     ],
     "waveform_edge.inc": [("util/src/Waveform.cxx", r"^std::pair<int, int> WireCell::Waveform::edge\(")],
     "coldelec.inc": [("util/src/Response.cxx", r"^double Response::coldelec\(")],
+    "pimpos_class.inc": [("util/inc/WireCellUtil/Pimpos.h", r"^\s*class Pimpos\s*\{")],
+    # the whole file after its one #include line
+    "pimpos_fns.inc": [("util/src/Pimpos.cxx", r"^using namespace WireCell;", "rest")],
 }
 
 
@@ -62,9 +67,17 @@ def main():
     os.makedirs(out, exist_ok=True)
     for name, parts in PIECES.items():
         chunks = []
-        for path, start in parts:
+        for part in parts:
+            path, start = part[0], part[1]
             with open(os.path.join(ref, path)) as f:
-                chunks.append("// %s\n" % path + block(f.read(), start))
+                text = f.read()
+            if len(part) > 2 and part[2] == "rest":
+                m = re.search(start, text, flags=re.M)
+                if m is None:
+                    raise SystemExit("not found: " + start)
+                chunks.append("// %s\n" % path + text[m.start():])
+            else:
+                chunks.append("// %s\n" % path + block(text, start))
         with open(os.path.join(out, name), "w") as f:
             f.write("\n".join(chunks))
 

@@ -102,6 +102,9 @@ def _sig(L, prefix):
         f = getattr(L, prefix + n)
         f.restype = rt
         f.argtypes = at
+    f = getattr(L, prefix + "_pimpos")
+    f.restype = None
+    f.argtypes = [i, d, d, p, p, p, i, i, p, p, p]
     if prefix == "ref":
         L.ref_gd_sigma_range.restype = None
         L.ref_gd_sigma_range.argtypes = [d, d, d, p]
@@ -124,6 +127,19 @@ def gd_weight(L, prefix, center, sigma, start, step, nbins, pvec):
     out = np.zeros(max(nbins, 1))
     n = getattr(L, prefix + "_gd_weight")(center, sigma, start, step, nbins, pv.ctypes.data, out.ctypes.data)
     return out[:n]
+
+
+def pimpos(L, prefix, nwires, minp, maxp, wire, pitch, origin, nbins, pts):
+    """Pimpos(nwires, minp, maxp, wire, pitch, origin, nbins) through library L:
+    ([region nbins, min, max, impact nbins, min, max, axis0, axis1, axis2],
+    pitch coordinates of pts [n][3])."""
+    w, pd, o = (np.ascontiguousarray(v, dtype=np.float64) for v in (wire, pitch, origin))
+    pts = np.ascontiguousarray(pts, dtype=np.float64).reshape(-1, 3)
+    out = np.zeros(15)
+    dist = np.zeros(len(pts))
+    getattr(L, prefix + "_pimpos")(nwires, minp, maxp, w.ctypes.data, pd.ctypes.data, o.ctypes.data, nbins, len(pts),
+                                   pts.ctypes.data, out.ctypes.data, dist.ctypes.data)
+    return out, dist
 
 
 class OrcPlane(C.Structure):

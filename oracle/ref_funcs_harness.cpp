@@ -3,21 +3,30 @@
 // GausDesc struct and its sample/binint/weight
 // (gen/inc/WireCellGen/GaussianDiffusion.h:20-63,
 // gen/src/GaussianDiffusion.cxx:8-92), Waveform::edge
-// (util/src/Waveform.cxx:136-153) and Response::coldelec
-// (util/src/Response.cxx:311-340).  oracle/extract_ref.py cuts them out of
-// the reference tree into oracle/_ref/*.inc and oracle/Makefile compiles this
+// (util/src/Waveform.cxx:136-153), Response::coldelec
+// (util/src/Response.cxx:311-340) and Pimpos (util/inc/WireCellUtil/Pimpos.h,
+// util/src/Pimpos.cxx:5-68).  oracle/extract_ref.py cuts them out of the
+// reference tree into oracle/_ref/*.inc and oracle/Makefile compiles this
 // file with them into oracle/_ref/libref_funcs.so.  They pin the oracle's bin
-// integrals and impact weights, its trace edges and the noise model's
-// cold-electronics response to the reference's compiled code.
+// integrals and impact weights, its trace edges, its plane geometry (pitch
+// coordinate, wire and impact binning) and the noise model's
+// cold-electronics response to the reference's compiled code.  Point and
+// Vector are the reference's D3Vector<double> (util/inc/WireCellUtil/Point.h
+// names them so; that header itself needs jsoncpp).
 #include <cmath>
 #include <iostream>
 #include <utility>
 #include <vector>
 
+#include "WireCellUtil/Binning.h"
+#include "WireCellUtil/D3Vector.h"
 #include "WireCellUtil/Units.h"
 #include "WireCellUtil/Waveform.h"
 
 namespace WireCell {
+typedef D3Vector<double> Point;
+typedef Point Vector;
+#include "pimpos_class.inc"
 namespace Gen {
 #include "gausdesc_struct.inc"
 }
@@ -32,6 +41,7 @@ using namespace std;
 #include "gausdesc_fns.inc"
 #include "waveform_edge.inc"
 #include "coldelec.inc"
+#include "pimpos_fns.inc"
 
 extern "C" {
 // Length of the result; out must hold max(nbins, 1) values.
@@ -64,4 +74,20 @@ void ref_wave_edge(const float* wave, int n, int* out)
     out[1] = r.second;
 }
 double ref_coldelec(double time, double gain, double shaping) { return Response::coldelec(time, gain, shaping); }
+// Pimpos of a plane: out = {region nbins, min, max, impact nbins, min, max,
+// axis0[3], axis1[3], axis2[3]}; pts [n][3] -> dist [n], the pitch
+// coordinate Pimpos::distance(pt, 2).
+void ref_pimpos(int nwires, double minp, double maxp, const double* wire, const double* pitch, const double* origin,
+                int nbins, int n, const double* pts, double* out, double* dist)
+{
+    Pimpos p(nwires, minp, maxp, Vector(wire[0], wire[1], wire[2]), Vector(pitch[0], pitch[1], pitch[2]),
+             Point(origin[0], origin[1], origin[2]), nbins);
+    const Binning& r = p.region_binning();
+    const Binning& i = p.impact_binning();
+    const double head[6] = {(double)r.nbins(), r.min(), r.max(), (double)i.nbins(), i.min(), i.max()};
+    for (int k = 0; k < 6; ++k) out[k] = head[k];
+    for (int a = 0; a < 3; ++a)
+        for (int k = 0; k < 3; ++k) out[6 + 3 * a + k] = p.axis(a)[k];
+    for (int j = 0; j < n; ++j) dist[j] = p.distance(Point(pts[3 * j], pts[3 * j + 1], pts[3 * j + 2]));
+}
 }

@@ -1409,4 +1409,23 @@ int orc_gd_weight(double center, double sigma, double start, double step, int nb
 }
 double orc_gd_distance(double center, double sigma, double x) { return orc::GausDesc{center, sigma}.distance(x); }
 
+// The restatement's Pimpos, laid out as the reference harness's ref_pimpos:
+// out = {region nbins, min, max, impact nbins, min, max, axis0..2}; dist [n]
+// = pitch coordinate of pts [n][3].
+void orc_pimpos(int nwires, double minp, double maxp, const double* wire, const double* pitch, const double* origin,
+                int nbins, int n, const double* pts, double* out, double* dist)
+{
+    orc::Pimpos p(nwires, minp, maxp, orc::V3{wire[0], wire[1], wire[2]}, orc::V3{pitch[0], pitch[1], pitch[2]},
+                  orc::V3{origin[0], origin[1], origin[2]}, nbins);
+    const double head[6] = {(double)p.region.nbins, p.region.minv, p.region.maxv,
+                            (double)p.impact.nbins, p.impact.minv, p.impact.maxv};
+    for (int k = 0; k < 6; ++k) out[k] = head[k];
+    for (int a = 0; a < 3; ++a) {
+        out[6 + 3 * a] = p.axis[a].x;
+        out[7 + 3 * a] = p.axis[a].y;
+        out[8 + 3 * a] = p.axis[a].z;
+    }
+    for (int j = 0; j < n; ++j) dist[j] = p.distance(orc::V3{pts[3 * j], pts[3 * j + 1], pts[3 * j + 2]});
+}
+
 }  // extern "C"

@@ -1,8 +1,9 @@
 """Generate tests/golden/ref_funcs.json from reference code compiled here:
 GausDesc::binint / weight / distance (gen/src/GaussianDiffusion.cxx:30-92,
 gen/inc/WireCellGen/GaussianDiffusion.h:33-49), Waveform::edge
-(util/src/Waveform.cxx:136-153) and Response::coldelec
-(util/src/Response.cxx:311-340), from oracle/_ref/libref_funcs.so (built by
+(util/src/Waveform.cxx:136-153), Response::coldelec
+(util/src/Response.cxx:311-340) and Pimpos (util/src/Pimpos.cxx:5-68), from
+oracle/_ref/libref_funcs.so (built by
 oracle/Makefile with extract_ref.py and ref_funcs_harness.cpp).
 
 Run from the repository root:  python tests/golden/make_ref_funcs.py"""
@@ -42,6 +43,29 @@ def gausdesc_cases(rng, n):
     return out
 
 
+def pimpos_cases(rng, n):
+    """Wire planes as AnodePlane builds Pimpos (gen/src/AnodePlane.cxx:200-219):
+    wire directions at an angle in the (y, z) plane, the pitch direction
+    normal to it (not always unit length), and points in a 2.5 m x 6 m x 2.3 m
+    volume."""
+    out = []
+    for k in range(n):
+        ang = float(rng.choice([0.0, 35.7, -35.7, 60.0])) if k % 4 else float(rng.uniform(-90.0, 90.0))
+        a = np.radians(ang)
+        wire = [0.0, float(np.cos(a)), float(np.sin(a))]
+        s = float(rng.choice([1.0, 3.0, 0.25]))
+        pitch = [0.0, float(-np.sin(a) * s), float(np.cos(a) * s)]
+        nw = int(rng.integers(2, 1200))
+        pw = float(rng.uniform(3.0, 5.0))
+        minp = float(-0.5 * pw * (nw - 1) + rng.uniform(-10.0, 10.0))
+        pts = np.column_stack([rng.uniform(-50.0, 2500.0, 40), rng.uniform(-3000.0, 3000.0, 40),
+                               rng.uniform(-1150.0, 1150.0, 40)])
+        out.append(dict(nwires=nw, minp=minp, maxp=minp + pw * (nw - 1), wire=wire, pitch=pitch,
+                        origin=[float(rng.uniform(-10.0, 100.0)), 0.0, float(rng.uniform(-5.0, 5.0))],
+                        nbins=int(rng.choice([10, 6, 20])), pts=pts.tolist()))
+    return out
+
+
 def main():
     O.build()
     R = O.ref_funcs()
@@ -77,11 +101,19 @@ def main():
             cold.append(dict(gain=gain, shaping=shaping, time=[float(t) for t in times],
                              value=[R.ref_coldelec(float(t), gain, shaping) for t in times]))
 
-    out = {"source": ["gen/src/GaussianDiffusion.cxx", "util/src/Waveform.cxx", "util/src/Response.cxx"],
-           "gausdesc": gd, "edge": edges, "coldelec": cold}
+    pim = []
+    prng = np.random.default_rng(77)
+    for c in pimpos_cases(prng, 24):
+        head, dist = O.pimpos(R, "ref", c["nwires"], c["minp"], c["maxp"], c["wire"], c["pitch"], c["origin"],
+                              c["nbins"], c["pts"])
+        pim.append(dict(c, head=[float(v) for v in head], dist=[float(v) for v in dist]))
+
+    out = {"source": ["gen/src/GaussianDiffusion.cxx", "util/src/Waveform.cxx", "util/src/Response.cxx",
+                      "util/src/Pimpos.cxx"],
+           "gausdesc": gd, "edge": edges, "coldelec": cold, "pimpos": pim}
     with open(os.path.join(ROOT, "tests", "golden", "ref_funcs.json"), "w") as f:
         json.dump(out, f)
-    print("%d GausDesc cases, %d edges, %d coldelec curves" % (len(gd), len(edges), len(cold)))
+    print("%d GausDesc cases, %d edges, %d coldelec curves, %d planes" % (len(gd), len(edges), len(cold), len(pim)))
 
 
 if __name__ == "__main__":

@@ -85,3 +85,31 @@ def test_coldelec_against_reference(golden):
         got = noise.coldelec(t, c["gain"], c["shaping"])
         assert np.array_equal(got == 0.0, want == 0.0)
         assert np.max(np.abs(got - want)) <= 1e-12 * np.max(np.abs(want))
+
+
+def test_pimpos_against_reference(oracle, golden):
+    """The oracle's plane geometry (Pimpos: normalised axes, wire and impact
+    binning, pitch coordinate of a point) is bit for bit the reference's."""
+    L = oracle.lib()
+    for c in golden["pimpos"]:
+        head, dist = oracle.pimpos(L, "orc", c["nwires"], c["minp"], c["maxp"], c["wire"], c["pitch"], c["origin"],
+                                   c["nbins"], c["pts"])
+        assert head.tolist() == c["head"], c["nwires"]
+        assert dist.tolist() == c["dist"], c["nwires"]
+    R = oracle.ref_funcs()
+    if R is None:
+        return
+    rng = np.random.default_rng(123)
+    for _ in range(200):
+        a = rng.uniform(-np.pi, np.pi)
+        wire = [rng.normal() * 1e-3, np.cos(a), np.sin(a)]
+        pitch = np.array([0.0, -np.sin(a), np.cos(a)]) * rng.uniform(0.1, 10.0)
+        nw = int(rng.integers(2, 3000))
+        minp = rng.uniform(-4000.0, 0.0)
+        maxp = minp + rng.uniform(1.0, 8000.0)
+        pts = rng.uniform(-4000.0, 4000.0, (50, 3))
+        origin = rng.uniform(-100.0, 100.0, 3)
+        nb = int(rng.integers(1, 12)) * 2
+        got = oracle.pimpos(L, "orc", nw, minp, maxp, wire, pitch, origin, nb, pts)
+        want = oracle.pimpos(R, "ref", nw, minp, maxp, wire, pitch, origin, nb, pts)
+        assert np.array_equal(got[0], want[0]) and np.array_equal(got[1], want[1])
