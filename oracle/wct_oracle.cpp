@@ -15,6 +15,12 @@
 // Every function cites the reference file:line it restates (paths relative to
 // the wire-cell-toolkit source tree).
 //
+// Pins: Binning, GausDesc (distance, binint, weight), Pimpos and the trace
+// edges equal the reference's own code compiled from its source tree
+// (oracle/_ref, tests/golden/*_ref.json, tests/test_oracle.py and
+// tests/test_ref_funcs.py); the FFT length tables equal the reference's text.
+// No reference test pins whole frames.
+//
 // Deliberate differences from the reference, all without numerical effect
 // beyond double round-off:
 //   * the reference iterates its GaussianDiffusion std::set in heap-pointer
