@@ -17,8 +17,9 @@
 //
 // Pins: Binning, GausDesc (distance, binint, weight), Pimpos and the trace
 // edges equal the reference's own code compiled from its source tree
-// (oracle/_ref, tests/golden/*_ref.json, tests/test_oracle.py and
-// tests/test_ref_funcs.py); the FFT length tables equal the reference's text.
+// (oracle/_ref; tests/golden/binning_ref.json and ref_funcs.json;
+// tests/test_oracle.py and tests/test_ref_funcs.py); the FFT length tables
+// equal the reference's text (tests/golden/fft_lengths_ref.json).
 // No reference test pins whole frames.
 //
 // Deliberate differences from the reference, all without numerical effect
