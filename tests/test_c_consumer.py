@@ -1,8 +1,10 @@
-"""The C ABI from plain C: include/wctb200.h compiles as C99 and as C++, and a
-C program (tests/c_consumer.c) linked against libwctb200.so builds a
+"""The C ABI from plain C: include/wctb200.h compiles as C99 and as C++, its
+structs have the layout of the Python mirrors, and a C program
+(tests/c_consumer.c) linked against libwctb200.so builds a
 PlaneImpactResponse through it with the same results as the Python binding.
 Host-side entry points only; CPU."""
 
+import ctypes
 import os
 import shutil
 import subprocess
@@ -74,3 +76,39 @@ def test_c_program_builds_a_pir(tmp_path, wct, synth):
     waves = out[12 + len(rel):].reshape(info["npaths"], info["nticks"])
     for p in range(info["npaths"]):
         assert np.array_equal(waves[p].astype(np.float32), pir.waveform(p))
+
+
+STRUCTS = {  # C struct of the header -> ctypes mirror in the package
+    "wct_plane_desc": "PlaneDesc",
+    "wct_fr_plane": "FrPlane",
+    "wct_plane_window": "PlaneWindow",
+    "wct_splat_config": "SplatConfig",
+}
+
+
+def test_struct_layouts_match_ctypes(tmp_path, wct):
+    """sizeof and every member's offset of the header's structs, as the C
+    compiler lays them out, equal the Python mirrors' (same member names in
+    the same order)."""
+    _need("gcc")
+    lines = ['#include <stddef.h>', '#include <stdio.h>', '#include "wctb200.h"', "int main(void) {"]
+    for cname, pyname in STRUCTS.items():
+        lines.append('printf("%s size %%zu\\n", sizeof(%s));' % (cname, cname))
+        for f, _ in getattr(wct, pyname)._fields_:
+            lines.append('printf("%s %s %%zu\\n", offsetof(%s, %s));' % (cname, f, cname, f))
+    lines += ["return 0;", "}"]
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines) + "\n")
+    exe = str(tmp_path / "layout")
+    r = subprocess.run(["gcc", "-std=c99", "-Wall", "-Werror", "-I", INCLUDE, str(src), "-o", exe],
+                       capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    got = {}
+    for ln in subprocess.run([exe], capture_output=True, text=True, check=True).stdout.splitlines():
+        c, f, v = ln.split()
+        got[(c, f)] = int(v)
+    for cname, pyname in STRUCTS.items():
+        cls = getattr(wct, pyname)
+        assert got[(cname, "size")] == ctypes.sizeof(cls), cname
+        for f, _ in cls._fields_:
+            assert got[(cname, f)] == getattr(cls, f).offset, (cname, f)

@@ -142,3 +142,51 @@ def test_dt_create_reports_cuda_state(wct):
         with pytest.raises(wct.WctError) as e:
             wct.DepoTransform({})
         assert e.value.code == wct.WCT_ERR_CUDA
+
+
+def _header_prototypes():
+    src = open(HEADER).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    src = re.sub(r"#[^\n]*", "", src)
+    out = {}
+    for m in re.finditer(r"([A-Za-z_][\w \t\*]*?)\b(wct_[a-z0-9_]+)\s*\(([^)]*)\)\s*;", src):
+        ret, name, params = m.group(1), m.group(2), m.group(3).strip()
+        ps = [] if params in ("", "void") else [p.strip() for p in params.split(",")]
+        # drop the parameter name: the last identifier of each parameter
+        types = [re.sub(r"\b\w+$", "", p).strip() if re.search(r"[\w\*]\s*\w+$", p) else p for p in ps]
+        out[name] = (ret.strip(), types)
+    return out
+
+
+# argument classes of the x86-64 LP64 calling convention, which is what a
+# ctypes prototype must match (ctypes itself aliases long long to long and
+# size_t to unsigned long there)
+def _c_kind(t):
+    t = " ".join(t.replace("*", " * ").split())
+    if "*" in t:
+        return "ptr"
+    t = t.replace("const ", "")
+    return {"int": "i32", "long": "i64", "long long": "i64", "double": "f64", "size_t": "u64",
+            "unsigned long long": "u64"}[t]
+
+
+def _ct_kind(c):
+    import ctypes as C
+    if c in (C.c_void_p, C.c_char_p) or (isinstance(c, type) and issubclass(c, C._Pointer)):
+        return "ptr"
+    if C.sizeof(C.c_long) != 8:
+        pytest.skip("an LP64 platform is assumed")
+    return {C.c_int: "i32", C.c_long: "i64", C.c_double: "f64", C.c_ulong: "u64"}[c]
+
+
+def test_python_argtypes_match_header(wct):
+    """Every ctypes prototype has the header's arity and argument classes
+    (pointer, 32-bit int, signed and unsigned 64-bit int, double) and return
+    class."""
+    protos = _header_prototypes()
+    assert sorted(protos) == sorted(wct.SIGNATURES)
+    for name, (rt, at) in wct.SIGNATURES.items():
+        hret, htypes = protos[name]
+        assert len(at) == len(htypes), (name, len(at), htypes)
+        assert [_ct_kind(a) for a in at] == [_c_kind(t) for t in htypes], name
+        assert _ct_kind(rt) == _c_kind(hret), name
