@@ -12,6 +12,7 @@ reference's own header-only Units.h, Waveform.h, Binning.h and D3Vector.h.
                                              gen/src/GaussianDiffusion.cxx
   waveform_edge.inc    Waveform::edge        util/src/Waveform.cxx
   coldelec.inc         Response::coldelec    util/src/Response.cxx
+  digitize.inc         Digitizer::digitize   gen/src/Digitizer.cxx
   pimpos_class.inc     class Pimpos          util/inc/WireCellUtil/Pimpos.h
   pimpos_fns.inc       Pimpos methods        util/src/Pimpos.cxx (all but its #include)
 
@@ -33,6 +34,7 @@ PIECES = {
     ],
     "waveform_edge.inc": [("util/src/Waveform.cxx", r"^std::pair<int, int> WireCell::Waveform::edge\(")],
     "coldelec.inc": [("util/src/Response.cxx", r"^double Response::coldelec\(")],
+    "digitize.inc": [("gen/src/Digitizer.cxx", r"^double Gen::Digitizer::digitize\(")],
     "pimpos_class.inc": [("util/inc/WireCellUtil/Pimpos.h", r"^\s*class Pimpos\s*\{")],
     # the whole file after its one #include line
     "pimpos_fns.inc": [("util/src/Pimpos.cxx", r"^using namespace WireCell;", "rest")],

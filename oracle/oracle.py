@@ -112,6 +112,8 @@ def _sig(L, prefix):
         L.ref_wave_edge.argtypes = [p, i, p]
         L.ref_coldelec.restype = d
         L.ref_coldelec.argtypes = [d, d, d]
+        L.ref_digitize.restype = None
+        L.ref_digitize.argtypes = [p, i, i, p, d, d, d, i, i, p]
 
 
 def gd_binint(L, prefix, center, sigma, start, step, nbins):

@@ -4,13 +4,14 @@
 // (gen/inc/WireCellGen/GaussianDiffusion.h:20-63,
 // gen/src/GaussianDiffusion.cxx:8-92), Waveform::edge
 // (util/src/Waveform.cxx:136-153), Response::coldelec
-// (util/src/Response.cxx:311-340) and Pimpos (util/inc/WireCellUtil/Pimpos.h,
+// (util/src/Response.cxx:311-340), Digitizer::digitize
+// (gen/src/Digitizer.cxx:77-93) and Pimpos (util/inc/WireCellUtil/Pimpos.h,
 // util/src/Pimpos.cxx:5-68).  oracle/extract_ref.py cuts them out of the
 // reference tree into oracle/_ref/*.inc and oracle/Makefile compiles this
 // file with them into oracle/_ref/libref_funcs.so.  They pin the oracle's bin
 // integrals and impact weights, its trace edges, its plane geometry (pitch
-// coordinate, wire and impact binning) and the noise model's
-// cold-electronics response to the reference's compiled code.  Point and
+// coordinate, wire and impact binning), its ADC arithmetic and the noise
+// model's cold-electronics response to the reference's compiled code.  Point and
 // Vector are the reference's D3Vector<double> (util/inc/WireCellUtil/Point.h
 // names them so; that header itself needs jsoncpp).
 #include <cmath>
@@ -29,6 +30,13 @@ typedef Point Vector;
 #include "pimpos_class.inc"
 namespace Gen {
 #include "gausdesc_struct.inc"
+// the members that Digitizer::digitize reads (gen/inc/WireCellGen/Digitizer.h:43-56)
+struct Digitizer {
+    int m_resolution{12};
+    std::vector<double> m_fullscale;
+    bool m_round{false};
+    double digitize(double voltage);
+};
 }
 namespace Response {
 double coldelec(double time, double gain, double shaping);
@@ -42,6 +50,7 @@ using namespace std;
 #include "waveform_edge.inc"
 #include "coldelec.inc"
 #include "pimpos_fns.inc"
+#include "digitize.inc"
 
 extern "C" {
 // Length of the result; out must hold max(nbins, 1) values.
@@ -74,6 +83,24 @@ void ref_wave_edge(const float* wave, int n, int* out)
     out[1] = r.second;
 }
 double ref_coldelec(double time, double gain, double shaping) { return Response::coldelec(time, gain, shaping); }
+// Digitizer::operator() per sample (gen/src/Digitizer.cxx:126-131): the
+// voltage gain * value + baseline (the baseline read into a float), its ADC
+// value from digitize(), stored as a float.
+void ref_digitize(const float* frame, int nrows, int ncols, const float* row_baseline, double gain, double fs_lo,
+                  double fs_hi, int resolution, int round_adc, float* adc)
+{
+    Gen::Digitizer d;
+    d.m_resolution = resolution;
+    d.m_fullscale = {fs_lo, fs_hi};
+    d.m_round = round_adc != 0;
+    for (int r = 0; r < nrows; ++r) {
+        const float baseline = row_baseline[r];
+        for (int c = 0; c < ncols; ++c) {
+            const double voltage = gain * frame[(size_t)r * ncols + c] + baseline;
+            adc[(size_t)r * ncols + c] = d.digitize(voltage);
+        }
+    }
+}
 // Pimpos of a plane: out = {region nbins, min, max, impact nbins, min, max,
 // axis0[3], axis1[3], axis2[3]}; pts [n][3] -> dist [n], the pitch
 // coordinate Pimpos::distance(pt, 2).

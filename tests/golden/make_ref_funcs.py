@@ -2,7 +2,8 @@
 GausDesc::binint / weight / distance (gen/src/GaussianDiffusion.cxx:30-92,
 gen/inc/WireCellGen/GaussianDiffusion.h:33-49), Waveform::edge
 (util/src/Waveform.cxx:136-153), Response::coldelec
-(util/src/Response.cxx:311-340) and Pimpos (util/src/Pimpos.cxx:5-68), from
+(util/src/Response.cxx:311-340), Pimpos (util/src/Pimpos.cxx:5-68) and
+Digitizer::digitize (gen/src/Digitizer.cxx:77-93), from
 oracle/_ref/libref_funcs.so (built by
 oracle/Makefile with extract_ref.py and ref_funcs_harness.cpp).
 
@@ -101,6 +102,21 @@ def main():
             cold.append(dict(gain=gain, shaping=shaping, time=[float(t) for t in times],
                              value=[R.ref_coldelec(float(t), gain, shaping) for t in times]))
 
+    digi = []
+    drng = np.random.default_rng(31)
+    volt = 1.0e-6
+    for gain, resolution in ((1.0, 12), (2.5, 14), (0.7, 10)):
+        for rnd in (0, 1):
+            f = drng.normal(0.0, 0.4 * volt, (8, 60)).astype(np.float32)
+            f[0, :5] = [-5 * volt, 5 * volt, 0.0, 1.1 * volt, -0.9 * volt]
+            base = (np.array([0.9, 0.9, 0.9, 0.9, 0.2, 0.2, 0.2, 0.2]) * volt).astype(np.float32)
+            adc = np.zeros_like(f)
+            R.ref_digitize(f.ctypes.data, f.shape[0], f.shape[1], base.ctypes.data, gain, 0.0, 2.0 * volt, resolution,
+                           rnd, adc.ctypes.data)
+            digi.append(dict(gain=gain, resolution=resolution, round=rnd, fullscale=[0.0, 2.0 * volt],
+                             baseline=[float(v) for v in base], frame=f.astype(float).tolist(),
+                             adc=adc.astype(float).tolist()))
+
     pim = []
     prng = np.random.default_rng(77)
     for c in pimpos_cases(prng, 24):
@@ -109,11 +125,12 @@ def main():
         pim.append(dict(c, head=[float(v) for v in head], dist=[float(v) for v in dist]))
 
     out = {"source": ["gen/src/GaussianDiffusion.cxx", "util/src/Waveform.cxx", "util/src/Response.cxx",
-                      "util/src/Pimpos.cxx"],
-           "gausdesc": gd, "edge": edges, "coldelec": cold, "pimpos": pim}
+                      "util/src/Pimpos.cxx", "gen/src/Digitizer.cxx"],
+           "gausdesc": gd, "edge": edges, "coldelec": cold, "pimpos": pim, "digitize": digi}
     with open(os.path.join(ROOT, "tests", "golden", "ref_funcs.json"), "w") as f:
         json.dump(out, f)
-    print("%d GausDesc cases, %d edges, %d coldelec curves, %d planes" % (len(gd), len(edges), len(cold), len(pim)))
+    print("%d GausDesc cases, %d edges, %d coldelec curves, %d planes, %d digitizer frames"
+          % (len(gd), len(edges), len(cold), len(pim), len(digi)))
 
 
 if __name__ == "__main__":

@@ -113,3 +113,26 @@ def test_pimpos_against_reference(oracle, golden):
         got = oracle.pimpos(L, "orc", nw, minp, maxp, wire, pitch, origin, nb, pts)
         want = oracle.pimpos(R, "ref", nw, minp, maxp, wire, pitch, origin, nb, pts)
         assert np.array_equal(got[0], want[0]) and np.array_equal(got[1], want[1])
+
+
+def test_digitizer_against_reference(oracle, golden):
+    """The oracle's ADC arithmetic (which the GPU digitizer equals bit for bit)
+    against the reference's compiled Digitizer::digitize, sample by sample."""
+    for c in golden["digitize"]:
+        f = np.array(c["frame"], dtype=np.float32)
+        got = oracle.digitize(f, np.array(c["baseline"], dtype=np.float32), c["gain"], tuple(c["fullscale"]),
+                              c["resolution"], bool(c["round"]))
+        assert np.array_equal(got, np.array(c["adc"], dtype=np.float32)), (c["gain"], c["resolution"], c["round"])
+    R = oracle.ref_funcs()
+    if R is None:
+        return
+    rng = np.random.default_rng(8)
+    volt = 1.0e-6
+    for k in range(12):
+        f = rng.normal(0.0, rng.uniform(0.05, 1.5) * volt, (16, 200)).astype(np.float32)
+        base = rng.uniform(0.0, 1.0, 16).astype(np.float32) * np.float32(volt)
+        gain, res, rnd = rng.uniform(0.3, 4.0), int(rng.integers(8, 16)), k % 2
+        fs = (0.0, float(rng.uniform(1.0, 3.0)) * volt)
+        want = np.zeros_like(f)
+        R.ref_digitize(f.ctypes.data, 16, 200, base.ctypes.data, gain, fs[0], fs[1], res, rnd, want.ctypes.data)
+        assert np.array_equal(oracle.digitize(f, base, gain, fs, res, bool(rnd)), want)
