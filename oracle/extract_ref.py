@@ -13,6 +13,9 @@ reference's own header-only Units.h, Waveform.h, Binning.h and D3Vector.h.
   waveform_edge.inc    Waveform::edge        util/src/Waveform.cxx
   coldelec.inc         Response::coldelec    util/src/Response.cxx
   digitize.inc         Digitizer::digitize   gen/src/Digitizer.cxx
+  noise_spectrum.inc   struct NoiseSpectrum  gen/inc/WireCellGen/EmpiricalNoiseModel.h
+  noise_fns.inc        EmpiricalNoiseModel::gen_elec_resp_default, resample
+                                             gen/src/EmpiricalNoiseModel.cxx
   pimpos_class.inc     class Pimpos          util/inc/WireCellUtil/Pimpos.h
   pimpos_fns.inc       Pimpos methods        util/src/Pimpos.cxx (all but its #include)
 
@@ -35,6 +38,11 @@ PIECES = {
     "waveform_edge.inc": [("util/src/Waveform.cxx", r"^std::pair<int, int> WireCell::Waveform::edge\(")],
     "coldelec.inc": [("util/src/Response.cxx", r"^double Response::coldelec\(")],
     "digitize.inc": [("gen/src/Digitizer.cxx", r"^double Gen::Digitizer::digitize\(")],
+    "noise_spectrum.inc": [("gen/inc/WireCellGen/EmpiricalNoiseModel.h", r"^\s*struct NoiseSpectrum\s*\{")],
+    "noise_fns.inc": [
+        ("gen/src/EmpiricalNoiseModel.cxx", r"^void Gen::EmpiricalNoiseModel::gen_elec_resp_default\("),
+        ("gen/src/EmpiricalNoiseModel.cxx", r"^void Gen::EmpiricalNoiseModel::resample\("),
+    ],
     "pimpos_class.inc": [("util/inc/WireCellUtil/Pimpos.h", r"^\s*class Pimpos\s*\{")],
     # the whole file after its one #include line
     "pimpos_fns.inc": [("util/src/Pimpos.cxx", r"^using namespace WireCell;", "rest")],

@@ -114,6 +114,10 @@ def _sig(L, prefix):
         L.ref_coldelec.argtypes = [d, d, d]
         L.ref_digitize.restype = None
         L.ref_digitize.argtypes = [p, i, i, p, d, d, d, i, i, p]
+        L.ref_noise_resample.restype = i
+        L.ref_noise_resample.argtypes = [i, d, i, C.c_float, C.POINTER(d), p, i, p, i, p]
+        L.ref_noise_freqs.restype = None
+        L.ref_noise_freqs.argtypes = [i, d, p]
 
 
 def gd_binint(L, prefix, center, sigma, start, step, nbins):
@@ -129,6 +133,18 @@ def gd_weight(L, prefix, center, sigma, start, step, nbins, pvec):
     out = np.zeros(max(nbins, 1))
     n = getattr(L, prefix + "_gd_weight")(center, sigma, start, step, nbins, pv.ctypes.data, out.ctypes.data)
     return out[:n]
+
+
+def ref_noise_resample(R, fft_length, period, entry):
+    """The reference's EmpiricalNoiseModel::resample of one spectra-file entry
+    (its float fields rounded as asFloat reads them): (constant, amplitudes)."""
+    fr = np.asarray(entry["freqs"], dtype=np.float32)
+    am = np.asarray(entry["amps"], dtype=np.float32)
+    out = np.zeros(max(fft_length, len(am)), dtype=np.float32)
+    c = C.c_double(float(entry.get("const", 0.0)))
+    n = R.ref_noise_resample(fft_length, period, int(entry["nsamples"]), float(np.float32(entry["period"])),
+                             C.byref(c), fr.ctypes.data, len(fr), am.ctypes.data, len(am), out.ctypes.data)
+    return c.value, out[:n]
 
 
 def pimpos(L, prefix, nwires, minp, maxp, wire, pitch, origin, nbins, pts):

@@ -5,13 +5,16 @@
 // gen/src/GaussianDiffusion.cxx:8-92), Waveform::edge
 // (util/src/Waveform.cxx:136-153), Response::coldelec
 // (util/src/Response.cxx:311-340), Digitizer::digitize
-// (gen/src/Digitizer.cxx:77-93) and Pimpos (util/inc/WireCellUtil/Pimpos.h,
+// (gen/src/Digitizer.cxx:77-93), EmpiricalNoiseModel's frequency grid and
+// spectrum resampling (gen/src/EmpiricalNoiseModel.cxx:55-147) and Pimpos
+// (util/inc/WireCellUtil/Pimpos.h,
 // util/src/Pimpos.cxx:5-68).  oracle/extract_ref.py cuts them out of the
 // reference tree into oracle/_ref/*.inc and oracle/Makefile compiles this
 // file with them into oracle/_ref/libref_funcs.so.  They pin the oracle's bin
 // integrals and impact weights, its trace edges, its plane geometry (pitch
 // coordinate, wire and impact binning), its ADC arithmetic and the noise
-// model's cold-electronics response to the reference's compiled code.  Point and
+// model's resampling and cold-electronics response to the reference's
+// compiled code.  Point and
 // Vector are the reference's D3Vector<double> (util/inc/WireCellUtil/Point.h
 // names them so; that header itself needs jsoncpp).
 #include <cmath>
@@ -37,6 +40,19 @@ struct Digitizer {
     bool m_round{false};
     double digitize(double voltage);
 };
+// the members that EmpiricalNoiseModel::gen_elec_resp_default and resample
+// use (gen/inc/WireCellGen/EmpiricalNoiseModel.h:65-125; amplitude_t is
+// IChannelSpectrum's)
+class EmpiricalNoiseModel {
+   public:
+    typedef std::vector<float> amplitude_t;
+#include "noise_spectrum.inc"
+    void gen_elec_resp_default();
+    void resample(NoiseSpectrum& spectrum) const;
+    int m_fft_length{0};
+    double m_period{0};
+    Waveform::realseq_t m_elec_resp_freq;
+};
 }
 namespace Response {
 double coldelec(double time, double gain, double shaping);
@@ -51,6 +67,7 @@ using namespace std;
 #include "coldelec.inc"
 #include "pimpos_fns.inc"
 #include "digitize.inc"
+#include "noise_fns.inc"
 
 extern "C" {
 // Length of the result; out must hold max(nbins, 1) values.
@@ -100,6 +117,38 @@ void ref_digitize(const float* frame, int nrows, int ncols, const float* row_bas
             adc[(size_t)r * ncols + c] = d.digitize(voltage);
         }
     }
+}
+// One spectrum of the noise model's "spectra_file" resampled as configure()
+// does (gen/src/EmpiricalNoiseModel.cxx:175-188,193-221): the model grid of
+// fft_length bins at period; the entry's float fields as read by asFloat.
+// Returns the resampled amplitude count (amps_out holds max(fft_length,
+// namps)); *constant receives the scaled constant.
+int ref_noise_resample(int fft_length, double period, int nsamples, float entry_period, double* constant,
+                       const float* freqs, int nfreqs, const float* amps, int namps, float* amps_out)
+{
+    Gen::EmpiricalNoiseModel m;
+    m.m_fft_length = fft_length;
+    m.m_period = period;
+    m.gen_elec_resp_default();
+    Gen::EmpiricalNoiseModel::NoiseSpectrum ns{};
+    ns.nsamples = nsamples;
+    ns.period = entry_period;
+    ns.constant = *constant;
+    ns.freqs.assign(freqs, freqs + nfreqs);
+    ns.amps.assign(amps, amps + namps);
+    m.resample(ns);
+    *constant = ns.constant;
+    for (size_t i = 0; i < ns.amps.size(); ++i) amps_out[i] = ns.amps[i];
+    return (int)ns.amps.size();
+}
+// The model's frequency grid (gen_elec_resp_default, :55-70), fft_length floats.
+void ref_noise_freqs(int fft_length, double period, float* out)
+{
+    Gen::EmpiricalNoiseModel m;
+    m.m_fft_length = fft_length;
+    m.m_period = period;
+    m.gen_elec_resp_default();
+    for (int i = 0; i < fft_length; ++i) out[i] = m.m_elec_resp_freq[i];
 }
 // Pimpos of a plane: out = {region nbins, min, max, impact nbins, min, max,
 // axis0[3], axis1[3], axis2[3]}; pts [n][3] -> dist [n], the pitch

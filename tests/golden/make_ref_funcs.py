@@ -2,8 +2,9 @@
 GausDesc::binint / weight / distance (gen/src/GaussianDiffusion.cxx:30-92,
 gen/inc/WireCellGen/GaussianDiffusion.h:33-49), Waveform::edge
 (util/src/Waveform.cxx:136-153), Response::coldelec
-(util/src/Response.cxx:311-340), Pimpos (util/src/Pimpos.cxx:5-68) and
-Digitizer::digitize (gen/src/Digitizer.cxx:77-93), from
+(util/src/Response.cxx:311-340), Pimpos (util/src/Pimpos.cxx:5-68),
+Digitizer::digitize (gen/src/Digitizer.cxx:77-93) and EmpiricalNoiseModel's
+resampling (gen/src/EmpiricalNoiseModel.cxx:55-147), from
 oracle/_ref/libref_funcs.so (built by
 oracle/Makefile with extract_ref.py and ref_funcs_harness.cpp).
 
@@ -59,8 +60,8 @@ def pimpos_cases(rng, n):
         nw = int(rng.integers(2, 1200))
         pw = float(rng.uniform(3.0, 5.0))
         minp = float(-0.5 * pw * (nw - 1) + rng.uniform(-10.0, 10.0))
-        pts = np.column_stack([rng.uniform(-50.0, 2500.0, 40), rng.uniform(-3000.0, 3000.0, 40),
-                               rng.uniform(-1150.0, 1150.0, 40)])
+        pts = np.column_stack([rng.uniform(-50.0, 2500.0, 20), rng.uniform(-3000.0, 3000.0, 20),
+                               rng.uniform(-1150.0, 1150.0, 20)])
         out.append(dict(nwires=nw, minp=minp, maxp=minp + pw * (nw - 1), wire=wire, pitch=pitch,
                         origin=[float(rng.uniform(-10.0, 100.0)), 0.0, float(rng.uniform(-5.0, 5.0))],
                         nbins=int(rng.choice([10, 6, 20])), pts=pts.tolist()))
@@ -74,7 +75,7 @@ def main():
         raise SystemExit("reference function harness not built (reference tree absent)")
     rng = np.random.default_rng(2024)
     gd = []
-    for c in gausdesc_cases(rng, 200):
+    for c in gausdesc_cases(rng, 100):
         b = O.gd_binint(R, "ref", c["center"], c["sigma"], c["start"], c["step"], c["nbins"])
         w = O.gd_weight(R, "ref", c["center"], c["sigma"], c["start"], c["step"], len(b), b)
         d = R.ref_gd_distance(c["center"], c["sigma"], c["x"])
@@ -107,7 +108,7 @@ def main():
     volt = 1.0e-6
     for gain, resolution in ((1.0, 12), (2.5, 14), (0.7, 10)):
         for rnd in (0, 1):
-            f = drng.normal(0.0, 0.4 * volt, (8, 60)).astype(np.float32)
+            f = drng.normal(0.0, 0.4 * volt, (8, 24)).astype(np.float32)
             f[0, :5] = [-5 * volt, 5 * volt, 0.0, 1.1 * volt, -0.9 * volt]
             base = (np.array([0.9, 0.9, 0.9, 0.9, 0.2, 0.2, 0.2, 0.2]) * volt).astype(np.float32)
             adc = np.zeros_like(f)
@@ -117,20 +118,44 @@ def main():
                              baseline=[float(v) for v in base], frame=f.astype(float).tolist(),
                              adc=adc.astype(float).tolist()))
 
+    nm = []
+    nrng = np.random.default_rng(55)
+    us = 1000.0
+    for nsamples, period, model_n, kind in ((256, 0.5 * us, 600, "line"), (128, 0.4 * us, 400, "random"),
+                                            (300, 0.5 * us, 500, "inner"), (0, 0.5 * us, 200, "same"),
+                                            (200, 1.0 * us, 560, "random")):
+        L = O.fft_best_length(model_n)
+        nyq = 1.0 / (2 * period)
+        if kind == "line":
+            freqs = np.linspace(0.0, nyq, nsamples // 2 + 1)
+        elif kind == "inner":  # the model grid reaches past both ends: clamped
+            freqs = np.linspace(0.1 * nyq, 0.8 * nyq, 50)
+        elif kind == "same":  # the model's own sampling: kept as given
+            nsamples = L
+            freqs = np.linspace(0.0, nyq, L)
+        else:
+            freqs = np.sort(nrng.uniform(0.0, nyq, 40))
+        amps = nrng.uniform(0.2, 3.0, len(freqs))
+        ent = dict(nsamples=nsamples, period=period, const=float(nrng.uniform(0.0, 0.1)),
+                   freqs=[float(v) for v in np.float32(freqs)], amps=[float(v) for v in np.float32(amps)])
+        const, out = O.ref_noise_resample(R, L, period, ent)
+        nm.append(dict(ent, model_nsamples=model_n, model_period=period, fft_length=L, const_out=const,
+                       amps_out=[float(v) for v in out]))
+
     pim = []
     prng = np.random.default_rng(77)
-    for c in pimpos_cases(prng, 24):
+    for c in pimpos_cases(prng, 12):
         head, dist = O.pimpos(R, "ref", c["nwires"], c["minp"], c["maxp"], c["wire"], c["pitch"], c["origin"],
                               c["nbins"], c["pts"])
         pim.append(dict(c, head=[float(v) for v in head], dist=[float(v) for v in dist]))
 
     out = {"source": ["gen/src/GaussianDiffusion.cxx", "util/src/Waveform.cxx", "util/src/Response.cxx",
-                      "util/src/Pimpos.cxx", "gen/src/Digitizer.cxx"],
-           "gausdesc": gd, "edge": edges, "coldelec": cold, "pimpos": pim, "digitize": digi}
+                      "util/src/Pimpos.cxx", "gen/src/Digitizer.cxx", "gen/src/EmpiricalNoiseModel.cxx"],
+           "gausdesc": gd, "edge": edges, "coldelec": cold, "pimpos": pim, "digitize": digi, "noise_resample": nm}
     with open(os.path.join(ROOT, "tests", "golden", "ref_funcs.json"), "w") as f:
         json.dump(out, f)
-    print("%d GausDesc cases, %d edges, %d coldelec curves, %d planes, %d digitizer frames"
-          % (len(gd), len(edges), len(cold), len(pim), len(digi)))
+    print("%d GausDesc cases, %d edges, %d coldelec curves, %d planes, %d digitizer frames, %d noise spectra"
+          % (len(gd), len(edges), len(cold), len(pim), len(digi), len(nm)))
 
 
 if __name__ == "__main__":

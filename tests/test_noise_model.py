@@ -119,7 +119,8 @@ def _scalar_resample(freq_grid, nsamples_model, ent):
                     lo, hi = j, j + 1
                 else:
                     break
-            mu = (frequency - freqs[lo]) / (freqs[hi] - freqs[lo])
+            # frequency is a double, the entry's freqs are floats: float - float is a float subtraction
+            mu = (frequency - freqs[lo]) / float(np.float32(freqs[hi]) - np.float32(freqs[lo]))
         out.append(float(np.float32((1 - mu) * amps[lo] + mu * amps[hi])))
     return np.array(out)
 

@@ -136,3 +136,39 @@ def test_digitizer_against_reference(oracle, golden):
         want = np.zeros_like(f)
         R.ref_digitize(f.ctypes.data, 16, 200, base.ctypes.data, gain, fs[0], fs[1], res, rnd, want.ctypes.data)
         assert np.array_equal(oracle.digitize(f, base, gain, fs, res, bool(rnd)), want)
+
+
+def _model_entry(e):
+    return dict(plane=0, gain=14.0, shaping=2000.0, wirelen=1000.0, const=e["const"], nsamples=e["nsamples"],
+                period=e["period"], freqs=e["freqs"], amps=e["amps"])
+
+
+def test_noise_resampling_against_reference(golden, oracle):
+    """The noise model's spectrum resampling (noise.EmpiricalNoiseModel, the
+    product's host code) equals the reference's compiled
+    EmpiricalNoiseModel::resample bit for bit: float frequency grid, sqrt(L/n)
+    scale, clamped linear interpolation, float amplitudes."""
+    import importlib
+    noise = importlib.import_module("wire-cell-toolkit_b200.noise")
+    for e in golden["noise_resample"]:
+        m = noise.EmpiricalNoiseModel([_model_entry(e)], nsamples=e["model_nsamples"], period=e["model_period"])
+        assert m.L == e["fft_length"]
+        s = m.planes[0][0]
+        assert s["const"] == e["const_out"]
+        assert np.array_equal(np.asarray(s["amps"], dtype=np.float32), np.array(e["amps_out"], dtype=np.float32))
+    R = oracle.ref_funcs()
+    if R is None:
+        return
+    rng = np.random.default_rng(21)
+    for k in range(20):
+        period = float(rng.choice([400.0, 500.0, 1000.0]))
+        nyq = 1.0 / (2 * period)
+        nf = int(rng.integers(2, 300))
+        freqs = np.sort(rng.uniform(-0.1 * nyq, 1.2 * nyq, nf)).astype(np.float32)
+        e = dict(const=float(rng.uniform(0, 1)), nsamples=int(rng.integers(16, 2000)), period=period,
+                 freqs=list(freqs.astype(float)), amps=list(rng.uniform(0.0, 5.0, nf).astype(np.float32).astype(float)))
+        model_n = int(rng.integers(100, 3000))
+        m = noise.EmpiricalNoiseModel([_model_entry(e)], nsamples=model_n, period=period)
+        const, amps = oracle.ref_noise_resample(R, m.L, period, e)
+        assert m.planes[0][0]["const"] == const
+        assert np.array_equal(np.asarray(m.planes[0][0]["amps"], dtype=np.float32), amps)

@@ -5,7 +5,8 @@ amplitude spectra per plane at several wire lengths (its "spectra_file":
 entries with plane, gain, shaping, wirelen, const, nsamples, period, freqs,
 amps).  At configuration (:96-175) every entry is resampled onto the model's
 frequency grid of L = fft_best_length(nsamples) bins (:58-70: bin i holds
-i / (L period) up to L/2, mirrored above), its amplitudes and constant scaled
+i / (L period) up to L/2, mirrored above, rounded to float as the reference
+stores it), its amplitudes and constant scaled
 by sqrt(L / entry nsamples), by linear interpolation between the entry's
 frequencies (clamped at both ends).  A channel's spectrum (:250-330) is the
 linear interpolation between the plane's entries bracketing the channel's
@@ -54,7 +55,9 @@ class EmpiricalNoiseModel:
         self.L = fft_best_length(self.nsamples)
         L = self.L
         i = np.arange(L)
-        self.freq = np.where(i <= L / 2.0, i / (L * 1.0) / self.period, (L - i) / (L * 1.0) / self.period)
+        # the grid is held in floats (m_elec_resp_freq is a Waveform::realseq_t)
+        f = np.where(i <= L / 2.0, i / (L * 1.0) / self.period, (L - i) / (L * 1.0) / self.period)
+        self.freq = f.astype(np.float32).astype(np.float64)
         self.planes = {}
         self._resp = {}  # shaping step -> response magnitude (L values)
         for e in spectra:  # file order: by wire length within a plane
@@ -84,7 +87,8 @@ class EmpiricalNoiseModel:
             else:
                 lo = int(np.searchsorted(fr, f, side="left")) - 1  # last j with f > fr[j]
                 hi = lo + 1
-                mu = (f - fr[lo]) / (fr[hi] - fr[lo])
+                # the entry's frequencies are floats: their difference is a float subtraction
+                mu = (f - fr[lo]) / float(np.float32(fr[hi]) - np.float32(fr[lo]))
             out[i] = (1 - mu) * amps[lo] + mu * amps[hi]
         s["amps"] = out.astype(np.float32).astype(np.float64)
 
