@@ -133,3 +133,22 @@ def test_resample_matches_scalar_loop():
     m = noise.EmpiricalNoiseModel(ents, nsamples=6000, period=0.5 * US)
     for k in range(3):
         np.testing.assert_array_equal(m.planes[0][k]["amps"], _scalar_resample(m.freq, m.L, ents[k]))
+
+
+def test_channel_spectrum_float_steps():
+    """EmpiricalNoiseModel::channel_spectrum (gen/src/EmpiricalNoiseModel.cxx:357-412)
+    bin by bin with the reference's types: the gain factor cast to float
+    (Waveform::scale), float amplitudes times the float ratio of the float
+    response magnitudes, then sqrt(val * val + constant^2) with the square
+    in float and the rest in double."""
+    import math
+    m = noise.EmpiricalNoiseModel(_entries(), nsamples=6000, period=0.5 * US)
+    wl, gain, shaping = 250 * CM, 1.3 * 14.0, 3.0 * US
+    got = m.channel_spectrum(0, wl, gain, shaping)
+    const, amp = m.interpolate_wire_length(0, int(wl / m.wlres) * m.wlres)
+    r1, r2 = m._response(shaping), m._response(2.0 * US)
+    g = np.float32(gain / 14.0)  # a double quotient cast to float
+    for i in range(0, m.L, 7):
+        a = np.float32(amp[i]) * g
+        a = a * (np.float32(r1[i]) / np.float32(r2[i]))
+        assert got[i] == np.float32(math.sqrt(float(a * a) + const * const)), i

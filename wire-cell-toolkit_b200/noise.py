@@ -18,7 +18,10 @@ from the entries' by more than 1% has its amplitudes scaled by the ratio of
 the cold-electronics response magnitudes (util/src/Response.cxx:311-340,
 sampled at i * period for i < L) at the two shaping times; responses are
 cached by shaping time in 0.1 us steps, the first channel of a step setting
-it (as the reference caches them).
+it (as the reference caches them).  Floats stay floats where the reference
+holds them so (amplitudes, the frequency grid, the response magnitudes, the
+gain factor of Waveform::scale), so the spectra are the reference's bit for
+bit except where its single-precision DFT of the response enters.
 """
 
 import numpy as np
@@ -110,12 +113,17 @@ class EmpiricalNoiseModel:
         raise ValueError("EmpiricalNoiseModel: data corruption")
 
     def _response(self, shaping):
-        """|DFT| of ColdElec(10, shaping) sampled at i * period, i < L (float
-        samples), cached per 0.1 us step of the shaping time."""
+        """|DFT| (float) of ColdElec(10, shaping) generated on the domain
+        [0, L period) in L float samples (Response::Generator::generate,
+        util/src/Response.cxx:267-276: t = i (L period) / L), cached per 0.1 us
+        step of the shaping time.  The reference transforms the float samples
+        with its single-precision IDFT; this one in double, so the magnitudes
+        agree to float rounding."""
         key = int(shaping / US / 0.1)
         if key not in self._resp:
-            sig = coldelec(np.arange(self.L) * self.period, 10.0, shaping).astype(np.float32)
-            self._resp[key] = np.abs(np.fft.fft(sig.astype(np.float64))).astype(np.float32).astype(np.float64)
+            tick = (self.L * self.period - 0.0) / self.L
+            sig = coldelec(0.0 + np.arange(self.L) * tick, 10.0, shaping).astype(np.float32)
+            self._resp[key] = np.abs(np.fft.fft(sig.astype(np.float64))).astype(np.float32)
         return self._resp[key]
 
     def channel_spectrum(self, plane, wire_length, gain=None, shaping=None):
@@ -127,12 +135,15 @@ class EmpiricalNoiseModel:
         const, amp = self.interpolate_wire_length(plane, ilen * self.wlres)
         db_gain = self.planes[plane][0]["gain"]
         db_shaping = self.planes[plane][0]["shaping"]
+        amp = np.asarray(amp, dtype=np.float32)
         if gain is not None and abs(gain - db_gain) > 0.01 * gain:
-            amp = (amp * (gain / db_gain)).astype(np.float32).astype(np.float64)
+            # Waveform::scale(float seq, double) multiplies by the factor cast to float
+            amp = amp * np.float32(gain / db_gain)
         if shaping is not None and abs(shaping - db_shaping) > 0.01 * shaping:
             r1, r2 = self._response(shaping), self._response(db_shaping)
-            amp = (amp * (r1 / r2)).astype(np.float32).astype(np.float64)
-        return np.sqrt(amp * amp + const * const).astype(np.float32)
+            amp = amp * (r1 / r2)  # float amplitudes times a float ratio of float magnitudes
+        # sqrt(val * val + constant^2): the square in float, the sum and root in double
+        return np.sqrt((amp * amp).astype(np.float64) + const * const).astype(np.float32)
 
     def frame_spectra(self, row_plane, row_wire_length, row_gain=None, row_shaping=None):
         """Spectra for ``add_noise``: (spectra [k][L] float32, row_spec [rows])
