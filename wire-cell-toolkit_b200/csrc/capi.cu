@@ -328,10 +328,12 @@ static int configure(Core& c, const std::string& js)
         d.nxr = (int)xr.arr.size();
         for (int i = 0; i < d.nxr; ++i) {
             const auto& r = xr.arr[i];
-            // Drifter::Xregion (gen/src/Drifter.cxx:36-52): cathode may be given
-            // directly or as response + drift length is not supported here.
-            d.xr[i][0] = r["anode"].as_number(0.0);
-            d.xr[i][1] = r["response"].as_number(0.0);
+            // Drifter::Xregion (gen/src/Drifter.cxx:35-52): a missing anode
+            // takes the response plane's x, a missing response the anode's
+            const json::Value& ja = r["anode"].is_null() ? r["response"] : r["anode"];
+            const json::Value& jr = r["response"].is_null() ? r["anode"] : r["response"];
+            d.xr[i][0] = ja.as_number(0.0);
+            d.xr[i][1] = jr.as_number(0.0);
             d.xr[i][2] = r["cathode"].as_number(0.0);
         }
         if (d.speed <= 0) return fail(WCT_ERR_CONFIG, "illegal drift speed");
