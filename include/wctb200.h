@@ -271,7 +271,10 @@ int wct_digitize(const float* frame, int nrows, int ncols, const float* row_base
  * xregions:[{anode, response, cathode}]} to drift depos on the device before
  * the transform (Drifter, gen/src/Drifter.cxx:94-123; fluctuate defaults to
  * false here), "device" (CUDA ordinal) and "seed" (key of the random streams
- * that "fluctuate" draws from, in place of the reference's "rng" component). */
+ * that "fluctuate" draws from, in place of the reference's "rng" component).
+ * WCT_ERR_CONFIG where DepoTransform::configure throws (empty "pirs"), for
+ * malformed JSON, for a non-positive tick, readout_time or drift_speed, a
+ * readout of less than one tick, and integer keys out of their range. */
 int wct_dt_create(const char* json_config, wct_depotransform** out);
 /* The calls below that take a component are serialised on it: configuration
  * calls and forwards from several host threads take turns (as the

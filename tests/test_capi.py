@@ -59,6 +59,10 @@ def test_configuration_errors_are_status_codes(wct):
     h = C.c_void_p()
     assert wct.lib().wct_dt_create(b"{not json", C.byref(h)) == wct.WCT_ERR_CONFIG
     assert wct.lib().wct_last_error()
+    # integer keys out of range, and a readout shorter than one tick, are refused before any device work
+    for bad in ({"seed": -1}, {"seed": 2.0 ** 64}, {"first_frame_number": 1e12}, {"device": -1},
+                {"readout_time": 100.0, "tick": 500.0}, {"readout_time": 1e30}, {"nsigma": 3.0, "tick": 0.0}):
+        assert wct.lib().wct_dt_create(json.dumps(bad).encode(), C.byref(h)) == wct.WCT_ERR_CONFIG, bad
 
 
 def test_null_arguments_are_rejected(wct):

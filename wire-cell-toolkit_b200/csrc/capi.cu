@@ -298,19 +298,30 @@ static int configure(Core& c, const std::string& js)
     }
     c.nsigma = cfg["nsigma"].as_number(c.nsigma);
     c.fluctuate = cfg["fluctuate"].as_bool(false);
-    c.seed = (unsigned long long)cfg["seed"].as_number(0.0);
+    // integer keys: in range before the conversion (an out-of-range conversion is undefined)
+    const double seed = cfg["seed"].as_number(0.0);
+    const double first = cfg["first_frame_number"].as_number(c.frame_count);
+    const double device = cfg["device"].as_number(0.0);
+    if (!(seed >= 0.0 && seed < 18446744073709551616.0))
+        return fail(WCT_ERR_CONFIG, "seed must be a non-negative 64-bit integer");
+    if (!(first >= -2147483648.0 && first <= 2147483647.0))
+        return fail(WCT_ERR_CONFIG, "first_frame_number out of the int range");
+    if (!(device >= 0.0 && device <= 1024.0)) return fail(WCT_ERR_CONFIG, "device must be a CUDA device ordinal");
+    c.seed = (unsigned long long)seed;
     c.readout_time = cfg["readout_time"].as_number(c.readout_time);
     c.tick = cfg["tick"].as_number(c.tick);
     c.start_time = cfg["start_time"].as_number(c.start_time);
     c.drift_speed = cfg["drift_speed"].as_number(c.drift_speed);
-    c.frame_count = (int)cfg["first_frame_number"].as_number(c.frame_count);
-    c.device = (int)cfg["device"].as_number(0);
+    c.frame_count = (int)first;
+    c.device = (int)device;
     if (cfg.has("pirs")) {
         const auto& p = cfg["pirs"];
         if (p.kind != json::Value::Array || p.arr.empty())
             return fail(WCT_ERR_CONFIG, "must configure with some plane impact response components");
     }
     if (c.tick <= 0 || c.readout_time <= 0) return fail(WCT_ERR_CONFIG, "tick and readout_time must be positive");
+    if (!(c.readout_time / c.tick >= 1.0 && c.readout_time / c.tick < 2147483647.0))
+        return fail(WCT_ERR_CONFIG, "readout_time / tick must give between 1 and 2^31 - 1 ticks");
     if (c.drift_speed <= 0) return fail(WCT_ERR_CONFIG, "illegal drift speed");
     const auto& dr = cfg["drifter"];
     if (dr.kind == json::Value::Object) {
