@@ -7,6 +7,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <charconv>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -1384,6 +1385,18 @@ static int forward_batch_device(Core& c, const double* d_depos, const long long*
 // Coordinate search over the launch shapes of the batched path on the
 // caller's batch: each candidate is captured, run once, then timed over three
 // graph replays (CUDA events on the stream); the fastest is kept.
+
+// A time in milliseconds as a JSON number, 4 decimals, independent of the
+// process locale (printf's %f follows LC_NUMERIC, which a host framework may
+// set to a decimal comma).
+static std::string json_ms(double ms)
+{
+    if (!std::isfinite(ms)) return "null";
+    char buf[64];
+    const auto r = std::to_chars(buf, buf + sizeof buf, ms, std::chars_format::fixed, 4);
+    return std::string(buf, r.ptr);
+}
+
 static int autotune_batch(Core& c, const double* d_depos, const long long* offsets, int nev, float* d_frames,
                           cudaStream_t s, std::string& report)
 {
@@ -1416,9 +1429,9 @@ static int autotune_batch(Core& c, const double* d_depos, const long long* offse
         char buf[200];
         std::snprintf(buf, sizeof buf,
                       "%s{\"slots\": %d, \"raster_per_sm\": %d, \"fft_threads\": %d, \"fft_per_sm\": %d, "
-                      "\"conv_per_sm\": %d, \"ms\": %.4f}",
+                      "\"conv_per_sm\": %d, \"ms\": %s}",
                       rows.empty() ? "" : ", ", t.slots, t.raster_per_sm, t.fft_threads, t.fft_per_sm, t.conv_per_sm,
-                      ms);
+                      json_ms(ms).c_str());
         rows += buf;
     };
     BatchTune best = b.tune;
@@ -1457,8 +1470,9 @@ static int autotune_batch(Core& c, const double* d_depos, const long long* offse
     char buf[200];
     std::snprintf(buf, sizeof buf,
                   "{\"best\": {\"slots\": %d, \"raster_per_sm\": %d, \"fft_threads\": %d, \"fft_per_sm\": %d, "
-                  "\"conv_per_sm\": %d, \"ms\": %.4f}, \"tried\": [",
-                  best.slots, best.raster_per_sm, best.fft_threads, best.fft_per_sm, best.conv_per_sm, best_ms);
+                  "\"conv_per_sm\": %d, \"ms\": %s}, \"tried\": [",
+                  best.slots, best.raster_per_sm, best.fft_threads, best.fft_per_sm, best.conv_per_sm,
+                  json_ms(best_ms).c_str());
     report = std::string(buf) + rows + "]}";
     return WCT_OK;
 }
