@@ -545,21 +545,41 @@ def run_reference(args):
     synth = importlib.import_module("wire-cell-toolkit_b200.synth")
     cfg = synth.apa_config()
     depos = synth.apa_depos(seed=2)
-    nth = max(1, min(len(cfg["planes"]), os.cpu_count() or 1))
+    # every host core: each event's planes on their own threads, and as many
+    # independent events at once as the remaining cores take (events share
+    # nothing, as they do in the reference), bounded by a quarter of the free
+    # host memory at ~0.7 GB per event in flight
+    ncpu = os.cpu_count() or 1
+    nth = max(1, min(len(cfg["planes"]), ncpu))
+    nev = max(1, ncpu // nth)
+    try:
+        import psutil
+        nev = max(1, min(nev, int(psutil.virtual_memory().available * 0.25 // (700 << 20))))
+    except Exception:
+        nev = min(nev, 4)
+    nev = min(nev, 64)
+    import concurrent.futures as cf
+    pool = cf.ThreadPoolExecutor(nev)  # the oracle's C call releases the GIL
+
+    def step():
+        list(pool.map(lambda _: O.run(cfg, depos, nthreads=nth), range(nev)))
+
     for _ in range(args.warmup):
-        O.run(cfg, depos, nthreads=nth)
+        step()
     t0 = time.perf_counter()
     for _ in range(args.steps):
-        O.run(cfg, depos, nthreads=nth)
+        step()
     dt = time.perf_counter() - t0
-    value = len(depos) * args.steps / dt
-    sample = "one full-APA event (%d depos) per step, FP32 restatement, planes on %d threads" % (len(depos), nth)
+    pool.shutdown()
+    value = len(depos) * nev * args.steps / dt
+    sample = ("%d full-APA events (%d depos each) at once per step, FP32 restatement, each event's planes on %d "
+              "threads" % (nev, len(depos), nth))
     print(json.dumps({
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt / args.steps * 1e3,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": {"workload": "full-APA plain forward, %d depos per event" % len(depos)},
-        "cpu_baseline": {"value": value, "unit": UNIT, "cores": nth, "kind": "port", "sample": sample},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": nth * nev, "kind": "port", "sample": sample},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }), flush=True)
 
