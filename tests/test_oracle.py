@@ -88,18 +88,24 @@ def test_fft_length_tables_are_the_references():
         assert [int(x) for x in line.split(None, 2)[2].split(",")] == g[key]
 
 
-def test_fft_best_length_every_size(oracle, wct):
+def test_fft_best_length_every_edge(oracle, wct):
     """util/src/FFTBestLength.cxx:52-58: the first table entry >= n while n is
     within the table, else n itself; the even or odd table by n's parity when
-    keep_odd_even.  Every n up to past the tables' end, oracle and product."""
+    keep_odd_even.  Oracle and product at every table entry and its two
+    neighbours, below the first entry, past the last, and at 3000 random n."""
     g = _fft_tables()
 
     def expect(n, keep):
         t = g["any"] if not keep else (g["even"] if n % 2 == 0 else g["odd"])
         return next((e for e in t if e >= n), n)
 
+    ns = set(range(0, 64)) | set(range(16300, 17001))
+    for t in (g["any"], g["even"], g["odd"]):
+        for e in t:
+            ns |= {e - 2, e - 1, e, e + 1, e + 2}
+    ns |= set(int(v) for v in np.random.default_rng(1).integers(0, 17000, 3000))
     for keep in (False, True):
-        for n in range(0, 17001):
+        for n in sorted(v for v in ns if v >= 0):
             e = expect(n, keep)
             assert oracle.fft_best_length(n, keep) == e, (n, keep)
             assert wct.fft_best_length(n, keep) == e, (n, keep)
