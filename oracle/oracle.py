@@ -505,12 +505,13 @@ class OrcSplat(C.Structure):
         [("time_offsets", C.c_double * 3), ("smear_long", C.c_double * 3), ("smear_tran", C.c_double * 3)]
 
 
-def splat(cfg, depos, scfg):
+def splat(cfg, depos, scfg, float_sums=False):
     """DepoFluxSplat's dense truth frame (gen/src/DepoFluxSplat.cxx:247-390) of
     drifted depos for the planes of ``cfg`` (its face cut included):
-    [sum of nwires][nbins] float64.  ``scfg``: tick, window_start,
-    window_duration, nsigma, drift_speed, response_plane, and optional
-    3-lists time_offsets, smear_long, smear_tran."""
+    [sum of nwires][nbins], cells summed in float64, or with ``float_sums``
+    in float32 in depo order as the reference's accumulator does.  ``scfg``:
+    tick, window_start, window_duration, nsigma, drift_speed, response_plane,
+    and optional 3-lists time_offsets, smear_long, smear_tran."""
     job = Job(cfg, depos, drift=False)
     sp = OrcSplat()
     for k in ("tick", "window_start", "window_duration", "nsigma", "drift_speed", "response_plane"):
@@ -521,9 +522,10 @@ def splat(cfg, depos, scfg):
             getattr(sp, k)[i] = float(v[i])
     nbins = int(scfg["window_duration"] / scfg["tick"])
     nrows = sum(p["nwires"] for p in cfg["planes"])
-    out = np.zeros((nrows, nbins))
+    out = np.zeros((nrows, nbins), dtype=np.float32 if float_sums else np.float64)
     L = lib()
-    L.orc_splat.argtypes = [C.POINTER(OrcJob), C.POINTER(OrcSplat), C.c_void_p]
-    if L.orc_splat(C.byref(job.job), C.byref(sp), out.ctypes.data) != 0:
+    f = L.orc_splat_float if float_sums else L.orc_splat
+    f.argtypes = [C.POINTER(OrcJob), C.POINTER(OrcSplat), C.c_void_p]
+    if f(C.byref(job.job), C.byref(sp), out.ctypes.data) != 0:
         raise RuntimeError("orc_splat failed")
     return out

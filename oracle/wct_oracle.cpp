@@ -1326,14 +1326,20 @@ struct OrcSplat {
     double time_offsets[3], smear_long[3], smear_tran[3];
 };
 
-int orc_splat(const OrcJob* job, const OrcSplat* sp, double* frame)
+}  // extern "C"
+
+// The splat with its cells summed in A: double (as the device sums them) or
+// float in depo order (as the reference's dense accumulator sums its float
+// trace charges).
+template <typename A>
+static int splat_impl(const OrcJob* job, const OrcSplat* sp, A* frame)
 {
     try {
         const int nbins = (int)(sp->window_duration / sp->tick);
         orc::Binning tb(nbins, sp->window_start, sp->window_start + nbins * sp->tick);
         std::vector<size_t> row0(job->nplanes + 1, 0);
         for (int p = 0; p < job->nplanes; ++p) row0[p + 1] = row0[p] + job->planes[p].nwires;
-        std::fill(frame, frame + row0[job->nplanes] * (size_t)nbins, 0.0);
+        std::fill(frame, frame + row0[job->nplanes] * (size_t)nbins, (A)0);
         for (int i = 0; i < job->ndepos; ++i) {
             const double* q = job->depos + 7 * (size_t)i;
             orc::Depo d{q[0], q[1], q[2], q[3], q[4], q[5], q[6], i};
@@ -1372,7 +1378,7 @@ int orc_splat(const OrcJob* job, const OrcSplat* sp, double* frame)
                         const int tick = tstart + k;
                         if (tick < 0 || tick >= nbins) continue;
                         frame[(row0[ip] + pbin) * (size_t)nbins + tick] +=
-                            std::abs(patch.val[(size_t)a * patch.nt + k]);
+                            (A)std::abs(patch.val[(size_t)a * patch.nt + k]);
                     }
                 }
             }
@@ -1383,6 +1389,11 @@ int orc_splat(const OrcJob* job, const OrcSplat* sp, double* frame)
         return -1;
     }
 }
+
+extern "C" {
+
+int orc_splat(const OrcJob* job, const OrcSplat* sp, double* frame) { return splat_impl(job, sp, frame); }
+int orc_splat_float(const OrcJob* job, const OrcSplat* sp, float* frame) { return splat_impl(job, sp, frame); }
 
 void orc_edge(const float* wave, int size, int* out)
 {
