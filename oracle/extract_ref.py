@@ -5,7 +5,8 @@ into oracle/_ref/ (git-ignored build output) so that oracle/Makefile can
 compile them with ref_funcs_harness.cpp.  The surrounding reference files
 cannot be compiled here (they include Boost, Eigen, jsoncpp or spdlog
 headers); the pieces themselves need only the standard library and the
-reference's own header-only Units.h, Waveform.h, Binning.h and D3Vector.h.
+reference's own header-only Units.h, Waveform.h, Binning.h, D3Vector.h and
+Interpolate.h.
 
   gausdesc_struct.inc  struct GausDesc       gen/inc/WireCellGen/GaussianDiffusion.h
   gausdesc_fns.inc     GausDesc::sample, binint, weight
@@ -16,6 +17,8 @@ reference's own header-only Units.h, Waveform.h, Binning.h and D3Vector.h.
   noise_spectrum.inc   struct NoiseSpectrum  gen/inc/WireCellGen/EmpiricalNoiseModel.h
   noise_fns.inc        EmpiricalNoiseModel::gen_elec_resp_default, resample
                                              gen/src/EmpiricalNoiseModel.cxx
+  spectrum_fns.inc     Spectrum::conjugate, hermitian_mirror, interp, extrap,
+                       alias, resample       util/inc/WireCellUtil/Spectrum.h
   pimpos_class.inc     class Pimpos          util/inc/WireCellUtil/Pimpos.h
   pimpos_fns.inc       Pimpos methods        util/src/Pimpos.cxx (all but its #include)
 
@@ -42,6 +45,17 @@ PIECES = {
     "noise_fns.inc": [
         ("gen/src/EmpiricalNoiseModel.cxx", r"^void Gen::EmpiricalNoiseModel::gen_elec_resp_default\("),
         ("gen/src/EmpiricalNoiseModel.cxx", r"^void Gen::EmpiricalNoiseModel::resample\("),
+    ],
+    "spectrum_fns.inc": [
+        ("util/inc/WireCellUtil/Spectrum.h", r"^\s*template<typename T>\s*\n\s*std::complex<T> conjugate\("),
+        ("util/inc/WireCellUtil/Spectrum.h", r"^\s*template<typename T> T conjugate\("),
+        ("util/inc/WireCellUtil/Spectrum.h", r"^\s*template<typename It>\s*\n\s*void hermitian_mirror\(It beg"),
+        ("util/inc/WireCellUtil/Spectrum.h",
+         r"^\s*template<typename InputIt, typename OutputIt>\s*\n\s*OutputIt hermitian_mirror\("),
+        ("util/inc/WireCellUtil/Spectrum.h", r"^\s*template<typename InputIt, typename OutputIt>\s*\n\s*void interp\("),
+        ("util/inc/WireCellUtil/Spectrum.h", r"^\s*template<typename InputIt, typename OutputIt>\s*\n\s*void extrap\("),
+        ("util/inc/WireCellUtil/Spectrum.h", r"^\s*template<typename InputIt, typename OutputIt>\s*\n\s*void alias\("),
+        ("util/inc/WireCellUtil/Spectrum.h", r"^\s*template<typename InputIt, typename OutputIt>\s*\n\s*void resample\("),
     ],
     "pimpos_class.inc": [("util/inc/WireCellUtil/Pimpos.h", r"^\s*class Pimpos\s*\{")],
     # the whole file after its one #include line

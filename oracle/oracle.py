@@ -118,6 +118,8 @@ def _sig(L, prefix):
         L.ref_noise_resample.argtypes = [i, d, i, C.c_float, C.POINTER(d), p, i, p, i, p]
         L.ref_noise_freqs.restype = None
         L.ref_noise_freqs.argtypes = [i, d, p]
+        L.ref_group_spectrum.restype = i
+        L.ref_group_spectrum.argtypes = [i, d, i, p, p, d, i, d, p]
 
 
 def gd_binint(L, prefix, center, sigma, start, step, nbins):
@@ -145,6 +147,17 @@ def ref_noise_resample(R, fft_length, period, entry):
     n = R.ref_noise_resample(fft_length, period, int(entry["nsamples"]), float(np.float32(entry["period"])),
                              C.byref(c), fr.ctypes.data, len(fr), am.ctypes.data, len(am), out.ctypes.data)
     return c.value, out[:n]
+
+
+def ref_group_spectrum(R, freqs, amps, nsamples_orig, period_orig, nsamples, tick, scale=1.0):
+    """The reference's GroupNoiseModel treatment of one spectrum (float
+    frequencies and amplitudes as asFloat reads them), or None where it throws."""
+    fr = np.asarray(freqs, dtype=np.float32)
+    am = np.asarray(amps, dtype=np.float32)
+    out = np.zeros(int(nsamples), dtype=np.float32)
+    rc = R.ref_group_spectrum(int(nsamples_orig), float(period_orig), len(fr), fr.ctypes.data, am.ctypes.data,
+                              float(scale), int(nsamples), float(tick), out.ctypes.data)
+    return None if rc else out
 
 
 def pimpos(L, prefix, nwires, minp, maxp, wire, pitch, origin, nbins, pts):

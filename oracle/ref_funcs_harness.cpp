@@ -6,7 +6,9 @@
 // (util/src/Waveform.cxx:136-153), Response::coldelec
 // (util/src/Response.cxx:311-340), Digitizer::digitize
 // (gen/src/Digitizer.cxx:77-93), EmpiricalNoiseModel's frequency grid and
-// spectrum resampling (gen/src/EmpiricalNoiseModel.cxx:55-147) and Pimpos
+// spectrum resampling (gen/src/EmpiricalNoiseModel.cxx:55-147), the group
+// spectra of GroupNoiseModel (gen/src/GroupNoiseModel.cxx:97-146 on
+// util/inc/WireCellUtil/Interpolate.h and Spectrum.h) and Pimpos
 // (util/inc/WireCellUtil/Pimpos.h,
 // util/src/Pimpos.cxx:5-68).  oracle/extract_ref.py cuts them out of the
 // reference tree into oracle/_ref/*.inc and oracle/Makefile compiles this
@@ -18,11 +20,15 @@
 // Vector are the reference's D3Vector<double> (util/inc/WireCellUtil/Point.h
 // names them so; that header itself needs jsoncpp).
 #include <cmath>
+#include <complex>
 #include <iostream>
+#include <stdexcept>
+#include <unordered_map>
 #include <utility>
 #include <vector>
 
 #include "WireCellUtil/Binning.h"
+#include "WireCellUtil/Interpolate.h"
 #include "WireCellUtil/D3Vector.h"
 #include "WireCellUtil/Units.h"
 #include "WireCellUtil/Waveform.h"
@@ -56,6 +62,18 @@ class EmpiricalNoiseModel {
 }
 namespace Response {
 double coldelec(double time, double gain, double shaping);
+}
+// Spectrum's extrap and alias raise their errors with the toolkit's THROW
+// (WireCellUtil/Exceptions.h, which needs Boost): a plain exception here.
+struct errmsg {
+    const char* what;
+};
+struct ValueError {
+    ValueError& operator<<(const errmsg&) { return *this; }
+};
+#define THROW(e) throw std::runtime_error("reference THROW")
+namespace Spectrum {
+#include "spectrum_fns.inc"
 }
 }  // namespace WireCell
 
@@ -149,6 +167,38 @@ void ref_noise_freqs(int fft_length, double period, float* out)
     m.m_period = period;
     m.gen_elec_resp_default();
     for (int i = 0; i < fft_length; ++i) out[i] = m.m_elec_resp_freq[i];
+}
+// GroupNoiseModel::configure's treatment of one spectrum
+// (gen/src/GroupNoiseModel.cxx:97-146), restated line for line around the
+// reference's irrterp, Spectrum::hermitian_mirror and Spectrum::resample:
+// the half spectrum up to Nyquist interpolated onto norig Rayleigh steps,
+// mirrored, and resampled to nsamples at tick.  Returns 0, or -1 where the
+// reference throws (no points below Nyquist).
+int ref_group_spectrum(int norig, double porig, int npts, const float* freqs, const float* amps, double spec_scale,
+                       int nsamples, double tick, float* out)
+{
+    const double Fnyquist = 1.0 / (2 * porig);
+    const double Frayleigh = 1.0 / ((size_t)norig * porig);
+    std::unordered_map<float, float> pts;
+    for (int ind = 0; ind < npts; ++ind) {
+        const float freq = freqs[ind];
+        if (freq > Fnyquist) continue;
+        pts[freq] = spec_scale * amps[ind];
+    }
+    if (pts.empty()) return -1;
+    irrterp<float> terp(pts.begin(), pts.end());
+    std::vector<float> sorig(norig, 0);
+    terp(sorig.begin(), norig, 0, Frayleigh);
+    Spectrum::hermitian_mirror(sorig.begin(), sorig.end());
+    std::vector<float> spec(nsamples, 0);
+    try {
+        Spectrum::resample(sorig.begin(), sorig.end(), spec.begin(), spec.end(), tick / porig);
+    }
+    catch (const std::exception&) {
+        return -1;
+    }
+    for (int i = 0; i < nsamples; ++i) out[i] = spec[i];
+    return 0;
 }
 // Pimpos of a plane: out = {region nbins, min, max, impact nbins, min, max,
 // axis0[3], axis1[3], axis2[3]}; pts [n][3] -> dist [n], the pitch

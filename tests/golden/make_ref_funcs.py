@@ -3,8 +3,9 @@ GausDesc::binint / weight / distance (gen/src/GaussianDiffusion.cxx:30-92,
 gen/inc/WireCellGen/GaussianDiffusion.h:33-49), Waveform::edge
 (util/src/Waveform.cxx:136-153), Response::coldelec
 (util/src/Response.cxx:311-340), Pimpos (util/src/Pimpos.cxx:5-68),
-Digitizer::digitize (gen/src/Digitizer.cxx:77-93) and EmpiricalNoiseModel's
-resampling (gen/src/EmpiricalNoiseModel.cxx:55-147), from
+Digitizer::digitize (gen/src/Digitizer.cxx:77-93), EmpiricalNoiseModel's
+resampling (gen/src/EmpiricalNoiseModel.cxx:55-147) and GroupNoiseModel's
+spectra (gen/src/GroupNoiseModel.cxx:97-146), from
 oracle/_ref/libref_funcs.so (built by
 oracle/Makefile with extract_ref.py and ref_funcs_harness.cpp).
 
@@ -142,6 +143,18 @@ def main():
         nm.append(dict(ent, model_nsamples=model_n, model_period=period, fft_length=L, const_out=const,
                        amps_out=[float(v) for v in out]))
 
+    grp = []
+    grng = np.random.default_rng(91)
+    for porig, norig, ns, tick in ((500.0, 256, 300, 500.0), (500.0, 400, 150, 1000.0), (400.0, 300, 200, 250.0),
+                                   (512.0, 128, 128, 512.0), (500.0, 333, 257, 800.0), (500.0, 200, 301, 200.0)):
+        nf = int(grng.integers(5, 60))
+        f = np.sort(grng.uniform(0.0, 1.2 / (2 * porig), nf)).astype(np.float32)
+        f[0] = 0.0
+        a = grng.uniform(0.0, 3.0, nf).astype(np.float32)
+        out = O.ref_group_spectrum(R, f, a, norig, porig, ns, tick, 1.5)
+        grp.append(dict(freqs=[float(v) for v in f], amps=[float(v) for v in a], nsamples_orig=norig,
+                        period_orig=porig, nsamples=ns, tick=tick, scale=1.5, spectrum=[float(v) for v in out]))
+
     pim = []
     prng = np.random.default_rng(77)
     for c in pimpos_cases(prng, 12):
@@ -150,12 +163,13 @@ def main():
         pim.append(dict(c, head=[float(v) for v in head], dist=[float(v) for v in dist]))
 
     out = {"source": ["gen/src/GaussianDiffusion.cxx", "util/src/Waveform.cxx", "util/src/Response.cxx",
-                      "util/src/Pimpos.cxx", "gen/src/Digitizer.cxx", "gen/src/EmpiricalNoiseModel.cxx"],
-           "gausdesc": gd, "edge": edges, "coldelec": cold, "pimpos": pim, "digitize": digi, "noise_resample": nm}
+                      "util/src/Pimpos.cxx", "gen/src/Digitizer.cxx", "gen/src/EmpiricalNoiseModel.cxx", "gen/src/GroupNoiseModel.cxx"],
+           "gausdesc": gd, "edge": edges, "coldelec": cold, "pimpos": pim, "digitize": digi, "noise_resample": nm,
+           "group_spectrum": grp}
     with open(os.path.join(ROOT, "tests", "golden", "ref_funcs.json"), "w") as f:
         json.dump(out, f)
-    print("%d GausDesc cases, %d edges, %d coldelec curves, %d planes, %d digitizer frames, %d noise spectra"
-          % (len(gd), len(edges), len(cold), len(pim), len(digi), len(nm)))
+    print("%d GausDesc cases, %d edges, %d coldelec curves, %d planes, %d digitizer frames, %d noise spectra, "
+          "%d group spectra" % (len(gd), len(edges), len(cold), len(pim), len(digi), len(nm), len(grp)))
 
 
 if __name__ == "__main__":

@@ -152,3 +152,25 @@ def test_channel_spectrum_float_steps():
         a = np.float32(amp[i]) * g
         a = a * (np.float32(r1[i]) / np.float32(r2[i]))
         assert got[i] == np.float32(math.sqrt(float(a * a) + const * const)), i
+
+
+def test_group_noise_model_groups():
+    """GroupNoiseModel (gen/src/GroupNoiseModel.cxx:84-206): channels map to
+    groups by "group" or "groupID"; a spectrum without a group id takes its
+    position; channels without a group (or a group without a spectrum) get
+    no noise; frame_spectra gives each row its group's spectrum and the group
+    as its random stream."""
+    freqs = list(np.linspace(0.0, 1.0 / (2 * 0.5 * US), 20))
+    spectra = [dict(nsamples=128, period=0.5 * US, freqs=freqs, amps=list(np.linspace(1.0, 2.0, 20))),
+               dict(groupID=7, nsamples=128, period=0.5 * US, freqs=freqs, amps=list(np.linspace(3.0, 1.0, 20)))]
+    groups = [dict(group=0, channels=[10, 11, 12]), dict(groupID=7, channels=[20, 21]), dict(group=9, channels=[30])]
+    m = noise.GroupNoiseModel(spectra, groups, nsamples=256, tick=0.5 * US)
+    assert sorted(m.grp2amp) == [0, 7]
+    assert m.groupid(11) == 0 and m.groupid(21) == 7 and m.groupid(30) == 9 and m.groupid(99) == -1
+    assert m.channel_spectrum(30).size == 0 and m.channel_spectrum(99).size == 0
+    assert m.channel_spectrum(12).shape == (256,) and m.channel_spectrum(12).dtype == np.float32
+    sp, row_spec, row_stream = m.frame_spectra([10, 20, 11, 30, 99, 21])
+    assert sp.shape == (2, 256)
+    assert row_spec.tolist() == [0, 1, 0, -1, -1, 1]
+    assert row_stream.tolist() == [0, 7, 0, -1, -1, 7]
+    assert np.array_equal(sp[1], m.group_spectrum(7))

@@ -172,3 +172,36 @@ def test_noise_resampling_against_reference(golden, oracle):
         const, amps = oracle.ref_noise_resample(R, m.L, period, e)
         assert m.planes[0][0]["const"] == const
         assert np.array_equal(np.asarray(m.planes[0][0]["amps"], dtype=np.float32), amps)
+
+
+def test_group_noise_spectra_against_reference(golden, oracle):
+    """GroupNoiseModel's spectra (noise.group_spectrum, host code) equal the
+    reference's bit for bit: irrterp onto Rayleigh steps, the Hermitian
+    mirror, Spectrum::resample with its aliasing or extrapolation, in the
+    reference's float arithmetic (std::lerp included)."""
+    import importlib
+    noise = importlib.import_module("wire-cell-toolkit_b200.noise")
+    for c in golden["group_spectrum"]:
+        got = noise.group_spectrum(c["freqs"], c["amps"], c["nsamples_orig"], c["period_orig"], c["nsamples"],
+                                   c["tick"], c["scale"])
+        assert np.array_equal(got, np.array(c["spectrum"], dtype=np.float32))
+    R = oracle.ref_funcs()
+    if R is None:
+        return
+    rng = np.random.default_rng(17)
+    for k in range(40):
+        porig = float(rng.choice([400.0, 500.0, 512.0]))
+        nyq = 1.0 / (2 * porig)
+        nf = int(rng.integers(1, 80))
+        f = np.sort(rng.uniform(0.0, 1.3 * nyq, nf)).astype(np.float32)
+        if k % 2:
+            f[0] = 0.0
+        a = rng.uniform(0.0, 3.0, nf).astype(np.float32)
+        norig, ns = int(rng.integers(2, 500)), int(rng.integers(2, 600))
+        tick = float(rng.choice([200.0, 250.0, 500.0, 1000.0]))
+        want = oracle.ref_group_spectrum(R, f, a, norig, porig, ns, tick, 0.8)
+        if want is None:
+            with pytest.raises(ValueError):
+                noise.group_spectrum(f, a, norig, porig, ns, tick, 0.8)
+        else:
+            assert np.array_equal(noise.group_spectrum(f, a, norig, porig, ns, tick, 0.8), want), k

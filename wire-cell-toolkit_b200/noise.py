@@ -158,3 +158,228 @@ class EmpiricalNoiseModel:
                 spectra.append(self.channel_spectrum(int(p), wl, g, sh))
             row_spec[r] = keys[key]
         return np.stack(spectra) if spectra else np.zeros((0, self.L), np.float32), row_spec
+
+
+# ---------------------------------------------------------------------------
+# GroupNoiseModel (gen/src/GroupNoiseModel.cxx): coherent noise spectra per
+# channel group, for add_noise with one random stream per group.  The float
+# arithmetic of the reference's helpers is kept step for step: irrterp and
+# linterp (util/inc/WireCellUtil/Interpolate.h, with std::lerp on floats),
+# Spectrum::hermitian_mirror, interp, extrap, alias and resample
+# (util/inc/WireCellUtil/Spectrum.h).
+# ---------------------------------------------------------------------------
+F32 = np.float32
+
+
+def _lerp(a, b, t):
+    """std::lerp(a, b, t) on floats as the GNU C++ library evaluates it (exact
+    at t = 0 and t = 1, monotonic): the C++20 definition's steps."""
+    a, b, t = F32(a), F32(b), F32(t)
+    if (a <= 0 and b >= 0) or (a >= 0 and b <= 0):
+        return t * b + (F32(1) - t) * a
+    if t == F32(1):
+        return b
+    x = a + t * (b - a)
+    if (t > F32(1)) == (b > a):
+        return x if b < x else b
+    return x if b > x else b
+
+
+def _irrterp(keys, vals, num, xstep):
+    """irrterp<float>(points)(out, num, 0, xstep): num samples from x = 0 in
+    float steps of xstep over the sorted irregular points (keys, vals), flat
+    beyond both ends (Interpolate.h:73-168)."""
+    keys = [F32(k) for k in keys]
+    vals = [F32(v) for v in vals]
+    n = len(keys)
+    xstep = F32(xstep)
+    out = np.zeros(num, dtype=np.float32)
+    if num == 0:
+        return out
+    xcur = F32(0)
+
+    def upper_bound(x):
+        lo, hi = 0, n
+        while lo < hi:
+            mid = (lo + hi) // 2
+            if x < keys[mid]:
+                hi = mid
+            else:
+                lo = mid + 1
+        return lo
+
+    ub = upper_bound(xcur)
+    if num == 1:  # the single-point form, operator()(x)
+        if ub == 0:
+            out[0] = vals[0]
+        elif ub == n:
+            out[0] = vals[-1]
+        else:
+            dX = keys[ub] - keys[ub - 1]
+            dY = vals[ub] - vals[ub - 1]
+            out[0] = vals[ub - 1] + dY * (xcur - keys[ub - 1]) / dX
+        return out
+    for i in range(num):
+        if ub == 0:  # before the domain
+            out[i] = vals[0]
+            xcur = xcur + xstep
+            while xcur > keys[ub]:
+                ub += 1
+                if ub == n:
+                    break
+            continue
+        if ub == n:  # after the domain
+            out[i] = vals[-1]
+            xcur = xcur + xstep
+            continue
+        lb = ub - 1
+        delta = (xcur - keys[lb]) / (keys[ub] - keys[lb])
+        out[i] = _lerp(vals[lb], vals[ub], delta)
+        xcur = xcur + xstep
+        while xcur > keys[ub]:
+            ub += 1
+            if ub == n:
+                break
+    return out
+
+
+def _hermitian_mirror(v):
+    """Spectrum::hermitian_mirror of a real (amplitude) sequence, in place."""
+    n = len(v)
+    mid = n // 2
+    if n % 2:
+        v[mid + 1:] = v[1:mid + 1][::-1]
+    else:
+        v[mid + 1:] = v[1:mid][::-1]
+    return v
+
+
+def _linterpolate(dat, olen):
+    """linterpolate: the input spread over [0, 1) in len(dat) steps (double
+    abscissae, float values), sampled at olen steps of 1 / olen."""
+    ilen = len(dat)
+    step = (1.0 - 0.0) / ilen
+    re = 0.0 + step * (ilen - 1)
+    newdx = (1.0 - 0.0) / olen
+    out = np.zeros(olen, dtype=np.float32)
+    for i in range(olen):
+        x = 0.0 + i * newdx
+        if x <= 0.0:
+            out[i] = dat[0]
+        elif x >= re:
+            out[i] = dat[-1]
+        else:
+            ind = int((x - 0.0) / step)
+            x0 = 0.0 + ind * step
+            out[i] = _lerp(dat[ind], dat[ind + 1], F32((x - x0) / step))
+    return out
+
+
+def _spectrum_resample(sorig, olen, relperiod):
+    """Spectrum::resample: interp to ceil(olen * relperiod) bins (times
+    sqrt(new / old)), then alias (relperiod > 1) or zero-extrapolate."""
+    tmpsiz = int(np.ceil(olen * relperiod))
+    temp = _linterpolate(sorig, tmpsiz)
+    norm = np.sqrt(tmpsiz / float(len(sorig)))
+    temp = (temp.astype(np.float64) * norm).astype(np.float32)
+    ilen = len(temp)
+    out = np.zeros(olen, dtype=np.float32)
+    if ilen == olen:
+        return temp.copy()
+    if relperiod > 1:  # alias
+        if ilen < olen:
+            raise ValueError("alias requires smaller output than input")
+        half = ilen // 2
+        L = int(np.ceil(ilen / float(olen)))
+        M = olen // 2
+        for m in range(M + 1):
+            for l in range(L):
+                old = m + l * M
+                if old > half:
+                    break
+                out[m] = out[m] + temp[old]
+        _hermitian_mirror(out)
+        return (out.astype(np.float64) * np.sqrt(olen / float(ilen))).astype(np.float32)
+    if ilen > olen:  # extrap
+        raise ValueError("extrap requires larger output than input")
+    half = ilen // 2
+    lo, hi, extra = half, half + 1, 1
+    if ilen % 2:
+        lo, extra = lo + 1, 0
+    out[:lo] = temp[:lo]
+    if ilen - hi > 0:
+        out[olen - (ilen - hi):] = temp[hi:]
+    return out  # the middle olen - ilen + extra bins stay at the constant 0
+
+
+def group_spectrum(freqs, amps, nsamples_orig, period_orig, nsamples, tick, scale=1.0):
+    """One spectrum of GroupNoiseModel's "spectra" (gen/src/GroupNoiseModel.cxx:97-146):
+    the points up to Nyquist (amplitudes times ``scale``; a repeated
+    frequency keeps its last amplitude) interpolated onto nsamples_orig
+    Rayleigh steps, mirrored, and resampled to ``nsamples`` bins at ``tick``."""
+    norig, porig = int(nsamples_orig), float(period_orig)
+    if not norig:
+        raise ValueError("GroupNoiseModel: a spectrum lacks nsamples")
+    fnyq = 1.0 / (2 * porig)
+    fray = 1.0 / (norig * porig)
+    pts = {}
+    for f, a in zip(np.asarray(freqs, dtype=np.float32), np.asarray(amps, dtype=np.float32)):
+        if float(f) > fnyq:
+            continue
+        pts[F32(f)] = F32(scale * float(a))
+    if not pts:
+        raise ValueError("GroupNoiseModel: no spectrum points below Nyquist")
+    keys = sorted(pts)
+    sorig = _irrterp(keys, [pts[k] for k in keys], norig, F32(fray))
+    _hermitian_mirror(sorig)
+    return _spectrum_resample(sorig, int(nsamples), float(tick) / porig)
+
+
+class GroupNoiseModel:
+    """GroupNoiseModel (gen/src/GroupNoiseModel.cxx:52-206): ``groups`` =
+    [{group (or groupID), channels}], ``spectra`` = [{group (or groupID;
+    else the entry's position), nsamples, period, freqs, amps}].  The spectra
+    are built at configuration as the reference builds them."""
+
+    def __init__(self, spectra, groups, nsamples=1024, tick=0.5 * US, scale=1.0):
+        self.nsamples = int(nsamples)
+        self.ch2grp = {}
+        for g in groups:
+            gid = g.get("group") if g.get("group") is not None else g.get("groupID")
+            for ch in g["channels"]:
+                self.ch2grp[int(ch)] = int(gid)
+        self.grp2amp = {}
+        for count, s in enumerate(spectra):
+            gid = s.get("group") if s.get("group") is not None else s.get("groupID")
+            group = int(gid) if isinstance(gid, (int, np.integer)) and not isinstance(gid, bool) else count
+            self.grp2amp[group] = group_spectrum(s["freqs"], s["amps"], s["nsamples"], s["period"], self.nsamples,
+                                                 tick, scale)
+
+    def groupid(self, ch):
+        return self.ch2grp.get(int(ch), -1)
+
+    def group_spectrum(self, group):
+        return self.grp2amp.get(int(group), np.zeros(0, dtype=np.float32))
+
+    def channel_spectrum(self, ch):
+        return self.group_spectrum(self.groupid(ch))
+
+    def frame_spectra(self, row_channels):
+        """For coherent ``add_noise``: (spectra [k][nsamples] float32, row_spec,
+        row_stream): each row's group spectrum (-1: no group or no spectrum,
+        the row gets no noise) and the group id as its random stream, so the
+        channels of a group share one waveform."""
+        keys, spectra = {}, []
+        row_spec = np.full(len(row_channels), -1, dtype=np.int32)
+        row_stream = np.full(len(row_channels), -1, dtype=np.int32)
+        for r, ch in enumerate(row_channels):
+            g = self.groupid(ch)
+            if g < 0 or g not in self.grp2amp:
+                continue
+            if g not in keys:
+                keys[g] = len(spectra)
+                spectra.append(self.grp2amp[g])
+            row_spec[r] = keys[g]
+            row_stream[r] = g
+        out = np.stack(spectra) if spectra else np.zeros((0, self.nsamples), np.float32)
+        return out, row_spec, row_stream
