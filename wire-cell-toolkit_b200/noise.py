@@ -1,4 +1,5 @@
-"""Channel noise spectra of the empirical noise model, for ``add_noise``.
+"""Channel noise spectra for ``add_noise``: the empirical (incoherent) noise
+model and, at the end of this module, the group (coherent) noise model.
 
 EmpiricalNoiseModel (gen/src/EmpiricalNoiseModel.cxx) holds measured
 amplitude spectra per plane at several wire lengths (its "spectra_file":
