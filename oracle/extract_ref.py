@@ -15,7 +15,8 @@ Interpolate.h.
   coldelec.inc         Response::coldelec    util/src/Response.cxx
   digitize.inc         Digitizer::digitize   gen/src/Digitizer.cxx
   noise_spectrum.inc   struct NoiseSpectrum  gen/inc/WireCellGen/EmpiricalNoiseModel.h
-  noise_fns.inc        EmpiricalNoiseModel::gen_elec_resp_default, resample
+  noise_fns.inc        EmpiricalNoiseModel::gen_elec_resp_default, resample,
+                       interpolate_wire_length
                                              gen/src/EmpiricalNoiseModel.cxx
   spectrum_fns.inc     Spectrum::conjugate, hermitian_mirror, interp, extrap,
                        alias, resample       util/inc/WireCellUtil/Spectrum.h
@@ -45,6 +46,8 @@ PIECES = {
     "noise_fns.inc": [
         ("gen/src/EmpiricalNoiseModel.cxx", r"^void Gen::EmpiricalNoiseModel::gen_elec_resp_default\("),
         ("gen/src/EmpiricalNoiseModel.cxx", r"^void Gen::EmpiricalNoiseModel::resample\("),
+        ("gen/src/EmpiricalNoiseModel.cxx",
+         r"^Gen::EmpiricalNoiseModel::spectrum_data_t\s*\nGen::EmpiricalNoiseModel::interpolate_wire_length\("),
     ],
     "spectrum_fns.inc": [
         ("util/inc/WireCellUtil/Spectrum.h", r"^\s*template<typename T>\s*\n\s*std::complex<T> conjugate\("),

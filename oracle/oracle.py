@@ -118,6 +118,8 @@ def _sig(L, prefix):
         L.ref_noise_resample.argtypes = [i, d, i, C.c_float, C.POINTER(d), p, i, p, i, p]
         L.ref_noise_freqs.restype = None
         L.ref_noise_freqs.argtypes = [i, d, p]
+        L.ref_noise_interp.restype = i
+        L.ref_noise_interp.argtypes = [i, p, p, p, i, d, C.POINTER(d), p]
         L.ref_group_spectrum.restype = i
         L.ref_group_spectrum.argtypes = [i, d, i, p, p, d, i, d, p]
 

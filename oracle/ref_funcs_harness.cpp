@@ -5,8 +5,9 @@
 // gen/src/GaussianDiffusion.cxx:8-92), Waveform::edge
 // (util/src/Waveform.cxx:136-153), Response::coldelec
 // (util/src/Response.cxx:311-340), Digitizer::digitize
-// (gen/src/Digitizer.cxx:77-93), EmpiricalNoiseModel's frequency grid and
-// spectrum resampling (gen/src/EmpiricalNoiseModel.cxx:55-147), the group
+// (gen/src/Digitizer.cxx:77-93), EmpiricalNoiseModel's frequency grid,
+// spectrum resampling and wire-length interpolation
+// (gen/src/EmpiricalNoiseModel.cxx:55-147,232-275), the group
 // spectra of GroupNoiseModel (gen/src/GroupNoiseModel.cxx:97-146 on
 // util/inc/WireCellUtil/Interpolate.h and Spectrum.h) and Pimpos
 // (util/inc/WireCellUtil/Pimpos.h,
@@ -22,6 +23,7 @@
 #include <cmath>
 #include <complex>
 #include <iostream>
+#include <map>
 #include <stdexcept>
 #include <unordered_map>
 #include <utility>
@@ -55,9 +57,12 @@ class EmpiricalNoiseModel {
 #include "noise_spectrum.inc"
     void gen_elec_resp_default();
     void resample(NoiseSpectrum& spectrum) const;
+    using spectrum_data_t = std::pair<double, amplitude_t>;
+    spectrum_data_t interpolate_wire_length(int plane, double wire_length) const;
     int m_fft_length{0};
     double m_period{0};
     Waveform::realseq_t m_elec_resp_freq;
+    std::map<int, std::vector<NoiseSpectrum*> > m_spectral_data;
 };
 }
 namespace Response {
@@ -158,6 +163,30 @@ int ref_noise_resample(int fft_length, double period, int nsamples, float entry_
     *constant = ns.constant;
     for (size_t i = 0; i < ns.amps.size(); ++i) amps_out[i] = ns.amps[i];
     return (int)ns.amps.size();
+}
+// EmpiricalNoiseModel::interpolate_wire_length (:232-275) over nspec spectra
+// of one plane (in file order: wire lengths ascending), each namps floats.
+// Returns 0, or -1 where the reference throws.
+int ref_noise_interp(int nspec, const double* wirelen, const double* constant, const float* amps, int namps,
+                     double wire_length, double* const_out, float* amps_out)
+{
+    std::vector<Gen::EmpiricalNoiseModel::NoiseSpectrum> specs(nspec);
+    Gen::EmpiricalNoiseModel m;
+    for (int k = 0; k < nspec; ++k) {
+        specs[k].wirelen = wirelen[k];
+        specs[k].constant = constant[k];
+        specs[k].amps.assign(amps + (size_t)k * namps, amps + (size_t)(k + 1) * namps);
+        m.m_spectral_data[0].push_back(&specs[k]);
+    }
+    try {
+        auto r = m.interpolate_wire_length(0, wire_length);
+        *const_out = r.first;
+        for (size_t i = 0; i < r.second.size(); ++i) amps_out[i] = r.second[i];
+        return 0;
+    }
+    catch (const std::exception&) {
+        return -1;
+    }
 }
 // The model's frequency grid (gen_elec_resp_default, :55-70), fft_length floats.
 void ref_noise_freqs(int fft_length, double period, float* out)

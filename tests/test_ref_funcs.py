@@ -205,3 +205,37 @@ def test_group_noise_spectra_against_reference(golden, oracle):
                 noise.group_spectrum(f, a, norig, porig, ns, tick, 0.8)
         else:
             assert np.array_equal(noise.group_spectrum(f, a, norig, porig, ns, tick, 0.8), want), k
+
+
+def test_noise_wire_length_interpolation_against_reference(oracle):
+    """EmpiricalNoiseModel::interpolate_wire_length (gen/src/EmpiricalNoiseModel.cxx:232-275):
+    clamped at the shortest and longest entries, linear in between (float
+    amplitudes, double constant), bit for bit against the compiled reference."""
+    import ctypes as C
+    import importlib
+    noise = importlib.import_module("wire-cell-toolkit_b200.noise")
+    R = oracle.ref_funcs()
+    if R is None:
+        pytest.skip("reference function harness not built")
+    rng = np.random.default_rng(5)
+    L = 400
+    freqs = list(np.linspace(0.0, 1.0 / (2 * 500.0), 60))
+    for k in range(10):
+        nspec = int(rng.integers(1, 5))
+        lens = np.sort(rng.uniform(500.0, 8000.0, nspec)).astype(np.float32).astype(np.float64)
+        ents = [dict(plane=0, gain=14.0, shaping=2000.0, wirelen=float(wl), const=float(rng.uniform(0, 0.1)),
+                     nsamples=L, period=500.0, freqs=freqs, amps=list(rng.uniform(0.1, 3.0, 60)))
+                for wl in lens]
+        m = noise.EmpiricalNoiseModel(ents, nsamples=L, period=500.0)
+        sp = m.planes[0]
+        wls = np.array([s["wirelen"] for s in sp])
+        cs = np.array([s["const"] for s in sp])
+        am = np.ascontiguousarray(np.stack([np.asarray(s["amps"], dtype=np.float32) for s in sp]))
+        for wl in list(rng.uniform(0.0, 9000.0, 20)) + list(wls):
+            c = C.c_double()
+            out = np.zeros(am.shape[1], dtype=np.float32)
+            assert R.ref_noise_interp(len(sp), wls.ctypes.data, cs.ctypes.data, am.ctypes.data, am.shape[1], float(wl),
+                                      C.byref(c), out.ctypes.data) == 0
+            const, amp = m.interpolate_wire_length(0, float(wl))
+            assert const == c.value
+            assert np.array_equal(np.asarray(amp, dtype=np.float32), out)
