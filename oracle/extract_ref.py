@@ -20,6 +20,7 @@ Interpolate.h.
                                              gen/src/EmpiricalNoiseModel.cxx
   spectrum_fns.inc     Spectrum::conjugate, hermitian_mirror, interp, extrap,
                        alias, resample       util/inc/WireCellUtil/Spectrum.h
+  generatorn.inc       GeneratorN::spec      aux/src/NoiseTools.cxx
   pimpos_class.inc     class Pimpos          util/inc/WireCellUtil/Pimpos.h
   pimpos_fns.inc       Pimpos methods        util/src/Pimpos.cxx (all but its #include)
 
@@ -60,6 +61,7 @@ PIECES = {
         ("util/inc/WireCellUtil/Spectrum.h", r"^\s*template<typename InputIt, typename OutputIt>\s*\n\s*void alias\("),
         ("util/inc/WireCellUtil/Spectrum.h", r"^\s*template<typename InputIt, typename OutputIt>\s*\n\s*void resample\("),
     ],
+    "generatorn.inc": [("aux/src/NoiseTools.cxx", r"^complex_vector_t\s*\nGeneratorN::spec\(")],
     "pimpos_class.inc": [("util/inc/WireCellUtil/Pimpos.h", r"^\s*class Pimpos\s*\{")],
     # the whole file after its one #include line
     "pimpos_fns.inc": [("util/src/Pimpos.cxx", r"^using namespace WireCell;", "rest")],

@@ -120,6 +120,8 @@ def _sig(L, prefix):
         L.ref_noise_freqs.argtypes = [i, d, p]
         L.ref_noise_interp.restype = i
         L.ref_noise_interp.argtypes = [i, p, p, p, i, d, C.POINTER(d), p]
+        L.ref_generator_spec.restype = i
+        L.ref_generator_spec.argtypes = [i, p, p, i, p]
         L.ref_group_spectrum.restype = i
         L.ref_group_spectrum.argtypes = [i, d, i, p, p, d, i, d, p]
 
@@ -491,13 +493,13 @@ def digitize(frame, row_baseline, gain=1.0, fullscale=(0.0, 2.0e-6), resolution=
     return adc.astype(np.float32)
 
 
-def noise_wave(spectrum, normals):
-    """One noise waveform as IncoherentAddNoise makes it
-    (gen/src/AddNoise.cxx:79-84 and aux/src/NoiseTools.cxx GeneratorN::spec,
-    ::wave), float64: sigma_k = S_k * sqrt(2 / 3.141592); for k <= N/2 +
-    (N even) the bin is sigma_k (n_k, n_{k + N/2}); DC and (N even) Nyquist
-    become their modulus; the spectrum is made Hermitian and inverted with
-    1/N.  ``normals`` holds at least 2 (N/2 + (N even)) + 1 standard normals."""
+def noise_spec(spectrum, normals):
+    """The spectrum of one noise waveform as IncoherentAddNoise makes it
+    (gen/src/AddNoise.cxx:79-84 and aux/src/NoiseTools.cxx GeneratorN::spec),
+    float64: sigma_k = S_k * sqrt(2 / 3.141592); for k <= N/2 + (N even) the
+    bin is sigma_k (n_k, n_{k + N/2}); DC and (N even) Nyquist become their
+    modulus; the spectrum is made Hermitian.  ``normals`` holds at least
+    2 (N/2 + (N even)) + 1 standard normals."""
     S = np.asarray(spectrum, dtype=np.float64)
     n = S.size
     nextra = (n + 1) % 2
@@ -511,7 +513,13 @@ def noise_wave(spectrum, normals):
         spec[nhalf] = abs(spec[nhalf])
     for k in range(1, (n + 1) // 2):  # Hermitian mirror
         spec[n - k] = np.conj(spec[k])
-    return np.real(np.fft.ifft(spec))
+    return spec
+
+
+def noise_wave(spectrum, normals):
+    """One noise waveform as IncoherentAddNoise makes it: the inverse DFT
+    (with 1/N) of ``noise_spec``."""
+    return np.real(np.fft.ifft(noise_spec(spectrum, normals)))
 
 
 class OrcSplat(C.Structure):

@@ -9,7 +9,9 @@
 // spectrum resampling and wire-length interpolation
 // (gen/src/EmpiricalNoiseModel.cxx:55-147,232-275), the group
 // spectra of GroupNoiseModel (gen/src/GroupNoiseModel.cxx:97-146 on
-// util/inc/WireCellUtil/Interpolate.h and Spectrum.h) and Pimpos
+// util/inc/WireCellUtil/Interpolate.h and Spectrum.h), the noise
+// generator's spectrum (GeneratorN::spec, aux/src/NoiseTools.cxx:178-204) and
+// Pimpos
 // (util/inc/WireCellUtil/Pimpos.h,
 // util/src/Pimpos.cxx:5-68).  oracle/extract_ref.py cuts them out of the
 // reference tree into oracle/_ref/*.inc and oracle/Makefile compiles this
@@ -22,6 +24,7 @@
 // names them so; that header itself needs jsoncpp).
 #include <cmath>
 #include <complex>
+#include <functional>
 #include <iostream>
 #include <map>
 #include <stdexcept>
@@ -80,6 +83,18 @@ struct ValueError {
 namespace Spectrum {
 #include "spectrum_fns.inc"
 }
+// the parts of aux/inc/WireCellAux/NoiseTools.h:19-20,237-253 that
+// GeneratorN::spec uses: its types and the source of normal variates
+namespace Aux::NoiseTools {
+using real_vector_t = std::vector<float>;
+using complex_vector_t = std::vector<std::complex<float> >;
+class GeneratorN {
+   public:
+    using normal_f = std::function<real_vector_t(size_t n)>;
+    normal_f normal;
+    complex_vector_t spec(const real_vector_t& sigmas);
+};
+}  // namespace Aux::NoiseTools
 }  // namespace WireCell
 
 using namespace WireCell;
@@ -91,6 +106,9 @@ using namespace std;
 #include "pimpos_fns.inc"
 #include "digitize.inc"
 #include "noise_fns.inc"
+using namespace WireCell::Spectrum;
+using namespace WireCell::Aux::NoiseTools;
+#include "generatorn.inc"
 
 extern "C" {
 // Length of the result; out must hold max(nbins, 1) values.
@@ -182,6 +200,28 @@ int ref_noise_interp(int nspec, const double* wirelen, const double* constant, c
         auto r = m.interpolate_wire_length(0, wire_length);
         *const_out = r.first;
         for (size_t i = 0; i < r.second.size(); ++i) amps_out[i] = r.second[i];
+        return 0;
+    }
+    catch (const std::exception&) {
+        return -1;
+    }
+}
+// GeneratorN::spec (aux/src/NoiseTools.cxx:178-204) of n sigmas with the
+// given normals (2 (n/2 + (n even)) + 1 of them): the complex spectrum as n
+// (re, im) float pairs.  Returns 0, or -1 where the reference throws.
+int ref_generator_spec(int n, const float* sigmas, const float* normals, int nnormals, float* out)
+{
+    Aux::NoiseTools::GeneratorN g;
+    g.normal = [&](size_t k) {
+        if ((int)k > nnormals) throw std::runtime_error("too few normals");
+        return Aux::NoiseTools::real_vector_t(normals, normals + k);
+    };
+    try {
+        auto spec = g.spec(Aux::NoiseTools::real_vector_t(sigmas, sigmas + n));
+        for (int i = 0; i < n; ++i) {
+            out[2 * i] = spec[i].real();
+            out[2 * i + 1] = spec[i].imag();
+        }
         return 0;
     }
     catch (const std::exception&) {

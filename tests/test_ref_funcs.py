@@ -239,3 +239,25 @@ def test_noise_wire_length_interpolation_against_reference(oracle):
             const, amp = m.interpolate_wire_length(0, float(wl))
             assert const == c.value
             assert np.array_equal(np.asarray(amp, dtype=np.float32), out)
+
+
+def test_noise_generator_spectrum_against_reference(oracle):
+    """The oracle's noise spectrum (oracle.noise_spec, which the GPU noise is
+    checked against in distribution) against the reference's compiled
+    GeneratorN::spec given the same normals: the same bins draw the same
+    normals, DC and Nyquist by modulus, the same Hermitian mirror; equal to
+    float rounding (the reference multiplies in float)."""
+    R = oracle.ref_funcs()
+    if R is None:
+        pytest.skip("reference function harness not built")
+    rng = np.random.default_rng(12)
+    for n in (3, 4, 5, 16, 17, 255, 256, 1000, 1001):
+        S = rng.uniform(0.0, 2.0, n)
+        nn = 2 * (n // 2 + (n + 1) % 2) + 1
+        normals = rng.normal(size=nn).astype(np.float32)
+        sig = (S * np.sqrt(2.0 / 3.141592)).astype(np.float32)
+        out = np.zeros(2 * n, dtype=np.float32)
+        assert R.ref_generator_spec(n, sig.ctypes.data, normals.ctypes.data, nn, out.ctypes.data) == 0
+        want = out[0::2].astype(np.float64) + 1j * out[1::2].astype(np.float64)
+        got = oracle.noise_spec(sig.astype(np.float64) / np.sqrt(2.0 / 3.141592), normals.astype(np.float64))
+        assert np.abs(got - want).max() <= 1e-6 * np.abs(want).max(), n
