@@ -7,9 +7,17 @@ straight muon tracks with one depo per 0.1 mm (~520k depos), drift + diffusion
 + erf patches + FFT convolution + frame.  One step = one event through
 DepoTransform::operator() with its depos already resident in HBM.
 
-Output: one JSON line (rank 0).  Multi-GPU: one process per GPU (torchrun),
-every rank simulates its own event (events are independent: weak scaling, no
-data-path collective).
+Output: one JSON line (rank 0).  Multi-GPU: one process per GPU; `--gpus N`
+starts the N ranks itself (torch.distributed.run on 127.0.0.1) unless a
+launcher already did, and refuses a launcher's world that is not N.  Every
+rank simulates its own event (events are independent: weak scaling, no
+data-path collective); times are the slowest rank's.
+
+"cpu_baseline": the CPU restatement of the reference (oracle/, FP32) on the
+same event, one thread, transforms by libtorch-CPU (MKL; the reference's
+TorchDFT backend), plane responses built once; 1 warm-up, median of 5, split
+by stage.  "parity": that leg's checker run, the FP64 oracle's frame of the
+same event against the GPU frame (rel-L2, windows), outside the timed region.
 
 On one GPU the line also carries "patterns": forward + adjoint on 20k track
 depos (full-APA geometry), a batch of 64 uneven full-APA events through one
@@ -20,7 +28,7 @@ with CUDA events on the launch stream (skip with --no-patterns,
 --no-calibration).
 
 ``--impl reference`` times the CPU restatement of the reference (oracle/,
-FP32, one event per step) on the host cores instead.
+FP32, MKL transforms, one event per step) on every host core instead.
 """
 
 import argparse
@@ -112,10 +120,50 @@ class ClockSampler:
 
 
 def dist_setup(args):
+    """Rank, world size and local rank of this process (torch.distributed.run
+    sets them; a plain run is rank 0 of 1).  A world that is not the --gpus
+    count the caller asked for is an error, never a relabelled result."""
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args is not None and world != args.gpus:
+        raise SystemExit("bench.py: --gpus %d but WORLD_SIZE=%d" % (args.gpus, world))
     return rank, world, local
+
+
+def free_port():
+    import socket
+    with socket.socket(socket.AF_INET, socket.SOCK_STREAM) as so:
+        so.bind(("127.0.0.1", 0))
+        return so.getsockname()[1]
+
+
+def relaunch(nproc, script, argv, timeout_s=None):
+    """Run `script argv` as nproc ranks of one node (one process per GPU)
+    under torch.distributed.run on 127.0.0.1 and return its exit status."""
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", "--nproc-per-node", str(nproc),
+           "--master-addr", "127.0.0.1", "--master-port", str(free_port()), script] + list(argv)
+    env = dict(os.environ, OMP_NUM_THREADS=os.environ.get("OMP_NUM_THREADS", "4"))
+    return subprocess.run(cmd, env=env, timeout=timeout_s).returncode
+
+
+def init_group(world, backend="nccl", timeout_s=120):
+    """The process group of a multi-rank run (a short timeout, so ranks that
+    wait for a missing peer end with an error)."""
+    if world <= 1:
+        return
+    import datetime
+    import torch.distributed as dist
+    dist.init_process_group(backend, timeout=datetime.timedelta(seconds=timeout_s))
+
+
+def max_over_ranks(x, world, device="cuda"):
+    """The largest of each rank's x (the whole job's time is the slowest rank's)."""
+    import torch
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    if world > 1:
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    return float(t.item())
 
 
 STAGE_KERNELS = {"raster": "k_fill + k_raster_wires", "time_fft": "k_rfft_rows x planes",
@@ -152,10 +200,7 @@ def run_b200(args):
     import torch
     rank, world, local = dist_setup(args)
     torch.cuda.set_device(local)
-    if world > 1:
-        import datetime
-        import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    init_group(world, "nccl")
     wct = importlib.import_module("wire-cell-toolkit_b200")
     synth = importlib.import_module("wire-cell-toolkit_b200.synth")
     cfg = synth.apa_config()
@@ -208,10 +253,8 @@ def run_b200(args):
     clk = clocks.stop()
     total_ms = sum(a.elapsed_time(b) for a, b in evs)
     stages, launches = dt.stage_times(reset=True)
-    t = torch.tensor([total_ms], dtype=torch.float64, device="cuda")
-    if world > 1:
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-    max_ms = float(t.item())
+    max_ms = max_over_ranks(total_ms, world)
+    gpu_frame = d_frame.cpu().numpy() if rank == 0 else None  # the last timed step's frame
     total_depos = n * world
     value = total_depos * args.steps / (max_ms / 1e3)
 
@@ -228,10 +271,7 @@ def run_b200(args):
     for _ in range(args.steps):
         dt(hd, out=hf)
     e2e_s = time.perf_counter() - t0
-    te = torch.tensor([e2e_s], dtype=torch.float64, device="cuda")
-    if world > 1:
-        torch.distributed.all_reduce(te, op=torch.distributed.ReduceOp.MAX)
-    e2e_value = total_depos * args.steps / float(te.item())
+    e2e_value = total_depos * args.steps / max_over_ranks(e2e_s, world)
 
     # --- roofline of the dominant stage (live CUDA events on the launch stream).
     # A "launch" here is one execution of the stage for one event (all planes):
@@ -305,8 +345,8 @@ def run_b200(args):
                 result["patterns"]["calibration"] = calibration(wct, synth, torch, local)
             except Exception as e:
                 result["patterns"]["calibration"] = {"error": repr(e)[:300]}
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        result["cpu_baseline"] = cpu_baseline(cfg, depos, nthreads=1)
+    if rank == 0 and not args.no_cpu_baseline:
+        result["cpu_baseline"], result["parity"] = cpu_baseline(cfg, depos, gpu_frame, wins, timed=world == 1)
     if rank == 0:
         print(json.dumps(result), flush=True)
     if world > 1:
@@ -522,26 +562,80 @@ def calibration(wct, synth, torch, local, nevents=16, ndepos=4_000_000, steps=20
     return out
 
 
-def cpu_baseline(cfg, depos, nthreads=1):
-    """The oracle (FP32 restatement of the reference) on one full event."""
+def host_cpu():
+    """Model name and logical core count of this host."""
+    model = "unknown"
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    model = line.split(":", 1)[1].strip()
+                    break
+    except OSError:
+        pass
+    return {"model": model, "logical_cores": os.cpu_count()}
+
+
+def cpu_baseline(cfg, depos, gpu_frame=None, gpu_windows=None, timed=True, reps=5):
+    """The CPU restatement of the reference (oracle/, FP32) on the bench's own
+    full event, one thread: its transforms through libtorch-CPU (Intel MKL),
+    the reference's TorchDFT backend, the plane responses built once as the
+    reference's configured PlaneImpactResponse is; one warm-up run, then the
+    median of `reps` runs, split into the reference's stages.  Also the
+    checker of this event: the FP64 oracle's frame against the GPU frame
+    (rel-L2, windows), outside every timed region.  Returns (baseline or
+    None when not timed, parity)."""
+    import torch
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle as O
     O.lib()
-    t0 = time.perf_counter()
-    O.run(cfg, depos, nthreads=nthreads)
-    dt = time.perf_counter() - t0
-    return {"value": len(depos) / dt, "unit": UNIT, "cores": nthreads, "kind": "port",
-            "sample": "one full-APA event (%d depos), FP32 restatement, %d thread(s), %.1f s" %
-                      (len(depos), nthreads, dt)}
+    parity = None
+    if gpu_frame is not None:
+        ref = O.run(cfg, depos, fp64=True, nthreads=min(3, os.cpu_count() or 1))
+        r = np.concatenate(ref["frames"])
+        g = gpu_frame.astype(np.float64)
+        keys = ("start_ch", "end_ch", "start_tick", "end_tick", "ndepos_added", "outside_time", "outside_pitch")
+        same = all(all(w[k] == o[k] for k in keys) for w, o in zip(gpu_windows, ref["windows"]))
+        parity = {"rel_l2_vs_fp64": float(np.linalg.norm(g - r) / np.linalg.norm(r)), "tolerance": 1e-5,
+                  "windows_and_counters_equal": bool(same),
+                  "event": "the benchmarked event (%d depos), last timed step's frame" % len(depos)}
+    if not timed:
+        return None, parity
+    nth0 = torch.get_num_threads()
+    torch.set_num_threads(1)
+    O.set_fft_backend("mkl")
+    try:
+        O.run(cfg, depos, nthreads=1)  # warm-up: plane responses, transform plans
+        runs = []
+        for _ in range(reps):
+            t0 = time.perf_counter()
+            res = O.run(cfg, depos, nthreads=1, stages=True)
+            runs.append((time.perf_counter() - t0, res["stages"]))
+    finally:
+        O.set_fft_backend("own")
+        torch.set_num_threads(nth0)
+    med = statistics.median(t for t, _ in runs)
+    stages = {k: statistics.median(st[k] for _, st in runs) for k in O.STAGES}
+    return ({"value": len(depos) / med, "unit": UNIT, "cores": 1, "kind": "port",
+             "sample": "the benchmarked full-APA event (%d depos), FP32 restatement, one thread; transforms by "
+                       "libtorch-CPU (MKL, the reference's TorchDFT backend); plane responses built once; 1 warm-up, "
+                       "median of %d runs (%.2f s)" % (len(depos), reps, med),
+             "seconds_median": med, "seconds_runs": [t for t, _ in runs],
+             "stages_s_median": stages, "host_cpu": host_cpu()}, parity)
 
 
 def run_reference(args):
     rank, world, local = dist_setup(args)
     if rank != 0:
         return
+    import torch
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle as O
     O.lib()
+    # transforms through libtorch-CPU (MKL), the reference's TorchDFT backend;
+    # one intra-op thread per call, the parallelism is over planes and events
+    torch.set_num_threads(1)
+    O.set_fft_backend("mkl")
     synth = importlib.import_module("wire-cell-toolkit_b200.synth")
     cfg = synth.apa_config()
     depos = synth.apa_depos(seed=2)
@@ -573,13 +667,14 @@ def run_reference(args):
     pool.shutdown()
     value = len(depos) * nev * args.steps / dt
     sample = ("%d full-APA events (%d depos each) at once per step, FP32 restatement, each event's planes on %d "
-              "threads" % (nev, len(depos), nth))
+              "threads, transforms by libtorch-CPU (MKL), plane responses built once" % (nev, len(depos), nth))
     print(json.dumps({
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt / args.steps * 1e3,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": {"workload": "full-APA plain forward, %d depos per event" % len(depos)},
-        "cpu_baseline": {"value": value, "unit": UNIT, "cores": nth * nev, "kind": "port", "sample": sample},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": nth * nev, "kind": "port", "sample": sample,
+                         "host_cpu": host_cpu()},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }), flush=True)
 
@@ -596,6 +691,11 @@ def main():
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
+    if args.gpus < 1:
+        raise SystemExit("bench.py: --gpus must be at least 1")
+    if args.gpus > 1 and "WORLD_SIZE" not in os.environ:
+        # one process per GPU: start the ranks here when no launcher did
+        sys.exit(relaunch(args.gpus, os.path.abspath(__file__), sys.argv[1:]))
     if args.impl == "reference":
         run_reference(args)
     else:

@@ -147,8 +147,10 @@ int wct_convolve_rows_device(const float* in, long ld_in, int nrows, int n_in, c
  * device image, held by every GPU that loads the library until the process
  * exits; a call needs (nrows + 3) * nfft / 2 <= 4194304 complex values and
  * returns WCT_ERR_SIZE beyond that.  The first call on a device looks up the
- * array's address (cudaGetSymbolAddress) with that device current; make that
- * first call before any stream capture.  All calls share the array and each
+ * array's address (cudaGetSymbolAddress) with that device current and keeps
+ * it for the life of the process; make that first call before any stream
+ * capture, and make no call on a device after a cudaDeviceReset of it (the
+ * kept address would be stale).  All calls share the array and each
  * overwrites what it uses: calls that overlap on the GPU (other streams or
  * threads) race, so serialise them. */
 int wct_convolve_rows_device_noalloc(const float* in, long ld_in, int nrows, int n_in, const float* resp,
@@ -304,6 +306,24 @@ int wct_dt_set_response_table(wct_depotransform* dt, int face, int plane, int ng
                               double pitch, double impact, int waveform_pad, const float* table);
 /* Frame geometry: total wire rows and nticks. */
 int wct_dt_frame_shape(const wct_depotransform* dt, int* nrows, int* nticks);
+
+/* DepoTransform::modify_depo (gen/inc/WireCellGen/DepoTransform.h:33-35),
+ * the per-plane hook a subclass overrides to rescale each depo's charge
+ * before BinnedDiffusion_transform::add (gen/src/DepoTransform.cxx:182;
+ * dQ/dx calibrations of larwirecell and uboonecode), as data: depo i brings
+ * charge * scale[i * nplanes + p] to plane p (p over every plane of every
+ * face, in frame order), after the drift and the face's sensitive-volume
+ * cut, before the rejection tests, the patch normalisation and the
+ * fluctuation draws.  scale has ndepos * nplanes doubles, in host memory
+ * (on_device = 0) or device memory of the component's device (on_device !=
+ * 0); it is copied, and the copy is complete when the call returns.  It holds
+ * for every later forward, batched forward (ndepos = the batch's total, depos
+ * concatenated) and adjoint call with exactly ndepos depos and the same
+ * planes; other counts return WCT_ERR_ARG.  The adjoint's charge gradient
+ * carries the scale.  scale == NULL removes it.  Work already enqueued on
+ * other streams must be done with the previous scale before this call
+ * overwrites it (synchronise those streams first). */
+int wct_dt_set_charge_scale(wct_depotransform* dt, const double* scale, size_t ndepos, int on_device);
 
 /* DepoTransform::operator() (gen/src/DepoTransform.cxx:155-224) on host
  * buffers: depos [ndepos][7] in, dense frame [nrows][nticks] out, one window

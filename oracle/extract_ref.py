@@ -23,6 +23,16 @@ Interpolate.h.
   generatorn.inc       GeneratorN::spec      aux/src/NoiseTools.cxx
   pimpos_class.inc     class Pimpos          util/inc/WireCellUtil/Pimpos.h
   pimpos_fns.inc       Pimpos methods        util/src/Pimpos.cxx (all but its #include)
+  idepo_class.inc      class IDepo           iface/inc/WireCellIface/IDepo.h
+  simpledepo_class.inc class SimpleDepo      aux/inc/WireCellAux/SimpleDepo.h
+  simpledepo_fns.inc   SimpleDepo methods    aux/src/SimpleDepo.cxx (all but its #include)
+  drifter_structs.inc  Drifter's DepoTimeCompare, Xregion, IsInsideBulk,
+                       IsInsideResp          gen/inc/WireCellGen/Drifter.h
+  drifter_fns.inc      DepoTimeCompare::operator(), the Xregion constructor,
+                       inside_response, inside_bulk, Drifter::insert
+                                             gen/src/Drifter.cxx
+  bdt_add.inc          BinnedDiffusion_transform::add
+                                             gen/src/BinnedDiffusion_transform.cxx
 
 Each piece is found by its declaration (not by line number) and ends at the
 brace that closes it, or at the end of the file for "rest" pieces.
@@ -65,6 +75,23 @@ PIECES = {
     "pimpos_class.inc": [("util/inc/WireCellUtil/Pimpos.h", r"^\s*class Pimpos\s*\{")],
     # the whole file after its one #include line
     "pimpos_fns.inc": [("util/src/Pimpos.cxx", r"^using namespace WireCell;", "rest")],
+    "idepo_class.inc": [("iface/inc/WireCellIface/IDepo.h", r"^\s*class IDepo : public IData<IDepo>\s*\{")],
+    "simpledepo_class.inc": [("aux/inc/WireCellAux/SimpleDepo.h", r"^\s*class SimpleDepo : public WireCell::IDepo\s*\{")],
+    "simpledepo_fns.inc": [("aux/src/SimpleDepo.cxx", r"^using namespace WireCell::Aux;", "rest")],
+    "drifter_structs.inc": [
+        ("gen/inc/WireCellGen/Drifter.h", r"^\s*struct DepoTimeCompare\s*\{"),
+        ("gen/inc/WireCellGen/Drifter.h", r"^\s*struct Xregion\s*\{"),
+        ("gen/inc/WireCellGen/Drifter.h", r"^\s*struct IsInsideBulk\s*\{"),
+        ("gen/inc/WireCellGen/Drifter.h", r"^\s*struct IsInsideResp\s*\{"),
+    ],
+    "drifter_fns.inc": [
+        ("gen/src/Drifter.cxx", r"^bool Gen::Drifter::DepoTimeCompare::operator\(\)"),
+        ("gen/src/Drifter.cxx", r"^Gen::Drifter::Xregion::Xregion\(Configuration cfg\)"),
+        ("gen/src/Drifter.cxx", r"^bool Gen::Drifter::Xregion::inside_response\("),
+        ("gen/src/Drifter.cxx", r"^bool Gen::Drifter::Xregion::inside_bulk\("),
+        ("gen/src/Drifter.cxx", r"^bool Gen::Drifter::insert\("),
+    ],
+    "bdt_add.inc": [("gen/src/BinnedDiffusion_transform.cxx", r"^bool Gen::BinnedDiffusion_transform::add\(")],
 }
 
 

@@ -105,6 +105,12 @@ def _sig(L, prefix):
     f = getattr(L, prefix + "_pimpos")
     f.restype = None
     f.argtypes = [i, d, d, p, p, p, i, i, p, p, p]
+    f = getattr(L, prefix + "_drift_one")
+    f.restype = i
+    f.argtypes = [p, i, d, d, d, d, d, p, p]
+    f = getattr(L, prefix + "_bdt_add")
+    f.restype = i
+    f.argtypes = [i, d, d, p, p, p, i, i, d, d, d, p, d, d, p]
     if prefix == "ref":
         L.ref_gd_sigma_range.restype = None
         L.ref_gd_sigma_range.argtypes = [d, d, d, p]
@@ -164,6 +170,90 @@ def ref_group_spectrum(R, freqs, amps, nsamples_orig, period_orig, nsamples, tic
     return None if rc else out
 
 
+def drift_one(L, prefix, c):
+    """Drifter::insert of one depo (fluctuation off) through library L (the
+    oracle "orc" or the reference harness "ref"): (kept, drifted depo)."""
+    xr = np.ascontiguousarray(c["xregions"], dtype=np.float64).reshape(-1, 3)
+    dep = np.ascontiguousarray(c["depo"], dtype=np.float64)
+    out = np.zeros(7)
+    k = getattr(L, prefix + "_drift_one")(xr.ctypes.data, xr.shape[0], c["DL"], c["DT"], c["lifetime"], c["speed"],
+                                          c["toffset"], dep.ctypes.data, out.ctypes.data)
+    return k, out
+
+
+def bdt_add(L, prefix, c):
+    """BinnedDiffusion_transform::add of one depo through library L:
+    (added, [outside_time, outside_pitch])."""
+    pl = c["plane"]
+    w = np.ascontiguousarray(pl["wire"], dtype=np.float64)
+    pi = np.ascontiguousarray(pl["pitch"], dtype=np.float64)
+    o = np.ascontiguousarray(pl["origin"], dtype=np.float64)
+    dep = np.ascontiguousarray(c["depo"], dtype=np.float64)
+    cnt = np.zeros(2, dtype=np.int32)
+    k = getattr(L, prefix + "_bdt_add")(pl["nwires"], pl["minp"], pl["maxp"], w.ctypes.data, pi.ctypes.data,
+                                        o.ctypes.data, pl["nimp"], c["ntbins"], c["tmin"], c["tmax"], c["nsigma"],
+                                        dep.ctypes.data, c["sigma_time"], c["sigma_pitch"], cnt.ctypes.data)
+    return k, cnt.tolist()
+
+
+def drift_cases(rng, n):
+    """Depos for the Drifter::insert pin: one face, two mirrored faces or a
+    region without an anode; positions across and exactly on the anode,
+    response and cathode planes; zero, negative and positive charge."""
+    out = []
+    for k in range(n):
+        kind = k % 3
+        if kind == 0:
+            xr = [[0.0, 100.0, 2700.0]]
+        elif kind == 1:
+            xr = [[0.0, 100.0, 2700.0], [0.0, -100.0, -2700.0]]
+        else:
+            xr = [[100.0, 100.0, -2500.0]]  # anode taken from the response plane
+        planes = [v for r in xr for v in r]
+        x = float(rng.choice(planes)) if k % 5 == 0 else float(rng.uniform(-2800.0, 2800.0))
+        q = 0.0 if k % 11 == 0 else float(rng.choice([-1.0, 1.0]) * rng.uniform(1.0, 1e5))
+        out.append(dict(xregions=xr, DL=float(rng.uniform(5.0, 10.0) * 1e-7), DT=float(rng.uniform(8.0, 15.0) * 1e-7),
+                        lifetime=float(rng.uniform(3.0, 30.0) * 1e6), speed=float(rng.uniform(1.0, 2.0) * 1e-3),
+                        toffset=float(rng.choice([0.0, rng.uniform(-1e4, 1e4)])),
+                        depo=[float(rng.uniform(-1e5, 3e6)), q, x, float(rng.uniform(-3000.0, 3000.0)),
+                              float(rng.uniform(-2300.0, 2300.0)), float(rng.choice([0.0, rng.uniform(0.0, 30.0)])),
+                              float(rng.choice([0.0, rng.uniform(0.0, 3.0)]))]))
+    return out
+
+
+def bdt_add_cases(rng, n):
+    """Depos for the BinnedDiffusion_transform::add pin: random planes (as
+    AnodePlane builds Pimpos), readout windows, widths including 0, centres
+    within a few sigma of the window and impact-range edges, some exactly
+    nsigma away."""
+    out = []
+    for k in range(n):
+        ang = np.radians(float(rng.choice([0.0, 35.7, -35.7, rng.uniform(-90.0, 90.0)])))
+        wire = [0.0, float(np.cos(ang)), float(np.sin(ang))]
+        pdir = np.array([0.0, -np.sin(ang), np.cos(ang)])
+        nw = int(rng.integers(2, 1000))
+        pw = float(rng.uniform(3.0, 5.0))
+        minp = -0.5 * pw * (nw - 1)
+        plane = dict(nwires=nw, minp=minp, maxp=minp + pw * (nw - 1), wire=wire, pitch=pdir.tolist(),
+                     origin=[100.0, 0.0, 0.0], nimp=int(rng.choice([10, 6])))
+        ntb = int(rng.choice([6000, 1000]))
+        tick = float(rng.choice([500.0, 400.0]))
+        tmin = float(rng.choice([0.0, -1000.0]))
+        nsigma = float(rng.choice([3.0, 2.5]))
+        st = 0.0 if k % 7 == 0 else float(np.exp(rng.uniform(np.log(1.0), np.log(3000.0))))
+        sp = 0.0 if k % 5 == 0 else float(np.exp(rng.uniform(np.log(0.01), np.log(10.0))))
+        tedge = tmin if rng.random() < 0.5 else tmin + ntb * tick
+        t = tedge + (rng.choice([-1.0, 1.0]) * nsigma * st if k % 4 == 0 else rng.uniform(-5.0, 5.0) * (st or 100.0))
+        lo, hi = minp - 0.5 * pw, minp + pw * (nw - 1) + 0.5 * pw
+        pedge = lo if rng.random() < 0.5 else hi
+        c = pedge + (rng.choice([-1.0, 1.0]) * nsigma * sp if k % 6 == 0 else rng.uniform(-5.0, 5.0) * (sp or 1.0))
+        pos = np.array(plane["origin"]) + c * pdir + rng.uniform(-1000.0, 1000.0) * np.array(wire)
+        out.append(dict(plane=plane, ntbins=ntb, tmin=tmin, tmax=tmin + ntb * tick, nsigma=nsigma,
+                        depo=[float(t), -1000.0, float(pos[0]), float(pos[1]), float(pos[2]), 0.0, 0.0],
+                        sigma_time=st, sigma_pitch=sp))
+    return out
+
+
 def pimpos(L, prefix, nwires, minp, maxp, wire, pitch, origin, nbins, pts):
     """Pimpos(nwires, minp, maxp, wire, pitch, origin, nbins) through library L:
     ([region nbins, min, max, impact nbins, min, max, axis0, axis1, axis2],
@@ -204,6 +294,9 @@ class OrcJob(C.Structure):
         ("fp64", C.c_int), ("nthreads", C.c_int),
         ("fluctuate", C.c_int), ("drift_fluctuate", C.c_int), ("seed", C.c_ulonglong),
         ("nlong", C.c_int), ("long_len", C.c_void_p), ("long_wave", C.c_void_p), ("long_padding", C.c_double),
+        ("stage_s", C.c_void_p),
+        ("nfaces", C.c_int), ("face_bb", C.c_void_p), ("face_have_bb", C.c_void_p), ("plane_face", C.c_void_p),
+        ("charge_scale", C.c_void_p),
     ]
 
 
@@ -216,7 +309,7 @@ class Job:
     """Owns the numpy buffers an OrcJob points into."""
 
     def __init__(self, cfg, depos, drift=True, fp64=False, nthreads=1, fluctuate=False, drift_fluctuate=False,
-                 seed=0):
+                 seed=0, charge_scale=None):
         self.keep = []
         j = OrcJob()
         j.fluctuate = 1 if fluctuate else 0
@@ -281,6 +374,28 @@ class Job:
         self.keep.append(planes)
         j.nplanes = len(cfg["planes"])
         j.planes = C.cast(planes, C.c_void_p)
+        if cfg.get("faces"):
+            # several anode faces: each face's box and each plane's face
+            fl = cfg["faces"]
+            fb = np.zeros((len(fl), 6), dtype=np.float64)
+            fh = np.zeros(len(fl), dtype=np.int32)
+            pf = np.full(j.nplanes, -1, dtype=np.int32)
+            for f, face in enumerate(fl):
+                if face.get("bb") is not None:
+                    fb[f, :3] = face["bb"][0]
+                    fb[f, 3:] = face["bb"][1]
+                    fh[f] = 1
+                for k in face["planes"]:
+                    pf[k] = f
+            assert (pf >= 0).all(), "every plane belongs to a face"
+            j.nfaces = len(fl)
+            j.face_bb = self._arr(fb).ctypes.data
+            j.face_have_bb = self._arr(fh).ctypes.data
+            j.plane_face = self._arr(pf).ctypes.data
+        if charge_scale is not None:
+            cs = self._arr(np.ascontiguousarray(charge_scale, dtype=np.float64))
+            assert cs.shape == (len(depos), j.nplanes), cs.shape
+            j.charge_scale = cs.ctypes.data
         d = self._arr(np.ascontiguousarray(depos, dtype=np.float64).reshape(-1, 7))
         j.ndepos = d.shape[0]
         j.depos = d.ctypes.data
@@ -298,14 +413,48 @@ def fft_best_length(n, keep=False):
     return lib().orc_fft_best_length(int(n), 1 if keep else 0)
 
 
+STAGES = ("drift+cut", "raster+scatter", "response_prep", "fft_convolution", "extraction", "pir_build")
+TORCH_FFT_PATH = os.path.join(HERE, "libtorchfft.so")
+_torch_fft = None
+
+
+def set_fft_backend(name):
+    """The oracle's transforms: "own" (its scalar Stockham FFTs, the parity
+    default) or "mkl" (libtorch-CPU, i.e. Intel MKL, through
+    oracle/torch_fft.cpp: the reference's TorchDFT backend).  Process-wide."""
+    global _torch_fft
+    L = lib()
+    L.orc_set_fft_backend.argtypes = [C.c_void_p]
+    L.orc_set_fft_backend.restype = None
+    if name == "own":
+        L.orc_set_fft_backend(None)
+        return
+    if name != "mkl":
+        raise ValueError(name)
+    import torch  # noqa: F401  (loads the libtorch_cpu the shim binds to)
+    if _torch_fft is None:
+        if not os.path.exists(TORCH_FFT_PATH):
+            build()
+        _torch_fft = C.CDLL(TORCH_FFT_PATH)
+    L.orc_set_fft_backend(C.cast(_torch_fft.orc_torch_fft, C.c_void_p))
+
+
 def run(cfg, depos, drift=True, fp64=False, nthreads=1, records=False, fluctuate=False, drift_fluctuate=False,
-        seed=0):
+        seed=0, stages=False, charge_scale=None):
     """Run the restated DepoTransform. Returns dict(frames=[per-plane
-    [nwires][nticks]], windows=[OrcPlaneOut as dict], records=optional).
+    [nwires][nticks]], windows=[OrcPlaneOut as dict], records=optional,
+    stages=optional {STAGES name: seconds, summed over planes}).
     ``fluctuate`` / ``drift_fluctuate`` draw the reference's binomial
-    fluctuations with std::mt19937 streams seeded from ``seed``."""
+    fluctuations with std::mt19937 streams seeded from ``seed``.  Several
+    faces: cfg["faces"] (each {"bb", "planes"}), else one face with
+    cfg["face_bb"].  ``charge_scale`` [ndepos][nplanes]: modify_depo's
+    per-plane charge factor."""
     job = Job(cfg, depos, drift=drift, fp64=fp64, nthreads=nthreads, fluctuate=fluctuate,
-              drift_fluctuate=drift_fluctuate, seed=seed)
+              drift_fluctuate=drift_fluctuate, seed=seed, charge_scale=charge_scale)
+    st = None
+    if stages:
+        st = job._arr(np.zeros(len(STAGES), dtype=np.float64))
+        job.job.stage_s = st.ctypes.data
     nticks = int(cfg["readout_time"] / cfg["tick"])
     nw = [pl["nwires"] for pl in cfg["planes"]]
     dt = np.float64 if fp64 else np.float32
@@ -324,7 +473,10 @@ def run(cfg, depos, drift=True, fp64=False, nthreads=1, records=False, fluctuate
         frames.append(frame[r0:r0 + n])
         r0 += n
     wins = [{f: getattr(p, f) for f, _ in OrcPlaneOut._fields_} for p in pouts]
-    return dict(frames=frames, windows=wins, records=rec)
+    out = dict(frames=frames, windows=wins, records=rec)
+    if st is not None:
+        out["stages"] = {k: float(v) for k, v in zip(STAGES, st)}
+    return out
 
 
 def binomial_samples(n, p, count, seed=1):

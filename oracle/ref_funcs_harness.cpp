@@ -10,8 +10,12 @@
 // (gen/src/EmpiricalNoiseModel.cxx:55-147,232-275), the group
 // spectra of GroupNoiseModel (gen/src/GroupNoiseModel.cxx:97-146 on
 // util/inc/WireCellUtil/Interpolate.h and Spectrum.h), the noise
-// generator's spectrum (GeneratorN::spec, aux/src/NoiseTools.cxx:178-204) and
-// Pimpos
+// generator's spectrum (GeneratorN::spec, aux/src/NoiseTools.cxx:178-204),
+// Drifter::insert with its Xregion helpers (gen/src/Drifter.cxx:22-60,127-196;
+// gen/inc/WireCellGen/Drifter.h), BinnedDiffusion_transform::add
+// (gen/src/BinnedDiffusion_transform.cxx:37-92) over the reference's IDepo and
+// SimpleDepo (iface/inc/WireCellIface/IDepo.h, aux/inc/WireCellAux/SimpleDepo.h,
+// aux/src/SimpleDepo.cxx), and Pimpos
 // (util/inc/WireCellUtil/Pimpos.h,
 // util/src/Pimpos.cxx:5-68).  oracle/extract_ref.py cuts them out of the
 // reference tree into oracle/_ref/*.inc and oracle/Makefile compiles this
@@ -26,12 +30,17 @@
 #include <complex>
 #include <functional>
 #include <iostream>
+#include <algorithm>
 #include <map>
+#include <memory>
+#include <set>
 #include <stdexcept>
+#include <string>
 #include <unordered_map>
 #include <utility>
 #include <vector>
 
+#include "WireCellIface/IData.h"
 #include "WireCellUtil/Binning.h"
 #include "WireCellUtil/Interpolate.h"
 #include "WireCellUtil/D3Vector.h"
@@ -95,7 +104,84 @@ class GeneratorN {
     complex_vector_t spec(const real_vector_t& sigmas);
 };
 }  // namespace Aux::NoiseTools
+
+// ---- Drifter::insert and BinnedDiffusion_transform::add ----
+// The depo interface and its plain implementation are the reference's own
+// (iface/inc/WireCellIface/IData.h compiles as it is; IDepo and SimpleDepo
+// are cut out of their headers, whose Point.h include needs jsoncpp).
+#include "idepo_class.inc"
+namespace Aux {
+#include "simpledepo_class.inc"
+}
+// IRandom::binomial (iface/inc/WireCellIface/IRandom.h), the one call of
+// Drifter::insert into its random source, when "fluctuate" is on.
+class IRandom {
+   public:
+    typedef std::shared_ptr<IRandom> pointer;
+    virtual ~IRandom() {}
+    virtual int binomial(int max, double prob) = 0;
+};
+// The configuration values that Drifter::Xregion's constructor reads
+// (Json::Value's operator[], isNull and asDouble).
+struct ConfigValue {
+    bool null{true};
+    double v{0};
+    bool isNull() const { return null; }
+    double asDouble() const { return v; }
+};
+struct Configuration {
+    std::map<std::string, ConfigValue> m;
+    ConfigValue operator[](const char* k) const
+    {
+        auto it = m.find(k);
+        return it == m.end() ? ConfigValue{} : it->second;
+    }
+};
+namespace Gen {
+// the members of gen/inc/WireCellGen/Drifter.h that Drifter::insert uses;
+// the nested helper types are the header's own text
+class Drifter {
+   public:
+    typedef IDepo::pointer input_pointer;
+    bool insert(const input_pointer& depo);
+    IRandom::pointer m_rng;
+    double m_DL, m_DT;
+    double m_lifetime;
+    bool m_fluctuate;
+    double m_speed;
+    double m_toffset;
+#include "drifter_structs.inc"
+    std::vector<Xregion> m_xregions;
+};
+// the members of GaussianDiffusion (gen/inc/WireCellGen/GaussianDiffusion.h:80)
+// and BinnedDiffusion_transform (gen/inc/WireCellGen/BinnedDiffusion_transform.h:105-121)
+// that BinnedDiffusion_transform::add uses
+class GaussianDiffusion {
+   public:
+    GaussianDiffusion(const IDepo::pointer& depo, const GausDesc& time_desc, const GausDesc& pitch_desc)
+      : m_deposition(depo), m_time_desc(time_desc), m_pitch_desc(pitch_desc)
+    {
+    }
+    IDepo::pointer m_deposition;
+    GausDesc m_time_desc, m_pitch_desc;
+};
+class BinnedDiffusion_transform {
+   public:
+    BinnedDiffusion_transform(const Pimpos& pimpos, const Binning& tbins, double nsigma)
+      : m_pimpos(pimpos), m_tbins(tbins), m_nsigma(nsigma)
+    {
+    }
+    bool add(IDepo::pointer depo, double sigma_time, double sigma_pitch);
+    const Pimpos& m_pimpos;
+    const Binning& m_tbins;
+    double m_nsigma;
+    std::set<std::shared_ptr<GaussianDiffusion> > m_diffs;
+    int m_outside_pitch{0};
+    int m_outside_time{0};
+};
+}  // namespace Gen
 }  // namespace WireCell
+WireCell::IDepo::~IDepo() {}
 
 using namespace WireCell;
 using namespace std;
@@ -109,6 +195,9 @@ using namespace std;
 using namespace WireCell::Spectrum;
 using namespace WireCell::Aux::NoiseTools;
 #include "generatorn.inc"
+#include "simpledepo_fns.inc"
+#include "drifter_fns.inc"
+#include "bdt_add.inc"
 
 extern "C" {
 // Length of the result; out must hold max(nbins, 1) values.
@@ -284,5 +373,63 @@ void ref_pimpos(int nwires, double minp, double maxp, const double* wire, const 
     for (int a = 0; a < 3; ++a)
         for (int k = 0; k < 3; ++k) out[6 + 3 * a + k] = p.axis(a)[k];
     for (int j = 0; j < n; ++j) dist[j] = p.distance(Point(pts[3 * j], pts[3 * j + 1], pts[3 * j + 2]));
+}
+
+// Drifter::insert (gen/src/Drifter.cxx:127-196) of one depo, fluctuation
+// off: xr [nxr][3] (anode, response, cathode) as Xregion configurations,
+// depo (t, q, x, y, z, extent_long, extent_tran).  Returns 1 and the drifted
+// depo in out (same layout) when insert keeps it, else 0.
+int ref_drift_one(const double* xr, int nxr, double DL, double DT, double lifetime, double speed, double toffset,
+                  const double* depo, double* out)
+{
+    Gen::Drifter d;
+    d.m_DL = DL;
+    d.m_DT = DT;
+    d.m_lifetime = lifetime;
+    d.m_fluctuate = false;
+    d.m_speed = speed;
+    d.m_toffset = toffset;
+    for (int k = 0; k < nxr; ++k) {
+        Configuration c;
+        c.m["anode"] = ConfigValue{false, xr[3 * k]};
+        c.m["response"] = ConfigValue{false, xr[3 * k + 1]};
+        c.m["cathode"] = ConfigValue{false, xr[3 * k + 2]};
+        d.m_xregions.emplace_back(c);
+    }
+    auto in = std::make_shared<Aux::SimpleDepo>(depo[0], Point(depo[2], depo[3], depo[4]), depo[1], nullptr, depo[5],
+                                                depo[6], 7);
+    if (!d.insert(in)) return 0;
+    for (auto& x : d.m_xregions)
+        for (auto& o : x.depos) {
+            out[0] = o->time();
+            out[1] = o->charge();
+            out[2] = o->pos().x();
+            out[3] = o->pos().y();
+            out[4] = o->pos().z();
+            out[5] = o->extent_long();
+            out[6] = o->extent_tran();
+            return 1;
+        }
+    return -1;
+}
+// BinnedDiffusion_transform::add (gen/src/BinnedDiffusion_transform.cxx:37-92)
+// of one depo on a plane (the Pimpos arguments as ref_pimpos) and the
+// readout binning (ntbins over [tmin, tmax]); sigma_time and sigma_pitch as
+// DepoTransform passes them.  Returns 1 when added; counters[0..1] get
+// m_outside_time and m_outside_pitch.
+int ref_bdt_add(int nwires, double minp, double maxp, const double* wire, const double* pitch, const double* origin,
+                int nimp, int ntbins, double tmin, double tmax, double nsigma, const double* depo, double sigma_time,
+                double sigma_pitch, int* counters)
+{
+    Pimpos pim(nwires, minp, maxp, Vector(wire[0], wire[1], wire[2]), Vector(pitch[0], pitch[1], pitch[2]),
+               Point(origin[0], origin[1], origin[2]), nimp);
+    Binning tb(ntbins, tmin, tmax);
+    Gen::BinnedDiffusion_transform bd(pim, tb, nsigma);
+    auto in = std::make_shared<Aux::SimpleDepo>(depo[0], Point(depo[2], depo[3], depo[4]), depo[1], nullptr, depo[5],
+                                                depo[6], 7);
+    const bool ok = bd.add(in, sigma_time, sigma_pitch);
+    counters[0] = bd.m_outside_time;
+    counters[1] = bd.m_outside_pitch;
+    return ok ? 1 : 0;
 }
 }

@@ -34,6 +34,7 @@
 
 #include <algorithm>
 #include <atomic>
+#include <chrono>
 #include <cmath>
 #include <complex>
 #include <cstdint>
@@ -44,6 +45,7 @@
 #include <mutex>
 #include <random>
 #include <stdexcept>
+#include <string>
 #include <thread>
 #include <unordered_map>
 #include <vector>
@@ -253,25 +255,51 @@ static void fft_1d(std::complex<T>* data, int n, int sign, std::complex<T>* work
     if (src != data) std::copy(src, src + n, data);
 }
 
+// Optional external transform in place of fft_1d: a [nrows][ncols] complex
+// array (float or double per fp64) transformed along axis (1: each row, 0:
+// each column), sign -1 forward / +1 backward, unnormalised.  The timed CPU
+// baseline sets it to libtorch-CPU's MKL transforms (oracle/torch_fft.cpp),
+// the reference's TorchDFT backend (pytorch/src/DFT.cxx:80-123); parity runs
+// leave it unset.
+typedef void (*ExtFft)(void* a, int nrows, int ncols, int axis, int sign, int fp64);
+static std::atomic<ExtFft> g_ext_fft{nullptr};
+
 template <typename T>
 struct Dft {
     using C = std::complex<T>;
+    static bool ext(C* a, int nrows, int ncols, int axis, int sign)
+    {
+        ExtFft f = g_ext_fft.load();
+        if (!f) return false;
+        f(a, nrows, ncols, axis, sign, sizeof(T) == sizeof(double) ? 1 : 0);
+        return true;
+    }
     // aux/src/FftwDFT.cxx:88-115 (1d)
     static void fwd1d(C* x, int n)
     {
+        if (ext(x, 1, n, 1, -1)) return;
         std::vector<C> w(n);
         fft_1d<T>(x, n, -1, w.data());
     }
     static void inv1d(C* x, int n)
     {
-        std::vector<C> w(n);
-        fft_1d<T>(x, n, +1, w.data());
+        if (!ext(x, 1, n, 1, +1)) {
+            std::vector<C> w(n);
+            fft_1d<T>(x, n, +1, w.data());
+        }
         for (int i = 0; i < n; ++i) x[i] /= (T)n;
     }
     // Row-major [nrows][ncols]; axis=1 transforms each row, axis=0 each column
     // (aux/src/FftwDFT.cxx:119-176, 1b methods).
     static void do1b(C* a, int nrows, int ncols, int axis, int sign, bool norm)
     {
+        if (ext(a, nrows, ncols, axis, sign)) {
+            if (norm) {
+                const T n = (T)(axis == 1 ? ncols : nrows);
+                for (size_t k = 0; k < (size_t)nrows * ncols; ++k) a[k] /= n;
+            }
+            return;
+        }
         if (axis == 1) {
             std::vector<C> w(ncols);
             for (int r = 0; r < nrows; ++r) {
@@ -334,6 +362,14 @@ static std::vector<std::complex<T>> fwd_r2c(const std::vector<T>& v)
     Dft<T>::fwd1d(c.data(), (int)c.size());
     return c;
 }
+
+// Stage clock of the timed CPU baseline: seconds since an arbitrary origin.
+static double now_s()
+{
+    return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+// Stages timed by orc_run (seconds, summed over planes).
+enum { kStDrift = 0, kStRaster, kStRespPrep, kStFftConv, kStExtract, kStPir, kNStages };
 
 // ---------------------------------------------------------------------------
 // Depos. Layout of one depo: t, q, x, y, z, extent_long, extent_tran.
@@ -697,6 +733,44 @@ static void build_pir(const FRPlane& fr, double tstart, double period, const std
 // ---------------------------------------------------------------------------
 // BinnedDiffusion_transform -- gen/src/BinnedDiffusion_transform.cxx.
 // ---------------------------------------------------------------------------
+// PlaneImpactResponse is a configured component: the reference builds it
+// once (PlaneImpactResponse::configure -> build_responses) and every event
+// reuses it.  The oracle keeps the built responses keyed by every input of
+// the build, so repeated runs of one configuration (the timed baseline) do
+// not rebuild them per event.
+template <typename T>
+static std::shared_ptr<const PIR<T>> cached_pir(const FRPlane& fr, double tstart, double period,
+                                                const std::vector<std::vector<double>>& shorts,
+                                                double overall_short_padding, double tick, int nbins,
+                                                const std::vector<std::vector<double>>& longs, double long_padding)
+{
+    std::string key;
+    auto put = [&](const void* p, size_t n) { key.append(reinterpret_cast<const char*>(p), n); };
+    const double sc[6] = {tstart, period, overall_short_padding, tick, long_padding, fr.pitch};
+    const int ic[3] = {fr.npaths, fr.nsamp, nbins};
+    const ExtFft backend = g_ext_fft.load();  // the build's transforms are part of the key
+    put(&backend, sizeof backend);
+    put(sc, sizeof sc);
+    put(ic, sizeof ic);
+    put(fr.pitchpos, sizeof(double) * fr.npaths);
+    put(fr.current, sizeof(double) * fr.npaths * (size_t)fr.nsamp);
+    for (auto& v : shorts) { const size_t n = v.size(); put(&n, sizeof n); put(v.data(), sizeof(double) * n); }
+    for (auto& v : longs) { const size_t n = v.size(); put(&n, sizeof n); put(v.data(), sizeof(double) * n); }
+    static std::mutex mtx;
+    static std::map<std::string, std::shared_ptr<const PIR<T>>> cache;
+    {
+        std::lock_guard<std::mutex> lk(mtx);
+        auto it = cache.find(key);
+        if (it != cache.end()) return it->second;
+    }
+    auto pir = std::make_shared<PIR<T>>();
+    build_pir<T>(fr, tstart, period, shorts, overall_short_padding, tick, nbins, *pir, longs, long_padding);
+    std::lock_guard<std::mutex> lk(mtx);
+    if (cache.size() >= 32) cache.clear();
+    cache[key] = pir;
+    return pir;
+}
+
 struct Diff {
     Depo depo;
     GausDesc td, pd;
@@ -869,8 +943,16 @@ struct ImpactTransform {
     mutable int long_n{0};
     mutable std::vector<C> long_spec;  // spectrum of the long waveform at long_n
 
-    ImpactTransform(const PIR<T>& pir, BinnedDiffusion<T>& bd, std::vector<PlaneRecord>* rec) : m_pir(&pir)
+    // st: optional stage clocks (kNStages seconds, added to)
+    ImpactTransform(const PIR<T>& pir, BinnedDiffusion<T>& bd, std::vector<PlaneRecord>* rec, double* st = nullptr)
+        : m_pir(&pir)
     {
+        double t_mark = now_s();
+        auto lap = [&](int k) {
+            const double t = now_s();
+            if (st) st[k] += t - t_mark;
+            t_mark = t;
+        };
         const int G = std::round(pir.pitch / pir.impact) + 1;
         const int npad = std::round((pir.nwires() - 1) / 2.);
         std::vector<int> vec_impact;
@@ -889,7 +971,9 @@ struct ImpactTransform {
             vmr.push_back(mr);
         }
         std::vector<std::vector<std::tuple<int, int, double>>> vvc(G);
+        lap(kStRespPrep);
         bd.get_charge_vec(vvc, vec_impact, rec);
+        lap(kStRaster);
 
         auto ir = bd.impact_bin_range();
         auto tr = bd.time_bin_range();
@@ -943,7 +1027,9 @@ struct ImpactTransform {
                     C(0, (T)std::get<2>(e));
             vvc.at(ii).clear();
             Dft<T>::fwd2d(c.data(), NW, NT);
+            lap(kStFftConv);
             auto resp = build_resp(i);
+            lap(kStRespPrep);
             for (size_t k = 0; k < c.size(); ++k) c[k] *= resp[k];
             Dft<T>::inv1b(c.data(), NW, NT, 0);
             for (size_t k = 0; k < c.size(); ++k) acc[k] += c[k];
@@ -960,7 +1046,9 @@ struct ImpactTransform {
             for (size_t k = 0; k < d.size(); ++k) d[k] = C(dtw[k], 0);
             Dft<T>::fwd1b(d.data(), NW, NT, 1);
             Dft<T>::fwd1b(d.data(), NW, NT, 0);
+            lap(kStFftConv);
             auto resp = build_resp(i);
+            lap(kStRespPrep);
             for (size_t k = 0; k < d.size(); ++k) d[k] *= resp[k];
             Dft<T>::inv1b(d.data(), NW, NT, 0);
             for (size_t k = 0; k < d.size(); ++k) acc[k] += d[k];
@@ -971,6 +1059,7 @@ struct ImpactTransform {
             for (int c2 = 0; c2 < NT; ++c2)
                 decon[(size_t)r * NT + c2] = std::real(acc[(size_t)r * NT + c2]) +
                                              std::imag(acc[(size_t)(NW - 1 - r) * NT + c2]);
+        lap(kStFftConv);
     }
 
     // ImpactTransform::waveform, ImpactTransform.cxx:312-347, with the
@@ -1054,7 +1143,28 @@ struct OrcJob {
     const int* long_len;
     const double* long_wave;
     double long_padding;
+    // optional: seconds per stage of orc_run (kNStages: drift + sensitive cut,
+    // rasterise + scatter, response prep, FFT convolution, extraction, PIR
+    // build), summed over planes; null: not timed
+    double* stage_s;
+    // several anode faces (DepoTransform.cxx:169-213 loops over
+    // IAnodePlane::faces()): nfaces > 0 gives each face's sensitive box
+    // (face_bb [nfaces][lo xyz, hi xyz], face_have_bb 0: no cut) and each
+    // plane's face (plane_face [nplanes], planes of a face consecutive);
+    // nfaces = 0: one face with the box above
+    int nfaces;
+    const double* face_bb;
+    const int* face_have_bb;
+    const int* plane_face;
+    // modify_depo (gen/inc/WireCellGen/DepoTransform.h:33-35, called before
+    // BinnedDiffusion_transform::add at DepoTransform.cxx:182) as a charge
+    // scale: depo i brings charge * charge_scale[i][plane] to the plane
+    // ([ndepos][nplanes]); null: unmodified
+    const double* charge_scale;
 };
+
+// The external transform of the timed CPU baseline (null: the oracle's own).
+void orc_set_fft_backend(orc::ExtFft f) { orc::g_ext_fft.store(f); }
 
 static std::vector<std::vector<double>> job_longs(const OrcJob* job)
 {
@@ -1206,6 +1316,8 @@ int orc_pir_build(const OrcJob* job, int iplane, double* waveforms, int* bywire,
 int orc_run(const OrcJob* job, void* frame, OrcPlaneOut* pout, int* rec)
 {
     try {
+        std::mutex st_mtx;
+        double t_drift = orc::now_s();
         std::vector<orc::Depo> depos;
         for (int i = 0; i < job->ndepos; ++i) {
             const double* p = job->depos + 7 * (size_t)i;
@@ -1219,10 +1331,19 @@ int orc_run(const OrcJob* job, void* frame, OrcPlaneOut* pout, int* rec)
             if (job->drift_fluctuate) dp.rng = &drng;
             depos = orc::drift_all(dp, depos);  // keeps each depo's input index
         }
-        // face sensitive volume: DepoTools.cxx:110-123
-        std::vector<orc::Depo> face;
-        for (auto& d : depos)
-            if (!job->have_bb || orc::bb_inside(job->bb_lo, job->bb_hi, d)) face.push_back(d);
+        // each face's sensitive volume: DepoTools.cxx:110-123
+        const int nfaces = job->nfaces > 0 ? job->nfaces : 1;
+        std::vector<std::vector<orc::Depo>> faces(nfaces);
+        for (int f = 0; f < nfaces; ++f) {
+            const bool have = job->nfaces > 0 ? job->face_have_bb[f] != 0 : job->have_bb != 0;
+            const double* lo = job->nfaces > 0 ? job->face_bb + 6 * f : job->bb_lo;
+            const double* hi = job->nfaces > 0 ? job->face_bb + 6 * f + 3 : job->bb_hi;
+            for (auto& d : depos)
+                if (!have || orc::bb_inside(lo, hi, d)) faces[f].push_back(d);
+        }
+        for (int ip = 0; ip < job->nplanes; ++ip)
+            if (job->nfaces > 0 && (job->plane_face[ip] < 0 || job->plane_face[ip] >= nfaces)) return -1;
+        if (job->stage_s) job->stage_s[orc::kStDrift] += orc::now_s() - t_drift;
 
         const int nticks = (int)(job->readout_time / job->tick);
         std::vector<std::vector<double>> shorts;
@@ -1242,20 +1363,29 @@ int orc_run(const OrcJob* job, void* frame, OrcPlaneOut* pout, int* rec)
             orc::Pimpos pim(pl.nwires, pl.pitchmin, pl.pitchmax, orc::V3{pl.wire[0], pl.wire[1], pl.wire[2]},
                             orc::V3{pl.pitch[0], pl.pitch[1], pl.pitch[2]},
                             orc::V3{pl.origin[0], pl.origin[1], pl.origin[2]}, pl.nimp);
+            double st[orc::kNStages] = {0, 0, 0, 0, 0, 0};
+            double t0 = orc::now_s();
             orc::FRPlane fr{pl.npaths, pl.nfr, pl.pitchpos, pl.current, pl.fr_pitch};
-            orc::PIR<T> pir;
-            orc::build_pir<T>(fr, job->fr_tstart, job->fr_period, shorts, job->overall_short_padding, job->tick,
-                              job->pir_nticks, pir, longs, job->long_padding);
+            const auto pir_ptr = orc::cached_pir<T>(fr, job->fr_tstart, job->fr_period, shorts,
+                                                    job->overall_short_padding, job->tick, job->pir_nticks, longs,
+                                                    job->long_padding);
+            const orc::PIR<T>& pir = *pir_ptr;
+            st[orc::kStPir] += orc::now_s() - t0;
+            t0 = orc::now_s();
             orc::Binning tbins(job->readout_time / job->tick, job->start_time, job->start_time + job->readout_time);
             orc::BinnedDiffusion<T> bd(pim, tbins, job->nsigma);
             std::mt19937 prng((std::uint32_t)(job->seed * 2654435761ull + 31 * (unsigned long long)ip + 1));
             if (job->fluctuate) bd.fluctuate = &prng;
             std::vector<orc::PlaneRecord> precs(ndep_rec);
-            for (auto& d : face) {
+            const std::vector<orc::Depo>& face = faces[job->nfaces > 0 ? job->plane_face[ip] : 0];
+            for (const auto& d0 : face) {
+                orc::Depo d = d0;
+                if (job->charge_scale) d.q = d.q * job->charge_scale[(size_t)d.index * job->nplanes + ip];
                 bool ok = bd.add(d, d.el / job->drift_speed, d.et);
                 precs[d.index].added = ok ? 1 : 0;
             }
-            orc::ImpactTransform<T> it(pir, bd, &precs);
+            st[orc::kStRaster] += orc::now_s() - t0;
+            orc::ImpactTransform<T> it(pir, bd, &precs, st);
             OrcPlaneOut& po = pout[ip];
             po.start_ch = it.win.start_ch;
             po.end_ch = it.win.end_ch;
@@ -1267,7 +1397,13 @@ int orc_run(const OrcJob* job, void* frame, OrcPlaneOut* pout, int* rec)
             po.outside_time = bd.outside_time;
             po.outside_pitch = bd.outside_pitch;
             T* fr_out = reinterpret_cast<T*>(frame) + row0[ip] * (size_t)nticks;
+            t0 = orc::now_s();
             for (int w = 0; w < pl.nwires; ++w) it.waveform(w, nticks, fr_out + (size_t)w * nticks);
+            st[orc::kStExtract] += orc::now_s() - t0;
+            if (job->stage_s) {
+                std::lock_guard<std::mutex> lk(st_mtx);
+                for (int k = 0; k < orc::kNStages; ++k) job->stage_s[k] += st[k];
+            }
             if (rec) {
                 for (size_t k = 0; k < ndep_rec; ++k) {
                     int* r = rec + ((size_t)ip * ndep_rec + k) * 5;
@@ -1444,6 +1580,39 @@ void orc_pimpos(int nwires, double minp, double maxp, const double* wire, const 
         out[8 + 3 * a] = p.axis[a].z;
     }
     for (int j = 0; j < n; ++j) dist[j] = p.distance(orc::V3{pts[3 * j], pts[3 * j + 1], pts[3 * j + 2]});
+}
+
+// Drifter::insert of one depo, fluctuation off (the restatement's drift_one):
+// xr [nxr][3] (anode, response, cathode), depo and out (t, q, x, y, z,
+// extent_long, extent_tran).  Returns 1 and the drifted depo when kept, else 0.
+int orc_drift_one(const double* xr, int nxr, double DL, double DT, double lifetime, double speed, double toffset,
+                  const double* depo, double* out)
+{
+    orc::DriftParams dp{DL, DT, lifetime, speed, toffset, {}};
+    for (int k = 0; k < nxr; ++k) dp.xregions.push_back({xr[3 * k], xr[3 * k + 1], xr[3 * k + 2]});
+    orc::Depo in{depo[0], depo[1], depo[2], depo[3], depo[4], depo[5], depo[6], 0}, o{};
+    if (!orc::drift_one(dp, in, o)) return 0;
+    const double v[7] = {o.t, o.q, o.x, o.y, o.z, o.el, o.et};
+    for (int k = 0; k < 7; ++k) out[k] = v[k];
+    return 1;
+}
+
+// BinnedDiffusion_transform::add of one depo (the restatement's
+// BinnedDiffusion::add) on a plane given by its Pimpos arguments and the
+// readout binning; counters[0..1] get outside_time and outside_pitch.
+int orc_bdt_add(int nwires, double minp, double maxp, const double* wire, const double* pitch, const double* origin,
+                int nimp, int ntbins, double tmin, double tmax, double nsigma, const double* depo, double sigma_time,
+                double sigma_pitch, int* counters)
+{
+    orc::Pimpos pim(nwires, minp, maxp, orc::V3{wire[0], wire[1], wire[2]}, orc::V3{pitch[0], pitch[1], pitch[2]},
+                    orc::V3{origin[0], origin[1], origin[2]}, nimp);
+    orc::Binning tb(ntbins, tmin, tmax);
+    orc::BinnedDiffusion<double> bd(pim, tb, nsigma);
+    orc::Depo d{depo[0], depo[1], depo[2], depo[3], depo[4], depo[5], depo[6], 0};
+    const bool ok = bd.add(d, sigma_time, sigma_pitch);
+    counters[0] = bd.outside_time;
+    counters[1] = bd.outside_pitch;
+    return ok ? 1 : 0;
 }
 
 }  // extern "C"

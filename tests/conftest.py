@@ -40,3 +40,13 @@ def rel_l2(a, b):
     b = np.asarray(b, dtype=dt)
     nb = np.linalg.norm(b)
     return float(np.linalg.norm(a - b) / (nb if nb > 0 else 1.0))
+
+
+def parity_log(entry):
+    """Append one measured parity figure (a dict) as a JSON line to the file
+    named by WCT_PARITY_LOG, when that variable is set."""
+    import json
+    path = os.environ.get("WCT_PARITY_LOG")
+    if path:
+        with open(path, "a") as f:
+            f.write(json.dumps(entry) + "\n")

@@ -26,7 +26,9 @@ def tables(text):
 
 
 def main():
-    ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    ref = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("WCT_REFERENCE")
+    if not ref:
+        raise SystemExit("usage: make_fft_lengths.py <reference tree> (or set WCT_REFERENCE)")
     with open(os.path.join(ref, SRC)) as f:
         any_, even, odd = tables(f.read())
     out = {"source": SRC, "any": any_, "even": even, "odd": odd}

@@ -4,8 +4,10 @@ gen/inc/WireCellGen/GaussianDiffusion.h:33-49), Waveform::edge
 (util/src/Waveform.cxx:136-153), Response::coldelec
 (util/src/Response.cxx:311-340), Pimpos (util/src/Pimpos.cxx:5-68),
 Digitizer::digitize (gen/src/Digitizer.cxx:77-93), EmpiricalNoiseModel's
-resampling (gen/src/EmpiricalNoiseModel.cxx:55-147) and GroupNoiseModel's
-spectra (gen/src/GroupNoiseModel.cxx:97-146), from
+resampling (gen/src/EmpiricalNoiseModel.cxx:55-147), GroupNoiseModel's
+spectra (gen/src/GroupNoiseModel.cxx:97-146), Drifter::insert
+(gen/src/Drifter.cxx:127-196) and BinnedDiffusion_transform::add
+(gen/src/BinnedDiffusion_transform.cxx:37-92), from
 oracle/_ref/libref_funcs.so (built by
 oracle/Makefile with extract_ref.py and ref_funcs_harness.cpp).
 
@@ -162,14 +164,26 @@ def main():
                               c["nbins"], c["pts"])
         pim.append(dict(c, head=[float(v) for v in head], dist=[float(v) for v in dist]))
 
+    drift = []
+    for c in O.drift_cases(np.random.default_rng(13), 120):
+        k, o = O.drift_one(R, "ref", c)
+        drift.append(dict(c, kept=int(k), out=[float(v) for v in o]))
+    bdt = []
+    for c in O.bdt_add_cases(np.random.default_rng(17), 200):
+        k, cnt = O.bdt_add(R, "ref", c)
+        bdt.append(dict(c, added=int(k), counters=cnt))
+
     out = {"source": ["gen/src/GaussianDiffusion.cxx", "util/src/Waveform.cxx", "util/src/Response.cxx",
-                      "util/src/Pimpos.cxx", "gen/src/Digitizer.cxx", "gen/src/EmpiricalNoiseModel.cxx", "gen/src/GroupNoiseModel.cxx"],
+                      "util/src/Pimpos.cxx", "gen/src/Digitizer.cxx", "gen/src/EmpiricalNoiseModel.cxx",
+                      "gen/src/GroupNoiseModel.cxx", "gen/src/Drifter.cxx", "gen/src/BinnedDiffusion_transform.cxx"],
            "gausdesc": gd, "edge": edges, "coldelec": cold, "pimpos": pim, "digitize": digi, "noise_resample": nm,
-           "group_spectrum": grp}
+           "group_spectrum": grp, "drift": drift, "bdt_add": bdt}
     with open(os.path.join(ROOT, "tests", "golden", "ref_funcs.json"), "w") as f:
         json.dump(out, f)
     print("%d GausDesc cases, %d edges, %d coldelec curves, %d planes, %d digitizer frames, %d noise spectra, "
-          "%d group spectra" % (len(gd), len(edges), len(cold), len(pim), len(digi), len(nm), len(grp)))
+          "%d group spectra, %d drifted depos, %d add decisions" % (len(gd), len(edges), len(cold), len(pim),
+                                                                    len(digi), len(nm), len(grp), len(drift),
+                                                                    len(bdt)))
 
 
 if __name__ == "__main__":

@@ -2,8 +2,10 @@
 source (oracle/extract_ref.py + oracle/ref_funcs_harness.cpp): GausDesc bin
 integrals, impact weights and distance (gen/src/GaussianDiffusion.cxx:30-92,
 gen/inc/WireCellGen/GaussianDiffusion.h:33-49), Waveform::edge
-(util/src/Waveform.cxx:136-153) and Response::coldelec
-(util/src/Response.cxx:311-340).  Against the committed vectors
+(util/src/Waveform.cxx:136-153), Response::coldelec
+(util/src/Response.cxx:311-340), Drifter::insert (gen/src/Drifter.cxx:127-196)
+and BinnedDiffusion_transform::add (gen/src/BinnedDiffusion_transform.cxx:37-92),
+among others.  Against the committed vectors
 (tests/golden/ref_funcs.json, written by tests/golden/make_ref_funcs.py) and,
 where the harness was built, live on fresh random cases.  CPU only."""
 
@@ -261,3 +263,50 @@ def test_noise_generator_spectrum_against_reference(oracle):
         want = out[0::2].astype(np.float64) + 1j * out[1::2].astype(np.float64)
         got = oracle.noise_spec(sig.astype(np.float64) / np.sqrt(2.0 / 3.141592), normals.astype(np.float64))
         assert np.abs(got - want).max() <= 1e-6 * np.abs(want).max(), n
+
+
+def test_drift_against_reference_vectors(oracle, golden):
+    """Drifter::insert (gen/src/Drifter.cxx:127-196, fluctuation off): which
+    depos are kept and their drifted (t, q, x, y, z, extent_long,
+    extent_tran), bit for bit the reference's compiled code, over one face,
+    two mirrored faces, a region without an anode, and positions exactly on
+    the anode, response and cathode planes."""
+    L = oracle.lib()
+    for c in golden["drift"]:
+        k, o = oracle.drift_one(L, "orc", c)
+        assert k == c["kept"], c
+        if k:
+            assert o.tolist() == c["out"], c
+
+
+def test_drift_against_compiled_reference(oracle):
+    R = oracle.ref_funcs()
+    if R is None:
+        pytest.skip("reference function harness not built")
+    L = oracle.lib()
+    for c in oracle.drift_cases(np.random.default_rng(1234), 3000):
+        ka, a = oracle.drift_one(L, "orc", c)
+        kb, b = oracle.drift_one(R, "ref", c)
+        assert ka == kb, c
+        if ka:
+            assert np.array_equal(a, b), c
+
+
+def test_bdt_add_against_reference_vectors(oracle, golden):
+    """BinnedDiffusion_transform::add (gen/src/BinnedDiffusion_transform.cxx:37-92):
+    the time and pitch rejections and their counters, bit for bit the
+    reference's compiled code, including zero widths and centres exactly
+    nsigma outside the window or the impact range."""
+    L = oracle.lib()
+    for c in golden["bdt_add"]:
+        k, cnt = oracle.bdt_add(L, "orc", c)
+        assert (k, cnt) == (c["added"], c["counters"]), c
+
+
+def test_bdt_add_against_compiled_reference(oracle):
+    R = oracle.ref_funcs()
+    if R is None:
+        pytest.skip("reference function harness not built")
+    L = oracle.lib()
+    for c in oracle.bdt_add_cases(np.random.default_rng(4321), 3000):
+        assert oracle.bdt_add(L, "orc", c) == oracle.bdt_add(R, "ref", c), c

@@ -60,3 +60,42 @@ def test_noalloc_matches_allocating_entry_point_on_two_calls(wct):
         g = got.cpu().numpy()
         assert np.abs(w).max() > 0
         assert rel_l2(g, w) < TOL, (nrows, n_in, rel_l2(g, w))
+
+
+@pytest.mark.gpu
+def test_noalloc_strided_on_a_stream_and_at_the_limit(wct):
+    """Strided rows in and out, fewer output samples than input samples, a
+    caller's stream (the twiddle tables are built on it), and a call whose
+    (nrows + 3) * nfft / 2 is exactly the 4194304 complex values the fixed
+    array holds; each against the allocating entry point on the same stream."""
+    import torch
+    torch.cuda.set_device(0)
+    rng = np.random.default_rng(77)
+    st = torch.cuda.Stream()
+    cases = [
+        # (nrows, n_in, ld_in, n_resp, nfft, n_out, ld_out)
+        (64, 3000, 3072, 300, 0, 2500, 2600),
+        (1021, 6000, 6000, 200, 8192, 6000, 6000),  # (1021 + 3) * 4096 = 4194304
+    ]
+    for nrows, n_in, ld_in, n_resp, nfft, n_out, ld_out in cases:
+        if nfft:
+            assert (nrows + 3) * nfft // 2 == 4194304
+        x = rng.normal(size=(nrows, ld_in)).astype(np.float32)
+        resp = rng.normal(size=n_resp).astype(np.float32)
+        with torch.cuda.stream(st):
+            dx = torch.from_numpy(x).cuda()
+            dr = torch.from_numpy(resp).cuda()
+            want = torch.full((nrows, ld_out), -3.0, dtype=torch.float32, device="cuda")
+            got = torch.full((nrows, ld_out), 7.0, dtype=torch.float32, device="cuda")
+        st.synchronize()
+        wct.convolve_rows(dx.data_ptr(), ld_in, nrows, n_in, dr.data_ptr(), n_resp, want.data_ptr(), ld_out, n_out,
+                          nfft=nfft, stream=st.cuda_stream)
+        wct.convolve_rows_noalloc(dx.data_ptr(), ld_in, nrows, n_in, dr.data_ptr(), n_resp, got.data_ptr(), ld_out,
+                                  n_out, nfft=nfft, stream=st.cuda_stream)
+        st.synchronize()
+        w = want.cpu().numpy()
+        g = got.cpu().numpy()
+        assert np.abs(w[:, :n_out]).max() > 0
+        assert rel_l2(g[:, :n_out], w[:, :n_out]) < TOL, (nrows, n_in, rel_l2(g[:, :n_out], w[:, :n_out]))
+        # the row padding beyond n_out is not written
+        assert (g[:, n_out:] == 7.0).all() and (w[:, n_out:] == -3.0).all()

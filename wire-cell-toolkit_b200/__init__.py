@@ -124,6 +124,7 @@ SIGNATURES = {
     "wct_dt_set_response_table": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_double,
                                             C.c_double, C.c_int, C.c_void_p]),
     "wct_dt_frame_shape": (C.c_int, [C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
+    "wct_dt_set_charge_scale": (C.c_int, [C.c_void_p, C.c_void_p, C.c_size_t, C.c_int]),
     "wct_dt_forward": (C.c_int, [C.c_void_p, C.c_void_p, C.c_size_t, C.c_void_p, C.c_void_p, C.POINTER(C.c_int)]),
     "wct_dt_forward_device": (C.c_int, [C.c_void_p, C.c_void_p, C.c_size_t, C.c_void_p, C.c_void_p,
                                         C.POINTER(C.c_int), C.c_void_p]),
@@ -444,6 +445,23 @@ class DepoTransform:
         _check(lib().wct_dt_set_response_table(self.h, face, plane, G, (J - 1) // 2, K, pitch, impact, waveform_pad,
                                                t.ctypes.data))
 
+    def set_charge_scale(self, scale=None, d_scale_ptr=None, ndepos=None):
+        """DepoTransform::modify_depo as a per-plane charge scale: depo i
+        brings charge * scale[i][p] to plane p (frame order over all faces)
+        for the following calls with that many depos.  ``scale``: host array
+        [ndepos][nplanes]; or a device pointer ``d_scale_ptr`` with
+        ``ndepos``; neither: remove it."""
+        if scale is None and d_scale_ptr is None:
+            _check(lib().wct_dt_set_charge_scale(self.h, None, 0, 0))
+            return
+        if d_scale_ptr is not None:
+            _check(lib().wct_dt_set_charge_scale(self.h, C.c_void_p(d_scale_ptr), int(ndepos), 1))
+            return
+        a = np.ascontiguousarray(scale, dtype=np.float64)
+        assert a.ndim == 2 and a.shape[1] == len(self.planes), a.shape
+        self._qscale = a
+        _check(lib().wct_dt_set_charge_scale(self.h, a.ctypes.data, a.shape[0], 0))
+
     def frame_shape(self):
         r, t = C.c_int(), C.c_int()
         _check(lib().wct_dt_frame_shape(self.h, C.byref(r), C.byref(t)))
@@ -649,21 +667,39 @@ def drifter_json(dr):
     return d
 
 
+def faces_of(cfg):
+    """The anode faces of a workload description: cfg["faces"] (a list of
+    {"bb": face sensitive box or None, "planes": indices into cfg["planes"]},
+    planes of a face consecutive, faces in order) or one face holding every
+    plane with cfg["face_bb"]."""
+    if cfg.get("faces"):
+        return [(f.get("bb"), list(f["planes"])) for f in cfg["faces"]]
+    return [(cfg.get("face_bb"), list(range(len(cfg["planes"]))))]
+
+
 def from_config(cfg, device=0):
     """Build a DepoTransform for a synthetic workload description (see synth.py):
-    one face with cfg["planes"], PIRs from cfg["fr"] and the short responses."""
+    its faces (faces_of) with cfg["planes"], PIRs from cfg["fr"] and the short
+    responses.  Each plane's PIR is built once per distinct field response and
+    shared, as the reference shares pirs[plane] across faces."""
     dcfg = {k: cfg[k] for k in ("tick", "start_time", "readout_time", "drift_speed", "nsigma", "fluctuate",
                                  "seed", "first_frame_number") if k in cfg}
     if cfg.get("drifter"):
         dcfg["drifter"] = drifter_json(cfg["drifter"])
     dcfg["device"] = device
     dt = DepoTransform(dcfg)
-    face = dt.add_face(cfg.get("face_bb"))
-    for pl, fr in zip(cfg["planes"], cfg["fr"]):
-        p = dt.add_plane(face, pl)
-        pir = PlaneImpactResponse(fr, cfg.get("short_responses", []), cfg["overall_short_padding"], cfg["tick"],
-                                  cfg["pir_nticks"], cfg.get("long_responses", []), cfg.get("long_padding", 1.5e6))
-        dt.set_response_pir(face, p, pir)
+    pirs = {}
+    for bb, idx in faces_of(cfg):
+        face = dt.add_face(bb)
+        for k in idx:
+            p = dt.add_plane(face, cfg["planes"][k])
+            fr = cfg["fr"][k]
+            key = id(fr)
+            if key not in pirs:
+                pirs[key] = PlaneImpactResponse(fr, cfg.get("short_responses", []), cfg["overall_short_padding"],
+                                                cfg["tick"], cfg["pir_nticks"], cfg.get("long_responses", []),
+                                                cfg.get("long_padding", 1.5e6))
+            dt.set_response_pir(face, p, pirs[key])
     return dt
 
 

@@ -181,7 +181,8 @@ __device__ __forceinline__ float warp_sum_f(float v)
 __global__ void __launch_bounds__(kGatherWarps * 32, 5) k_adj_gather(int n, PlaneSet ps, AdjSet as, double inv_vd,
                                                                      const PatchRec* __restrict__ rec,
                                                                      const float* __restrict__ dQ,
-                                                                     double* __restrict__ grad)
+                                                                     double* __restrict__ grad,
+                                                                     const double* __restrict__ qscale)
 {
     __shared__ BinTab s_p[kGatherWarps][kChunkP];
     __shared__ float4 s_t[kGatherWarps][kChunkT];
@@ -336,7 +337,8 @@ __global__ void __launch_bounds__(kGatherWarps * 32, 5) k_adj_gather(int n, Plan
         s_sT += qn * acc_sp - acc_qn * (double)(r.qn * iSp * dSp_s);                  // sigma_pitch = extent_tran
         s_ct += qn * acc_ct - acc_qn * (double)(r.qn * iSt * dSt_c);
         s_sL += (qn * acc_st - acc_qn * (double)(r.qn * iSt * dSt_s)) * inv_vd;      // sigma_time = extent_long / v
-        s_qf += acc_qn * (double)(iSp * iSt);
+        // the plane's charge is qscale * q' (modify_depo): its share of dL/dq' carries the scale
+        s_qf += acc_qn * (double)(iSp * iSt) * (qscale ? qscale[(size_t)i * ps.nplanes + ip] : 1.0);
         s_px += gcp * A.ax;
         s_py += gcp * A.ay;
         s_pz += gcp * A.az;
@@ -435,11 +437,11 @@ __global__ void __launch_bounds__(256) k_adj_drift(const double* __restrict__ de
 
 void launch_adj_gather(const double* depos, int n, const DriftDev& dd, int do_drift, const PlaneSet& ps,
                        const AdjSet& as, double drift_speed, const PatchRec* rec, const float* dQ, double* grad,
-                       double* gglob, cudaStream_t s)
+                       double* gglob, cudaStream_t s, const double* qscale)
 {
     if (n <= 0) return;
     const int blocks = (n + kGatherWarps - 1) / kGatherWarps;
-    k_adj_gather<<<blocks, kGatherWarps * 32, 0, s>>>(n, ps, as, 1.0 / drift_speed, rec, dQ, grad);
+    k_adj_gather<<<blocks, kGatherWarps * 32, 0, s>>>(n, ps, as, 1.0 / drift_speed, rec, dQ, grad, qscale);
     if (do_drift) k_adj_drift<<<(n + 255) / 256, 256, 0, s>>>(depos, n, dd, grad, gglob);
 }
 

@@ -191,6 +191,13 @@ struct Core {
     DevBuf d_fq, d_fluc;               // fluctuation: drifted charges, per (plane, depo) draw sums
     DevBuf d_pool, d_pool_off, d_pool_used;  // time profiles of long patches
     DevBuf d_wide;                           // per visit key: holds a long patch
+    // modify_depo charge scale ([depo][plane], wct_dt_set_charge_scale); used
+    // by calls whose depo count is qscale_n
+    DevBuf d_qscale;
+    size_t qscale_n{0};
+    int qscale_planes{0};
+    bool have_qscale{false};
+    const double* qscale() const { return have_qscale ? d_qscale.as<double>() : nullptr; }
     int config_gen{0};                 // bumped by every change of planes or responses
     std::unique_ptr<struct BatchState> batch;
     WindowDev* h_win{nullptr};
@@ -469,6 +476,8 @@ static int prepare_event(Core& c, const double* d_depos, size_t ndepos, cudaStre
     for (auto& p : c.planes)
         if (!p->have_resp) return fail(WCT_ERR_STATE, "a plane has no response");
     if (ndepos > (size_t)0x7fffffff) return fail(WCT_ERR_SIZE, "too many depos");
+    if (c.have_qscale && (ndepos != c.qscale_n || c.qscale_planes != (int)c.planes.size()))
+        return fail(WCT_ERR_ARG, "the charge scale was set for another depo count or plane set");
     CUDA_TRY(cudaSetDevice(c.device));
     const int n = (int)ndepos;
     const int np = (int)c.planes.size();
@@ -524,14 +533,14 @@ static int prepare_event(Core& c, const double* d_depos, size_t ndepos, cudaStre
     et.blk0[1] = (n + 255) / 256;
     ev.fp = fluc_params(c, fluct, c.frame_count, nullptr);
     if (ev.fp.on_patch) {
-        CUDA_TRY(c.d_fq.ensure(sizeof(double) * (size_t)std::max(n, 1)));
+        CUDA_TRY(c.d_fq.ensure(sizeof(double) * (size_t)np * std::max(n, 1)));
         CUDA_TRY(c.d_fluc.ensure(sizeof(FlucRec) * (size_t)np * std::max(n, 1)));
     }
     auto prep = [&](int b0, int b1) {
         launch_prep_all(d_depos, et, nkeys, c.drifter, c.have_drifter ? 1 : 0, pset, tb, c.drift_speed, c.nsigma,
                         c.d_rec.as<PatchRec>(), c.d_win.as<WindowDev>(), c.d_wcnt.as<int>(), c.d_tprof.as<float>(),
                         c.d_kbound.as<unsigned long long>(), ev.fp, ev.fp.on_patch ? c.d_fq.as<double>() : nullptr,
-                        c.d_wide.as<unsigned char>(), s, b0, b1);
+                        c.d_wide.as<unsigned char>(), s, b0, b1, c.qscale());
     };
     if (h_depos && n > 0) {
         // 4 chunks (whole 256-depo blocks): upload k + 1 runs while the prep of chunk k does
@@ -851,7 +860,7 @@ static int adjoint_device(Core& c, const double* d_depos, size_t ndepos, const f
     }
     Core::StageTimer t_g(&c, 9, s);
     launch_adj_gather(d_depos, n, c.drifter, c.have_drifter ? 1 : 0, ev.pset, as, c.drift_speed,
-                      c.d_rec.as<PatchRec>(), c.d_Q.as<float>(), d_gdep, gg, s);
+                      c.d_rec.as<PatchRec>(), c.d_Q.as<float>(), d_gdep, gg, s, c.qscale());
     t_g.close(n ? (c.have_drifter ? 2 : 1) : 0);
     CUDA_TRY(cudaGetLastError());
     return WCT_OK;
@@ -921,7 +930,9 @@ static std::mutex g_noalloc_mtx;
 static float2* g_noalloc_addr[kNoAllocMaxDevices] = {};
 
 // Device address of the scratch array on the current device, looked up once
-// per device (cudaGetSymbolAddress with that device current).
+// per device (cudaGetSymbolAddress with that device current) and kept for the
+// life of the process: a cudaDeviceReset of that device would leave it stale,
+// and the header rules out calls after one.
 static int noalloc_scratch(float2** out)
 {
     int dev = 0;
@@ -1131,6 +1142,8 @@ static int forward_batch_device(Core& c, const double* d_depos, const long long*
     for (int e = 0; e < nev; ++e)
         if (offsets[e + 1] < offsets[e]) return fail(WCT_ERR_ARG, "forward batch: offsets must not decrease");
     if (nev > 0 && offsets[nev] > 0 && !d_depos) return fail(WCT_ERR_ARG, "forward batch: null depos");
+    if (c.have_qscale && ((size_t)offsets[nev] != c.qscale_n || c.qscale_planes != (int)c.planes.size()))
+        return fail(WCT_ERR_ARG, "the charge scale was set for another depo count or plane set");
     if (first_ident) *first_ident = c.frame_count;
     if (nev == 0) return WCT_OK;
     CUDA_TRY(cudaSetDevice(c.device));
@@ -1180,7 +1193,8 @@ static int forward_batch_device(Core& c, const double* d_depos, const long long*
         const long long nkeysK = (long long)K * bs.nkeys;
         std::vector<void*> before = {b.d_Q.p, b.d_V.p, b.d_rec.p, b.d_tprof.p, b.d_win.p, b.d_wcnt.p, b.d_woff.p,
                                      b.d_wcur.p, b.d_kbound.p, b.d_wlist.p, b.d_plans.p, b.d_fq.p, b.d_fluc.p,
-                                     b.d_ident.p, b.d_pool.p, b.d_pool_off.p, b.d_pool_used.p, b.d_wide.p};
+                                     b.d_ident.p, b.d_pool.p, b.d_pool_off.p, b.d_pool_used.p, b.d_wide.p,
+                                    const_cast<double*>(c.qscale())};
         CUDA_TRY(b.d_Q.ensure(sizeof(float) * (size_t)bs.qslot_total * K));
         CUDA_TRY(b.d_V.ensure(sizeof(float2) * (size_t)bs.vslot_total * K));
         CUDA_TRY(b.d_rec.ensure(sizeof(PatchRec) * (size_t)np * maxdep));
@@ -1200,7 +1214,7 @@ static int forward_batch_device(Core& c, const double* d_depos, const long long*
         CUDA_TRY(b.d_pool_off.ensure(sizeof(int) * (size_t)maxdep));
         CUDA_TRY(b.d_pool_used.ensure(sizeof(unsigned long long)));
         if (c.fluctuate) {
-            CUDA_TRY(b.d_fq.ensure(sizeof(double) * (size_t)maxdep));
+            CUDA_TRY(b.d_fq.ensure(sizeof(double) * (size_t)np * maxdep));
             CUDA_TRY(b.d_fluc.ensure(sizeof(FlucRec) * (size_t)np * maxdep));
         }
         if (!b.h_ident) CUDA_TRY(cudaMallocHost(&b.h_ident, sizeof(int)));
@@ -1251,7 +1265,8 @@ static int forward_batch_device(Core& c, const double* d_depos, const long long*
                 launch_prep_all(dep, et, bs.nkeys, c.drifter, c.have_drifter ? 1 : 0, pset, tb, c.drift_speed,
                                 c.nsigma, b.d_rec.as<PatchRec>(), b.d_win.as<WindowDev>(), b.d_wcnt.as<int>(),
                                 b.d_tprof.as<float>(), b.d_kbound.as<unsigned long long>(), fp,
-                                fp.on_patch ? b.d_fq.as<double>() : nullptr, b.d_wide.as<unsigned char>(), s);
+                                fp.on_patch ? b.d_fq.as<double>() : nullptr, b.d_wide.as<unsigned char>(), s, 0, -1,
+                                c.qscale() ? c.qscale() + (size_t)offsets[c0] * np : nullptr);
                 launch_scan(b.d_wcnt.as<int>(), (int)nk, b.d_woff.as<int>(), b.d_wcur.as<int>(), s);
                 launch_plan_batch(plans + ch, bs, ne, b.d_win.as<WindowDev>(), b.vcap, s);
                 launch_fill(b.d_rec.as<PatchRec>(), et, bs.nkeys, pset, b.d_wcur.as<int>(), b.d_wlist.as<Visit>(),
@@ -2112,6 +2127,35 @@ int wct_dt_frame_shape(const wct_depotransform* h, int* nrows, int* nticks)
     if (!h) return fail(WCT_ERR_ARG, "null component");
     if (nrows) *nrows = h->core.nrows();
     if (nticks) *nticks = h->core.nticks();
+    return WCT_OK;
+}
+
+int wct_dt_set_charge_scale(wct_depotransform* h, const double* scale, size_t ndepos, int on_device)
+{
+    if (!h) return fail(WCT_ERR_ARG, "null component");
+    std::lock_guard<std::mutex> lk(h->core.mtx);
+    Core& c = h->core;
+    if (!scale) {
+        c.have_qscale = false;
+        c.qscale_n = 0;
+        c.qscale_planes = 0;
+        return WCT_OK;
+    }
+    const int np = (int)c.planes.size();
+    if (np == 0) return fail(WCT_ERR_STATE, "wct_dt_set_charge_scale: no planes configured");
+    if (ndepos == 0 || ndepos > (size_t)0x7fffffff)
+        return fail(WCT_ERR_ARG, "wct_dt_set_charge_scale: depo count out of range");
+    CUDA_TRY(cudaSetDevice(c.device));
+    const size_t bytes = sizeof(double) * ndepos * (size_t)np;
+    CUDA_TRY(c.d_qscale.ensure(bytes));
+    // ordered after the work already queued on the component's stream, which
+    // may still read the previous scale
+    CUDA_TRY(cudaMemcpyAsync(c.d_qscale.p, scale, bytes,
+                             on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, c.own_stream));
+    CUDA_TRY(cudaStreamSynchronize(c.own_stream));
+    c.have_qscale = true;
+    c.qscale_n = ndepos;
+    c.qscale_planes = np;
     return WCT_OK;
 }
 

@@ -166,7 +166,8 @@ __global__ void __launch_bounds__(256, 3) k_prep_all(const double* __restrict__ 
                                                   WindowDev* __restrict__ win_all, int* __restrict__ cnt_all,
                                                   float* __restrict__ tprof, unsigned long long* __restrict__ kb_all,
                                                   FlucParams fp, double* __restrict__ fq,
-                                                  unsigned char* __restrict__ wide_all, int blk_offset)
+                                                  unsigned char* __restrict__ wide_all, int blk_offset,
+                                                  const double* __restrict__ qscale)
 {
     const int bid = blockIdx.x + blk_offset;  // a launch may cover a range of the table's blocks
     const int ev = event_of_block(evt, bid);
@@ -224,7 +225,11 @@ __global__ void __launch_bounds__(256, 3) k_prep_all(const double* __restrict__ 
         }
     }
     const int ip = blockIdx.y;
-    if (fq && in && ip == 0) fq[i] = q;  // drifted charge, the trial count of fluctuated patches
+    // DepoTransform::modify_depo (DepoTransform.h:33-35, applied before
+    // BinnedDiffusion_transform::add at DepoTransform.cxx:182) as a per-plane
+    // charge scale, [depo][plane]
+    if (qscale && in) q = __dmul_rn(q, qscale[(size_t)i * ps.nplanes + ip]);
+    if (fq && in) fq[(size_t)ip * n + i] = q;  // the plane's charge: trial count of its fluctuated patch
     // The time profile depends on the depo only (GaussianDiffusion.cxx:124-136):
     // compute it once here for every plane's raster.
     if (ok && ip == 0) {
@@ -422,14 +427,14 @@ void launch_prep_all(const double* depos, const EventTable& et, int nkeys, const
                      const PlaneSet& ps, const TimeDev& tb, double drift_speed, double nsigma, PatchRec* rec,
                      WindowDev* win, int* wire_cnt, float* tprof, unsigned long long* key_bound,
                      const FlucParams& fp, double* fq, unsigned char* wide, cudaStream_t s, int blk_begin,
-                     int blk_end)
+                     int blk_end, const double* qscale)
 {
     const int nb = et.blk0[et.nev];
     const int b0 = std::max(0, blk_begin), b1 = blk_end < 0 ? nb : std::min(blk_end, nb);
     if (b1 <= b0) return;
     k_prep_all<<<dim3(b1 - b0, ps.nplanes), 256, 0, s>>>(depos, et, nkeys, dd, do_drift, ps, tb, drift_speed,
                                                          nsigma, rec, win, wire_cnt, tprof, key_bound, fp, fq, wide,
-                                                         b0);
+                                                         b0, qscale);
 }
 
 // Exclusive scan of the per-key visit counts: block sums, a scan of the
@@ -963,7 +968,7 @@ __global__ void __launch_bounds__(kFlucWarps * 32) k_fluc_sums(const PatchRec* _
         for (int t = lane; t < nt; t += 32) s_t[wib][t] = unit_bin(t, tbs, r.tcr, r.st);
         __syncwarp();
         const float invS = patch_inv_norm(r, pbs, tbs);
-        const double Q = fq[i];
+        const double Q = fq[(size_t)ip * n + i];
         const int nq = (int)fabs(Q);
         const int ev = event_of_depo(evt, i);
         const int ident = fluc_ident(fp, ev), i_ev = i - evt.dep0[ev];

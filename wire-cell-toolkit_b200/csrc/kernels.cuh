@@ -233,7 +233,9 @@ void launch_prep_all(const double* depos, const EventTable& et, int nkeys, const
                      const PlaneSet& ps, const TimeDev& tb, double drift_speed, double nsigma, PatchRec* rec,
                      WindowDev* win, int* wire_cnt, float* tprof, unsigned long long* key_bound,
                      const FlucParams& fp, double* fq, unsigned char* wide, cudaStream_t s, int blk_begin = 0,
-                     int blk_end = -1);  // blocks [blk_begin, blk_end) of the table (-1: to the end)
+                     int blk_end = -1,  // blocks [blk_begin, blk_end) of the table (-1: to the end)
+                     const double* qscale = nullptr);  // [depo][plane] charge scale of the table's depos, or null
+// fq (fluctuation): [plane][depo] charge each plane's patch draws from, written by the prep
 void launch_binomial_samples(unsigned long long seed, int ident, int n, double p, long long count, int* out,
                              cudaStream_t s);
 void launch_fluc_sums(const PatchRec* rec, const EventTable& et, const PlaneSet& ps, float tbs, const FlucParams& fp,
@@ -341,6 +343,6 @@ void launch_wire_conv_adj(const float2* Gh, const float2* Rh, float2* dQh, int G
                           cudaStream_t s);
 void launch_adj_gather(const double* depos, int n, const DriftDev& dd, int do_drift, const PlaneSet& ps,
                        const AdjSet& as, double drift_speed, const PatchRec* rec, const float* dQ, double* grad,
-                       double* gglob, cudaStream_t s);
+                       double* gglob, cudaStream_t s, const double* qscale = nullptr);
 
 }  // namespace wctb200

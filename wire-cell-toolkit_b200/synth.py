@@ -134,6 +134,44 @@ def apa_config(nticks=6000, nwire_half=21):
     return base_config(nticks, planes, ["induction", "induction", "collection"], nwire_half)
 
 
+def apa2_config(nticks=6000, nwire_half=21):
+    """A two-face APA: face 0 drifts from x = +2700 mm to its response plane
+    at +100 mm, face 1 from -2700 mm to -100 mm, the wire planes at x = 0
+    between them (one Drifter x-region per face).  Face 1 sees the
+    induction wires wrapped around the frame: its U and V wires run at the
+    mirrored angles and keep the channel numbers of face 0's U and V (a
+    channel then has a trace from each face, as in the reference's frame);
+    its collection plane has channels of its own.  pirs are per plane index
+    and shared by the faces (DepoTransform.cxx:188)."""
+    f0 = [
+        _plane(800, 4.67 * mm, 35.7, 0, 0, RESPONSE_X),
+        _plane(800, 4.67 * mm, -35.7, 1, 800, RESPONSE_X),
+        _plane(960, 4.79 * mm, 0.0, 2, 1600, RESPONSE_X),
+    ]
+    f1 = [
+        _plane(800, 4.67 * mm, -35.7, 0, 0, -RESPONSE_X),
+        _plane(800, 4.67 * mm, 35.7, 1, 800, -RESPONSE_X),
+        _plane(960, 4.79 * mm, 0.0, 2, 2560, -RESPONSE_X),
+    ]
+    cfg = base_config(nticks, f0 + f1, ["induction", "induction", "collection"] * 2, nwire_half)
+    cfg["fr"] = cfg["fr"][:3] * 2  # the same response objects: one PIR per plane index
+    cfg["drifter"]["xregions"] = [(ANODE_X, RESPONSE_X, CATHODE_X), (ANODE_X, -RESPONSE_X, -CATHODE_X)]
+    cfg["faces"] = [
+        dict(bb=((ANODE_X, -3000.0 * mm, -2300.0 * mm), (CATHODE_X, 3000.0 * mm, 2300.0 * mm)), planes=[0, 1, 2]),
+        dict(bb=((-CATHODE_X, -3000.0 * mm, -2300.0 * mm), (ANODE_X, 3000.0 * mm, 2300.0 * mm)), planes=[3, 4, 5]),
+    ]
+    cfg.pop("face_bb", None)
+    return cfg
+
+
+def apa2_depos(seed=6, ntracks=8, step=0.5 * mm):
+    """Muon tracks through both drift volumes of the two-face APA (some cross
+    the wire planes at x = 0)."""
+    rng = np.random.default_rng(seed)
+    return track_depos(rng, ntracks=ntracks, step=step, lo=(-RESPONSE_X - 2500.0, -3000.0, -1150.0),
+                       hi=(RESPONSE_X + 2500.0, 3000.0, 1150.0))
+
+
 def plane1_depos(n=2000, seed=1, charge=-5000.0, span=4.6 * m, drift=2.5 * m):
     """Point depos uniform in the wire (pitch) coordinate over ``span`` from the
     first wire region edge and in drift distance over [0, drift]."""
