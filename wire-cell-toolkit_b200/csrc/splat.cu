@@ -45,6 +45,10 @@ __global__ void __launch_bounds__(256) k_splat(const double* __restrict__ dep, i
     if (i >= n) return;
     const double* p = dep + 7 * (size_t)i;
     const double t = p[0], q = p[1], x = p[2], y = p[3], z = p[4], el = p[5], et = p[6];
+    // a depo with a NaN or infinite value is dropped, as the transform drops it:
+    // its bin arithmetic is undefined and it would put NaNs in the frame
+    if (!(isfinite(t) && isfinite(q) && isfinite(x) && isfinite(y) && isfinite(z) && isfinite(el) && isfinite(et)))
+        return;
     if (ps.nplanes > 0 && ps.p[0].have_bb) {  // the face's sensitive volume
         const double pp[3] = {x, y, z};
         for (int k = 0; k < 3; ++k) {
