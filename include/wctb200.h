@@ -112,6 +112,18 @@ int wct_pir_waveform(const wct_pir* pir, int path, float* out);
  * removes it. */
 int wct_pir_set_long_responses(wct_pir* pir, int nlong, const int* long_len, const double* long_wave,
                                double long_padding);
+/* The same two builds on the current CUDA device, in the reference's single
+ * precision: its fwd_r2c / spectrum product / inv_c2r chain
+ * (PlaneImpactResponse.cxx:96-146,185-240) through the library's GPU
+ * transforms, the field response binned onto ticks with float sums as the
+ * reference's realseq_t.  The result is the same host-side wct_pir (the
+ * waveforms agree with wct_pir_create's double-precision direct
+ * convolution to single-precision rounding); the grouping, symmetry and
+ * checks are wct_pir_create's. */
+int wct_pir_create_device(const wct_fr_plane* fr, int nshort, const int* short_len, const double* short_wave,
+                          double overall_short_padding, double tick, int nticks, wct_pir** out);
+int wct_pir_set_long_responses_device(wct_pir* pir, int nlong, const int* long_len, const double* long_wave,
+                                      double long_padding);
 /* Length (0: no long-range response) and pad of the long-range response, and its samples. */
 int wct_pir_long_info(const wct_pir* pir, int* nsamples, int* pad);
 int wct_pir_long_waveform(const wct_pir* pir, float* out);
@@ -335,6 +347,24 @@ int wct_dt_set_charge_scale(wct_depotransform* dt, const double* scale, size_t n
  * the kernels. */
 int wct_dt_forward(wct_depotransform* dt, const double* depos, size_t ndepos, float* frame,
                    wct_plane_window* windows, int* frame_ident);
+/* DepoTransform::operator() (gen/src/DepoTransform.cxx:155-224) with its
+ * output as the reference builds it: the trace list of SimpleFrame
+ * (:193-215), one trace per wire with a non-zero sample, trimmed to
+ * [first non-zero, last non-zero] by Waveform::edge
+ * (util/src/Waveform.cxx:136-153), in frame row order (faces, planes,
+ * wires).  Trace k is channel[k], tbin[k], length[k] samples at
+ * charge + offset[k]; *ntraces receives the count (channel, tbin, length and
+ * offset have room for nrows entries).  Every trace lies inside its plane's
+ * window (the frame is zero elsewhere), so only the window blocks cross from
+ * the device: charge holds them one after another and needs at most the sum
+ * over planes of window rows x window ticks floats (capacity; nrows * nticks
+ * always suffices; WCT_ERR_SIZE if it is too small).  The edges are found on
+ * the device and each plane's block comes back as soon as the plane is
+ * final.  *nsamples (may be NULL) receives the number of charge values
+ * written.  windows and frame_ident as wct_dt_forward (may be NULL). */
+int wct_dt_forward_traces(wct_depotransform* dt, const double* depos, size_t ndepos, float* charge, size_t capacity,
+                          int* channel, int* tbin, int* length, long* offset, int* ntraces, size_t* nsamples,
+                          wct_plane_window* windows, int* frame_ident);
 /* The same on device buffers, enqueued on stream (cudaStream_t, NULL = the
  * component's own stream).  Returns after the work is enqueued; one small
  * device-to-host read of the window sizes synchronises the stream mid-way. */

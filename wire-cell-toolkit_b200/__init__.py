@@ -85,6 +85,9 @@ SIGNATURES = {
     "wct_pir_info": (C.c_int, [C.c_void_p] + [C.c_void_p] * 8),
     "wct_pir_waveform": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p]),
     "wct_pir_destroy": (C.c_int, [C.c_void_p]),
+    "wct_pir_create_device": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_double, C.c_double, C.c_int,
+                                        C.POINTER(C.c_void_p)]),
+    "wct_pir_set_long_responses_device": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_double]),
     "wct_pir_set_long_responses": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_double]),
     "wct_pir_long_info": (C.c_int, [C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
     "wct_pir_long_waveform": (C.c_int, [C.c_void_p, C.c_void_p]),
@@ -125,6 +128,9 @@ SIGNATURES = {
                                             C.c_double, C.c_int, C.c_void_p]),
     "wct_dt_frame_shape": (C.c_int, [C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
     "wct_dt_set_charge_scale": (C.c_int, [C.c_void_p, C.c_void_p, C.c_size_t, C.c_int]),
+    "wct_dt_forward_traces": (C.c_int, [C.c_void_p, C.c_void_p, C.c_size_t, C.c_void_p, C.c_size_t, C.c_void_p,
+                                        C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(C.c_int),
+                                        C.POINTER(C.c_size_t), C.c_void_p, C.POINTER(C.c_int)]),
     "wct_dt_forward": (C.c_int, [C.c_void_p, C.c_void_p, C.c_size_t, C.c_void_p, C.c_void_p, C.POINTER(C.c_int)]),
     "wct_dt_forward_device": (C.c_int, [C.c_void_p, C.c_void_p, C.c_size_t, C.c_void_p, C.c_void_p,
                                         C.POINTER(C.c_int), C.c_void_p]),
@@ -195,10 +201,12 @@ def _check(rc):
 class PlaneImpactResponse:
     """Gen::PlaneImpactResponse built from a Response::Schema plane, short
     responses and optional long responses with their padding
-    (gen/src/PlaneImpactResponse.cxx:56-269)."""
+    (gen/src/PlaneImpactResponse.cxx:56-269); ``device=True`` builds the
+    waveforms on the current CUDA device in single precision (the
+    reference's FFT chain), else on the host in double precision."""
 
     def __init__(self, fr, short_responses, overall_short_padding, tick, nticks, long_responses=(),
-                 long_padding=1.5e6):
+                 long_padding=1.5e6, device=False):
         L = lib()
         pp = np.ascontiguousarray(fr["pitchpos"], dtype=np.float64)
         cur = np.ascontiguousarray(fr["current"], dtype=np.float64)
@@ -208,14 +216,16 @@ class PlaneImpactResponse:
         sl = np.array([len(s) for s in shorts] or [0], dtype=np.int32)
         sw = np.concatenate(shorts) if shorts else np.zeros(1)
         h = C.c_void_p()
-        _check(L.wct_pir_create(C.byref(d), len(shorts), sl.ctypes.data, sw.ctypes.data, overall_short_padding,
-                                tick, nticks, C.byref(h)))
+        create = L.wct_pir_create_device if device else L.wct_pir_create
+        _check(create(C.byref(d), len(shorts), sl.ctypes.data, sw.ctypes.data, overall_short_padding, tick, nticks,
+                      C.byref(h)))
         self.h = h
         longs = [np.asarray(w, dtype=np.float64) for w in long_responses]
         if longs:
             ll = np.array([len(w) for w in longs], dtype=np.int32)
             lw = np.concatenate(longs)
-            _check(L.wct_pir_set_long_responses(h, len(longs), ll.ctypes.data, lw.ctypes.data, long_padding))
+            setl = L.wct_pir_set_long_responses_device if device else L.wct_pir_set_long_responses
+            _check(setl(h, len(longs), ll.ctypes.data, lw.ctypes.data, long_padding))
 
     def long_waveform(self):
         """(long-range response samples, pad in ticks); an empty array without one."""
@@ -482,6 +492,48 @@ class DepoTransform:
         _check(lib().wct_dt_forward(self.h, d.ctypes.data if len(d) else None, len(d), frame.ctypes.data,
                                     C.cast(wins, C.c_void_p), C.byref(ident)))
         return frame, [w.as_dict() for w in wins], ident.value
+
+    def forward_traces(self, depos, charge=None, meta=None):
+        """Host-buffer forward returning the reference's trace list: (traces,
+        windows, ident, nsamples) with traces a list of (channel, tbin, charges
+        view) and nsamples the charge values that came back from the device.
+        ``charge`` (float32, e.g. pinned) receives the window blocks (default:
+        nrows * nticks floats); ``meta`` may supply the four per-trace arrays
+        (trace_meta())."""
+        nrows, nticks = self.frame_shape()
+        if charge is None:
+            charge = np.empty(nrows * nticks, dtype=np.float32)
+        if meta is None:
+            meta = self.trace_meta()
+        ch, tb, ln, off = meta
+        wins = (PlaneWindow * len(self.planes))()
+        k, ns, ident = self.forward_traces_raw(depos, charge, meta, wins)
+        flat = charge.reshape(-1)
+        traces = [(int(ch[i]), int(tb[i]), flat[off[i]:off[i] + ln[i]]) for i in range(k)]
+        return traces, [w.as_dict() for w in wins], ident, ns
+
+    def trace_meta(self):
+        """The four per-trace arrays of forward_traces_raw (channel, tbin,
+        length, offset), one entry per frame row."""
+        nrows, _ = self.frame_shape()
+        return (np.empty(nrows, np.int32), np.empty(nrows, np.int32), np.empty(nrows, np.int32),
+                np.empty(nrows, np.int64))
+
+    def forward_traces_raw(self, depos, charge, meta, windows=None):
+        """wct_dt_forward_traces into caller arrays, as a C adapter calls it:
+        returns (ntraces, nsamples, ident); the traces are in meta and charge."""
+        d = np.ascontiguousarray(depos, dtype=np.float64).reshape(-1, 7)
+        assert charge.dtype == np.float32 and charge.flags.c_contiguous
+        ch, tb, ln, off = meta
+        k = C.c_int()
+        ns = C.c_size_t()
+        ident = C.c_int()
+        _check(lib().wct_dt_forward_traces(self.h, d.ctypes.data if len(d) else None, len(d), charge.ctypes.data,
+                                           charge.size, ch.ctypes.data, tb.ctypes.data, ln.ctypes.data,
+                                           off.ctypes.data, C.byref(k), C.byref(ns),
+                                           C.cast(windows, C.c_void_p) if windows is not None else None,
+                                           C.byref(ident)))
+        return k.value, ns.value, ident.value
 
     def forward_device(self, d_depos_ptr, ndepos, d_frame_ptr, stream=None):
         """Device-buffer forward (pointers as ints, e.g. torch.Tensor.data_ptr())."""

@@ -182,15 +182,24 @@ struct Core {
     std::vector<std::unique_ptr<PlaneState>> planes;
     cudaStream_t own_stream{nullptr};
     cudaStream_t copy_stream{nullptr};  // frame downloads of the host API, overlapped with later planes
+    cudaStream_t plane_streams[kMaxPlanes]{};  // each plane's FFT / convolution / inverse chain
+    int plane_stream(int ip, cudaStream_t& out)
+    {
+        if (!plane_streams[ip]) {
+            cudaError_t e = cudaStreamCreateWithFlags(&plane_streams[ip], cudaStreamNonBlocking);
+            if (e != cudaSuccess) return fail(WCT_ERR_CUDA, std::string("plane stream: ") + cudaGetErrorString(e));
+        }
+        out = plane_streams[ip];
+        return WCT_OK;
+    }
     std::map<int, std::unique_ptr<FftPlanDev>> plans;
     // workspace
-    DevBuf d_rec, d_win, d_Q, d_V, d_depos, d_frame, d_wcnt, d_woff, d_wcur, d_wlist, d_tprof, d_kbound;
+    DevBuf d_rec, d_win, d_Q, d_V, d_depos, d_frame, d_wcnt, d_woff, d_wcur, d_wlist, d_tprof;
     DevBuf d_long_z, d_glong;  // long-range step: packed row spectra; adjoint's frame-gradient rows
     DevBuf d_splat;            // DepoFluxSplat accumulator (doubles)
     DevBuf d_gframe, d_gdep, d_gglob;  // adjoint host entry point
     DevBuf d_fq, d_fluc;               // fluctuation: drifted charges, per (plane, depo) draw sums
     DevBuf d_pool, d_pool_off, d_pool_used;  // time profiles of long patches
-    DevBuf d_wide;                           // per visit key: holds a long patch
     // modify_depo charge scale ([depo][plane], wct_dt_set_charge_scale); used
     // by calls whose depo count is qscale_n
     DevBuf d_qscale;
@@ -202,6 +211,9 @@ struct Core {
     std::unique_ptr<struct BatchState> batch;
     WindowDev* h_win{nullptr};
     size_t last_n{0};
+    DevBuf d_edges;             // trace edges of the frame rows (wct_dt_forward_traces)
+    int2* h_edges{nullptr};
+    size_t h_edges_n{0};
     // stage profiling
     static constexpr int kStages = 10;
     bool profiling{false};
@@ -277,8 +289,11 @@ struct Core {
         harvest();
         for (auto e : event_pool) cudaEventDestroy(e);
         if (h_win) cudaFreeHost(h_win);
+        if (h_edges) cudaFreeHost(h_edges);
         if (own_stream) cudaStreamDestroy(own_stream);
         if (copy_stream) cudaStreamDestroy(copy_stream);
+        for (auto& pst : plane_streams)
+            if (pst) cudaStreamDestroy(pst);
     }
 
     int plan_for(int M, FftDesc& d)
@@ -449,6 +464,7 @@ struct EventPlan {
     PlaneSet pset{};
     GridSet gset{};
     std::vector<PlaneWindow> pw;
+    std::vector<size_t> voff;  // per plane: its wire-convolution rows in d_V (complex values)
     int total_visits{0};
 };
 
@@ -520,10 +536,6 @@ static int prepare_event(Core& c, const double* d_depos, size_t ndepos, cudaStre
 
     Core::StageTimer t_prep(&c, 0, s);
     CUDA_TRY(cudaMemsetAsync(c.d_wcnt.p, 0, sizeof(int) * (nkeys + 1), s));
-    CUDA_TRY(c.d_kbound.ensure(sizeof(unsigned long long) * (size_t)nkeys * kTileBlocks));
-    CUDA_TRY(c.d_wide.ensure((size_t)nkeys));
-    CUDA_TRY(cudaMemsetAsync(c.d_wide.p, 0, (size_t)nkeys, s));
-    CUDA_TRY(cudaMemsetAsync(c.d_kbound.p, 0, sizeof(unsigned long long) * (size_t)nkeys * kTileBlocks, s));
     k_win_init<<<1, 64, 0, s>>>(c.d_win.as<WindowDev>(), np);
     EventTable& et = ev.et;
     et.nev = 1;
@@ -539,8 +551,7 @@ static int prepare_event(Core& c, const double* d_depos, size_t ndepos, cudaStre
     auto prep = [&](int b0, int b1) {
         launch_prep_all(d_depos, et, nkeys, c.drifter, c.have_drifter ? 1 : 0, pset, tb, c.drift_speed, c.nsigma,
                         c.d_rec.as<PatchRec>(), c.d_win.as<WindowDev>(), c.d_wcnt.as<int>(), c.d_tprof.as<float>(),
-                        c.d_kbound.as<unsigned long long>(), ev.fp, ev.fp.on_patch ? c.d_fq.as<double>() : nullptr,
-                        c.d_wide.as<unsigned char>(), s, b0, b1, c.qscale());
+                        ev.fp, ev.fp.on_patch ? c.d_fq.as<double>() : nullptr, s, b0, b1, c.qscale());
     };
     if (h_depos && n > 0) {
         // 4 chunks (whole 256-depo blocks): upload k + 1 runs while the prep of chunk k does
@@ -584,8 +595,9 @@ static int prepare_event(Core& c, const double* d_depos, size_t ndepos, cudaStre
     gset = GridSet{};
     gset.nplanes = np;
     gset.ntiles_abs = pset.ntiles;
-    size_t qfloats = 0, vbytes = 0, smem = 0;
+    size_t qfloats = 0, vcomplex = 0, smem = 0;
     int rows = 0;
+    ev.voff.assign(np, 0);
     for (int ip = 0; ip < np; ++ip) {
         PlaneState& ps = *c.planes[ip];
         pw[ip] = window_of(c, ps, c.h_win[ip]);
@@ -611,7 +623,8 @@ static int prepare_event(Core& c, const double* d_depos, size_t ndepos, cudaStre
         g.ntile = fdiv(g.col0 + g.N - 1, kTile) - g.ktile0 + 1;
         rows += g.nin * g.ntile;
         qfloats += (size_t)ps.G * g.nin * g.N;
-        vbytes = std::max(vbytes, sizeof(float2) * (size_t)(g.nin + 2 * ps.npad) * (g.N / 2));
+        ev.voff[ip] = vcomplex;  // each plane its own rows: the planes' chains may run at once
+        if (g.nin) vcomplex += (size_t)(g.nin + 2 * ps.npad) * (g.N / 2);
         if (g.nin) {
             smem = std::max(smem, raster_smem_bytes(g.G));
             int rc = ensure_spectra(c, ps, g.N);
@@ -622,7 +635,7 @@ static int prepare_event(Core& c, const double* d_depos, size_t ndepos, cudaStre
     if (smem > 227 * 1024) return fail(WCT_ERR_SIZE, "event time window too long for the shared-memory charge grid");
     if (qfloats >= (size_t)1 << 40) return fail(WCT_ERR_SIZE, "charge grid too large");
     CUDA_TRY(c.d_Q.ensure(sizeof(float) * std::max<size_t>(qfloats, 1)));
-    CUDA_TRY(c.d_V.ensure(std::max<size_t>(vbytes, 1)));
+    CUDA_TRY(c.d_V.ensure(sizeof(float2) * std::max<size_t>(vcomplex, 1)));
     return WCT_OK;
 }
 
@@ -672,14 +685,26 @@ struct FrameRegion {
     int rlo{0}, rhi{0}, tlo{0}, thi{0};
 };
 
-// plane_done (optional, one event per plane): recorded on s once the plane's
-// frame rows are final, so a caller can download them while later planes run;
+// plane_done (optional, one event per plane): recorded once the plane's
+// frame rows are final (on the plane's stream), so a caller can download them while later planes run;
 // zeroed (optional): recorded once the frame is cleared; regions (optional):
 // each plane's written block, so the zero rest can go first.
+//
+// after_plane (optional): called once a plane's frame work is enqueued, with
+// the plane, its written block and the stream that work is on, to enqueue
+// work that reads the plane's rows (a non-zero return aborts the call with
+// that status).
+//
+// After the raster, each plane's time FFT, wire convolution and inverse run
+// on a stream of their own (forked from s, joined back into s at the end), so
+// the planes' kernels fill one another's last waves; with stage profiling on,
+// or a plane with a long-range response (one shared workspace), they run on
+// s one plane after another.
 static int forward_device(Core& c, const double* d_depos, size_t ndepos, float* d_frame, wct_plane_window* wins,
                           int* frame_ident, cudaStream_t s, cudaEvent_t* plane_done = nullptr,
                           cudaEvent_t zeroed = nullptr, std::vector<FrameRegion>* regions = nullptr,
-                          const double* h_depos = nullptr)
+                          const double* h_depos = nullptr,
+                          const std::function<int(int, const FrameRegion&, cudaStream_t)>& after_plane = nullptr)
 {
     EventPlan ev;
     int prc = prepare_event(c, d_depos, ndepos, s, ev, true, h_depos);
@@ -716,15 +741,25 @@ static int forward_device(Core& c, const double* d_depos, size_t ndepos, float* 
                            c.d_Q.as<float>(), s);
     }
     else
-        launch_raster_wires(c.d_rec.as<PatchRec>(), c.d_tprof.as<float>(), pool, c.d_wide.as<unsigned char>(),
-                            c.d_wcnt.as<int>(),
-                            c.d_woff.as<int>(), c.d_wlist.as<Visit>(), (long long)std::max(total_visits, 1),
-                            c.d_kbound.as<unsigned long long>(), gset, c.d_Q.as<float>(), s);
+        launch_raster_wires(c.d_rec.as<PatchRec>(), c.d_tprof.as<float>(), pool, c.d_wcnt.as<int>(),
+                            c.d_woff.as<int>(), c.d_wlist.as<Visit>(), (long long)std::max(total_visits, 1), gset,
+                            c.d_Q.as<float>(), s);
     t_r.close((n > 0 ? 1 : 0) + (ev.fp.on_patch && n > 0 ? 1 : 0) + (!ev.fp.on_patch && wide > 0 ? 1 : 0) +
               (rows > 0 ? 1 : 0));
     CUDA_TRY(cudaGetLastError());
 
-    for (int ip = 0; ip < np; ++ip) {
+    // the planes' chains: on streams of their own unless profiling or a long-range step needs s alone
+    bool fork = !c.profiling && np > 1;
+    for (int ip = 0; ip < np; ++ip)
+        if (!c.planes[ip]->long_wf.empty()) fork = false;
+    cudaEvent_t rastered = nullptr;
+    if (fork) {
+        rastered = c.take_event();
+        CUDA_TRY(cudaEventRecord(rastered, s));
+    }
+    std::vector<cudaEvent_t> joined;
+    int rc_planes = WCT_OK;
+    for (int ip = 0; ip < np && rc_planes == WCT_OK; ++ip) {
         PlaneState& ps = *c.planes[ip];
         const PlaneWindow& w = pw[ip];
         const GridPlane& g = gset.p[ip];
@@ -745,44 +780,73 @@ static int forward_device(Core& c, const double* d_depos, size_t ndepos, float* 
             o.outside_time = c.h_win[ip].out_time;
             o.outside_pitch = c.h_win[ip].out_pitch;
         }
-        if (g.nin == 0) {  // no charge: the plane's frame rows stay zero
-            if (plane_done) CUDA_TRY(cudaEventRecord(plane_done[ip], s));
-            continue;
+        cudaStream_t ps_s = s;
+        if (fork && g.nin > 0) {
+            int rc = c.plane_stream(ip, ps_s);
+            if (rc) {
+                rc_planes = rc;
+                break;
+            }
+            CUDA_TRY(cudaStreamWaitEvent(ps_s, rastered, 0));
         }
-        const int nin = g.nin;
-        const int nout = nin + 2 * ps.npad;
-        const int N = g.N, M = N / 2;
-        FftDesc d;
-        int rc = c.plan_for(M, d);
-        if (rc) return rc;
-        float* Q = c.d_Q.as<float>() + g.qoff;
-        Core::StageTimer t_f(&c, 2, s);
-        launch_rfft_rows(Q, N, N, reinterpret_cast<float2*>(Q), M, ps.G * nin, d, s);
-        t_f.close(1);
-        Core::StageTimer t_c(&c, 3, s);
-        launch_wire_conv(reinterpret_cast<const float2*>(Q), ps.d_spec.as<float2>(), c.d_V.as<float2>(), ps.G, ps.npad,
-                         nin, nout, M, ps.mirror, s);
-        t_c.close(1);
-        const int wlo = std::max(0, w.m_start_ch), whi = std::min(ps.desc.nwires, w.m_end_ch);
-        Core::StageTimer t_i(&c, 4, s);
-        launch_irfft_rows(c.d_V.as<float2>(), nout, d, w.start_ch - ps.npad, wlo, whi, w.start_tick,
-                          std::min(N, w.nt_ref), nticks, d_frame + (size_t)ps.row0 * nticks, s);
-        if (!ps.long_wf.empty() && whi > wlo) {
-            rc = long_conv_rows(c, ps, d_frame + ((size_t)ps.row0 + wlo) * nticks, nticks, whi - wlo, nticks, false, s);
-            if (rc) return rc;
+        auto plane_chain = [&]() -> int {
+            FrameRegion r;
+            if (g.nin > 0) {  // else: no charge, the plane's frame rows stay zero
+                const int nin = g.nin;
+                const int nout = nin + 2 * ps.npad;
+                const int N = g.N, M = N / 2;
+                FftDesc d;
+                int rc = c.plan_for(M, d);
+                if (rc) return rc;
+                float* Q = c.d_Q.as<float>() + g.qoff;
+                float2* V = c.d_V.as<float2>() + ev.voff[ip];
+                Core::StageTimer t_f(&c, 2, ps_s);
+                launch_rfft_rows(Q, N, N, reinterpret_cast<float2*>(Q), M, ps.G * nin, d, ps_s);
+                t_f.close(1);
+                Core::StageTimer t_c(&c, 3, ps_s);
+                launch_wire_conv(reinterpret_cast<const float2*>(Q), ps.d_spec.as<float2>(), V, ps.G, ps.npad, nin,
+                                 nout, M, ps.mirror, ps_s);
+                t_c.close(1);
+                const int wlo = std::max(0, w.m_start_ch), whi = std::min(ps.desc.nwires, w.m_end_ch);
+                Core::StageTimer t_i(&c, 4, ps_s);
+                launch_irfft_rows(V, nout, d, w.start_ch - ps.npad, wlo, whi, w.start_tick, std::min(N, w.nt_ref),
+                                  nticks, d_frame + (size_t)ps.row0 * nticks, ps_s);
+                if (!ps.long_wf.empty() && whi > wlo) {
+                    rc = long_conv_rows(c, ps, d_frame + ((size_t)ps.row0 + wlo) * nticks, nticks, whi - wlo, nticks,
+                                        false, ps_s);
+                    if (rc) return rc;
+                }
+                if (whi > wlo) {  // what the inverse (and the long-range step) wrote
+                    r.rlo = wlo;
+                    r.rhi = whi;
+                    r.tlo = ps.long_wf.empty() ? std::max(0, w.start_tick) : 0;
+                    r.thi = ps.long_wf.empty() ? std::min(nticks, w.start_tick + std::min(N, w.nt_ref)) : nticks;
+                    if (r.thi < r.tlo) r.thi = r.tlo;
+                }
+                t_i.close(ps.long_wf.empty() || whi <= wlo ? 1 : 6);
+                CUDA_TRY(cudaGetLastError());
+            }
+            if (regions) (*regions)[ip] = r;
+            if (after_plane) {
+                const int arc = after_plane(ip, r, ps_s);
+                if (arc) return arc;
+            }
+            if (plane_done) CUDA_TRY(cudaEventRecord(plane_done[ip], ps_s));
+            return WCT_OK;
+        };
+        rc_planes = plane_chain();
+        if (ps_s != s) {  // join back into s (also after an error, so nothing is left behind)
+            cudaEvent_t e = c.take_event();
+            joined.push_back(e);
+            cudaError_t ce = cudaEventRecord(e, ps_s);
+            if (ce == cudaSuccess) ce = cudaStreamWaitEvent(s, e, 0);
+            if (ce != cudaSuccess && rc_planes == WCT_OK)
+                rc_planes = fail(WCT_ERR_CUDA, std::string("plane join: ") + cudaGetErrorString(ce));
         }
-        if (regions && whi > wlo) {  // what the inverse (and the long-range step) wrote
-            FrameRegion& r = (*regions)[ip];
-            r.rlo = wlo;
-            r.rhi = whi;
-            r.tlo = ps.long_wf.empty() ? std::max(0, w.start_tick) : 0;
-            r.thi = ps.long_wf.empty() ? std::min(nticks, w.start_tick + std::min(N, w.nt_ref)) : nticks;
-            if (r.thi < r.tlo) r.thi = r.tlo;
-        }
-        t_i.close(ps.long_wf.empty() || whi <= wlo ? 1 : 6);
-        CUDA_TRY(cudaGetLastError());
-        if (plane_done) CUDA_TRY(cudaEventRecord(plane_done[ip], s));
     }
+    if (rastered) c.event_pool.push_back(rastered);  // reusable: s and the plane streams have enqueued their waits
+    for (auto e : joined) c.event_pool.push_back(e);
+    if (rc_planes) return rc_planes;
     if (frame_ident) *frame_ident = c.frame_count;
     ++c.frame_count;
     c.last_n = ndepos;
@@ -967,10 +1031,9 @@ struct BatchState {
     std::vector<std::unique_ptr<DevBuf>> spec;  // [plane * ncls + cls]
     DevBuf d_spec_tab;                          // const float2* [plane][ncls]
     int maxM{0}, maxG{0}, nsm{148};
-    DevBuf d_Q, d_V, d_rec, d_tprof, d_win, d_wcnt, d_woff, d_wcur, d_kbound, d_wlist, d_plans;
+    DevBuf d_Q, d_V, d_rec, d_tprof, d_win, d_wcnt, d_woff, d_wcur, d_wlist, d_plans;
     DevBuf d_fq, d_fluc, d_ident;  // fluctuation: drifted charges, draw sums, first frame ident of the call
     DevBuf d_pool, d_pool_off, d_pool_used;  // time profiles of long patches
-    DevBuf d_wide;                           // per key: holds a long patch
     long long pool_cap{0};
     int* h_ident{nullptr};         // pinned source of d_ident
     long long vcap{0};
@@ -1112,7 +1175,7 @@ static size_t batch_slot_bytes(const BatchState& b)
 {
     const BatchStatic& bs = b.bs;
     return sizeof(float) * (size_t)bs.qslot_total + sizeof(float2) * (size_t)bs.vslot_total +
-           (sizeof(int) * 3 + sizeof(unsigned long long) * kTileBlocks) * (size_t)bs.nkeys;
+           sizeof(int) * 3 * (size_t)bs.nkeys;
 }
 
 static int batch_slots(Core& c, int nev)
@@ -1192,8 +1255,8 @@ static int forward_batch_device(Core& c, const double* d_depos, const long long*
     for (int attempt = 0; attempt < 8; ++attempt) {
         const long long nkeysK = (long long)K * bs.nkeys;
         std::vector<void*> before = {b.d_Q.p, b.d_V.p, b.d_rec.p, b.d_tprof.p, b.d_win.p, b.d_wcnt.p, b.d_woff.p,
-                                     b.d_wcur.p, b.d_kbound.p, b.d_wlist.p, b.d_plans.p, b.d_fq.p, b.d_fluc.p,
-                                     b.d_ident.p, b.d_pool.p, b.d_pool_off.p, b.d_pool_used.p, b.d_wide.p,
+                                     b.d_wcur.p, b.d_wlist.p, b.d_plans.p, b.d_fq.p, b.d_fluc.p,
+                                     b.d_ident.p, b.d_pool.p, b.d_pool_off.p, b.d_pool_used.p,
                                      const_cast<double*>(c.qscale())};
         CUDA_TRY(b.d_Q.ensure(sizeof(float) * (size_t)bs.qslot_total * K));
         CUDA_TRY(b.d_V.ensure(sizeof(float2) * (size_t)bs.vslot_total * K));
@@ -1203,8 +1266,6 @@ static int forward_batch_device(Core& c, const double* d_depos, const long long*
         CUDA_TRY(b.d_wcnt.ensure(sizeof(int) * (size_t)(nkeysK + 1)));
         CUDA_TRY(b.d_woff.ensure(sizeof(int) * (size_t)(nkeysK + 1)));
         CUDA_TRY(b.d_wcur.ensure(sizeof(int) * (size_t)(nkeysK + 1 + (nkeysK + 1023) / 1024)));
-        CUDA_TRY(b.d_kbound.ensure(sizeof(unsigned long long) * (size_t)nkeysK * kTileBlocks));
-        CUDA_TRY(b.d_wide.ensure((size_t)nkeysK));
         CUDA_TRY(b.d_wlist.ensure(sizeof(Visit) * (size_t)b.vcap));
         CUDA_TRY(b.d_plans.ensure(sizeof(BatchPlan) * (size_t)nch));
         CUDA_TRY(b.d_ident.ensure(sizeof(int)));
@@ -1219,8 +1280,8 @@ static int forward_batch_device(Core& c, const double* d_depos, const long long*
         }
         if (!b.h_ident) CUDA_TRY(cudaMallocHost(&b.h_ident, sizeof(int)));
         std::vector<void*> after = {b.d_Q.p, b.d_V.p, b.d_rec.p, b.d_tprof.p, b.d_win.p, b.d_wcnt.p, b.d_woff.p,
-                                    b.d_wcur.p, b.d_kbound.p, b.d_wlist.p, b.d_plans.p, b.d_fq.p, b.d_fluc.p,
-                                    b.d_ident.p, b.d_pool.p, b.d_pool_off.p, b.d_pool_used.p, b.d_wide.p,
+                                    b.d_wcur.p, b.d_wlist.p, b.d_plans.p, b.d_fq.p, b.d_fluc.p,
+                                    b.d_ident.p, b.d_pool.p, b.d_pool_off.p, b.d_pool_used.p,
                                     const_cast<double*>(c.qscale())};
         if (b.h_plans_n < (size_t)nch) {
             if (b.h_plans) cudaFreeHost(b.h_plans);
@@ -1257,16 +1318,13 @@ static int forward_batch_device(Core& c, const double* d_depos, const long long*
                 const long long nk = (long long)ne * bs.nkeys;
                 const double* dep = d_depos ? d_depos + 7 * offsets[c0] : nullptr;
                 cudaMemsetAsync(b.d_wcnt.p, 0, sizeof(int) * (size_t)(nk + 1), s);
-                cudaMemsetAsync(b.d_kbound.p, 0, sizeof(unsigned long long) * (size_t)nk * kTileBlocks, s);
-                cudaMemsetAsync(b.d_wide.p, 0, (size_t)nk, s);
                 k_win_init<<<(ne * np + 63) / 64, 64, 0, s>>>(b.d_win.as<WindowDev>(), ne * np);
                 // random streams keyed by the frame ident of each event: base (a device
                 // value written before every launch of the graph) + c0 + event
                 const FlucParams fp = fluc_params(c, true, c0, b.d_ident.as<int>());
                 launch_prep_all(dep, et, bs.nkeys, c.drifter, c.have_drifter ? 1 : 0, pset, tb, c.drift_speed,
                                 c.nsigma, b.d_rec.as<PatchRec>(), b.d_win.as<WindowDev>(), b.d_wcnt.as<int>(),
-                                b.d_tprof.as<float>(), b.d_kbound.as<unsigned long long>(), fp,
-                                fp.on_patch ? b.d_fq.as<double>() : nullptr, b.d_wide.as<unsigned char>(), s, 0, -1,
+                                b.d_tprof.as<float>(), fp, fp.on_patch ? b.d_fq.as<double>() : nullptr, s, 0, -1,
                                 c.qscale() ? c.qscale() + (size_t)offsets[c0] * np : nullptr);
                 launch_scan(b.d_wcnt.as<int>(), (int)nk, b.d_woff.as<int>(), b.d_wcur.as<int>(), s);
                 launch_plan_batch(plans + ch, bs, ne, b.d_win.as<WindowDev>(), b.vcap, s);
@@ -1283,9 +1341,8 @@ static int forward_batch_device(Core& c, const double* d_depos, const long long*
                     launch_tprof_pool(b.d_rec.as<PatchRec>(), et, np, (float)tb.bs, pool, &plans[ch].status, s);
                 }
                 launch_raster_batch(plans + ch, bs, pset, b.d_rec.as<PatchRec>(), et.dep0[ne], b.d_tprof.as<float>(),
-                                    pool, b.d_wide.as<unsigned char>(), b.d_wcnt.as<int>(), b.d_woff.as<int>(), b.d_wlist.as<Visit>(), b.vcap,
-                                    b.d_kbound.as<unsigned long long>(), b.d_Q.as<float>(), nb_r, b.maxG, et, fp,
-                                    b.d_fluc.as<FlucRec>(), s);
+                                    pool, b.d_wcnt.as<int>(), b.d_woff.as<int>(), b.d_wlist.as<Visit>(), b.vcap,
+                                    b.d_Q.as<float>(), nb_r, b.maxG, et, fp, b.d_fluc.as<FlucRec>(), s);
                 launch_rfft_batch(plans + ch, b.d_descs.as<FftDesc>(), b.d_Q.as<float>(), nb_f, b.tune.fft_threads,
                                   b.maxM, s);
                 // one launch per run of planes that share the pad and the group pairing
@@ -1800,6 +1857,112 @@ int wct_pir_create(const wct_fr_plane* fr, int nshort, const int* short_len, con
     catch (std::exception& e) {
         return fail(WCT_ERR_CONFIG, e.what());
     }
+}
+
+// The spectrum product of nw real responses (concatenated in wave, lengths
+// len; each cut or zero padded to n), and optionally its real inverse: the
+// reference's "short_spec" / "long_spec" chain (PlaneImpactResponse.cxx:96-146)
+// in single precision on the current device.  spec receives the product
+// spectrum [n]; real (optional, host) the real inverse [n].
+static int response_chain_device(int nw, const int* len, const double* wave, int n, DevBuf& spec, float* real,
+                                 cudaStream_t s)
+{
+    std::vector<float2> rows((size_t)nw * n, make_float2(0.f, 0.f));
+    size_t off = 0;
+    for (int i = 0; i < nw; ++i) {
+        for (int k = 0; k < n && k < len[i]; ++k) rows[(size_t)i * n + k].x = (float)wave[off + k];
+        off += len[i];
+    }
+    DevBuf d_rows, d_out;
+    CUDA_TRY(d_rows.ensure(sizeof(float2) * rows.size()));
+    CUDA_TRY(spec.ensure(sizeof(float2) * (size_t)n));
+    CUDA_TRY(cudaMemcpyAsync(d_rows.p, rows.data(), sizeof(float2) * rows.size(), cudaMemcpyHostToDevice, s));
+    int rc = dft_rows(d_rows.as<float2>(), n, d_rows.as<float2>(), n, nw, n, -1, s);
+    if (rc) return rc;
+    launch_spec_chain(d_rows.as<float2>(), nw, n, spec.as<float2>(), s);
+    if (real) {
+        CUDA_TRY(d_out.ensure(sizeof(float) * (size_t)n));
+        rc = dft_rows(spec.as<float2>(), n, d_rows.as<float2>(), n, 1, n, +1, s);
+        if (rc) return rc;
+        launch_real_rows(d_rows.as<float2>(), 1, n, d_out.as<float>(), n, s);
+        CUDA_TRY(cudaMemcpyAsync(real, d_out.p, sizeof(float) * (size_t)n, cudaMemcpyDeviceToHost, s));
+    }
+    CUDA_TRY(cudaGetLastError());
+    CUDA_TRY(cudaStreamSynchronize(s));  // rows, d_rows and d_out go out of scope
+    return WCT_OK;
+}
+
+int wct_pir_create_device(const wct_fr_plane* fr, int nshort, const int* short_len, const double* short_wave,
+                          double overall_short_padding, double tick, int nticks, wct_pir** out)
+{
+    if (!fr || !out || !fr->pitchpos || !fr->current || fr->npaths <= 0 || fr->nsamples <= 0 || nticks <= 0 ||
+        tick <= 0 || nshort < 0 || (nshort && (!short_len || !short_wave)))
+        return fail(WCT_ERR_ARG, "wct_pir_create_device: bad arguments");
+    for (int i = 0; i < nshort; ++i)
+        if (short_len[i] < 0) return fail(WCT_ERR_ARG, "wct_pir_create_device: negative short response length");
+    std::unique_ptr<wct_pir> p;
+    try {
+        p = std::make_unique<wct_pir>();
+        p->pir = build_pir_layout(fr->npaths, fr->nsamples, fr->pitchpos, fr->pitch, fr->tstart, fr->period,
+                                  overall_short_padding, tick, nticks);
+    }
+    catch (std::exception& e) {
+        return fail(WCT_ERR_CONFIG, e.what());
+    }
+    Pir& pir = p->pir;
+    const int n = pir.n_short, np = fr->npaths;
+    cudaStream_t s = cudaStreamPerThread;
+    DevBuf d_short, d_cur, d_Z, d_wf;
+    // short responses: the product of their spectra (PlaneImpactResponse.cxx:96-121)
+    if (nshort) {
+        int rc = response_chain_device(nshort, short_len, short_wave, n, d_short, nullptr, s);
+        if (rc) return rc;
+    }
+    // each path: tick-binned charge, spectrum x short spectrum, real inverse, cut to nticks (:185-240)
+    CUDA_TRY(d_cur.ensure(sizeof(double) * (size_t)np * fr->nsamples));
+    CUDA_TRY(d_Z.ensure(sizeof(float2) * (size_t)np * n));
+    CUDA_TRY(d_wf.ensure(sizeof(float) * (size_t)np * nticks));
+    CUDA_TRY(cudaMemcpyAsync(d_cur.p, fr->current, sizeof(double) * (size_t)np * fr->nsamples,
+                             cudaMemcpyHostToDevice, s));
+    const double rawbs = (fr->tstart + fr->nsamples * fr->period - fr->tstart) / fr->nsamples;  // Binning
+    launch_pir_bin(d_cur.as<double>(), np, fr->nsamples, fr->tstart, rawbs, fr->period, tick, n, d_Z.as<float2>(), s);
+    if (nshort) {
+        int rc = dft_rows(d_Z.as<float2>(), n, d_Z.as<float2>(), n, np, n, -1, s);
+        if (rc) return rc;
+        launch_cmul_rows(d_Z.as<float2>(), n, np, d_short.as<float2>(), false, s);
+        rc = dft_rows(d_Z.as<float2>(), n, d_Z.as<float2>(), n, np, n, +1, s);
+        if (rc) return rc;
+    }
+    launch_real_rows(d_Z.as<float2>(), np, n, d_wf.as<float>(), nticks, s);
+    std::vector<float> wf((size_t)np * nticks);
+    CUDA_TRY(cudaMemcpyAsync(wf.data(), d_wf.p, sizeof(float) * wf.size(), cudaMemcpyDeviceToHost, s));
+    CUDA_TRY(cudaGetLastError());
+    CUDA_TRY(cudaStreamSynchronize(s));
+    for (int ip = 0; ip < np; ++ip)
+        pir.waveform[ip].assign(wf.begin() + (size_t)ip * nticks, wf.begin() + (size_t)(ip + 1) * nticks);
+    *out = p.release();
+    return WCT_OK;
+}
+
+int wct_pir_set_long_responses_device(wct_pir* p, int nlong, const int* long_len, const double* long_wave,
+                                      double long_padding)
+{
+    if (!p || nlong < 0 || (nlong && (!long_len || !long_wave)) || long_padding < 0)
+        return fail(WCT_ERR_ARG, "wct_pir_set_long_responses_device: bad arguments");
+    for (int i = 0; i < nlong; ++i)
+        if (long_len[i] < 0) return fail(WCT_ERR_ARG, "wct_pir_set_long_responses_device: negative length");
+    Pir& pir = p->pir;
+    pir.long_wf.clear();
+    pir.long_pad = 0;
+    if (nlong == 0) return WCT_OK;
+    const int n = (int)fft_best_length((size_t)pir.nticks, false);
+    std::vector<float> wf(n);
+    DevBuf spec;
+    int rc = response_chain_device(nlong, long_len, long_wave, n, spec, wf.data(), cudaStreamPerThread);
+    if (rc) return rc;
+    pir.long_wf.assign(wf.begin(), wf.end());
+    pir.long_pad = (int)(long_padding / pir.tick);
+    return WCT_OK;
 }
 
 int wct_pir_set_long_responses(wct_pir* p, int nlong, const int* long_len, const double* long_wave,
@@ -2417,6 +2580,91 @@ int wct_dt_eos(wct_depotransform* h)
 {
     if (!h) return fail(WCT_ERR_ARG, "null component");
     return WCT_EOS;
+}
+
+int wct_dt_forward_traces(wct_depotransform* h, const double* depos, size_t ndepos, float* charge, size_t capacity,
+                          int* channel, int* tbin, int* length, long* offset, int* ntraces, size_t* nsamples,
+                          wct_plane_window* windows, int* frame_ident)
+{
+    if (!h || (ndepos && !depos) || !channel || !tbin || !length || !offset || !ntraces)
+        return fail(WCT_ERR_ARG, "wct_dt_forward_traces: bad arguments");
+    std::lock_guard<std::mutex> lk(h->core.mtx);
+    Core& c = h->core;
+    CUDA_TRY(cudaSetDevice(c.device));
+    cudaStream_t s = c.own_stream;
+    const int np = (int)c.planes.size(), nt = c.nticks();
+    CUDA_TRY(c.d_depos.ensure(sizeof(double) * 7 * std::max<size_t>(ndepos, 1)));
+    CUDA_TRY(c.d_frame.ensure(sizeof(float) * (size_t)c.nrows() * nt));
+    CUDA_TRY(c.d_edges.ensure(sizeof(int2) * (size_t)std::max(c.nrows(), 1)));
+    if (c.h_edges_n < (size_t)c.nrows()) {
+        if (c.h_edges) cudaFreeHost(c.h_edges);
+        c.h_edges = nullptr;
+        CUDA_TRY(cudaMallocHost(&c.h_edges, sizeof(int2) * (size_t)std::max(c.nrows(), 1)));
+        c.h_edges_n = c.nrows();
+    }
+    std::vector<cudaEvent_t> done(np);
+    for (auto& ev : done) ev = c.take_event();
+    // each plane's block (window rows x window ticks; the frame is zero
+    // outside it) and the edges of its rows go back on the copy stream as
+    // soon as the plane is final, while later planes are transformed
+    std::vector<FrameRegion> reg(np);
+    std::vector<size_t> boff(np + 1, 0);
+    const float* df = c.d_frame.as<float>();
+    int2* de = c.d_edges.as<int2>();
+    auto after = [&](int ip, const FrameRegion& r, cudaStream_t ps_s) -> int {
+        reg[ip] = r;
+        const size_t w = (size_t)std::max(0, r.thi - r.tlo);
+        const size_t blk = r.rhi > r.rlo ? (size_t)(r.rhi - r.rlo) * w : 0;
+        boff[ip + 1] = boff[ip] + blk;
+        if (blk == 0) return WCT_OK;
+        if (boff[ip + 1] > capacity)
+            return fail(WCT_ERR_SIZE, "wct_dt_forward_traces: the charge buffer holds fewer samples than the windows");
+        if (!charge) return fail(WCT_ERR_ARG, "wct_dt_forward_traces: null charge buffer");
+        const int base = c.planes[ip]->row0;
+        launch_row_edges(df, nt, base + r.rlo, r.rhi - r.rlo, r.tlo, r.thi, de + base + r.rlo, ps_s);
+        cudaError_t e = cudaGetLastError();
+        if (e == cudaSuccess) e = cudaEventRecord(done[ip], ps_s);
+        if (e == cudaSuccess) e = cudaStreamWaitEvent(c.copy_stream, done[ip], 0);
+        if (e == cudaSuccess)
+            e = cudaMemcpy2DAsync(charge + boff[ip], sizeof(float) * w, df + (size_t)(base + r.rlo) * nt + r.tlo,
+                                  sizeof(float) * (size_t)nt, sizeof(float) * w, r.rhi - r.rlo, cudaMemcpyDeviceToHost,
+                                  c.copy_stream);
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(c.h_edges + base + r.rlo, de + base + r.rlo, sizeof(int2) * (r.rhi - r.rlo),
+                                cudaMemcpyDeviceToHost, c.copy_stream);
+        if (e != cudaSuccess)
+            return fail(WCT_ERR_CUDA, std::string("wct_dt_forward_traces: download: ") + cudaGetErrorString(e));
+        return WCT_OK;
+    };
+    int rc = forward_device(c, c.d_depos.as<double>(), ndepos, c.d_frame.as<float>(), windows, frame_ident, s,
+                            nullptr, nullptr, nullptr, ndepos ? depos : nullptr, after);
+    cudaError_t e1 = cudaStreamSynchronize(c.copy_stream);
+    cudaError_t e2 = cudaStreamSynchronize(s);
+    for (auto& ev : done) c.event_pool.push_back(ev);
+    if (rc) return rc;
+    if (e1 != cudaSuccess || e2 != cudaSuccess)
+        return fail(WCT_ERR_CUDA,
+                    std::string("wct_dt_forward_traces: ") + cudaGetErrorString(e1 != cudaSuccess ? e1 : e2));
+    // traces in frame row order (DepoTransform.cxx:193-208)
+    int k = 0;
+    for (int ip = 0; ip < np; ++ip) {
+        const FrameRegion& r = reg[ip];
+        if (boff[ip + 1] == boff[ip]) continue;
+        const PlaneState& ps = *c.planes[ip];
+        const size_t w = (size_t)(r.thi - r.tlo);
+        for (int row = r.rlo; row < r.rhi; ++row) {
+            const int2 ed = c.h_edges[ps.row0 + row];
+            if (ed.y <= ed.x) continue;
+            channel[k] = ps.channels[row];
+            tbin[k] = r.tlo + ed.x;
+            length[k] = ed.y - ed.x;
+            offset[k] = (long)(boff[ip] + (size_t)(row - r.rlo) * w + ed.x);
+            ++k;
+        }
+    }
+    *ntraces = k;
+    if (nsamples) *nsamples = boff[np];
+    return WCT_OK;
 }
 
 int wct_dt_traces(const wct_depotransform* h, const float* frame, int* channel, int* tbin, int* length, long* offset,

@@ -47,9 +47,8 @@ int Pir::closest(double relpitch) const
     return irind;
 }
 
-Pir build_pir(int npaths, int nsamples, const double* pitchpos, const double* current, double fr_pitch,
-              double tstart, double period, const std::vector<std::vector<double>>& shorts,
-              double overall_short_padding, double tick, int nticks)
+Pir build_pir_layout(int npaths, int nsamples, const double* pitchpos, double fr_pitch, double tstart,
+                     double period, double overall_short_padding, double tick, int nticks)
 {
     const int n_per = 6;  // six paths per wire region (PlaneImpactResponse.cxx:164)
     if (npaths < n_per || npaths % n_per) throw std::runtime_error("field response must hold 6 paths per wire");
@@ -61,6 +60,43 @@ Pir build_pir(int npaths, int nsamples, const double* pitchpos, const double* cu
     p.waveform_pad = (int)(overall_short_padding / tick);
     const size_t n_short = fft_best_length((size_t)(overall_short_padding / tick), false);
     p.n_short = (int)n_short;
+    const int n_wires = npaths / n_per;
+    const int n_wires_half = n_wires / 2;
+    p.impact = std::abs(pitchpos[1] - pitchpos[0]);
+    p.half_extent = std::max(std::abs(pitchpos[0]), std::abs(pitchpos[npaths - 1]));
+    p.pitch = 2.0 * std::abs(pitchpos[n_per - 1] - pitchpos[0]);
+    // every sample of the field response must land in the short window (:196-205);
+    // sample times grow with the index, so the first and the last decide
+    const double rawmax = tstart + nsamples * period;
+    const double rawbs = (rawmax - tstart) / nsamples;
+    for (int r = 0; r < nsamples; r += std::max(1, nsamples - 1)) {
+        const double time = tstart + (r + 0.5) * rawbs;  // Binning::center
+        if (!(time >= 0.0)) throw std::runtime_error("out of bounds field response (sample before t = 0)");
+        if ((size_t)(time / tick) >= n_short) throw std::runtime_error("out of bounds field response");
+    }
+    const double oopsilon = 1e-15 * fr_pitch;
+    std::map<int, std::vector<int>> wire_to_ind;
+    for (int ip = 0; ip < npaths; ++ip)
+        wire_to_ind[int(std::ceil((pitchpos[ip] - oopsilon) / fr_pitch))].push_back(ip);
+    for (int irel = -n_wires_half; irel <= n_wires_half; ++irel) {
+        const auto& direct = wire_to_ind[irel];
+        const auto& other = wire_to_ind[-irel];
+        std::vector<int> idx(direct.begin(), direct.end());
+        if (!other.empty())
+            for (auto it = other.rbegin() + 1; it != other.rend(); ++it) idx.push_back(*it);
+        p.bywire.push_back(idx);
+    }
+    p.waveform.assign(npaths, std::vector<float>(nticks, 0.0f));
+    return p;
+}
+
+Pir build_pir(int npaths, int nsamples, const double* pitchpos, const double* current, double fr_pitch,
+              double tstart, double period, const std::vector<std::vector<double>>& shorts,
+              double overall_short_padding, double tick, int nticks)
+{
+    Pir p = build_pir_layout(npaths, nsamples, pitchpos, fr_pitch, tstart, period, overall_short_padding, tick,
+                             nticks);
+    const size_t n_short = (size_t)p.n_short;
     // circular product of the short responses, each cut or zero padded to n_short
     std::vector<double> kern(n_short, 0.0);
     kern[0] = 1.0;
@@ -74,19 +110,9 @@ Pir build_pir(int npaths, int nsamples, const double* pitchpos, const double* cu
         }
         kern.swap(out);
     }
-    const int n_wires = npaths / n_per;
-    const int n_wires_half = n_wires / 2;
-    p.impact = std::abs(pitchpos[1] - pitchpos[0]);
-    p.half_extent = std::max(std::abs(pitchpos[0]), std::abs(pitchpos[npaths - 1]));
-    p.pitch = 2.0 * std::abs(pitchpos[n_per - 1] - pitchpos[0]);
     const double rawmax = tstart + nsamples * period;
     const double rawbs = (rawmax - tstart) / nsamples;
-    const double oopsilon = 1e-15 * fr_pitch;
-    std::map<int, std::vector<int>> wire_to_ind;
-    p.waveform.assign(npaths, std::vector<float>(nticks, 0.0f));
     for (int ip = 0; ip < npaths; ++ip) {
-        const int wirenum = int(std::ceil((pitchpos[ip] - oopsilon) / fr_pitch));
-        wire_to_ind[wirenum].push_back(ip);
         std::vector<double> wave(n_short, 0.0);
         for (int r = 0; r < nsamples; ++r) {
             const double time = tstart + (r + 0.5) * rawbs;  // Binning::center
@@ -103,14 +129,6 @@ Pir build_pir(int npaths, int nsamples, const double* pitchpos, const double* cu
                 for (size_t b = 0; b < n_short; ++b) wf[(a + b) % n_short] += wave[a] * kern[b];
             }
         for (int k = 0; k < nticks && k < (int)n_short; ++k) p.waveform[ip][k] = (float)wf[k];
-    }
-    for (int irel = -n_wires_half; irel <= n_wires_half; ++irel) {
-        const auto& direct = wire_to_ind[irel];
-        const auto& other = wire_to_ind[-irel];
-        std::vector<int> idx(direct.begin(), direct.end());
-        if (!other.empty())
-            for (auto it = other.rbegin() + 1; it != other.rend(); ++it) idx.push_back(*it);
-        p.bywire.push_back(idx);
     }
     return p;
 }

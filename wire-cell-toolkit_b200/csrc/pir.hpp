@@ -37,6 +37,13 @@ struct Pir {
     int closest(double relpitch) const;
 };
 
+// Everything of PlaneImpactResponse::build_responses but the waveforms
+// (left zero): pitch, impact, half extent, the wire grouping of the paths by
+// ceil() and its mirror symmetry (:155-268), the short window length, and the
+// check that every field-response sample lands in it.
+Pir build_pir_layout(int npaths, int nsamples, const double* pitchpos, double fr_pitch, double tstart,
+                     double period, double overall_short_padding, double tick, int nticks);
+
 // PlaneImpactResponse::build_responses without long responses.  The
 // per-path response is the circular convolution (length n_short) of the
 // tick-binned field-response charge with the product of the short responses,
