@@ -205,6 +205,8 @@ def run_b200(args):
     synth = importlib.import_module("wire-cell-toolkit_b200.synth")
     cfg = synth.apa_config()
     depos = synth.apa_depos(seed=2 + rank)
+    if args.depos:  # a smaller workload (profiling): the event's first depos
+        depos = np.ascontiguousarray(depos[:args.depos])
     n = len(depos)
     dt = wct.from_config(cfg, device=local)
     # a dedicated (non-default) stream: the library and the timing events share it
@@ -712,6 +714,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-patterns", action="store_true", help="skip the adjoint / batched / fluctuated lines")
     ap.add_argument("--no-calibration", action="store_true", help="skip the large batched calibration")
+    ap.add_argument("--depos", type=int, default=0,
+                    help="time only the event's first DEPOS depos (a small case for profilers); 0: the whole event")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
