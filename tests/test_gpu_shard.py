@@ -2,8 +2,7 @@
 (the shares never wait on one another), checked against the whole.
 
 * plane split: a DepoTransform configured with a subset of the planes gives
-  the full configuration's frame rows of those planes (to FP32 rounding:
-  charge-grid cells are summed in visit-list order);
+  the full configuration's frame rows of those planes, bit for bit;
 * event split: the calibration objective (loss and drift-parameter
   gradients) of all events equals the sum of the objectives of the greedy
   event shards, which is what the per-step all-reduce of a multi-rank fit
@@ -13,8 +12,6 @@ import importlib
 
 import numpy as np
 import pytest
-
-from conftest import rel_l2
 
 
 @pytest.mark.gpu
@@ -31,7 +28,7 @@ def test_plane_split_rows_match(wct, synth):
         rows.append(np.asarray(f))
     import torch
     stacked = shard.face_order(torch.from_numpy(np.concatenate(rows)), parts, nw).numpy()
-    assert rel_l2(stacked, np.asarray(full)) < 1e-6  # FP32 cell sums in visit-list order
+    assert np.array_equal(stacked, np.asarray(full))
 
 
 @pytest.mark.gpu

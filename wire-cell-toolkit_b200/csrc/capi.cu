@@ -194,12 +194,13 @@ struct Core {
     }
     std::map<int, std::unique_ptr<FftPlanDev>> plans;
     // workspace
-    DevBuf d_rec, d_win, d_Q, d_V, d_depos, d_frame, d_wcnt, d_woff, d_wcur, d_wlist, d_tprof;
+    DevBuf d_rec, d_win, d_Q, d_V, d_depos, d_frame, d_wcnt, d_woff, d_wcur, d_wlist, d_tprof, d_kbound;
     DevBuf d_long_z, d_glong;  // long-range step: packed row spectra; adjoint's frame-gradient rows
     DevBuf d_splat;            // DepoFluxSplat accumulator (doubles)
     DevBuf d_gframe, d_gdep, d_gglob;  // adjoint host entry point
     DevBuf d_fq, d_fluc;               // fluctuation: drifted charges, per (plane, depo) draw sums
     DevBuf d_pool, d_pool_off, d_pool_used;  // time profiles of long patches
+    DevBuf d_wide;                           // per visit key: holds a long patch
     // modify_depo charge scale ([depo][plane], wct_dt_set_charge_scale); used
     // by calls whose depo count is qscale_n
     DevBuf d_qscale;
@@ -536,6 +537,10 @@ static int prepare_event(Core& c, const double* d_depos, size_t ndepos, cudaStre
 
     Core::StageTimer t_prep(&c, 0, s);
     CUDA_TRY(cudaMemsetAsync(c.d_wcnt.p, 0, sizeof(int) * (nkeys + 1), s));
+    CUDA_TRY(c.d_kbound.ensure(sizeof(unsigned long long) * (size_t)nkeys * kTileBlocks));
+    CUDA_TRY(c.d_wide.ensure((size_t)nkeys));
+    CUDA_TRY(cudaMemsetAsync(c.d_wide.p, 0, (size_t)nkeys, s));
+    CUDA_TRY(cudaMemsetAsync(c.d_kbound.p, 0, sizeof(unsigned long long) * (size_t)nkeys * kTileBlocks, s));
     k_win_init<<<1, 64, 0, s>>>(c.d_win.as<WindowDev>(), np);
     EventTable& et = ev.et;
     et.nev = 1;
@@ -551,7 +556,8 @@ static int prepare_event(Core& c, const double* d_depos, size_t ndepos, cudaStre
     auto prep = [&](int b0, int b1) {
         launch_prep_all(d_depos, et, nkeys, c.drifter, c.have_drifter ? 1 : 0, pset, tb, c.drift_speed, c.nsigma,
                         c.d_rec.as<PatchRec>(), c.d_win.as<WindowDev>(), c.d_wcnt.as<int>(), c.d_tprof.as<float>(),
-                        ev.fp, ev.fp.on_patch ? c.d_fq.as<double>() : nullptr, s, b0, b1, c.qscale());
+                        c.d_kbound.as<unsigned long long>(), ev.fp, ev.fp.on_patch ? c.d_fq.as<double>() : nullptr,
+                        c.d_wide.as<unsigned char>(), s, b0, b1, c.qscale());
     };
     if (h_depos && n > 0) {
         // 4 chunks (whole 256-depo blocks): upload k + 1 runs while the prep of chunk k does
@@ -741,9 +747,10 @@ static int forward_device(Core& c, const double* d_depos, size_t ndepos, float* 
                            c.d_Q.as<float>(), s);
     }
     else
-        launch_raster_wires(c.d_rec.as<PatchRec>(), c.d_tprof.as<float>(), pool, c.d_wcnt.as<int>(),
-                            c.d_woff.as<int>(), c.d_wlist.as<Visit>(), (long long)std::max(total_visits, 1), gset,
-                            c.d_Q.as<float>(), s);
+        launch_raster_wires(c.d_rec.as<PatchRec>(), c.d_tprof.as<float>(), pool, c.d_wide.as<unsigned char>(),
+                            c.d_wcnt.as<int>(),
+                            c.d_woff.as<int>(), c.d_wlist.as<Visit>(), (long long)std::max(total_visits, 1),
+                            c.d_kbound.as<unsigned long long>(), gset, c.d_Q.as<float>(), s);
     t_r.close((n > 0 ? 1 : 0) + (ev.fp.on_patch && n > 0 ? 1 : 0) + (!ev.fp.on_patch && wide > 0 ? 1 : 0) +
               (rows > 0 ? 1 : 0));
     CUDA_TRY(cudaGetLastError());
@@ -1031,9 +1038,10 @@ struct BatchState {
     std::vector<std::unique_ptr<DevBuf>> spec;  // [plane * ncls + cls]
     DevBuf d_spec_tab;                          // const float2* [plane][ncls]
     int maxM{0}, maxG{0}, nsm{148};
-    DevBuf d_Q, d_V, d_rec, d_tprof, d_win, d_wcnt, d_woff, d_wcur, d_wlist, d_plans;
+    DevBuf d_Q, d_V, d_rec, d_tprof, d_win, d_wcnt, d_woff, d_wcur, d_kbound, d_wlist, d_plans;
     DevBuf d_fq, d_fluc, d_ident;  // fluctuation: drifted charges, draw sums, first frame ident of the call
     DevBuf d_pool, d_pool_off, d_pool_used;  // time profiles of long patches
+    DevBuf d_wide;                           // per key: holds a long patch
     long long pool_cap{0};
     int* h_ident{nullptr};         // pinned source of d_ident
     long long vcap{0};
@@ -1175,7 +1183,7 @@ static size_t batch_slot_bytes(const BatchState& b)
 {
     const BatchStatic& bs = b.bs;
     return sizeof(float) * (size_t)bs.qslot_total + sizeof(float2) * (size_t)bs.vslot_total +
-           sizeof(int) * 3 * (size_t)bs.nkeys;
+           (sizeof(int) * 3 + sizeof(unsigned long long) * kTileBlocks) * (size_t)bs.nkeys;
 }
 
 static int batch_slots(Core& c, int nev)
@@ -1255,8 +1263,8 @@ static int forward_batch_device(Core& c, const double* d_depos, const long long*
     for (int attempt = 0; attempt < 8; ++attempt) {
         const long long nkeysK = (long long)K * bs.nkeys;
         std::vector<void*> before = {b.d_Q.p, b.d_V.p, b.d_rec.p, b.d_tprof.p, b.d_win.p, b.d_wcnt.p, b.d_woff.p,
-                                     b.d_wcur.p, b.d_wlist.p, b.d_plans.p, b.d_fq.p, b.d_fluc.p,
-                                     b.d_ident.p, b.d_pool.p, b.d_pool_off.p, b.d_pool_used.p,
+                                     b.d_wcur.p, b.d_kbound.p, b.d_wlist.p, b.d_plans.p, b.d_fq.p, b.d_fluc.p,
+                                     b.d_ident.p, b.d_pool.p, b.d_pool_off.p, b.d_pool_used.p, b.d_wide.p,
                                      const_cast<double*>(c.qscale())};
         CUDA_TRY(b.d_Q.ensure(sizeof(float) * (size_t)bs.qslot_total * K));
         CUDA_TRY(b.d_V.ensure(sizeof(float2) * (size_t)bs.vslot_total * K));
@@ -1266,6 +1274,8 @@ static int forward_batch_device(Core& c, const double* d_depos, const long long*
         CUDA_TRY(b.d_wcnt.ensure(sizeof(int) * (size_t)(nkeysK + 1)));
         CUDA_TRY(b.d_woff.ensure(sizeof(int) * (size_t)(nkeysK + 1)));
         CUDA_TRY(b.d_wcur.ensure(sizeof(int) * (size_t)(nkeysK + 1 + (nkeysK + 1023) / 1024)));
+        CUDA_TRY(b.d_kbound.ensure(sizeof(unsigned long long) * (size_t)nkeysK * kTileBlocks));
+        CUDA_TRY(b.d_wide.ensure((size_t)nkeysK));
         CUDA_TRY(b.d_wlist.ensure(sizeof(Visit) * (size_t)b.vcap));
         CUDA_TRY(b.d_plans.ensure(sizeof(BatchPlan) * (size_t)nch));
         CUDA_TRY(b.d_ident.ensure(sizeof(int)));
@@ -1280,8 +1290,8 @@ static int forward_batch_device(Core& c, const double* d_depos, const long long*
         }
         if (!b.h_ident) CUDA_TRY(cudaMallocHost(&b.h_ident, sizeof(int)));
         std::vector<void*> after = {b.d_Q.p, b.d_V.p, b.d_rec.p, b.d_tprof.p, b.d_win.p, b.d_wcnt.p, b.d_woff.p,
-                                    b.d_wcur.p, b.d_wlist.p, b.d_plans.p, b.d_fq.p, b.d_fluc.p,
-                                    b.d_ident.p, b.d_pool.p, b.d_pool_off.p, b.d_pool_used.p,
+                                    b.d_wcur.p, b.d_kbound.p, b.d_wlist.p, b.d_plans.p, b.d_fq.p, b.d_fluc.p,
+                                    b.d_ident.p, b.d_pool.p, b.d_pool_off.p, b.d_pool_used.p, b.d_wide.p,
                                     const_cast<double*>(c.qscale())};
         if (b.h_plans_n < (size_t)nch) {
             if (b.h_plans) cudaFreeHost(b.h_plans);
@@ -1318,13 +1328,16 @@ static int forward_batch_device(Core& c, const double* d_depos, const long long*
                 const long long nk = (long long)ne * bs.nkeys;
                 const double* dep = d_depos ? d_depos + 7 * offsets[c0] : nullptr;
                 cudaMemsetAsync(b.d_wcnt.p, 0, sizeof(int) * (size_t)(nk + 1), s);
+                cudaMemsetAsync(b.d_kbound.p, 0, sizeof(unsigned long long) * (size_t)nk * kTileBlocks, s);
+                cudaMemsetAsync(b.d_wide.p, 0, (size_t)nk, s);
                 k_win_init<<<(ne * np + 63) / 64, 64, 0, s>>>(b.d_win.as<WindowDev>(), ne * np);
                 // random streams keyed by the frame ident of each event: base (a device
                 // value written before every launch of the graph) + c0 + event
                 const FlucParams fp = fluc_params(c, true, c0, b.d_ident.as<int>());
                 launch_prep_all(dep, et, bs.nkeys, c.drifter, c.have_drifter ? 1 : 0, pset, tb, c.drift_speed,
                                 c.nsigma, b.d_rec.as<PatchRec>(), b.d_win.as<WindowDev>(), b.d_wcnt.as<int>(),
-                                b.d_tprof.as<float>(), fp, fp.on_patch ? b.d_fq.as<double>() : nullptr, s, 0, -1,
+                                b.d_tprof.as<float>(), b.d_kbound.as<unsigned long long>(), fp,
+                                fp.on_patch ? b.d_fq.as<double>() : nullptr, b.d_wide.as<unsigned char>(), s, 0, -1,
                                 c.qscale() ? c.qscale() + (size_t)offsets[c0] * np : nullptr);
                 launch_scan(b.d_wcnt.as<int>(), (int)nk, b.d_woff.as<int>(), b.d_wcur.as<int>(), s);
                 launch_plan_batch(plans + ch, bs, ne, b.d_win.as<WindowDev>(), b.vcap, s);
@@ -1341,8 +1354,9 @@ static int forward_batch_device(Core& c, const double* d_depos, const long long*
                     launch_tprof_pool(b.d_rec.as<PatchRec>(), et, np, (float)tb.bs, pool, &plans[ch].status, s);
                 }
                 launch_raster_batch(plans + ch, bs, pset, b.d_rec.as<PatchRec>(), et.dep0[ne], b.d_tprof.as<float>(),
-                                    pool, b.d_wcnt.as<int>(), b.d_woff.as<int>(), b.d_wlist.as<Visit>(), b.vcap,
-                                    b.d_Q.as<float>(), nb_r, b.maxG, et, fp, b.d_fluc.as<FlucRec>(), s);
+                                    pool, b.d_wide.as<unsigned char>(), b.d_wcnt.as<int>(), b.d_woff.as<int>(), b.d_wlist.as<Visit>(), b.vcap,
+                                    b.d_kbound.as<unsigned long long>(), b.d_Q.as<float>(), nb_r, b.maxG, et, fp,
+                                    b.d_fluc.as<FlucRec>(), s);
                 launch_rfft_batch(plans + ch, b.d_descs.as<FftDesc>(), b.d_Q.as<float>(), nb_f, b.tune.fft_threads,
                                   b.maxM, s);
                 // one launch per run of planes that share the pad and the group pairing

@@ -165,8 +165,10 @@ __global__ void __launch_bounds__(256, 3) k_prep_all(const double* __restrict__ 
                                                   DriftDev dd, int do_drift, PlaneSet ps, TimeDev tb,
                                                   double drift_speed, double nsigma, PatchRec* __restrict__ rec,
                                                   WindowDev* __restrict__ win_all, int* __restrict__ cnt_all,
-                                                  float* __restrict__ tprof, FlucParams fp, double* __restrict__ fq,
-                                                  int blk_offset, const double* __restrict__ qscale)
+                                                  float* __restrict__ tprof, unsigned long long* __restrict__ kb_all,
+                                                  FlucParams fp, double* __restrict__ fq,
+                                                  unsigned char* __restrict__ wide_all, int blk_offset,
+                                                  const double* __restrict__ qscale)
 {
     const int bid = blockIdx.x + blk_offset;  // a launch may cover a range of the table's blocks
     const int ev = event_of_block(evt, bid);
@@ -175,6 +177,7 @@ __global__ void __launch_bounds__(256, 3) k_prep_all(const double* __restrict__ 
     const bool in = i < evt.dep0[ev + 1];
     WindowDev* win = win_all + (size_t)ev * ps.nplanes;
     int* wire_cnt = cnt_all + (size_t)ev * nkeys;
+    unsigned long long* key_bound = kb_all + (size_t)ev * nkeys * kTileBlocks;
     double t = 0, q = 0, x = 0, y = 0, z = 0, el = 0, et = 0;
     bool ok = false;
     if (in) {
@@ -348,10 +351,24 @@ __global__ void __launch_bounds__(256, 3) k_prep_all(const double* __restrict__ 
         const int kspan = r.np ? (r.toff + r.nt - 1) / kTile - k0 + 1 : 0;
         count_visits(wire_cnt, pl.wire_base, w0, span, k0, kspan, ps.ntiles);
         myvis += (unsigned long long)span * (unsigned long long)kspan;
-        // the fluctuated raster sums cells in 64-bit fixed point of 2^-16 electron:
-        // a patch whose cells could reach kMaxVisitBound is refused there
-        if (r.np && fp.on_patch && visit_bound(r.qn, r.sp, r.st, (float)pl.imp_bs, (float)tb.bs) > kMaxVisitBound)
-            nbig = 1;
+        if (r.nt > kTprof) {  // keys that hold a long patch: their raster block spreads visits over warps
+            unsigned char* wk = wide_all + (size_t)ev * nkeys;
+            for (int ww = 0; ww < span; ++ww)
+                for (int kk = 0; kk < kspan; ++kk) wk[(pl.wire_base + w0 + ww) * ps.ntiles + k0 + kk] = 1;
+        }
+        // fixed-point bounds of the raster: per (wire, tile, 64-tick block), summed
+        // as integers in units of 2^-16 (each term rounded up), so the bound --
+        // and with it the raster's scale -- does not depend on the order of the adds
+        if (r.np) {
+            const float b = visit_bound(r.qn, r.sp, r.st, (float)pl.imp_bs, (float)tb.bs);
+            if (b > kMaxVisitBound) nbig = 1;
+            const unsigned long long bu = __float2ull_ru(fminf(b, kMaxVisitBound) * 65536.0f);
+            const int b0 = r.toff / kScaleBlock, b1 = (r.toff + r.nt - 1) / kScaleBlock;
+            for (int ww = 0; ww < span; ++ww) {
+                unsigned long long* kb = key_bound + (size_t)(pl.wire_base + w0 + ww) * ps.ntiles * kTileBlocks;
+                for (int bb = b0; bb <= b1; ++bb) atomicAdd(kb + bb, bu);
+            }
+        }
         // block reduction, one atomic per block per quantity
         kpmin = warp_reduce(kpmin, umin);
         ktmin = warp_reduce(ktmin, umin);
@@ -409,14 +426,16 @@ __global__ void __launch_bounds__(256, 3) k_prep_all(const double* __restrict__ 
 
 void launch_prep_all(const double* depos, const EventTable& et, int nkeys, const DriftDev& dd, int do_drift,
                      const PlaneSet& ps, const TimeDev& tb, double drift_speed, double nsigma, PatchRec* rec,
-                     WindowDev* win, int* wire_cnt, float* tprof, const FlucParams& fp, double* fq, cudaStream_t s,
-                     int blk_begin, int blk_end, const double* qscale)
+                     WindowDev* win, int* wire_cnt, float* tprof, unsigned long long* key_bound,
+                     const FlucParams& fp, double* fq, unsigned char* wide, cudaStream_t s, int blk_begin,
+                     int blk_end, const double* qscale)
 {
     const int nb = et.blk0[et.nev];
     const int b0 = std::max(0, blk_begin), b1 = blk_end < 0 ? nb : std::min(blk_end, nb);
     if (b1 <= b0) return;
     k_prep_all<<<dim3(b1 - b0, ps.nplanes), 256, 0, s>>>(depos, et, nkeys, dd, do_drift, ps, tb, drift_speed,
-                                                         nsigma, rec, win, wire_cnt, tprof, fp, fq, b0, qscale);
+                                                         nsigma, rec, win, wire_cnt, tprof, key_bound, fp, fq, wide,
+                                                         b0, qscale);
 }
 
 // Exclusive scan of the per-key visit counts: block sums, a scan of the
@@ -578,8 +597,17 @@ __global__ void __launch_bounds__(256) k_fill(const PatchRec* __restrict__ rec, 
                 if (lane == leader) base = atomicAdd(cur + key, __popc(m));
                 base = __shfl_sync(m, base, leader);
                 const int rank = __popc(m & ((1u << lane) - 1u));
+                Visit v;
+                v.toff = r.toff;
+                v.poff = r.poff;
+                v.nt_np = ((unsigned)r.nt << 16) | (unsigned)r.np;
+                v.pcr = r.pcr;
+                v.sp = r.sp;
+                v.qn = r.qn;
+                v.d = i;
+                v.pad = 0;
                 const long long at = (long long)base + rank;
-                if (at >= 0 && at < cap) list[at] = i;  // outside: the caller reports an overflow
+                if (at >= 0 && at < cap) list[at] = v;  // outside: the caller reports an overflow
             }
         }
     }
@@ -594,86 +622,116 @@ void launch_fill(const PatchRec* rec, const EventTable& et, int nkeys, const Pla
 }
 
 // ---------------------------------------------------------------------------
-// Charge grids: one block per (charge wire row, 256-tick tile) of every
-// plane.  Each patch bin adds weight*q to the group of its lower impact edge
-// and (1-weight)*q to the next (BinnedDiffusion_transform.cxx:296-367,
-// linear weights of GausDesc::weight, GaussianDiffusion.cxx:61-92).
+// Charge grids: one block per charge wire row of every plane.  The block
+// accumulates the row's impact-group x tick grid in shared memory (one thread
+// per depo visit of the wire), then writes the G rows of the plane grid with
+// zero padding up to the FFT length.  Each patch bin adds weight*q to the
+// group of its lower impact edge and (1-weight)*q to the next
+// (BinnedDiffusion_transform.cxx:296-367, linear weights of
+// GausDesc::weight, GaussianDiffusion.cxx:61-92).
 //
-// A gather, without atomics: every thread owns one tick column of the tile
-// and keeps the sums of all impact groups of that column in registers (lane =
-// tick within a 32-tick slab, warp = slab).  The tile's visits are taken 256
-// at a time: each thread stages one visit (its group coefficients -- the
-// erfc pitch bins of the wire times their linear weights -- and its time
-// profile times the charge) in shared memory and enters it in the list of
-// every slab its ticks touch; each warp then walks its slab's list, every
-// lane adding coefficient x its tick's profile value to its group sums.  The
-// sums are written once, as the tile's G rows of the plane grid, coalesced.
+// Accumulation is in 32-bit fixed point (native shared-memory integer
+// atomics; FP32 shared atomics are compare-and-swap loops).  Every 64-tick
+// block of the row has its own scale 2^30 / B, where B bounds the magnitude
+// any cell of the block can reach: the sum over the visits touching the block
+// of |q| * max bin fraction in pitch * max bin fraction in time * 2.  Cells
+// cannot overflow and one add is resolved to ~2^-30 of that local bound.
+// Integer sums are order independent (the bounds too are integer sums), so
+// the grid is bit-reproducible.
 // ---------------------------------------------------------------------------
 constexpr int kRasterThreads = 256;
-constexpr int kSlab = 32;                    // ticks per warp (one per lane)
-constexpr int kSlabs = kTile / kSlab;        // warps per block
-constexpr int kMaxG = 12;                    // impact groups (wct_dt_set_response_table refuses more)
-constexpr int kStageLd = kMaxG + kTprof;     // floats per staged visit: coefficients, then charge x time profile
-static_assert(kSlabs * 32 == kRasterThreads, "one warp per slab");
-static_assert(kStageLd % 4 == 0, "staged visits are 128-bit aligned");
+// staged per visit: 12 group coefficients, q, and 16 scaled tick values (odd stride: no bank conflicts)
+constexpr int kStageQ = 12;
+constexpr int kStageT = 13;
+constexpr int kStageStride = 29;
+constexpr int kTileLd = kTile + 8;  // row stride with an 8-word skew between groups
 
-size_t raster_smem_bytes(int)
+size_t raster_smem_bytes(int G)
 {
-    return sizeof(float) * (size_t)kRasterThreads * kStageLd + sizeof(int4) * (size_t)kRasterThreads +
-           (size_t)kSlabs * kRasterThreads;
+    return sizeof(int) * (size_t)G * kTileLd + sizeof(float) * (size_t)kRasterThreads * kStageStride +
+           sizeof(int4) * (size_t)kRasterThreads;
 }
 
 // One raster work item: charge row `row` (wire start_ch + row) of plane P and
 // absolute tick tile ktile.  Visit keys are key_base + wire * ntiles_abs +
-// tile; the visit list holds depo indices (at most vcap).  Called by all
-// threads of the block; smem_i holds the dynamic shared memory of
-// raster_smem_bytes.
+// tile; at most vcap visits exist.  Called by all threads of the block;
+// smem_i holds the dynamic shared memory of raster_smem_bytes(P.G).
 __device__ __forceinline__ void raster_tile(const GridPlane& P, int row, int ktile, int key_base, int ntiles_abs,
                                             const PatchRec* __restrict__ rec, const float* __restrict__ tprof,
-                                            const TprofPool& pool, const int* __restrict__ wire_cnt,
-                                            const int* __restrict__ wire_off, const Visit* __restrict__ visits,
-                                            long long vcap, float* __restrict__ Q, int* smem_i)
+                                            const TprofPool& pool, const unsigned char* __restrict__ wide_key,
+                                            const int* __restrict__ wire_cnt, const int* __restrict__ wire_off,
+                                            const Visit* __restrict__ visits, long long vcap,
+                                            const unsigned long long* __restrict__ key_bound,
+                                            float* __restrict__ Q, int* smem_i, float* scale, float* iscale)
 {
-    __shared__ int s_ns[kSlabs];
     __syncthreads();  // the previous item of a persistent block is done with the shared arrays
     const int w = P.start_ch + row;
-    const int nimp = P.nimp;
-    const int tick_lo = ktile * kTile;  // absolute first tick of the tile
+    const int G = P.G, nimp = P.nimp;
+    const int tick_lo = ktile * kTile;                      // absolute first tick of the tile
     const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
-    float* stage = reinterpret_cast<float*>(smem_i);                                   // [256][kStageLd]
-    int4* meta = reinterpret_cast<int4*>(stage + (size_t)kRasterThreads * kStageLd);   // [256]
-    unsigned char* slist = reinterpret_cast<unsigned char*>(meta + kRasterThreads);    // [kSlabs][256]
+    int* grid = smem_i;                                       // [G][kTileLd], column = tick - tick_lo
+    float* stage = reinterpret_cast<float*>(smem_i + (size_t)G * kTileLd);
+    int4* stagei = reinterpret_cast<int4*>(stage + (size_t)kRasterThreads * kStageStride);
     int cnt = 0;
     const Visit* list = nullptr;
+    int key = -1;
     if (w >= 0 && w < P.nwires && ktile >= 0 && ktile < ntiles_abs) {
-        const int key = key_base + (P.wire_base + w) * ntiles_abs + ktile;
+        key = key_base + (P.wire_base + w) * ntiles_abs + ktile;
         const int off = wire_off[key];
         cnt = off < 0 ? 0 : (int)min((long long)wire_cnt[key], max(0ll, vcap - off));  // no reads past the list
         list = visits + max(off, 0);
     }
-    float acc[kMaxG];
-#pragma unroll
-    for (int g = 0; g < kMaxG; ++g) acc[g] = 0.f;
-    const float pbs = P.pbs, tbs = P.tbs, inv_pbs = 1.0f / pbs;
+    if (cnt == 0) {
+        // no visit (block-uniform): the tile's G rows are zero
+        const int qc0 = tick_lo - P.col0;
+        for (int k = tid; k < G * kTile; k += kRasterThreads) {
+            const int g = k / kTile, c = k - g * kTile;
+            const int qc = qc0 + c;
+            if (qc >= 0 && qc < P.N) Q[P.qoff + ((size_t)g * P.nin + row) * P.N + qc] = 0.f;
+        }
+        return;
+    }
+    const bool spread = key >= 0 && wide_key[key];
+    {
+        int4* g4 = reinterpret_cast<int4*>(grid);
+        const int n4 = G * kTileLd / 4;
+        for (int k = tid; k < n4; k += kRasterThreads) g4[k] = make_int4(0, 0, 0, 0);
+        if (tid < kTileBlocks) {
+            const float b = key >= 0 ? __ull2float_ru(key_bound[(size_t)key * kTileBlocks + tid]) * (1.0f / 65536.0f)
+                                     : 0.f;
+            scale[tid] = b > 0.f ? 1073741824.0f / b : 0.f;
+            iscale[tid] = b > 0.f ? b / 1073741824.0f : 0.f;
+        }
+    }
+    __syncthreads();
+    const float pbs = P.pbs, tbs = P.tbs;
     const int wlo = w * nimp;
-    const int col = wid * kSlab + lane;  // this thread's tile column
-    for (int ch = 0; ch < cnt; ch += kRasterThreads) {  // block-uniform
-        if (tid < kSlabs) s_ns[tid] = 0;
-        // stage visit ch + tid: group coefficients and charge x time profile
-        const int e = ch + tid;
-        int4 m = make_int4(0, 0, -1, 0);  // cb (first patch tick - tick_lo), nt (0: nothing), pool offset, depo
-        float* my = stage + (size_t)tid * kStageLd;
+    // pass 2: each lane stages the group coefficients of one visit, then the
+    // warp scatters its 32 staged visits, two at a time (half-warp per visit,
+    // lanes over ticks, loop over the covered groups; whole warp for a pair
+    // with a visit longer than 16 ticks).
+    float* my = stage + (size_t)tid * kStageStride;
+    const int wbase = wid * 32;
+    const float inv_pbs = 1.0f / pbs;
+    const int nchunks = (cnt + kRasterThreads - 1) / kRasterThreads;
+    for (int ch = 0; ch < nchunks; ++ch) {
+        // visit of this thread: in blocks with long patches, lanes 2k, 2k+1
+        // hold consecutive visits (a pair) and consecutive pairs go to
+        // different warps (the lists hold one depo kind in runs: long patches
+        // would otherwise pile up on a few warps); elsewhere visits stay in
+        // list order (coalesced reads, alike neighbours along a track)
+        const int e = ch * kRasterThreads +
+                      (spread ? (lane >> 1) * (kRasterThreads / 16) + wid * 2 + (lane & 1) : tid);
+        int4 si = make_int4(0, 0, 0, 0);  // d, l_lo, ng, (cb << 11) | nt  (cb = toff - tick_lo, ng = 0: none)
         if (e < cnt) {
-            const int d = list[e];
-            const PatchRec r = rec[P.recoff + d];
-            const int rnp = r.np, rnt = r.nt;
+            const Visit r = list[e];
+            const int d = r.d;
+            const int rnp = (int)(r.nt_np & 0xffffu), rnt = (int)(r.nt_np >> 16);
             const int l_lo = max(r.poff, wlo) - wlo;
             const int l_hi = min(r.poff + rnp, wlo + nimp) - wlo;
-            if (l_hi > l_lo && rnt > 0) {
-                float4* my4 = reinterpret_cast<float4*>(my);
-#pragma unroll
-                for (int k4 = 0; k4 < kMaxG / 4; ++k4) my4[k4] = make_float4(0.f, 0.f, 0.f, 0.f);
+            if (l_hi > l_lo) {
                 const int ng = l_hi - l_lo + 1;
+                for (int g = 0; g < ng; ++g) my[g] = 0.f;
                 if (r.sp > 0.f) {
                     const float isg = __frcp_rn(r.sp);
                     const float inv = 0.70710678118654752f * isg;            // 1/(sqrt2 sigma)
@@ -683,7 +741,6 @@ __device__ __forceinline__ void raster_tile(const GridPlane& P, int row, int kti
                     float e1 = copysignf(erfc_nr(fabsf(x1 * inv)), x1);
                     float u1 = x1 * isg;
                     float g1 = __expf(-0.5f * u1 * u1);
-                    float carry = 0.f;  // the upper-edge share of the previous bin
                     for (int lb = 0; lb < ng - 1; ++lb) {
                         const float x2 = (float)(k0 + lb + 1) * pbs - r.pcr;
                         const float e2 = copysignf(erfc_nr(fabsf(x2 * inv)), x2);
@@ -691,98 +748,135 @@ __device__ __forceinline__ void raster_tile(const GridPlane& P, int row, int kti
                         const float g2 = __expf(-0.5f * u2 * u2);
                         const float p = bin_from_edges(e1, e2);
                         const float wt = p > 0.f ? fmaf(c0 * (g2 - g1), __fdividef(1.0f, p), x2 * inv_pbs) : 0.0f;
-                        my[l_lo + lb] = carry + p * wt;
-                        carry = p * (1.0f - wt);
+                        my[lb] += p * wt;
+                        my[lb + 1] += p * (1.0f - wt);
                         e1 = e2;
                         g1 = g2;
                     }
-                    my[l_lo + ng - 1] = carry;
                 }
                 else {
                     const float wt = (pbs - r.pcr) * inv_pbs;
-                    my[l_lo] = wt;
-                    my[l_lo + 1] = 1.0f - wt;
+                    my[0] += wt;
+                    my[1] += 1.0f - wt;
                 }
-                m.x = r.toff - tick_lo;  // may be negative for patches starting in an earlier tile
-                m.y = rnt;
-                m.w = d;
-                if (rnt <= kTprof) {
-                    // charge x time profile, the 16-value row in four 128-bit loads
+                const int cb = r.toff - tick_lo;  // may be negative for patches starting in the previous tile
+                si = make_int4(d, l_lo, ng, ((cb + 1024) << 11) | rnt);
+                my[kStageQ] = r.qn;
+                if (rnt <= 16) {
+                    // tick values scaled to the fixed point of their 64-tick block (0 outside the tile);
+                    // the whole 16-value profile row in four 128-bit loads (one L1 wavefront per
+                    // lane each, against one per value with scalar loads)
                     static_assert(kTprof == 16, "profile rows are four float4");
                     const float4* tp4 = reinterpret_cast<const float4*>(tprof + (size_t)d * kTprof);
-                    float4* dst = reinterpret_cast<float4*>(my + kMaxG);
-                    const float qn = r.qn;
+                    float tv[16];
 #pragma unroll
                     for (int k4 = 0; k4 < 4; ++k4) {
                         const float4 x = __ldg(tp4 + k4);
-                        dst[k4] = make_float4(x.x * qn, x.y * qn, x.z * qn, x.w * qn);
+                        tv[4 * k4] = x.x;
+                        tv[4 * k4 + 1] = x.y;
+                        tv[4 * k4 + 2] = x.z;
+                        tv[4 * k4 + 3] = x.w;
+                    }
+#pragma unroll
+                    for (int k = 0; k < 16; ++k) {
+                        const int c = cb + k;
+                        float v = 0.f;
+                        if (k < rnt && c >= 0 && c < kTile) v = tv[k] * r.qn * scale[c / kScaleBlock];
+                        my[kStageT + k] = v;
                     }
                 }
-                else {
-                    // a long patch: its values come from the pool (or are recomputed) per tick
-                    m.z = __ldg(pool.off + d);
-                    my[kMaxG] = r.qn;
-                    my[kMaxG + 1] = r.tcr;
-                    my[kMaxG + 2] = r.st;
+            }
+        }
+        stagei[tid] = si;
+        __syncwarp();
+        // lanes 0 .. nv-1 of this warp hold visits (e grows with the lane)
+        const int nv = __popc(__ballot_sync(0xffffffffu, e < cnt));
+        // eight visits at a time: four lanes per visit, each lane four ticks (hl + 4k)
+        const int qv = lane >> 2, hl = lane & 3;
+        for (int v0 = 0; v0 < nv; v0 += 8) {
+            const int v = v0 + qv;
+            int4 vi = make_int4(0, 0, 0, 0);
+            if (v < nv) vi = stagei[wbase + v];
+            const int nt = vi.w & 2047;
+            const bool wide = __any_sync(0xffffffffu, nt > 16);
+            if (!wide) {
+                const int ng = vi.z;
+                const int c0 = (vi.w >> 11) - 1024 + hl;  // tile column of this lane's first tick
+                const float* vc = stage + (size_t)(wbase + min(v, 31)) * kStageStride;
+                float tq[4];
+                int gl[4];  // groups this lane adds at tick hl + 4k (0: tick outside the patch or tile)
+                int mgl = 0;
+#pragma unroll
+                for (int k = 0; k < 4; ++k) {
+                    const int c = c0 + 4 * k;
+                    const bool on = hl + 4 * k < nt && c >= 0 && c < kTile;
+                    tq[k] = on ? vc[kStageT + hl + 4 * k] : 0.f;
+                    gl[k] = on ? ng : 0;
+                    mgl = max(mgl, gl[k]);
+                }
+                const int mg = __reduce_max_sync(0xffffffffu, mgl);
+                int* dst = grid + vi.y * kTileLd + c0;
+                for (int g = 0; g < mg; ++g) {
+                    const float cf = vc[g];
+#pragma unroll
+                    for (int k = 0; k < 4; ++k)
+                        if (g < gl[k]) atomicAdd(dst + 4 * k, __float2int_rn(cf * tq[k]));
+                    dst += kTileLd;
+                }
+            }
+            else {
+                // at least one of the eight has more than 16 ticks: whole warp per visit
+                for (int hv = 0; hv < 8; ++hv) {
+                    const int vv = v0 + hv;
+                    if (vv >= nv) break;
+                    const int4 wi = stagei[wbase + vv];
+                    const int ng = wi.z;
+                    if (ng == 0) continue;
+                    const int wnt = wi.w & 2047;
+                    const int cb = (wi.w >> 11) - 1024;
+                    const float* vc = stage + (size_t)(wbase + vv) * kStageStride;
+                    const float qn = vc[kStageQ];
+                    const int tstart = max(0, -cb), tend = min(wnt, kTile - cb);  // ticks inside the tile
+                    const int poff = wnt > kTprof ? __ldg(pool.off + wi.x) : -1;
+                    float rtcr = 0.f, rst = 0.f;
+                    if (wnt > kTprof && poff < 0) {
+                        const PatchRec r = rec[P.recoff + wi.x];
+                        rtcr = r.tcr;
+                        rst = r.st;
+                    }
+                    for (int tc = tstart; tc < tend; tc += 32) {
+                        const int it = tc + lane;
+                        const bool on = it < tend;
+                        float tq = 0.f;
+                        if (on) {
+                            float tv;
+                            if (wnt <= kTprof) tv = __ldg(tprof + (size_t)wi.x * kTprof + it);
+                            else if (poff >= 0) tv = __ldg(pool.val + poff + it);
+                            else tv = unit_bin(it, tbs, rtcr, rst);
+                            tq = tv * qn * scale[(cb + it) / kScaleBlock];
+                        }
+                        int* dst = grid + wi.y * kTileLd + cb + it;
+                        for (int g = 0; g < ng; ++g) {
+                            if (on) atomicAdd(dst, __float2int_rn(vc[g] * tq));
+                            dst += kTileLd;
+                        }
+                    }
                 }
             }
         }
-        meta[tid] = m;
-        __syncthreads();  // s_ns cleared, visits staged
-        // slab lists: the visit enters every slab its ticks inside the tile touch
-        {
-            const int t0 = max(m.x, 0), t1 = min(m.x + m.y, kTile);
-            const bool any = m.y > 0 && t1 > t0;
-            const int s0 = any ? t0 / kSlab : kSlabs, s1 = any ? (t1 - 1) / kSlab : -1;
-#pragma unroll
-            for (int sl = 0; sl < kSlabs; ++sl) {
-                const bool in = sl >= s0 && sl <= s1;
-                const unsigned b = __ballot_sync(0xffffffffu, in);
-                if (b) {
-                    const int leader = __ffs(b) - 1;
-                    int base = 0;
-                    if (lane == leader) base = atomicAdd(&s_ns[sl], __popc(b));
-                    base = __shfl_sync(0xffffffffu, base, leader);
-                    if (in) slist[sl * kRasterThreads + base + __popc(b & ((1u << lane) - 1u))] = (unsigned char)tid;
-                }
-            }
-        }
-        __syncthreads();
-        // this warp's slab: every lane adds coefficient x its tick's value to its group sums
-        const int nsl = s_ns[wid];
-        const unsigned char* mylist = slist + wid * kRasterThreads;
-        for (int k = 0; k < nsl; ++k) {
-            const int v = mylist[k];
-            const int4 mv = meta[v];
-            const float* sv = stage + (size_t)v * kStageLd;
-            const int i = col - mv.x;
-            float tv = 0.f;
-            if (i >= 0 && i < mv.y) {
-                if (mv.y <= kTprof) tv = sv[kMaxG + i];
-                else if (mv.z >= 0) tv = __ldg(pool.val + mv.z + i) * sv[kMaxG];
-                else tv = unit_bin(i, tbs, sv[kMaxG + 1], sv[kMaxG + 2]) * sv[kMaxG];
-            }
-            const float4* c4 = reinterpret_cast<const float4*>(sv);
-#pragma unroll
-            for (int k4 = 0; k4 < kMaxG / 4; ++k4) {
-                const float4 cf = c4[k4];
-                acc[4 * k4] = fmaf(cf.x, tv, acc[4 * k4]);
-                acc[4 * k4 + 1] = fmaf(cf.y, tv, acc[4 * k4 + 1]);
-                acc[4 * k4 + 2] = fmaf(cf.z, tv, acc[4 * k4 + 2]);
-                acc[4 * k4 + 3] = fmaf(cf.w, tv, acc[4 * k4 + 3]);
-            }
-        }
-        __syncthreads();  // the next chunk restages
+        __syncwarp();
     }
-    // the tile's G rows: grid column c is plane column tick_lo + c - col0 (zero past the window's columns)
-    const int qc = tick_lo - P.col0 + col;
-    if (qc >= 0 && qc < P.N) {
-        const bool inwin = qc < P.ncols;
-        float* q = Q + P.qoff + (size_t)row * P.N + qc;
-        const size_t gstride = (size_t)P.nin * P.N;
-#pragma unroll
-        for (int g = 0; g < kMaxG; ++g)
-            if (g < P.G) q[g * gstride] = inwin ? acc[g] : 0.f;
+    __syncthreads();
+    // write the tile's G rows: grid column c is plane column tick_lo + c - col0
+    const int qc0 = tick_lo - P.col0;
+    for (int k = tid; k < G * kTile; k += kRasterThreads) {
+        const int g = k / kTile, c = k - g * kTile;
+        const int qc = qc0 + c;
+        if (qc < 0 || qc >= P.N) continue;
+        const int ccol = tick_lo + c;                  // absolute tick
+        float v = 0.f;
+        if (ccol - P.col0 < P.ncols) v = (float)grid[g * kTileLd + c] * iscale[c / kScaleBlock];
+        Q[P.qoff + ((size_t)g * P.nin + row) * P.N + qc] = v;
     }
 }
 
@@ -791,27 +885,33 @@ __global__ void __launch_bounds__(kRasterThreads, 4) k_raster_wires(const PatchR
                                                                  const int* __restrict__ wire_cnt,
                                                                  const int* __restrict__ wire_off,
                                                                  const Visit* __restrict__ visits, long long vcap,
-                                                                 GridSet gs, float* __restrict__ Q, TprofPool pool)
+                                                                 const unsigned long long* __restrict__ key_bound,
+                                                                 GridSet gs, float* __restrict__ Q, TprofPool pool,
+                                                                 const unsigned char* __restrict__ wide_key)
 {
     extern __shared__ int smem_i[];
+    __shared__ float scale[kTileBlocks], iscale[kTileBlocks];
     int ip = 0;
     while (ip + 1 < gs.nplanes && (int)blockIdx.x >= gs.p[ip + 1].row_base) ++ip;
     const GridPlane& P = gs.p[ip];
     const int rel = blockIdx.x - P.row_base;
     const int row = rel / P.ntile;
     const int ktile = P.ktile0 + (rel - row * P.ntile);  // absolute tick tile
-    raster_tile(P, row, ktile, 0, gs.ntiles_abs, rec, tprof, pool, wire_cnt, wire_off, visits, vcap, Q, smem_i);
+    raster_tile(P, row, ktile, 0, gs.ntiles_abs, rec, tprof, pool, wide_key, wire_cnt, wire_off, visits, vcap,
+                key_bound, Q, smem_i, scale, iscale);
 }
 
-void launch_raster_wires(const PatchRec* rec, const float* tprof, const TprofPool& pool, const int* wire_cnt,
-                         const int* wire_off, const Visit* visits, long long vcap, const GridSet& gs, float* Q,
-                         cudaStream_t s)
+void launch_raster_wires(const PatchRec* rec, const float* tprof, const TprofPool& pool, const unsigned char* wide_key,
+                         const int* wire_cnt,
+                         const int* wire_off, const Visit* visits, long long vcap,
+                         const unsigned long long* key_bound, const GridSet& gs, float* Q, cudaStream_t s)
 {
     if (gs.nrows_total <= 0) return;
-    const size_t smem = raster_smem_bytes(kMaxG);
+    size_t smem = 0;
+    for (int i = 0; i < gs.nplanes; ++i) smem = std::max(smem, raster_smem_bytes(gs.p[i].G));
     cudaFuncSetAttribute((const void*)k_raster_wires, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    k_raster_wires<<<gs.nrows_total, kRasterThreads, smem, s>>>(rec, tprof, wire_cnt, wire_off, visits, vcap, gs, Q,
-                                                                pool);
+    k_raster_wires<<<gs.nrows_total, kRasterThreads, smem, s>>>(rec, tprof, wire_cnt, wire_off, visits, vcap,
+                                                                    key_bound, gs, Q, pool, wide_key);
 }
 
 // ---------------------------------------------------------------------------
@@ -905,7 +1005,6 @@ void launch_fluc_sums(const PatchRec* rec, const EventTable& et, const PlaneSet&
 // depend on the order of the adds.
 constexpr int kFlucRasterThreads = 256;
 constexpr float kFlucFix = 65536.0f;
-constexpr int kTileLd = kTile + 8;  // grid row stride with an 8-word skew between groups
 
 size_t raster_fluc_smem_bytes(int G) { return sizeof(long long) * (size_t)G * kTileLd; }
 
@@ -937,14 +1036,15 @@ __device__ __forceinline__ void raster_tile_fluc(const GridPlane& P, int ip, int
     const float pbs = P.pbs, tbs = P.tbs, inv_pbs = 1.0f / pbs;
     const int wlo = w * nimp;
     for (int e = wid; e < cnt; e += nwarps) {
-        const int d = list[e];
+        const Visit v = list[e];
+        const int d = v.d;
         const FlucRec fr = fluc[P.recoff + d];
-        const PatchRec r = rec[P.recoff + d];
-        const int rnp = r.np, rnt = r.nt;
-        const int l_lo = max(r.poff, wlo) - wlo, l_hi = min(r.poff + rnp, wlo + nimp) - wlo;
+        const int rnp = (int)(v.nt_np & 0xffffu), rnt = (int)(v.nt_np >> 16);
+        const int l_lo = max(v.poff, wlo) - wlo, l_hi = min(v.poff + rnp, wlo + nimp) - wlo;
         if (fr.scale == 0.f || l_hi <= l_lo) continue;  // warp-uniform
+        const PatchRec r = rec[P.recoff + d];
         const int nb = l_hi - l_lo;
-        const int k0 = wlo + l_lo - r.poff;  // first patch bin on this wire
+        const int k0 = wlo + l_lo - v.poff;  // first patch bin on this wire
         if (lane < nb) {
             const int k = k0 + lane;
             const float p = unit_bin(k, pbs, r.pcr, r.sp);
@@ -963,7 +1063,7 @@ __device__ __forceinline__ void raster_tile_fluc(const GridPlane& P, int ip, int
         __syncwarp();
         const int ev = event_of_depo(evt, d);
         const int ident = fluc_ident(fp, ev), i_ev = d - evt.dep0[ev];
-        const int cb = r.toff - tick_lo;
+        const int cb = v.toff - tick_lo;
         const int tstart = max(0, -cb), tend = min(rnt, kTile - cb);
         const int ntt = tend - tstart;
         if (ntt <= 0) continue;  // warp-uniform
@@ -1656,13 +1756,16 @@ __global__ void __launch_bounds__(kRasterThreads, FLUC ? 1 : 4) k_raster_batch(c
                                                                  PlaneSet ps, const PatchRec* __restrict__ rec,
                                                                  long long recstride,
                                                                  const float* __restrict__ tprof, TprofPool pool,
+                                                                 const unsigned char* __restrict__ wide_key,
                                                                  const int* __restrict__ wire_cnt,
                                                                  const int* __restrict__ wire_off,
                                                                  const Visit* __restrict__ visits, long long vcap,
+                                                                 const unsigned long long* __restrict__ key_bound,
                                                                  float* __restrict__ Q, EventTable evt, FlucParams fp,
                                                                  const FlucRec* __restrict__ fluc)
 {
     extern __shared__ int smem_i[];
+    __shared__ float scale[kTileBlocks], iscale[kTileBlocks];
     if (plan->status & kBatchSkip) return;
     __shared__ int s_item;
     const int ne = plan->nev * plan->np;
@@ -1696,23 +1799,27 @@ __global__ void __launch_bounds__(kRasterThreads, FLUC ? 1 : 4) k_raster_batch(c
                              fluc, wire_cnt, wire_off, visits, vcap, Q, reinterpret_cast<long long*>(smem_i));
         else
             raster_tile(P, row, E.ktile0 + (rel - row * E.ntile), e * bs.nkeys, bs.ntiles, rec, tprof, pool,
-                        wire_cnt, wire_off, visits, vcap, Q, smem_i);
+                        wide_key, wire_cnt, wire_off, visits, vcap, key_bound, Q, smem_i, scale, iscale);
     }
 }
 
 void launch_raster_batch(const BatchPlan* plan, const BatchStatic& bs, const PlaneSet& ps, const PatchRec* rec,
-                         long long recstride, const float* tprof, const TprofPool& pool, const int* wire_cnt,
-                         const int* wire_off, const Visit* visits, long long vcap, float* Q, int nblocks, int maxG,
-                         const EventTable& evt, const FlucParams& fp, const FlucRec* fluc, cudaStream_t s)
+                         long long recstride, const float* tprof, const TprofPool& pool,
+                         const unsigned char* wide_key, const int* wire_cnt, const int* wire_off,
+                         const Visit* visits, long long vcap, const unsigned long long* key_bound, float* Q,
+                         int nblocks, int maxG, const EventTable& evt, const FlucParams& fp, const FlucRec* fluc,
+                         cudaStream_t s)
 {
     const size_t smem = std::max(raster_smem_bytes(maxG), raster_fluc_smem_bytes(maxG));
     if (fp.on_patch)
-        k_raster_batch<true><<<nblocks, kRasterThreads, smem, s>>>(plan, bs, ps, rec, recstride, tprof, pool,
-                                                                    wire_cnt, wire_off, visits, vcap, Q, evt, fp,
+        k_raster_batch<true><<<nblocks, kRasterThreads, smem, s>>>(plan, bs, ps, rec, recstride, tprof, pool, wide_key,
+                                                                    wire_cnt,
+                                                                    wire_off, visits, vcap, key_bound, Q, evt, fp,
                                                                     fluc);
     else
         k_raster_batch<false><<<nblocks, kRasterThreads, smem, s>>>(plan, bs, ps, rec, recstride, tprof, pool,
-                                                                     wire_cnt, wire_off, visits, vcap, Q, evt, fp,
+                                                                     wide_key, wire_cnt,
+                                                                     wire_off, visits, vcap, key_bound, Q, evt, fp,
                                                                      fluc);
 }
 

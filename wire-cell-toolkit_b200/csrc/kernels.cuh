@@ -58,9 +58,15 @@ struct __align__(16) PatchRec {  // 16-byte aligned: two 128-bit loads per recor
 };
 static_assert(sizeof(PatchRec) == 32, "PatchRec layout");
 
-// One depo visit of a (wire, tick tile): the depo's index in the launch's
-// depo array (its PatchRec, time profile and pool entry are read from there).
-typedef int Visit;
+// One depo visit of a (wire, tick tile): what the raster needs of a PatchRec.
+struct __align__(16) Visit {
+    int toff, poff;
+    unsigned int nt_np;  // nt << 16 | np
+    float pcr, sp, qn;
+    int d;               // depo index (time profile, full record)
+    int pad;
+};
+static_assert(sizeof(Visit) == 32, "Visit layout");
 
 // Per-plane window reduction (BinnedDiffusion_transform.cxx:416-464).
 struct WindowDev {
@@ -69,15 +75,17 @@ struct WindowDev {
     // its patches longer than kTprof, and raster visits of all its patches
     unsigned long long wide_ticks, nvisits;
     int nadded, out_time, out_pitch, oversize;
-    int bigcharge;  // fluctuated patches whose cell bound exceeds kMaxVisitBound
+    int bigcharge;  // patches whose raster bound exceeds kMaxVisitBound
 };
 
 constexpr int kTprof = 16;        // time profiles up to this many ticks are computed once per depo
 constexpr int kTile = 256;        // ticks per charge-grid tile (one raster block per wire x tile)
+constexpr int kScaleBlock = 64;   // ticks sharing one fixed-point scale in the raster
+constexpr int kTileBlocks = kTile / kScaleBlock;
 constexpr int kMaxPatchT = 1024;  // ticks per patch
 constexpr int kMaxPatchP = 1024;  // impact bins per patch
-// Largest per-visit cell bound (2 |q| x peak bin fractions, in electrons) of
-// the fluctuated raster's 64-bit fixed-point sums (units of 2^-16).
+// Largest per-visit bound (2 |q| x peak bin fractions, in electrons) of the
+// raster's integer bound sums (units of 2^-16 in 64 bits).
 constexpr float kMaxVisitBound = 1.0e12f;
 
 // Per-plane parameters of the charge-grid stage of one event.
@@ -223,8 +231,8 @@ struct TprofPool {
 // ---- launchers (kernels.cu) ----
 void launch_prep_all(const double* depos, const EventTable& et, int nkeys, const DriftDev& dd, int do_drift,
                      const PlaneSet& ps, const TimeDev& tb, double drift_speed, double nsigma, PatchRec* rec,
-                     WindowDev* win, int* wire_cnt, float* tprof, const FlucParams& fp, double* fq, cudaStream_t s,
-                     int blk_begin = 0,
+                     WindowDev* win, int* wire_cnt, float* tprof, unsigned long long* key_bound,
+                     const FlucParams& fp, double* fq, unsigned char* wide, cudaStream_t s, int blk_begin = 0,
                      int blk_end = -1,  // blocks [blk_begin, blk_end) of the table (-1: to the end)
                      const double* qscale = nullptr);  // [depo][plane] charge scale of the table's depos, or null
 // fq (fluctuation): [plane][depo] charge each plane's patch draws from, written by the prep
@@ -241,9 +249,10 @@ void launch_tprof_pool(const PatchRec* rec, const EventTable& et, int nplanes, f
 void launch_fill(const PatchRec* rec, const EventTable& et, int nkeys, const PlaneSet& ps, int* wire_cur,
                  Visit* visits, long long cap, cudaStream_t s);
 size_t raster_smem_bytes(int G);
-void launch_raster_wires(const PatchRec* rec, const float* tprof, const TprofPool& pool, const int* wire_cnt,
-                         const int* wire_off, const Visit* visits, long long vcap, const GridSet& gs, float* Q,
-                         cudaStream_t s);
+void launch_raster_wires(const PatchRec* rec, const float* tprof, const TprofPool& pool, const unsigned char* wide_key,
+                         const int* wire_cnt,
+                         const int* wire_off, const Visit* visits, long long vcap,
+                         const unsigned long long* key_bound, const GridSet& gs, float* Q, cudaStream_t s);
 void launch_rfft_rows(const float* in, long in_ld, int in_len, float2* out, long out_ld, int nrows,
                       const FftDesc& d, cudaStream_t s);
 void launch_wire_conv(const float2* Qh, const float2* Rh, float2* Vh, int ngroups, int npad, int nrows_in,
@@ -322,9 +331,11 @@ void launch_twiddles(float2* tw, float2* twh, int M, cudaStream_t s);
 void launch_plan_batch(BatchPlan* plan, const BatchStatic& bs, int nev, const WindowDev* win, long long vcap,
                        cudaStream_t s);
 void launch_raster_batch(const BatchPlan* plan, const BatchStatic& bs, const PlaneSet& ps, const PatchRec* rec,
-                         long long recstride, const float* tprof, const TprofPool& pool, const int* wire_cnt,
-                         const int* wire_off, const Visit* visits, long long vcap, float* Q, int nblocks, int maxG,
-                         const EventTable& evt, const FlucParams& fp, const FlucRec* fluc, cudaStream_t s);
+                         long long recstride, const float* tprof, const TprofPool& pool,
+                         const unsigned char* wide_key, const int* wire_cnt, const int* wire_off,
+                         const Visit* visits, long long vcap, const unsigned long long* key_bound, float* Q,
+                         int nblocks, int maxG, const EventTable& evt, const FlucParams& fp, const FlucRec* fluc,
+                         cudaStream_t s);
 void launch_rfft_batch(const BatchPlan* plan, const FftDesc* descs, float* Q, int nblocks, int nthreads, int maxM,
                        cudaStream_t s);
 // Wire convolution of planes [ip0, ip1) (all with the same pad and pairing) in one launch.
