@@ -701,16 +701,20 @@ struct FrameRegion {
 // work that reads the plane's rows (a non-zero return aborts the call with
 // that status).
 //
-// After the raster, each plane's time FFT, wire convolution and inverse run
-// on a stream of their own (forked from s, joined back into s at the end), so
-// the planes' kernels fill one another's last waves; with stage profiling on,
-// or a plane with a long-range response (one shared workspace), they run on
-// s one plane after another.
+// fork_planes: after the raster, each plane's time FFT, wire convolution and
+// inverse run on a stream of their own (forked from s, joined back into s at
+// the end), so the planes' kernels fill one another's last waves (the
+// device-buffer call).  The host-buffer calls keep the planes one after
+// another on s instead: each plane's rows then go back while the next planes
+// are transformed, which hides more copy time than the overlap of the planes
+// saves.  With stage profiling on, or a plane with a long-range response
+// (one shared workspace), the planes always run one after another.
 static int forward_device(Core& c, const double* d_depos, size_t ndepos, float* d_frame, wct_plane_window* wins,
                           int* frame_ident, cudaStream_t s, cudaEvent_t* plane_done = nullptr,
                           cudaEvent_t zeroed = nullptr, std::vector<FrameRegion>* regions = nullptr,
                           const double* h_depos = nullptr,
-                          const std::function<int(int, const FrameRegion&, cudaStream_t)>& after_plane = nullptr)
+                          const std::function<int(int, const FrameRegion&, cudaStream_t)>& after_plane = nullptr,
+                          bool fork_planes = false)
 {
     EventPlan ev;
     int prc = prepare_event(c, d_depos, ndepos, s, ev, true, h_depos);
@@ -756,7 +760,7 @@ static int forward_device(Core& c, const double* d_depos, size_t ndepos, float* 
     CUDA_TRY(cudaGetLastError());
 
     // the planes' chains: on streams of their own unless profiling or a long-range step needs s alone
-    bool fork = !c.profiling && np > 1;
+    bool fork = fork_planes && !c.profiling && np > 1;
     for (int ip = 0; ip < np; ++ip)
         if (!c.planes[ip]->long_wf.empty()) fork = false;
     cudaEvent_t rastered = nullptr;
@@ -2343,7 +2347,8 @@ int wct_dt_forward_device(wct_depotransform* h, const double* d_depos, size_t nd
     if (!h || !d_frame || (ndepos && !d_depos)) return fail(WCT_ERR_ARG, "wct_dt_forward_device: bad arguments");
     std::lock_guard<std::mutex> lk(h->core.mtx);
     cudaStream_t s = stream ? (cudaStream_t)stream : h->core.own_stream;
-    return forward_device(h->core, d_depos, ndepos, d_frame, windows, frame_ident, s);
+    return forward_device(h->core, d_depos, ndepos, d_frame, windows, frame_ident, s, nullptr, nullptr, nullptr,
+                          nullptr, nullptr, true);
 }
 
 int wct_dt_forward(wct_depotransform* h, const double* depos, size_t ndepos, float* frame, wct_plane_window* windows,

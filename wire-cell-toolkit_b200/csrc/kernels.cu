@@ -597,17 +597,8 @@ __global__ void __launch_bounds__(256) k_fill(const PatchRec* __restrict__ rec, 
                 if (lane == leader) base = atomicAdd(cur + key, __popc(m));
                 base = __shfl_sync(m, base, leader);
                 const int rank = __popc(m & ((1u << lane) - 1u));
-                Visit v;
-                v.toff = r.toff;
-                v.poff = r.poff;
-                v.nt_np = ((unsigned)r.nt << 16) | (unsigned)r.np;
-                v.pcr = r.pcr;
-                v.sp = r.sp;
-                v.qn = r.qn;
-                v.d = i;
-                v.pad = 0;
                 const long long at = (long long)base + rank;
-                if (at >= 0 && at < cap) list[at] = v;  // outside: the caller reports an overflow
+                if (at >= 0 && at < cap) list[at] = i;  // outside: the caller reports an overflow
             }
         }
     }
@@ -724,9 +715,9 @@ __device__ __forceinline__ void raster_tile(const GridPlane& P, int row, int kti
                       (spread ? (lane >> 1) * (kRasterThreads / 16) + wid * 2 + (lane & 1) : tid);
         int4 si = make_int4(0, 0, 0, 0);  // d, l_lo, ng, (cb << 11) | nt  (cb = toff - tick_lo, ng = 0: none)
         if (e < cnt) {
-            const Visit r = list[e];
-            const int d = r.d;
-            const int rnp = (int)(r.nt_np & 0xffffu), rnt = (int)(r.nt_np >> 16);
+            const int d = list[e];
+            const PatchRec r = rec[P.recoff + d];
+            const int rnp = r.np, rnt = r.nt;
             const int l_lo = max(r.poff, wlo) - wlo;
             const int l_hi = min(r.poff + rnp, wlo + nimp) - wlo;
             if (l_hi > l_lo) {
@@ -867,16 +858,20 @@ __device__ __forceinline__ void raster_tile(const GridPlane& P, int row, int kti
         __syncwarp();
     }
     __syncthreads();
-    // write the tile's G rows: grid column c is plane column tick_lo + c - col0
+    // write the tile's G rows, four columns per thread: grid column c is plane
+    // column tick_lo + c - col0 (zero at or past the window's ncols)
     const int qc0 = tick_lo - P.col0;
-    for (int k = tid; k < G * kTile; k += kRasterThreads) {
-        const int g = k / kTile, c = k - g * kTile;
-        const int qc = qc0 + c;
-        if (qc < 0 || qc >= P.N) continue;
-        const int ccol = tick_lo + c;                  // absolute tick
-        float v = 0.f;
-        if (ccol - P.col0 < P.ncols) v = (float)grid[g * kTileLd + c] * iscale[c / kScaleBlock];
-        Q[P.qoff + ((size_t)g * P.nin + row) * P.N + qc] = v;
+    constexpr int kQuads = kTile / 4;
+    for (int k = tid; k < G * kQuads; k += kRasterThreads) {
+        const int g = k / kQuads, c = (k - g * kQuads) * 4;
+        const int4 cell = *reinterpret_cast<const int4*>(grid + g * kTileLd + c);
+        const float is = iscale[c / kScaleBlock];  // the four columns share one 64-tick block
+        float* dst = Q + P.qoff + ((size_t)g * P.nin + row) * P.N + qc0 + c;
+        const int q0 = qc0 + c;
+        const float v[4] = {(float)cell.x * is, (float)cell.y * is, (float)cell.z * is, (float)cell.w * is};
+#pragma unroll
+        for (int u = 0; u < 4; ++u)
+            if (q0 + u >= 0 && q0 + u < P.N) dst[u] = q0 + u < P.ncols ? v[u] : 0.f;
     }
 }
 
@@ -1036,15 +1031,14 @@ __device__ __forceinline__ void raster_tile_fluc(const GridPlane& P, int ip, int
     const float pbs = P.pbs, tbs = P.tbs, inv_pbs = 1.0f / pbs;
     const int wlo = w * nimp;
     for (int e = wid; e < cnt; e += nwarps) {
-        const Visit v = list[e];
-        const int d = v.d;
+        const int d = list[e];
         const FlucRec fr = fluc[P.recoff + d];
-        const int rnp = (int)(v.nt_np & 0xffffu), rnt = (int)(v.nt_np >> 16);
-        const int l_lo = max(v.poff, wlo) - wlo, l_hi = min(v.poff + rnp, wlo + nimp) - wlo;
-        if (fr.scale == 0.f || l_hi <= l_lo) continue;  // warp-uniform
         const PatchRec r = rec[P.recoff + d];
+        const int rnp = r.np, rnt = r.nt;
+        const int l_lo = max(r.poff, wlo) - wlo, l_hi = min(r.poff + rnp, wlo + nimp) - wlo;
+        if (fr.scale == 0.f || l_hi <= l_lo) continue;  // warp-uniform
         const int nb = l_hi - l_lo;
-        const int k0 = wlo + l_lo - v.poff;  // first patch bin on this wire
+        const int k0 = wlo + l_lo - r.poff;  // first patch bin on this wire
         if (lane < nb) {
             const int k = k0 + lane;
             const float p = unit_bin(k, pbs, r.pcr, r.sp);
@@ -1063,7 +1057,7 @@ __device__ __forceinline__ void raster_tile_fluc(const GridPlane& P, int ip, int
         __syncwarp();
         const int ev = event_of_depo(evt, d);
         const int ident = fluc_ident(fp, ev), i_ev = d - evt.dep0[ev];
-        const int cb = v.toff - tick_lo;
+        const int cb = r.toff - tick_lo;
         const int tstart = max(0, -cb), tend = min(rnt, kTile - cb);
         const int ntt = tend - tstart;
         if (ntt <= 0) continue;  // warp-uniform

@@ -58,15 +58,9 @@ struct __align__(16) PatchRec {  // 16-byte aligned: two 128-bit loads per recor
 };
 static_assert(sizeof(PatchRec) == 32, "PatchRec layout");
 
-// One depo visit of a (wire, tick tile): what the raster needs of a PatchRec.
-struct __align__(16) Visit {
-    int toff, poff;
-    unsigned int nt_np;  // nt << 16 | np
-    float pcr, sp, qn;
-    int d;               // depo index (time profile, full record)
-    int pad;
-};
-static_assert(sizeof(Visit) == 32, "Visit layout");
+// One depo visit of a (wire, tick tile): the depo's index in the launch's
+// depo array (its PatchRec, time profile and pool entry are read from there).
+typedef int Visit;
 
 // Per-plane window reduction (BinnedDiffusion_transform.cxx:416-464).
 struct WindowDev {
