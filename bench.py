@@ -196,6 +196,14 @@ def stage_bytes(wins, cfg, n_depos, G=11):
     return out
 
 
+WORKLOAD_TEXT = {
+    "apa": "full-APA plain forward: U/V 800 + W 960 wires, 6000 ticks, 20 muon tracks, %d depos per event per GPU, "
+           "drift+diffusion+FFT convolution",
+    "plane": "one collection plane (960 wires, 4.79 mm, 6000 ticks), %d point depos per event per GPU (5000 "
+             "electrons each, uniform in wire coordinate and drift distance), drift+diffusion+FFT convolution",
+}
+
+
 def run_b200(args):
     import torch
     rank, world, local = dist_setup(args)
@@ -203,8 +211,12 @@ def run_b200(args):
     init_group(world, "nccl")
     wct = importlib.import_module("wire-cell-toolkit_b200")
     synth = importlib.import_module("wire-cell-toolkit_b200.synth")
-    cfg = synth.apa_config()
-    depos = synth.apa_depos(seed=2 + rank)
+    if args.workload == "plane":
+        cfg = synth.plane1_config()
+        depos = synth.plane1_depos(seed=1 + rank)
+    else:
+        cfg = synth.apa_config()
+        depos = synth.apa_depos(seed=2 + rank)
     if args.depos:  # a smaller workload (profiling): the event's first depos
         depos = np.ascontiguousarray(depos[:args.depos])
     n = len(depos)
@@ -325,8 +337,7 @@ def run_b200(args):
         "dtype": "f32",
         "data": "synthetic",
         "config": {
-            "workload": "full-APA plain forward: U/V 800 + W 960 wires, 6000 ticks, 20 muon tracks, "
-                        "%d depos per event per GPU, drift+diffusion+FFT convolution" % n,
+            "workload": (WORKLOAD_TEXT[args.workload] % n),
             "depos_per_event": n,
             "planes": [dict(w) for w in wins],
             "l2": "flushed between timed steps (320 MB write, untimed)",
@@ -357,7 +368,7 @@ def run_b200(args):
         "clocks": clk,
     }
     result["frame_ticks_per_s"] = world * nrows * nticks * args.steps / (max_ms / 1e3)
-    if rank == 0 and world == 1 and not args.no_patterns:
+    if rank == 0 and world == 1 and not args.no_patterns and args.workload == "apa":
         try:
             result["patterns"] = patterns(wct, synth, torch, stream, local)
         except Exception as e:  # the headline line must print whatever happens here
@@ -643,7 +654,7 @@ def cpu_baseline(cfg, depos, gpu_frame=None, gpu_windows=None, timed=True, reps=
     med = statistics.median(t for t, _ in runs)
     stages = {k: statistics.median(st[k] for _, st in runs) for k in O.STAGES}
     return ({"value": len(depos) / med, "unit": UNIT, "cores": 1, "kind": "port",
-             "sample": "the benchmarked full-APA event (%d depos), FP32 restatement, one thread; transforms by "
+             "sample": "the benchmarked event (%d depos), FP32 restatement, one thread; transforms by "
                        "libtorch-CPU (MKL, the reference's TorchDFT backend); plane responses built once; 1 warm-up, "
                        "median of %d runs (%.2f s)" % (len(depos), reps, med),
              "seconds_median": med, "seconds_runs": [t for t, _ in runs],
@@ -663,8 +674,10 @@ def run_reference(args):
     torch.set_num_threads(1)
     O.set_fft_backend("mkl")
     synth = importlib.import_module("wire-cell-toolkit_b200.synth")
-    cfg = synth.apa_config()
-    depos = synth.apa_depos(seed=2)
+    if args.workload == "plane":
+        cfg, depos = synth.plane1_config(), synth.plane1_depos(seed=1)
+    else:
+        cfg, depos = synth.apa_config(), synth.apa_depos(seed=2)
     # every host core: each event's planes on their own threads, and as many
     # independent events at once as the remaining cores take (events share
     # nothing, as they do in the reference), bounded by a quarter of the free
@@ -692,13 +705,13 @@ def run_reference(args):
     dt = time.perf_counter() - t0
     pool.shutdown()
     value = len(depos) * nev * args.steps / dt
-    sample = ("%d full-APA events (%d depos each) at once per step, FP32 restatement, each event's planes on %d "
+    sample = ("%d events (%d depos each) at once per step, FP32 restatement, each event's planes on %d "
               "threads, transforms by libtorch-CPU (MKL), plane responses built once" % (nev, len(depos), nth))
     print(json.dumps({
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt / args.steps * 1e3,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": "full-APA plain forward, %d depos per event" % len(depos)},
+        "config": {"workload": WORKLOAD_TEXT[args.workload] % len(depos)},
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": nth * nev, "kind": "port", "sample": sample,
                          "host_cpu": host_cpu()},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -714,6 +727,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-patterns", action="store_true", help="skip the adjoint / batched / fluctuated lines")
     ap.add_argument("--no-calibration", action="store_true", help="skip the large batched calibration")
+    ap.add_argument("--workload", default="apa", choices=["apa", "plane"],
+                    help="apa: the full-APA event (default); plane: the single collection-plane workload")
     ap.add_argument("--depos", type=int, default=0,
                     help="time only the event's first DEPOS depos (a small case for profilers); 0: the whole event")
     args = ap.parse_args()

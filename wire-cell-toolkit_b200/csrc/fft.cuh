@@ -148,30 +148,84 @@ __device__ __forceinline__ void bfly(float2* v)
     else if constexpr (R == 8) bfly8<SIGN>(v);
 }
 
-// One Stockham stage: sub-transforms of length Ns grow to Ns*R.
-template <int R, int SIGN>
+// Bank swizzle of the intermediate stage buffers (float2 index; used when M
+// is a multiple of 16): the low four bits are XORed with bits 3..6, a
+// bijection inside every aligned block of 16.  Stockham stages with short
+// sub-transforms (Ns = 1, 8) write with a stride of R or R*Ns elements, which
+// in natural order puts up to 16 lanes of a half-warp on one bank pair;
+// swizzled, those writes and the contiguous reads of the next stage both
+// spread over all 32 banks.
+__device__ __forceinline__ int swz(int i) { return i ^ ((i >> 3) & 15); }
+
+// j mod Ns without a division: q = floor(j / Ns) as the high word of
+// j * ceil(2^32 / Ns), exact for j, Ns < 2^16 (the error term j * (m Ns - 2^32)
+// stays below 2^32).
+struct FastMod {
+    unsigned m;
+    int d;
+    __device__ __forceinline__ explicit FastMod(int ns) : m(0xffffffffu / (unsigned)ns + 1u), d(ns) {}
+    __device__ __forceinline__ int operator()(int j) const
+    {
+        return d == 1 ? 0 : j - (int)__umulhi((unsigned)j, m) * d;
+    }
+};
+
+// One Stockham stage: sub-transforms of length Ns grow to Ns*R.  SWI / SWO:
+// src / dst hold the swizzled order.
+template <int R, int SIGN, bool SWI, bool SWO>
 __device__ __forceinline__ void stage(const float2* __restrict__ src, float2* __restrict__ dst, int M, int Ns,
                                       const float2* __restrict__ tw, int tid, int nth)
 {
     const int nR = M / R;
     const int step = M / (Ns * R);
+    const FastMod mod(Ns);
     for (int j = tid; j < nR; j += nth) {
-        const int k = j % Ns;
+        const int k = mod(j);
         float2 v[R];
 #pragma unroll
-        for (int r = 0; r < R; ++r) v[r] = src[j + r * nR];
+        for (int r = 0; r < R; ++r) {
+            const int i = j + r * nR;
+            v[r] = src[SWI ? swz(i) : i];
+        }
         if (k) {
+            // w^1 and w^2 from the table, higher powers as products of them
+            // (two loads per item instead of R - 1; at most five factors)
+            float2 w[R];
+            w[1] = __ldg(tw + k * step);
+            if (R > 2) w[2] = __ldg(tw + 2 * k * step);
+            if (R > 3) w[3] = cmul(w[1], w[2]);
+            if (R > 4) w[4] = cmul(w[2], w[2]);
+            if (R > 5) w[5] = cmul(w[2], w[3]);
+            if (R > 6) w[6] = cmul(w[3], w[3]);
+            if (R > 7) w[7] = cmul(w[3], w[4]);
 #pragma unroll
             for (int r = 1; r < R; ++r) {
-                float2 w = __ldg(tw + k * r * step);
-                if (SIGN > 0) w.y = -w.y;
-                v[r] = cmul(v[r], w);
+                float2 wr = w[r];
+                if (SIGN > 0) wr.y = -wr.y;
+                v[r] = cmul(v[r], wr);
             }
         }
         bfly<R, SIGN>(v);
         const int base = (j - k) * R + k;
 #pragma unroll
-        for (int r = 0; r < R; ++r) dst[base + r * Ns] = v[r];
+        for (int r = 0; r < R; ++r) {
+            const int i = base + r * Ns;
+            dst[SWO ? swz(i) : i] = v[r];
+        }
+    }
+}
+
+template <int R, int SIGN>
+__device__ __forceinline__ void stage_any(const float2* __restrict__ src, float2* __restrict__ dst, int M, int Ns,
+                                          const float2* __restrict__ tw, int tid, int nth, bool swi, bool swo)
+{
+    if (swi) {
+        if (swo) stage<R, SIGN, true, true>(src, dst, M, Ns, tw, tid, nth);
+        else stage<R, SIGN, true, false>(src, dst, M, Ns, tw, tid, nth);
+    }
+    else {
+        if (swo) stage<R, SIGN, false, true>(src, dst, M, Ns, tw, tid, nth);
+        else stage<R, SIGN, false, false>(src, dst, M, Ns, tw, tid, nth);
     }
 }
 
@@ -183,22 +237,28 @@ __device__ __forceinline__ void stage(const float2* __restrict__ src, float2* __
 template <int SIGN>
 __device__ float2* fft_c2c(float2* a, float2* b, const FftDesc& d, int tid, int nth)
 {
+    // input and result in natural order; a stage's output swizzled where its
+    // writes are strided (Ns < 16) and another stage reads it
+    const bool sw = (d.M & 15) == 0;
     int Ns = 1;
+    bool swi = false;
     for (int s = 0; s < d.nst; ++s) {
         const int R = d.radix[s];
+        const bool swo = sw && s + 1 < d.nst && Ns < 16;
         switch (R) {
-            case 2: fftk::stage<2, SIGN>(a, b, d.M, Ns, d.tw, tid, nth); break;
-            case 3: fftk::stage<3, SIGN>(a, b, d.M, Ns, d.tw, tid, nth); break;
-            case 4: fftk::stage<4, SIGN>(a, b, d.M, Ns, d.tw, tid, nth); break;
-            case 5: fftk::stage<5, SIGN>(a, b, d.M, Ns, d.tw, tid, nth); break;
-            case 7: fftk::stage<7, SIGN>(a, b, d.M, Ns, d.tw, tid, nth); break;
-            default: fftk::stage<8, SIGN>(a, b, d.M, Ns, d.tw, tid, nth); break;
+            case 2: fftk::stage_any<2, SIGN>(a, b, d.M, Ns, d.tw, tid, nth, swi, swo); break;
+            case 3: fftk::stage_any<3, SIGN>(a, b, d.M, Ns, d.tw, tid, nth, swi, swo); break;
+            case 4: fftk::stage_any<4, SIGN>(a, b, d.M, Ns, d.tw, tid, nth, swi, swo); break;
+            case 5: fftk::stage_any<5, SIGN>(a, b, d.M, Ns, d.tw, tid, nth, swi, swo); break;
+            case 7: fftk::stage_any<7, SIGN>(a, b, d.M, Ns, d.tw, tid, nth, swi, swo); break;
+            default: fftk::stage_any<8, SIGN>(a, b, d.M, Ns, d.tw, tid, nth, swi, swo); break;
         }
         __syncthreads();
         float2* t = a;
         a = b;
         b = t;
         Ns *= R;
+        swi = swo;
     }
     return a;
 }

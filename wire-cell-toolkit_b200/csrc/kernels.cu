@@ -635,11 +635,14 @@ constexpr int kRasterThreads = 256;
 constexpr int kStageQ = 12;
 constexpr int kStageT = 13;
 constexpr int kStageStride = 29;
-constexpr int kTileLd = kTile + 8;  // row stride with an 8-word skew between groups
+constexpr int kTileLd = kTile + 8;  // fluctuated raster: row stride with an 8-word skew between groups
+// Forward raster grid row stride: 4 words of skew, so eight visits scattering
+// to eight consecutive group rows at the same four columns hit 32 distinct banks.
+constexpr int kGridLd = kTile + 4;
 
 size_t raster_smem_bytes(int G)
 {
-    return sizeof(int) * (size_t)G * kTileLd + sizeof(float) * (size_t)kRasterThreads * kStageStride +
+    return sizeof(int) * (size_t)G * kGridLd + sizeof(float) * (size_t)kRasterThreads * kStageStride +
            sizeof(int4) * (size_t)kRasterThreads;
 }
 
@@ -660,8 +663,8 @@ __device__ __forceinline__ void raster_tile(const GridPlane& P, int row, int kti
     const int G = P.G, nimp = P.nimp;
     const int tick_lo = ktile * kTile;                      // absolute first tick of the tile
     const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
-    int* grid = smem_i;                                       // [G][kTileLd], column = tick - tick_lo
-    float* stage = reinterpret_cast<float*>(smem_i + (size_t)G * kTileLd);
+    int* grid = smem_i;                                       // [G][kGridLd], column = tick - tick_lo
+    float* stage = reinterpret_cast<float*>(smem_i + (size_t)G * kGridLd);
     int4* stagei = reinterpret_cast<int4*>(stage + (size_t)kRasterThreads * kStageStride);
     int cnt = 0;
     const Visit* list = nullptr;
@@ -685,7 +688,7 @@ __device__ __forceinline__ void raster_tile(const GridPlane& P, int row, int kti
     const bool spread = key >= 0 && wide_key[key];
     {
         int4* g4 = reinterpret_cast<int4*>(grid);
-        const int n4 = G * kTileLd / 4;
+        const int n4 = G * kGridLd / 4;
         for (int k = tid; k < n4; k += kRasterThreads) g4[k] = make_int4(0, 0, 0, 0);
         if (tid < kTileBlocks) {
             const float b = key >= 0 ? __ull2float_ru(key_bound[(size_t)key * kTileBlocks + tid]) * (1.0f / 65536.0f)
@@ -722,7 +725,6 @@ __device__ __forceinline__ void raster_tile(const GridPlane& P, int row, int kti
             const int l_hi = min(r.poff + rnp, wlo + nimp) - wlo;
             if (l_hi > l_lo) {
                 const int ng = l_hi - l_lo + 1;
-                for (int g = 0; g < ng; ++g) my[g] = 0.f;
                 if (r.sp > 0.f) {
                     const float isg = __frcp_rn(r.sp);
                     const float inv = 0.70710678118654752f * isg;            // 1/(sqrt2 sigma)
@@ -732,6 +734,9 @@ __device__ __forceinline__ void raster_tile(const GridPlane& P, int row, int kti
                     float e1 = copysignf(erfc_nr(fabsf(x1 * inv)), x1);
                     float u1 = x1 * isg;
                     float g1 = __expf(-0.5f * u1 * u1);
+                    // group lb gets p_lb * w_lb + p_(lb-1) * (1 - w_(lb-1)): the
+                    // second term is carried in a register to the next bin
+                    float carry = 0.f;
                     for (int lb = 0; lb < ng - 1; ++lb) {
                         const float x2 = (float)(k0 + lb + 1) * pbs - r.pcr;
                         const float e2 = copysignf(erfc_nr(fabsf(x2 * inv)), x2);
@@ -739,16 +744,17 @@ __device__ __forceinline__ void raster_tile(const GridPlane& P, int row, int kti
                         const float g2 = __expf(-0.5f * u2 * u2);
                         const float p = bin_from_edges(e1, e2);
                         const float wt = p > 0.f ? fmaf(c0 * (g2 - g1), __fdividef(1.0f, p), x2 * inv_pbs) : 0.0f;
-                        my[lb] += p * wt;
-                        my[lb + 1] += p * (1.0f - wt);
+                        my[lb] = carry + p * wt;
+                        carry = p * (1.0f - wt);
                         e1 = e2;
                         g1 = g2;
                     }
+                    my[ng - 1] = carry;
                 }
                 else {
                     const float wt = (pbs - r.pcr) * inv_pbs;
-                    my[0] += wt;
-                    my[1] += 1.0f - wt;
+                    my[0] = wt;
+                    my[1] = 1.0f - wt;
                 }
                 const int cb = r.toff - tick_lo;  // may be negative for patches starting in the previous tile
                 si = make_int4(d, l_lo, ng, ((cb + 1024) << 11) | rnt);
@@ -806,13 +812,21 @@ __device__ __forceinline__ void raster_tile(const GridPlane& P, int row, int kti
                     mgl = max(mgl, gl[k]);
                 }
                 const int mg = __reduce_max_sync(0xffffffffu, mgl);
-                int* dst = grid + vi.y * kTileLd + c0;
+                // the eight visits start at spread-out groups and wrap around
+                // (visit slot qv at group qv*ng/8): visits of one track share
+                // their columns and would otherwise hit the same words together
+                int gg = (qv * ng) >> 3;
+                int* dst = grid + (vi.y + gg) * kGridLd + c0;
+                int* const wrap = grid + vi.y * kGridLd + c0;
+                int* const last = wrap + (ng - 1) * kGridLd;
                 for (int g = 0; g < mg; ++g) {
-                    const float cf = vc[g];
+                    const float cf = vc[gg];
 #pragma unroll
                     for (int k = 0; k < 4; ++k)
                         if (g < gl[k]) atomicAdd(dst + 4 * k, __float2int_rn(cf * tq[k]));
-                    dst += kTileLd;
+                    const bool w = dst == last;
+                    dst = w ? wrap : dst + kGridLd;
+                    gg = w ? 0 : gg + 1;
                 }
             }
             else {
@@ -846,10 +860,10 @@ __device__ __forceinline__ void raster_tile(const GridPlane& P, int row, int kti
                             else tv = unit_bin(it, tbs, rtcr, rst);
                             tq = tv * qn * scale[(cb + it) / kScaleBlock];
                         }
-                        int* dst = grid + wi.y * kTileLd + cb + it;
+                        int* dst = grid + wi.y * kGridLd + cb + it;
                         for (int g = 0; g < ng; ++g) {
                             if (on) atomicAdd(dst, __float2int_rn(vc[g] * tq));
-                            dst += kTileLd;
+                            dst += kGridLd;
                         }
                     }
                 }
@@ -864,7 +878,7 @@ __device__ __forceinline__ void raster_tile(const GridPlane& P, int row, int kti
     constexpr int kQuads = kTile / 4;
     for (int k = tid; k < G * kQuads; k += kRasterThreads) {
         const int g = k / kQuads, c = (k - g * kQuads) * 4;
-        const int4 cell = *reinterpret_cast<const int4*>(grid + g * kTileLd + c);
+        const int4 cell = *reinterpret_cast<const int4*>(grid + g * kGridLd + c);
         const float is = iscale[c / kScaleBlock];  // the four columns share one 64-tick block
         float* dst = Q + P.qoff + ((size_t)g * P.nin + row) * P.N + qc0 + c;
         const int q0 = qc0 + c;
@@ -1187,10 +1201,199 @@ static void allow_smem(const void* f, size_t bytes)
     if (bytes > 48 * 1024) cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
 }
 
+// ---------------------------------------------------------------------------
+// Many rows: a persistent block per SM slot loops over rows, with
+//  * the first stage (radix 8, no twiddles) run from registers: each thread
+//    loads the eight inputs of its butterfly straight from global memory,
+//    and loads them for its next row while the later stages of the current
+//    row run in shared memory (the row loads never stall the transform);
+//  * the twiddle factors of every later stage and the real-packing twiddles
+//    copied into shared memory once per block (stage s holds w^(r k) for
+//    r = 1..R-1, k < Ns at [(r-1) Ns + k]: M - 1 values over all stages).
+// Needs M % 16 == 0 (radix 8 first; swizzled stage buffers), aligned float2
+// rows, and M / 8 <= 2 * threads.
+// ---------------------------------------------------------------------------
+namespace fftk {
+template <int R, bool SWI, bool SWO>
+__device__ __forceinline__ void stage_smtw(const float2* __restrict__ src, float2* __restrict__ dst, int M, int Ns,
+                                           const float2* __restrict__ tws, int tid, int nth)
+{
+    const int nR = M / R;
+    const FastMod mod(Ns);
+    for (int j = tid; j < nR; j += nth) {
+        const int k = mod(j);
+        float2 v[R];
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+            const int i = j + r * nR;
+            v[r] = src[SWI ? swz(i) : i];
+        }
+        if (k) {
+#pragma unroll
+            for (int r = 1; r < R; ++r) v[r] = cmul(v[r], tws[(r - 1) * Ns + k]);
+        }
+        bfly<R, -1>(v);
+        const int base = (j - k) * R + k;
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+            const int i = base + r * Ns;
+            dst[SWO ? swz(i) : i] = v[r];
+        }
+    }
+}
+
+template <int R>
+__device__ __forceinline__ void stage_smtw_any(const float2* __restrict__ src, float2* __restrict__ dst, int M,
+                                               int Ns, const float2* __restrict__ tws, int tid, int nth, bool swi,
+                                               bool swo)
+{
+    if (swi) {
+        if (swo) stage_smtw<R, true, true>(src, dst, M, Ns, tws, tid, nth);
+        else stage_smtw<R, true, false>(src, dst, M, Ns, tws, tid, nth);
+    }
+    else {
+        if (swo) stage_smtw<R, false, true>(src, dst, M, Ns, tws, tid, nth);
+        else stage_smtw<R, false, false>(src, dst, M, Ns, tws, tid, nth);
+    }
+}
+}  // namespace fftk
+
+// IT: first-stage butterflies per thread (M / 8 <= IT * 256)
+template <int IT>
+__global__ void __launch_bounds__(256) k_rfft_rows_pf(const float* __restrict__ in, long in_ld, int in_len,
+                                                      float2* __restrict__ out, long out_ld, int nrows, FftDesc d)
+{
+    extern __shared__ float2 sm[];
+    const int M = d.M, tid = threadIdx.x, nth = blockDim.x;
+    float2* a = sm;
+    float2* b = sm + M;
+    float2* tws = sm + 2 * M;
+    float2* twh = sm + 3 * M;
+    {
+        int Ns = d.radix[0], off = 0;
+        for (int s = 1; s < d.nst; ++s) {
+            const int R = d.radix[s], step = M / (Ns * R), n = (R - 1) * Ns;
+            for (int e = tid; e < n; e += nth) {
+                const int r = e / Ns + 1, k = e - (r - 1) * Ns;
+                tws[off + e] = __ldg(d.tw + k * r * step);
+            }
+            off += n;
+            Ns *= R;
+        }
+        for (int k = tid; k < M; k += nth) twh[k] = __ldg(d.twh + k);
+    }
+    const int nR = M / 8;
+    float2 v[IT][8];
+    auto fetch = [&](int row) {
+        const float* x = in + (size_t)row * in_ld;
+        const float2* x2 = reinterpret_cast<const float2*>(x);
+#pragma unroll
+        for (int it = 0; it < IT; ++it) {
+            const int j = tid + it * nth;
+#pragma unroll
+            for (int q = 0; q < 8; ++q) {
+                const int m = j + q * nR, k = 2 * m;
+                float2 val = make_float2(0.f, 0.f);
+                if (j < nR) {
+                    if (k + 1 < in_len) val = __ldcs(x2 + m);  // streamed once: evict first
+                    else if (k < in_len) val.x = x[k];
+                }
+                v[it][q] = val;
+            }
+        }
+    };
+    int row = blockIdx.x;
+    if (row < nrows) fetch(row);
+    __syncthreads();  // twiddle tables
+    const bool more = d.nst > 1;
+    while (row < nrows) {
+#pragma unroll
+        for (int it = 0; it < IT; ++it) {
+            const int j = tid + it * nth;
+            if (j < nR) {
+                fftk::bfly8<-1>(v[it]);
+#pragma unroll
+                for (int q = 0; q < 8; ++q) {
+                    const int i = j * 8 + q;
+                    a[more ? fftk::swz(i) : i] = v[it][q];
+                }
+            }
+        }
+        __syncthreads();
+        const int next = row + gridDim.x;
+        if (next < nrows) fetch(next);
+        float2* src = a;
+        float2* dst = b;
+        int Ns = 8, off = 0;
+        bool swi = more;  // stage 1 wrote swizzled (its writes have stride 8)
+        for (int s = 1; s < d.nst; ++s) {
+            const int R = d.radix[s];
+            const bool swo = s + 1 < d.nst && Ns < 16;  // strided writes only while Ns < 16
+            switch (R) {
+                case 2: fftk::stage_smtw_any<2>(src, dst, M, Ns, tws + off, tid, nth, swi, swo); break;
+                case 3: fftk::stage_smtw_any<3>(src, dst, M, Ns, tws + off, tid, nth, swi, swo); break;
+                case 4: fftk::stage_smtw_any<4>(src, dst, M, Ns, tws + off, tid, nth, swi, swo); break;
+                case 5: fftk::stage_smtw_any<5>(src, dst, M, Ns, tws + off, tid, nth, swi, swo); break;
+                case 7: fftk::stage_smtw_any<7>(src, dst, M, Ns, tws + off, tid, nth, swi, swo); break;
+                default: fftk::stage_smtw_any<8>(src, dst, M, Ns, tws + off, tid, nth, swi, swo); break;
+            }
+            __syncthreads();
+            off += (R - 1) * Ns;
+            Ns *= R;
+            swi = swo;
+            float2* t = src;
+            src = dst;
+            dst = t;
+        }
+        float2* o = out + (size_t)row * out_ld;
+        for (int k = tid; k < M; k += nth) {
+            const float2 zk = src[k];
+            float2 res;
+            if (k == 0) res = make_float2(zk.x + zk.y, zk.x - zk.y);
+            else {
+                const float2 zm = cconj(src[M - k]);
+                const float2 E = make_float2(0.5f * (zk.x + zm.x), 0.5f * (zk.y + zm.y));
+                const float2 D = make_float2(0.5f * (zk.x - zm.x), 0.5f * (zk.y - zm.y));
+                res = cadd(E, cmul(twh[k], make_float2(D.y, -D.x)));
+            }
+            o[k] = res;
+        }
+        __syncthreads();  // src is the next row's stage-1 output buffer or its stage scratch
+        row = next;
+    }
+}
+
+template <int IT>
+static int rfft_pf_blocks(size_t smem)
+{
+    int dev = 0, nsm = 0, per = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return 0;
+    if (cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) return 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_rfft_rows_pf<IT>, 256, smem) != cudaSuccess) return 0;
+    return per * nsm;
+}
+
+template <int IT>
+static bool launch_rfft_pf(const float* in, long in_ld, int in_len, float2* out, long out_ld, int nrows,
+                           const FftDesc& d, cudaStream_t s)
+{
+    const size_t smem = 4 * (size_t)d.M * sizeof(float2);
+    allow_smem((const void*)k_rfft_rows_pf<IT>, smem);
+    const int grid = std::min(nrows, rfft_pf_blocks<IT>(smem));
+    if (grid <= 0 || nrows < 2 * grid) return false;  // under two rows per block: the per-row kernel
+    k_rfft_rows_pf<IT><<<grid, 256, smem, s>>>(in, in_ld, in_len, out, out_ld, nrows, d);
+    return true;
+}
+
 void launch_rfft_rows(const float* in, long in_ld, int in_len, float2* out, long out_ld, int nrows, const FftDesc& d,
                       cudaStream_t s)
 {
     if (nrows <= 0) return;
+    const bool aligned = ((reinterpret_cast<uintptr_t>(in) & 7) == 0) && (in_ld % 2 == 0);
+    if (aligned && d.M % 16 == 0 && d.nst >= 2 && d.radix[0] == 8 && 4 * (size_t)d.M * sizeof(float2) <= 128 * 1024) {
+        if (d.M / 8 <= 256 && launch_rfft_pf<1>(in, in_ld, in_len, out, out_ld, nrows, d, s)) return;
+        if (d.M / 8 > 256 && d.M / 8 <= 512 && launch_rfft_pf<2>(in, in_ld, in_len, out, out_ld, nrows, d, s)) return;
+    }
     allow_smem((const void*)k_rfft_rows, 2 * d.M * sizeof(float2));
     const int nth = d.M >= 2048 ? 512 : 256;
     k_rfft_rows<<<nrows, nth, 2 * d.M * sizeof(float2), s>>>(in, in_ld, in_len, out, out_ld, nrows, d);
@@ -1384,8 +1587,167 @@ __global__ void __launch_bounds__(32 * kConvRG) k_wire_conv_any(const float2* __
     }
 }
 
+// ---------------------------------------------------------------------------
+// The same convolution with the staging of the next group (pair) overlapped
+// with the arithmetic of the current one: 16 frequencies x 16 row groups per
+// block (128 output rows), the input rows, mirrored rows and taps of group
+// gi + 1 copied by cp.async into the second of two shared-memory buffers
+// while group gi is multiplied out of the first.  Needs 16-byte aligned
+// spectra and an even M (two frequencies per 16-byte copy).
+// ---------------------------------------------------------------------------
+constexpr int kConv2F = 16;  // frequencies per block
+constexpr int kConv2RG = 16; // row groups per block (kConvRB output rows each)
+constexpr int kConv2Rows = kConv2RG * kConvRB;
+
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem, int src_bytes)
+{
+    const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(sa), "l"(gmem), "r"(src_bytes) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
+
+template <int PAD, bool PAIR>
+constexpr size_t conv2_stage_f2()  // float2 values per pipeline stage
+{
+    return (size_t)kConv2F * ((PAIR ? 2 : 1) * (kConv2Rows + 2 * PAD) + (2 * PAD + 1));
+}
+
+template <int PAD, bool PAIR>
+__global__ void __launch_bounds__(kConv2F * kConv2RG) k_wire_conv2(const float2* __restrict__ Qh,
+                                                                  const float2* __restrict__ Rh,
+                                                                  float2* __restrict__ Vh, int G, int nin, int nout,
+                                                                  int M)
+{
+    constexpr int SROWS = kConv2Rows + 2 * PAD;
+    constexpr int NT = 2 * PAD + 1;
+    constexpr size_t STAGE = conv2_stage_f2<PAD, PAIR>();
+    extern __shared__ __align__(16) float2 conv2_smem[];
+    const int lane = threadIdx.x, rg = threadIdx.y;
+    const int tid = rg * kConv2F + lane;
+    const int f0 = blockIdx.x * kConv2F;
+    const int f = f0 + lane;
+    const int o0 = blockIdx.y * kConv2Rows;
+    const bool fok = f < M;
+    const bool dc = f == 0;
+    const int ng = PAIR ? (G + 1) / 2 : G;
+    // copy of group gi into stage buffer st: 8 16-byte pieces per row of 16 frequencies
+    auto issue = [&](int gi, int st) {
+        float2* base = conv2_smem + (size_t)st * STAGE;
+        float2* Qs = base;
+        float2* Qs2 = base + SROWS * kConv2F;
+        float2* Rs = base + (PAIR ? 2 : 1) * SROWS * kConv2F;
+        const int g = gi, g2 = G - 1 - gi;
+        const bool pair = PAIR && g2 != g;
+        const int fp = f0 + 2 * (tid & 7);           // first frequency of this thread's piece
+        const int fbytes = fp < M ? 16 : 0;          // M even: both or neither of fp, fp + 1
+        constexpr int kPieces = kConv2F / 2;
+        constexpr int nthr = kConv2F * kConv2RG;
+        for (int e = tid; e < SROWS * kPieces; e += nthr) {
+            const int srow = e / kPieces;
+            const int i = o0 - 2 * PAD + srow;
+            const bool ok = i >= 0 && i < nin && fbytes;
+            const float2* src = ok ? Qh + ((size_t)g * nin + i) * M + fp : Qh;
+            cp_async16(Qs + srow * kConv2F + 2 * (e % kPieces), src, ok ? 16 : 0);
+            if (PAIR) {
+                const bool ok2 = ok && pair;
+                const float2* src2 = ok2 ? Qh + ((size_t)g2 * nin + i) * M + fp : Qh;
+                cp_async16(Qs2 + srow * kConv2F + 2 * (e % kPieces), src2, ok2 ? 16 : 0);
+            }
+        }
+        for (int e = tid; e < NT * kPieces; e += nthr) {
+            const int jj = e / kPieces;
+            const float2* src = fbytes ? Rh + ((size_t)g * NT + jj) * M + fp : Rh;
+            cp_async16(Rs + jj * kConv2F + 2 * (e % kPieces), src, fbytes);
+        }
+        cp_async_commit();
+    };
+    float2 acc[kConvRB];
+#pragma unroll
+    for (int r = 0; r < kConvRB; ++r) acc[r] = make_float2(0.f, 0.f);
+    const int rb0 = rg * kConvRB;
+    issue(0, 0);
+    for (int gi = 0; gi < ng; ++gi) {
+        if (gi + 1 < ng) {
+            issue(gi + 1, (gi + 1) & 1);
+            cp_async_wait<1>();
+        }
+        else
+            cp_async_wait<0>();
+        __syncthreads();
+        const float2* base = conv2_smem + (size_t)(gi & 1) * STAGE;
+        const float2* Qs = base;
+        const float2* Qs2 = base + SROWS * kConv2F;
+        const float2* Rs = base + (PAIR ? 2 : 1) * SROWS * kConv2F;
+        float2 win[kConvRB], win2[kConvRB];
+#pragma unroll
+        for (int r = 0; r < kConvRB; ++r) {
+            win[r] = Qs[(rb0 + r + 2 * PAD) * kConv2F + lane];  // input row o - PAD - j at j = -PAD
+            if (PAIR) win2[r] = Qs2[(rb0 + r) * kConv2F + lane];  // input row o - PAD + j at j = -PAD
+        }
+#pragma unroll
+        for (int jj = 0; jj < NT; ++jj) {
+            const float2 rr = Rs[jj * kConv2F + lane];
+            // bin 0 packs two real spectra (DC, Nyquist): multiply component-wise there
+            const float rc = dc ? 0.f : rr.y;
+            const float ry = dc ? rr.y : rr.x;
+#pragma unroll
+            for (int r = 0; r < kConvRB; ++r) {
+                float2 q = win[r];
+                if (PAIR) q = make_float2(q.x + win2[r].x, q.y + win2[r].y);
+                acc[r].x = fmaf(rr.x, q.x, fmaf(-rc, q.y, acc[r].x));
+                acc[r].y = fmaf(ry, q.y, fmaf(rc, q.x, acc[r].y));
+            }
+            if (jj < NT - 1) {
+#pragma unroll
+                for (int r = kConvRB - 1; r > 0; --r) win[r] = win[r - 1];
+                win[0] = Qs[(rb0 + 2 * PAD - jj - 1) * kConv2F + lane];
+                if (PAIR) {
+#pragma unroll
+                    for (int r = 0; r < kConvRB - 1; ++r) win2[r] = win2[r + 1];
+                    win2[kConvRB - 1] = Qs2[(rb0 + kConvRB + jj) * kConv2F + lane];
+                }
+            }
+        }
+        __syncthreads();  // buffer gi & 1 is refilled with group gi + 2 next
+    }
+    if (fok) {
+#pragma unroll
+        for (int r = 0; r < kConvRB; ++r) {
+            const int o = o0 + rb0 + r;
+            if (o < nout) Vh[(size_t)o * M + f] = acc[r];
+        }
+    }
+}
+
 void launch_wire_conv(const float2* Qh, const float2* Rh, float2* Vh, int ngroups, int npad, int nrows_in,
                       int nrows_out, int M, bool pair, cudaStream_t s)
+{
+    if (nrows_out <= 0) return;
+    const bool al16 = ((reinterpret_cast<uintptr_t>(Qh) | reinterpret_cast<uintptr_t>(Rh)) & 15) == 0 && M % 2 == 0;
+    if (al16 && (npad == 21 || npad == 10)) {
+        dim3 grid2((M + kConv2F - 1) / kConv2F, (nrows_out + kConv2Rows - 1) / kConv2Rows);
+        dim3 block2(kConv2F, kConv2RG);
+#define WCT_CONV2(P, B)                                                                                       \
+    do {                                                                                                      \
+        const size_t sm = 2 * conv2_stage_f2<P, B>() * sizeof(float2);                                       \
+        cudaFuncSetAttribute((const void*)k_wire_conv2<P, B>, cudaFuncAttributeMaxDynamicSharedMemorySize,   \
+                             (int)sm);                                                                        \
+        k_wire_conv2<P, B><<<grid2, block2, sm, s>>>(Qh, Rh, Vh, ngroups, nrows_in, nrows_out, M);            \
+        return;                                                                                               \
+    } while (0)
+        if (npad == 10 && pair) WCT_CONV2(10, true);
+        if (npad == 10) WCT_CONV2(10, false);
+        if (npad == 21 && pair) WCT_CONV2(21, true);
+        WCT_CONV2(21, false);
+#undef WCT_CONV2
+    }
+    launch_wire_conv_tiles(Qh, Rh, Vh, ngroups, npad, nrows_in, nrows_out, M, pair, s);
+}
+
+void launch_wire_conv_tiles(const float2* Qh, const float2* Rh, float2* Vh, int ngroups, int npad, int nrows_in,
+                            int nrows_out, int M, bool pair, cudaStream_t s)
 {
     if (nrows_out <= 0) return;
     dim3 grid((M + 31) / 32, (nrows_out + kConvRows - 1) / kConvRows);

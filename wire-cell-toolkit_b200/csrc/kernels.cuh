@@ -251,6 +251,9 @@ void launch_rfft_rows(const float* in, long in_ld, int in_len, float2* out, long
                       const FftDesc& d, cudaStream_t s);
 void launch_wire_conv(const float2* Qh, const float2* Rh, float2* Vh, int ngroups, int npad, int nrows_in,
                       int nrows_out, int M, bool pair, cudaStream_t s);
+// the single-buffered 32-frequency tiles (any alignment; the fallback of launch_wire_conv)
+void launch_wire_conv_tiles(const float2* Qh, const float2* Rh, float2* Vh, int ngroups, int npad, int nrows_in,
+                            int nrows_out, int M, bool pair, cudaStream_t s);
 void launch_irfft_rows(const float2* Vh, int nrows, const FftDesc& d, int wire0, int wlo, int whi, int tick0,
                        int ncols, int nticks, float* frame, cudaStream_t s);
 
