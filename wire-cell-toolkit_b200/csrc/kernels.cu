@@ -889,7 +889,7 @@ __device__ __forceinline__ void raster_tile(const GridPlane& P, int row, int kti
     }
 }
 
-__global__ void __launch_bounds__(kRasterThreads, 4) k_raster_wires(const PatchRec* __restrict__ rec,
+__global__ void __launch_bounds__(kRasterThreads, 5) k_raster_wires(const PatchRec* __restrict__ rec,
                                                                  const float* __restrict__ tprof,
                                                                  const int* __restrict__ wire_cnt,
                                                                  const int* __restrict__ wire_off,
@@ -2108,7 +2108,7 @@ __device__ __forceinline__ int find_entry(const int* __restrict__ pre, int n, in
 }
 
 template <bool FLUC>
-__global__ void __launch_bounds__(kRasterThreads, FLUC ? 1 : 4) k_raster_batch(const BatchPlan* __restrict__ plan, BatchStatic bs,
+__global__ void __launch_bounds__(kRasterThreads, FLUC ? 1 : 5) k_raster_batch(const BatchPlan* __restrict__ plan, BatchStatic bs,
                                                                  PlaneSet ps, const PatchRec* __restrict__ rec,
                                                                  long long recstride,
                                                                  const float* __restrict__ tprof, TprofPool pool,
