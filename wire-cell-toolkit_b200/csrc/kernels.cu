@@ -716,8 +716,9 @@ __device__ __forceinline__ void raster_tile(const GridPlane& P, int row, int kti
         // list order (coalesced reads, alike neighbours along a track)
         const int e = ch * kRasterThreads +
                       (spread ? (lane >> 1) * (kRasterThreads / 16) + wid * 2 + (lane & 1) : tid);
+        const bool valid = e < cnt;
         int4 si = make_int4(0, 0, 0, 0);  // d, l_lo, ng, (cb << 11) | nt  (cb = toff - tick_lo, ng = 0: none)
-        if (e < cnt) {
+        if (valid) {
             const int d = list[e];
             const PatchRec r = rec[P.recoff + d];
             const int rnp = r.np, rnt = r.nt;
@@ -787,7 +788,7 @@ __device__ __forceinline__ void raster_tile(const GridPlane& P, int row, int kti
         stagei[tid] = si;
         __syncwarp();
         // lanes 0 .. nv-1 of this warp hold visits (e grows with the lane)
-        const int nv = __popc(__ballot_sync(0xffffffffu, e < cnt));
+        const int nv = __popc(__ballot_sync(0xffffffffu, valid));
         // eight visits at a time: four lanes per visit, each lane four ticks (hl + 4k)
         const int qv = lane >> 2, hl = lane & 3;
         for (int v0 = 0; v0 < nv; v0 += 8) {
@@ -819,14 +820,20 @@ __device__ __forceinline__ void raster_tile(const GridPlane& P, int row, int kti
                 int* dst = grid + (vi.y + gg) * kGridLd + c0;
                 int* const wrap = grid + vi.y * kGridLd + c0;
                 int* const last = wrap + (ng - 1) * kGridLd;
+                float cf = vc[gg];
                 for (int g = 0; g < mg; ++g) {
-                    const float cf = vc[gg];
+                    const bool w = dst == last;
+                    const int gn = w ? 0 : gg + 1;
+                    const float cfn = vc[gn];  // next group's coefficient, loaded ahead
+                    int v4[4];
+#pragma unroll
+                    for (int k = 0; k < 4; ++k) v4[k] = __float2int_rn(cf * tq[k]);
 #pragma unroll
                     for (int k = 0; k < 4; ++k)
-                        if (g < gl[k]) atomicAdd(dst + 4 * k, __float2int_rn(cf * tq[k]));
-                    const bool w = dst == last;
+                        if (g < gl[k]) atomicAdd(dst + 4 * k, v4[k]);
                     dst = w ? wrap : dst + kGridLd;
-                    gg = w ? 0 : gg + 1;
+                    gg = gn;
+                    cf = cfn;
                 }
             }
             else {
@@ -1214,7 +1221,8 @@ static void allow_smem(const void* f, size_t bytes)
 // rows, and M / 8 <= 2 * threads.
 // ---------------------------------------------------------------------------
 namespace fftk {
-template <int R, bool SWI, bool SWO>
+// SIGN -1 forward, +1 inverse; tws holds the stage's twiddles of that sign
+template <int R, int SIGN, bool SWI, bool SWO>
 __device__ __forceinline__ void stage_smtw(const float2* __restrict__ src, float2* __restrict__ dst, int M, int Ns,
                                            const float2* __restrict__ tws, int tid, int nth)
 {
@@ -1232,7 +1240,7 @@ __device__ __forceinline__ void stage_smtw(const float2* __restrict__ src, float
 #pragma unroll
             for (int r = 1; r < R; ++r) v[r] = cmul(v[r], tws[(r - 1) * Ns + k]);
         }
-        bfly<R, -1>(v);
+        bfly<R, SIGN>(v);
         const int base = (j - k) * R + k;
 #pragma unroll
         for (int r = 0; r < R; ++r) {
@@ -1242,19 +1250,72 @@ __device__ __forceinline__ void stage_smtw(const float2* __restrict__ src, float
     }
 }
 
-template <int R>
+template <int R, int SIGN = -1>
 __device__ __forceinline__ void stage_smtw_any(const float2* __restrict__ src, float2* __restrict__ dst, int M,
                                                int Ns, const float2* __restrict__ tws, int tid, int nth, bool swi,
                                                bool swo)
 {
     if (swi) {
-        if (swo) stage_smtw<R, true, true>(src, dst, M, Ns, tws, tid, nth);
-        else stage_smtw<R, true, false>(src, dst, M, Ns, tws, tid, nth);
+        if (swo) stage_smtw<R, SIGN, true, true>(src, dst, M, Ns, tws, tid, nth);
+        else stage_smtw<R, SIGN, true, false>(src, dst, M, Ns, tws, tid, nth);
     }
     else {
-        if (swo) stage_smtw<R, false, true>(src, dst, M, Ns, tws, tid, nth);
-        else stage_smtw<R, false, false>(src, dst, M, Ns, tws, tid, nth);
+        if (swo) stage_smtw<R, SIGN, false, true>(src, dst, M, Ns, tws, tid, nth);
+        else stage_smtw<R, SIGN, false, false>(src, dst, M, Ns, tws, tid, nth);
     }
+}
+
+// Stages 1 .. nst-1 of a transform whose first stage (radix 8) wrote src,
+// swizzled when more stages follow; returns the buffer with the result in
+// natural order.  All threads of the block call it.
+template <int SIGN>
+__device__ __forceinline__ float2* stages_after_first(float2* src, float2* dst, const FftDesc& d,
+                                                      const float2* __restrict__ tws, int tid, int nth)
+{
+    const int M = d.M;
+    int Ns = 8, off = 0;
+    bool swi = d.nst > 1;  // the first stage's writes have stride 8
+    for (int s = 1; s < d.nst; ++s) {
+        const int R = d.radix[s];
+        const bool swo = s + 1 < d.nst && Ns < 16;  // strided writes only while Ns < 16
+        switch (R) {
+            case 2: stage_smtw_any<2, SIGN>(src, dst, M, Ns, tws + off, tid, nth, swi, swo); break;
+            case 3: stage_smtw_any<3, SIGN>(src, dst, M, Ns, tws + off, tid, nth, swi, swo); break;
+            case 4: stage_smtw_any<4, SIGN>(src, dst, M, Ns, tws + off, tid, nth, swi, swo); break;
+            case 5: stage_smtw_any<5, SIGN>(src, dst, M, Ns, tws + off, tid, nth, swi, swo); break;
+            case 7: stage_smtw_any<7, SIGN>(src, dst, M, Ns, tws + off, tid, nth, swi, swo); break;
+            default: stage_smtw_any<8, SIGN>(src, dst, M, Ns, tws + off, tid, nth, swi, swo); break;
+        }
+        __syncthreads();
+        off += (R - 1) * Ns;
+        Ns *= R;
+        swi = swo;
+        float2* t = src;
+        src = dst;
+        dst = t;
+    }
+    return src;
+}
+
+// The twiddles of stages 1 .. nst-1 (conjugated for SIGN +1) and the
+// real-packing twiddles into shared memory, once per block.
+template <int SIGN>
+__device__ __forceinline__ void load_stage_twiddles(const FftDesc& d, float2* tws, float2* twh, int tid, int nth)
+{
+    const int M = d.M;
+    int Ns = d.radix[0], off = 0;
+    for (int s = 1; s < d.nst; ++s) {
+        const int R = d.radix[s], step = M / (Ns * R), n = (R - 1) * Ns;
+        for (int e = tid; e < n; e += nth) {
+            const int r = e / Ns + 1, k = e - (r - 1) * Ns;
+            float2 w = __ldg(d.tw + k * r * step);
+            if (SIGN > 0) w.y = -w.y;
+            tws[off + e] = w;
+        }
+        off += n;
+        Ns *= R;
+    }
+    for (int k = tid; k < M; k += nth) twh[k] = __ldg(d.twh + k);
 }
 }  // namespace fftk
 
@@ -1269,19 +1330,7 @@ __global__ void __launch_bounds__(256) k_rfft_rows_pf(const float* __restrict__ 
     float2* b = sm + M;
     float2* tws = sm + 2 * M;
     float2* twh = sm + 3 * M;
-    {
-        int Ns = d.radix[0], off = 0;
-        for (int s = 1; s < d.nst; ++s) {
-            const int R = d.radix[s], step = M / (Ns * R), n = (R - 1) * Ns;
-            for (int e = tid; e < n; e += nth) {
-                const int r = e / Ns + 1, k = e - (r - 1) * Ns;
-                tws[off + e] = __ldg(d.tw + k * r * step);
-            }
-            off += n;
-            Ns *= R;
-        }
-        for (int k = tid; k < M; k += nth) twh[k] = __ldg(d.twh + k);
-    }
+    fftk::load_stage_twiddles<-1>(d, tws, twh, tid, nth);
     const int nR = M / 8;
     float2 v[IT][8];
     auto fetch = [&](int row) {
@@ -1322,29 +1371,7 @@ __global__ void __launch_bounds__(256) k_rfft_rows_pf(const float* __restrict__ 
         __syncthreads();
         const int next = row + gridDim.x;
         if (next < nrows) fetch(next);
-        float2* src = a;
-        float2* dst = b;
-        int Ns = 8, off = 0;
-        bool swi = more;  // stage 1 wrote swizzled (its writes have stride 8)
-        for (int s = 1; s < d.nst; ++s) {
-            const int R = d.radix[s];
-            const bool swo = s + 1 < d.nst && Ns < 16;  // strided writes only while Ns < 16
-            switch (R) {
-                case 2: fftk::stage_smtw_any<2>(src, dst, M, Ns, tws + off, tid, nth, swi, swo); break;
-                case 3: fftk::stage_smtw_any<3>(src, dst, M, Ns, tws + off, tid, nth, swi, swo); break;
-                case 4: fftk::stage_smtw_any<4>(src, dst, M, Ns, tws + off, tid, nth, swi, swo); break;
-                case 5: fftk::stage_smtw_any<5>(src, dst, M, Ns, tws + off, tid, nth, swi, swo); break;
-                case 7: fftk::stage_smtw_any<7>(src, dst, M, Ns, tws + off, tid, nth, swi, swo); break;
-                default: fftk::stage_smtw_any<8>(src, dst, M, Ns, tws + off, tid, nth, swi, swo); break;
-            }
-            __syncthreads();
-            off += (R - 1) * Ns;
-            Ns *= R;
-            swi = swo;
-            float2* t = src;
-            src = dst;
-            dst = t;
-        }
+        float2* src = fftk::stages_after_first<-1>(a, b, d, tws, tid, nth);
         float2* o = out + (size_t)row * out_ld;
         for (int k = tid; k < M; k += nth) {
             const float2 zk = src[k];
@@ -1437,10 +1464,116 @@ __global__ void k_irfft_rows(const float2* __restrict__ Vh, int nrows, FftDesc d
     irfft_row(Vh + (size_t)row * d.M, d, frame + (size_t)W * nticks, tick0, ncols, nticks, sm);
 }
 
+// Many rows: persistent blocks (as k_rfft_rows_pf) over the rows that are
+// frame wires, each thread holding its share of the next row's packed
+// spectrum in registers while the current row is transformed; the complex
+// pre-processing of the real inverse is fused into the first (radix-8)
+// stage; twiddles in shared memory.  IT: spectrum values per thread
+// (M <= 256 IT).
+template <int IT>
+__global__ void __launch_bounds__(256) k_irfft_rows_pf(const float2* __restrict__ Vh, int r0, int r1, FftDesc d,
+                                                       int wire0, int tick0, int ncols, int nticks,
+                                                       float* __restrict__ frame)
+{
+    extern __shared__ float2 sm[];
+    const int M = d.M, tid = threadIdx.x, nth = blockDim.x;
+    float2* a = sm;
+    float2* b = sm + M;
+    float2* tws = sm + 2 * M;
+    float2* twh = sm + 3 * M;
+    fftk::load_stage_twiddles<+1>(d, tws, twh, tid, nth);
+    float2 pv[IT];
+    auto fetch = [&](int row) {
+        const float2* v = Vh + (size_t)row * M;
+#pragma unroll
+        for (int it = 0; it < IT; ++it) {
+            const int k = tid + it * nth;
+            pv[it] = k < M ? __ldcs(v + k) : make_float2(0.f, 0.f);
+        }
+    };
+    int row = r0 + blockIdx.x;
+    if (row < r1) fetch(row);
+    __syncthreads();  // twiddle tables
+    const bool more = d.nst > 1;
+    const int nR = M / 8;
+    const float sc = 1.0f / (float)M;
+    while (row < r1) {
+#pragma unroll
+        for (int it = 0; it < IT; ++it) {
+            const int k = tid + it * nth;
+            if (k < M) b[k] = pv[it];
+        }
+        __syncthreads();
+        const int next = row + gridDim.x;
+        if (next < r1) fetch(next);
+        // first stage (radix 8, no twiddles) on the pre-processed bins
+        for (int j = tid; j < nR; j += nth) {
+            float2 v[8];
+#pragma unroll
+            for (int q = 0; q < 8; ++q) {
+                const int k = j + q * nR;
+                const float2 xk = b[k];
+                if (k == 0) {
+                    v[q] = make_float2(0.5f * (xk.x + xk.y), 0.5f * (xk.x - xk.y));
+                }
+                else {
+                    const float2 xm = cconj(b[M - k]);
+                    const float2 E = make_float2(0.5f * (xk.x + xm.x), 0.5f * (xk.y + xm.y));
+                    const float2 D = make_float2(0.5f * (xk.x - xm.x), 0.5f * (xk.y - xm.y));
+                    const float2 O = cmulc(D, twh[k]);
+                    v[q] = make_float2(E.x - O.y, E.y + O.x);
+                }
+            }
+            fftk::bfly8<+1>(v);
+#pragma unroll
+            for (int q = 0; q < 8; ++q) {
+                const int i = j * 8 + q;
+                a[more ? fftk::swz(i) : i] = v[q];
+            }
+        }
+        __syncthreads();  // b is read by the first stage and written by the second
+        const float2* z = fftk::stages_after_first<+1>(a, b, d, tws, tid, nth);
+        float* f = frame + (size_t)(wire0 + row) * nticks;
+        for (int m = tid; m < M; m += nth) {
+            const float2 zz = z[m];
+            const int c0 = 2 * m;
+            const int t0 = tick0 + c0;
+            if (c0 < ncols && t0 >= 0 && t0 < nticks) f[t0] = zz.x * sc;
+            if (c0 + 1 < ncols && t0 + 1 >= 0 && t0 + 1 < nticks) f[t0 + 1] = zz.y * sc;
+        }
+        __syncthreads();  // z is the next row's spectrum or first-stage buffer
+        row = next;
+    }
+}
+
+template <int IT>
+static bool launch_irfft_pf(const float2* Vh, int r0, int r1, const FftDesc& d, int wire0, int tick0, int ncols,
+                            int nticks, float* frame, cudaStream_t s)
+{
+    const size_t smem = 4 * (size_t)d.M * sizeof(float2);
+    allow_smem((const void*)k_irfft_rows_pf<IT>, smem);
+    int dev = 0, nsm = 0, per = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return false;
+    if (cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) return false;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_irfft_rows_pf<IT>, 256, smem) != cudaSuccess) return false;
+    const int grid = std::min(r1 - r0, per * nsm);
+    if (grid <= 0 || r1 - r0 < 2 * grid) return false;  // under two rows per block: one block per row
+    k_irfft_rows_pf<IT><<<grid, 256, smem, s>>>(Vh, r0, r1, d, wire0, tick0, ncols, nticks, frame);
+    return true;
+}
+
 void launch_irfft_rows(const float2* Vh, int nrows, const FftDesc& d, int wire0, int wlo, int whi, int tick0,
                        int ncols, int nticks, float* frame, cudaStream_t s)
 {
     if (nrows <= 0) return;
+    if (d.M % 16 == 0 && d.nst >= 2 && d.radix[0] == 8 && 4 * (size_t)d.M * sizeof(float2) <= 128 * 1024) {
+        // the rows that are frame wires: wire0 + r in [wlo, whi)
+        const int r0 = std::max(0, wlo - wire0), r1 = std::min(nrows, whi - wire0);
+        if (r1 <= r0) return;
+        if (d.M <= 1024 && launch_irfft_pf<4>(Vh, r0, r1, d, wire0, tick0, ncols, nticks, frame, s)) return;
+        if (d.M > 1024 && d.M <= 2048 && launch_irfft_pf<8>(Vh, r0, r1, d, wire0, tick0, ncols, nticks, frame, s))
+            return;
+    }
     allow_smem((const void*)k_irfft_rows, 2 * d.M * sizeof(float2));
     const int nth = d.M >= 2048 ? 512 : 256;
     k_irfft_rows<<<nrows, nth, 2 * d.M * sizeof(float2), s>>>(Vh, nrows, d, wire0, wlo, whi, tick0, ncols, nticks,
