@@ -50,3 +50,28 @@ def test_convolve_rows_matches_numpy(wct, nrows, n_in, n_resp, nfft):
     got = do.cpu().numpy()
     assert rel_l2(got[:, :n_out], want) < 2e-6
     assert not got[:, n_out:].any()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("nrows,n_in,n_resp,nfft", [
+    (1500, 3000, 200, 3200),  # M = 1600: persistent forward (one first-stage butterfly per thread) and inverse
+    (1500, 6000, 200, 6400),  # M = 3200: persistent forward with two butterflies per thread, per-row inverse
+    (1500, 1700, 100, 2048),  # M = 1024: persistent forward and inverse (four values per thread)
+    (1300, 900, 100, 1000),   # M = 500, not a multiple of 16: the per-row kernels
+])
+def test_convolve_many_rows_matches_numpy(wct, nrows, n_in, n_resp, nfft):
+    """Enough rows (at least two per resident block) for the persistent row
+    transforms; each shape against numpy in float64."""
+    import torch
+    rng = np.random.default_rng(nrows + nfft)
+    x = rng.normal(size=(nrows, n_in)).astype(np.float32)
+    resp = rng.normal(size=n_resp).astype(np.float32)
+    dx = torch.from_numpy(x).cuda()
+    dr = torch.from_numpy(resp).cuda()
+    n_out = min(nfft, n_in)
+    want = _ref(x, resp, nfft, n_out)
+    do = torch.zeros((nrows, n_out), dtype=torch.float32, device="cuda")
+    wct.convolve_rows(dx.data_ptr(), n_in, nrows, n_in, dr.data_ptr(), n_resp, do.data_ptr(), n_out, n_out,
+                      nfft=nfft)
+    torch.cuda.synchronize()
+    assert rel_l2(do.cpu().numpy(), want) < 2e-6
