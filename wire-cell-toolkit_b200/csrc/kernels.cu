@@ -161,7 +161,7 @@ __device__ __forceinline__ int fluc_ident(const FlucParams& fp, int ev)
 // records [plane][depo]; plane 0's threads also write the drifted charge and
 // the time profiles indexed by the depo's position in the concatenated depo
 // array.
-__global__ void __launch_bounds__(256, 3) k_prep_all(const double* __restrict__ dep, EventTable evt, int nkeys,
+__global__ void __launch_bounds__(256, 4) k_prep_all(const double* __restrict__ dep, EventTable evt, int nkeys,
                                                   DriftDev dd, int do_drift, PlaneSet ps, TimeDev tb,
                                                   double drift_speed, double nsigma, PatchRec* __restrict__ rec,
                                                   WindowDev* __restrict__ win_all, int* __restrict__ cnt_all,
