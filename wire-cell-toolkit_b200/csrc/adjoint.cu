@@ -52,8 +52,10 @@ void launch_grad_rows(const float* gframe, int nticks, int wire0, int wlo, int w
 // ---------------------------------------------------------------------------
 // Transposed wire convolution in the (wire, frequency) domain:
 //   dQ_g[i][f] = sum_{j=-P}^{P} conj(R_g[j][f]) * G[i + P + j][f],  i in [0, nin)
-// Block: 32 frequencies x 8 row groups, 8 consecutive rows per thread, the
-// needed G rows staged in shared memory once for all groups.
+// Block: 32 frequencies x 8 row groups, 8 consecutive rows per thread with a
+// register window over the G rows staged in shared memory once for all
+// groups; the taps of group g + 1 are copied by cp.async into the second of
+// two tap buffers while group g is multiplied out of the first.
 // ---------------------------------------------------------------------------
 constexpr int kAdjRB = 8;
 constexpr int kAdjRG = 8;
@@ -64,16 +66,30 @@ __global__ void __launch_bounds__(32 * kAdjRG) k_wire_conv_adj(const float2* __r
                                                                 float2* __restrict__ dQh, int G, int PAD, int nin,
                                                                 int nout, int M)
 {
-    extern __shared__ float2 adj_smem[];
+    extern __shared__ __align__(16) float2 adj_smem[];
     const int SROWS = kAdjRows + 2 * PAD;
     const int NT = 2 * PAD + 1;
     float2(*Gs)[32] = reinterpret_cast<float2(*)[32]>(adj_smem);
-    float2(*Rs)[32] = reinterpret_cast<float2(*)[32]>(adj_smem + (size_t)SROWS * 32);
+    float2* Rbuf = adj_smem + (size_t)SROWS * 32;  // two tap buffers of NT x 32
     const int lane = threadIdx.x, rg = threadIdx.y;
-    const int f = blockIdx.x * 32 + lane;
+    const int tid = rg * 32 + lane;
+    const int f0 = blockIdx.x * 32;
+    const int f = f0 + lane;
     const int i0 = blockIdx.y * kAdjRows;
     const bool fok = f < M;
     const bool dc = f == 0;
+    // taps of group g into buffer st: 16 pieces of 16 bytes per 32-frequency row (M even)
+    auto issue = [&](int g, int st) {
+        float2* Rs = Rbuf + (size_t)st * NT * 32;
+        const int fp = f0 + 2 * (tid & 15);
+        const int nb = fp < M ? 16 : 0;
+        for (int e = tid; e < NT * 16; e += 32 * kAdjRG) {
+            const int jj = e >> 4;
+            cp_async16(Rs + jj * 32 + 2 * (e & 15), nb ? Rh + ((size_t)g * NT + jj) * M + fp : Rh, nb);
+        }
+        cp_async_commit();
+    };
+    issue(0, 0);
     // rows i0 + s of G, s in [0, SROWS): input row i uses G rows i .. i + 2P
     for (int s = rg; s < SROWS; s += kAdjRG) {
         const int o = i0 + s;
@@ -81,31 +97,43 @@ __global__ void __launch_bounds__(32 * kAdjRG) k_wire_conv_adj(const float2* __r
     }
     const int rb0 = rg * kAdjRB;
     for (int g = 0; g < G; ++g) {
-        __syncthreads();
-        for (int jj = rg; jj < NT; jj += kAdjRG)
-            Rs[jj][lane] = fok ? Rh[((size_t)g * NT + jj) * M + f] : make_float2(0.f, 0.f);
-        __syncthreads();
-        if (!fok) continue;
-        float2 acc[kAdjRB];
-#pragma unroll
-        for (int r = 0; r < kAdjRB; ++r) acc[r] = make_float2(0.f, 0.f);
-        for (int jj = 0; jj < NT; ++jj) {
-            const float2 rr = Rs[jj][lane];
-            // conj(R) * G, component-wise in bin 0
-            const float rc = dc ? 0.f : rr.y;
-            const float ry = dc ? rr.y : rr.x;
+        if (g + 1 < G) {
+            issue(g + 1, (g + 1) & 1);
+            cp_async_wait<1>();
+        }
+        else
+            cp_async_wait<0>();
+        __syncthreads();  // group g's taps (and, at g = 0, the G rows) visible to every thread
+        const float2* Rs = Rbuf + (size_t)(g & 1) * NT * 32;
+        if (fok) {
+            float2 acc[kAdjRB], win[kAdjRB];
 #pragma unroll
             for (int r = 0; r < kAdjRB; ++r) {
-                const float2 q = Gs[rb0 + r + jj][lane];
-                acc[r].x = fmaf(rr.x, q.x, fmaf(rc, q.y, acc[r].x));
-                acc[r].y = fmaf(ry, q.y, fmaf(-rc, q.x, acc[r].y));
+                acc[r] = make_float2(0.f, 0.f);
+                win[r] = Gs[rb0 + r][lane];
+            }
+            for (int jj = 0; jj < NT; ++jj) {
+                const float2 rr = Rs[jj * 32 + lane];
+                // conj(R) * G, component-wise in bin 0
+                const float rc = dc ? 0.f : rr.y;
+                const float ry = dc ? rr.y : rr.x;
+#pragma unroll
+                for (int r = 0; r < kAdjRB; ++r) {
+                    const float2 q = win[r];  // G row rb0 + r + jj
+                    acc[r].x = fmaf(rr.x, q.x, fmaf(rc, q.y, acc[r].x));
+                    acc[r].y = fmaf(ry, q.y, fmaf(-rc, q.x, acc[r].y));
+                }
+#pragma unroll
+                for (int r = 0; r < kAdjRB - 1; ++r) win[r] = win[r + 1];
+                win[kAdjRB - 1] = Gs[min(rb0 + kAdjRB + jj, SROWS - 1)][lane];
+            }
+#pragma unroll
+            for (int r = 0; r < kAdjRB; ++r) {
+                const int i = i0 + rb0 + r;
+                if (i < nin) dQh[((size_t)g * nin + i) * M + f] = acc[r];
             }
         }
-#pragma unroll
-        for (int r = 0; r < kAdjRB; ++r) {
-            const int i = i0 + rb0 + r;
-            if (i < nin) dQh[((size_t)g * nin + i) * M + f] = acc[r];
-        }
+        __syncthreads();  // buffer g & 1 is refilled with group g + 2 next
     }
 }
 
@@ -115,7 +143,7 @@ void launch_wire_conv_adj(const float2* Gh, const float2* Rh, float2* dQh, int G
     if (nin <= 0) return;
     dim3 grid((M + 31) / 32, (nin + kAdjRows - 1) / kAdjRows);
     dim3 block(32, kAdjRG);
-    const size_t smem = sizeof(float2) * 32 * ((size_t)(kAdjRows + 2 * npad) + (2 * npad + 1));
+    const size_t smem = sizeof(float2) * 32 * ((size_t)(kAdjRows + 2 * npad) + 2 * (size_t)(2 * npad + 1));
     cudaFuncSetAttribute((const void*)k_wire_conv_adj, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     k_wire_conv_adj<<<grid, block, smem, s>>>(Gh, Rh, dQh, G, npad, nin, nout, M);
 }

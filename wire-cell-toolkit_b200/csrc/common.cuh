@@ -45,4 +45,17 @@ __host__ __device__ __forceinline__ double dkey_inv(unsigned long long k)
 #endif
 }
 
+#ifdef __CUDACC__
+// Asynchronous 16-byte global -> shared copies (sm_80+ cp.async, no
+// multicast): src_bytes = 0 fills the 16 bytes with zeros and reads nothing.
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem, int src_bytes)
+{
+    const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(sa), "l"(gmem), "r"(src_bytes) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
+#endif
+
 }  // namespace wctb200

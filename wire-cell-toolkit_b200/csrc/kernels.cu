@@ -1732,14 +1732,6 @@ constexpr int kConv2F = 16;  // frequencies per block
 constexpr int kConv2RG = 16; // row groups per block (kConvRB output rows each)
 constexpr int kConv2Rows = kConv2RG * kConvRB;
 
-__device__ __forceinline__ void cp_async16(void* smem, const void* gmem, int src_bytes)
-{
-    const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(sa), "l"(gmem), "r"(src_bytes) : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
-template <int N>
-__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
 
 template <int PAD, bool PAIR>
 constexpr size_t conv2_stage_f2()  // float2 values per pipeline stage
