@@ -390,8 +390,9 @@ def run_b200(args):
         torch.distributed.destroy_process_group()
 
 
-def _time_ms(torch, stream, fn, reps=5, warm=2):
-    """Median milliseconds of fn() (device time, CUDA events on the launch stream)."""
+def _time_ms(torch, stream, fn, reps=5, warm=2, spread=False):
+    """Median milliseconds of fn() (device time, CUDA events on the launch stream);
+    with spread, also the fastest and slowest repetition."""
     for _ in range(warm):
         fn()
     torch.cuda.synchronize()
@@ -404,7 +405,8 @@ def _time_ms(torch, stream, fn, reps=5, warm=2):
         b.record(stream)
         b.synchronize()
         ts.append(a.elapsed_time(b))
-    return float(statistics.median(ts))
+    med = float(statistics.median(ts))
+    return (med, float(min(ts)), float(max(ts))) if spread else med
 
 
 def patterns(wct, synth, torch, stream, local):
@@ -449,12 +451,18 @@ def patterns(wct, synth, torch, stream, local):
                 if off[k + 1] > off[k]:
                     dtb.forward_device(db[off[k]:off[k + 1]].data_ptr(), int(off[k + 1] - off[k]),
                                        frames[k].data_ptr(), sid)
-        t_pe = _time_ms(torch, stream, per_event, reps=3, warm=1)
+        # both forms end with a host synchronisation per call (the per-event
+        # call also one per event), so host-side delays on a busy machine
+        # land in these device times: five repetitions, the median reported
+        # with the range beside it
+        t_pe, pe_lo, pe_hi = _time_ms(torch, stream, per_event, reps=5, warm=1, spread=True)
         rep = dtb.autotune_batch(db.data_ptr(), off, frames.data_ptr(), stream=sid)
-        t_b = _time_ms(torch, stream, lambda: dtb.forward_batch_device(db.data_ptr(), off, frames.data_ptr(), sid),
-                       reps=3, warm=1)
+        t_b, b_lo, b_hi = _time_ms(torch, stream,
+                                   lambda: dtb.forward_batch_device(db.data_ptr(), off, frames.data_ptr(), sid),
+                                   reps=5, warm=2, spread=True)
         nd = int(off[-1])
         r = {"workload": label, "events": len(events), "depos": nd, "per_event_ms": t_pe, "batched_ms": t_b,
+             "per_event_ms_range": [pe_lo, pe_hi], "batched_ms_range": [b_lo, b_hi],
              "speedup_batched_over_per_event": t_pe / t_b, "depos_per_s_batched": nd / (t_b / 1e3),
              "frame_ticks_per_s_batched": len(events) * nrows * nticks / (t_b / 1e3),
              "autotuned": rep["best"], "target_speedup": ">= 2"}
